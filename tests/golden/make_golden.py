@@ -1,0 +1,156 @@
+"""Generate the golden fixtures of tests/golden/ from the reference implementation.
+
+Run in a container where the reference source tree is available (it is read,
+never modified):
+
+    python tests/golden/make_golden.py /path/to/warpSPHBoundaries-checkout
+
+Writes
+  edge2d_golden_subset.json   the reference's 40-digit golden vectors (tests/fixtures/edge2d_golden.json):
+                              element cases with value, grad, moments |alpha| <= 2 and moment_grad |alpha| <= 2
+  np2d_c1.npz                 the regular 256-gon scene (radius 0.45, centre (0.5, 0.5), w4, h = 0.05): a seeded
+                              subset of particles with the twelve channels from the reference's numpy path
+                              (edge/np2d.py, whole polygon) for cubic, w2, w4, w6
+  torch2d_grad.npz            gradients of lam and the moments with respect to particle positions and polygon
+                              vertices from torch autograd through the reference's edge/torch2d.py (star polygon, w4)
+
+The reference package is imported with a stub parent package because its
+`__init__` needs the GPU stack (warp, warpSPHCore), which the CPU modules used
+here do not.
+"""
+import importlib
+import json
+import sys
+import types
+from fractions import Fraction as F
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+KERNELS = ["cubic", "w2", "w4", "w6"]
+
+
+def load_reference(root):
+    pkg = types.ModuleType("warpSPHBoundaries")
+    pkg.__path__ = [str(Path(root) / "src" / "warpSPHBoundaries")]
+    sys.modules["warpSPHBoundaries"] = pkg
+    np2d = importlib.import_module("warpSPHBoundaries.edge.np2d")
+    torch2d = importlib.import_module("warpSPHBoundaries.edge.torch2d")
+    return np2d, torch2d
+
+
+def c1_scene(n_particles=4096, seed=0):
+    """regular 256-gon of radius 0.45 around (0.5, 0.5) (vertices at angles 2 pi k / 256) and particles uniform in
+    [0.05, 0.95]^2 rejected outside the polygon (seeded)."""
+    k = np.arange(256)
+    P = np.stack([0.5 + 0.45 * np.cos(2 * np.pi * k / 256), 0.5 + 0.45 * np.sin(2 * np.pi * k / 256)], 1)
+    rng = np.random.default_rng(seed)
+    pts = []
+    while len(pts) < n_particles:
+        c = rng.uniform(0.05, 0.95, size=(4 * n_particles, 2))
+        r2 = ((c - 0.5) ** 2).sum(1)
+        # inside the polygon: the inscribed-circle test is not enough near edges; use the exact crossing rule
+        inside = _inside_polygon(c, P)
+        pts.extend(c[inside][: n_particles - len(pts)])
+    return P, np.asarray(pts[:n_particles])
+
+
+def _inside_polygon(x, P):
+    a = P
+    b = np.roll(P, -1, 0)
+    cnt = np.zeros(len(x), dtype=np.int64)
+    for i in range(len(P)):
+        ay, by = a[i, 1], b[i, 1]
+        straddle = (ay > x[:, 1]) != (by > x[:, 1])
+        xc = a[i, 0] + (x[:, 1] - ay) * (b[i, 0] - a[i, 0]) / np.where(by == ay, 1, by - ay)
+        cnt += straddle & (x[:, 0] < xc)
+    return cnt % 2 == 1
+
+
+def golden_subset(root):
+    d = json.loads((Path(root) / "tests" / "fixtures" / "edge2d_golden.json").read_text())
+    out = {"meta": {"source": "tests/fixtures/edge2d_golden.json of the reference", "format": d["meta"]["format"],
+                    "digits": d["meta"]["digits"], "conventions": d["meta"]["conventions"]}, "cases": []}
+    moms = ["1,0", "0,1", "2,0", "1,1", "0,2"]
+    grads = ["0,0", "1,0", "0,1", "2,0", "1,1", "0,2"]
+    for c in d["cases"]:
+        if c["kind"] != "element":
+            continue
+        rec = {"id": c["id"], "tags": c["tags"], "polygon": c["polygon"], "x": c["x"], "h": c["h"], "where": c["where"], "kernels": {}}
+        for k, e in c["kernels"].items():
+            rec["kernels"][k] = {"value": e["value"], "grad": e["grad"], "moments": {m: e["moments"][m] for m in moms},
+                                 "moment_grad": {g: e["moment_grad"][g] for g in grads}}
+        out["cases"].append(rec)
+    (HERE / "edge2d_golden_subset.json").write_text(json.dumps(out, indent=1))
+    print("edge2d_golden_subset.json:", len(out["cases"]), "cases")
+
+
+def np2d_c1(np2d, n_sub=384, seed=0):
+    P, X = c1_scene()
+    h = 0.05
+    rng = np.random.default_rng(seed + 1)
+    # the subset mixes near-wall particles (the interesting ones) and interior ones
+    d_wall = 0.45 * np.cos(np.pi / 256) - np.sqrt(((X - 0.5) ** 2).sum(1))
+    near = np.flatnonzero(d_wall < h)
+    far = np.flatnonzero(d_wall >= h)
+    sub = np.sort(np.concatenate([rng.choice(near, n_sub * 3 // 4, replace=False), rng.choice(far, n_sub // 4, replace=False)]))
+    xs = X[sub]
+    K = len(P)
+    out = {}
+    for k in KERNELS:
+        V = (P[None, :, :] - xs[:, None, :]) / h          # normalised coordinates: the reference functions at h = 1
+        Z = np.zeros((len(xs), 2))
+        ch = np.zeros((len(xs), 12))
+        ch[:, 0] = np2d.moment(V, Z, k, (0, 0), 1.0)
+        ch[:, 1] = np2d.moment(V, Z, k, (1, 0), 1.0) * h
+        ch[:, 2] = np2d.moment(V, Z, k, (0, 1), 1.0) * h
+        g0 = np2d.grad_moment(V, Z, k, (0, 0), 1.0)
+        g10 = np2d.grad_moment(V, Z, k, (1, 0), 1.0)
+        g01 = np2d.grad_moment(V, Z, k, (0, 1), 1.0)
+        ch[:, 3:5] = g0 / h
+        ch[:, 5:7] = g10
+        ch[:, 7:9] = g01
+        ch[:, 9] = np2d.moment(V, Z, k, (2, 0), 1.0) * h * h
+        ch[:, 10] = np2d.moment(V, Z, k, (1, 1), 1.0) * h * h
+        ch[:, 11] = np2d.moment(V, Z, k, (0, 2), 1.0) * h * h
+        out[k] = ch
+        print("np2d", k, "done")
+    np.savez_compressed(HERE / "np2d_c1.npz", polygon=P, particles=X, subset=sub, h=h, **{f"ch_{k}": v for k, v in out.items()})
+
+
+def star(n, rbar, center, jitter, rng):
+    t = 2 * np.pi * np.arange(n) / n
+    r = rbar * (1 + rng.uniform(-jitter, jitter, n))
+    return np.stack([center[0] + r * np.cos(t), center[1] + r * np.sin(t)], 1)
+
+
+def torch2d_grads(torch2d, seed=0, n_pts=96):
+    import torch
+    rng = np.random.default_rng(seed + 7)
+    P = star(128, 0.1, (0.5, 0.5), 0.15, rng)                    # ccw star polygon, 128 vertices
+    h = 0.02
+    r = np.sqrt(((P - 0.5) ** 2).sum(1))
+    ang = rng.uniform(0, 2 * np.pi, n_pts)
+    rad = np.interp(ang, 2 * np.pi * np.arange(129) / 128, np.concatenate([r, r[:1]])) + rng.uniform(-0.8 * h, 0.8 * h, n_pts)
+    X = np.stack([0.5 + rad * np.cos(ang), 0.5 + rad * np.sin(ang)], 1)
+    res = {}
+    for al in [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]:
+        Vt = torch.tensor(np.broadcast_to(P, (n_pts, 128, 2)).copy(), dtype=torch.float64, requires_grad=True)
+        Xt = torch.tensor(X, dtype=torch.float64, requires_grad=True)
+        m = torch2d.moment(Vt, Xt, "w4", al, h)
+        m.sum().backward()
+        key = f"{al[0]}{al[1]}"
+        res[f"m_{key}"] = m.detach().numpy()
+        res[f"dx_{key}"] = Xt.grad.numpy()
+        res[f"dv_{key}"] = Vt.grad.numpy()
+        print("torch2d", al, "done")
+    np.savez_compressed(HERE / "torch2d_grad.npz", polygon=P, particles=X, h=h, **res)
+
+
+if __name__ == "__main__":
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    np2d, torch2d = load_reference(root)
+    golden_subset(root)
+    np2d_c1(np2d)
+    torch2d_grads(torch2d)

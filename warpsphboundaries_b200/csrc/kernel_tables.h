@@ -1,0 +1,536 @@
+// GENERATED by warpsphboundaries_b200/kernels.py (emit_header); do not edit by hand.
+// Exact rational kernel profiles rounded once to double; see that module for the algebra.
+#pragma once
+
+namespace wsb {
+
+constexpr int kNumKernels = 7;
+constexpr int kMaxA = 14;   // A_n, n = 0 .. kMaxA-1
+
+struct BlockSums {      // per (pair, block) chord sums, before the 1/pi and the edge frame
+  double W0, W1;        // int P ds, int s P ds
+  double P0, P1;        // int Psi ds, int s Psi ds
+  double Lreg, Preg;    // int M/r^2 ds, int MPsi/r^2 ds (regular parts of the value terms)
+  double Mhat, MPhat;   // singular coefficients M(R), MPsi(R)
+};
+
+struct AdjSums {        // per (pair, block) chord sums of the adjoint
+  double W0, W1, W2, W3;   // int s^j P ds, j = 0..3
+};
+
+// ---- cubic: C2*pi = 80/7, plane second moment 31/392
+struct Kern_cubic {
+  static constexpr int kId = 0;
+  static constexpr int kBlocks = 2;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.07908163265306123;
+  static constexpr double kR[kBlocks] = {1.0, 0.5};
+  static constexpr int kNA[kBlocks] = {6, 6};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {6, 6};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_cubic::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['80/7', '-240/7', '240/7', '-80/7']
+  o.W0 = 11.428571428571429*A[0] + -34.285714285714285*A[1] + 34.285714285714285*A[2] + -11.428571428571429*A[3];
+  o.W1 = (fma(fma(fma(fma(fma(-2.2857142857142856, rhi, 8.571428571428571), rhi, -11.428571428571429), rhi, 5.714285714285714), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(-2.2857142857142856, rlo, 8.571428571428571), rlo, -11.428571428571429), rlo, 5.714285714285714), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.5714285714285714*A[0] + 5.714285714285714*A[2] + -11.428571428571429*A[3] + 8.571428571428571*A[4] + -2.2857142857142856*A[5];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(-0.32653061224489793, rhi, 1.4285714285714286), rhi, -2.2857142857142856), rhi, 1.4285714285714286), rhi, 0.0), rhi, -0.2857142857142857), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-0.32653061224489793, rlo, 1.4285714285714286), rlo, -2.2857142857142856), rlo, 1.4285714285714286), rlo, 0.0), rlo, -0.2857142857142857), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 5.714285714285714*A[0] + -11.428571428571429*A[1] + 8.571428571428571*A[2] + -2.2857142857142856*A[3];
+  o.Preg = -0.2857142857142857*A[0] + 1.4285714285714286*A[2] + -2.2857142857142856*A[3] + 1.4285714285714286*A[4] + -0.32653061224489793*A[5];
+  o.Mhat = 0.5714285714285714;
+  o.MPhat = -0.04081632653061224;
+}
+template <> __host__ __device__ __forceinline__ void Kern_cubic::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 11.428571428571429*A[0] + -34.285714285714285*A[1] + 34.285714285714285*A[2] + -11.428571428571429*A[3];
+  const double a2 = 11.428571428571429*A[2] + -34.285714285714285*A[3] + 34.285714285714285*A[4] + -11.428571428571429*A[5];
+  const double m1 = (fma(fma(fma(fma(fma(-2.2857142857142856, rhi, 8.571428571428571), rhi, -11.428571428571429), rhi, 5.714285714285714), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(-2.2857142857142856, rlo, 8.571428571428571), rlo, -11.428571428571429), rlo, 5.714285714285714), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(-1.6326530612244898, rhi, 5.714285714285714), rhi, -6.857142857142857), rhi, 2.857142857142857), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-1.6326530612244898, rlo, 5.714285714285714), rlo, -6.857142857142857), rlo, 2.857142857142857), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+template <> __host__ __device__ __forceinline__ void Kern_cubic::sums<1>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1/2: P = ['-40/7', '240/7', '-480/7', '320/7']
+  o.W0 = -5.714285714285714*A[0] + 34.285714285714285*A[1] + -68.57142857142857*A[2] + 45.714285714285715*A[3];
+  o.W1 = (fma(fma(fma(fma(fma(9.142857142857142, rhi, -17.142857142857142), rhi, 11.428571428571429), rhi, -2.857142857142857), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(9.142857142857142, rlo, -17.142857142857142), rlo, 11.428571428571429), rlo, -2.857142857142857), rlo, 0.0), rlo, 0.0));
+  o.P0 = 0.07142857142857142*A[0] + -2.857142857142857*A[2] + 11.428571428571429*A[3] + -17.142857142857142*A[4] + 9.142857142857142*A[5];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(1.3061224489795917, rhi, -2.857142857142857), rhi, 2.2857142857142856), rhi, -0.7142857142857143), rhi, 0.0), rhi, 0.03571428571428571), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(1.3061224489795917, rlo, -2.857142857142857), rlo, 2.2857142857142856), rlo, -0.7142857142857143), rlo, 0.0), rlo, 0.03571428571428571), rlo, 0.0), rlo, 0.0));
+  o.Lreg = -2.857142857142857*A[0] + 11.428571428571429*A[1] + -17.142857142857142*A[2] + 9.142857142857142*A[3];
+  o.Preg = 0.03571428571428571*A[0] + -0.7142857142857143*A[2] + 2.2857142857142856*A[3] + -2.857142857142857*A[4] + 1.3061224489795917*A[5];
+  o.Mhat = -0.07142857142857142;
+  o.MPhat = 0.0012755102040816326;
+}
+template <> __host__ __device__ __forceinline__ void Kern_cubic::adj<1>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = -5.714285714285714*A[0] + 34.285714285714285*A[1] + -68.57142857142857*A[2] + 45.714285714285715*A[3];
+  const double a2 = -5.714285714285714*A[2] + 34.285714285714285*A[3] + -68.57142857142857*A[4] + 45.714285714285715*A[5];
+  const double m1 = (fma(fma(fma(fma(fma(9.142857142857142, rhi, -17.142857142857142), rhi, 11.428571428571429), rhi, -2.857142857142857), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(9.142857142857142, rlo, -17.142857142857142), rlo, 11.428571428571429), rlo, -2.857142857142857), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(6.530612244897959, rhi, -11.428571428571429), rhi, 6.857142857142857), rhi, -1.4285714285714286), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(6.530612244897959, rlo, -11.428571428571429), rlo, 6.857142857142857), rlo, -1.4285714285714286), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- w2: C2*pi = 7, plane second moment 5/72
+struct Kern_w2 {
+  static constexpr int kId = 1;
+  static constexpr int kBlocks = 1;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.06944444444444445;
+  static constexpr double kR[kBlocks] = {1.0};
+  static constexpr int kNA[kBlocks] = {8};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {8};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_w2::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['7', '0', '-70', '140', '-105', '28']
+  o.W0 = 7.0*A[0] + -70.0*A[2] + 140.0*A[3] + -105.0*A[4] + 28.0*A[5];
+  o.W1 = (fma(fma(fma(fma(fma(fma(fma(4.0, rhi, -17.5), rhi, 28.0), rhi, -17.5), rhi, 0.0), rhi, 3.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(4.0, rlo, -17.5), rlo, 28.0), rlo, -17.5), rlo, 0.0), rlo, 3.5), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.5*A[0] + 3.5*A[2] + -17.5*A[4] + 28.0*A[5] + -17.5*A[6] + 4.0*A[7];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(0.4444444444444444, rhi, -2.1875), rhi, 4.0), rhi, -2.9166666666666665), rhi, 0.0), rhi, 0.875), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(0.4444444444444444, rlo, -2.1875), rlo, 4.0), rlo, -2.9166666666666665), rlo, 0.0), rlo, 0.875), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 3.5*A[0] + -17.5*A[2] + 28.0*A[3] + -17.5*A[4] + 4.0*A[5];
+  o.Preg = -0.25*A[0] + 0.875*A[2] + -2.9166666666666665*A[4] + 4.0*A[5] + -2.1875*A[6] + 0.4444444444444444*A[7];
+  o.Mhat = 0.5;
+  o.MPhat = -0.034722222222222224;
+}
+template <> __host__ __device__ __forceinline__ void Kern_w2::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 7.0*A[0] + -70.0*A[2] + 140.0*A[3] + -105.0*A[4] + 28.0*A[5];
+  const double a2 = 7.0*A[2] + -70.0*A[4] + 140.0*A[5] + -105.0*A[6] + 28.0*A[7];
+  const double m1 = (fma(fma(fma(fma(fma(fma(fma(4.0, rhi, -17.5), rhi, 28.0), rhi, -17.5), rhi, 0.0), rhi, 3.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(4.0, rlo, -17.5), rlo, 28.0), rlo, -17.5), rlo, 0.0), rlo, 3.5), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.111111111111111, rhi, -13.125), rhi, 20.0), rhi, -11.666666666666666), rhi, 0.0), rhi, 1.75), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.111111111111111, rlo, -13.125), rlo, 20.0), rlo, -11.666666666666666), rlo, 0.0), rlo, 1.75), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- w4: C2*pi = 9, plane second moment 7/132
+struct Kern_w4 {
+  static constexpr int kId = 2;
+  static constexpr int kBlocks = 1;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.05303030303030303;
+  static constexpr double kR[kBlocks] = {1.0};
+  static constexpr int kNA[kBlocks] = {11};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {11};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_w4::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['9', '0', '-84', '0', '630', '-1344', '1260', '-576', '105']
+  o.W0 = 9.0*A[0] + -84.0*A[2] + 630.0*A[4] + -1344.0*A[5] + 1260.0*A[6] + -576.0*A[7] + 105.0*A[8];
+  o.W1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rhi, -64.0), rhi, 157.5), rhi, -192.0), rhi, 105.0), rhi, 0.0), rhi, -21.0), rhi, 0.0), rhi, 4.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rlo, -64.0), rlo, 157.5), rlo, -192.0), rlo, 105.0), rlo, 0.0), rlo, -21.0), rlo, 0.0), rlo, 4.5), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.5*A[0] + 4.5*A[2] + -21.0*A[4] + 105.0*A[6] + -192.0*A[7] + 157.5*A[8] + -64.0*A[9] + 10.5*A[10];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.875, rhi, -5.818181818181818), rhi, 15.75), rhi, -21.333333333333332), rhi, 13.125), rhi, 0.0), rhi, -3.5), rhi, 0.0), rhi, 1.125), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.875, rlo, -5.818181818181818), rlo, 15.75), rlo, -21.333333333333332), rlo, 13.125), rlo, 0.0), rlo, -3.5), rlo, 0.0), rlo, 1.125), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 4.5*A[0] + -21.0*A[2] + 105.0*A[4] + -192.0*A[5] + 157.5*A[6] + -64.0*A[7] + 10.5*A[8];
+  o.Preg = -0.25*A[0] + 1.125*A[2] + -3.5*A[4] + 13.125*A[6] + -21.333333333333332*A[7] + 15.75*A[8] + -5.818181818181818*A[9] + 0.875*A[10];
+  o.Mhat = 0.5;
+  o.MPhat = -0.026515151515151516;
+}
+template <> __host__ __device__ __forceinline__ void Kern_w4::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 9.0*A[0] + -84.0*A[2] + 630.0*A[4] + -1344.0*A[5] + 1260.0*A[6] + -576.0*A[7] + 105.0*A[8];
+  const double a2 = 9.0*A[2] + -84.0*A[4] + 630.0*A[6] + -1344.0*A[7] + 1260.0*A[8] + -576.0*A[9] + 105.0*A[10];
+  const double m1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rhi, -64.0), rhi, 157.5), rhi, -192.0), rhi, 105.0), rhi, 0.0), rhi, -21.0), rhi, 0.0), rhi, 4.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rlo, -64.0), rlo, 157.5), rlo, -192.0), rlo, 105.0), rlo, 0.0), rlo, -21.0), rlo, 0.0), rlo, 4.5), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(8.75, rhi, -52.36363636363637), rhi, 126.0), rhi, -149.33333333333334), rhi, 78.75), rhi, 0.0), rhi, -14.0), rhi, 0.0), rhi, 2.25), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(8.75, rlo, -52.36363636363637), rlo, 126.0), rlo, -149.33333333333334), rlo, 78.75), rlo, 0.0), rlo, -14.0), rlo, 0.0), rlo, 2.25), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- w6: C2*pi = 78/7, plane second moment 3/70
+struct Kern_w6 {
+  static constexpr int kId = 3;
+  static constexpr int kBlocks = 1;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.04285714285714286;
+  static constexpr double kR[kBlocks] = {1.0};
+  static constexpr int kNA[kBlocks] = {14};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {14};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_w6::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['78/7', '0', '-858/7', '0', '5148/7', '0', '-5148', '82368/7', '-12870', '54912/7', '-2574', '2496/7']
+  o.W0 = 11.142857142857142*A[0] + -122.57142857142857*A[2] + 735.4285714285714*A[4] + -5148.0*A[6] + 11766.857142857143*A[7] + -12870.0*A[8] + 7844.571428571428*A[9] + -2574.0*A[10] + 356.57142857142856*A[11];
+  o.W1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rhi, -214.5), rhi, 713.1428571428571), rhi, -1287.0), rhi, 1307.4285714285713), rhi, -643.5), rhi, 0.0), rhi, 122.57142857142857), rhi, 0.0), rhi, -30.642857142857142), rhi, 0.0), rhi, 5.571428571428571), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rlo, -214.5), rlo, 713.1428571428571), rlo, -1287.0), rlo, 1307.4285714285713), rlo, -643.5), rlo, 0.0), rlo, 122.57142857142857), rlo, 0.0), rlo, -30.642857142857142), rlo, 0.0), rlo, 5.571428571428571), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.5*A[0] + 5.571428571428571*A[2] + -30.642857142857142*A[4] + 122.57142857142857*A[6] + -643.5*A[8] + 1307.4285714285713*A[9] + -1287.0*A[10] + 713.1428571428571*A[11] + -214.5*A[12] + 27.428571428571427*A[13];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.8285714285714285, rhi, -15.321428571428571), rhi, 54.857142857142854), rhi, -107.25), rhi, 118.85714285714286), rhi, -64.35), rhi, 0.0), rhi, 15.321428571428571), rhi, 0.0), rhi, -5.107142857142857), rhi, 0.0), rhi, 1.3928571428571428), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.8285714285714285, rlo, -15.321428571428571), rlo, 54.857142857142854), rlo, -107.25), rlo, 118.85714285714286), rlo, -64.35), rlo, 0.0), rlo, 15.321428571428571), rlo, 0.0), rlo, -5.107142857142857), rlo, 0.0), rlo, 1.3928571428571428), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 5.571428571428571*A[0] + -30.642857142857142*A[2] + 122.57142857142857*A[4] + -643.5*A[6] + 1307.4285714285713*A[7] + -1287.0*A[8] + 713.1428571428571*A[9] + -214.5*A[10] + 27.428571428571427*A[11];
+  o.Preg = -0.25*A[0] + 1.3928571428571428*A[2] + -5.107142857142857*A[4] + 15.321428571428571*A[6] + -64.35*A[8] + 118.85714285714286*A[9] + -107.25*A[10] + 54.857142857142854*A[11] + -15.321428571428571*A[12] + 1.8285714285714285*A[13];
+  o.Mhat = 0.5;
+  o.MPhat = -0.02142857142857143;
+}
+template <> __host__ __device__ __forceinline__ void Kern_w6::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 11.142857142857142*A[0] + -122.57142857142857*A[2] + 735.4285714285714*A[4] + -5148.0*A[6] + 11766.857142857143*A[7] + -12870.0*A[8] + 7844.571428571428*A[9] + -2574.0*A[10] + 356.57142857142856*A[11];
+  const double a2 = 11.142857142857142*A[2] + -122.57142857142857*A[4] + 735.4285714285714*A[6] + -5148.0*A[8] + 11766.857142857143*A[9] + -12870.0*A[10] + 7844.571428571428*A[11] + -2574.0*A[12] + 356.57142857142856*A[13];
+  const double m1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rhi, -214.5), rhi, 713.1428571428571), rhi, -1287.0), rhi, 1307.4285714285713), rhi, -643.5), rhi, 0.0), rhi, 122.57142857142857), rhi, 0.0), rhi, -30.642857142857142), rhi, 0.0), rhi, 5.571428571428571), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rlo, -214.5), rlo, 713.1428571428571), rlo, -1287.0), rlo, 1307.4285714285713), rlo, -643.5), rlo, 0.0), rlo, 122.57142857142857), rlo, 0.0), rlo, -30.642857142857142), rlo, 0.0), rlo, 5.571428571428571), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(23.771428571428572, rhi, -183.85714285714286), rhi, 603.4285714285714), rhi, -1072.5), rhi, 1069.7142857142858), rhi, -514.8), rhi, 0.0), rhi, 91.92857142857143), rhi, 0.0), rhi, -20.428571428571427), rhi, 0.0), rhi, 2.7857142857142856), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(23.771428571428572, rlo, -183.85714285714286), rlo, 603.4285714285714), rlo, -1072.5), rlo, 1069.7142857142858), rlo, -514.8), rlo, 0.0), rlo, 91.92857142857143), rlo, 0.0), rlo, -20.428571428571427), rlo, 0.0), rlo, 2.7857142857142856), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- quartic: C2*pi = 46875/2398, plane second moment 9759/152600
+struct Kern_quartic {
+  static constexpr int kId = 4;
+  static constexpr int kBlocks = 3;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.06395150720838794;
+  static constexpr double kR[kBlocks] = {1.0, 0.6, 0.2};
+  static constexpr int kNA[kBlocks] = {7, 7, 7};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {7, 7, 7};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['46875/2398', '-93750/1199', '140625/1199', '-93750/1199', '46875/2398']
+  o.W0 = 19.547539616346956*A[0] + -78.19015846538782*A[1] + 117.28523769808173*A[2] + -78.19015846538782*A[3] + 19.547539616346956*A[4];
+  o.W1 = (fma(fma(fma(fma(fma(fma(3.2579232693911595, rhi, -15.638031693077565), rhi, 29.321309424520432), rhi, -26.063386155129276), rhi, 9.773769808173478), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(3.2579232693911595, rlo, -15.638031693077565), rlo, 29.321309424520432), rlo, -26.063386155129276), rlo, 9.773769808173478), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.6515846538782318*A[0] + 9.773769808173478*A[2] + -26.063386155129276*A[3] + 29.321309424520432*A[4] + -15.638031693077565*A[5] + 3.2579232693911595*A[6];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(0.40724040867389494, rhi, -2.2340045275825093), rhi, 4.886884904086739), rhi, -5.212677231025855), rhi, 2.4434424520433695), rhi, 0.0), rhi, -0.3257923269391159), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(0.40724040867389494, rlo, -2.2340045275825093), rlo, 4.886884904086739), rlo, -5.212677231025855), rlo, 2.4434424520433695), rlo, 0.0), rlo, -0.3257923269391159), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 9.773769808173478*A[0] + -26.063386155129276*A[1] + 29.321309424520432*A[2] + -15.638031693077565*A[3] + 3.2579232693911595*A[4];
+  o.Preg = -0.3257923269391159*A[0] + 2.4434424520433695*A[2] + -5.212677231025855*A[3] + 4.886884904086739*A[4] + -2.2340045275825093*A[5] + 0.40724040867389494*A[6];
+  o.Mhat = 0.6515846538782318;
+  o.MPhat = -0.03490632074347671;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quartic::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 19.547539616346956*A[0] + -78.19015846538782*A[1] + 117.28523769808173*A[2] + -78.19015846538782*A[3] + 19.547539616346956*A[4];
+  const double a2 = 19.547539616346956*A[2] + -78.19015846538782*A[3] + 117.28523769808173*A[4] + -78.19015846538782*A[5] + 19.547539616346956*A[6];
+  const double m1 = (fma(fma(fma(fma(fma(fma(3.2579232693911595, rhi, -15.638031693077565), rhi, 29.321309424520432), rhi, -26.063386155129276), rhi, 9.773769808173478), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(3.2579232693911595, rlo, -15.638031693077565), rlo, 29.321309424520432), rlo, -26.063386155129276), rlo, 9.773769808173478), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(2.4434424520433695, rhi, -11.170022637912545), rhi, 19.547539616346956), rhi, -15.638031693077565), rhi, 4.886884904086739), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(2.4434424520433695, rlo, -11.170022637912545), rlo, 19.547539616346956), rlo, -15.638031693077565), rlo, 4.886884904086739), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<1>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 3/5: P = ['-30375/2398', '101250/1199', '-253125/1199', '281250/1199', '-234375/2398']
+  o.W0 = -12.666805671392828*A[0] + 84.44537114261885*A[1] + -211.11342785654713*A[2] + 234.57047539616346*A[3] + -97.73769808173478*A[4];
+  o.W1 = (fma(fma(fma(fma(fma(fma(-16.289616346955796, rhi, 46.914095079232695), rhi, -52.77835696413678), rhi, 28.148457047539615), rhi, -6.333402835696414), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(-16.289616346955796, rlo, 46.914095079232695), rlo, -52.77835696413678), rlo, 28.148457047539615), rlo, -6.333402835696414), rlo, 0.0), rlo, 0.0));
+  o.P0 = 0.15200166805671392*A[0] + -6.333402835696414*A[2] + 28.148457047539615*A[3] + -52.77835696413678*A[4] + 46.914095079232695*A[5] + -16.289616346955796*A[6];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(-2.0362020433694745, rhi, 6.702013582747528), rhi, -8.79639282735613), rhi, 5.629691409507923), rhi, -1.5833507089241035), rhi, 0.0), rhi, 0.07600083402835696), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-2.0362020433694745, rlo, 6.702013582747528), rlo, -8.79639282735613), rlo, 5.629691409507923), rlo, -1.5833507089241035), rlo, 0.0), rlo, 0.07600083402835696), rlo, 0.0), rlo, 0.0));
+  o.Lreg = -6.333402835696414*A[0] + 28.148457047539615*A[1] + -52.77835696413678*A[2] + 46.914095079232695*A[3] + -16.289616346955796*A[4];
+  o.Preg = 0.07600083402835696*A[0] + -1.5833507089241035*A[2] + 5.629691409507923*A[3] + -8.79639282735613*A[4] + 6.702013582747528*A[5] + -2.0362020433694745*A[6];
+  o.Mhat = -0.15200166805671392;
+  o.MPhat = 0.0029314607410937687;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quartic::adj<1>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = -12.666805671392828*A[0] + 84.44537114261885*A[1] + -211.11342785654713*A[2] + 234.57047539616346*A[3] + -97.73769808173478*A[4];
+  const double a2 = -12.666805671392828*A[2] + 84.44537114261885*A[3] + -211.11342785654713*A[4] + 234.57047539616346*A[5] + -97.73769808173478*A[6];
+  const double m1 = (fma(fma(fma(fma(fma(fma(-16.289616346955796, rhi, 46.914095079232695), rhi, -52.77835696413678), rhi, 28.148457047539615), rhi, -6.333402835696414), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(-16.289616346955796, rlo, 46.914095079232695), rlo, -52.77835696413678), rlo, 28.148457047539615), rlo, -6.333402835696414), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(-12.217212260216847, rhi, 33.510067913737636), rhi, -35.18557130942452), rhi, 16.88907422852377), rhi, -3.166701417848207), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-12.217212260216847, rlo, 33.510067913737636), rlo, -35.18557130942452), rlo, 16.88907422852377), rlo, -3.166701417848207), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<2>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1/5: P = ['375/1199', '-7500/1199', '56250/1199', '-187500/1199', '234375/1199']
+  o.W0 = 0.3127606338615513*A[0] + -6.255212677231026*A[1] + 46.914095079232695*A[2] + -156.38031693077565*A[3] + 195.47539616346955*A[4];
+  o.W1 = (fma(fma(fma(fma(fma(fma(32.57923269391159, rhi, -31.27606338615513), rhi, 11.728523769808174), rhi, -2.085070892410342), rhi, 0.15638031693077564), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(32.57923269391159, rlo, -31.27606338615513), rlo, 11.728523769808174), rlo, -2.085070892410342), rlo, 0.15638031693077564), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.0004170141784820684*A[0] + 0.15638031693077564*A[2] + -2.085070892410342*A[3] + 11.728523769808174*A[4] + -31.27606338615513*A[5] + 32.57923269391159*A[6];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(4.072404086738949, rhi, -4.468009055165019), rhi, 1.9547539616346956), rhi, -0.4170141784820684), rhi, 0.03909507923269391), rhi, 0.0), rhi, -0.0002085070892410342), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(4.072404086738949, rlo, -4.468009055165019), rlo, 1.9547539616346956), rlo, -0.4170141784820684), rlo, 0.03909507923269391), rlo, 0.0), rlo, -0.0002085070892410342), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 0.15638031693077564*A[0] + -2.085070892410342*A[1] + 11.728523769808174*A[2] + -31.27606338615513*A[3] + 32.57923269391159*A[4];
+  o.Preg = -0.0002085070892410342*A[0] + 0.03909507923269391*A[2] + -0.4170141784820684*A[3] + 1.9547539616346956*A[4] + -4.468009055165019*A[5] + 4.072404086738949*A[6];
+  o.Mhat = 0.0004170141784820684;
+  o.MPhat = -8.936018110330037e-07;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quartic::adj<2>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 0.3127606338615513*A[0] + -6.255212677231026*A[1] + 46.914095079232695*A[2] + -156.38031693077565*A[3] + 195.47539616346955*A[4];
+  const double a2 = 0.3127606338615513*A[2] + -6.255212677231026*A[3] + 46.914095079232695*A[4] + -156.38031693077565*A[5] + 195.47539616346955*A[6];
+  const double m1 = (fma(fma(fma(fma(fma(fma(32.57923269391159, rhi, -31.27606338615513), rhi, 11.728523769808174), rhi, -2.085070892410342), rhi, 0.15638031693077564), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(32.57923269391159, rlo, -31.27606338615513), rlo, 11.728523769808174), rlo, -2.085070892410342), rlo, 0.15638031693077564), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(24.434424520433694, rhi, -22.34004527582509), rhi, 7.8190158465387825), rhi, -1.2510425354462051), rhi, 0.07819015846538782), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(24.434424520433694, rlo, -22.34004527582509), rlo, 7.8190158465387825), rlo, -1.2510425354462051), rlo, 0.07819015846538782), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- quintic: C2*pi = 15309/478, plane second moment 2771/51624
+struct Kern_quintic {
+  static constexpr int kId = 5;
+  static constexpr int kBlocks = 3;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.05367658453432512;
+  static constexpr double kR[kBlocks] = {1.0, 0.6666666666666666, 0.3333333333333333};
+  static constexpr int kNA[kBlocks] = {8, 8, 8};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {8, 8, 8};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['15309/478', '-76545/478', '76545/239', '-76545/239', '76545/478', '-15309/478']
+  o.W0 = 32.02719665271967*A[0] + -160.13598326359832*A[1] + 320.27196652719664*A[2] + -320.27196652719664*A[3] + 160.13598326359832*A[4] + -32.02719665271967*A[5];
+  o.W1 = (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rhi, 26.689330543933053), rhi, -64.05439330543933), rhi, 80.06799163179916), rhi, -53.37866108786611), rhi, 16.013598326359833), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rlo, 26.689330543933053), rlo, -64.05439330543933), rlo, 80.06799163179916), rlo, -53.37866108786611), rlo, 16.013598326359833), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.7625523012552301*A[0] + 16.013598326359833*A[2] + -53.37866108786611*A[3] + 80.06799163179916*A[4] + -64.05439330543933*A[5] + 26.689330543933053*A[6] + -4.575313807531381*A[7];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.5083682008368201, rhi, 3.3361663179916317), rhi, -9.150627615062762), rhi, 13.344665271966527), rhi, -10.675732217573222), rhi, 4.003399581589958), rhi, 0.0), rhi, -0.38127615062761505), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.5083682008368201, rlo, 3.3361663179916317), rlo, -9.150627615062762), rlo, 13.344665271966527), rlo, -10.675732217573222), rlo, 4.003399581589958), rlo, 0.0), rlo, -0.38127615062761505), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 16.013598326359833*A[0] + -53.37866108786611*A[1] + 80.06799163179916*A[2] + -64.05439330543933*A[3] + 26.689330543933053*A[4] + -4.575313807531381*A[5];
+  o.Preg = -0.38127615062761505*A[0] + 4.003399581589958*A[2] + -10.675732217573222*A[3] + 13.344665271966527*A[4] + -9.150627615062762*A[5] + 3.3361663179916317*A[6] + -0.5083682008368201*A[7];
+  o.Mhat = 0.7625523012552301;
+  o.MPhat = -0.03177301255230126;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quintic::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 32.02719665271967*A[0] + -160.13598326359832*A[1] + 320.27196652719664*A[2] + -320.27196652719664*A[3] + 160.13598326359832*A[4] + -32.02719665271967*A[5];
+  const double a2 = 32.02719665271967*A[2] + -160.13598326359832*A[3] + 320.27196652719664*A[4] + -320.27196652719664*A[5] + 160.13598326359832*A[6] + -32.02719665271967*A[7];
+  const double m1 = (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rhi, 26.689330543933053), rhi, -64.05439330543933), rhi, 80.06799163179916), rhi, -53.37866108786611), rhi, 16.013598326359833), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rlo, 26.689330543933053), rlo, -64.05439330543933), rlo, 80.06799163179916), rlo, -53.37866108786611), rlo, 16.013598326359833), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-3.5585774058577404, rhi, 20.01699790794979), rhi, -45.75313807531381), rhi, 53.37866108786611), rhi, -32.02719665271967), rhi, 8.006799163179917), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-3.5585774058577404, rlo, 20.01699790794979), rlo, -45.75313807531381), rlo, 53.37866108786611), rlo, -32.02719665271967), rlo, 8.006799163179917), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<1>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 2/3: P = ['-6048/239', '45360/239', '-136080/239', '204120/239', '-153090/239', '45927/239']
+  o.W0 = -25.305439330543933*A[0] + 189.7907949790795*A[1] + -569.3723849372385*A[2] + 854.0585774058577*A[3] + -640.5439330543933*A[4] + 192.163179916318*A[5];
+  o.W1 = (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rhi, -106.75732217573221), rhi, 170.81171548117155), rhi, -142.34309623430963), rhi, 63.26359832635983), rhi, -12.652719665271967), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rlo, -106.75732217573221), rlo, 170.81171548117155), rlo, -142.34309623430963), rlo, 63.26359832635983), rlo, -12.652719665271967), rlo, 0.0), rlo, 0.0));
+  o.P0 = 0.26778242677824265*A[0] + -12.652719665271967*A[2] + 63.26359832635983*A[3] + -142.34309623430963*A[4] + 170.81171548117155*A[5] + -106.75732217573221*A[6] + 27.451882845188283*A[7];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.0502092050209204, rhi, -13.344665271966527), rhi, 24.401673640167363), rhi, -23.723849372384937), rhi, 12.652719665271967), rhi, -3.1631799163179917), rhi, 0.0), rhi, 0.13389121338912133), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.0502092050209204, rlo, -13.344665271966527), rlo, 24.401673640167363), rlo, -23.723849372384937), rlo, 12.652719665271967), rlo, -3.1631799163179917), rlo, 0.0), rlo, 0.13389121338912133), rlo, 0.0), rlo, 0.0));
+  o.Lreg = -12.652719665271967*A[0] + 63.26359832635983*A[1] + -142.34309623430963*A[2] + 170.81171548117155*A[3] + -106.75732217573221*A[4] + 27.451882845188283*A[5];
+  o.Preg = 0.13389121338912133*A[0] + -3.1631799163179917*A[2] + 12.652719665271967*A[3] + -23.723849372384937*A[4] + 24.401673640167363*A[5] + -13.344665271966527*A[6] + 3.0502092050209204*A[7];
+  o.Mhat = -0.26778242677824265;
+  o.MPhat = 0.004958933829226716;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quintic::adj<1>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = -25.305439330543933*A[0] + 189.7907949790795*A[1] + -569.3723849372385*A[2] + 854.0585774058577*A[3] + -640.5439330543933*A[4] + 192.163179916318*A[5];
+  const double a2 = -25.305439330543933*A[2] + 189.7907949790795*A[3] + -569.3723849372385*A[4] + 854.0585774058577*A[5] + -640.5439330543933*A[6] + 192.163179916318*A[7];
+  const double m1 = (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rhi, -106.75732217573221), rhi, 170.81171548117155), rhi, -142.34309623430963), rhi, 63.26359832635983), rhi, -12.652719665271967), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rlo, -106.75732217573221), rlo, 170.81171548117155), rlo, -142.34309623430963), rlo, 63.26359832635983), rlo, -12.652719665271967), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(21.351464435146443, rhi, -80.06799163179916), rhi, 122.00836820083683), rhi, -94.89539748953975), rhi, 37.9581589958159), rhi, -6.326359832635983), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(21.351464435146443, rlo, -80.06799163179916), rlo, 122.00836820083683), rlo, -94.89539748953975), rlo, 37.9581589958159), rlo, -6.326359832635983), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<2>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1/3: P = ['945/478', '-14175/478', '42525/239', '-127575/239', '382725/478', '-229635/478']
+  o.W0 = 1.9769874476987448*A[0] + -29.65481171548117*A[1] + 177.92887029288704*A[2] + -533.7866108786611*A[3] + 800.6799163179917*A[4] + -480.407949790795*A[5];
+  o.W1 = (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rhi, 133.44665271966528), rhi, -106.75732217573221), rhi, 44.48221757322176), rhi, -9.884937238493723), rhi, 0.9884937238493724), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rlo, 133.44665271966528), rlo, -106.75732217573221), rlo, 44.48221757322176), rlo, -9.884937238493723), rlo, 0.9884937238493724), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.005230125523012552*A[0] + 0.9884937238493724*A[2] + -9.884937238493723*A[3] + 44.48221757322176*A[4] + -106.75732217573221*A[5] + 133.44665271966528*A[6] + -68.6297071129707*A[7];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-7.625523012552302, rhi, 16.68083158995816), rhi, -15.251046025104603), rhi, 7.4137029288702925), rhi, -1.9769874476987448), rhi, 0.2471234309623431), rhi, 0.0), rhi, -0.002615062761506276), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-7.625523012552302, rlo, 16.68083158995816), rlo, -15.251046025104603), rlo, 7.4137029288702925), rlo, -1.9769874476987448), rlo, 0.2471234309623431), rlo, 0.0), rlo, -0.002615062761506276), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 0.9884937238493724*A[0] + -9.884937238493723*A[1] + 44.48221757322176*A[2] + -106.75732217573221*A[3] + 133.44665271966528*A[4] + -68.6297071129707*A[5];
+  o.Preg = -0.002615062761506276*A[0] + 0.2471234309623431*A[2] + -1.9769874476987448*A[3] + 7.4137029288702925*A[4] + -15.251046025104603*A[5] + 16.68083158995816*A[6] + -7.625523012552302*A[7];
+  o.Mhat = 0.005230125523012552;
+  o.MPhat = -2.4213544088021077e-05;
+}
+template <> __host__ __device__ __forceinline__ void Kern_quintic::adj<2>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 1.9769874476987448*A[0] + -29.65481171548117*A[1] + 177.92887029288704*A[2] + -533.7866108786611*A[3] + 800.6799163179917*A[4] + -480.407949790795*A[5];
+  const double a2 = 1.9769874476987448*A[2] + -29.65481171548117*A[3] + 177.92887029288704*A[4] + -533.7866108786611*A[5] + 800.6799163179917*A[6] + -480.407949790795*A[7];
+  const double m1 = (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rhi, 133.44665271966528), rhi, -106.75732217573221), rhi, 44.48221757322176), rhi, -9.884937238493723), rhi, 0.9884937238493724), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rlo, 133.44665271966528), rlo, -106.75732217573221), rlo, 44.48221757322176), rlo, -9.884937238493723), rlo, 0.9884937238493724), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-53.37866108786611, rhi, 100.08498953974896), rhi, -76.25523012552301), rhi, 29.65481171548117), rhi, -5.930962343096234), rhi, 0.4942468619246862), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-53.37866108786611, rlo, 100.08498953974896), rlo, -76.25523012552301), rlo, 29.65481171548117), rlo, -5.930962343096234), rlo, 0.4942468619246862), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- poly6: C2*pi = 4, plane second moment 1/10
+struct Kern_poly6 {
+  static constexpr int kId = 6;
+  static constexpr int kBlocks = 1;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.1;
+  static constexpr double kR[kBlocks] = {1.0};
+  static constexpr int kNA[kBlocks] = {9};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {9};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_poly6::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['4', '0', '-12', '0', '12', '0', '-4']
+  o.W0 = 4.0*A[0] + -12.0*A[2] + 12.0*A[4] + -4.0*A[6];
+  o.W1 = (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, -3.0), rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, -3.0), rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, 0.0));
+  o.P0 = -0.5*A[0] + 2.0*A[2] + -3.0*A[4] + 2.0*A[6] + -0.5*A[8];
+  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.05, rhi, 0.0), rhi, 0.25), rhi, 0.0), rhi, -0.5), rhi, 0.0), rhi, 0.5), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.05, rlo, 0.0), rlo, 0.25), rlo, 0.0), rlo, -0.5), rlo, 0.0), rlo, 0.5), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.Lreg = 2.0*A[0] + -3.0*A[2] + 2.0*A[4] + -0.5*A[6];
+  o.Preg = -0.25*A[0] + 0.5*A[2] + -0.5*A[4] + 0.25*A[6] + -0.05*A[8];
+  o.Mhat = 0.5;
+  o.MPhat = -0.05;
+}
+template <> __host__ __device__ __forceinline__ void Kern_poly6::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 4.0*A[0] + -12.0*A[2] + 12.0*A[4] + -4.0*A[6];
+  const double a2 = 4.0*A[2] + -12.0*A[4] + 12.0*A[6] + -4.0*A[8];
+  const double m1 = (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, -3.0), rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, -3.0), rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, 0.0));
+  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.4, rhi, 0.0), rhi, 1.5), rhi, 0.0), rhi, -2.0), rhi, 0.0), rhi, 1.0), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.4, rlo, 0.0), rlo, 1.5), rlo, 0.0), rlo, -2.0), rlo, 0.0), rlo, 1.0), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- reference term plans (plain FP64 interpreter): per kernel offsets into flat tables
+constexpr int kPlanEdgeTerms = 132;
+constexpr int kPlanValueTerms = 60;
+constexpr int kPlanCoeffs = 1140;
+constexpr int kPlanRadii = 12;
+struct PlanOffsets { int e0, e1, v0, v1; };
+static const PlanOffsets kPlanOffsets[kNumKernels] = {{0, 22, 0, 10}, {22, 33, 10, 15}, {33, 44, 15, 20}, {44, 55, 20, 25}, {55, 88, 25, 40}, {88, 121, 40, 55}, {121, 132, 55, 60}};
+static const int kPlanE[kPlanEdgeTerms][7] = {   // ch, i, a, b, radius index, c0, c1
+  {1, 0, 0, 0, 0, 8, 13},
+  {1, 0, 0, 0, 1, 13, 18},
+  {2, 1, 0, 0, 0, 18, 23},
+  {2, 1, 0, 0, 1, 23, 28},
+  {3, 0, 0, 0, 0, 28, 32},
+  {3, 0, 0, 0, 1, 32, 36},
+  {4, 1, 0, 0, 0, 36, 40},
+  {4, 1, 0, 0, 1, 40, 44},
+  {5, 0, 1, 0, 0, 44, 48},
+  {5, 0, 1, 0, 1, 48, 52},
+  {6, 1, 1, 0, 0, 60, 64},
+  {6, 1, 1, 0, 1, 64, 68},
+  {7, 0, 0, 1, 0, 68, 72},
+  {7, 0, 0, 1, 1, 72, 76},
+  {8, 1, 0, 1, 0, 76, 80},
+  {8, 1, 0, 1, 1, 80, 84},
+  {9, 0, 1, 0, 0, 92, 97},
+  {9, 0, 1, 0, 1, 97, 102},
+  {10, 0, 0, 1, 0, 112, 117},
+  {10, 0, 0, 1, 1, 117, 122},
+  {11, 1, 0, 1, 0, 122, 127},
+  {11, 1, 0, 1, 1, 127, 132},
+  {1, 0, 0, 0, 2, 147, 153},
+  {2, 1, 0, 0, 2, 153, 159},
+  {3, 0, 0, 0, 2, 159, 164},
+  {4, 1, 0, 0, 2, 164, 169},
+  {5, 0, 1, 0, 2, 169, 174},
+  {6, 1, 1, 0, 2, 179, 184},
+  {7, 0, 0, 1, 2, 184, 189},
+  {8, 1, 0, 1, 2, 189, 194},
+  {9, 0, 1, 0, 2, 199, 205},
+  {10, 0, 0, 1, 2, 211, 217},
+  {11, 1, 0, 1, 2, 217, 223},
+  {1, 0, 0, 0, 3, 236, 244},
+  {2, 1, 0, 0, 3, 244, 252},
+  {3, 0, 0, 0, 3, 252, 259},
+  {4, 1, 0, 0, 3, 259, 266},
+  {5, 0, 1, 0, 3, 266, 273},
+  {6, 1, 1, 0, 3, 280, 287},
+  {7, 0, 0, 1, 3, 287, 294},
+  {8, 1, 0, 1, 3, 294, 301},
+  {9, 0, 1, 0, 3, 308, 316},
+  {10, 0, 0, 1, 3, 324, 332},
+  {11, 1, 0, 1, 3, 332, 340},
+  {1, 0, 0, 0, 4, 357, 367},
+  {2, 1, 0, 0, 4, 367, 377},
+  {3, 0, 0, 0, 4, 377, 386},
+  {4, 1, 0, 0, 4, 386, 395},
+  {5, 0, 1, 0, 4, 395, 404},
+  {6, 1, 1, 0, 4, 413, 422},
+  {7, 0, 0, 1, 4, 422, 431},
+  {8, 1, 0, 1, 4, 431, 440},
+  {9, 0, 1, 0, 4, 449, 459},
+  {10, 0, 0, 1, 4, 469, 479},
+  {11, 1, 0, 1, 4, 479, 489},
+  {1, 0, 0, 0, 5, 514, 520},
+  {1, 0, 0, 0, 6, 520, 526},
+  {1, 0, 0, 0, 7, 526, 532},
+  {2, 1, 0, 0, 5, 532, 538},
+  {2, 1, 0, 0, 6, 538, 544},
+  {2, 1, 0, 0, 7, 544, 550},
+  {3, 0, 0, 0, 5, 550, 555},
+  {3, 0, 0, 0, 6, 555, 560},
+  {3, 0, 0, 0, 7, 560, 565},
+  {4, 1, 0, 0, 5, 565, 570},
+  {4, 1, 0, 0, 6, 570, 575},
+  {4, 1, 0, 0, 7, 575, 580},
+  {5, 0, 1, 0, 5, 580, 585},
+  {5, 0, 1, 0, 6, 585, 590},
+  {5, 0, 1, 0, 7, 590, 595},
+  {6, 1, 1, 0, 5, 610, 615},
+  {6, 1, 1, 0, 6, 615, 620},
+  {6, 1, 1, 0, 7, 620, 625},
+  {7, 0, 0, 1, 5, 625, 630},
+  {7, 0, 0, 1, 6, 630, 635},
+  {7, 0, 0, 1, 7, 635, 640},
+  {8, 1, 0, 1, 5, 640, 645},
+  {8, 1, 0, 1, 6, 645, 650},
+  {8, 1, 0, 1, 7, 650, 655},
+  {9, 0, 1, 0, 5, 670, 676},
+  {9, 0, 1, 0, 6, 676, 682},
+  {9, 0, 1, 0, 7, 682, 688},
+  {10, 0, 0, 1, 5, 706, 712},
+  {10, 0, 0, 1, 6, 712, 718},
+  {10, 0, 0, 1, 7, 718, 724},
+  {11, 1, 0, 1, 5, 724, 730},
+  {11, 1, 0, 1, 6, 730, 736},
+  {11, 1, 0, 1, 7, 736, 742},
+  {1, 0, 0, 0, 8, 778, 785},
+  {1, 0, 0, 0, 9, 785, 792},
+  {1, 0, 0, 0, 10, 792, 799},
+  {2, 1, 0, 0, 8, 799, 806},
+  {2, 1, 0, 0, 9, 806, 813},
+  {2, 1, 0, 0, 10, 813, 820},
+  {3, 0, 0, 0, 8, 820, 826},
+  {3, 0, 0, 0, 9, 826, 832},
+  {3, 0, 0, 0, 10, 832, 838},
+  {4, 1, 0, 0, 8, 838, 844},
+  {4, 1, 0, 0, 9, 844, 850},
+  {4, 1, 0, 0, 10, 850, 856},
+  {5, 0, 1, 0, 8, 856, 862},
+  {5, 0, 1, 0, 9, 862, 868},
+  {5, 0, 1, 0, 10, 868, 874},
+  {6, 1, 1, 0, 8, 892, 898},
+  {6, 1, 1, 0, 9, 898, 904},
+  {6, 1, 1, 0, 10, 904, 910},
+  {7, 0, 0, 1, 8, 910, 916},
+  {7, 0, 0, 1, 9, 916, 922},
+  {7, 0, 0, 1, 10, 922, 928},
+  {8, 1, 0, 1, 8, 928, 934},
+  {8, 1, 0, 1, 9, 934, 940},
+  {8, 1, 0, 1, 10, 940, 946},
+  {9, 0, 1, 0, 8, 964, 971},
+  {9, 0, 1, 0, 9, 971, 978},
+  {9, 0, 1, 0, 10, 978, 985},
+  {10, 0, 0, 1, 8, 1006, 1013},
+  {10, 0, 0, 1, 9, 1013, 1020},
+  {10, 0, 0, 1, 10, 1020, 1027},
+  {11, 1, 0, 1, 8, 1027, 1034},
+  {11, 1, 0, 1, 9, 1034, 1041},
+  {11, 1, 0, 1, 10, 1041, 1048},
+  {1, 0, 0, 0, 11, 1073, 1078},
+  {2, 1, 0, 0, 11, 1078, 1083},
+  {3, 0, 0, 0, 11, 1083, 1087},
+  {4, 1, 0, 0, 11, 1087, 1091},
+  {5, 0, 1, 0, 11, 1091, 1095},
+  {6, 1, 1, 0, 11, 1099, 1103},
+  {7, 0, 0, 1, 11, 1103, 1107},
+  {8, 1, 0, 1, 11, 1107, 1111},
+  {9, 0, 1, 0, 11, 1115, 1120},
+  {10, 0, 0, 1, 11, 1125, 1130},
+  {11, 1, 0, 1, 11, 1130, 1135},
+};
+static const int kPlanVi[kPlanValueTerms][4] = {   // ch, radius index, c0, c1
+  {0, 0, 0, 4},
+  {0, 1, 4, 8},
+  {5, 0, 52, 56},
+  {5, 1, 56, 60},
+  {8, 0, 84, 88},
+  {8, 1, 88, 92},
+  {9, 0, 102, 107},
+  {9, 1, 107, 112},
+  {11, 0, 132, 137},
+  {11, 1, 137, 142},
+  {0, 2, 142, 147},
+  {5, 2, 174, 179},
+  {8, 2, 194, 199},
+  {9, 2, 205, 211},
+  {11, 2, 223, 229},
+  {0, 3, 229, 236},
+  {5, 3, 273, 280},
+  {8, 3, 301, 308},
+  {9, 3, 316, 324},
+  {11, 3, 340, 348},
+  {0, 4, 348, 357},
+  {5, 4, 404, 413},
+  {8, 4, 440, 449},
+  {9, 4, 459, 469},
+  {11, 4, 489, 499},
+  {0, 5, 499, 504},
+  {0, 6, 504, 509},
+  {0, 7, 509, 514},
+  {5, 5, 595, 600},
+  {5, 6, 600, 605},
+  {5, 7, 605, 610},
+  {8, 5, 655, 660},
+  {8, 6, 660, 665},
+  {8, 7, 665, 670},
+  {9, 5, 688, 694},
+  {9, 6, 694, 700},
+  {9, 7, 700, 706},
+  {11, 5, 742, 748},
+  {11, 6, 748, 754},
+  {11, 7, 754, 760},
+  {0, 8, 760, 766},
+  {0, 9, 766, 772},
+  {0, 10, 772, 778},
+  {5, 8, 874, 880},
+  {5, 9, 880, 886},
+  {5, 10, 886, 892},
+  {8, 8, 946, 952},
+  {8, 9, 952, 958},
+  {8, 10, 958, 964},
+  {9, 8, 985, 992},
+  {9, 9, 992, 999},
+  {9, 10, 999, 1006},
+  {11, 8, 1048, 1055},
+  {11, 9, 1055, 1062},
+  {11, 10, 1062, 1069},
+  {0, 11, 1069, 1073},
+  {5, 11, 1095, 1099},
+  {8, 11, 1111, 1115},
+  {9, 11, 1120, 1125},
+  {11, 11, 1135, 1140},
+};
+static const double kPlanVmR[kPlanValueTerms] = {0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.04081632653061224, -0.0012755102040816326, 0.04081632653061224, -0.0012755102040816326, 0.5, 0.5, 0.5, 0.034722222222222224, 0.034722222222222224, 0.5, 0.5, 0.5, 0.026515151515151516, 0.026515151515151516, 0.5, 0.5, 0.5, 0.02142857142857143, 0.02142857142857143, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.5, 0.5, 0.5, 0.05, 0.05};
+static const int kPlanCn[kPlanCoeffs] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8};
+static const double kPlanCc[kPlanCoeffs] = {5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05};
+static const double kPlanRadii[kPlanRadii] = {1.0, 0.5, 1.0, 1.0, 1.0, 1.0, 0.6, 0.2, 1.0, 0.6666666666666666, 0.3333333333333333, 1.0};
+
+}  // namespace wsb

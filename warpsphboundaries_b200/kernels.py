@@ -1,0 +1,436 @@
+"""Exact kernel algebra for the 2-D edge reductions (host side, offline).
+
+Every SPH kernel of this package is a piecewise polynomial in r = |y|/h on [0, 1].
+Written as a sum of *blocks* ("truncated monomials"),
+
+    pi * W(r) = sum_b  P_b(r) * 1[r <= R_b],      P_b(r) = sum_n c_{b,n} r^n,
+
+each block is integrated on its own chord (the part of an edge within r <= R_b)
+and the channels are linear in the blocks.  This is the decomposition of
+`src/warpSPHBoundaries/edge/kernels.py:96-109` (`_blocks_from_pieces`): the
+outer piece at R = 1, and for every inner knot the difference of the two pieces
+that meet there.
+
+For one block the edge reduction needs six radial functions, all exact
+rationals derived here once:
+
+    P(r)            the profile                          (kernel gradient G, g1)
+    M(r)   = int_0^r t P dt                              (odd chord integral of P)
+    Psi(r) = M(r) - M(R)                                 (first moments m1, second moments m2)
+    Flam   = M(r) / r^2,   singular part  -M(R) / r^2    (lambda value term)
+    MPsi(r)= int_0^r t Psi dt                            (odd chord integral of Psi)
+    FPsi   = MPsi(r) / r^2, singular part -MPsi(R) / r^2 (the Psi area term of m20 / m02)
+
+`emit_header()` writes them as literal coefficients into a C++ header that the
+CUDA kernels include (`csrc/kernel_tables.h`), so the per-pair code carries
+every coefficient as an immediate operand.
+
+The kernel shapes and their 2-D normalisations follow
+`src/warpSPHBoundaries/curvbound/kernels.py:1-14,37-50` (cubic, Wendland C2/C4/C6)
+and `src/warpSPHBoundaries/edge/kernels.py:124-181` (truncated-power kernels).
+The normalisation is recomputed here from 2 * int_0^1 r (pi W) dr = 1 and checked
+against the published constants.
+"""
+from dataclasses import dataclass, field
+from fractions import Fraction as F
+from functools import lru_cache
+from math import comb
+from typing import Dict, List, Tuple
+
+# kernel ids of the C ABI (include/wsb.h: WSB_KERNEL_*); order is part of the ABI
+KERNEL_IDS = {"cubic": 0, "w2": 1, "w4": 2, "w6": 3, "quartic": 4, "quintic": 5, "poly6": 6}
+KERNEL_NAMES = {v: k for k, v in KERNEL_IDS.items()}
+
+# published 2-D normalisations C2 * pi (src/warpSPHBoundaries/curvbound/kernels.py:5-13,
+# src/warpSPHBoundaries/edge/kernels.py:183-185); only used to check the recomputed ones
+_PUBLISHED_C2PI = {"cubic": F(80, 7), "w2": F(7), "w4": F(9), "w6": F(78, 7),
+                   "quartic": F(46875, 2398), "quintic": F(15309, 478), "poly6": F(4)}
+
+
+# ------------------------------------------------------------------ polynomial helpers (ascending coefficient lists)
+def _padd(a, b):
+    n = max(len(a), len(b))
+    return [(a[i] if i < len(a) else 0) + (b[i] if i < len(b) else 0) for i in range(n)]
+
+
+def _pmul(a, b):
+    out = [F(0)] * (len(a) + len(b) - 1)
+    for i, x in enumerate(a):
+        for j, y in enumerate(b):
+            out[i + j] += x * y
+    return out
+
+
+def _ppow(a, k):
+    out = [F(1)]
+    for _ in range(k):
+        out = _pmul(out, a)
+    return out
+
+
+def _peval(a, x):
+    acc = F(0)
+    for c in reversed(a):
+        acc = acc * x + c
+    return acc
+
+
+def _trim(a):
+    a = list(a)
+    while len(a) > 1 and a[-1] == 0:
+        a.pop()
+    return a
+
+
+def _shape_integral(pieces):
+    """int_0^1 r * shape(r) dr over the pieces [(lo, hi, coeffs)]."""
+    tot = F(0)
+    for lo, hi, c in pieces:
+        P = [F(0)] + [F(0)] + [x / (i + 2) for i, x in enumerate(c)]     # int r^(n+1) = r^(n+2)/(n+2)
+        tot += _peval(P, hi) - _peval(P, lo)
+    return tot
+
+
+# ------------------------------------------------------------------ kernel shapes
+def _pieces(name):
+    """pieces [(lo, hi, shape coefficients)] of the UNNORMALISED shape on [0, 1]."""
+    one_minus = [F(1), F(-1)]
+    if name == "cubic":
+        half = [F(1, 2), F(-1)]
+        inner = _padd(_ppow(one_minus, 3), [-4 * x for x in _ppow(half, 3)])
+        return [(F(0), F(1, 2), inner), (F(1, 2), F(1), _ppow(one_minus, 3))]
+    if name in ("w2", "w4", "w6"):
+        n, poly = {"w2": (4, [F(1), F(4)]),
+                   "w4": (6, [F(1), F(6), F(35, 3)]),
+                   "w6": (8, [F(1), F(8), F(25), F(32)])}[name]
+        return [(F(0), F(1), _pmul(_ppow(one_minus, n), poly))]
+    if name == "poly6":
+        return [(F(0), F(1), [F(1), F(0), F(-3), F(0), F(3), F(0), F(-1)])]
+    terms = {"quartic": [(1, F(1), 4), (-5, F(3, 5), 4), (10, F(1, 5), 4)],
+             "quintic": [(1, F(1), 5), (-6, F(2, 3), 5), (15, F(1, 3), 5)]}.get(name)
+    if terms is None:
+        raise KeyError(f"unknown kernel {name!r}; expected one of {sorted(KERNEL_IDS)}")
+    knots = sorted({R for _, R, _ in terms})
+    pieces, lo = [], F(0)
+    for hi in knots:
+        poly = [F(0)]
+        for c, R, p in terms:
+            if R >= hi:
+                poly = _padd(poly, [F(c) * x for x in _ppow([R, F(-1)], p)])
+        pieces.append((lo, hi, poly))
+        lo = hi
+    return pieces
+
+
+@dataclass(frozen=True)
+class Block:
+    """one truncated block  P(r) 1[r <= R]  of pi*W and its derived exact profiles (h = 1)."""
+    R: F
+    c: Tuple[F, ...]          # P
+    m: Tuple[F, ...]          # M(r) = int_0^r t P dt        (coefficient list in r)
+    Mhat: F                   # M(R)
+    psi: Tuple[F, ...]        # Psi = M - M(R)
+    flam: Tuple[F, ...]       # M(r)/r^2                     (regular part of the lambda value profile)
+    mpsi: Tuple[F, ...]       # MPsi(r) = int_0^r t Psi dt
+    MPhat: F                  # MPsi(R)
+    fpsi: Tuple[F, ...]       # MPsi(r)/r^2
+    n4: Tuple[F, ...]         # N(r) = int_0^r t^3 P dt      (odd cubic chord integral, adjoint)
+
+
+@dataclass(frozen=True)
+class Kernel:
+    name: str
+    kid: int
+    c2pi: F                                   # C2 * pi of the normalised kernel
+    pieces: Tuple[Tuple[F, F, Tuple[F, ...]], ...]   # normalised pi*W pieces (lo, hi, coeffs)
+    blocks: Tuple[Block, ...]                 # sorted by R descending
+    mass: F                                   # int_plane W dA  (= 1)
+    plane2: F                                 # int_plane y_x^2 W dA  (h = 1)
+
+    @property
+    def max_degree(self):
+        """largest monomial power of r whose chord integral the forward channels need (Psi / FPsi)."""
+        return max(max(len(b.psi), len(b.fpsi), len(b.c)) - 1 for b in self.blocks)
+
+
+def _block(R, c):
+    c = _trim(c)
+    m = [F(0), F(0)] + [x / (n + 2) for n, x in enumerate(c)]
+    Mhat = _peval(m, R)
+    psi = list(m)
+    psi[0] -= Mhat
+    flam = [x / (n + 2) for n, x in enumerate(c)]
+    mpsi = [F(0), F(0)] + [x / (n + 2) for n, x in enumerate(psi)]
+    MPhat = _peval(mpsi, R)
+    fpsi = [x / (n + 2) for n, x in enumerate(psi)]
+    n4 = [F(0)] * 4 + [x / (n + 4) for n, x in enumerate(c)]
+    t = lambda a: tuple(_trim(a))
+    return Block(F(R), t(c), t(m), Mhat, t(psi), t(flam), t(mpsi), MPhat, t(fpsi), t(n4))
+
+
+@lru_cache(maxsize=None)
+def kernel(name: str) -> Kernel:
+    """the exact kernel table of `name` (cubic, w2, w4, w6, quartic, quintic, poly6)."""
+    raw = _pieces(name)
+    C = 1 / (2 * _shape_integral(raw))
+    if C != _PUBLISHED_C2PI[name]:
+        raise AssertionError(f"normalisation of {name}: {C} != published {_PUBLISHED_C2PI[name]}")
+    pieces = tuple((lo, hi, tuple(C * x for x in c)) for lo, hi, c in raw)
+    blocks = []
+    for j in range(len(pieces) - 1, -1, -1):          # outer piece first, then the differences at the inner knots
+        lo, hi, c = pieces[j]
+        coeffs = list(c) if j == len(pieces) - 1 else _padd(list(c), [-x for x in pieces[j + 1][2]])
+        blocks.append(_block(hi, coeffs))
+    blocks = tuple(sorted(blocks, key=lambda b: -b.R))
+    mass = 2 * sum(b.Mhat for b in blocks)
+    plane2 = -2 * sum(b.MPhat for b in blocks)
+    if mass != 1:
+        raise AssertionError(f"{name}: block masses sum to {mass}")
+    return Kernel(name, KERNEL_IDS[name], C, pieces, blocks, mass, plane2)
+
+
+def pi_w(name, r: F) -> F:
+    """exact pi * W(r) (h = 1) from the blocks (tests)."""
+    return sum((_peval(b.c, r) for b in kernel(name).blocks if r <= b.R), F(0))
+
+
+# ------------------------------------------------------------------ reference term plan (the "plain" interpreter route)
+def _phi(P, R):
+    """Phi[f](r) = -int_r^R t f dt as {n: c} (the compact potential of src/warpSPHBoundaries/edge/np2d.py:45-52)."""
+    out, const = {}, F(0)
+    for n, c in P.items():
+        out[n + 2] = out.get(n + 2, 0) + c / (n + 2)
+        const -= c * F(R) ** (n + 2) / (n + 2)
+    out[0] = out.get(0, 0) + const
+    return {n: c for n, c in out.items() if c != 0}
+
+
+def _compile(P, R, alpha, mult, edges, values):
+    """the compact-potential recursion of src/warpSPHBoundaries/edge/np2d.py:63-79 (truncated form only)."""
+    a, b = alpha
+    if a + b == 0:
+        d = values.setdefault(R, {})
+        for n, c in P.items():
+            d[n] = d.get(n, 0) + mult * c
+        return
+    i = 0 if a > 0 else 1
+    beta = (a - 1, b) if i == 0 else (a, b - 1)
+    Ph = _phi(P, R)
+    d = edges.setdefault((i, beta, R), {})
+    for n, c in Ph.items():
+        d[n] = d.get(n, 0) + mult * c
+    bi = beta[i]
+    if bi >= 1:
+        bm = (beta[0] - (i == 0), beta[1] - (i == 1))
+        _compile(Ph, R, bm, -mult * bi, edges, values)
+
+
+def compile_moment(name, alpha):
+    """exact truncated plan of m_alpha: edges {(i, beta, R): {n: c}}, values {R: {n: c}} (pi-free)."""
+    edges, values = {}, {}
+    for blk in kernel(name).blocks:
+        P = {n: c for n, c in enumerate(blk.c) if c != 0}
+        _compile(P, blk.R, tuple(alpha), F(1), edges, values)
+    edges = {k: {n: c for n, c in d.items() if c != 0} for k, d in edges.items()}
+    values = {R: {n: c for n, c in d.items() if c != 0} for R, d in values.items()}
+    return edges, {R: d for R, d in values.items() if d}
+
+
+@dataclass
+class TermPlan:
+    """flat term tables of the twelve edge channels (the layout of the reference's per-pair interpreter,
+    src/warpSPHBoundaries/edge/warpbc.py:40-129 restricted to the truncated terms its edge kernels evaluate,
+    warpbc.py:637-661, plus the second-moment plan of warpbc.py:970-991 as channels 9..11)."""
+    radii: List[float] = field(default_factory=list)
+    cn: List[int] = field(default_factory=list)
+    cc: List[float] = field(default_factory=list)
+    E: List[tuple] = field(default_factory=list)     # (ch, i, a, b, Ridx, c0, c1)
+    V: List[tuple] = field(default_factory=list)     # (ch, Ridx, c0, c1, mR)
+
+    def R(self, R):
+        f = float(R)
+        if f not in self.radii:
+            self.radii.append(f)
+        return self.radii.index(f)
+
+    def coef(self, P, scale):
+        c0 = len(self.cn)
+        for n, c in sorted(P.items()):
+            self.cn.append(n)
+            self.cc.append(float(F(c) * scale))
+        return c0, len(self.cn)
+
+    def edge(self, ch, i, beta, R, P, scale):
+        self.E.append((ch, i, beta[0], beta[1], self.R(R), *self.coef(P, scale)))
+
+    def value(self, ch, R, P, scale):
+        mR = sum(c * F(R) ** (n + 2) / (n + 2) for n, c in P.items())
+        self.V.append((ch, self.R(R), *self.coef({n: c / (n + 2) for n, c in P.items()}, scale), float(mR * scale)))
+
+    def moment(self, name, ch, alpha, scale):
+        edges, vals = compile_moment(name, alpha)
+        for (i, beta, R), P in edges.items():
+            self.edge(ch, i, beta, R, P, scale)
+        for R, P in vals.items():
+            self.value(ch, R, P, scale)
+
+
+@lru_cache(maxsize=None)
+def term_plan(name) -> TermPlan:
+    """the twelve-channel truncated term plan of `name`:
+    0 lam, 1-2 m1, 3-4 G, 5-8 g1 (g(1,0)_x, g(1,0)_y, g(0,1)_x, g(0,1)_y), 9-11 m20, m11, m02."""
+    k = kernel(name)
+    tp = TermPlan()
+    for ch, al in enumerate([(0, 0), (1, 0), (0, 1)]):
+        tp.moment(name, ch, al, F(1))
+    for kk, al in enumerate([(0, 0), (1, 0), (0, 1)]):
+        for j in (0, 1):
+            ch = 3 + 2 * kk + j
+            for blk in k.blocks:
+                tp.edge(ch, j, al, blk.R, {n: c for n, c in enumerate(blk.c) if c != 0}, F(-1))
+            if al[j]:
+                beta = (al[0] - (j == 0), al[1] - (j == 1))
+                tp.moment(name, ch, beta, F(al[j]))
+    for ch, al in zip((9, 10, 11), [(2, 0), (1, 1), (0, 2)]):
+        tp.moment(name, ch, al, F(1))
+    return tp
+
+
+# ------------------------------------------------------------------ C++ header generation
+def _lit(x) -> str:
+    v = float(x)
+    if v == 0:
+        return "0.0"
+    return repr(v)
+
+
+def _dot(coeffs, arr, start=0):
+    """C expression  sum_n coeffs[n] * arr[n + start]  (zero coefficients dropped)."""
+    parts = [f"{_lit(c)}*{arr}[{n + start}]" for n, c in enumerate(coeffs) if c != 0]
+    return " + ".join(parts) if parts else "0.0"
+
+
+def _horner(coeffs, var):
+    """C expression evaluating sum_n coeffs[n] var^n by Horner's rule (leading zero coefficients
+    become a power factor, so no fma(x, r, 0.0) appears)."""
+    cs = list(coeffs)
+    while len(cs) > 1 and cs[-1] == 0:
+        cs.pop()
+    low = 0
+    while low < len(cs) - 1 and cs[low] == 0:
+        low += 1
+    cs = cs[low:]
+    expr = _lit(cs[-1])
+    for c in reversed(cs[:-1]):
+        expr = f"fma({expr}, {var}, {_lit(c)})"
+    for _ in range(low):
+        expr = f"({expr})*{var}"
+    return expr
+
+
+def emit_header() -> str:
+    """the generated C++ header with every kernel's block profiles as literal code."""
+    out = ["// GENERATED by warpsphboundaries_b200/kernels.py (emit_header); do not edit by hand.",
+           "// Exact rational kernel profiles rounded once to double; see that module for the algebra.",
+           "#pragma once", "", "namespace wsb {", ""]
+    out.append(f"constexpr int kNumKernels = {len(KERNEL_IDS)};")
+    # the largest A_n index any kernel needs: forward max_degree, adjoint needs c up to deg+2 (s^2 W) on A
+    amax = max(max(kernel(n).max_degree, max(len(b.c) + 1 for b in kernel(n).blocks)) for n in KERNEL_IDS)
+    out.append(f"constexpr int kMaxA = {amax + 1};   // A_n, n = 0 .. kMaxA-1")
+    out.append("")
+    out.append("struct BlockSums {      // per (pair, block) chord sums, before the 1/pi and the edge frame")
+    out.append("  double W0, W1;        // int P ds, int s P ds")
+    out.append("  double P0, P1;        // int Psi ds, int s Psi ds")
+    out.append("  double Lreg, Preg;    // int M/r^2 ds, int MPsi/r^2 ds (regular parts of the value terms)")
+    out.append("  double Mhat, MPhat;   // singular coefficients M(R), MPsi(R)")
+    out.append("};")
+    out.append("")
+    out.append("struct AdjSums {        // per (pair, block) chord sums of the adjoint")
+    out.append("  double W0, W1, W2, W3;   // int s^j P ds, j = 0..3")
+    out.append("};")
+    out.append("")
+    for name, kid in sorted(KERNEL_IDS.items(), key=lambda t: t[1]):
+        k = kernel(name)
+        out.append(f"// ---- {name}: C2*pi = {k.c2pi}, plane second moment {k.plane2}")
+        out.append(f"struct Kern_{name} {{")
+        out.append(f"  static constexpr int kId = {kid};")
+        out.append(f"  static constexpr int kBlocks = {len(k.blocks)};")
+        out.append(f"  static constexpr double kMass = {_lit(k.mass)};")
+        out.append(f"  static constexpr double kPlane2 = {_lit(k.plane2)};")
+        nA = [max(len(b.psi), len(b.fpsi), len(b.c)) for b in k.blocks]
+        nAadj = [len(b.c) + 2 for b in k.blocks]
+        out.append("  static constexpr double kR[kBlocks] = {" + ", ".join(_lit(b.R) for b in k.blocks) + "};")
+        out.append("  static constexpr int kNA[kBlocks] = {" + ", ".join(str(n) for n in nA) + "};   // A_0..A_{kNA-1} for the forward sums")
+        out.append("  static constexpr int kNAadj[kBlocks] = {" + ", ".join(str(n) for n in nAadj) + "};   // for the adjoint sums")
+        out.append("  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);")
+        out.append("  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);")
+        out.append("};")
+        for bi, b in enumerate(k.blocks):
+            out.append(f"template <> __host__ __device__ __forceinline__ void Kern_{name}::sums<{bi}>(const double* A, double rlo, double rhi, BlockSums& o) {{")
+            out.append(f"  // block R = {b.R}: P = {[str(x) for x in b.c]}")
+            out.append(f"  o.W0 = {_dot(b.c, 'A')};")
+            out.append(f"  o.W1 = ({_horner(b.m, 'rhi')}) - ({_horner(b.m, 'rlo')});")
+            out.append(f"  o.P0 = {_dot(b.psi, 'A')};")
+            out.append(f"  o.P1 = ({_horner(b.mpsi, 'rhi')}) - ({_horner(b.mpsi, 'rlo')});")
+            out.append(f"  o.Lreg = {_dot(b.flam, 'A')};")
+            out.append(f"  o.Preg = {_dot(b.fpsi, 'A')};")
+            out.append(f"  o.Mhat = {_lit(b.Mhat)};")
+            out.append(f"  o.MPhat = {_lit(b.MPhat)};")
+            out.append("}")
+            out.append(f"template <> __host__ __device__ __forceinline__ void Kern_{name}::adj<{bi}>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {{")
+            out.append(f"  const double a0 = {_dot(b.c, 'A')};")
+            out.append(f"  const double a2 = {_dot(b.c, 'A', 2)};")
+            out.append(f"  const double m1 = ({_horner(b.m, 'rhi')}) - ({_horner(b.m, 'rlo')});")
+            out.append(f"  const double m3 = ({_horner(b.n4, 'rhi')}) - ({_horner(b.n4, 'rlo')});")
+            out.append("  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;")
+            out.append("}")
+        out.append("")
+    # the reference term plan tables for the plain interpreter route
+    out.append("// ---- reference term plans (plain FP64 interpreter): per kernel offsets into flat tables")
+    E, V, CN, CC, RAD, offs = [], [], [], [], [], []
+    for name, kid in sorted(KERNEL_IDS.items(), key=lambda t: t[1]):
+        tp = term_plan(name)
+        e0, v0, c0, r0 = len(E), len(V), len(CN), len(RAD)
+        for (ch, i, a, b, Ri, ca, cb) in tp.E:
+            E.append((ch, i, a, b, r0 + Ri, c0 + ca, c0 + cb))
+        for (ch, Ri, ca, cb, mR) in tp.V:
+            V.append((ch, r0 + Ri, c0 + ca, c0 + cb, mR))
+        CN.extend(tp.cn)
+        CC.extend(tp.cc)
+        RAD.extend(tp.radii)
+        offs.append((e0, len(E), v0, len(V)))
+    out.append(f"constexpr int kPlanEdgeTerms = {len(E)};")
+    out.append(f"constexpr int kPlanValueTerms = {len(V)};")
+    out.append(f"constexpr int kPlanCoeffs = {len(CN)};")
+    out.append(f"constexpr int kPlanRadii = {len(RAD)};")
+    out.append("struct PlanOffsets { int e0, e1, v0, v1; };")
+    out.append("static const PlanOffsets kPlanOffsets[kNumKernels] = {" + ", ".join("{%d, %d, %d, %d}" % o for o in offs) + "};")
+    out.append("static const int kPlanE[kPlanEdgeTerms][7] = {   // ch, i, a, b, radius index, c0, c1")
+    out.extend("  {%d, %d, %d, %d, %d, %d, %d}," % e for e in E)
+    out.append("};")
+    out.append("static const int kPlanVi[kPlanValueTerms][4] = {   // ch, radius index, c0, c1")
+    out.extend("  {%d, %d, %d, %d}," % v[:4] for v in V)
+    out.append("};")
+    out.append("static const double kPlanVmR[kPlanValueTerms] = {" + ", ".join(_lit(v[4]) for v in V) + "};")
+    out.append("static const int kPlanCn[kPlanCoeffs] = {" + ", ".join(str(x) for x in CN) + "};")
+    out.append("static const double kPlanCc[kPlanCoeffs] = {" + ", ".join(_lit(x) for x in CC) + "};")
+    out.append("static const double kPlanRadii[kPlanRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
+    out.append("")
+    out.append("}  // namespace wsb")
+    out.append("")
+    return "\n".join(out)
+
+
+def plane_channels(name):
+    """the twelve channel values of a solid that covers the whole support (indicator 1), h = 1:
+    lam = 1, g1 diagonal = 1, m20 = m02 = plane second moment; zero elsewhere."""
+    k = kernel(name)
+    m, p2 = float(k.mass), float(k.plane2)
+    return [m, 0.0, 0.0, 0.0, 0.0, m, 0.0, 0.0, m, p2, 0.0, p2]
+
+
+if __name__ == "__main__":       # python -m warpsphboundaries_b200.kernels  -> regenerate the header
+    import pathlib
+    p = pathlib.Path(__file__).parent / "csrc" / "kernel_tables.h"
+    p.write_text(emit_header())
+    print("wrote", p)
