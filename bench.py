@@ -1,0 +1,381 @@
+"""Throughput of the boundary-integral hot path on the large 2-D scene.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference] [--precision mixed|fp64] [--route fused|plain]
+
+Workload (one step): lambda + the twelve moments of every particle of the large 2-D scene (2^20 particles uniform in
+[0, 4]^2, h = 0.02, 64 seeded star polygons in one multi-loop surface, near-tangent particles) for each of the kernels
+cubic, w2, w4, w6.  Metric: particle-edge neighbour pairs per second (pairs = pairs passing the float64 neighbour
+predicate, counted once, times the number of kernels).  `value` is measured with inputs resident on the device;
+`e2e` through the public provider API with host buffers (pinned host -> device copy of positions and supports, device
+-> host copy of lam, G, Cov of every kernel) inside the timed region.  Between timed steps L2 is flushed by writing a
+256 MiB buffer (outside the events).  Multi-GPU: one process per GPU, each its own particle set of the same size over
+the same geometry (weak scaling, no data-path collective); time = max over ranks.
+
+--impl reference times the reference algorithm on the host cores: the oracle port (oracle/edge2d.py, a CPU
+restatement of the reference's numpy path) over a bounded particle sample, all cores in worker processes.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+KERNELS = ["cubic", "w2", "w4", "w6"]
+METRIC = "particle-edge pairs/s (lambda + 12 moments, 4 kernels, 2^20-particle 2-D scene)"
+UNIT = "pairs/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--route", default="fused", choices=["fused", "plain"])
+    p.add_argument("--particles", type=int, default=1 << 20)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
+    return p.parse_args()
+
+
+def workload(n, rank):
+    from warpsphboundaries_b200 import workloads
+    loops, X, h = workloads.c2(n_particles=n, seed=0)
+    if rank:
+        X = np.random.default_rng(1000 + rank).uniform(0, 4.0, size=X.shape)
+    return loops, X, h
+
+
+# ----------------------------------------------------------------------------------------------- reference (CPU) arm
+def _oracle_chunk(args):
+    loops, X, h, kernel = args
+    from oracle import edge2d as O
+    from warpsphboundaries_b200 import workloads
+    V, E = workloads.edges_of(loops)
+    out, slots, ind = O.local_twelve(V, E, 0, X, np.full(len(X), h), kernel, h, return_slots=True)
+    return sum(len(s) for s in slots)
+
+
+def cpu_reference(loops, X, h, seconds=15.0, procs=None):
+    """pairs/s of the oracle port over a bounded sample: chunks of near-wall-rich particles across all host cores."""
+    import multiprocessing as mp
+    procs = procs or os.cpu_count() or 1
+    rng = np.random.default_rng(7)
+    chunk = 2048
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    pairs = 0
+    done = 0
+    with ctx.Pool(procs) as pool:
+        while True:
+            jobs = [(loops, X[rng.choice(len(X), chunk, replace=False)], h, KERNELS[(done + i) % 4]) for i in range(procs)]
+            pairs += sum(pool.map(_oracle_chunk, jobs))
+            done += procs
+            if time.perf_counter() - t0 > seconds:
+                break
+    dt = time.perf_counter() - t0
+    return pairs / dt, procs, f"{done} chunks of {chunk} random particles of the scene, kernels cycled; {pairs} pairs in {dt:.1f} s"
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    loops, X, h = workload(args.particles, 0)
+    steps = []
+    sample = ""
+    procs = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference(loops, X, h, seconds=1.0, procs=procs)
+    for _ in range(args.steps):
+        v, procs, sample = cpu_reference(loops, X, h, seconds=8.0, procs=procs)
+        steps.append(v)
+    value = float(statistics.mean(steps))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "c2: 2^20 particles in [0,4]^2, h=0.02, 64 star polygons (32-512 vertices), "
+                                   "kernels cubic/w2/w4/w6", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------------- clocks
+class Clocks:
+    def __init__(self):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self, index):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        for ln in open(self.path):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------------- our arm
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    from warpsphboundaries_b200 import _lib
+    from warpsphboundaries_b200.fixedadj import fixed_topology
+    from warpsphboundaries_b200.kernels import KERNEL_IDS, pair_work
+    from warpsphboundaries_b200.provider import AnalyticBoundary, WallOutput
+    from warpsphboundaries_b200.scene import Body, Scene, SurfaceRep, _stream
+    from warpsphboundaries_b200.shim import KernelFunctions, ParticleState
+
+    loops, X, h = workload(args.particles, rank)
+    N = len(X)
+    rep = SurfaceRep.loops(loops)
+    body = Body(center=(0.0, 0.0), angle=0.0, reps=[rep])
+    scene = Scene([body], dev)
+    pos = torch.tensor(X, dtype=torch.float64, device=dev).contiguous()
+    sup = torch.full((N,), h, dtype=torch.float64, device=dev)
+    ns = rep.native(h, dev)
+    # neighbour pairs of the workload (kernel independent), counted once outside the timing
+    ft = fixed_topology(rep, pos, sup, torch.ones(N, dtype=torch.bool, device=dev), h)
+    P = int((ft.e >= 0).sum())
+    del ft
+    torch.cuda.empty_cache()
+    ws, need = ns.workspace(N)
+    pose = body.pose_tensor(dev)
+    obb = (_lib.ctypes.c_double * 4)(*body.obb())
+    outs = {k: [torch.zeros(N, dtype=torch.float64, device=dev), torch.zeros((N, 2), dtype=torch.float64, device=dev),
+                torch.zeros((N, 4), dtype=torch.float64, device=dev), torch.zeros((N, 2), dtype=torch.float64, device=dev),
+                torch.zeros((N, 4), dtype=torch.float64, device=dev)] for k in KERNELS}
+    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(precision, timers=None):
+        ev = []
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(_lib.lib.wsb_aggregate_prepare(ns.handle, _lib.ptr(pos), _lib.ptr(sup), None, N, _lib.ptr(pose),
+                                                  obb, 0, _lib.ptr(ws), need, _stream()), "prepare")
+        e1 = torch.cuda.Event(enable_timing=True)
+        e1.record(stream)
+        ev.append(("prepare", e0, e1))
+        for k in KERNELS:
+            o = outs[k]
+            for t in o:
+                t.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _lib.check(_lib.lib.wsb_aggregate_evaluate(ns.handle, KERNEL_IDS[k], prec[precision], _lib.ptr(sup), N,
+                                                       _lib.ptr(pose), _lib.OUT_ALL, *[_lib.ptr(t) for t in o],
+                                                       _lib.ptr(ws), need, _stream()), "evaluate")
+            b = torch.cuda.Event(enable_timing=True)
+            b.record(stream)
+            ev.append((k, a, b))
+        if timers is not None:
+            timers.append(ev)
+
+    def timed(precision, steps, warmup):
+        for _ in range(warmup):
+            step(precision)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        timers = []
+        for _ in range(steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            step(precision, timers)
+            torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        step_ms = [ev[0][1].elapsed_time(ev[-1][2]) for ev in timers]
+        eval_ms = {k: statistics.mean(e[i + 1][1].elapsed_time(e[i + 1][2]) for e in timers)
+                   for i, k in enumerate(KERNELS)}
+        prep_ms = statistics.mean(e[0][1].elapsed_time(e[0][2]) for e in timers)
+        return sum(step_ms), eval_ms, prep_ms
+
+    clocks = Clocks()
+    clocks.start(local)
+    total_ms, eval_ms, prep_ms = timed(args.precision, args.steps, args.warmup)
+    clk = clocks.stop()
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    pairs_step = P * len(KERNELS)
+    value = pairs_step * args.steps * world / (total_ms * 1e-3)
+
+    # ---- roofline of the dominant kernel (the fused evaluate pass): algorithmic float64 flops per launch
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    import ctypes
+    pk = ctypes.CDLL(os.path.join(ROOT, "warpsphboundaries_b200", "_build", "libwsbpeak.so"))
+    pk.wsbpeak_fp64_tflops.restype = ctypes.c_double
+    pk.wsbpeak_fp32_tflops.restype = ctypes.c_double
+    fp64_peak = max(pk.wsbpeak_fp64_tflops(200000) for _ in range(3))
+    fp32_peak = max(pk.wsbpeak_fp32_tflops(200000) for _ in range(3))
+    flops = {k: P * pair_work(k)["flops"] for k in KERNELS}
+    achieved = sum(flops.values()) / (sum(eval_ms.values()) * 1e-3) / 1e12
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "agg_main_traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    extra = {}
+    if args.extra and world == 1:
+        other = "fp64" if args.precision == "mixed" else "mixed"
+        ms_o, ev_o, _ = timed(other, max(3, args.steps // 2), 1)
+        extra[f"fused_{other}_pairs_per_s"] = pairs_step * max(3, args.steps // 2) / (ms_o * 1e-3)
+        # the plain FP64 route (the reference's structure: slots, per-slot plan interpreter, contraction)
+        ab = AnalyticBoundary(scene, route="plain")
+        ps = ParticleState(pos, sup)
+        for _ in range(1):
+            ab.aggregate(ps, h, kernel=KernelFunctions.Wendland4, lean=True)
+        torch.cuda.synchronize()
+        tp0 = time.perf_counter()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for kf in (KernelFunctions.CubicSpline, KernelFunctions.Wendland2, KernelFunctions.Wendland4, KernelFunctions.Wendland6):
+            ab.aggregate(ps, h, kernel=kf, lean=True)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        extra["plain_fp64_pairs_per_s"] = pairs_step / (s0.elapsed_time(s1) * 1e-3)
+        del ab
+        torch.cuda.empty_cache()
+
+    # ---- end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        ab = AnalyticBoundary(scene, route="fused", precision=args.precision)
+        hpos = torch.tensor(X, dtype=torch.float64).pin_memory()
+        hsup = torch.full((N,), h, dtype=torch.float64).pin_memory()
+        dpos = torch.empty_like(pos)
+        dsup = torch.empty_like(sup)
+        host_out = {k: [torch.empty((1, N), dtype=torch.float64).pin_memory(),
+                        torch.empty((1, N, 2), dtype=torch.float64).pin_memory(),
+                        torch.empty((1, N, 2, 2), dtype=torch.float64).pin_memory()] for k in KERNELS}
+        kf = {"cubic": KernelFunctions.CubicSpline, "w2": KernelFunctions.Wendland2, "w4": KernelFunctions.Wendland4,
+              "w6": KernelFunctions.Wendland6}
+
+        def e2e_step():
+            dpos.copy_(hpos, non_blocking=True)
+            dsup.copy_(hsup, non_blocking=True)
+            ps = ParticleState(dpos, dsup)
+            for k in KERNELS:
+                fw = ab.aggregate(ps, h, kernel=kf[k], lean=True)
+                for dst, name in zip(host_out[k], ("lam", "G", "Cov")):
+                    dst.copy_(fw.out[name], non_blocking=True)
+
+        for _ in range(args.warmup):
+            e2e_step()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            e2e_step()
+            b.record(stream)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        t = torch.tensor([tot], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = {"value": pairs_step * args.steps * world / (float(t.item()) * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": N * 3 * 8, "d2h_bytes_per_step": len(KERNELS) * N * 7 * 8,
+               "ms_per_step": float(t.item()) / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, procs, sample = cpu_reference(loops, X, h, seconds=12.0, procs=1)
+        cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+                "data": "synthetic (seeded)",
+                "config": {"workload": "c2: 2^20 particles uniform in [0,4]^2, h=0.02, 64 star polygons (32-512 "
+                                       "vertices, one multi-loop surface), kernels cubic/w2/w4/w6, lambda + 12 moments",
+                           "pairs_per_kernel": P, "particles_per_gpu": N, "route": args.route,
+                           "precision": args.precision, "l2": "flushed between steps (256 MiB write, untimed)"},
+                "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                             "frac": achieved / fp64_peak, "traffic": traffic,
+                             "kernel": "k_agg_main (wsb_aggregate_evaluate)",
+                             "flops_per_pair": {k: pair_work(k)["flops"] for k in KERNELS},
+                             "peak_source": "measured: libwsbpeak FP64 FMA stream (this GPU, this run)",
+                             "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
+                "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
+                "gpu_launches": args.steps * (2 + len(KERNELS)),
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, **({"extra": extra} if extra else {})}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

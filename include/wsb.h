@@ -1,0 +1,149 @@
+/*
+ * wsb.h -- C ABI of the B200 boundary-integral library (libwsb.so).
+ *
+ * Exact semi-analytic SPH boundary integrals of 2-D polygonal walls: the kernel
+ * mass lambda and the twelve surface moments (m1, G, g1 = int y (x) grad W,
+ * m2) at fluid particles, their adjoint, signed distance and body kinematics.
+ * Plain pointers and sizes only; every array argument is DEVICE memory unless
+ * its comment says "host".  Streams are cudaStream_t passed as void*.
+ * Every entry point returns WSB_OK (0) or a negative WSB_ERR_* code; the text
+ * of the last error of the calling thread is wsb_last_error().
+ *
+ * Each entry point names the reference interface (wi-re/warpSPHBoundaries,
+ * path:line inside that project) it replaces.
+ */
+#ifndef WSB_H
+#define WSB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  WSB_OK = 0,
+  WSB_ERR_ARG = -1,          /* invalid argument (the Python facade raises ValueError) */
+  WSB_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+  WSB_ERR_UNSUPPORTED = -3,  /* unsupported kernel / mode (NotImplementedError) */
+  WSB_ERR_SIZE = -4,         /* a buffer or workspace is too small */
+  WSB_ERR_DEVICE = -5        /* a device-side check failed (status word set) */
+};
+
+/* kernel ids (warpsphboundaries_b200/kernels.py: KERNEL_IDS) */
+enum {
+  WSB_KERNEL_CUBIC = 0, WSB_KERNEL_W2 = 1, WSB_KERNEL_W4 = 2, WSB_KERNEL_W6 = 3,
+  WSB_KERNEL_QUARTIC = 4, WSB_KERNEL_QUINTIC = 5, WSB_KERNEL_POLY6 = 6
+};
+
+/* arithmetic of the fused aggregate */
+enum {
+  WSB_PREC_FP64 = 0,   /* every step in float64 */
+  WSB_PREC_MIXED = 1   /* float32 special functions where the per-pair error bound allows, float64 guards and sums */
+};
+
+/* output selection bits of wsb_aggregate */
+enum { WSB_OUT_LAM = 1, WSB_OUT_G = 2, WSB_OUT_COV = 4, WSB_OUT_M1 = 8, WSB_OUT_M2 = 16, WSB_OUT_ALL = 31 };
+
+typedef struct wsb_surface wsb_surface;
+
+typedef struct {
+  int64_t n_verts, n_edges;
+  int32_t nx, ny;            /* edge cell grid (cell = support_max) */
+  double lo_x, lo_y, cell;
+  int32_t K;                 /* largest number of edges in one cell: slots per row of the fixed topology */
+  int64_t n_items;           /* entries of the cell list */
+  int32_t n_bins;            /* y bins of the ray-cast indicator */
+  double bbox_lo_x, bbox_lo_y, bbox_hi_x, bbox_hi_y;   /* vertex bounding box (body frame) */
+  int background;
+  double support_max;
+} wsb_surface_info;
+
+const char* wsb_last_error(void);
+int wsb_version(void);
+
+/* Static structures of one closed surface (loops counter-clockwise around the solid) for supports <= support_max:
+ * edge cell list, per-cell indicator cache, y bins.  verts [n_verts*2] and edges [n_edges*2] are HOST arrays.
+ * Replaces SurfaceRep.__init__/_celllist/_cell_indicator/_ybins (src/warpSPHBoundaries/scene/scene.py:222-327)
+ * and fixedadj._static (src/warpSPHBoundaries/scene/fixedadj.py:150-165). */
+int wsb_surface_create(const double* verts, int64_t n_verts, const int32_t* edges, int64_t n_edges,
+                       int background, double support_max, int device, wsb_surface** out);
+int wsb_surface_destroy(wsb_surface* s);
+int wsb_surface_info_get(const wsb_surface* s, wsb_surface_info* out);
+/* host copies of the cell list (start [nx*ny+1], items [n_items]) for tests */
+int wsb_surface_cells(const wsb_surface* s, int32_t* start_host, int32_t* items_host);
+
+/* Fixed-capacity slots and indicator of rows lpos [n*2] (body frame), supports lsup [n], valid [n] (int32, may be NULL):
+ * slots [n*K] int32 (-1 = empty), edges in cell-list order; ind [n] float64 (winding number + background, 0 for
+ * invalid rows).  Replaces fixedadj.fixed_topology (src/warpSPHBoundaries/scene/fixedadj.py:67-147, 168-182). */
+int wsb_fixed_topology(const wsb_surface* s, const double* lpos, const double* lsup, const int32_t* valid, int64_t n,
+                       int32_t* slots, double* ind, void* stream);
+
+/* Plain FP64 route, stage 1: the twelve edge channels of every slot, c [n*K*12] (units of h): one thread per slot
+ * interpreting the exact truncated term plan.  Replaces warpbc.edge_channels + second_channels
+ * (src/warpSPHBoundaries/edge/warpbc.py:619-661, 919-991) on a fixed topology. */
+int wsb_slot_channels_plain(const wsb_surface* s, int kernel, const double* lpos, const double* lsup,
+                            const int32_t* slots, int64_t n, double* c, void* stream);
+
+/* Plain FP64 route, stage 2: per row the slot channels in slot order + ind * plane channels, physical scaling,
+ * rotation to the world frame by rot [4] = (c, -s, s, c) (device), ADDED into lam [n], G [n*2], cov [n*4], m1 [n*2],
+ * m2 [n*4] (any of them may be NULL).  Replaces FusedWall.evaluate's _wall_contract_kernel and
+ * _second_contract_kernel (src/warpSPHBoundaries/scene/fused.py:69-154, 612-659). */
+int wsb_contract(const wsb_surface* s, int kernel, const int32_t* slots, const double* c, const double* ind,
+                 const double* lsup, int64_t n, const double* rot, double* lam, double* G, double* cov, double* m1,
+                 double* m2, void* stream);
+
+/* Workspace bytes wsb_aggregate needs for n rows. */
+size_t wsb_aggregate_workspace_size(const wsb_surface* s, int64_t n);
+
+/* Fused route: body-frame coordinates (Pose.toLocal), the body broadphase (support circle against the body box
+ * [obb_lo, obb_hi]; unbounded != 0 skips it), the fixed-capacity neighbour predicate, the twelve channels of every
+ * neighbour pair and the per-row contraction in ONE pass over rows sorted by cell; outputs ADDED as wsb_contract.
+ * pos [n*2] world, sup [n], allowed [n] int32 (may be NULL = all), pose [4] = (cx, cy, cos, sin) (device),
+ * obb [4] = (lo_x, lo_y, hi_x, hi_y) (host).  status [1] (device, may be NULL) receives a device error code.
+ * Replaces AnalyticBoundary.aggregate for one (body, SurfaceRep) (src/warpSPHBoundaries/scene/provider.py:89-110:
+ * fixed_adjacency fixedadj.py:249-270, FusedWall fused.py:506-564 and evaluate fused.py:612-659). */
+int wsb_aggregate(const wsb_surface* s, int kernel, int precision, const double* pos, const double* sup,
+                  const int32_t* allowed, int64_t n, const double* pose, const double* obb, int unbounded,
+                  int out_mask, double* lam, double* G, double* cov, double* m1, double* m2,
+                  void* workspace, size_t workspace_bytes, int32_t* status, void* stream);
+
+/* The two halves of wsb_aggregate, for callers that time or overlap them separately: _prepare forms the body-frame
+ * positions, the broadphase and the cell-sorted row order in the workspace; _evaluate runs the fused channel pass on a
+ * prepared workspace (any kernel / precision, repeatable for several kernels over one prepared position set). */
+int wsb_aggregate_prepare(const wsb_surface* s, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
+                          const double* pose, const double* obb, int unbounded, void* workspace,
+                          size_t workspace_bytes, void* stream);
+int wsb_aggregate_evaluate(const wsb_surface* s, int kernel, int precision, const double* sup, int64_t n,
+                           const double* pose, int out_mask, double* lam, double* G, double* cov, double* m1,
+                           double* m2, const void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint of wsb_aggregate's lam, m1, m2 (the moments m_alpha, |alpha| <= 2) by recomputation: given world-frame
+ * gradients g_lam [n], g_m1 [n*2], g_m2 [n*4] (any may be NULL), ADD dL/dpos into d_pos [n*2] (world) and dL/dvertex
+ * into d_verts [n_verts*2] (body frame; may be NULL).  Replaces warp2d.TorchMoment's backward and np2d
+ * moment_gradient / shape_gradient (src/warpSPHBoundaries/edge/warp2d.py:287-365, 482-500;
+ * src/warpSPHBoundaries/edge/np2d.py:554-565, 626-652). */
+int wsb_aggregate_backward(const wsb_surface* s, int kernel, const double* pos, const double* sup,
+                           const int32_t* allowed, int64_t n, const double* pose, const double* obb, int unbounded,
+                           const double* g_lam, const double* g_m1, const double* g_m2, double* d_pos,
+                           double* d_verts, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Signed distance of body-frame points lpos [m*2] to the surface: d [m] (> 0 in the fluid), closest point cp [m*2],
+ * unit normal n_loc [m*2] into the fluid, edge [m] int32.  norm_support > 0: the indicator uses that support
+ * normalisation (the sync-free route), else none.  Replaces the SurfaceRep branch of Scene.signed_distance
+ * (src/warpSPHBoundaries/scene/scene.py:1312-1350). */
+int wsb_signed_distance(const wsb_surface* s, const double* lpos, int64_t m, double norm_support, double* d,
+                        double* cp, double* n_loc, int32_t* edge, void* stream);
+
+/* Rigid-body fields of B bodies at world points x [n*2]: body [b] = (cx, cy, cos, sin, vx, vy, omega, ax, ay, alpha)
+ * (device [B*10]); writes rel, local, velocity, acceleration [B*n*2] (any may be NULL).  Replaces BodyKinematics
+ * (src/warpSPHBoundaries/scene/scene.py:1155-1225) and Body.velocityAt / accelerationAt (scene.py:934-939, 1063-1067). */
+int wsb_kinematics(const double* bodies, int32_t n_bodies, const double* x, int64_t n, double* rel, double* local,
+                   double* velocity, double* acceleration, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WSB_H */

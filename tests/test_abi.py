@@ -1,0 +1,47 @@
+"""libwsb.so loads on a machine without a GPU and exports every entry point include/wsb.h declares."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "wsb.h"
+LIB = ROOT / "warpsphboundaries_b200" / "_build" / "libwsb.so"
+
+
+def declared():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(wsb_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    for must in ("wsb_surface_create", "wsb_fixed_topology", "wsb_aggregate", "wsb_aggregate_backward",
+                 "wsb_signed_distance", "wsb_kinematics", "wsb_slot_channels_plain", "wsb_contract"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    if not LIB.exists():
+        from warpsphboundaries_b200 import build
+        build.build()
+    lib = ctypes.CDLL(str(LIB))
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_header():
+    from warpsphboundaries_b200 import _lib
+    assert sorted(_lib.EXPORTS) == declared()
+
+
+def test_errors_without_device_are_raised_not_silent():
+    """a compute call with invalid arguments returns an error code (no CPU fallback answers instead)."""
+    from warpsphboundaries_b200 import _lib
+    rc = _lib.lib.wsb_fixed_topology(None, None, None, None, 4, None, None, None)
+    assert rc == _lib.WSB_ERR_ARG
+    with pytest.raises(ValueError):
+        _lib.check(rc, "wsb_fixed_topology")
+    assert _lib.lib.wsb_version() >= 100

@@ -1,0 +1,81 @@
+"""The oracle (oracle/edge2d.py) against the reference's golden vectors and its own numpy / torch paths."""
+import json
+from fractions import Fraction as F
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import edge2d as O
+
+G = Path(__file__).parent / "golden"
+GOLD = json.loads((G / "edge2d_golden_subset.json").read_text())
+KERNELS = ["cubic", "w2", "w4", "w6"]
+
+
+def _case(c):
+    P = np.array([[float(F(a)), float(F(b))] for a, b in c["polygon"]])
+    x = np.array([float(F(s)) for s in c["x"]])
+    return P, x, float(F(c["h"]))
+
+
+@pytest.mark.parametrize("case", GOLD["cases"], ids=[c["id"] for c in GOLD["cases"]])
+def test_oracle_matches_40_digit_golden_vectors(case):
+    """value, moments |alpha| <= 2, gradient and moment gradients of every golden element, all four kernels:
+    absolute error <= 1e-11 (1 + |ref|) (float64 monomial closed form; the golden values are exact to 1e-35)."""
+    P, x, h = _case(case)
+    tags = set(case["tags"])
+    for k in KERNELS:
+        e = case["kernels"][k]
+        r = O.polygon_moments(P, x, h, k)
+        pairs = [(r[(0, 0)], e["value"])]
+        for al in [(1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]:
+            pairs.append((r[al], e["moments"][f"{al[0]},{al[1]}"]))
+        pairs += [(r["G"][0], e["grad"][0]), (r["G"][1], e["grad"][1])]
+        for al in [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]:
+            g = O.moment_gradient(P, x, h, k, al)
+            ref = e["moment_grad"][f"{al[0]},{al[1]}"]
+            pairs += [(g[0], ref[0]), (g[1], ref[1])]
+        for got, ref in pairs:
+            ref = float(ref)
+            assert abs(got - ref) <= 1e-11 * (1 + abs(ref)), (case["id"], k, got, ref, tags)
+
+
+def test_golden_coverage():
+    tags = {t for c in GOLD["cases"] for t in c["tags"]}
+    assert {"x_on_edge", "x_at_vertex", "z_to_0", "tiny_chord", "small_element", "half_plane", "nonconvex",
+            "clockwise", "h_scaled", "outside_support", "cubic_knot", "generic"} <= tags
+    assert {c["where"] for c in GOLD["cases"]} == {"inside", "outside", "edge", "vertex"}
+
+
+def test_oracle_matches_reference_numpy_path_on_c1():
+    """the twelve channels of the 256-gon scene against the reference's np2d run on the same particles:
+    scaled absolute error <= 5e-12 (G scaled by 1/h, m1 by h, m2 by h^2)."""
+    d = np.load(G / "np2d_c1.npz")
+    P, X, sub, h = d["polygon"], d["particles"], d["subset"], float(d["h"])
+    n = len(P)
+    E = np.stack([np.arange(n), (np.arange(n) + 1) % n], 1)
+    scale = np.array([1, h, h, 1 / h, 1 / h, 1, 1, 1, 1, h * h, h * h, h * h])
+    for k in KERNELS:
+        out = O.local_twelve(P, E, 0, X[sub], np.full(len(sub), h), k, h)
+        err = np.abs(out - d["ch_" + k]) / scale
+        assert err.max() < 5e-12, (k, err.max(0))
+
+
+def test_oracle_gradients_match_reference_torch_autograd():
+    """d m_alpha / dx and d m_alpha / d vertex (|alpha| <= 2, w4) against torch autograd through the reference's
+    torch2d on a star polygon: scaled error <= 1e-11."""
+    g = np.load(G / "torch2d_grad.npz")
+    P, X, h = g["polygon"], g["particles"], float(g["h"])
+    for al in [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]:
+        key = f"{al[0]}{al[1]}"
+        sc = h ** (al[0] + al[1] - 1)
+        for i in range(0, len(X), 3):
+            assert np.abs(O.moment_gradient(P, X[i], h, "w4", al) - g["dx_" + key][i]).max() / sc < 1e-11
+            assert np.abs(O.shape_gradient(P, X[i], h, "w4", al) - g["dv_" + key][i]).max() / sc < 1e-11
+
+
+def test_plane_constants():
+    for k, (m, p2) in {"w4": (1, F(7, 132)), "w2": (1, F(5, 72)), "w6": (1, F(3, 70)), "cubic": (1, F(31, 392))}.items():
+        mass, plane2 = O.kernel_mass_and_plane(k)
+        assert mass == m and plane2 == p2

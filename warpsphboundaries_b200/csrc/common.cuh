@@ -1,0 +1,347 @@
+// Shared device code of libwsb: the surface handle, rounding-exact predicates, the winding-number
+// indicator and the closed-form chord engine of the twelve edge channels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/wsb.h"
+#include "kernel_tables.h"
+
+namespace wsb {
+
+constexpr double kInvPi = 0.318309886183790671537767526745028724;
+constexpr double kTwoPi = 6.283185307179586;
+
+// device-side status codes written into the optional status word (atomicMax)
+enum : int32_t { kStatusOk = 0, kStatusBadEdge = 1, kStatusBadCell = 2 };
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* where);
+
+#define WSB_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t e__ = (call);                            \
+    if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
+  } while (0)
+
+// ----------------------------------------------------------------------------------------------- surface
+struct Surface {
+  int device = 0;
+  int64_t n_verts = 0, n_edges = 0;
+  int background = 0;
+  double support_max = 0;
+  // edge cell grid
+  int32_t nx = 0, ny = 0;
+  double lo_x = 0, lo_y = 0, cell = 0;
+  int32_t K = 1;
+  int64_t n_items = 0;
+  // y bins
+  int32_t nb = 1;
+  double y0 = 0, dy = 1;
+  int64_t n_bitems = 0;
+  double bbox[4] = {0, 0, 0, 0};
+  // device arrays
+  double* verts = nullptr;      // [n_verts*2]
+  int32_t* edges = nullptr;     // [n_edges*2]
+  int32_t* cstart = nullptr;    // [nx*ny+1]
+  int32_t* citems = nullptr;    // [n_items]
+  double4* crec = nullptr;      // [n_items] (ax, ay, bx, by) of the item's edge, cell-list order
+  double* cind = nullptr;       // [nx*ny] indicator of edge-free cells
+  int32_t* cempty = nullptr;    // [nx*ny]
+  int32_t* bstart = nullptr;    // [nb+1]
+  int32_t* bitems = nullptr;    // [n_bitems]
+  double4* erec = nullptr;      // [n_edges] (ax, ay, bx, by) by edge id
+  // host copies (tests, signed distance set-up)
+  std::string err;
+};
+
+// ----------------------------------------------------------------------------------------------- rounding-exact helpers
+// a x b with both products rounded before the subtraction (no FMA contraction): the orientation predicate shared by the
+// indicator and the edge terms, src/warpSPHBoundaries/edge/predicates.py:21-31
+__device__ __forceinline__ double cross2_rn(double ax, double ay, double bx, double by) {
+  return __dsub_rn(__dmul_rn(ax, by), __dmul_rn(ay, bx));
+}
+
+__device__ __forceinline__ double dot2_rn(double ax, double ay, double bx, double by) {
+  return __dadd_rn(__dmul_rn(ax, bx), __dmul_rn(ay, by));
+}
+
+// Pose.toLocal (scene.py:75-79): d = p - c;  (d0 c + d1 s, d1 c - d0 s), every operation rounded on its own
+__device__ __forceinline__ void to_local_rn(double px, double py, double cx, double cy, double c, double s, double& lx,
+                                            double& ly) {
+  const double d0 = __dsub_rn(px, cx), d1 = __dsub_rn(py, cy);
+  lx = __dadd_rn(__dmul_rn(d0, c), __dmul_rn(d1, s));
+  ly = __dsub_rn(__dmul_rn(d1, c), __dmul_rn(d0, s));
+}
+
+// the neighbour predicate |x - seg(a, b)| < h in float64 with the operation order of
+// scene.py:135-139 / fixedadj.py:92-96 and no contraction
+__device__ __forceinline__ bool seg_within(double px, double py, double ax, double ay, double bx, double by, double h) {
+  const double dx = __dsub_rn(bx, ax), dy = __dsub_rn(by, ay);
+  const double num = __dadd_rn(__dmul_rn(__dsub_rn(px, ax), dx), __dmul_rn(__dsub_rn(py, ay), dy));
+  const double den = fmax(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), 1e-300);
+  double t = __ddiv_rn(num, den);
+  t = fmin(fmax(t, 0.0), 1.0);
+  const double ex = __dsub_rn(px, __dadd_rn(ax, __dmul_rn(t, dx)));
+  const double ey = __dsub_rn(py, __dadd_rn(ay, __dmul_rn(t, dy)));
+  return __dsqrt_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey))) < h;
+}
+
+// ----------------------------------------------------------------------------------------------- indicator
+struct SurfView {        // the device pointers and scalars a kernel needs (passed by value)
+  const double* verts;
+  const int32_t* edges;
+  int64_t n_edges;
+  const int32_t* cstart;
+  const double4* crec;
+  const int32_t* citems;
+  const double* cind;
+  const int32_t* cempty;
+  const int32_t* bstart;
+  const int32_t* bitems;
+  const double4* erec;
+  int32_t nx, ny, nb, K;
+  double lo_x, lo_y, cell, y0, dy;
+  double background;
+};
+
+// Winding number + background of a point in the body frame, relative coordinates normalised by h (h = 1: none), with the
+// logic of the fixed-topology kernel (fixedadj.py:98-145): the cell cache for edge-free cells, ray casting along the y bin
+// otherwise, the principal-value angle sum over all edges for points on the boundary; outside the grid the background.
+__device__ __forceinline__ double indicator_at(const SurfView& S, double px, double py, double h, bool in_grid,
+                                               int32_t cid) {
+  if (!in_grid) return S.background;
+  if (S.cempty[cid] != 0) return S.cind[cid];
+  const double iyd = floor(__ddiv_rn(__dsub_rn(py, S.y0), S.dy));
+  if (!(iyd >= 0.0 && iyd <= (double)S.nb)) return S.background;
+  int iy = (int)iyd;
+  if (iy > S.nb - 1) iy = S.nb - 1;
+  double w = 0.0;
+  bool boundary = false;
+  for (int i = S.bstart[iy]; i < S.bstart[iy + 1]; ++i) {
+    const double4 r = S.erec[S.bitems[i]];
+    const double arx = __ddiv_rn(__dsub_rn(r.x, px), h), ary = __ddiv_rn(__dsub_rn(r.y, py), h);
+    const double crx = __ddiv_rn(__dsub_rn(r.z, px), h), cry = __ddiv_rn(__dsub_rn(r.w, py), h);
+    const double cr = cross2_rn(arx, ary, crx, cry);
+    if (r.y <= py && py < r.w && cr > 0.0) w += 1.0;
+    if (r.w <= py && py < r.y && cr < 0.0) w -= 1.0;
+    if (cr == 0.0 && dot2_rn(arx, ary, crx, cry) <= 0.0) boundary = true;
+  }
+  if (boundary) {
+    double ang = 0.0;
+    for (int64_t e = 0; e < S.n_edges; ++e) {
+      const double4 r = S.erec[e];
+      const double arx = __ddiv_rn(__dsub_rn(r.x, px), h), ary = __ddiv_rn(__dsub_rn(r.y, py), h);
+      const double crx = __ddiv_rn(__dsub_rn(r.z, px), h), cry = __ddiv_rn(__dsub_rn(r.w, py), h);
+      const double cr = cross2_rn(arx, ary, crx, cry);
+      if (cr != 0.0) ang += atan2(cr, dot2_rn(arx, ary, crx, cry));
+    }
+    w = ang / kTwoPi;
+  }
+  return w + S.background;
+}
+
+__device__ __forceinline__ bool cell_of(const SurfView& S, double px, double py, int32_t& cid) {
+  const double fx = floor(__ddiv_rn(__dsub_rn(px, S.lo_x), S.cell));
+  const double fy = floor(__ddiv_rn(__dsub_rn(py, S.lo_y), S.cell));
+  if (!(fx >= 0.0 && fx < (double)S.nx && fy >= 0.0 && fy < (double)S.ny)) {
+    cid = -1;
+    return false;
+  }
+  cid = (int32_t)fx * S.ny + (int32_t)fy;
+  return true;
+}
+
+// ----------------------------------------------------------------------------------------------- the chord engine
+struct PairGeo {
+  double t0, t1, n0, n1, z, s0, s1;
+};
+
+// edge frame of a pair from the relative vertices p, q (units of h): warpbc.py:628-643
+__device__ __forceinline__ bool pair_geo(double p0, double p1, double q0, double q1, PairGeo& g) {
+  const double d0 = q0 - p0, d1 = q1 - p1;
+  const double ell = sqrt(d0 * d0 + d1 * d1);
+  if (ell == 0.0) return false;
+  const double ie = 1.0 / ell;
+  g.t0 = d0 * ie;
+  g.t1 = d1 * ie;
+  g.n0 = g.t1;
+  g.n1 = -g.t0;
+  g.z = cross2_rn(p0, p1, q0, q1) / ell;   // the same rounded orientation as the indicator
+  g.s0 = (d0 * p0 + d1 * p1) * ie;
+  g.s1 = (d0 * q0 + d1 * q1) * ie;
+  return true;
+}
+
+// asinh(hi/|z|) - asinh(lo/|z|) as one logarithm of positive factors (no cancellation of a + sqrt(a^2 + 1) for a < 0)
+template <typename T>
+__device__ __forceinline__ T asinh_diff(T lo, T hi, T rlo, T rhi, T zz) {
+  if (lo >= T(0)) return log((hi + rhi) / (lo + rlo));
+  if (hi <= T(0)) return log((rlo - lo) / (rhi - hi));
+  return log((hi + rhi) * (rlo - lo) / zz);
+}
+
+// The MIXED route evaluates the chord angle in float.  The angle enters every channel only through M(R) * angle and
+// MPsi(R) * angle with |M(R)| <= 1/2, so float rounding (<= 2.4e-7 absolute for |angle| <= pi) moves lam by < 4e-8.
+// The logarithm stays in double: its coefficient in the monomial sums reaches 1.7e3 (w6 gradient profile at |z| -> 1),
+// which would amplify float rounding to 1e-4.  Near the foot point (|z| < kMixedGuardZ) the angle is kept in double so
+// its jump across z = 0 stays consistent with the float64 winding indicator.
+constexpr double kMixedGuardZ = 1.0 / 64.0;
+
+template <int PREC>
+__device__ __forceinline__ void special_fns(double lo, double hi, double rlo, double rhi, double z, double zz,
+                                            double& dasinh, double& dang) {
+  dasinh = 0.0;
+  dang = 0.0;
+  if (z == 0.0) return;
+  const double y = z * (hi - lo), x = zz + lo * hi;
+  dasinh = asinh_diff<double>(lo, hi, rlo, rhi, zz);
+  if (PREC == WSB_PREC_MIXED && fabs(z) >= kMixedGuardZ) {
+    dang = (double)atan2f((float)y, (float)x);
+    return;
+  }
+  dang = (y == 0.0 && x == 0.0) ? 0.0 : atan2(y, x);
+}
+
+// One kernel block (truncated monomial profile on r <= R_B) of one pair: the chord, the monomial chord integrals
+// A_n = int_lo^hi r^n ds by the parity recurrence, the six chord sums of the block and their contribution to the twelve
+// channels (before the common 1/pi).  acc layout: 0 lam, 1-2 m1, 3-4 G, 5-8 g1 (g(1,0)_x, g(1,0)_y, g(0,1)_x,
+// g(0,1)_y), 9-11 m20, m11, m02 -- the per-edge values of the reference plan (warpbc.py:98-117, 970-991).
+template <class KT, int B, int PREC>
+__device__ __forceinline__ void block_channels(const PairGeo& g, double acc[12]) {
+  constexpr double R = KT::kR[B];
+  constexpr int NA = KT::kNA[B];
+  const double az = fabs(g.z);
+  if (!(az < R)) return;
+  const double L = sqrt(fmax((R - az) * (R + az), 0.0));
+  const double lo = fmax(g.s0, -L), hi = fmin(g.s1, L);
+  if (!(lo < hi)) return;
+  const double zz = g.z * g.z;
+  const double rlo = sqrt(lo * lo + zz), rhi = sqrt(hi * hi + zz);
+  double dasinh, dang;
+  special_fns<PREC>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
+  double A[NA];
+  A[0] = hi - lo;
+  if (NA > 1) A[1] = 0.5 * (hi * rhi - lo * rlo + zz * dasinh);
+  double ph = rhi, pl = rlo;
+#pragma unroll
+  for (int n = 2; n < NA; ++n) {
+    ph *= rhi;
+    pl *= rlo;
+    A[n] = (hi * ph - lo * pl + (double)n * zz * A[n - 2]) * (1.0 / (double)(n + 1));
+  }
+  BlockSums S;
+  KT::template sums<B>(A, rlo, rhi, S);
+  const double Vl = g.z * S.Lreg - S.Mhat * dang;
+  const double Vp = g.z * S.Preg - S.MPhat * dang;
+  acc[0] += Vl;
+  acc[1] += g.n0 * S.P0;
+  acc[2] += g.n1 * S.P0;
+  acc[3] -= g.n0 * S.W0;
+  acc[4] -= g.n1 * S.W0;
+  const double zW = g.z * S.W0;
+  const double Y0 = g.n0 * zW + g.t0 * S.W1, Y1 = g.n1 * zW + g.t1 * S.W1;
+  acc[5] += Vl - g.n0 * Y0;
+  acc[6] -= g.n1 * Y0;
+  acc[7] -= g.n0 * Y1;
+  acc[8] += Vl - g.n1 * Y1;
+  const double zP = g.z * S.P0;
+  const double Z0 = g.n0 * zP + g.t0 * S.P1, Z1 = g.n1 * zP + g.t1 * S.P1;
+  acc[9] += g.n0 * Z0 - Vp;
+  acc[10] += g.n0 * Z1;
+  acc[11] += g.n1 * Z1 - Vp;
+}
+
+template <class KT, int B, int PREC>
+__device__ __forceinline__ void all_blocks(const PairGeo& g, double acc[12]) {
+  if constexpr (B < KT::kBlocks) {
+    block_channels<KT, B, PREC>(g, acc);
+    all_blocks<KT, B + 1, PREC>(g, acc);
+  }
+}
+
+// the adjoint chord sums of one block: int s^j P ds, j = 0..3 (units of h, pi-free)
+template <class KT, int B>
+__device__ __forceinline__ bool block_adjoint(const PairGeo& g, AdjSums& o) {
+  constexpr double R = KT::kR[B];
+  constexpr int NA = KT::kNAadj[B];
+  const double az = fabs(g.z);
+  if (!(az < R)) return false;
+  const double L = sqrt(fmax((R - az) * (R + az), 0.0));
+  const double lo = fmax(g.s0, -L), hi = fmin(g.s1, L);
+  if (!(lo < hi)) return false;
+  const double zz = g.z * g.z;
+  const double rlo = sqrt(lo * lo + zz), rhi = sqrt(hi * hi + zz);
+  double dasinh, dang;
+  special_fns<WSB_PREC_FP64>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
+  double A[NA];
+  A[0] = hi - lo;
+  if (NA > 1) A[1] = 0.5 * (hi * rhi - lo * rlo + zz * dasinh);
+  double ph = rhi, pl = rlo;
+#pragma unroll
+  for (int n = 2; n < NA; ++n) {
+    ph *= rhi;
+    pl *= rlo;
+    A[n] = (hi * ph - lo * pl + (double)n * zz * A[n - 2]) * (1.0 / (double)(n + 1));
+  }
+  KT::template adj<B>(A, rlo, rhi, zz, o);
+  return true;
+}
+
+// per-row contraction of slot channels (src/warpSPHBoundaries/scene/fused.py:69-154): fixed slot order, + indicator *
+// plane channels, physical scaling, rotation R v, R M R^T; added into the outputs
+__device__ __forceinline__ void write_outputs(const double ch[12], double h, const double* rot, int64_t r, double* lam,
+                                              double* G, double* cov, double* m1, double* m2) {
+  const double R00 = rot[0], R01 = rot[1], R10 = rot[2], R11 = rot[3];
+  if (lam) lam[r] += ch[0];
+  if (m1) {
+    const double vx = h * ch[1], vy = h * ch[2];
+    m1[2 * r] += R00 * vx + R01 * vy;
+    m1[2 * r + 1] += R10 * vx + R11 * vy;
+  }
+  if (G) {
+    const double vx = ch[3] / h, vy = ch[4] / h;
+    G[2 * r] += R00 * vx + R01 * vy;
+    G[2 * r + 1] += R10 * vx + R11 * vy;
+  }
+  if (cov) {
+    const double a = ch[5], b = ch[6], c = ch[7], d = ch[8];
+    cov[4 * r + 0] += R00 * (a * R00 + b * R01) + R01 * (c * R00 + d * R01);
+    cov[4 * r + 1] += R00 * (a * R10 + b * R11) + R01 * (c * R10 + d * R11);
+    cov[4 * r + 2] += R10 * (a * R00 + b * R01) + R11 * (c * R00 + d * R01);
+    cov[4 * r + 3] += R10 * (a * R10 + b * R11) + R11 * (c * R10 + d * R11);
+  }
+  if (m2) {
+    const double hh = h * h;
+    const double xx = ch[9] * hh, xy = ch[10] * hh, yy = ch[11] * hh;
+    m2[4 * r + 0] += R00 * R00 * xx + 2.0 * R00 * R01 * xy + R01 * R01 * yy;
+    const double off = R00 * R10 * xx + (R00 * R11 + R01 * R10) * xy + R01 * R11 * yy;
+    m2[4 * r + 1] += off;
+    m2[4 * r + 2] += off;
+    m2[4 * r + 3] += R10 * R10 * xx + 2.0 * R10 * R11 * xy + R11 * R11 * yy;
+  }
+}
+
+// dispatch a functor templated on the kernel table type
+template <class F>
+inline int dispatch_kernel(int kernel, F&& f) {
+  switch (kernel) {
+    case WSB_KERNEL_CUBIC: return f(Kern_cubic{});
+    case WSB_KERNEL_W2: return f(Kern_w2{});
+    case WSB_KERNEL_W4: return f(Kern_w4{});
+    case WSB_KERNEL_W6: return f(Kern_w6{});
+    case WSB_KERNEL_QUARTIC: return f(Kern_quartic{});
+    case WSB_KERNEL_QUINTIC: return f(Kern_quintic{});
+    case WSB_KERNEL_POLY6: return f(Kern_poly6{});
+    default: return fail(WSB_ERR_UNSUPPORTED, "unknown kernel id " + std::to_string(kernel));
+  }
+}
+
+SurfView view_of(const Surface* s);
+
+}  // namespace wsb

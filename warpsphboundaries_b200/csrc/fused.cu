@@ -1,0 +1,472 @@
+// The fused aggregate route: rows sorted by edge cell (integer counting sort), one pass per row that forms the
+// body-frame position, runs the float64 neighbour predicate over the row's cell and accumulates the closed-form
+// channels of every neighbour pair in registers, then adds the indicator, scales and rotates.  Also the adjoint of the
+// moments, signed distance and rigid-body kinematics.
+#include <cub/device/device_scan.cuh>
+
+#include "common.cuh"
+
+namespace wsb {
+
+constexpr int kThreads = 128;
+
+static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Workspace {
+  int32_t* key;      // [n] bucket of a row: cell id, ncells = outside the grid, ncells + 1 = not a candidate
+  double* lpos;      // [2n] body-frame positions
+  int32_t* counts;   // [nbk + 1]
+  int32_t* offs;     // [nbk + 1] exclusive prefix sums of counts
+  int32_t* cursor;   // [nbk]
+  int32_t* order;    // [n] rows sorted by bucket
+  void* cub_tmp;
+  size_t cub_bytes;
+  size_t total;
+};
+
+static size_t cub_scan_bytes(int64_t items) {
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, (int32_t*)nullptr, (int32_t*)nullptr, (int)items);
+  return bytes;
+}
+
+static Workspace carve(const Surface* s, int64_t n, void* base) {
+  Workspace w{};
+  const int64_t nbk = (int64_t)s->nx * s->ny + 2;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += align256(bytes);
+    return (char*)base + o;
+  };
+  w.key = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.lpos = (double*)take(sizeof(double) * 2 * std::max<int64_t>(n, 1));
+  w.counts = (int32_t*)take(sizeof(int32_t) * (nbk + 1));
+  w.offs = (int32_t*)take(sizeof(int32_t) * (nbk + 1));
+  w.cursor = (int32_t*)take(sizeof(int32_t) * nbk);
+  w.order = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.cub_bytes = cub_scan_bytes(nbk + 1);
+  w.cub_tmp = take(w.cub_bytes);
+  w.total = off;
+  return w;
+}
+
+// body-frame position (bit-for-bit Pose.toLocal), broadphase (fixedadj.py:257-265) and the bucket of every row
+__global__ void k_agg_prep(SurfView S, const double* __restrict__ pos, const double* __restrict__ sup,
+                           const int32_t* __restrict__ allowed, int64_t n, const double* __restrict__ pose,
+                           double4 obb, int unbounded, int32_t* __restrict__ key, double* __restrict__ lpos,
+                           int32_t* __restrict__ counts) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double lx, ly;
+  to_local_rn(pos[2 * i], pos[2 * i + 1], pose[0], pose[1], pose[2], pose[3], lx, ly);
+  lpos[2 * i] = lx;
+  lpos[2 * i + 1] = ly;
+  const int32_t ncells = S.nx * S.ny;
+  bool valid = allowed ? (allowed[i] != 0) : true;
+  if (valid && !unbounded) {
+    const double dx = __dadd_rn(fmax(__dsub_rn(obb.x, lx), 0.0), fmax(__dsub_rn(lx, obb.z), 0.0));
+    const double dy = __dadd_rn(fmax(__dsub_rn(obb.y, ly), 0.0), fmax(__dsub_rn(ly, obb.w), 0.0));
+    valid = __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy))) < sup[i];
+  }
+  int32_t b;
+  if (!valid) {
+    b = ncells + 1;
+  } else {
+    int32_t cid;
+    b = cell_of(S, lx, ly, cid) ? cid : ncells;
+  }
+  key[i] = b;
+  atomicAdd(&counts[b], 1);
+}
+
+__global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const int32_t* __restrict__ offs,
+                              int32_t* __restrict__ cursor, int32_t* __restrict__ order) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t b = key[i];
+  order[offs[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
+}
+
+// one thread per candidate row, rows in bucket order (threads of a warp share a cell and its edge records)
+template <class KT, int PREC>
+__global__ void __launch_bounds__(kThreads) k_agg_main(SurfView S, const double* __restrict__ sup,
+                                                      const int32_t* __restrict__ key,
+                                                      const double* __restrict__ lpos,
+                                                      const int32_t* __restrict__ offs,
+                                                      const int32_t* __restrict__ order, int64_t n,
+                                                      const double* __restrict__ pose, double* lam, double* G,
+                                                      double* cov, double* m1, double* m2) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int32_t ncells = S.nx * S.ny;
+  if (j >= n || j >= offs[ncells + 1]) return;       // rows past the candidates (bucket ncells + 1) take no part
+  const int32_t i = order[j];
+  const int32_t b = key[i];
+  const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
+  double acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+  double ind = S.background;
+  if (b < ncells) {
+    const int e0 = S.cstart[b], e1 = S.cstart[b + 1];
+    const double ih = 1.0 / h;
+    for (int k = e0; k < e1; ++k) {
+      const double4 e = S.crec[k];
+      if (!seg_within(lx, ly, e.x, e.y, e.z, e.w, h)) continue;
+      PairGeo g;
+      if (!pair_geo((e.x - lx) / h, (e.y - ly) / h, (e.z - lx) / h, (e.w - ly) / h, g)) continue;
+      all_blocks<KT, 0, PREC>(g, acc);
+    }
+    (void)ih;
+    ind = indicator_at(S, lx, ly, h, true, b);
+  }
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] *= kInvPi;
+  acc[0] += ind * KT::kMass;
+  acc[5] += ind * KT::kMass;
+  acc[8] += ind * KT::kMass;
+  acc[9] += ind * KT::kPlane2;
+  acc[11] += ind * KT::kPlane2;
+  const double c = pose[2], s = pose[3];
+  const double rot[4] = {c, -s, s, c};
+  write_outputs(acc, h, rot, i, lam, G, cov, m1, m2);
+}
+
+// ------------------------------------------------------------------------------------------------ adjoint
+// d/dx and d/dvertex of lam, m1, m2 by recomputation of the chord integrals int s^j W ds (j <= 3) of every neighbour
+// pair: grad_x m_alpha = -sum_e n_e int y^alpha W ds, d m_alpha / d p_e = n_e int (1 - tau) y^alpha W ds,
+// d m_alpha / d q_e = n_e int tau y^alpha W ds (np2d.py:554-565, 626-652)
+template <class KT, int B>
+__device__ __forceinline__ void adj_blocks(const PairGeo& g, AdjSums& tot) {
+  if constexpr (B < KT::kBlocks) {
+    AdjSums o;
+    if (block_adjoint<KT, B>(g, o)) {
+      tot.W0 += o.W0;
+      tot.W1 += o.W1;
+      tot.W2 += o.W2;
+      tot.W3 += o.W3;
+    }
+    adj_blocks<KT, B + 1>(g, tot);
+  }
+}
+
+template <class KT>
+__global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const double* __restrict__ sup,
+                                                          const int32_t* __restrict__ key,
+                                                          const double* __restrict__ lpos,
+                                                          const int32_t* __restrict__ offs,
+                                                          const int32_t* __restrict__ order, int64_t n,
+                                                          const double* __restrict__ pose,
+                                                          const double* __restrict__ g_lam,
+                                                          const double* __restrict__ g_m1,
+                                                          const double* __restrict__ g_m2, double* d_pos,
+                                                          double* d_verts) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int32_t ncells = S.nx * S.ny;
+  if (j >= n || j >= offs[ncells]) return;            // only rows inside the grid have neighbour pairs
+  const int32_t i = order[j];
+  const int32_t b = key[i];
+  if (b >= ncells) return;
+  const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
+  const double c = pose[2], s = pose[3];
+  // upstream gradients in the body frame and in channel units: m1_world = R m1, m2_world = R m2 R^T
+  const double gl = g_lam ? g_lam[i] : 0.0;
+  double g10 = 0.0, g01 = 0.0, g20 = 0.0, g11 = 0.0, g02 = 0.0;
+  if (g_m1) {
+    const double wx = g_m1[2 * i], wy = g_m1[2 * i + 1];
+    g10 = c * wx + s * wy;
+    g01 = -s * wx + c * wy;
+  }
+  if (g_m2) {
+    const double a = g_m2[4 * i], bb = g_m2[4 * i + 1], cc = g_m2[4 * i + 2], d = g_m2[4 * i + 3];
+    // GL = R^T Gw R with R = [[c, -s], [s, c]]
+    const double t00 = c * a + s * cc, t01 = c * bb + s * d, t10 = -s * a + c * cc, t11 = -s * bb + c * d;
+    const double l00 = t00 * c + t01 * s, l01 = -t00 * s + t01 * c, l10 = t10 * c + t11 * s, l11 = -t10 * s + t11 * c;
+    g20 = l00;
+    g11 = l01 + l10;
+    g02 = l11;
+  }
+  // physical units: d m_alpha = h^(|alpha| - 1) / pi * (unit integral)
+  const double u0 = gl / h, u1x = g10, u1y = g01, u2x = g20 * h, u2m = g11 * h, u2y = g02 * h;
+  double dx = 0.0, dy = 0.0;
+  for (int k = S.cstart[b]; k < S.cstart[b + 1]; ++k) {
+    const double4 e = S.crec[k];
+    if (!seg_within(lx, ly, e.x, e.y, e.z, e.w, h)) continue;
+    PairGeo g;
+    if (!pair_geo((e.x - lx) / h, (e.y - ly) / h, (e.z - lx) / h, (e.w - ly) / h, g)) continue;
+    AdjSums W = {0.0, 0.0, 0.0, 0.0};
+    adj_blocks<KT, 0>(g, W);
+    const double z = g.z, zn0 = z * g.n0, zn1 = z * g.n1;
+    // F = sum_alpha u_alpha y^alpha as a polynomial in s: F0 + F1 s + F2 s^2
+    const double F0 = u0 + u1x * zn0 + u1y * zn1 + u2x * zn0 * zn0 + u2m * zn0 * zn1 + u2y * zn1 * zn1;
+    const double F1 = u1x * g.t0 + u1y * g.t1 + 2.0 * u2x * zn0 * g.t0 + u2m * (zn0 * g.t1 + zn1 * g.t0) +
+                      2.0 * u2y * zn1 * g.t1;
+    const double F2 = u2x * g.t0 * g.t0 + u2m * g.t0 * g.t1 + u2y * g.t1 * g.t1;
+    const double I0 = F0 * W.W0 + F1 * W.W1 + F2 * W.W2;     // int F W ds
+    const double I1 = F0 * W.W1 + F1 * W.W2 + F2 * W.W3;     // int s F W ds
+    dx -= g.n0 * I0;
+    dy -= g.n1 * I0;
+    if (d_verts) {
+      const double ell = g.s1 - g.s0;
+      const double a1 = (I1 - g.s0 * I0) / ell;              // int tau F W ds
+      const double a0 = I0 - a1;                             // int (1 - tau) F W ds
+      const int32_t ei = S.citems[k];
+      const int v0 = S.edges[2 * ei], v1 = S.edges[2 * ei + 1];
+      atomicAdd(&d_verts[2 * v0], kInvPi * g.n0 * a0);
+      atomicAdd(&d_verts[2 * v0 + 1], kInvPi * g.n1 * a0);
+      atomicAdd(&d_verts[2 * v1], kInvPi * g.n0 * a1);
+      atomicAdd(&d_verts[2 * v1 + 1], kInvPi * g.n1 * a1);
+    }
+  }
+  dx *= kInvPi;
+  dy *= kInvPi;
+  // world frame: x_local = R^T (x - c)  =>  dL/dx = R dL/dx_local
+  d_pos[2 * i] += c * dx - s * dy;
+  d_pos[2 * i + 1] += s * dx + c * dy;
+}
+
+// ------------------------------------------------------------------------------------------------ signed distance
+__global__ void k_signed_distance(SurfView S, const double* __restrict__ lpos, int64_t m, double norm_support,
+                                  double* d, double* cp, double* nl, int32_t* edge) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double px = lpos[2 * i], py = lpos[2 * i + 1];
+  double best = INFINITY, bx = 0.0, by = 0.0;
+  int64_t be = -1;
+  for (int64_t e = 0; e < S.n_edges; ++e) {
+    const double4 r = S.erec[e];
+    const double ex = __dsub_rn(r.z, r.x), ey = __dsub_rn(r.w, r.y);
+    double t = __ddiv_rn(__dadd_rn(__dmul_rn(__dsub_rn(px, r.x), ex), __dmul_rn(__dsub_rn(py, r.y), ey)),
+                         __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)));
+    t = fmin(fmax(t, 0.0), 1.0);
+    const double cx = __dadd_rn(r.x, __dmul_rn(t, ex)), cy = __dadd_rn(r.y, __dmul_rn(t, ey));
+    const double ddx = __dsub_rn(px, cx), ddy = __dsub_rn(py, cy);
+    const double dist = __dsqrt_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)));
+    if (dist < best) {
+      best = dist;
+      bx = cx;
+      by = cy;
+      be = e;
+    }
+  }
+  int32_t cid;
+  const bool in_grid = cell_of(S, px, py, cid);
+  const double ind = indicator_at(S, px, py, norm_support > 0.0 ? norm_support : 1.0, in_grid, cid);
+  const bool ins = ind > 0.5;
+  d[i] = ins ? -best : best;
+  cp[2 * i] = bx;
+  cp[2 * i + 1] = by;
+  edge[i] = (int32_t)be;
+  double n0 = 0.0, n1 = 0.0;
+  if (be >= 0) {
+    const double4 r = S.erec[be];
+    const double ex = r.z - r.x, ey = r.w - r.y;
+    const double el = sqrt(ex * ex + ey * ey);
+    n0 = ey / el;
+    n1 = -ex / el;
+  }
+  const double vx = px - bx, vy = py - by;
+  const double dn = sqrt(vx * vx + vy * vy);
+  if (dn > 1e-12 && !ins) {
+    n0 = vx / fmax(dn, 1e-300);
+    n1 = vy / fmax(dn, 1e-300);
+  }
+  nl[2 * i] = n0;
+  nl[2 * i + 1] = n1;
+}
+
+// ------------------------------------------------------------------------------------------------ kinematics
+__global__ void k_kinematics(const double* __restrict__ bodies, int32_t nb, const double* __restrict__ x, int64_t n,
+                             double* rel, double* local, double* vel, double* acc) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nb * n) return;
+  const int64_t b = t / n, i = t % n;
+  const double* B = bodies + 10 * b;
+  const double px = x[2 * i], py = x[2 * i + 1];
+  const double r0 = __dsub_rn(px, B[0]), r1 = __dsub_rn(py, B[1]);
+  if (rel) {
+    rel[2 * t] = r0;
+    rel[2 * t + 1] = r1;
+  }
+  if (local) {
+    double lx, ly;
+    to_local_rn(px, py, B[0], B[1], B[2], B[3], lx, ly);
+    local[2 * t] = lx;
+    local[2 * t + 1] = ly;
+  }
+  const double w = B[6];
+  if (vel) {      // v + w * (-r1, r0)
+    vel[2 * t] = __dadd_rn(B[4], __dmul_rn(w, -r1));
+    vel[2 * t + 1] = __dadd_rn(B[5], __dmul_rn(w, r0));
+  }
+  if (acc) {      // a + alpha * (-r1, r0) - (w * w) * r
+    const double ww = __dmul_rn(w, w), al = B[9];
+    acc[2 * t] = __dsub_rn(__dadd_rn(B[7], __dmul_rn(al, -r1)), __dmul_rn(ww, r0));
+    acc[2 * t + 1] = __dsub_rn(__dadd_rn(B[8], __dmul_rn(al, r0)), __dmul_rn(ww, r1));
+  }
+}
+
+// shared front half of the aggregate and its adjoint: body frame, broadphase, counting sort of the rows by cell
+static int sort_rows(const Surface* s, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
+                     const double* pose, const double* obb, int unbounded, const Workspace& w, cudaStream_t st) {
+  const int64_t nbk = (int64_t)s->nx * s->ny + 2;
+  WSB_CUDA(cudaMemsetAsync(w.counts, 0, sizeof(int32_t) * (nbk + 1), st));
+  WSB_CUDA(cudaMemsetAsync(w.cursor, 0, sizeof(int32_t) * nbk, st));
+  const SurfView v = view_of(s);
+  const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
+  k_agg_prep<<<grid, kThreads, 0, st>>>(v, pos, sup, allowed, n, pose, make_double4(obb[0], obb[1], obb[2], obb[3]),
+                                        unbounded, w.key, w.lpos, w.counts);
+  WSB_CUDA(cudaGetLastError());
+  size_t bytes = w.cub_bytes;
+  WSB_CUDA(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.counts, w.offs, (int)(nbk + 1), st));
+  k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+static int check_common(const Surface* s, int kernel, const double* pos, const double* sup, int64_t n,
+                        const double* pose, const double* obb, const char* who) {
+  if (!s) return fail(WSB_ERR_ARG, std::string(who) + ": NULL surface");
+  if (kernel < 0 || kernel >= kNumKernels) return fail(WSB_ERR_UNSUPPORTED, std::string(who) + ": unknown kernel id");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, std::string(who) + ": row count out of range");
+  if (n > 0 && (!pos || !sup || !pose || !obb)) return fail(WSB_ERR_ARG, std::string(who) + ": NULL array");
+  return WSB_OK;
+}
+
+}  // namespace wsb
+
+using namespace wsb;
+
+extern "C" size_t wsb_aggregate_workspace_size(const wsb_surface* s_, int64_t n) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s || n < 0) return 0;
+  return carve(s, n, nullptr).total;
+}
+
+extern "C" int wsb_aggregate_prepare(const wsb_surface* s_, const double* pos, const double* sup,
+                                     const int32_t* allowed, int64_t n, const double* pose, const double* obb,
+                                     int unbounded, void* workspace, size_t workspace_bytes, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  int rc = check_common(s, 0, pos, sup, n, pose, obb, "wsb_aggregate_prepare");
+  if (rc) return rc;
+  if (n == 0) return WSB_OK;
+  const Workspace w = carve(s, n, workspace);
+  if (!workspace || workspace_bytes < w.total)
+    return fail(WSB_ERR_SIZE, "wsb_aggregate_prepare: workspace of " + std::to_string(workspace_bytes) +
+                                  " bytes, need " + std::to_string(w.total));
+  WSB_CUDA(cudaSetDevice(s->device));
+  return sort_rows(s, pos, sup, allowed, n, pose, obb, unbounded, w, (cudaStream_t)stream);
+}
+
+extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int precision, const double* sup, int64_t n,
+                                      const double* pose, int out_mask, double* lam, double* G, double* cov,
+                                      double* m1, double* m2, const void* workspace, size_t workspace_bytes,
+                                      void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: NULL surface");
+  if (kernel < 0 || kernel >= kNumKernels) return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate: unknown kernel id");
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate: unknown precision mode");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: row count out of range");
+  if (n == 0) return WSB_OK;
+  if (!sup || !pose) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: NULL array");
+  const Workspace w = carve(s, n, const_cast<void*>(workspace));
+  if (!workspace || workspace_bytes < w.total) return fail(WSB_ERR_SIZE, "wsb_aggregate_evaluate: workspace too small");
+  WSB_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  double* L = (out_mask & WSB_OUT_LAM) ? lam : nullptr;
+  double* Gp = (out_mask & WSB_OUT_G) ? G : nullptr;
+  double* C = (out_mask & WSB_OUT_COV) ? cov : nullptr;
+  double* M1 = (out_mask & WSB_OUT_M1) ? m1 : nullptr;
+  double* M2 = (out_mask & WSB_OUT_M2) ? m2 : nullptr;
+  const SurfView v = view_of(s);
+  const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
+  int rc = dispatch_kernel(kernel, [&](auto kt) {
+    using KT = decltype(kt);
+    if (precision == WSB_PREC_MIXED)
+      k_agg_main<KT, WSB_PREC_MIXED><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, pose, L, Gp,
+                                                                C, M1, M2);
+    else
+      k_agg_main<KT, WSB_PREC_FP64><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, pose, L, Gp, C,
+                                                               M1, M2);
+    return 0;
+  });
+  if (rc) return rc;
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+extern "C" int wsb_aggregate(const wsb_surface* s_, int kernel, int precision, const double* pos, const double* sup,
+                             const int32_t* allowed, int64_t n, const double* pose, const double* obb, int unbounded,
+                             int out_mask, double* lam, double* G, double* cov, double* m1, double* m2,
+                             void* workspace, size_t workspace_bytes, int32_t* status, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  int rc = check_common(s, kernel, pos, sup, n, pose, obb, "wsb_aggregate");
+  if (rc) return rc;
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate: unknown precision mode");
+  if (n == 0) return WSB_OK;
+  if (status) {
+    WSB_CUDA(cudaSetDevice(s->device));
+    WSB_CUDA(cudaMemsetAsync(status, 0, sizeof(int32_t), (cudaStream_t)stream));
+  }
+  rc = wsb_aggregate_prepare(s_, pos, sup, allowed, n, pose, obb, unbounded, workspace, workspace_bytes, stream);
+  if (rc) return rc;
+  return wsb_aggregate_evaluate(s_, kernel, precision, sup, n, pose, out_mask, lam, G, cov, m1, m2, workspace,
+                                workspace_bytes, stream);
+}
+
+extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const double* pos, const double* sup,
+                                      const int32_t* allowed, int64_t n, const double* pose, const double* obb,
+                                      int unbounded, const double* g_lam, const double* g_m1, const double* g_m2,
+                                      double* d_pos, double* d_verts, void* workspace, size_t workspace_bytes,
+                                      void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  int rc = check_common(s, kernel, pos, sup, n, pose, obb, "wsb_aggregate_backward");
+  if (rc) return rc;
+  if (n == 0) return WSB_OK;
+  if (!d_pos) return fail(WSB_ERR_ARG, "wsb_aggregate_backward: d_pos is NULL");
+  const Workspace w = carve(s, n, workspace);
+  if (!workspace || workspace_bytes < w.total) return fail(WSB_ERR_SIZE, "wsb_aggregate_backward: workspace too small");
+  WSB_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = sort_rows(s, pos, sup, allowed, n, pose, obb, unbounded, w, st);
+  if (rc) return rc;
+  const SurfView v = view_of(s);
+  const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
+  rc = dispatch_kernel(kernel, [&](auto kt) {
+    using KT = decltype(kt);
+    k_agg_backward<KT><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, pose, g_lam, g_m1, g_m2,
+                                                  d_pos, d_verts);
+    return 0;
+  });
+  if (rc) return rc;
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+extern "C" int wsb_signed_distance(const wsb_surface* s_, const double* lpos, int64_t m, double norm_support,
+                                   double* d, double* cp, double* n_loc, int32_t* edge, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s) return fail(WSB_ERR_ARG, "wsb_signed_distance: NULL surface");
+  if (m < 0) return fail(WSB_ERR_ARG, "wsb_signed_distance: negative point count");
+  if (m == 0) return WSB_OK;
+  if (!lpos || !d || !cp || !n_loc || !edge) return fail(WSB_ERR_ARG, "wsb_signed_distance: NULL array");
+  WSB_CUDA(cudaSetDevice(s->device));
+  k_signed_distance<<<(unsigned)((m + kThreads - 1) / kThreads), kThreads, 0, (cudaStream_t)stream>>>(
+      view_of(s), lpos, m, norm_support, d, cp, n_loc, edge);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+extern "C" int wsb_kinematics(const double* bodies, int32_t n_bodies, const double* x, int64_t n, double* rel,
+                              double* local, double* velocity, double* acceleration, void* stream) {
+  if (n_bodies < 0 || n < 0) return fail(WSB_ERR_ARG, "wsb_kinematics: negative size");
+  if ((int64_t)n_bodies * n == 0) return WSB_OK;
+  if (!bodies || !x) return fail(WSB_ERR_ARG, "wsb_kinematics: NULL array");
+  const int64_t total = (int64_t)n_bodies * n;
+  k_kinematics<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(bodies, n_bodies, x, n, rel, local,
+                                                                                  velocity, acceleration);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}

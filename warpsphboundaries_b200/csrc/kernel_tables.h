@@ -33,9 +33,9 @@ struct Kern_cubic {
 template <> __host__ __device__ __forceinline__ void Kern_cubic::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1: P = ['80/7', '-240/7', '240/7', '-80/7']
   o.W0 = 11.428571428571429*A[0] + -34.285714285714285*A[1] + 34.285714285714285*A[2] + -11.428571428571429*A[3];
-  o.W1 = (fma(fma(fma(fma(fma(-2.2857142857142856, rhi, 8.571428571428571), rhi, -11.428571428571429), rhi, 5.714285714285714), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(-2.2857142857142856, rlo, 8.571428571428571), rlo, -11.428571428571429), rlo, 5.714285714285714), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(-2.2857142857142856, rhi, 8.571428571428571), rhi, -11.428571428571429), rhi, 5.714285714285714))*rhi)*rhi) - (((fma(fma(fma(-2.2857142857142856, rlo, 8.571428571428571), rlo, -11.428571428571429), rlo, 5.714285714285714))*rlo)*rlo);
   o.P0 = -0.5714285714285714*A[0] + 5.714285714285714*A[2] + -11.428571428571429*A[3] + 8.571428571428571*A[4] + -2.2857142857142856*A[5];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(-0.32653061224489793, rhi, 1.4285714285714286), rhi, -2.2857142857142856), rhi, 1.4285714285714286), rhi, 0.0), rhi, -0.2857142857142857), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-0.32653061224489793, rlo, 1.4285714285714286), rlo, -2.2857142857142856), rlo, 1.4285714285714286), rlo, 0.0), rlo, -0.2857142857142857), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(-0.32653061224489793, rhi, 1.4285714285714286), rhi, -2.2857142857142856), rhi, 1.4285714285714286), rhi, 0.0), rhi, -0.2857142857142857))*rhi)*rhi) - (((fma(fma(fma(fma(fma(-0.32653061224489793, rlo, 1.4285714285714286), rlo, -2.2857142857142856), rlo, 1.4285714285714286), rlo, 0.0), rlo, -0.2857142857142857))*rlo)*rlo);
   o.Lreg = 5.714285714285714*A[0] + -11.428571428571429*A[1] + 8.571428571428571*A[2] + -2.2857142857142856*A[3];
   o.Preg = -0.2857142857142857*A[0] + 1.4285714285714286*A[2] + -2.2857142857142856*A[3] + 1.4285714285714286*A[4] + -0.32653061224489793*A[5];
   o.Mhat = 0.5714285714285714;
@@ -44,16 +44,16 @@ template <> __host__ __device__ __forceinline__ void Kern_cubic::sums<0>(const d
 template <> __host__ __device__ __forceinline__ void Kern_cubic::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 11.428571428571429*A[0] + -34.285714285714285*A[1] + 34.285714285714285*A[2] + -11.428571428571429*A[3];
   const double a2 = 11.428571428571429*A[2] + -34.285714285714285*A[3] + 34.285714285714285*A[4] + -11.428571428571429*A[5];
-  const double m1 = (fma(fma(fma(fma(fma(-2.2857142857142856, rhi, 8.571428571428571), rhi, -11.428571428571429), rhi, 5.714285714285714), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(-2.2857142857142856, rlo, 8.571428571428571), rlo, -11.428571428571429), rlo, 5.714285714285714), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(-1.6326530612244898, rhi, 5.714285714285714), rhi, -6.857142857142857), rhi, 2.857142857142857), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-1.6326530612244898, rlo, 5.714285714285714), rlo, -6.857142857142857), rlo, 2.857142857142857), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(-2.2857142857142856, rhi, 8.571428571428571), rhi, -11.428571428571429), rhi, 5.714285714285714))*rhi)*rhi) - (((fma(fma(fma(-2.2857142857142856, rlo, 8.571428571428571), rlo, -11.428571428571429), rlo, 5.714285714285714))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(-1.6326530612244898, rhi, 5.714285714285714), rhi, -6.857142857142857), rhi, 2.857142857142857))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(-1.6326530612244898, rlo, 5.714285714285714), rlo, -6.857142857142857), rlo, 2.857142857142857))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 template <> __host__ __device__ __forceinline__ void Kern_cubic::sums<1>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1/2: P = ['-40/7', '240/7', '-480/7', '320/7']
   o.W0 = -5.714285714285714*A[0] + 34.285714285714285*A[1] + -68.57142857142857*A[2] + 45.714285714285715*A[3];
-  o.W1 = (fma(fma(fma(fma(fma(9.142857142857142, rhi, -17.142857142857142), rhi, 11.428571428571429), rhi, -2.857142857142857), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(9.142857142857142, rlo, -17.142857142857142), rlo, 11.428571428571429), rlo, -2.857142857142857), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(9.142857142857142, rhi, -17.142857142857142), rhi, 11.428571428571429), rhi, -2.857142857142857))*rhi)*rhi) - (((fma(fma(fma(9.142857142857142, rlo, -17.142857142857142), rlo, 11.428571428571429), rlo, -2.857142857142857))*rlo)*rlo);
   o.P0 = 0.07142857142857142*A[0] + -2.857142857142857*A[2] + 11.428571428571429*A[3] + -17.142857142857142*A[4] + 9.142857142857142*A[5];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(1.3061224489795917, rhi, -2.857142857142857), rhi, 2.2857142857142856), rhi, -0.7142857142857143), rhi, 0.0), rhi, 0.03571428571428571), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(1.3061224489795917, rlo, -2.857142857142857), rlo, 2.2857142857142856), rlo, -0.7142857142857143), rlo, 0.0), rlo, 0.03571428571428571), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(1.3061224489795917, rhi, -2.857142857142857), rhi, 2.2857142857142856), rhi, -0.7142857142857143), rhi, 0.0), rhi, 0.03571428571428571))*rhi)*rhi) - (((fma(fma(fma(fma(fma(1.3061224489795917, rlo, -2.857142857142857), rlo, 2.2857142857142856), rlo, -0.7142857142857143), rlo, 0.0), rlo, 0.03571428571428571))*rlo)*rlo);
   o.Lreg = -2.857142857142857*A[0] + 11.428571428571429*A[1] + -17.142857142857142*A[2] + 9.142857142857142*A[3];
   o.Preg = 0.03571428571428571*A[0] + -0.7142857142857143*A[2] + 2.2857142857142856*A[3] + -2.857142857142857*A[4] + 1.3061224489795917*A[5];
   o.Mhat = -0.07142857142857142;
@@ -62,8 +62,8 @@ template <> __host__ __device__ __forceinline__ void Kern_cubic::sums<1>(const d
 template <> __host__ __device__ __forceinline__ void Kern_cubic::adj<1>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = -5.714285714285714*A[0] + 34.285714285714285*A[1] + -68.57142857142857*A[2] + 45.714285714285715*A[3];
   const double a2 = -5.714285714285714*A[2] + 34.285714285714285*A[3] + -68.57142857142857*A[4] + 45.714285714285715*A[5];
-  const double m1 = (fma(fma(fma(fma(fma(9.142857142857142, rhi, -17.142857142857142), rhi, 11.428571428571429), rhi, -2.857142857142857), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(9.142857142857142, rlo, -17.142857142857142), rlo, 11.428571428571429), rlo, -2.857142857142857), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(6.530612244897959, rhi, -11.428571428571429), rhi, 6.857142857142857), rhi, -1.4285714285714286), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(6.530612244897959, rlo, -11.428571428571429), rlo, 6.857142857142857), rlo, -1.4285714285714286), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(9.142857142857142, rhi, -17.142857142857142), rhi, 11.428571428571429), rhi, -2.857142857142857))*rhi)*rhi) - (((fma(fma(fma(9.142857142857142, rlo, -17.142857142857142), rlo, 11.428571428571429), rlo, -2.857142857142857))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(6.530612244897959, rhi, -11.428571428571429), rhi, 6.857142857142857), rhi, -1.4285714285714286))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(6.530612244897959, rlo, -11.428571428571429), rlo, 6.857142857142857), rlo, -1.4285714285714286))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
@@ -82,9 +82,9 @@ struct Kern_w2 {
 template <> __host__ __device__ __forceinline__ void Kern_w2::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1: P = ['7', '0', '-70', '140', '-105', '28']
   o.W0 = 7.0*A[0] + -70.0*A[2] + 140.0*A[3] + -105.0*A[4] + 28.0*A[5];
-  o.W1 = (fma(fma(fma(fma(fma(fma(fma(4.0, rhi, -17.5), rhi, 28.0), rhi, -17.5), rhi, 0.0), rhi, 3.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(4.0, rlo, -17.5), rlo, 28.0), rlo, -17.5), rlo, 0.0), rlo, 3.5), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(fma(4.0, rhi, -17.5), rhi, 28.0), rhi, -17.5), rhi, 0.0), rhi, 3.5))*rhi)*rhi) - (((fma(fma(fma(fma(fma(4.0, rlo, -17.5), rlo, 28.0), rlo, -17.5), rlo, 0.0), rlo, 3.5))*rlo)*rlo);
   o.P0 = -0.5*A[0] + 3.5*A[2] + -17.5*A[4] + 28.0*A[5] + -17.5*A[6] + 4.0*A[7];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(0.4444444444444444, rhi, -2.1875), rhi, 4.0), rhi, -2.9166666666666665), rhi, 0.0), rhi, 0.875), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(0.4444444444444444, rlo, -2.1875), rlo, 4.0), rlo, -2.9166666666666665), rlo, 0.0), rlo, 0.875), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(0.4444444444444444, rhi, -2.1875), rhi, 4.0), rhi, -2.9166666666666665), rhi, 0.0), rhi, 0.875), rhi, 0.0), rhi, -0.25))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(0.4444444444444444, rlo, -2.1875), rlo, 4.0), rlo, -2.9166666666666665), rlo, 0.0), rlo, 0.875), rlo, 0.0), rlo, -0.25))*rlo)*rlo);
   o.Lreg = 3.5*A[0] + -17.5*A[2] + 28.0*A[3] + -17.5*A[4] + 4.0*A[5];
   o.Preg = -0.25*A[0] + 0.875*A[2] + -2.9166666666666665*A[4] + 4.0*A[5] + -2.1875*A[6] + 0.4444444444444444*A[7];
   o.Mhat = 0.5;
@@ -93,8 +93,8 @@ template <> __host__ __device__ __forceinline__ void Kern_w2::sums<0>(const doub
 template <> __host__ __device__ __forceinline__ void Kern_w2::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 7.0*A[0] + -70.0*A[2] + 140.0*A[3] + -105.0*A[4] + 28.0*A[5];
   const double a2 = 7.0*A[2] + -70.0*A[4] + 140.0*A[5] + -105.0*A[6] + 28.0*A[7];
-  const double m1 = (fma(fma(fma(fma(fma(fma(fma(4.0, rhi, -17.5), rhi, 28.0), rhi, -17.5), rhi, 0.0), rhi, 3.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(4.0, rlo, -17.5), rlo, 28.0), rlo, -17.5), rlo, 0.0), rlo, 3.5), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.111111111111111, rhi, -13.125), rhi, 20.0), rhi, -11.666666666666666), rhi, 0.0), rhi, 1.75), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.111111111111111, rlo, -13.125), rlo, 20.0), rlo, -11.666666666666666), rlo, 0.0), rlo, 1.75), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(fma(4.0, rhi, -17.5), rhi, 28.0), rhi, -17.5), rhi, 0.0), rhi, 3.5))*rhi)*rhi) - (((fma(fma(fma(fma(fma(4.0, rlo, -17.5), rlo, 28.0), rlo, -17.5), rlo, 0.0), rlo, 3.5))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(3.111111111111111, rhi, -13.125), rhi, 20.0), rhi, -11.666666666666666), rhi, 0.0), rhi, 1.75))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(3.111111111111111, rlo, -13.125), rlo, 20.0), rlo, -11.666666666666666), rlo, 0.0), rlo, 1.75))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
@@ -113,9 +113,9 @@ struct Kern_w4 {
 template <> __host__ __device__ __forceinline__ void Kern_w4::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1: P = ['9', '0', '-84', '0', '630', '-1344', '1260', '-576', '105']
   o.W0 = 9.0*A[0] + -84.0*A[2] + 630.0*A[4] + -1344.0*A[5] + 1260.0*A[6] + -576.0*A[7] + 105.0*A[8];
-  o.W1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rhi, -64.0), rhi, 157.5), rhi, -192.0), rhi, 105.0), rhi, 0.0), rhi, -21.0), rhi, 0.0), rhi, 4.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rlo, -64.0), rlo, 157.5), rlo, -192.0), rlo, 105.0), rlo, 0.0), rlo, -21.0), rlo, 0.0), rlo, 4.5), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(fma(fma(fma(fma(10.5, rhi, -64.0), rhi, 157.5), rhi, -192.0), rhi, 105.0), rhi, 0.0), rhi, -21.0), rhi, 0.0), rhi, 4.5))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(10.5, rlo, -64.0), rlo, 157.5), rlo, -192.0), rlo, 105.0), rlo, 0.0), rlo, -21.0), rlo, 0.0), rlo, 4.5))*rlo)*rlo);
   o.P0 = -0.5*A[0] + 4.5*A[2] + -21.0*A[4] + 105.0*A[6] + -192.0*A[7] + 157.5*A[8] + -64.0*A[9] + 10.5*A[10];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.875, rhi, -5.818181818181818), rhi, 15.75), rhi, -21.333333333333332), rhi, 13.125), rhi, 0.0), rhi, -3.5), rhi, 0.0), rhi, 1.125), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.875, rlo, -5.818181818181818), rlo, 15.75), rlo, -21.333333333333332), rlo, 13.125), rlo, 0.0), rlo, -3.5), rlo, 0.0), rlo, 1.125), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.875, rhi, -5.818181818181818), rhi, 15.75), rhi, -21.333333333333332), rhi, 13.125), rhi, 0.0), rhi, -3.5), rhi, 0.0), rhi, 1.125), rhi, 0.0), rhi, -0.25))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.875, rlo, -5.818181818181818), rlo, 15.75), rlo, -21.333333333333332), rlo, 13.125), rlo, 0.0), rlo, -3.5), rlo, 0.0), rlo, 1.125), rlo, 0.0), rlo, -0.25))*rlo)*rlo);
   o.Lreg = 4.5*A[0] + -21.0*A[2] + 105.0*A[4] + -192.0*A[5] + 157.5*A[6] + -64.0*A[7] + 10.5*A[8];
   o.Preg = -0.25*A[0] + 1.125*A[2] + -3.5*A[4] + 13.125*A[6] + -21.333333333333332*A[7] + 15.75*A[8] + -5.818181818181818*A[9] + 0.875*A[10];
   o.Mhat = 0.5;
@@ -124,8 +124,8 @@ template <> __host__ __device__ __forceinline__ void Kern_w4::sums<0>(const doub
 template <> __host__ __device__ __forceinline__ void Kern_w4::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 9.0*A[0] + -84.0*A[2] + 630.0*A[4] + -1344.0*A[5] + 1260.0*A[6] + -576.0*A[7] + 105.0*A[8];
   const double a2 = 9.0*A[2] + -84.0*A[4] + 630.0*A[6] + -1344.0*A[7] + 1260.0*A[8] + -576.0*A[9] + 105.0*A[10];
-  const double m1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rhi, -64.0), rhi, 157.5), rhi, -192.0), rhi, 105.0), rhi, 0.0), rhi, -21.0), rhi, 0.0), rhi, 4.5), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(10.5, rlo, -64.0), rlo, 157.5), rlo, -192.0), rlo, 105.0), rlo, 0.0), rlo, -21.0), rlo, 0.0), rlo, 4.5), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(8.75, rhi, -52.36363636363637), rhi, 126.0), rhi, -149.33333333333334), rhi, 78.75), rhi, 0.0), rhi, -14.0), rhi, 0.0), rhi, 2.25), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(8.75, rlo, -52.36363636363637), rlo, 126.0), rlo, -149.33333333333334), rlo, 78.75), rlo, 0.0), rlo, -14.0), rlo, 0.0), rlo, 2.25), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(fma(fma(fma(fma(10.5, rhi, -64.0), rhi, 157.5), rhi, -192.0), rhi, 105.0), rhi, 0.0), rhi, -21.0), rhi, 0.0), rhi, 4.5))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(10.5, rlo, -64.0), rlo, 157.5), rlo, -192.0), rlo, 105.0), rlo, 0.0), rlo, -21.0), rlo, 0.0), rlo, 4.5))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(fma(fma(fma(8.75, rhi, -52.36363636363637), rhi, 126.0), rhi, -149.33333333333334), rhi, 78.75), rhi, 0.0), rhi, -14.0), rhi, 0.0), rhi, 2.25))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(fma(fma(fma(8.75, rlo, -52.36363636363637), rlo, 126.0), rlo, -149.33333333333334), rlo, 78.75), rlo, 0.0), rlo, -14.0), rlo, 0.0), rlo, 2.25))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
@@ -144,9 +144,9 @@ struct Kern_w6 {
 template <> __host__ __device__ __forceinline__ void Kern_w6::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1: P = ['78/7', '0', '-858/7', '0', '5148/7', '0', '-5148', '82368/7', '-12870', '54912/7', '-2574', '2496/7']
   o.W0 = 11.142857142857142*A[0] + -122.57142857142857*A[2] + 735.4285714285714*A[4] + -5148.0*A[6] + 11766.857142857143*A[7] + -12870.0*A[8] + 7844.571428571428*A[9] + -2574.0*A[10] + 356.57142857142856*A[11];
-  o.W1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rhi, -214.5), rhi, 713.1428571428571), rhi, -1287.0), rhi, 1307.4285714285713), rhi, -643.5), rhi, 0.0), rhi, 122.57142857142857), rhi, 0.0), rhi, -30.642857142857142), rhi, 0.0), rhi, 5.571428571428571), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rlo, -214.5), rlo, 713.1428571428571), rlo, -1287.0), rlo, 1307.4285714285713), rlo, -643.5), rlo, 0.0), rlo, 122.57142857142857), rlo, 0.0), rlo, -30.642857142857142), rlo, 0.0), rlo, 5.571428571428571), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rhi, -214.5), rhi, 713.1428571428571), rhi, -1287.0), rhi, 1307.4285714285713), rhi, -643.5), rhi, 0.0), rhi, 122.57142857142857), rhi, 0.0), rhi, -30.642857142857142), rhi, 0.0), rhi, 5.571428571428571))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rlo, -214.5), rlo, 713.1428571428571), rlo, -1287.0), rlo, 1307.4285714285713), rlo, -643.5), rlo, 0.0), rlo, 122.57142857142857), rlo, 0.0), rlo, -30.642857142857142), rlo, 0.0), rlo, 5.571428571428571))*rlo)*rlo);
   o.P0 = -0.5*A[0] + 5.571428571428571*A[2] + -30.642857142857142*A[4] + 122.57142857142857*A[6] + -643.5*A[8] + 1307.4285714285713*A[9] + -1287.0*A[10] + 713.1428571428571*A[11] + -214.5*A[12] + 27.428571428571427*A[13];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.8285714285714285, rhi, -15.321428571428571), rhi, 54.857142857142854), rhi, -107.25), rhi, 118.85714285714286), rhi, -64.35), rhi, 0.0), rhi, 15.321428571428571), rhi, 0.0), rhi, -5.107142857142857), rhi, 0.0), rhi, 1.3928571428571428), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.8285714285714285, rlo, -15.321428571428571), rlo, 54.857142857142854), rlo, -107.25), rlo, 118.85714285714286), rlo, -64.35), rlo, 0.0), rlo, 15.321428571428571), rlo, 0.0), rlo, -5.107142857142857), rlo, 0.0), rlo, 1.3928571428571428), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.8285714285714285, rhi, -15.321428571428571), rhi, 54.857142857142854), rhi, -107.25), rhi, 118.85714285714286), rhi, -64.35), rhi, 0.0), rhi, 15.321428571428571), rhi, 0.0), rhi, -5.107142857142857), rhi, 0.0), rhi, 1.3928571428571428), rhi, 0.0), rhi, -0.25))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.8285714285714285, rlo, -15.321428571428571), rlo, 54.857142857142854), rlo, -107.25), rlo, 118.85714285714286), rlo, -64.35), rlo, 0.0), rlo, 15.321428571428571), rlo, 0.0), rlo, -5.107142857142857), rlo, 0.0), rlo, 1.3928571428571428), rlo, 0.0), rlo, -0.25))*rlo)*rlo);
   o.Lreg = 5.571428571428571*A[0] + -30.642857142857142*A[2] + 122.57142857142857*A[4] + -643.5*A[6] + 1307.4285714285713*A[7] + -1287.0*A[8] + 713.1428571428571*A[9] + -214.5*A[10] + 27.428571428571427*A[11];
   o.Preg = -0.25*A[0] + 1.3928571428571428*A[2] + -5.107142857142857*A[4] + 15.321428571428571*A[6] + -64.35*A[8] + 118.85714285714286*A[9] + -107.25*A[10] + 54.857142857142854*A[11] + -15.321428571428571*A[12] + 1.8285714285714285*A[13];
   o.Mhat = 0.5;
@@ -155,8 +155,8 @@ template <> __host__ __device__ __forceinline__ void Kern_w6::sums<0>(const doub
 template <> __host__ __device__ __forceinline__ void Kern_w6::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 11.142857142857142*A[0] + -122.57142857142857*A[2] + 735.4285714285714*A[4] + -5148.0*A[6] + 11766.857142857143*A[7] + -12870.0*A[8] + 7844.571428571428*A[9] + -2574.0*A[10] + 356.57142857142856*A[11];
   const double a2 = 11.142857142857142*A[2] + -122.57142857142857*A[4] + 735.4285714285714*A[6] + -5148.0*A[8] + 11766.857142857143*A[9] + -12870.0*A[10] + 7844.571428571428*A[11] + -2574.0*A[12] + 356.57142857142856*A[13];
-  const double m1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rhi, -214.5), rhi, 713.1428571428571), rhi, -1287.0), rhi, 1307.4285714285713), rhi, -643.5), rhi, 0.0), rhi, 122.57142857142857), rhi, 0.0), rhi, -30.642857142857142), rhi, 0.0), rhi, 5.571428571428571), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rlo, -214.5), rlo, 713.1428571428571), rlo, -1287.0), rlo, 1307.4285714285713), rlo, -643.5), rlo, 0.0), rlo, 122.57142857142857), rlo, 0.0), rlo, -30.642857142857142), rlo, 0.0), rlo, 5.571428571428571), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(23.771428571428572, rhi, -183.85714285714286), rhi, 603.4285714285714), rhi, -1072.5), rhi, 1069.7142857142858), rhi, -514.8), rhi, 0.0), rhi, 91.92857142857143), rhi, 0.0), rhi, -20.428571428571427), rhi, 0.0), rhi, 2.7857142857142856), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(23.771428571428572, rlo, -183.85714285714286), rlo, 603.4285714285714), rlo, -1072.5), rlo, 1069.7142857142858), rlo, -514.8), rlo, 0.0), rlo, 91.92857142857143), rlo, 0.0), rlo, -20.428571428571427), rlo, 0.0), rlo, 2.7857142857142856), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rhi, -214.5), rhi, 713.1428571428571), rhi, -1287.0), rhi, 1307.4285714285713), rhi, -643.5), rhi, 0.0), rhi, 122.57142857142857), rhi, 0.0), rhi, -30.642857142857142), rhi, 0.0), rhi, 5.571428571428571))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, rlo, -214.5), rlo, 713.1428571428571), rlo, -1287.0), rlo, 1307.4285714285713), rlo, -643.5), rlo, 0.0), rlo, 122.57142857142857), rlo, 0.0), rlo, -30.642857142857142), rlo, 0.0), rlo, 5.571428571428571))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(23.771428571428572, rhi, -183.85714285714286), rhi, 603.4285714285714), rhi, -1072.5), rhi, 1069.7142857142858), rhi, -514.8), rhi, 0.0), rhi, 91.92857142857143), rhi, 0.0), rhi, -20.428571428571427), rhi, 0.0), rhi, 2.7857142857142856))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(23.771428571428572, rlo, -183.85714285714286), rlo, 603.4285714285714), rlo, -1072.5), rlo, 1069.7142857142858), rlo, -514.8), rlo, 0.0), rlo, 91.92857142857143), rlo, 0.0), rlo, -20.428571428571427), rlo, 0.0), rlo, 2.7857142857142856))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
@@ -175,9 +175,9 @@ struct Kern_quartic {
 template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1: P = ['46875/2398', '-93750/1199', '140625/1199', '-93750/1199', '46875/2398']
   o.W0 = 19.547539616346956*A[0] + -78.19015846538782*A[1] + 117.28523769808173*A[2] + -78.19015846538782*A[3] + 19.547539616346956*A[4];
-  o.W1 = (fma(fma(fma(fma(fma(fma(3.2579232693911595, rhi, -15.638031693077565), rhi, 29.321309424520432), rhi, -26.063386155129276), rhi, 9.773769808173478), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(3.2579232693911595, rlo, -15.638031693077565), rlo, 29.321309424520432), rlo, -26.063386155129276), rlo, 9.773769808173478), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(3.2579232693911595, rhi, -15.638031693077565), rhi, 29.321309424520432), rhi, -26.063386155129276), rhi, 9.773769808173478))*rhi)*rhi) - (((fma(fma(fma(fma(3.2579232693911595, rlo, -15.638031693077565), rlo, 29.321309424520432), rlo, -26.063386155129276), rlo, 9.773769808173478))*rlo)*rlo);
   o.P0 = -0.6515846538782318*A[0] + 9.773769808173478*A[2] + -26.063386155129276*A[3] + 29.321309424520432*A[4] + -15.638031693077565*A[5] + 3.2579232693911595*A[6];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(0.40724040867389494, rhi, -2.2340045275825093), rhi, 4.886884904086739), rhi, -5.212677231025855), rhi, 2.4434424520433695), rhi, 0.0), rhi, -0.3257923269391159), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(0.40724040867389494, rlo, -2.2340045275825093), rlo, 4.886884904086739), rlo, -5.212677231025855), rlo, 2.4434424520433695), rlo, 0.0), rlo, -0.3257923269391159), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(0.40724040867389494, rhi, -2.2340045275825093), rhi, 4.886884904086739), rhi, -5.212677231025855), rhi, 2.4434424520433695), rhi, 0.0), rhi, -0.3257923269391159))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(0.40724040867389494, rlo, -2.2340045275825093), rlo, 4.886884904086739), rlo, -5.212677231025855), rlo, 2.4434424520433695), rlo, 0.0), rlo, -0.3257923269391159))*rlo)*rlo);
   o.Lreg = 9.773769808173478*A[0] + -26.063386155129276*A[1] + 29.321309424520432*A[2] + -15.638031693077565*A[3] + 3.2579232693911595*A[4];
   o.Preg = -0.3257923269391159*A[0] + 2.4434424520433695*A[2] + -5.212677231025855*A[3] + 4.886884904086739*A[4] + -2.2340045275825093*A[5] + 0.40724040867389494*A[6];
   o.Mhat = 0.6515846538782318;
@@ -186,16 +186,16 @@ template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<0>(const
 template <> __host__ __device__ __forceinline__ void Kern_quartic::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 19.547539616346956*A[0] + -78.19015846538782*A[1] + 117.28523769808173*A[2] + -78.19015846538782*A[3] + 19.547539616346956*A[4];
   const double a2 = 19.547539616346956*A[2] + -78.19015846538782*A[3] + 117.28523769808173*A[4] + -78.19015846538782*A[5] + 19.547539616346956*A[6];
-  const double m1 = (fma(fma(fma(fma(fma(fma(3.2579232693911595, rhi, -15.638031693077565), rhi, 29.321309424520432), rhi, -26.063386155129276), rhi, 9.773769808173478), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(3.2579232693911595, rlo, -15.638031693077565), rlo, 29.321309424520432), rlo, -26.063386155129276), rlo, 9.773769808173478), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(2.4434424520433695, rhi, -11.170022637912545), rhi, 19.547539616346956), rhi, -15.638031693077565), rhi, 4.886884904086739), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(2.4434424520433695, rlo, -11.170022637912545), rlo, 19.547539616346956), rlo, -15.638031693077565), rlo, 4.886884904086739), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(3.2579232693911595, rhi, -15.638031693077565), rhi, 29.321309424520432), rhi, -26.063386155129276), rhi, 9.773769808173478))*rhi)*rhi) - (((fma(fma(fma(fma(3.2579232693911595, rlo, -15.638031693077565), rlo, 29.321309424520432), rlo, -26.063386155129276), rlo, 9.773769808173478))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(2.4434424520433695, rhi, -11.170022637912545), rhi, 19.547539616346956), rhi, -15.638031693077565), rhi, 4.886884904086739))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(2.4434424520433695, rlo, -11.170022637912545), rlo, 19.547539616346956), rlo, -15.638031693077565), rlo, 4.886884904086739))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<1>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 3/5: P = ['-30375/2398', '101250/1199', '-253125/1199', '281250/1199', '-234375/2398']
   o.W0 = -12.666805671392828*A[0] + 84.44537114261885*A[1] + -211.11342785654713*A[2] + 234.57047539616346*A[3] + -97.73769808173478*A[4];
-  o.W1 = (fma(fma(fma(fma(fma(fma(-16.289616346955796, rhi, 46.914095079232695), rhi, -52.77835696413678), rhi, 28.148457047539615), rhi, -6.333402835696414), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(-16.289616346955796, rlo, 46.914095079232695), rlo, -52.77835696413678), rlo, 28.148457047539615), rlo, -6.333402835696414), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(-16.289616346955796, rhi, 46.914095079232695), rhi, -52.77835696413678), rhi, 28.148457047539615), rhi, -6.333402835696414))*rhi)*rhi) - (((fma(fma(fma(fma(-16.289616346955796, rlo, 46.914095079232695), rlo, -52.77835696413678), rlo, 28.148457047539615), rlo, -6.333402835696414))*rlo)*rlo);
   o.P0 = 0.15200166805671392*A[0] + -6.333402835696414*A[2] + 28.148457047539615*A[3] + -52.77835696413678*A[4] + 46.914095079232695*A[5] + -16.289616346955796*A[6];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(-2.0362020433694745, rhi, 6.702013582747528), rhi, -8.79639282735613), rhi, 5.629691409507923), rhi, -1.5833507089241035), rhi, 0.0), rhi, 0.07600083402835696), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-2.0362020433694745, rlo, 6.702013582747528), rlo, -8.79639282735613), rlo, 5.629691409507923), rlo, -1.5833507089241035), rlo, 0.0), rlo, 0.07600083402835696), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(-2.0362020433694745, rhi, 6.702013582747528), rhi, -8.79639282735613), rhi, 5.629691409507923), rhi, -1.5833507089241035), rhi, 0.0), rhi, 0.07600083402835696))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(-2.0362020433694745, rlo, 6.702013582747528), rlo, -8.79639282735613), rlo, 5.629691409507923), rlo, -1.5833507089241035), rlo, 0.0), rlo, 0.07600083402835696))*rlo)*rlo);
   o.Lreg = -6.333402835696414*A[0] + 28.148457047539615*A[1] + -52.77835696413678*A[2] + 46.914095079232695*A[3] + -16.289616346955796*A[4];
   o.Preg = 0.07600083402835696*A[0] + -1.5833507089241035*A[2] + 5.629691409507923*A[3] + -8.79639282735613*A[4] + 6.702013582747528*A[5] + -2.0362020433694745*A[6];
   o.Mhat = -0.15200166805671392;
@@ -204,16 +204,16 @@ template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<1>(const
 template <> __host__ __device__ __forceinline__ void Kern_quartic::adj<1>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = -12.666805671392828*A[0] + 84.44537114261885*A[1] + -211.11342785654713*A[2] + 234.57047539616346*A[3] + -97.73769808173478*A[4];
   const double a2 = -12.666805671392828*A[2] + 84.44537114261885*A[3] + -211.11342785654713*A[4] + 234.57047539616346*A[5] + -97.73769808173478*A[6];
-  const double m1 = (fma(fma(fma(fma(fma(fma(-16.289616346955796, rhi, 46.914095079232695), rhi, -52.77835696413678), rhi, 28.148457047539615), rhi, -6.333402835696414), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(-16.289616346955796, rlo, 46.914095079232695), rlo, -52.77835696413678), rlo, 28.148457047539615), rlo, -6.333402835696414), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(-12.217212260216847, rhi, 33.510067913737636), rhi, -35.18557130942452), rhi, 16.88907422852377), rhi, -3.166701417848207), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-12.217212260216847, rlo, 33.510067913737636), rlo, -35.18557130942452), rlo, 16.88907422852377), rlo, -3.166701417848207), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(-16.289616346955796, rhi, 46.914095079232695), rhi, -52.77835696413678), rhi, 28.148457047539615), rhi, -6.333402835696414))*rhi)*rhi) - (((fma(fma(fma(fma(-16.289616346955796, rlo, 46.914095079232695), rlo, -52.77835696413678), rlo, 28.148457047539615), rlo, -6.333402835696414))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(-12.217212260216847, rhi, 33.510067913737636), rhi, -35.18557130942452), rhi, 16.88907422852377), rhi, -3.166701417848207))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(-12.217212260216847, rlo, 33.510067913737636), rlo, -35.18557130942452), rlo, 16.88907422852377), rlo, -3.166701417848207))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<2>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1/5: P = ['375/1199', '-7500/1199', '56250/1199', '-187500/1199', '234375/1199']
   o.W0 = 0.3127606338615513*A[0] + -6.255212677231026*A[1] + 46.914095079232695*A[2] + -156.38031693077565*A[3] + 195.47539616346955*A[4];
-  o.W1 = (fma(fma(fma(fma(fma(fma(32.57923269391159, rhi, -31.27606338615513), rhi, 11.728523769808174), rhi, -2.085070892410342), rhi, 0.15638031693077564), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(32.57923269391159, rlo, -31.27606338615513), rlo, 11.728523769808174), rlo, -2.085070892410342), rlo, 0.15638031693077564), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(32.57923269391159, rhi, -31.27606338615513), rhi, 11.728523769808174), rhi, -2.085070892410342), rhi, 0.15638031693077564))*rhi)*rhi) - (((fma(fma(fma(fma(32.57923269391159, rlo, -31.27606338615513), rlo, 11.728523769808174), rlo, -2.085070892410342), rlo, 0.15638031693077564))*rlo)*rlo);
   o.P0 = -0.0004170141784820684*A[0] + 0.15638031693077564*A[2] + -2.085070892410342*A[3] + 11.728523769808174*A[4] + -31.27606338615513*A[5] + 32.57923269391159*A[6];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(4.072404086738949, rhi, -4.468009055165019), rhi, 1.9547539616346956), rhi, -0.4170141784820684), rhi, 0.03909507923269391), rhi, 0.0), rhi, -0.0002085070892410342), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(4.072404086738949, rlo, -4.468009055165019), rlo, 1.9547539616346956), rlo, -0.4170141784820684), rlo, 0.03909507923269391), rlo, 0.0), rlo, -0.0002085070892410342), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(4.072404086738949, rhi, -4.468009055165019), rhi, 1.9547539616346956), rhi, -0.4170141784820684), rhi, 0.03909507923269391), rhi, 0.0), rhi, -0.0002085070892410342))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(4.072404086738949, rlo, -4.468009055165019), rlo, 1.9547539616346956), rlo, -0.4170141784820684), rlo, 0.03909507923269391), rlo, 0.0), rlo, -0.0002085070892410342))*rlo)*rlo);
   o.Lreg = 0.15638031693077564*A[0] + -2.085070892410342*A[1] + 11.728523769808174*A[2] + -31.27606338615513*A[3] + 32.57923269391159*A[4];
   o.Preg = -0.0002085070892410342*A[0] + 0.03909507923269391*A[2] + -0.4170141784820684*A[3] + 1.9547539616346956*A[4] + -4.468009055165019*A[5] + 4.072404086738949*A[6];
   o.Mhat = 0.0004170141784820684;
@@ -222,8 +222,8 @@ template <> __host__ __device__ __forceinline__ void Kern_quartic::sums<2>(const
 template <> __host__ __device__ __forceinline__ void Kern_quartic::adj<2>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 0.3127606338615513*A[0] + -6.255212677231026*A[1] + 46.914095079232695*A[2] + -156.38031693077565*A[3] + 195.47539616346955*A[4];
   const double a2 = 0.3127606338615513*A[2] + -6.255212677231026*A[3] + 46.914095079232695*A[4] + -156.38031693077565*A[5] + 195.47539616346955*A[6];
-  const double m1 = (fma(fma(fma(fma(fma(fma(32.57923269391159, rhi, -31.27606338615513), rhi, 11.728523769808174), rhi, -2.085070892410342), rhi, 0.15638031693077564), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(32.57923269391159, rlo, -31.27606338615513), rlo, 11.728523769808174), rlo, -2.085070892410342), rlo, 0.15638031693077564), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(24.434424520433694, rhi, -22.34004527582509), rhi, 7.8190158465387825), rhi, -1.2510425354462051), rhi, 0.07819015846538782), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(24.434424520433694, rlo, -22.34004527582509), rlo, 7.8190158465387825), rlo, -1.2510425354462051), rlo, 0.07819015846538782), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(32.57923269391159, rhi, -31.27606338615513), rhi, 11.728523769808174), rhi, -2.085070892410342), rhi, 0.15638031693077564))*rhi)*rhi) - (((fma(fma(fma(fma(32.57923269391159, rlo, -31.27606338615513), rlo, 11.728523769808174), rlo, -2.085070892410342), rlo, 0.15638031693077564))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(24.434424520433694, rhi, -22.34004527582509), rhi, 7.8190158465387825), rhi, -1.2510425354462051), rhi, 0.07819015846538782))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(24.434424520433694, rlo, -22.34004527582509), rlo, 7.8190158465387825), rlo, -1.2510425354462051), rlo, 0.07819015846538782))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
@@ -242,9 +242,9 @@ struct Kern_quintic {
 template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1: P = ['15309/478', '-76545/478', '76545/239', '-76545/239', '76545/478', '-15309/478']
   o.W0 = 32.02719665271967*A[0] + -160.13598326359832*A[1] + 320.27196652719664*A[2] + -320.27196652719664*A[3] + 160.13598326359832*A[4] + -32.02719665271967*A[5];
-  o.W1 = (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rhi, 26.689330543933053), rhi, -64.05439330543933), rhi, 80.06799163179916), rhi, -53.37866108786611), rhi, 16.013598326359833), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rlo, 26.689330543933053), rlo, -64.05439330543933), rlo, 80.06799163179916), rlo, -53.37866108786611), rlo, 16.013598326359833), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(fma(-4.575313807531381, rhi, 26.689330543933053), rhi, -64.05439330543933), rhi, 80.06799163179916), rhi, -53.37866108786611), rhi, 16.013598326359833))*rhi)*rhi) - (((fma(fma(fma(fma(fma(-4.575313807531381, rlo, 26.689330543933053), rlo, -64.05439330543933), rlo, 80.06799163179916), rlo, -53.37866108786611), rlo, 16.013598326359833))*rlo)*rlo);
   o.P0 = -0.7625523012552301*A[0] + 16.013598326359833*A[2] + -53.37866108786611*A[3] + 80.06799163179916*A[4] + -64.05439330543933*A[5] + 26.689330543933053*A[6] + -4.575313807531381*A[7];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.5083682008368201, rhi, 3.3361663179916317), rhi, -9.150627615062762), rhi, 13.344665271966527), rhi, -10.675732217573222), rhi, 4.003399581589958), rhi, 0.0), rhi, -0.38127615062761505), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.5083682008368201, rlo, 3.3361663179916317), rlo, -9.150627615062762), rlo, 13.344665271966527), rlo, -10.675732217573222), rlo, 4.003399581589958), rlo, 0.0), rlo, -0.38127615062761505), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(-0.5083682008368201, rhi, 3.3361663179916317), rhi, -9.150627615062762), rhi, 13.344665271966527), rhi, -10.675732217573222), rhi, 4.003399581589958), rhi, 0.0), rhi, -0.38127615062761505))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(-0.5083682008368201, rlo, 3.3361663179916317), rlo, -9.150627615062762), rlo, 13.344665271966527), rlo, -10.675732217573222), rlo, 4.003399581589958), rlo, 0.0), rlo, -0.38127615062761505))*rlo)*rlo);
   o.Lreg = 16.013598326359833*A[0] + -53.37866108786611*A[1] + 80.06799163179916*A[2] + -64.05439330543933*A[3] + 26.689330543933053*A[4] + -4.575313807531381*A[5];
   o.Preg = -0.38127615062761505*A[0] + 4.003399581589958*A[2] + -10.675732217573222*A[3] + 13.344665271966527*A[4] + -9.150627615062762*A[5] + 3.3361663179916317*A[6] + -0.5083682008368201*A[7];
   o.Mhat = 0.7625523012552301;
@@ -253,16 +253,16 @@ template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<0>(const
 template <> __host__ __device__ __forceinline__ void Kern_quintic::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 32.02719665271967*A[0] + -160.13598326359832*A[1] + 320.27196652719664*A[2] + -320.27196652719664*A[3] + 160.13598326359832*A[4] + -32.02719665271967*A[5];
   const double a2 = 32.02719665271967*A[2] + -160.13598326359832*A[3] + 320.27196652719664*A[4] + -320.27196652719664*A[5] + 160.13598326359832*A[6] + -32.02719665271967*A[7];
-  const double m1 = (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rhi, 26.689330543933053), rhi, -64.05439330543933), rhi, 80.06799163179916), rhi, -53.37866108786611), rhi, 16.013598326359833), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-4.575313807531381, rlo, 26.689330543933053), rlo, -64.05439330543933), rlo, 80.06799163179916), rlo, -53.37866108786611), rlo, 16.013598326359833), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-3.5585774058577404, rhi, 20.01699790794979), rhi, -45.75313807531381), rhi, 53.37866108786611), rhi, -32.02719665271967), rhi, 8.006799163179917), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-3.5585774058577404, rlo, 20.01699790794979), rlo, -45.75313807531381), rlo, 53.37866108786611), rlo, -32.02719665271967), rlo, 8.006799163179917), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(fma(-4.575313807531381, rhi, 26.689330543933053), rhi, -64.05439330543933), rhi, 80.06799163179916), rhi, -53.37866108786611), rhi, 16.013598326359833))*rhi)*rhi) - (((fma(fma(fma(fma(fma(-4.575313807531381, rlo, 26.689330543933053), rlo, -64.05439330543933), rlo, 80.06799163179916), rlo, -53.37866108786611), rlo, 16.013598326359833))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(-3.5585774058577404, rhi, 20.01699790794979), rhi, -45.75313807531381), rhi, 53.37866108786611), rhi, -32.02719665271967), rhi, 8.006799163179917))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(-3.5585774058577404, rlo, 20.01699790794979), rlo, -45.75313807531381), rlo, 53.37866108786611), rlo, -32.02719665271967), rlo, 8.006799163179917))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<1>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 2/3: P = ['-6048/239', '45360/239', '-136080/239', '204120/239', '-153090/239', '45927/239']
   o.W0 = -25.305439330543933*A[0] + 189.7907949790795*A[1] + -569.3723849372385*A[2] + 854.0585774058577*A[3] + -640.5439330543933*A[4] + 192.163179916318*A[5];
-  o.W1 = (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rhi, -106.75732217573221), rhi, 170.81171548117155), rhi, -142.34309623430963), rhi, 63.26359832635983), rhi, -12.652719665271967), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rlo, -106.75732217573221), rlo, 170.81171548117155), rlo, -142.34309623430963), rlo, 63.26359832635983), rlo, -12.652719665271967), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(fma(27.451882845188283, rhi, -106.75732217573221), rhi, 170.81171548117155), rhi, -142.34309623430963), rhi, 63.26359832635983), rhi, -12.652719665271967))*rhi)*rhi) - (((fma(fma(fma(fma(fma(27.451882845188283, rlo, -106.75732217573221), rlo, 170.81171548117155), rlo, -142.34309623430963), rlo, 63.26359832635983), rlo, -12.652719665271967))*rlo)*rlo);
   o.P0 = 0.26778242677824265*A[0] + -12.652719665271967*A[2] + 63.26359832635983*A[3] + -142.34309623430963*A[4] + 170.81171548117155*A[5] + -106.75732217573221*A[6] + 27.451882845188283*A[7];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.0502092050209204, rhi, -13.344665271966527), rhi, 24.401673640167363), rhi, -23.723849372384937), rhi, 12.652719665271967), rhi, -3.1631799163179917), rhi, 0.0), rhi, 0.13389121338912133), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(3.0502092050209204, rlo, -13.344665271966527), rlo, 24.401673640167363), rlo, -23.723849372384937), rlo, 12.652719665271967), rlo, -3.1631799163179917), rlo, 0.0), rlo, 0.13389121338912133), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(3.0502092050209204, rhi, -13.344665271966527), rhi, 24.401673640167363), rhi, -23.723849372384937), rhi, 12.652719665271967), rhi, -3.1631799163179917), rhi, 0.0), rhi, 0.13389121338912133))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(3.0502092050209204, rlo, -13.344665271966527), rlo, 24.401673640167363), rlo, -23.723849372384937), rlo, 12.652719665271967), rlo, -3.1631799163179917), rlo, 0.0), rlo, 0.13389121338912133))*rlo)*rlo);
   o.Lreg = -12.652719665271967*A[0] + 63.26359832635983*A[1] + -142.34309623430963*A[2] + 170.81171548117155*A[3] + -106.75732217573221*A[4] + 27.451882845188283*A[5];
   o.Preg = 0.13389121338912133*A[0] + -3.1631799163179917*A[2] + 12.652719665271967*A[3] + -23.723849372384937*A[4] + 24.401673640167363*A[5] + -13.344665271966527*A[6] + 3.0502092050209204*A[7];
   o.Mhat = -0.26778242677824265;
@@ -271,16 +271,16 @@ template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<1>(const
 template <> __host__ __device__ __forceinline__ void Kern_quintic::adj<1>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = -25.305439330543933*A[0] + 189.7907949790795*A[1] + -569.3723849372385*A[2] + 854.0585774058577*A[3] + -640.5439330543933*A[4] + 192.163179916318*A[5];
   const double a2 = -25.305439330543933*A[2] + 189.7907949790795*A[3] + -569.3723849372385*A[4] + 854.0585774058577*A[5] + -640.5439330543933*A[6] + 192.163179916318*A[7];
-  const double m1 = (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rhi, -106.75732217573221), rhi, 170.81171548117155), rhi, -142.34309623430963), rhi, 63.26359832635983), rhi, -12.652719665271967), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(27.451882845188283, rlo, -106.75732217573221), rlo, 170.81171548117155), rlo, -142.34309623430963), rlo, 63.26359832635983), rlo, -12.652719665271967), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(21.351464435146443, rhi, -80.06799163179916), rhi, 122.00836820083683), rhi, -94.89539748953975), rhi, 37.9581589958159), rhi, -6.326359832635983), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(21.351464435146443, rlo, -80.06799163179916), rlo, 122.00836820083683), rlo, -94.89539748953975), rlo, 37.9581589958159), rlo, -6.326359832635983), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(fma(27.451882845188283, rhi, -106.75732217573221), rhi, 170.81171548117155), rhi, -142.34309623430963), rhi, 63.26359832635983), rhi, -12.652719665271967))*rhi)*rhi) - (((fma(fma(fma(fma(fma(27.451882845188283, rlo, -106.75732217573221), rlo, 170.81171548117155), rlo, -142.34309623430963), rlo, 63.26359832635983), rlo, -12.652719665271967))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(21.351464435146443, rhi, -80.06799163179916), rhi, 122.00836820083683), rhi, -94.89539748953975), rhi, 37.9581589958159), rhi, -6.326359832635983))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(21.351464435146443, rlo, -80.06799163179916), rlo, 122.00836820083683), rlo, -94.89539748953975), rlo, 37.9581589958159), rlo, -6.326359832635983))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<2>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1/3: P = ['945/478', '-14175/478', '42525/239', '-127575/239', '382725/478', '-229635/478']
   o.W0 = 1.9769874476987448*A[0] + -29.65481171548117*A[1] + 177.92887029288704*A[2] + -533.7866108786611*A[3] + 800.6799163179917*A[4] + -480.407949790795*A[5];
-  o.W1 = (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rhi, 133.44665271966528), rhi, -106.75732217573221), rhi, 44.48221757322176), rhi, -9.884937238493723), rhi, 0.9884937238493724), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rlo, 133.44665271966528), rlo, -106.75732217573221), rlo, 44.48221757322176), rlo, -9.884937238493723), rlo, 0.9884937238493724), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(fma(-68.6297071129707, rhi, 133.44665271966528), rhi, -106.75732217573221), rhi, 44.48221757322176), rhi, -9.884937238493723), rhi, 0.9884937238493724))*rhi)*rhi) - (((fma(fma(fma(fma(fma(-68.6297071129707, rlo, 133.44665271966528), rlo, -106.75732217573221), rlo, 44.48221757322176), rlo, -9.884937238493723), rlo, 0.9884937238493724))*rlo)*rlo);
   o.P0 = -0.005230125523012552*A[0] + 0.9884937238493724*A[2] + -9.884937238493723*A[3] + 44.48221757322176*A[4] + -106.75732217573221*A[5] + 133.44665271966528*A[6] + -68.6297071129707*A[7];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-7.625523012552302, rhi, 16.68083158995816), rhi, -15.251046025104603), rhi, 7.4137029288702925), rhi, -1.9769874476987448), rhi, 0.2471234309623431), rhi, 0.0), rhi, -0.002615062761506276), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-7.625523012552302, rlo, 16.68083158995816), rlo, -15.251046025104603), rlo, 7.4137029288702925), rlo, -1.9769874476987448), rlo, 0.2471234309623431), rlo, 0.0), rlo, -0.002615062761506276), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(-7.625523012552302, rhi, 16.68083158995816), rhi, -15.251046025104603), rhi, 7.4137029288702925), rhi, -1.9769874476987448), rhi, 0.2471234309623431), rhi, 0.0), rhi, -0.002615062761506276))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(-7.625523012552302, rlo, 16.68083158995816), rlo, -15.251046025104603), rlo, 7.4137029288702925), rlo, -1.9769874476987448), rlo, 0.2471234309623431), rlo, 0.0), rlo, -0.002615062761506276))*rlo)*rlo);
   o.Lreg = 0.9884937238493724*A[0] + -9.884937238493723*A[1] + 44.48221757322176*A[2] + -106.75732217573221*A[3] + 133.44665271966528*A[4] + -68.6297071129707*A[5];
   o.Preg = -0.002615062761506276*A[0] + 0.2471234309623431*A[2] + -1.9769874476987448*A[3] + 7.4137029288702925*A[4] + -15.251046025104603*A[5] + 16.68083158995816*A[6] + -7.625523012552302*A[7];
   o.Mhat = 0.005230125523012552;
@@ -289,8 +289,8 @@ template <> __host__ __device__ __forceinline__ void Kern_quintic::sums<2>(const
 template <> __host__ __device__ __forceinline__ void Kern_quintic::adj<2>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 1.9769874476987448*A[0] + -29.65481171548117*A[1] + 177.92887029288704*A[2] + -533.7866108786611*A[3] + 800.6799163179917*A[4] + -480.407949790795*A[5];
   const double a2 = 1.9769874476987448*A[2] + -29.65481171548117*A[3] + 177.92887029288704*A[4] + -533.7866108786611*A[5] + 800.6799163179917*A[6] + -480.407949790795*A[7];
-  const double m1 = (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rhi, 133.44665271966528), rhi, -106.75732217573221), rhi, 44.48221757322176), rhi, -9.884937238493723), rhi, 0.9884937238493724), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(-68.6297071129707, rlo, 133.44665271966528), rlo, -106.75732217573221), rlo, 44.48221757322176), rlo, -9.884937238493723), rlo, 0.9884937238493724), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(-53.37866108786611, rhi, 100.08498953974896), rhi, -76.25523012552301), rhi, 29.65481171548117), rhi, -5.930962343096234), rhi, 0.4942468619246862), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(-53.37866108786611, rlo, 100.08498953974896), rlo, -76.25523012552301), rlo, 29.65481171548117), rlo, -5.930962343096234), rlo, 0.4942468619246862), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(fma(-68.6297071129707, rhi, 133.44665271966528), rhi, -106.75732217573221), rhi, 44.48221757322176), rhi, -9.884937238493723), rhi, 0.9884937238493724))*rhi)*rhi) - (((fma(fma(fma(fma(fma(-68.6297071129707, rlo, 133.44665271966528), rlo, -106.75732217573221), rlo, 44.48221757322176), rlo, -9.884937238493723), rlo, 0.9884937238493724))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(-53.37866108786611, rhi, 100.08498953974896), rhi, -76.25523012552301), rhi, 29.65481171548117), rhi, -5.930962343096234), rhi, 0.4942468619246862))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(-53.37866108786611, rlo, 100.08498953974896), rlo, -76.25523012552301), rlo, 29.65481171548117), rlo, -5.930962343096234), rlo, 0.4942468619246862))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
@@ -309,9 +309,9 @@ struct Kern_poly6 {
 template <> __host__ __device__ __forceinline__ void Kern_poly6::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
   // block R = 1: P = ['4', '0', '-12', '0', '12', '0', '-4']
   o.W0 = 4.0*A[0] + -12.0*A[2] + 12.0*A[4] + -4.0*A[6];
-  o.W1 = (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, -3.0), rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, -3.0), rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, 0.0));
+  o.W1 = (((fma(fma(fma(fma(fma(fma(-0.5, rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, -3.0), rhi, 0.0), rhi, 2.0))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(-0.5, rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, -3.0), rlo, 0.0), rlo, 2.0))*rlo)*rlo);
   o.P0 = -0.5*A[0] + 2.0*A[2] + -3.0*A[4] + 2.0*A[6] + -0.5*A[8];
-  o.P1 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.05, rhi, 0.0), rhi, 0.25), rhi, 0.0), rhi, -0.5), rhi, 0.0), rhi, 0.5), rhi, 0.0), rhi, -0.25), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.05, rlo, 0.0), rlo, 0.25), rlo, 0.0), rlo, -0.5), rlo, 0.0), rlo, 0.5), rlo, 0.0), rlo, -0.25), rlo, 0.0), rlo, 0.0));
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(fma(-0.05, rhi, 0.0), rhi, 0.25), rhi, 0.0), rhi, -0.5), rhi, 0.0), rhi, 0.5), rhi, 0.0), rhi, -0.25))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(-0.05, rlo, 0.0), rlo, 0.25), rlo, 0.0), rlo, -0.5), rlo, 0.0), rlo, 0.5), rlo, 0.0), rlo, -0.25))*rlo)*rlo);
   o.Lreg = 2.0*A[0] + -3.0*A[2] + 2.0*A[4] + -0.5*A[6];
   o.Preg = -0.25*A[0] + 0.5*A[2] + -0.5*A[4] + 0.25*A[6] + -0.05*A[8];
   o.Mhat = 0.5;
@@ -320,8 +320,8 @@ template <> __host__ __device__ __forceinline__ void Kern_poly6::sums<0>(const d
 template <> __host__ __device__ __forceinline__ void Kern_poly6::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
   const double a0 = 4.0*A[0] + -12.0*A[2] + 12.0*A[4] + -4.0*A[6];
   const double a2 = 4.0*A[2] + -12.0*A[4] + 12.0*A[6] + -4.0*A[8];
-  const double m1 = (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, -3.0), rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(-0.5, rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, -3.0), rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, 0.0));
-  const double m3 = (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.4, rhi, 0.0), rhi, 1.5), rhi, 0.0), rhi, -2.0), rhi, 0.0), rhi, 1.0), rhi, 0.0), rhi, 0.0), rhi, 0.0), rhi, 0.0)) - (fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(-0.4, rlo, 0.0), rlo, 1.5), rlo, 0.0), rlo, -2.0), rlo, 0.0), rlo, 1.0), rlo, 0.0), rlo, 0.0), rlo, 0.0), rlo, 0.0));
+  const double m1 = (((fma(fma(fma(fma(fma(fma(-0.5, rhi, 0.0), rhi, 2.0), rhi, 0.0), rhi, -3.0), rhi, 0.0), rhi, 2.0))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(-0.5, rlo, 0.0), rlo, 2.0), rlo, 0.0), rlo, -3.0), rlo, 0.0), rlo, 2.0))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(fma(-0.4, rhi, 0.0), rhi, 1.5), rhi, 0.0), rhi, -2.0), rhi, 0.0), rhi, 1.0))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(fma(-0.4, rlo, 0.0), rlo, 1.5), rlo, 0.0), rlo, -2.0), rlo, 0.0), rlo, 1.0))*rlo)*rlo)*rlo)*rlo);
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
@@ -329,7 +329,7 @@ template <> __host__ __device__ __forceinline__ void Kern_poly6::adj<0>(const do
 constexpr int kPlanEdgeTerms = 132;
 constexpr int kPlanValueTerms = 60;
 constexpr int kPlanCoeffs = 1140;
-constexpr int kPlanRadii = 12;
+constexpr int kPlanNumRadii = 12;
 struct PlanOffsets { int e0, e1, v0, v1; };
 static const PlanOffsets kPlanOffsets[kNumKernels] = {{0, 22, 0, 10}, {22, 33, 10, 15}, {33, 44, 15, 20}, {44, 55, 20, 25}, {55, 88, 25, 40}, {88, 121, 40, 55}, {121, 132, 55, 60}};
 static const int kPlanE[kPlanEdgeTerms][7] = {   // ch, i, a, b, radius index, c0, c1
@@ -531,6 +531,6 @@ static const int kPlanVi[kPlanValueTerms][4] = {   // ch, radius index, c0, c1
 static const double kPlanVmR[kPlanValueTerms] = {0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.04081632653061224, -0.0012755102040816326, 0.04081632653061224, -0.0012755102040816326, 0.5, 0.5, 0.5, 0.034722222222222224, 0.034722222222222224, 0.5, 0.5, 0.5, 0.026515151515151516, 0.026515151515151516, 0.5, 0.5, 0.5, 0.02142857142857143, 0.02142857142857143, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.5, 0.5, 0.5, 0.05, 0.05};
 static const int kPlanCn[kPlanCoeffs] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8};
 static const double kPlanCc[kPlanCoeffs] = {5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05};
-static const double kPlanRadii[kPlanRadii] = {1.0, 0.5, 1.0, 1.0, 1.0, 1.0, 0.6, 0.2, 1.0, 0.6666666666666666, 0.3333333333333333, 1.0};
+static const double kPlanRadii[kPlanNumRadii] = {1.0, 0.5, 1.0, 1.0, 1.0, 1.0, 0.6, 0.2, 1.0, 0.6666666666666666, 0.3333333333333333, 1.0};
 
 }  // namespace wsb

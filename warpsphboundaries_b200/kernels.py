@@ -402,7 +402,7 @@ def emit_header() -> str:
     out.append(f"constexpr int kPlanEdgeTerms = {len(E)};")
     out.append(f"constexpr int kPlanValueTerms = {len(V)};")
     out.append(f"constexpr int kPlanCoeffs = {len(CN)};")
-    out.append(f"constexpr int kPlanRadii = {len(RAD)};")
+    out.append(f"constexpr int kPlanNumRadii = {len(RAD)};")
     out.append("struct PlanOffsets { int e0, e1, v0, v1; };")
     out.append("static const PlanOffsets kPlanOffsets[kNumKernels] = {" + ", ".join("{%d, %d, %d, %d}" % o for o in offs) + "};")
     out.append("static const int kPlanE[kPlanEdgeTerms][7] = {   // ch, i, a, b, radius index, c0, c1")
@@ -414,7 +414,7 @@ def emit_header() -> str:
     out.append("static const double kPlanVmR[kPlanValueTerms] = {" + ", ".join(_lit(v[4]) for v in V) + "};")
     out.append("static const int kPlanCn[kPlanCoeffs] = {" + ", ".join(str(x) for x in CN) + "};")
     out.append("static const double kPlanCc[kPlanCoeffs] = {" + ", ".join(_lit(x) for x in CC) + "};")
-    out.append("static const double kPlanRadii[kPlanRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
+    out.append("static const double kPlanRadii[kPlanNumRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
     out.append("")
     out.append("}  // namespace wsb")
     out.append("")
@@ -434,3 +434,35 @@ if __name__ == "__main__":       # python -m warpsphboundaries_b200.kernels  -> 
     p = pathlib.Path(__file__).parent / "csrc" / "kernel_tables.h"
     p.write_text(emit_header())
     print("wrote", p)
+
+
+# ------------------------------------------------------------------ algorithmic work per pair
+def _horner_flops(coeffs):
+    cs = list(coeffs)
+    while len(cs) > 1 and cs[-1] == 0:
+        cs.pop()
+    low = 0
+    while low < len(cs) - 1 and cs[low] == 0:
+        low += 1
+    return 2 * (len(cs) - 1 - low) + low          # one FMA per Horner step, one multiply per power factor
+
+
+def pair_work(name):
+    """algorithmic float64 work of one (particle, edge) neighbour pair in the closed form of the fused route, counted
+    from the formulas it evaluates (FMA = 2 flops; add, sub, mul = 1): {"flops": F, "sqrt": .., "div": .., "log": ..,
+    "atan2": ..} with every block's chord present (the work of a pair whose chords are all non-empty)."""
+    k = kernel(name)
+    flops = 2 + 3 + 2 + 3 + 4 + 4 + 4          # d, |d|^2, t, cross, s0, s1, relative vertices
+    sq, dv, lg, at = 1, 6, 0, 0                  # |d|, 1/ell, z/ell, four (v - x)/h
+    for b in k.blocks:
+        na = max(len(b.psi), len(b.fpsi), len(b.c))
+        flops += 3 + 1 + 4 + 3 + 4 + 1 + 6 + 9 * max(na - 2, 0)    # chord, zz, r_lo/r_hi, log args, angle args, A_0, A_1, A_n
+        sq += 3
+        dv += 1
+        lg += 1
+        at += 1
+        nz = lambda a: sum(1 for c in a if c != 0)
+        flops += (2 * nz(b.c) - 1) + (2 * nz(b.psi) - 1) + (2 * nz(b.flam) - 1) + (2 * nz(b.fpsi) - 1)
+        flops += 2 * _horner_flops(b.m) + 1 + 2 * _horner_flops(b.mpsi) + 1
+        flops += 50                                                  # the two value terms and the twelve accumulations
+    return {"flops": flops, "sqrt": sq, "div": dv, "log": lg, "atan2": at}

@@ -1,0 +1,252 @@
+"""The analytic boundary as a provider for an SPH scheme: the drop-in for `AnalyticBoundary` /
+`BoundaryProvider` (src/warpSPHBoundaries/scene/provider.py:38-113) and `FusedWall`
+(src/warpSPHBoundaries/scene/fused.py:500-725).
+
+    ab = AnalyticBoundary(scene)                      # route="fused" (default) or "plain"; precision "fp64" | "mixed"
+    fw = ab.aggregate(ps, support, kernel=KernelFunctions.Wendland4, lean=True)
+    fw.out["lam"] [B, N], fw.out["G"] [B, N, 2], fw.out["Cov"] [B, N, 2, 2]      # float64, world frame
+    fw.evaluate((WallOutput("m1", 0, "m1"), WallOutput("m2", 0, "m2"), WallOutput("A", 0, "a1g1")), a1=a1)
+
+Routes:
+  fused  wsb_aggregate: body frame, broadphase, cell-sorted rows, float64 neighbour predicate and the closed-form
+         channels of each neighbour pair accumulated in registers, indicator, scaling, rotation -- one pass per
+         (body, surface), no per-pair storage.
+  plain  the reference's structure on the GPU: fixed-capacity slots (wsb_fixed_topology), the per-slot plan
+         interpreter (wsb_slot_channels_plain) writing c[N*K, 12], and the per-row contraction (wsb_contract).
+
+Outputs that belong to kernels this build does not tabulate (the delta+ layout's cover vector `cone`, wall Laplacian
+`lw2`/`lw4`, tensile `w2p5`/`w4p5`) and `cone_area` / `dir_extreme` raise NotImplementedError; they never return zeros.
+"""
+from dataclasses import dataclass
+from typing import Optional, Protocol, runtime_checkable
+
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr
+from .fixedadj import body_candidates, fixed_adjacency
+from .kernels import KERNEL_IDS
+from .scene import Scene, SurfaceRep, _stream
+from .shim import (GradientScheme, KernelFunctions, OperationDirection, OperationProperties, WarpOperation, kernelName,
+                   queryAllowed)
+
+F64 = torch.float64
+KINDS = {"lam": (0, 1), "g0": (1, 2), "cov": (2, 4), "a1g1": (3, 2), "lap": (4, 1), "m1": (5, 2), "m2": (6, 4)}
+_PREC = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+
+
+@runtime_checkable
+class BoundaryProvider(Protocol):
+    """what a scheme needs from a boundary representation (provider.py:38-45)."""
+    bodies: list
+
+    def aggregate(self, ps, support, **kwargs): ...
+
+    def signed_distance(self, x, body=None, supportMax=None, want_body=False): ...
+
+
+@dataclass(frozen=True)
+class WallOutput:
+    name: str
+    group: int
+    kind: str
+
+
+@dataclass(frozen=True)
+class FusedGroup:
+    """one kernel of the fused evaluation (warpfused.py:31-55): `kernel` (registered name), `channels` (None = all)."""
+    kernel: str
+    channels: Optional[tuple] = None
+    route: Optional[str] = None
+    nodes: Optional[int] = None
+    panels: Optional[int] = None
+
+
+class WallAggregate:
+    """marker base of the wall aggregates a scheme consumes (fused.py:497-499)."""
+
+
+class FusedWall(WallAggregate):
+    """all twelve channels of every (body, surface) at one position set, per kernel group, world frame, float64:
+    lam [B, N], G [B, N, 2], Cov [B, N, 2, 2], m1 [B, N, 2], m2 [B, N, 2, 2]."""
+
+    def __init__(self, scene, ps, support, groups, route="fused", precision="fp64", allowed=None):
+        self.scene = scene
+        self.groups = tuple(groups)
+        self.dev = scene.device
+        self.route = route
+        self.precision = precision
+        self.support = float(support)
+        pos = ps.positions.to(self.dev, F64).contiguous()
+        sup = ps.supports.to(self.dev, F64).contiguous()
+        self.N = N = len(pos)
+        B = len(scene.bodies)
+        for g in self.groups:
+            if g.kernel not in KERNEL_IDS:
+                raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} (wall-operator layout: cover / "
+                                          f"Laplacian / tensile) is not built; use the lean layout")
+        for b in scene.bodies:
+            for r in b.reps:
+                if not isinstance(r, SurfaceRep):
+                    raise NotImplementedError(f"FusedWall: {type(r).__name__} is not built (surface loops only)")
+                if r._triangle:
+                    raise NotImplementedError("FusedWall: a conditioned single-triangle SurfaceRep takes the sliver "
+                                              "quadrature, which is not built; use SurfaceRep(..., conditioned=False)")
+        self.res = []
+        for g in self.groups:
+            out = {"lam": torch.zeros((B, N), dtype=F64, device=self.dev),
+                   "G": torch.zeros((B, N, 2), dtype=F64, device=self.dev),
+                   "Cov": torch.zeros((B, N, 2, 2), dtype=F64, device=self.dev),
+                   "m1": torch.zeros((B, N, 2), dtype=F64, device=self.dev),
+                   "m2": torch.zeros((B, N, 2, 2), dtype=F64, device=self.dev)}
+            kid = KERNEL_IDS[g.kernel]
+            if route == "fused":
+                self._fused(pos, sup, allowed, kid, out)
+            elif route == "plain":
+                self._plain(ps, kid, out)
+            else:
+                raise ValueError(f"unknown route {route!r}")
+            self.res.append(out)
+        self.out = {}
+
+    def _fused(self, pos, sup, allowed, kid, out):
+        N = self.N
+        al = None if allowed is None else allowed.to(torch.int32).contiguous()
+        for bi, body in enumerate(self.scene.bodies):
+            pose = body.pose_tensor(self.dev)
+            obb = (_lib.ctypes.c_double * 4)(*body.obb())
+            for rep in body.reps:
+                ns = rep.native(self.support, self.dev)
+                ws, need = ns.workspace(N)
+                check(lib.wsb_aggregate(ns.handle, kid, _PREC[self.precision], ptr(pos), ptr(sup), ptr(al), N,
+                                        ptr(pose), obb, int(body.unbounded()), _lib.OUT_ALL, ptr(out["lam"][bi]),
+                                        ptr(out["G"][bi]), ptr(out["Cov"][bi]), ptr(out["m1"][bi]),
+                                        ptr(out["m2"][bi]), ptr(ws), need, None, _stream()), "wsb_aggregate")
+
+    def _plain(self, ps, kid, out):
+        props = OperationProperties(operationMode=OperationDirection.BoundaryToFluid)
+        adj = fixed_adjacency(self.scene, ps, props, self.support)
+        for bi, ba in enumerate(adj.bodies):
+            R = ba.body.pose.Rflat().contiguous()
+            lp, ls = ba.lpos.contiguous(), ba.lsup.contiguous()
+            for rep, topo in zip(ba.repList, ba.reps):
+                ns = rep.native(self.support, self.dev)
+                c = torch.empty(self.N * topo.K * 12, dtype=F64, device=self.dev)
+                check(lib.wsb_slot_channels_plain(ns.handle, kid, ptr(lp), ptr(ls), ptr(topo.e), self.N, ptr(c),
+                                                  _stream()), "wsb_slot_channels_plain")
+                check(lib.wsb_contract(ns.handle, kid, ptr(topo.e), ptr(c), ptr(topo.ind), ptr(ls), self.N, ptr(R),
+                                       ptr(out["lam"][bi]), ptr(out["G"][bi]), ptr(out["Cov"][bi]), ptr(out["m1"][bi]),
+                                       ptr(out["m2"][bi]), _stream()), "wsb_contract")
+
+    @staticmethod
+    def supported(scene, lowering=True):
+        return all(isinstance(r, SurfaceRep) for b in scene.bodies for r in b.reps)
+
+    def evaluate(self, outputs, a1=None):
+        """{name: tensor [B, N, ...]} float64, world frame (fused.py:612-659).  `a1` [B, N, 2]: world vectors of the
+        'a1g1' outputs (sum_d a1_d g1_dj)."""
+        res = {}
+        for o in outputs:
+            if o.kind not in KINDS:
+                raise ValueError(f"unknown output kind {o.kind!r}")
+            r = self.res[o.group]
+            if o.kind == "lam":
+                res[o.name] = r["lam"]
+            elif o.kind == "g0":
+                res[o.name] = r["G"]
+            elif o.kind == "cov":
+                res[o.name] = r["Cov"]
+            elif o.kind == "m1":
+                res[o.name] = r["m1"]
+            elif o.kind == "m2":
+                res[o.name] = r["m2"]
+            elif o.kind == "a1g1":
+                if a1 is None:
+                    raise ValueError("FusedWall.evaluate: a1 [B, N, 2] is required for 'a1g1' outputs")
+                res[o.name] = torch.einsum("bnd,bndj->bnj", a1.to(self.dev, F64), r["Cov"])
+            else:
+                raise NotImplementedError("FusedWall.evaluate: the wall Laplacian ('lap', kernels lw2 / lw4) is not "
+                                          "built")
+        return res
+
+    def _tensors(self):
+        out = []
+        for k, r in enumerate(self.res):
+            for name in sorted(r):
+                out.append((name, k, r[name]))
+        return out
+
+    def copy_from(self, other):
+        """overwrite this aggregate's buffers in place with `other`'s (same scene, groups and N), so kernels and CUDA
+        graphs that read these buffers see the new position set (fused.py:707-719)."""
+        a, b = self._tensors(), other._tensors()
+        if [(n, k, t.shape) for n, k, t in a] != [(n, k, t.shape) for n, k, t in b]:
+            raise ValueError("FusedWall.copy_from: different structure")
+        for (_, _, ta), (_, _, tb) in zip(a, b):
+            ta.copy_(tb)
+        for name in self.out:
+            if name in other.out:
+                self.out[name].copy_(other.out[name])
+
+    def reset_derived(self):
+        """no lazily derived buffers exist in this implementation (fused.py:721-725)."""
+
+    def cone_area(self, axes, half_angle):
+        raise NotImplementedError("FusedWall.cone_area (wedge area of the solid, fused.py:741-835) is not built")
+
+    def dir_extreme(self, vecs):
+        raise NotImplementedError("FusedWall.dir_extreme (fused.py:662-705) is not built")
+
+
+_FAMILY = {"Wendland2": "w2", "Wendland4": "w4"}
+
+
+class AnalyticBoundary:
+    """the analytic bodies of a `Scene` as a boundary provider (provider.py:48-113)."""
+
+    def __init__(self, scene: Scene, route: str = "fused", precision: str = "fp64"):
+        if precision not in _PREC:
+            raise ValueError(f"precision must be one of {sorted(_PREC)}")
+        self.scene = scene
+        self.route = route
+        self.precision = precision
+        self._layouts = {}
+
+    @property
+    def bodies(self):
+        return self.scene.bodies
+
+    def family(self, kernel):
+        fam = _FAMILY.get(getattr(kernel, "name", None))
+        if fam is None:
+            raise NotImplementedError("exact wall operations: Wendland C2 and C4 only")
+        return fam
+
+    def supported(self, fixedAdjacency=True):
+        return FusedWall.supported(self.scene, fixedAdjacency)
+
+    def properties(self, kernel, operation=WarpOperation.Density):
+        return OperationProperties(kernel=kernel, operation=operation, gradientMode=GradientScheme.Naive,
+                                   operationMode=OperationDirection.BoundaryToFluid)
+
+    def layout(self, kernel, laplacian, fixedAdjacency=True):
+        """the delta+ layout (kernel, cone, [lw], wp5) of provider.py:73-87: its wall-operator kernels are not built."""
+        raise NotImplementedError("AnalyticBoundary.layout: the delta+ wall-operator kernels (cover vector 'cone', "
+                                  "wall Laplacian, tensile) are not built; call aggregate(..., lean=True)")
+
+    def aggregate(self, ps, support, kernel=KernelFunctions.Wendland2, laplacian=False, fixedAdjacency=True,
+                  lean=False):
+        """the wall evaluation at the positions of `ps` (provider.py:89-110): `.out` holds lam, G, Cov per body;
+        `evaluate` serves m1, m2 and a1g1 as well.  `support`: host float >= every support of `ps`."""
+        if not lean:
+            self.layout(kernel, laplacian, fixedAdjacency)
+        groups = (FusedGroup(kernelName(kernel)),)
+        allowed = None
+        if getattr(ps, "kinds", None) is not None:      # without kinds every query is served: no mask, no host read
+            allowed = queryAllowed(ps, self.properties(kernel).operationMode, self.scene.device)
+        fw = FusedWall(self.scene, ps, support, groups, route=self.route, precision=self.precision, allowed=allowed)
+        fw.out = fw.evaluate([WallOutput("lam", 0, "lam"), WallOutput("G", 0, "g0"), WallOutput("Cov", 0, "cov")])
+        return fw
+
+    def signed_distance(self, x, body=None, supportMax=None, want_body=False):
+        return self.scene.signed_distance(x, body=body, supportMax=supportMax, want_body=want_body)

@@ -1,0 +1,423 @@
+"""Scene layer (2-D): rigid bodies with a pose, closed polygonal surfaces, kinematics and signed distance.
+
+The types and method names follow the reference's scene layer
+(src/warpSPHBoundaries/scene/scene.py): `Pose` (:64-97), `SurfaceRep` (:213-428),
+`Body` (:905-1067), `BodyKinematics` (:1155-1225), `Scene` (:1228-1372).  Every
+per-particle computation runs in libwsb.so on the GPU; this module holds the
+geometry, caches the device-resident static structures of each surface per
+(support, device) and marshals tensors.
+"""
+import ctypes
+from dataclasses import dataclass, field
+from fractions import Fraction
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr
+
+F64 = torch.float64
+
+
+# ----------------------------------------------------------------------------------------------------------- frames
+@dataclass
+class Pose:
+    center: torch.Tensor
+    angle: float = 0.0
+
+    def _cs(self):
+        a = float(self.angle)
+        return float(np.cos(a)), float(np.sin(a))
+
+    @property
+    def R(self):
+        c, s = self._cs()
+        return torch.tensor([[c, -s], [s, c]], dtype=F64, device=self.center.device)
+
+    def Rflat(self):
+        return self.R.reshape(-1)
+
+    def toLocal(self, p):
+        """(p - center) R with the rotation written out (scene.py:75-79)."""
+        c, s = self._cs()
+        d = p - self.center
+        return torch.stack([d[:, 0] * c + d[:, 1] * s, d[:, 1] * c - d[:, 0] * s], 1)
+
+    def toWorld(self, p):
+        c, s = self._cs()
+        return torch.stack([p[:, 0] * c - p[:, 1] * s + self.center[0], p[:, 0] * s + p[:, 1] * c + self.center[1]], 1)
+
+    def vecToWorld(self, v):
+        c, s = self._cs()
+        return torch.stack([v[:, 0] * c - v[:, 1] * s, v[:, 0] * s + v[:, 1] * c], 1)
+
+
+# ----------------------------------------------------------------------------------------------------------- native surface
+class NativeSurface:
+    """the device-resident static structures of one closed surface for supports <= support_max (wsb_surface)."""
+
+    def __init__(self, vertices, edges, background, support_max, device):
+        v = np.ascontiguousarray(vertices.detach().cpu().numpy(), dtype=np.float64).reshape(-1)
+        e = np.ascontiguousarray(edges.detach().cpu().numpy(), dtype=np.int32).reshape(-1)
+        self.device = torch.device(device)
+        idx = self.device.index if self.device.index is not None else torch.cuda.current_device()
+        h = ctypes.c_void_p()
+        check(lib.wsb_surface_create(v.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(v) // 2,
+                                     e.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(e) // 2, int(background),
+                                     float(support_max), idx, ctypes.byref(h)), "wsb_surface_create")
+        self.handle = h
+        info = _lib.SurfaceInfo()
+        check(lib.wsb_surface_info_get(h, ctypes.byref(info)), "wsb_surface_info_get")
+        self.info = info
+        self.K = int(info.K)
+        self.support_max = float(support_max)
+        self._ws = {}
+
+    def workspace(self, n):
+        """cached workspace tensor for n rows (the library allocates nothing per call)."""
+        need = int(lib.wsb_aggregate_workspace_size(self.handle, int(n)))
+        ws = self._ws.get(n)
+        if ws is None or ws.numel() < need:
+            ws = torch.empty(max(need, 1), dtype=torch.uint8, device=self.device)
+            self._ws[n] = ws
+        return ws, need
+
+    def cells(self):
+        """(start [nx*ny+1], items [n_items]) host copies of the edge cell list."""
+        start = np.zeros(self.info.nx * self.info.ny + 1, dtype=np.int32)
+        items = np.zeros(max(int(self.info.n_items), 1), dtype=np.int32)
+        check(lib.wsb_surface_cells(self.handle, start.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                    items.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))), "wsb_surface_cells")
+        return start, items[: int(self.info.n_items)]
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and lib is not None:
+            lib.wsb_surface_destroy(h)
+            self.handle = None
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+# ----------------------------------------------------------------------------------------------------------- representations
+class SurfaceRep:
+    """closed polylines in the body frame, counter-clockwise around the SOLID (solid on the left of every edge);
+    `background = 1` when the solid is the unbounded outside (scene.py:213-233)."""
+    kind = "surface"
+
+    def __init__(self, vertices, edges, background: int = 0, conditioned: bool = True):
+        self.vertices = torch.as_tensor(vertices, dtype=F64)
+        self.edges = torch.as_tensor(edges, dtype=torch.int32)
+        self.background = int(background)
+        # single-triangle reps would take the reference's conditioned sliver quadrature (warptriangle.py:126-201)
+        self._triangle = (len(self.vertices) == 3 and len(self.edges) == 3) if conditioned else False
+        self._native = {}
+
+    @staticmethod
+    def _orient(P, solid):
+        local = P.astype(np.longdouble) - P[0].astype(np.longdouble)
+        terms = local[:, 0] * np.roll(local[:, 1], -1) - np.roll(local[:, 0], -1) * local[:, 1]
+        a = np.sum(terms)
+        if len(P) == 3 or abs(a) <= 64 * np.finfo(np.longdouble).eps * np.sum(abs(terms)):
+            v = [[Fraction(float(c)) for c in p] for p in P]
+            a = sum((v[i][0] - v[0][0]) * (v[(i + 1) % len(v)][1] - v[0][1]) -
+                    (v[(i + 1) % len(v)][0] - v[0][0]) * (v[i][1] - v[0][1]) for i in range(len(v)))
+        if (a > 0) != (solid == "inside"):
+            P = P[::-1].copy()
+        return P
+
+    @staticmethod
+    def polygon(points, solid: str = "inside", conditioned: bool = True):
+        """one closed loop through `points` [n, 2]; 'inside': the polygon is the solid (made counter-clockwise),
+        'outside': a hole in an infinite solid (clockwise, background 1) (scene.py:235-256)."""
+        P = SurfaceRep._orient(np.asarray(points, dtype=float), solid)
+        n = len(P)
+        E = np.stack([np.arange(n), (np.arange(n) + 1) % n], 1)
+        return SurfaceRep(np.ascontiguousarray(P), E, background=0 if solid == "inside" else 1, conditioned=conditioned)
+
+    @staticmethod
+    def loops(loops, solid: str = "inside"):
+        """several closed loops in one representation (solids that overlap add through the winding number)."""
+        V, E, off = [], [], 0
+        for pts in loops:
+            P = SurfaceRep._orient(np.asarray(pts, dtype=float), solid)
+            n = len(P)
+            V.append(P)
+            E.append(np.stack([off + np.arange(n), off + (np.arange(n) + 1) % n], 1))
+            off += n
+        return SurfaceRep(np.concatenate(V), np.concatenate(E), background=0 if solid == "inside" else 1,
+                          conditioned=False)
+
+    @staticmethod
+    def box(lo, hi, solid: str = "inside"):
+        (x0, y0), (x1, y1) = lo, hi
+        return SurfaceRep.polygon([(x0, y0), (x1, y0), (x1, y1), (x0, y1)], solid)
+
+    @staticmethod
+    def regularPolygon(center, radius, n, solid="inside", areaPreserving=True):
+        r = radius * np.sqrt(2 * np.pi / (n * np.sin(2 * np.pi / n))) if areaPreserving else radius
+        t = 2 * np.pi * np.arange(n) / n
+        return SurfaceRep.polygon(np.stack([center[0] + r * np.cos(t), center[1] + r * np.sin(t)], 1), solid)
+
+    def to(self, device):
+        self.vertices = self.vertices.to(device)
+        self.edges = self.edges.to(device)
+        return self
+
+    def bounds(self):
+        return self.vertices.amin(0), self.vertices.amax(0)
+
+    def native(self, supportMax, device) -> NativeSurface:
+        """the static device structures for supports <= supportMax on `device` (built once, cached)."""
+        dev = torch.device(device)
+        if dev.type != "cuda":
+            raise RuntimeError("SurfaceRep: the boundary integrals run on CUDA devices only (no CPU fallback)")
+        key = (float(supportMax), str(dev))
+        ns = self._native.get(key)
+        if ns is None:
+            ns = NativeSurface(self.vertices, self.edges, self.background, float(supportMax), dev)
+            self._native[key] = ns
+        return ns
+
+    def _default_native(self, device):
+        if self._native:
+            for (sm, d), ns in self._native.items():
+                if d == str(torch.device(device)):
+                    return ns
+        lo, hi = self.bounds()
+        ext = float((hi - lo).max())
+        return self.native(max(ext / 64.0, 1e-9), device)
+
+    def indicator(self, p, supports=None):
+        """winding number of the loops around each point (+ background); on the boundary the angle fraction
+        (scene.py:350-396), evaluated on the device."""
+        ns = self._default_native(p.device)
+        p = p.to(F64).contiguous()
+        n = len(p)
+        sup = (supports.to(F64) if supports is not None else torch.ones(n, dtype=F64, device=p.device)).contiguous()
+        slots = torch.empty(n * ns.K, dtype=torch.int32, device=p.device)
+        ind = torch.empty(n, dtype=F64, device=p.device)
+        check(lib.wsb_fixed_topology(ns.handle, ptr(p), ptr(sup), None, n, ptr(slots), ptr(ind), _stream()),
+              "wsb_fixed_topology")
+        return ind
+
+    def topology(self, lpos, lsup):
+        """(query row, edge) pairs with segment distance < support (scene.py:374-382): a compacted fixed topology."""
+        from .fixedadj import fixed_topology
+        if len(lpos) == 0:
+            return None
+        supmax = float(lsup.max())
+        ft = fixed_topology(self, lpos, lsup, torch.ones(len(lpos), dtype=torch.bool, device=lpos.device), supmax)
+        keep = ft.e >= 0
+        return SurfaceTopology(ft.qi[keep], ft.e[keep], supmax, ft.ind)
+
+
+@dataclass
+class SurfaceTopology:
+    """the pair list of one SurfaceRep against a set of queries (scene.py:145-178)."""
+    qi: torch.Tensor
+    e: torch.Tensor
+    supMax: float
+    _ind: Optional[torch.Tensor] = None
+
+    def indicator(self, rep, lpos, lsup=None):
+        if self._ind is None:
+            self._ind = rep.indicator(lpos, lsup)
+        return self._ind
+
+
+@dataclass
+class RepMoments:
+    """per-query moments of one representation in physical units (scene.py:181-210): lam [P], g0 [P,2], m1 [P,2],
+    g1 [P,2,2] = int y (x) grad_x W, m2 [P,2,2]."""
+    q: torch.Tensor
+    lam: torch.Tensor
+    g0: torch.Tensor
+    m1: Optional[torch.Tensor] = None
+    g1: Optional[torch.Tensor] = None
+    m2: Optional[torch.Tensor] = None
+
+    def toWorld(self, pose: Pose):
+        R = pose.R
+        return RepMoments(self.q, self.lam, self.g0 @ R.T, None if self.m1 is None else self.m1 @ R.T,
+                          None if self.g1 is None else R @ self.g1 @ R.T, None if self.m2 is None else R @ self.m2 @ R.T)
+
+
+# ----------------------------------------------------------------------------------------------------------- bodies
+@dataclass
+class Body:
+    bodyId: int = 0
+    center: tuple = (0.0, 0.0)
+    angle: float = 0.0
+    linearVelocity: tuple = (0.0, 0.0)
+    angularVelocity: float = 0.0
+    reps: list = field(default_factory=list)
+    linearAcceleration: tuple = (0.0, 0.0)
+    angularAcceleration: float = 0.0
+    bc: str = "noSlip"
+    bcValue: tuple = (0.0, 0.0)
+
+    def __post_init__(self):
+        self.center = torch.as_tensor(self.center, dtype=F64)
+        self.linearVelocity = torch.as_tensor(self.linearVelocity, dtype=F64)
+        self.linearAcceleration = torch.as_tensor(self.linearAcceleration, dtype=F64)
+        self.bcValue = torch.as_tensor(self.bcValue, dtype=F64)
+
+    @property
+    def pose(self):
+        return Pose(self.center, float(self.angle))
+
+    def relative(self, world):
+        return world - self.center
+
+    def toLocal(self, world):
+        return self.pose.toLocal(world)
+
+    def velocityAt(self, world):
+        """v + omega J (x - c) (scene.py:1063-1067)."""
+        w = float(self.angularVelocity)
+        r = self.relative(world)
+        return self.linearVelocity.to(world.device) + w * torch.stack([-r[:, 1], r[:, 0]], 1)
+
+    def accelerationAt(self, world):
+        """a + alpha J s - omega^2 s (scene.py:934-939)."""
+        s = self.relative(world)
+        w, al = float(self.angularVelocity), float(self.angularAcceleration)
+        return self.linearAcceleration.to(world.device) + al * torch.stack([-s[:, 1], s[:, 0]], 1) - w * w * s
+
+    def move(self, dt: float):
+        """explicit Euler pose update (scene.py:968-973)."""
+        self.center = self.center + dt * self.linearVelocity
+        self.angle = float(self.angle) + dt * float(self.angularVelocity)
+        self.linearVelocity = self.linearVelocity + dt * self.linearAcceleration.to(self.linearVelocity.device)
+        self.angularVelocity = float(self.angularVelocity) + dt * float(self.angularAcceleration)
+
+    def obb(self):
+        """the bounding box of the representations in the body frame (host floats, cached)."""
+        key = tuple(id(r) for r in self.reps)
+        c = self.__dict__.get("_obbCache")
+        if c is None or c[0] != key:
+            los, his = zip(*[r.bounds() for r in self.reps])
+            lo = torch.stack([a.cpu() for a in los]).amin(0)
+            hi = torch.stack([a.cpu() for a in his]).amax(0)
+            c = (key, (float(lo[0]), float(lo[1]), float(hi[0]), float(hi[1])))
+            self._obbCache = c
+        return c[1]
+
+    def unbounded(self):
+        return any(isinstance(r, SurfaceRep) and r.background for r in self.reps)
+
+    def fusable(self):
+        return all(isinstance(r, SurfaceRep) for r in self.reps)
+
+    def pose_tensor(self, device):
+        """(cx, cy, cos, sin) on the device, cached while the pose is unchanged."""
+        c, s = self.pose._cs()
+        key = (self.center.data_ptr(), self.center._version, c, s, str(device))
+        hit = self.__dict__.get("_poseCache")
+        if hit is None or hit[0] != key:
+            t = torch.cat([self.center.to(device, F64).reshape(2), torch.tensor([c, s], dtype=F64, device=device)])
+            hit = (key, t)
+            self._poseCache = hit
+        return hit[1]
+
+    def state_row(self):
+        """(cx, cy, cos, sin, vx, vy, omega, ax, ay, alpha) of the kinematics kernel."""
+        c, s = self.pose._cs()
+        return [float(self.center[0]), float(self.center[1]), c, s, float(self.linearVelocity[0]),
+                float(self.linearVelocity[1]), float(self.angularVelocity), float(self.linearAcceleration[0]),
+                float(self.linearAcceleration[1]), float(self.angularAcceleration)]
+
+
+class BodyKinematics:
+    """rigid-body fields of all bodies at the positions x, [B, N, 2] each, from one kernel launch (scene.py:1155-1225):
+    rel = x - c, local = Pose.toLocal(x), velocity = v + omega J rel, acceleration = a + alpha J rel - omega^2 rel."""
+
+    def __init__(self, bodies, x):
+        self.x = x.to(F64).contiguous()
+        self._bodies = bodies
+        B, N, dev = len(bodies), len(x), x.device
+        state = torch.tensor([b.state_row() for b in bodies], dtype=F64, device=dev).reshape(-1)
+        self.rel = torch.empty((B, N, 2), dtype=F64, device=dev)
+        self._loc = torch.empty_like(self.rel)
+        self._vel = torch.empty_like(self.rel)
+        self._acc = torch.empty_like(self.rel)
+        check(lib.wsb_kinematics(ptr(state), B, ptr(self.x), N, ptr(self.rel), ptr(self._loc), ptr(self._vel),
+                                 ptr(self._acc), _stream()), "wsb_kinematics")
+
+    @property
+    def local(self):
+        return self._loc
+
+    @property
+    def velocity(self):
+        return self._vel
+
+    @property
+    def acceleration(self):
+        return self._acc
+
+
+class Scene:
+    def __init__(self, bodies: List[Body], device="cuda"):
+        self.bodies = bodies
+        self.device = torch.device(device)
+        for b in bodies:
+            b.center = b.center.to(self.device)
+            b.linearVelocity = b.linearVelocity.to(self.device)
+            b.linearAcceleration = b.linearAcceleration.to(self.device)
+            b.bcValue = b.bcValue.to(self.device)
+            for r in b.reps:
+                r.to(self.device)
+
+    def kinematics(self, x):
+        return BodyKinematics(self.bodies, x) if self.bodies else None
+
+    def signed_distance(self, points, body=None, supportMax=None, want_body=False):
+        """(d [M], n [M, 2], hit [M][, body [M]]) of world points to the nearest body: d > 0 in the fluid, n the unit
+        normal from the wall into the fluid (scene.py:1312-1372)."""
+        pts = points.to(self.device, F64).contiguous()
+        M = len(pts)
+        bidx = torch.full((M,), -1, dtype=torch.long, device=self.device)
+        best = torch.full((M,), float("inf"), dtype=F64, device=self.device)
+        normal = torch.zeros((M, 2), dtype=F64, device=self.device)
+        hit = torch.zeros(M, dtype=torch.bool, device=self.device)
+        for bi, bd in enumerate(self.bodies):
+            if body is not None and bi != body:
+                continue
+            lp = bd.toLocal(pts).contiguous()
+            for rep in bd.reps:
+                if not isinstance(rep, SurfaceRep):
+                    continue
+                ns = rep.native(supportMax, self.device) if supportMax is not None else rep._default_native(self.device)
+                d = torch.empty(M, dtype=F64, device=self.device)
+                cp = torch.empty((M, 2), dtype=F64, device=self.device)
+                nl = torch.empty((M, 2), dtype=F64, device=self.device)
+                ed = torch.empty(M, dtype=torch.int32, device=self.device)
+                check(lib.wsb_signed_distance(ns.handle, ptr(lp), M, float(supportMax) if supportMax else 0.0, ptr(d),
+                                              ptr(cp), ptr(nl), ptr(ed), _stream()), "wsb_signed_distance")
+                n = bd.pose.vecToWorld(nl)
+                better = d < best
+                best = torch.where(better, d, best)
+                normal = torch.where(better[:, None], n, normal)
+                bidx = torch.where(better, torch.full_like(bidx, bi), bidx)
+                hit |= True
+        if want_body:
+            return best, normal, hit, bidx
+        return best, normal, hit
+
+    def inside(self, points, body=None):
+        pts = points.to(self.device, F64)
+        out = torch.zeros(len(pts), dtype=torch.bool, device=self.device)
+        for bi, bd in enumerate(self.bodies):
+            if body is not None and bi != body:
+                continue
+            lp = bd.toLocal(pts)
+            for rep in bd.reps:
+                if isinstance(rep, SurfaceRep):
+                    out |= rep.indicator(lp) > 0.5
+        return out
