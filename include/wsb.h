@@ -119,6 +119,19 @@ int wsb_aggregate_evaluate(const wsb_surface* s, int kernel, int precision, cons
                            const double* pose, int out_mask, double* lam, double* G, double* cov, double* m1,
                            double* m2, const void* workspace, size_t workspace_bytes, void* stream);
 
+/* wsb_aggregate without a caller workspace, for hosts that cannot allocate device memory for this library (their
+ * allocator owns the GPU's memory, or their step loop may not call cudaMalloc / cudaFree, which synchronise the
+ * device).  No counterpart in the reference: it exists for such C-ABI callers.  The scratch is a static 8 MiB device
+ * array inside libwsb.so (per GPU, held until the library is unloaded); the call allocates nothing.  It serves about
+ * 24 bytes per row plus 12 bytes per cell of the surface's grid, e.g. 262144 rows over a 256 x 256 grid; larger
+ * requests fail with WSB_ERR_SIZE.  The first call on a device looks the scratch address up (make that first call
+ * before any stream capture).  All calls share the one array: calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialised by the caller; each call clears the counters it needs. */
+int wsb_aggregate_noalloc(const wsb_surface* s, int kernel, int precision, const double* pos, const double* sup,
+                          const int32_t* allowed, int64_t n, const double* pose, const double* obb, int unbounded,
+                          int out_mask, double* lam, double* G, double* cov, double* m1, double* m2, int32_t* status,
+                          void* stream);
+
 /* Adjoint of wsb_aggregate's lam, m1, m2 (the moments m_alpha, |alpha| <= 2) by recomputation: given world-frame
  * gradients g_lam [n], g_m1 [n*2], g_m2 [n*4] (any may be NULL), ADD dL/dpos into d_pos [n*2] (world) and dL/dvertex
  * into d_verts [n_verts*2] (body frame; may be NULL).  Replaces warp2d.TorchMoment's backward and np2d

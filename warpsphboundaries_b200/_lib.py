@@ -18,6 +18,7 @@ OUT_LAM, OUT_G, OUT_COV, OUT_M1, OUT_M2, OUT_ALL = 1, 2, 4, 8, 16, 31
 EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_destroy", "wsb_surface_info_get",
            "wsb_surface_cells", "wsb_fixed_topology", "wsb_slot_channels_plain", "wsb_contract",
            "wsb_aggregate_workspace_size", "wsb_aggregate", "wsb_aggregate_prepare", "wsb_aggregate_evaluate",
+           "wsb_aggregate_noalloc",
            "wsb_aggregate_backward", "wsb_signed_distance",
            "wsb_kinematics"]
 
@@ -50,6 +51,8 @@ def _load():
                                   P, P]),
         "wsb_aggregate_prepare": (c_int, [P, P, P, P, c_int64, P, D, c_int, P, c_size_t, P]),
         "wsb_aggregate_evaluate": (c_int, [P, c_int, c_int, P, c_int64, P, c_int, P, P, P, P, P, P, c_size_t, P]),
+        "wsb_aggregate_noalloc": (c_int, [P, c_int, c_int, P, P, P, c_int64, P, D, c_int, c_int, P, P, P, P, P, P,
+                                          P]),
         "wsb_aggregate_backward": (c_int, [P, c_int, P, P, P, c_int64, P, D, c_int, P, P, P, P, P, P, c_size_t, P]),
         "wsb_signed_distance": (c_int, [P, P, c_int64, c_double, P, P, P, P, P]),
         "wsb_kinematics": (c_int, [P, c_int32, P, c_int64, P, P, P, P, P]),

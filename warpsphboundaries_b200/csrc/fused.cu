@@ -4,6 +4,8 @@
 // moments, signed distance and rigid-body kinematics.
 #include <cub/device/device_scan.cuh>
 
+#include <mutex>
+
 #include "common.cuh"
 
 namespace wsb {
@@ -469,4 +471,52 @@ extern "C" int wsb_kinematics(const double* bodies, int32_t n_bodies, const doub
                                                                                   velocity, acceleration);
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
+}
+
+// ------------------------------------------------------------------------------------------------ allocation-free aggregate
+// Some hosts cannot give this library device memory: a solver whose allocator has already reserved the GPU's memory
+// for its own pool, or a time-step loop that must not call cudaMalloc / cudaFree (they synchronise the whole device),
+// and that links the library through the C ABI with no workspace buffer to lend.  For them the aggregate can run on
+// a scratch area compiled into the library: a static device array of kNoAllocScratchBytes per GPU, resident for as
+// long as the library is loaded.  The address of that array is looked up once per device (cudaGetSymbolAddress with
+// the device current) on the first call for that device; host code must never pass the array's own name to a kernel,
+// since on the host that name only stands in for the device symbol.
+constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static void* g_noalloc_addr[64] = {nullptr};
+static std::mutex g_noalloc_mu;
+
+static int noalloc_scratch(int device, void** out) {
+  if (device < 0 || device >= 64) return fail(WSB_ERR_ARG, "wsb_aggregate_noalloc: device id out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "wsb_aggregate_noalloc: cudaGetSymbolAddress(scratch)");
+    g_noalloc_addr[device] = p;
+  }
+  *out = g_noalloc_addr[device];
+  return WSB_OK;
+}
+
+extern "C" int wsb_aggregate_noalloc(const wsb_surface* s_, int kernel, int precision, const double* pos,
+                                     const double* sup, const int32_t* allowed, int64_t n, const double* pose,
+                                     const double* obb, int unbounded, int out_mask, double* lam, double* G,
+                                     double* cov, double* m1, double* m2, int32_t* status, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  int rc = check_common(s, kernel, pos, sup, n, pose, obb, "wsb_aggregate_noalloc");
+  if (rc) return rc;
+  const size_t need = carve(s, n, nullptr).total;
+  if (need > kNoAllocScratchBytes)
+    return fail(WSB_ERR_SIZE, "wsb_aggregate_noalloc: " + std::to_string(n) + " rows on a " + std::to_string(s->nx) +
+                                  " x " + std::to_string(s->ny) + " cell grid need " + std::to_string(need) +
+                                  " bytes of scratch; the built-in scratch holds " +
+                                  std::to_string(kNoAllocScratchBytes) + " bytes (use wsb_aggregate with a workspace)");
+  if (n == 0) return WSB_OK;
+  WSB_CUDA(cudaSetDevice(s->device));
+  void* scratch = nullptr;
+  rc = noalloc_scratch(s->device, &scratch);
+  if (rc) return rc;
+  return wsb_aggregate(s_, kernel, precision, pos, sup, allowed, n, pose, obb, unbounded, out_mask, lam, G, cov, m1, m2,
+                       scratch, kNoAllocScratchBytes, status, stream);
 }
