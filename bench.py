@@ -211,12 +211,11 @@ def our_arm(args):
         ev.append(("prepare", e0, e1))
         for k in KERNELS:
             o = outs[k]
-            for t in o:
-                t.zero_()
             a = torch.cuda.Event(enable_timing=True)
             a.record(stream)
             _lib.check(_lib.lib.wsb_aggregate_evaluate(ns.handle, KERNEL_IDS[k], prec[precision], _lib.ptr(sup), N,
-                                                       _lib.ptr(pose), _lib.OUT_ALL, *[_lib.ptr(t) for t in o],
+                                                       _lib.ptr(pose), _lib.OUT_ALL | _lib.OUT_ASSIGN,
+                                                       *[_lib.ptr(t) for t in o],
                                                        _lib.ptr(ws), need, _stream()), "evaluate")
             b = torch.cuda.Event(enable_timing=True)
             b.record(stream)
@@ -361,7 +360,7 @@ def our_arm(args):
                              "peak_source": "measured: libwsbpeak FP64 FMA stream (this GPU, this run)",
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
                 "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
-                "gpu_launches": args.steps * (2 + len(KERNELS)),
+                "gpu_launches": args.steps * (4 + 2 * len(KERNELS)),
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -44,7 +44,8 @@ enum {
 };
 
 /* output selection bits of wsb_aggregate */
-enum { WSB_OUT_LAM = 1, WSB_OUT_G = 2, WSB_OUT_COV = 4, WSB_OUT_M1 = 8, WSB_OUT_M2 = 16, WSB_OUT_ALL = 31 };
+enum { WSB_OUT_LAM = 1, WSB_OUT_G = 2, WSB_OUT_COV = 4, WSB_OUT_M1 = 8, WSB_OUT_M2 = 16, WSB_OUT_ALL = 31,
+       WSB_OUT_ASSIGN = 32 /* overwrite the outputs (rows that are not candidates get zeros) instead of adding */ };
 
 typedef struct wsb_surface wsb_surface;
 
@@ -123,7 +124,7 @@ int wsb_aggregate_evaluate(const wsb_surface* s, int kernel, int precision, cons
  * allocator owns the GPU's memory, or their step loop may not call cudaMalloc / cudaFree, which synchronise the
  * device).  No counterpart in the reference: it exists for such C-ABI callers.  The scratch is a static 8 MiB device
  * array inside libwsb.so (per GPU, held until the library is unloaded); the call allocates nothing.  It serves about
- * 24 bytes per row plus 12 bytes per cell of the surface's grid, e.g. 262144 rows over a 256 x 256 grid; larger
+ * 48 bytes per row plus 12 bytes per cell of the surface's grid, e.g. 131072 rows over a 256 x 256 grid; larger
  * requests fail with WSB_ERR_SIZE.  The first call on a device looks the scratch address up (make that first call
  * before any stream capture).  All calls share the one array: calls that overlap on the GPU (other streams, other
  * threads) race and must be serialised by the caller; each call clears the counters it needs. */

@@ -13,7 +13,7 @@ LIB_PATH = Path(os.environ.get("WSB_LIB", Path(__file__).resolve().parent / "_bu
 
 WSB_OK, WSB_ERR_ARG, WSB_ERR_CUDA, WSB_ERR_UNSUPPORTED, WSB_ERR_SIZE, WSB_ERR_DEVICE = 0, -1, -2, -3, -4, -5
 PREC_FP64, PREC_MIXED = 0, 1
-OUT_LAM, OUT_G, OUT_COV, OUT_M1, OUT_M2, OUT_ALL = 1, 2, 4, 8, 16, 31
+OUT_LAM, OUT_G, OUT_COV, OUT_M1, OUT_M2, OUT_ALL, OUT_ASSIGN = 1, 2, 4, 8, 16, 31, 32
 
 EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_destroy", "wsb_surface_info_get",
            "wsb_surface_cells", "wsb_fixed_topology", "wsb_slot_channels_plain", "wsb_contract",

@@ -92,6 +92,25 @@ __device__ __forceinline__ bool seg_within(double px, double py, double ax, doub
   return __dsqrt_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey))) < h;
 }
 
+// The same predicate decided in float first: the float squared distance of the relative vectors (formed in double,
+// then rounded) is off by at most ~1e-6 relative for candidates of one cell, so outside a band of 1e-4 around h^2 the
+// float answer equals the double answer and the exact test only runs inside the band.
+__device__ __forceinline__ bool seg_within_fast(double px, double py, double ax, double ay, double bx, double by,
+                                                double h) {
+  const float dx = (float)(bx - ax), dy = (float)(by - ay);
+  const float rx = (float)(px - ax), ry = (float)(py - ay);
+  const float den = dx * dx + dy * dy;
+  if (den > 1e-30f) {
+    const float t = fminf(fmaxf(__fdividef(rx * dx + ry * dy, den), 0.0f), 1.0f);
+    const float ex = rx - t * dx, ey = ry - t * dy;
+    const float d2 = ex * ex + ey * ey;
+    const float h2 = (float)(h * h);
+    if (d2 < h2 * 0.9999f) return true;
+    if (d2 > h2 * 1.0001f) return false;
+  }
+  return seg_within(px, py, ax, ay, bx, by, h);
+}
+
 // ----------------------------------------------------------------------------------------------- indicator
 struct SurfView {        // the device pointers and scalars a kernel needs (passed by value)
   const double* verts;
@@ -125,12 +144,21 @@ __device__ __forceinline__ double indicator_at(const SurfView& S, double px, dou
   bool boundary = false;
   for (int i = S.bstart[iy]; i < S.bstart[iy + 1]; ++i) {
     const double4 r = S.erec[S.bitems[i]];
-    const double arx = __ddiv_rn(__dsub_rn(r.x, px), h), ary = __ddiv_rn(__dsub_rn(r.y, py), h);
-    const double crx = __ddiv_rn(__dsub_rn(r.z, px), h), cry = __ddiv_rn(__dsub_rn(r.w, py), h);
-    const double cr = cross2_rn(arx, ary, crx, cry);
-    if (r.y <= py && py < r.w && cr > 0.0) w += 1.0;
-    if (r.w <= py && py < r.y && cr < 0.0) w -= 1.0;
-    if (cr == 0.0 && dot2_rn(arx, ary, crx, cry) <= 0.0) boundary = true;
+    const bool up = r.y <= py && py < r.w, down = r.w <= py && py < r.y;
+    const double ax = __dsub_rn(r.x, px), ay = __dsub_rn(r.y, py), cx = __dsub_rn(r.z, px), cy = __dsub_rn(r.w, py);
+    // the sign of the support-normalised, product-rounded cross product is certain when the unnormalised one
+    // clears 1e-10 of its terms' magnitude (the normalised form is accurate to a few ulp of that magnitude)
+    const double cu = ax * cy - ay * cx, mag = fabs(ax * cy) + fabs(ay * cx);
+    double cr;
+    if (fabs(cu) > 1e-10 * mag) {
+      cr = cu;
+    } else {
+      const double arx = __ddiv_rn(ax, h), ary = __ddiv_rn(ay, h), crx = __ddiv_rn(cx, h), cry = __ddiv_rn(cy, h);
+      cr = cross2_rn(arx, ary, crx, cry);
+      if (cr == 0.0 && dot2_rn(arx, ary, crx, cry) <= 0.0) boundary = true;
+    }
+    if (up && cr > 0.0) w += 1.0;
+    if (down && cr < 0.0) w -= 1.0;
   }
   if (boundary) {
     double ang = 0.0;
@@ -295,35 +323,42 @@ __device__ __forceinline__ bool block_adjoint(const PairGeo& g, AdjSums& o) {
 
 // per-row contraction of slot channels (src/warpSPHBoundaries/scene/fused.py:69-154): fixed slot order, + indicator *
 // plane channels, physical scaling, rotation R v, R M R^T; added into the outputs
+__device__ __forceinline__ void put(double* p, double v, bool assign) {
+  if (assign)
+    *p = v;
+  else
+    *p += v;
+}
+
 __device__ __forceinline__ void write_outputs(const double ch[12], double h, const double* rot, int64_t r, double* lam,
-                                              double* G, double* cov, double* m1, double* m2) {
+                                              double* G, double* cov, double* m1, double* m2, bool assign = false) {
   const double R00 = rot[0], R01 = rot[1], R10 = rot[2], R11 = rot[3];
-  if (lam) lam[r] += ch[0];
+  if (lam) put(&lam[r], ch[0], assign);
   if (m1) {
     const double vx = h * ch[1], vy = h * ch[2];
-    m1[2 * r] += R00 * vx + R01 * vy;
-    m1[2 * r + 1] += R10 * vx + R11 * vy;
+    put(&m1[2 * r], R00 * vx + R01 * vy, assign);
+    put(&m1[2 * r + 1], R10 * vx + R11 * vy, assign);
   }
   if (G) {
     const double vx = ch[3] / h, vy = ch[4] / h;
-    G[2 * r] += R00 * vx + R01 * vy;
-    G[2 * r + 1] += R10 * vx + R11 * vy;
+    put(&G[2 * r], R00 * vx + R01 * vy, assign);
+    put(&G[2 * r + 1], R10 * vx + R11 * vy, assign);
   }
   if (cov) {
     const double a = ch[5], b = ch[6], c = ch[7], d = ch[8];
-    cov[4 * r + 0] += R00 * (a * R00 + b * R01) + R01 * (c * R00 + d * R01);
-    cov[4 * r + 1] += R00 * (a * R10 + b * R11) + R01 * (c * R10 + d * R11);
-    cov[4 * r + 2] += R10 * (a * R00 + b * R01) + R11 * (c * R00 + d * R01);
-    cov[4 * r + 3] += R10 * (a * R10 + b * R11) + R11 * (c * R10 + d * R11);
+    put(&cov[4 * r + 0], R00 * (a * R00 + b * R01) + R01 * (c * R00 + d * R01), assign);
+    put(&cov[4 * r + 1], R00 * (a * R10 + b * R11) + R01 * (c * R10 + d * R11), assign);
+    put(&cov[4 * r + 2], R10 * (a * R00 + b * R01) + R11 * (c * R00 + d * R01), assign);
+    put(&cov[4 * r + 3], R10 * (a * R10 + b * R11) + R11 * (c * R10 + d * R11), assign);
   }
   if (m2) {
     const double hh = h * h;
     const double xx = ch[9] * hh, xy = ch[10] * hh, yy = ch[11] * hh;
-    m2[4 * r + 0] += R00 * R00 * xx + 2.0 * R00 * R01 * xy + R01 * R01 * yy;
+    put(&m2[4 * r + 0], R00 * R00 * xx + 2.0 * R00 * R01 * xy + R01 * R01 * yy, assign);
     const double off = R00 * R10 * xx + (R00 * R11 + R01 * R10) * xy + R01 * R11 * yy;
-    m2[4 * r + 1] += off;
-    m2[4 * r + 2] += off;
-    m2[4 * r + 3] += R10 * R10 * xx + 2.0 * R10 * R11 * xy + R11 * R11 * yy;
+    put(&m2[4 * r + 1], off, assign);
+    put(&m2[4 * r + 2], off, assign);
+    put(&m2[4 * r + 3], R10 * R10 * xx + 2.0 * R10 * R11 * xy + R11 * R11 * yy, assign);
   }
 }
 

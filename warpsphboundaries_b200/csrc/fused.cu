@@ -21,6 +21,11 @@ struct Workspace {
   int32_t* offs;     // [nbk + 1] exclusive prefix sums of counts
   int32_t* cursor;   // [nbk]
   int32_t* order;    // [n] rows sorted by bucket
+  double* ind;       // [n] indicator of a row (by row index)
+  int32_t* flag;     // [n] 0 not a candidate, 1 candidate without neighbour pairs, 2 row with pairs (by row index)
+  int32_t* has;      // [n + 1] 1 where the sorted row has pairs
+  int32_t* woff;     // [n + 1] exclusive prefix sums of has: the slot of a work row; woff[n] = number of work rows
+  int32_t* work;     // [n] sorted indices of the rows with pairs, in cell order
   void* cub_tmp;
   size_t cub_bytes;
   size_t total;
@@ -47,7 +52,12 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
   w.offs = (int32_t*)take(sizeof(int32_t) * (nbk + 1));
   w.cursor = (int32_t*)take(sizeof(int32_t) * nbk);
   w.order = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
-  w.cub_bytes = cub_scan_bytes(nbk + 1);
+  w.ind = (double*)take(sizeof(double) * std::max<int64_t>(n, 1));
+  w.flag = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.has = (int32_t*)take(sizeof(int32_t) * (n + 1));
+  w.woff = (int32_t*)take(sizeof(int32_t) * (n + 1));
+  w.work = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.cub_bytes = std::max(cub_scan_bytes(nbk + 1), cub_scan_bytes(n + 1));
   w.cub_tmp = take(w.cub_bytes);
   w.total = off;
   return w;
@@ -90,49 +100,140 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
   order[offs[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
 }
 
-// one thread per candidate row, rows in bucket order (threads of a warp share a cell and its edge records)
-template <class KT, int PREC>
-__global__ void __launch_bounds__(kThreads) k_agg_main(SurfView S, const double* __restrict__ sup,
-                                                      const int32_t* __restrict__ key,
-                                                      const double* __restrict__ lpos,
-                                                      const int32_t* __restrict__ offs,
-                                                      const int32_t* __restrict__ order, int64_t n,
-                                                      const double* __restrict__ pose, double* lam, double* G,
-                                                      double* cov, double* m1, double* m2) {
+// Per sorted row: does it have neighbour pairs (float-prefiltered exact predicate over its cell's candidates), and
+// its winding indicator -- both kernel independent, computed once per position set.
+__global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const int32_t* __restrict__ key,
+                              const double* __restrict__ lpos, const int32_t* __restrict__ offs,
+                              const int32_t* __restrict__ order, int64_t n, double* __restrict__ ind,
+                              int32_t* __restrict__ flag, int32_t* __restrict__ has) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j == 0) has[n] = 0;
+  if (j >= n) return;
   const int32_t ncells = S.nx * S.ny;
-  if (j >= n || j >= offs[ncells + 1]) return;       // rows past the candidates (bucket ncells + 1) take no part
   const int32_t i = order[j];
+  if (j >= (int64_t)offs[ncells + 1]) {      // not a candidate of this body
+    flag[i] = 0;
+    ind[i] = 0.0;
+    has[j] = 0;
+    return;
+  }
   const int32_t b = key[i];
   const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
-  double acc[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
-  double ind = S.background;
+  bool any = false;
   if (b < ncells) {
-    const int e0 = S.cstart[b], e1 = S.cstart[b + 1];
-    const double ih = 1.0 / h;
-    for (int k = e0; k < e1; ++k) {
+    for (int k = S.cstart[b]; k < S.cstart[b + 1]; ++k) {
       const double4 e = S.crec[k];
-      if (!seg_within(lx, ly, e.x, e.y, e.z, e.w, h)) continue;
-      PairGeo g;
-      if (!pair_geo((e.x - lx) / h, (e.y - ly) / h, (e.z - lx) / h, (e.w - ly) / h, g)) continue;
-      all_blocks<KT, 0, PREC>(g, acc);
+      if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
+        any = true;
+        break;
+      }
     }
-    (void)ih;
-    ind = indicator_at(S, lx, ly, h, true, b);
   }
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] *= kInvPi;
-  acc[0] += ind * KT::kMass;
-  acc[5] += ind * KT::kMass;
-  acc[8] += ind * KT::kMass;
-  acc[9] += ind * KT::kPlane2;
-  acc[11] += ind * KT::kPlane2;
+  ind[i] = (b < ncells) ? indicator_at(S, lx, ly, h, true, b) : S.background;
+  flag[i] = any ? 2 : 1;
+  has[j] = any ? 1 : 0;
+}
+
+__global__ void k_agg_compact(const int32_t* __restrict__ has, const int32_t* __restrict__ woff, int64_t n,
+                              int32_t* __restrict__ work) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j < n && has[j]) work[woff[j]] = (int32_t)j;
+}
+
+__device__ __forceinline__ void finish_row(double acc[12], double ind, double mass, double plane2, double h,
+                                           const double* pose, int64_t i, bool assign, double* lam, double* G,
+                                           double* cov, double* m1, double* m2) {
+  acc[0] += ind * mass;
+  acc[5] += ind * mass;
+  acc[8] += ind * mass;
+  acc[9] += ind * plane2;
+  acc[11] += ind * plane2;
   const double c = pose[2], s = pose[3];
   const double rot[4] = {c, -s, s, c};
-  write_outputs(acc, h, rot, i, lam, G, cov, m1, m2);
+  write_outputs(acc, h, rot, i, lam, G, cov, m1, m2, assign);
 }
+
+// rows without neighbour pairs: the indicator times the whole-plane channels (or zeros for non-candidates when the
+// outputs are assigned), coalesced over the row index
+template <class KT>
+__global__ void k_agg_rows(const double* __restrict__ sup, const double* __restrict__ ind,
+                           const int32_t* __restrict__ flag, int64_t n, const double* __restrict__ pose, bool assign,
+                           double* lam, double* G, double* cov, double* m1, double* m2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t f = flag[i];
+  if (f == 2 || (f == 0 && !assign)) return;
+  double acc[12];
+#pragma unroll
+  for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+  finish_row(acc, f == 1 ? ind[i] : 0.0, KT::kMass, KT::kPlane2, sup[i], pose, i, assign, lam, G, cov, m1, m2);
+}
+
+// Rows with neighbour pairs only (compacted, cell order).  A group of G adjacent lanes owns one row and splits its
+// cell's candidates (lane g takes candidates g, g + G, ...).  Each iteration every lane first advances, with the cheap
+// float-prefiltered predicate, to its next neighbour edge; then all lanes that found one evaluate the closed form
+// together.  The G partial sums are combined by an xor butterfly (the same additions on every lane, commutative, so
+// the result is deterministic and identical on the G lanes).
+template <class KT, int PREC, int G>
+__global__ void __launch_bounds__(kThreads) k_agg_pairs(SurfView S, const double* __restrict__ sup,
+                                                       const int32_t* __restrict__ key,
+                                                       const double* __restrict__ lpos,
+                                                       const int32_t* __restrict__ order,
+                                                       const int32_t* __restrict__ work,
+                                                       const int32_t* __restrict__ woff, int64_t n,
+                                                       const double* __restrict__ ind, const double* __restrict__ pose,
+                                                       bool assign, double* lam, double* G_, double* cov, double* m1,
+                                                       double* m2) {
+  static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "lanes per row");
+  const int64_t nwork = woff[n];
+  if ((int64_t)blockIdx.x * (blockDim.x / G) >= nwork) return;     // whole CTA past the work rows
+  const int64_t w = (int64_t)blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
+  const int sub = threadIdx.x % G;
+  const bool ok = w < nwork;
+  int32_t i = 0;
+  int k = 0, e1 = 0;
+  double lx = 0.0, ly = 0.0, h = 1.0;
+  if (ok) {
+    i = order[work[w]];
+    const int32_t b = key[i];
+    lx = lpos[2 * i];
+    ly = lpos[2 * i + 1];
+    h = sup[i];
+    k = S.cstart[b] + sub;
+    e1 = S.cstart[b + 1];
+  }
+  double acc[12];
+#pragma unroll
+  for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+  while (__any_sync(0xffffffffu, k < e1)) {
+    double4 e = make_double4(0.0, 0.0, 0.0, 0.0);
+    bool have = false;
+    while (k < e1) {
+      e = S.crec[k];
+      k += G;
+      if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
+        have = true;
+        break;
+      }
+    }
+    __syncwarp();
+    if (have) {
+      PairGeo g;
+      if (pair_geo((e.x - lx) / h, (e.y - ly) / h, (e.z - lx) / h, (e.w - ly) / h, g)) all_blocks<KT, 0, PREC>(g, acc);
+    }
+  }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+  }
+  if (!ok || sub != 0) return;
+#pragma unroll
+  for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
+  finish_row(acc, ind[i], KT::kMass, KT::kPlane2, h, pose, i, assign, lam, G_, cov, m1, m2);
+}
+
+constexpr int kLanesPerRow = 4;
 
 // ------------------------------------------------------------------------------------------------ adjoint
 // d/dx and d/dvertex of lam, m1, m2 by recomputation of the chord integrals int s^j W ds (j <= 3) of every neighbour
@@ -157,18 +258,17 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
                                                           const int32_t* __restrict__ key,
                                                           const double* __restrict__ lpos,
                                                           const int32_t* __restrict__ offs,
-                                                          const int32_t* __restrict__ order, int64_t n,
+                                                          const int32_t* __restrict__ order,
+                                                          const int32_t* __restrict__ work, int64_t n,
                                                           const double* __restrict__ pose,
                                                           const double* __restrict__ g_lam,
                                                           const double* __restrict__ g_m1,
                                                           const double* __restrict__ g_m2, double* d_pos,
                                                           double* d_verts) {
-  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int32_t ncells = S.nx * S.ny;
-  if (j >= n || j >= offs[ncells]) return;            // only rows inside the grid have neighbour pairs
-  const int32_t i = order[j];
+  const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (w >= n || w >= (int64_t)offs[n]) return;        // work rows only (rows with neighbour pairs)
+  const int32_t i = order[work[w]];
   const int32_t b = key[i];
-  if (b >= ncells) return;
   const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
   const double c = pose[2], s = pose[3];
   // upstream gradients in the body frame and in channel units: m1_world = R m1, m2_world = R m2 R^T
@@ -323,6 +423,12 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
   WSB_CUDA(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.counts, w.offs, (int)(nbk + 1), st));
   k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
   WSB_CUDA(cudaGetLastError());
+  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.has);
+  WSB_CUDA(cudaGetLastError());
+  bytes = w.cub_bytes;
+  WSB_CUDA(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.has, w.woff, (int)(n + 1), st));
+  k_agg_compact<<<grid, kThreads, 0, st>>>(w.has, w.woff, n, w.work);
+  WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }
 
@@ -383,14 +489,17 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   double* M2 = (out_mask & WSB_OUT_M2) ? m2 : nullptr;
   const SurfView v = view_of(s);
   const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
+  const bool assign = (out_mask & WSB_OUT_ASSIGN) != 0;
   int rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
+    k_agg_rows<KT><<<grid, kThreads, 0, st>>>(sup, w.ind, w.flag, n, pose, assign, L, Gp, C, M1, M2);
+    const unsigned pgrid = (unsigned)((n * kLanesPerRow + kThreads - 1) / kThreads);
     if (precision == WSB_PREC_MIXED)
-      k_agg_main<KT, WSB_PREC_MIXED><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, pose, L, Gp,
-                                                                C, M1, M2);
+      k_agg_pairs<KT, WSB_PREC_MIXED, kLanesPerRow><<<pgrid, kThreads, 0, st>>>(
+          v, sup, w.key, w.lpos, w.order, w.work, w.woff, n, w.ind, pose, assign, L, Gp, C, M1, M2);
     else
-      k_agg_main<KT, WSB_PREC_FP64><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, pose, L, Gp, C,
-                                                               M1, M2);
+      k_agg_pairs<KT, WSB_PREC_FP64, kLanesPerRow><<<pgrid, kThreads, 0, st>>>(
+          v, sup, w.key, w.lpos, w.order, w.work, w.woff, n, w.ind, pose, assign, L, Gp, C, M1, M2);
     return 0;
   });
   if (rc) return rc;
@@ -438,8 +547,8 @@ extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const d
   const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
   rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
-    k_agg_backward<KT><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, pose, g_lam, g_m1, g_m2,
-                                                  d_pos, d_verts);
+    k_agg_backward<KT><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.woff, w.order, w.work, n, pose, g_lam, g_m1,
+                                                  g_m2, d_pos, d_verts);
     return 0;
   });
   if (rc) return rc;

@@ -93,12 +93,13 @@ class FusedWall(WallAggregate):
                     raise NotImplementedError("FusedWall: a conditioned single-triangle SurfaceRep takes the sliver "
                                               "quadrature, which is not built; use SurfaceRep(..., conditioned=False)")
         self.res = []
+        alloc = torch.empty if route == "fused" else torch.zeros     # the fused route assigns every row of a body
         for g in self.groups:
-            out = {"lam": torch.zeros((B, N), dtype=F64, device=self.dev),
-                   "G": torch.zeros((B, N, 2), dtype=F64, device=self.dev),
-                   "Cov": torch.zeros((B, N, 2, 2), dtype=F64, device=self.dev),
-                   "m1": torch.zeros((B, N, 2), dtype=F64, device=self.dev),
-                   "m2": torch.zeros((B, N, 2, 2), dtype=F64, device=self.dev)}
+            out = {"lam": alloc((B, N), dtype=F64, device=self.dev),
+                   "G": alloc((B, N, 2), dtype=F64, device=self.dev),
+                   "Cov": alloc((B, N, 2, 2), dtype=F64, device=self.dev),
+                   "m1": alloc((B, N, 2), dtype=F64, device=self.dev),
+                   "m2": alloc((B, N, 2, 2), dtype=F64, device=self.dev)}
             kid = KERNEL_IDS[g.kernel]
             if route == "fused":
                 self._fused(pos, sup, allowed, kid, out)
@@ -113,13 +114,18 @@ class FusedWall(WallAggregate):
         N = self.N
         al = None if allowed is None else allowed.to(torch.int32).contiguous()
         for bi, body in enumerate(self.scene.bodies):
+            if not body.reps:
+                for t in out.values():
+                    t[bi].zero_()
+                continue
             pose = body.pose_tensor(self.dev)
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
-            for rep in body.reps:
+            for ri, rep in enumerate(body.reps):
                 ns = rep.native(self.support, self.dev)
                 ws, need = ns.workspace(N)
+                mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)     # the first surface of a body assigns
                 check(lib.wsb_aggregate(ns.handle, kid, _PREC[self.precision], ptr(pos), ptr(sup), ptr(al), N,
-                                        ptr(pose), obb, int(body.unbounded()), _lib.OUT_ALL, ptr(out["lam"][bi]),
+                                        ptr(pose), obb, int(body.unbounded()), mode, ptr(out["lam"][bi]),
                                         ptr(out["G"][bi]), ptr(out["Cov"][bi]), ptr(out["m1"][bi]),
                                         ptr(out["m2"][bi]), ptr(ws), need, None, _stream()), "wsb_aggregate")
 
