@@ -355,7 +355,7 @@ def our_arm(args):
                            "precision": args.precision, "l2": "flushed between steps (256 MiB write, untimed)"},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                              "frac": achieved / fp64_peak, "traffic": traffic,
-                             "kernel": "k_agg_main (wsb_aggregate_evaluate)",
+                             "kernel": "k_agg_pairs (wsb_aggregate_evaluate)",
                              "flops_per_pair": {k: pair_work(k)["flops"] for k in KERNELS},
                              "peak_source": "measured: libwsbpeak FP64 FMA stream (this GPU, this run)",
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},

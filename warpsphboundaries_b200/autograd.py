@@ -43,6 +43,7 @@ class BoundaryMoments(torch.autograd.Function):
                                 ptr(ws), need, None, _stream()), "wsb_aggregate")
         ctx.save_for_backward(posc, supc)
         ctx.body, ctx.rep, ctx.kid, ctx.support, ctx.nverts = body, rep, kid, support, len(verts)
+        ctx.verts_device, ctx.verts_dtype = verts.device, verts.dtype
         return lam, m1, m2, G, Cov
 
     @staticmethod
@@ -66,7 +67,8 @@ class BoundaryMoments(torch.autograd.Function):
         check(lib.wsb_aggregate_backward(ns.handle, ctx.kid, ptr(posc), ptr(supc), None, N, ptr(pose), obb,
                                          int(ctx.body.unbounded()), ptr(gl), ptr(g1), ptr(g2), ptr(d_pos),
                                          ptr(d_verts), ptr(ws), need, _stream()), "wsb_aggregate_backward")
-        return d_pos, d_verts, None, None, None, None, None, None
+        return (d_pos.to(posc.dtype), d_verts.to(ctx.verts_device, ctx.verts_dtype), None, None, None, None, None,
+                None)
 
 
 def aggregate_moments(body, rep, pos, sup, kernel, support, precision="fp64"):

@@ -56,6 +56,7 @@ struct Surface {
   int32_t* bstart = nullptr;    // [nb+1]
   int32_t* bitems = nullptr;    // [n_bitems]
   double4* erec = nullptr;      // [n_edges] (ax, ay, bx, by) by edge id
+  double4* brec = nullptr;      // [n_bitems] the records of the y-bin items, bin order
   // host copies (tests, signed distance set-up)
   std::string err;
 };
@@ -123,6 +124,7 @@ struct SurfView {        // the device pointers and scalars a kernel needs (pass
   const int32_t* cempty;
   const int32_t* bstart;
   const int32_t* bitems;
+  const double4* brec;
   const double4* erec;
   int32_t nx, ny, nb, K;
   double lo_x, lo_y, cell, y0, dy;
@@ -143,7 +145,7 @@ __device__ __forceinline__ double indicator_at(const SurfView& S, double px, dou
   double w = 0.0;
   bool boundary = false;
   for (int i = S.bstart[iy]; i < S.bstart[iy + 1]; ++i) {
-    const double4 r = S.erec[S.bitems[i]];
+    const double4 r = S.brec[i];
     const bool up = r.y <= py && py < r.w, down = r.w <= py && py < r.y;
     const double ax = __dsub_rn(r.x, px), ay = __dsub_rn(r.y, py), cx = __dsub_rn(r.z, px), cy = __dsub_rn(r.w, py);
     // the sign of the support-normalised, product-rounded cross product is certain when the unnormalised one
@@ -193,17 +195,33 @@ struct PairGeo {
 // edge frame of a pair from the relative vertices p, q (units of h): warpbc.py:628-643
 __device__ __forceinline__ bool pair_geo(double p0, double p1, double q0, double q1, PairGeo& g) {
   const double d0 = q0 - p0, d1 = q1 - p1;
-  const double ell = sqrt(d0 * d0 + d1 * d1);
-  if (ell == 0.0) return false;
-  const double ie = 1.0 / ell;
+  const double ll = d0 * d0 + d1 * d1;
+  if (ll == 0.0) return false;
+  const double ie = rsqrt(ll);             // 1 / |d|: every edge-frame quantity is a product with it
   g.t0 = d0 * ie;
   g.t1 = d1 * ie;
   g.n0 = g.t1;
   g.n1 = -g.t0;
-  g.z = cross2_rn(p0, p1, q0, q1) / ell;   // the same rounded orientation as the indicator
+  g.z = cross2_rn(p0, p1, q0, q1) * ie;   // the same rounded orientation as the indicator
   g.s0 = (d0 * p0 + d1 * p1) * ie;
   g.s1 = (d0 * q0 + d1 * q1) * ie;
   return true;
+}
+
+// The edge frame of the pair (row at (px, py), support h, 1/h = ih; edge a -> b).  The relative vertices are formed by
+// multiplying with 1/h; where the orientation is so close to zero that the rounding of that form could decide its sign
+// (|cross| <= 1e-10 of its terms), they are re-formed by division, exactly as the indicator forms them, so the sign of
+// z and the winding indicator always agree.
+__device__ __forceinline__ bool pair_geo_row(double px, double py, double h, double ih, const double4& e, PairGeo& g) {
+  double p0 = (e.x - px) * ih, p1 = (e.y - py) * ih, q0 = (e.z - px) * ih, q1 = (e.w - py) * ih;
+  const double cu = p0 * q1 - p1 * q0;
+  if (!(fabs(cu) > 1e-10 * (fabs(p0 * q1) + fabs(p1 * q0)))) {
+    p0 = __ddiv_rn(__dsub_rn(e.x, px), h);
+    p1 = __ddiv_rn(__dsub_rn(e.y, py), h);
+    q0 = __ddiv_rn(__dsub_rn(e.z, px), h);
+    q1 = __ddiv_rn(__dsub_rn(e.w, py), h);
+  }
+  return pair_geo(p0, p1, q0, q1, g);
 }
 
 // asinh(hi/|z|) - asinh(lo/|z|) as one logarithm of positive factors (no cancellation of a + sqrt(a^2 + 1) for a < 0)

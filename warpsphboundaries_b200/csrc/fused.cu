@@ -4,6 +4,7 @@
 // moments, signed distance and rigid-body kinematics.
 #include <cub/device/device_scan.cuh>
 
+#include <cstdlib>
 #include <mutex>
 
 #include "common.cuh"
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(kThreads) k_agg_pairs(SurfView S, const double
     k = S.cstart[b] + sub;
     e1 = S.cstart[b + 1];
   }
+  const double ih = 1.0 / h;
   double acc[12];
 #pragma unroll
   for (int c = 0; c < 12; ++c) acc[c] = 0.0;
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(kThreads) k_agg_pairs(SurfView S, const double
     __syncwarp();
     if (have) {
       PairGeo g;
-      if (pair_geo((e.x - lx) / h, (e.y - ly) / h, (e.z - lx) / h, (e.w - ly) / h, g)) all_blocks<KT, 0, PREC>(g, acc);
+      if (pair_geo_row(lx, ly, h, ih, e, g)) all_blocks<KT, 0, PREC>(g, acc);
     }
   }
 #pragma unroll
@@ -233,7 +235,32 @@ __global__ void __launch_bounds__(kThreads) k_agg_pairs(SurfView S, const double
   finish_row(acc, ind[i], KT::kMass, KT::kPlane2, h, pose, i, assign, lam, G_, cov, m1, m2);
 }
 
-constexpr int kLanesPerRow = 4;
+// lanes per row of k_agg_pairs: 4 unless WSB_LANES_PER_ROW (1, 2, 4, 8) says otherwise (a tuning knob, read once)
+static int lanes_per_row() {
+  static int v = [] {
+    const char* e = getenv("WSB_LANES_PER_ROW");
+    const int x = e ? atoi(e) : 4;
+    return (x == 1 || x == 2 || x == 4 || x == 8) ? x : 4;
+  }();
+  return v;
+}
+
+template <class KT, int PREC>
+static void launch_pairs(const SurfView& v, const double* sup, const Workspace& w, int64_t n, const double* pose,
+                         bool assign, double* L, double* Gp, double* C, double* M1, double* M2, cudaStream_t st) {
+  const int G = lanes_per_row();
+  const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads);
+#define WSB_PAIRS(GG)                                                                                          \
+  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.order, w.work, w.woff, n, w.ind, \
+                                                       pose, assign, L, Gp, C, M1, M2)
+  switch (G) {
+    case 1: WSB_PAIRS(1); break;
+    case 2: WSB_PAIRS(2); break;
+    case 8: WSB_PAIRS(8); break;
+    default: WSB_PAIRS(4); break;
+  }
+#undef WSB_PAIRS
+}
 
 // ------------------------------------------------------------------------------------------------ adjoint
 // d/dx and d/dvertex of lam, m1, m2 by recomputation of the chord integrals int s^j W ds (j <= 3) of every neighbour
@@ -295,7 +322,7 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
     const double4 e = S.crec[k];
     if (!seg_within(lx, ly, e.x, e.y, e.z, e.w, h)) continue;
     PairGeo g;
-    if (!pair_geo((e.x - lx) / h, (e.y - ly) / h, (e.z - lx) / h, (e.w - ly) / h, g)) continue;
+    if (!pair_geo_row(lx, ly, h, 1.0 / h, e, g)) continue;
     AdjSums W = {0.0, 0.0, 0.0, 0.0};
     adj_blocks<KT, 0>(g, W);
     const double z = g.z, zn0 = z * g.n0, zn1 = z * g.n1;
@@ -493,13 +520,10 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   int rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
     k_agg_rows<KT><<<grid, kThreads, 0, st>>>(sup, w.ind, w.flag, n, pose, assign, L, Gp, C, M1, M2);
-    const unsigned pgrid = (unsigned)((n * kLanesPerRow + kThreads - 1) / kThreads);
     if (precision == WSB_PREC_MIXED)
-      k_agg_pairs<KT, WSB_PREC_MIXED, kLanesPerRow><<<pgrid, kThreads, 0, st>>>(
-          v, sup, w.key, w.lpos, w.order, w.work, w.woff, n, w.ind, pose, assign, L, Gp, C, M1, M2);
+      launch_pairs<KT, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, L, Gp, C, M1, M2, st);
     else
-      k_agg_pairs<KT, WSB_PREC_FP64, kLanesPerRow><<<pgrid, kThreads, 0, st>>>(
-          v, sup, w.key, w.lpos, w.order, w.work, w.woff, n, w.ind, pose, assign, L, Gp, C, M1, M2);
+      launch_pairs<KT, WSB_PREC_FP64>(v, sup, w, n, pose, assign, L, Gp, C, M1, M2, st);
     return 0;
   });
   if (rc) return rc;

@@ -36,6 +36,7 @@ SurfView view_of(const Surface* s) {
   v.cempty = s->cempty;
   v.bstart = s->bstart;
   v.bitems = s->bitems;
+  v.brec = s->brec;
   v.erec = s->erec;
   v.nx = s->nx;
   v.ny = s->ny;
@@ -65,7 +66,7 @@ __global__ void k_cell_indicator(SurfView S, int64_t ncells) {
     int iy = (int)iyd;
     if (iy > S.nb - 1) iy = S.nb - 1;
     for (int i = S.bstart[iy]; i < S.bstart[iy + 1]; ++i) {
-      const double4 r = S.erec[S.bitems[i]];
+      const double4 r = S.brec[i];
       const double cr = cross2_rn(r.x - px, r.y - py, r.z - px, r.w - py);
       if (r.y <= py && py < r.w && cr > 0.0) w += 1.0;
       if (r.w <= py && py < r.y && cr < 0.0) w -= 1.0;
@@ -93,7 +94,8 @@ static int upload(T** dst, const std::vector<T>& src) {
 }
 
 static void free_surface(Surface* s) {
-  void* ptrs[] = {s->verts, s->edges, s->cstart, s->citems, s->crec, s->cind, s->cempty, s->bstart, s->bitems, s->erec};
+  void* ptrs[] = {s->verts, s->edges, s->cstart, s->citems, s->crec, s->cind, s->cempty, s->bstart, s->bitems, s->erec,
+                  s->brec};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -211,6 +213,8 @@ extern "C" int wsb_surface_create(const double* verts, int64_t n_verts, const in
   s->dy = dy;
   s->n_bitems = (int64_t)bitems.size();
   std::memcpy(s->bbox, bb, sizeof(bb));
+  std::vector<double4> brec(bitems.size());
+  for (size_t i = 0; i < bitems.size(); ++i) brec[i] = erec[bitems[i]];
   std::vector<double> hv(verts, verts + 2 * n_verts);
   std::vector<int32_t> he(edges, edges + 2 * n_edges);
   std::vector<double> cind(ncells, 0.0);
@@ -218,7 +222,7 @@ extern "C" int wsb_surface_create(const double* verts, int64_t n_verts, const in
   if ((rc = upload(&s->verts, hv)) || (rc = upload(&s->edges, he)) || (rc = upload(&s->cstart, start)) ||
       (rc = upload(&s->citems, items)) || (rc = upload(&s->crec, crec)) || (rc = upload(&s->cind, cind)) ||
       (rc = upload(&s->cempty, cempty)) || (rc = upload(&s->bstart, bstart)) || (rc = upload(&s->bitems, bitems)) ||
-      (rc = upload(&s->erec, erec))) {
+      (rc = upload(&s->erec, erec)) || (rc = upload(&s->brec, brec))) {
     free_surface(s);
     delete s;
     return rc;
