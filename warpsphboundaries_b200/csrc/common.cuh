@@ -51,7 +51,8 @@ struct Surface {
   int32_t* cstart = nullptr;    // [nx*ny+1]
   int32_t* citems = nullptr;    // [n_items]
   double4* crec = nullptr;      // [n_items] (ax, ay, bx, by) of the item's edge, cell-list order
-  double* cind = nullptr;       // [nx*ny] indicator of edge-free cells
+  double* cind = nullptr;       // [nx*ny] winding + background at the cell centre
+  int32_t* cok = nullptr;       // [nx*ny] 1 where the centre's winding is certain (clear of every edge line it tests)
   int32_t* cempty = nullptr;    // [nx*ny]
   int32_t* bstart = nullptr;    // [nb+1]
   int32_t* bitems = nullptr;    // [n_bitems]
@@ -121,6 +122,7 @@ struct SurfView {        // the device pointers and scalars a kernel needs (pass
   const double4* crec;
   const int32_t* citems;
   const double* cind;
+  const int32_t* cok;
   const int32_t* cempty;
   const int32_t* bstart;
   const int32_t* bitems;
@@ -174,6 +176,36 @@ __device__ __forceinline__ double indicator_at(const SurfView& S, double px, dou
     w = ang / kTwoPi;
   }
   return w + S.background;
+}
+
+// orientation of x against the line a -> b with a certainty test: returns +1 / -1, or 0 when |(b - a) x (x - a)| is
+// within 1e-10 of its terms (then the caller falls back to the reference's rounded ray cast)
+__device__ __forceinline__ int orient_certain(double ax, double ay, double bx, double by, double x, double y) {
+  const double ux = bx - ax, uy = by - ay, vx = x - ax, vy = y - ay;
+  const double o = ux * vy - uy * vx, mag = fabs(ux * vy) + fabs(uy * vx);
+  if (!(fabs(o) > 1e-10 * mag)) return 0;
+  return o > 0.0 ? 1 : -1;
+}
+
+// signed crossing of the segment r -> p with the edge a -> b (+1 when p lies on the edge's left = solid side and r on
+// its right, -1 the other way, 0 when they do not cross); *degenerate set when any orientation is uncertain
+__device__ __forceinline__ int segment_crossing(double rx, double ry, double px, double py, const double4& e,
+                                                bool* degenerate) {
+  const int orr = orient_certain(e.x, e.y, e.z, e.w, rx, ry), op = orient_certain(e.x, e.y, e.z, e.w, px, py);
+  if (orr == op && orr != 0) return 0;                               // same side of the edge line: no crossing
+  const int oa = orient_certain(rx, ry, px, py, e.x, e.y), ob = orient_certain(rx, ry, px, py, e.z, e.w);
+  if (orr == 0 || op == 0) {
+    // uncertain side of the edge line: it only matters if the segment reaches the edge
+    if (oa == ob && oa != 0) return 0;
+    *degenerate = true;
+    return 0;
+  }
+  if (oa == ob && oa != 0) return 0;                                 // the edge is on one side of the segment
+  if (oa == 0 || ob == 0) {
+    *degenerate = true;
+    return 0;
+  }
+  return op > 0 ? 1 : -1;
 }
 
 __device__ __forceinline__ bool cell_of(const SurfView& S, double px, double py, int32_t& cid) {

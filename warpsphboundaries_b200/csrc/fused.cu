@@ -2,6 +2,7 @@
 // body-frame position, runs the float64 neighbour predicate over the row's cell and accumulates the closed-form
 // channels of every neighbour pair in registers, then adds the indicator, scales and rotates.  Also the adjoint of the
 // moments, signed distance and rigid-body kinematics.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include <cstdlib>
@@ -24,9 +25,11 @@ struct Workspace {
   int32_t* order;    // [n] rows sorted by bucket
   double* ind;       // [n] indicator of a row (by row index)
   int32_t* flag;     // [n] 0 not a candidate, 1 candidate without neighbour pairs, 2 row with pairs (by row index)
-  int32_t* has;      // [n + 1] 1 where the sorted row has pairs
-  int32_t* woff;     // [n + 1] exclusive prefix sums of has: the slot of a work row; woff[n] = number of work rows
-  int32_t* work;     // [n] sorted indices of the rows with pairs, in cell order
+  int32_t* rkey;     // [n] radix key of a sorted row: 63 - min(pairs, 63) for rows with pairs, 64 otherwise
+  int32_t* rkey2;    // [n] sorted keys (unused after the sort)
+  int32_t* rval;     // [n] the sorted row index j
+  int32_t* work;     // [n] rows with pairs first, by decreasing pair count (stable: cell order within a count)
+  int32_t* nwork;    // [1] number of rows with pairs
   void* cub_tmp;
   size_t cub_bytes;
   size_t total;
@@ -35,6 +38,13 @@ struct Workspace {
 static size_t cub_scan_bytes(int64_t items) {
   size_t bytes = 0;
   cub::DeviceScan::ExclusiveSum(nullptr, bytes, (int32_t*)nullptr, (int32_t*)nullptr, (int)items);
+  return bytes;
+}
+
+static size_t cub_sort_bytes(int64_t items) {
+  size_t bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const int32_t*)nullptr, (int32_t*)nullptr, (const int32_t*)nullptr,
+                                  (int32_t*)nullptr, (int)std::max<int64_t>(items, 1), 0, 7);
   return bytes;
 }
 
@@ -55,10 +65,12 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
   w.order = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
   w.ind = (double*)take(sizeof(double) * std::max<int64_t>(n, 1));
   w.flag = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
-  w.has = (int32_t*)take(sizeof(int32_t) * (n + 1));
-  w.woff = (int32_t*)take(sizeof(int32_t) * (n + 1));
+  w.rkey = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.rkey2 = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.rval = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
   w.work = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
-  w.cub_bytes = std::max(cub_scan_bytes(nbk + 1), cub_scan_bytes(n + 1));
+  w.nwork = (int32_t*)take(sizeof(int32_t));
+  w.cub_bytes = std::max(cub_scan_bytes(nbk + 1), cub_sort_bytes(n));
   w.cub_tmp = take(w.cub_bytes);
   w.total = off;
   return w;
@@ -101,44 +113,48 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
   order[offs[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
 }
 
-// Per sorted row: does it have neighbour pairs (float-prefiltered exact predicate over its cell's candidates), and
-// its winding indicator -- both kernel independent, computed once per position set.
+// Per sorted row: its number of neighbour pairs (float-prefiltered exact predicate over its cell's candidates) as a
+// radix key, and its winding indicator -- both kernel independent, computed once per position set.
 __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const int32_t* __restrict__ key,
                               const double* __restrict__ lpos, const int32_t* __restrict__ offs,
                               const int32_t* __restrict__ order, int64_t n, double* __restrict__ ind,
-                              int32_t* __restrict__ flag, int32_t* __restrict__ has) {
+                              int32_t* __restrict__ flag, int32_t* __restrict__ rkey, int32_t* __restrict__ rval,
+                              int32_t* __restrict__ nwork) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j == 0) has[n] = 0;
-  if (j >= n) return;
-  const int32_t ncells = S.nx * S.ny;
-  const int32_t i = order[j];
-  if (j >= (int64_t)offs[ncells + 1]) {      // not a candidate of this body
-    flag[i] = 0;
-    ind[i] = 0.0;
-    has[j] = 0;
-    return;
-  }
-  const int32_t b = key[i];
-  const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
-  bool any = false;
-  if (b < ncells) {
-    for (int k = S.cstart[b]; k < S.cstart[b + 1]; ++k) {
-      const double4 e = S.crec[k];
-      if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
-        any = true;
-        break;
+  int cnt = 0;
+  if (j < n) {
+    const int32_t ncells = S.nx * S.ny;
+    const int32_t i = order[j];
+    if (j >= (int64_t)offs[ncells + 1]) {      // not a candidate of this body
+      flag[i] = 0;
+      ind[i] = 0.0;
+    } else {
+      const int32_t b = key[i];
+      const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
+      double w = S.background;
+      if (b < ncells) {
+        // one pass over the cell's candidates: the neighbour count and the signed crossings of the segment from the
+        // cell centre (whose exact winding is stored) to the row; an uncertain orientation falls back to the ray cast
+        const int64_t cx = b / S.ny, cy = b % S.ny;
+        const double rx = __dadd_rn(S.lo_x, __dmul_rn(__dadd_rn((double)cx, 0.5), S.cell));
+        const double ry = __dadd_rn(S.lo_y, __dmul_rn(__dadd_rn((double)cy, 0.5), S.cell));
+        bool degenerate = S.cok[b] == 0;
+        int cross = 0;
+        for (int k = S.cstart[b]; k < S.cstart[b + 1]; ++k) {
+          const double4 e = S.crec[k];
+          cnt += seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h) ? 1 : 0;
+          if (!degenerate) cross += segment_crossing(rx, ry, lx, ly, e, &degenerate);
+        }
+        w = degenerate ? indicator_at(S, lx, ly, h, true, b) : S.cind[b] + (double)cross;
       }
+      ind[i] = w;
+      flag[i] = cnt > 0 ? 2 : 1;
     }
+    rkey[j] = cnt > 0 ? 63 - min(cnt, 63) : 64;
+    rval[j] = (int32_t)j;
   }
-  ind[i] = (b < ncells) ? indicator_at(S, lx, ly, h, true, b) : S.background;
-  flag[i] = any ? 2 : 1;
-  has[j] = any ? 1 : 0;
-}
-
-__global__ void k_agg_compact(const int32_t* __restrict__ has, const int32_t* __restrict__ woff, int64_t n,
-                              int32_t* __restrict__ work) {
-  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j < n && has[j]) work[woff[j]] = (int32_t)j;
+  const unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(nwork, __popc(m));
 }
 
 __device__ __forceinline__ void finish_row(double acc[12], double ind, double mass, double plane2, double h,
@@ -181,12 +197,12 @@ __global__ void __launch_bounds__(kThreads) k_agg_pairs(SurfView S, const double
                                                        const double* __restrict__ lpos,
                                                        const int32_t* __restrict__ order,
                                                        const int32_t* __restrict__ work,
-                                                       const int32_t* __restrict__ woff, int64_t n,
+                                                       const int32_t* __restrict__ nwork_p, int64_t n,
                                                        const double* __restrict__ ind, const double* __restrict__ pose,
                                                        bool assign, double* lam, double* G_, double* cov, double* m1,
                                                        double* m2) {
   static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "lanes per row");
-  const int64_t nwork = woff[n];
+  const int64_t nwork = *nwork_p;
   if ((int64_t)blockIdx.x * (blockDim.x / G) >= nwork) return;     // whole CTA past the work rows
   const int64_t w = (int64_t)blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
   const int sub = threadIdx.x % G;
@@ -235,12 +251,13 @@ __global__ void __launch_bounds__(kThreads) k_agg_pairs(SurfView S, const double
   finish_row(acc, ind[i], KT::kMass, KT::kPlane2, h, pose, i, assign, lam, G_, cov, m1, m2);
 }
 
-// lanes per row of k_agg_pairs: 4 unless WSB_LANES_PER_ROW (1, 2, 4, 8) says otherwise (a tuning knob, read once)
+// lanes per row of k_agg_pairs: 2 unless WSB_LANES_PER_ROW (1, 2, 4, 8) says otherwise (a tuning knob, read once;
+// 2 measured fastest on the 2^20-particle scene: 1 / 2 / 4 lanes give 6.4 / 8.2 / 7.7e9 pairs/s)
 static int lanes_per_row() {
   static int v = [] {
     const char* e = getenv("WSB_LANES_PER_ROW");
-    const int x = e ? atoi(e) : 4;
-    return (x == 1 || x == 2 || x == 4 || x == 8) ? x : 4;
+    const int x = e ? atoi(e) : 2;
+    return (x == 1 || x == 2 || x == 4 || x == 8) ? x : 2;
   }();
   return v;
 }
@@ -251,13 +268,13 @@ static void launch_pairs(const SurfView& v, const double* sup, const Workspace& 
   const int G = lanes_per_row();
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads);
 #define WSB_PAIRS(GG)                                                                                          \
-  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.order, w.work, w.woff, n, w.ind, \
+  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.order, w.work, w.nwork, n, w.ind, \
                                                        pose, assign, L, Gp, C, M1, M2)
   switch (G) {
-    case 1: WSB_PAIRS(1); break;
-    case 2: WSB_PAIRS(2); break;
     case 8: WSB_PAIRS(8); break;
-    default: WSB_PAIRS(4); break;
+    case 1: WSB_PAIRS(1); break;
+    case 4: WSB_PAIRS(4); break;
+    default: WSB_PAIRS(2); break;
   }
 #undef WSB_PAIRS
 }
@@ -293,7 +310,7 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
                                                           const double* __restrict__ g_m2, double* d_pos,
                                                           double* d_verts) {
   const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (w >= n || w >= (int64_t)offs[n]) return;        // work rows only (rows with neighbour pairs)
+  if (w >= n || w >= (int64_t)offs[0]) return;        // work rows only (rows with neighbour pairs; offs = counter)
   const int32_t i = order[work[w]];
   const int32_t b = key[i];
   const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
@@ -450,12 +467,12 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
   WSB_CUDA(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.counts, w.offs, (int)(nbk + 1), st));
   k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
   WSB_CUDA(cudaGetLastError());
-  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.has);
+  WSB_CUDA(cudaMemsetAsync(w.nwork, 0, sizeof(int32_t), st));
+  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.rval,
+                                           w.nwork);
   WSB_CUDA(cudaGetLastError());
   bytes = w.cub_bytes;
-  WSB_CUDA(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.has, w.woff, (int)(n + 1), st));
-  k_agg_compact<<<grid, kThreads, 0, st>>>(w.has, w.woff, n, w.work);
-  WSB_CUDA(cudaGetLastError());
+  WSB_CUDA(cub::DeviceRadixSort::SortPairs(w.cub_tmp, bytes, w.rkey, w.rkey2, w.rval, w.work, (int)n, 0, 7, st));
   return WSB_OK;
 }
 
@@ -571,7 +588,7 @@ extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const d
   const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
   rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
-    k_agg_backward<KT><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.woff, w.order, w.work, n, pose, g_lam, g_m1,
+    k_agg_backward<KT><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.nwork, w.order, w.work, n, pose, g_lam, g_m1,
                                                   g_m2, d_pos, d_verts);
     return 0;
   });

@@ -33,6 +33,7 @@ SurfView view_of(const Surface* s) {
   v.crec = s->crec;
   v.citems = s->citems;
   v.cind = s->cind;
+  v.cok = s->cok;
   v.cempty = s->cempty;
   v.bstart = s->bstart;
   v.bitems = s->bitems;
@@ -51,28 +52,33 @@ SurfView view_of(const Surface* s) {
   return v;
 }
 
-// indicator of the centres of the edge-free cells (h = 1: no normalisation), scene.py:281-295
+// winding + background at every cell centre (h = 1: no normalisation) by the ray cast of scene.py:350-372.  For an
+// edge-free cell this is the indicator of every point of the cell (scene.py:281-295).  For a cell with edges it is
+// the reference point of the local crossing count; cok marks whether every orientation the ray cast tested was
+// certain (clear of rounding), i.e. whether the value is the exact winding number.
 __global__ void k_cell_indicator(SurfView S, int64_t ncells) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= ncells) return;
-  if (S.cempty[c] == 0) return;
   const int64_t cx = c / S.ny, cy = c % S.ny;
   const double px = __dadd_rn(S.lo_x, __dmul_rn(__dadd_rn((double)cx, 0.5), S.cell));
   const double py = __dadd_rn(S.lo_y, __dmul_rn(__dadd_rn((double)cy, 0.5), S.cell));
-  // ray casting over the y bin (the cache itself is not consulted for its own fill)
   const double iyd = floor(__ddiv_rn(__dsub_rn(py, S.y0), S.dy));
   double w = 0.0;
+  bool certain = true;
   if (iyd >= 0.0 && iyd <= (double)S.nb) {
     int iy = (int)iyd;
     if (iy > S.nb - 1) iy = S.nb - 1;
     for (int i = S.bstart[iy]; i < S.bstart[iy + 1]; ++i) {
       const double4 r = S.brec[i];
-      const double cr = cross2_rn(r.x - px, r.y - py, r.z - px, r.w - py);
+      const double ax = r.x - px, ay = r.y - py, bx = r.z - px, by = r.w - py;
+      const double cr = cross2_rn(ax, ay, bx, by);
+      if (!(fabs(cr) > 1e-10 * (fabs(ax * by) + fabs(ay * bx)))) certain = false;
       if (r.y <= py && py < r.w && cr > 0.0) w += 1.0;
       if (r.w <= py && py < r.y && cr < 0.0) w -= 1.0;
     }
   }
   const_cast<double*>(S.cind)[c] = w + S.background;
+  const_cast<int32_t*>(S.cok)[c] = (certain || S.cempty[c]) ? 1 : 0;
 }
 
 }  // namespace wsb
@@ -95,7 +101,7 @@ static int upload(T** dst, const std::vector<T>& src) {
 
 static void free_surface(Surface* s) {
   void* ptrs[] = {s->verts, s->edges, s->cstart, s->citems, s->crec, s->cind, s->cempty, s->bstart, s->bitems, s->erec,
-                  s->brec};
+                  s->brec, s->cok};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -222,7 +228,8 @@ extern "C" int wsb_surface_create(const double* verts, int64_t n_verts, const in
   if ((rc = upload(&s->verts, hv)) || (rc = upload(&s->edges, he)) || (rc = upload(&s->cstart, start)) ||
       (rc = upload(&s->citems, items)) || (rc = upload(&s->crec, crec)) || (rc = upload(&s->cind, cind)) ||
       (rc = upload(&s->cempty, cempty)) || (rc = upload(&s->bstart, bstart)) || (rc = upload(&s->bitems, bitems)) ||
-      (rc = upload(&s->erec, erec)) || (rc = upload(&s->brec, brec))) {
+      (rc = upload(&s->erec, erec)) || (rc = upload(&s->brec, brec)) ||
+      (rc = upload(&s->cok, std::vector<int32_t>(ncells, 0)))) {
     free_surface(s);
     delete s;
     return rc;
