@@ -17,6 +17,10 @@ restatement of the reference's numpy path) over a bounded particle sample, all c
 import argparse
 import json
 import os
+
+# expandable segments: the serving stream allocates buffers of widely varying sizes on several streams; without them
+# the caching allocator falls back to cudaMalloc (a device synchronisation) on most of those allocations
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 import statistics
 import subprocess
 import sys
@@ -44,6 +48,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
+    p.add_argument("--serve-requests", type=int, default=2000,
+                   help="requests of the serving stream measured after the main workload (0: skip)")
     return p.parse_args()
 
 
@@ -154,6 +160,82 @@ class Clocks:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------------- serving stream
+def serving_run(n_requests, dev, pair_density, seed=0, load=0.6):
+    """Poisson stream of boundary queries over 32 resident scenes of the large 2-D kind (64 star polygons each,
+    h = 0.02), particle counts log-uniform in [1e3, 1e6] (positions uniform in [0, 4]^2, produced on the device at
+    arrival), kernels uniform in {w2, w4, w6}, 25 % of the requests with the adjoint.  The arrival rate is `load` times
+    the capacity measured on a saturating run.  Returns p50 / p99 latency and rates."""
+    import torch
+    from warpsphboundaries_b200 import workloads
+    from warpsphboundaries_b200.scene import Body, Scene, SurfaceRep
+    from warpsphboundaries_b200.serve import BoundaryServer
+    h = 0.02
+    rng = np.random.default_rng(seed + 77)
+    scenes = {f"scene{k}": Scene([Body(reps=[SurfaceRep.loops(workloads.stars(64, (32, 512), seed=100 + k))])], dev)
+              for k in range(32)}
+    srv = BoundaryServer(dev, streams=4)
+    for sid, sc in scenes.items():
+        srv.register(sid, sc, h)
+    specs = [(f"scene{rng.integers(0, 32)}", int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))),
+              ["w2", "w4", "w6"][rng.integers(0, 3)], bool(rng.uniform() < 0.25)) for _ in range(n_requests)]
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    # the clients' particle positions: slices of a resident ring of positions (a simulation's state is resident)
+    ring = torch.rand((1 << 22, 2), dtype=torch.float64, device=dev, generator=gen) * 4.0
+    cursor = [0]
+
+    def make(rows):
+        start = cursor[0] if cursor[0] + rows <= len(ring) else 0
+        cursor[0] = start + rows
+        return ring[start:start + rows]
+
+    # saturation probes (every request submitted as soon as the previous submit returns, polling in between, as in the
+    # stream): the first warms graphs and workspaces, the second measures the sustainable capacity in rows/s
+    burst = specs[: min(300, n_requests)]
+    for rep in range(2):
+        t0 = time.perf_counter()
+        for sid, rows, k, g in burst:
+            srv.submit(sid, make(rows), h, k, grad=g)
+            srv.poll()
+        srv.run()
+        torch.cuda.synchronize()
+        cap_rows = sum(r for _, r, _, _ in burst) / (time.perf_counter() - t0)
+        for r in list(srv.completed):
+            srv.release(r.rid)
+        srv.completed.clear()
+    mean_rows = float(np.mean([r for _, r, _, _ in specs]))
+    rate = load * cap_rows / mean_rows                         # requests per second
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    for r in list(srv.completed):
+        srv.release(r.rid)
+    srv.completed.clear()
+    srv.t_first = srv.t_last = None
+    start = time.perf_counter()
+    i = 0
+    released = [0]
+    while i < n_requests or srv.poll():
+        now = time.perf_counter() - start
+        while i < n_requests and arrivals[i] <= now:
+            sid, rows, k, g = specs[i]
+            srv.submit(sid, make(rows), h, k, grad=g, arrival=start + arrivals[i])
+            i += 1
+        srv.poll()
+        while released[0] < len(srv.completed):               # the clients take their results and free them
+            srv.release(srv.completed[released[0]].rid)
+            released[0] += 1
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - start
+    st = srv.stats()
+    rows_total = sum(r for _, r, _, _ in specs)
+    return {"requests": n_requests, "scenes": 32, "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
+            "mean_ms": st.get("mean_ms"), "arrival_rate_per_s": rate, "wall_s": wall,
+            "rows_per_s": rows_total / wall, "pairs_per_s_est": rows_total * pair_density / wall,
+            "capacity_rows_per_s": cap_rows, "offered_load": load,
+            "note": "pairs estimated from the mean neighbour-pair density of the 2^20-particle scene; all 32 scenes "
+                    "2-D (the 3-D mesh scenes of the serving mix are not built)"}
 
 
 # ----------------------------------------------------------------------------------------------- our arm
@@ -339,6 +421,10 @@ def our_arm(args):
                "h2d_bytes_per_step": N * 3 * 8, "d2h_bytes_per_step": len(KERNELS) * N * 7 * 8,
                "ms_per_step": float(t.item()) / args.steps}
 
+    serving = None
+    if rank == 0 and world == 1 and args.serve_requests > 0:
+        serving = serving_run(args.serve_requests, dev, P / N)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, procs, sample = cpu_reference(loops, X, h, seconds=12.0, procs=1)
@@ -361,7 +447,8 @@ def our_arm(args):
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
                 "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
                 "gpu_launches": args.steps * (4 + 2 * len(KERNELS)),
-                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, **({"extra": extra} if extra else {})}
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving,
+                **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -2,9 +2,6 @@
 // body-frame position, runs the float64 neighbour predicate over the row's cell and accumulates the closed-form
 // channels of every neighbour pair in registers, then adds the indicator, scales and rotates.  Also the adjoint of the
 // moments, signed distance and rigid-body kinematics.
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
-
 #include <cstdlib>
 #include <mutex>
 
@@ -13,40 +10,26 @@
 namespace wsb {
 
 constexpr int kThreads = 128;
+constexpr int kKeys = 65;          // count keys: 0..63 rows with pairs (63 - min(pairs, 63)), 64 rows without
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Workspace {
   int32_t* key;      // [n] bucket of a row: cell id, ncells = outside the grid, ncells + 1 = not a candidate
   double* lpos;      // [2n] body-frame positions
-  int32_t* counts;   // [nbk + 1]
+  int32_t* counts;   // [nbk + 1]   } zeroed together
+  int32_t* cursor;   // [nbk]       }
   int32_t* offs;     // [nbk + 1] exclusive prefix sums of counts
-  int32_t* cursor;   // [nbk]
   int32_t* order;    // [n] rows sorted by bucket
   double* ind;       // [n] indicator of a row (by row index)
   int32_t* flag;     // [n] 0 not a candidate, 1 candidate without neighbour pairs, 2 row with pairs (by row index)
-  int32_t* rkey;     // [n] radix key of a sorted row: 63 - min(pairs, 63) for rows with pairs, 64 otherwise
-  int32_t* rkey2;    // [n] sorted keys (unused after the sort)
-  int32_t* rval;     // [n] the sorted row index j
-  int32_t* work;     // [n] rows with pairs first, by decreasing pair count (stable: cell order within a count)
+  int32_t* rkey;     // [n] count key of a sorted row: 63 - min(pairs, 63) for rows with pairs, 64 otherwise
+  int32_t* khist;    // [kKeys] rows per key   } zeroed together
+  int32_t* kcur;     // [kKeys] fill cursors   }
+  int32_t* work;     // [n] rows with pairs first, by decreasing pair count
   int32_t* nwork;    // [1] number of rows with pairs
-  void* cub_tmp;
-  size_t cub_bytes;
   size_t total;
 };
-
-static size_t cub_scan_bytes(int64_t items) {
-  size_t bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, bytes, (int32_t*)nullptr, (int32_t*)nullptr, (int)items);
-  return bytes;
-}
-
-static size_t cub_sort_bytes(int64_t items) {
-  size_t bytes = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const int32_t*)nullptr, (int32_t*)nullptr, (const int32_t*)nullptr,
-                                  (int32_t*)nullptr, (int)std::max<int64_t>(items, 1), 0, 7);
-  return bytes;
-}
 
 static Workspace carve(const Surface* s, int64_t n, void* base) {
   Workspace w{};
@@ -59,19 +42,17 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
   };
   w.key = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
   w.lpos = (double*)take(sizeof(double) * 2 * std::max<int64_t>(n, 1));
-  w.counts = (int32_t*)take(sizeof(int32_t) * (nbk + 1));
+  w.counts = (int32_t*)take(sizeof(int32_t) * (2 * nbk + 1));
+  w.cursor = w.counts + nbk + 1;
   w.offs = (int32_t*)take(sizeof(int32_t) * (nbk + 1));
-  w.cursor = (int32_t*)take(sizeof(int32_t) * nbk);
   w.order = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
   w.ind = (double*)take(sizeof(double) * std::max<int64_t>(n, 1));
   w.flag = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
   w.rkey = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
-  w.rkey2 = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
-  w.rval = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.khist = (int32_t*)take(sizeof(int32_t) * 2 * kKeys);
+  w.kcur = w.khist + kKeys;
   w.work = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
   w.nwork = (int32_t*)take(sizeof(int32_t));
-  w.cub_bytes = std::max(cub_scan_bytes(nbk + 1), cub_sort_bytes(n));
-  w.cub_tmp = take(w.cub_bytes);
   w.total = off;
   return w;
 }
@@ -118,8 +99,7 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
 __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const int32_t* __restrict__ key,
                               const double* __restrict__ lpos, const int32_t* __restrict__ offs,
                               const int32_t* __restrict__ order, int64_t n, double* __restrict__ ind,
-                              int32_t* __restrict__ flag, int32_t* __restrict__ rkey, int32_t* __restrict__ rval,
-                              int32_t* __restrict__ nwork) {
+                              int32_t* __restrict__ flag, int32_t* __restrict__ rkey, int32_t* __restrict__ khist) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int cnt = 0;
   if (j < n) {
@@ -150,11 +130,12 @@ __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const 
       ind[i] = w;
       flag[i] = cnt > 0 ? 2 : 1;
     }
-    rkey[j] = cnt > 0 ? 63 - min(cnt, 63) : 64;
-    rval[j] = (int32_t)j;
+    rkey[j] = cnt > 0 ? 63 - min(cnt, 63) : kKeys - 1;
   }
-  const unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
-  if ((threadIdx.x & 31) == 0 && m) atomicAdd(nwork, __popc(m));
+  // warp-aggregated histogram of the keys
+  const int ckey = j < n ? (cnt > 0 ? 63 - min(cnt, 63) : kKeys - 1) : -1;
+  const unsigned peers = __match_any_sync(0xffffffffu, ckey);
+  if (ckey >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&khist[ckey], __popc(peers));
 }
 
 __device__ __forceinline__ void finish_row(double acc[12], double ind, double mass, double plane2, double h,
@@ -452,27 +433,76 @@ __global__ void k_kinematics(const double* __restrict__ bodies, int32_t nb, cons
   }
 }
 
+// exclusive prefix sums of m counts in one block: each thread scans a contiguous chunk, the chunk totals are
+// scanned across the block (the bucket counts of the row sort: one cell grid's worth of entries)
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) k_scan_block(const int32_t* __restrict__ in, int32_t* __restrict__ out,
+                                                            int64_t m) {
+  __shared__ int32_t s_tot[kScanThreads];
+  const int t = threadIdx.x;
+  const int64_t chunk = (m + kScanThreads - 1) / kScanThreads;
+  const int64_t a = min((int64_t)t * chunk, m), b = min(a + chunk, m);
+  int32_t sum = 0;
+  for (int64_t i = a; i < b; ++i) sum += in[i];
+  s_tot[t] = sum;
+  __syncthreads();
+  for (int d = 1; d < kScanThreads; d <<= 1) {       // inclusive Hillis-Steele scan of the chunk totals
+    const int32_t v = t >= d ? s_tot[t - d] : 0;
+    __syncthreads();
+    s_tot[t] += v;
+    __syncthreads();
+  }
+  int32_t run = t ? s_tot[t - 1] : 0;
+  for (int64_t i = a; i < b; ++i) {
+    const int32_t v = in[i];
+    out[i] = run;
+    run += v;
+  }
+}
+
+// rows with pairs into `work`, grouped by count key (decreasing pair count): the prefix of the key histogram per
+// block, then warp-aggregated cursor atomics (the order inside a key group is arbitrary; every row's result is
+// independent of it)
+__global__ void k_key_scatter(const int32_t* __restrict__ rkey, int64_t n, const int32_t* __restrict__ khist,
+                              int32_t* __restrict__ kcur, int32_t* __restrict__ work, int32_t* __restrict__ nwork) {
+  __shared__ int32_t s_pre[kKeys + 1];
+  if (threadIdx.x == 0) {
+    int32_t run = 0;
+    for (int k = 0; k < kKeys; ++k) {
+      s_pre[k] = run;
+      run += khist[k];
+    }
+    s_pre[kKeys] = run;
+    if (blockIdx.x == 0) *nwork = s_pre[kKeys - 1];          // rows with key < 64
+  }
+  __syncthreads();
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int key = j < n ? rkey[j] : -1;
+  const bool mine = key >= 0 && key < kKeys - 1;
+  const unsigned peers = __match_any_sync(0xffffffffu, mine ? key : -1);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (mine && lane == leader) base = atomicAdd(&kcur[key], __popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (mine) work[s_pre[key] + base + __popc(peers & ((1u << lane) - 1))] = (int32_t)j;
+}
+
 // shared front half of the aggregate and its adjoint: body frame, broadphase, counting sort of the rows by cell
 static int sort_rows(const Surface* s, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
                      const double* pose, const double* obb, int unbounded, const Workspace& w, cudaStream_t st) {
   const int64_t nbk = (int64_t)s->nx * s->ny + 2;
-  WSB_CUDA(cudaMemsetAsync(w.counts, 0, sizeof(int32_t) * (nbk + 1), st));
-  WSB_CUDA(cudaMemsetAsync(w.cursor, 0, sizeof(int32_t) * nbk, st));
+  WSB_CUDA(cudaMemsetAsync(w.counts, 0, sizeof(int32_t) * (2 * nbk + 1), st));
+  WSB_CUDA(cudaMemsetAsync(w.khist, 0, sizeof(int32_t) * 2 * kKeys, st));
   const SurfView v = view_of(s);
   const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
   k_agg_prep<<<grid, kThreads, 0, st>>>(v, pos, sup, allowed, n, pose, make_double4(obb[0], obb[1], obb[2], obb[3]),
                                         unbounded, w.key, w.lpos, w.counts);
-  WSB_CUDA(cudaGetLastError());
-  size_t bytes = w.cub_bytes;
-  WSB_CUDA(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.counts, w.offs, (int)(nbk + 1), st));
+  k_scan_block<<<1, kScanThreads, 0, st>>>(w.counts, w.offs, nbk + 1);
   k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
+  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.khist);
+  k_key_scatter<<<grid, kThreads, 0, st>>>(w.rkey, n, w.khist, w.kcur, w.work, w.nwork);
   WSB_CUDA(cudaGetLastError());
-  WSB_CUDA(cudaMemsetAsync(w.nwork, 0, sizeof(int32_t), st));
-  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.rval,
-                                           w.nwork);
-  WSB_CUDA(cudaGetLastError());
-  bytes = w.cub_bytes;
-  WSB_CUDA(cub::DeviceRadixSort::SortPairs(w.cub_tmp, bytes, w.rkey, w.rkey2, w.rval, w.work, (int)n, 0, 7, st));
   return WSB_OK;
 }
 

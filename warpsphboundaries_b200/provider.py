@@ -70,13 +70,15 @@ class FusedWall(WallAggregate):
     """all twelve channels of every (body, surface) at one position set, per kernel group, world frame, float64:
     lam [B, N], G [B, N, 2], Cov [B, N, 2, 2], m1 [B, N, 2], m2 [B, N, 2, 2]."""
 
-    def __init__(self, scene, ps, support, groups, route="fused", precision="fp64", allowed=None):
+    def __init__(self, scene, ps, support, groups, route="fused", precision="fp64", allowed=None, workspaces=None,
+                 outs=None):
         self.scene = scene
         self.groups = tuple(groups)
         self.dev = scene.device
         self.route = route
         self.precision = precision
         self.support = float(support)
+        self.workspaces = workspaces           # optional {id(rep): uint8 tensor}: caller-owned workspaces (graphs)
         pos = ps.positions.to(self.dev, F64).contiguous()
         sup = ps.supports.to(self.dev, F64).contiguous()
         self.N = N = len(pos)
@@ -85,21 +87,30 @@ class FusedWall(WallAggregate):
             if g.kernel not in KERNEL_IDS:
                 raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} (wall-operator layout: cover / "
                                           f"Laplacian / tensile) is not built; use the lean layout")
-        for b in scene.bodies:
-            for r in b.reps:
-                if not isinstance(r, SurfaceRep):
-                    raise NotImplementedError(f"FusedWall: {type(r).__name__} is not built (surface loops only)")
-                if r._triangle:
-                    raise NotImplementedError("FusedWall: a conditioned single-triangle SurfaceRep takes the sliver "
-                                              "quadrature, which is not built; use SurfaceRep(..., conditioned=False)")
+        sig = tuple(id(r) for b in scene.bodies for r in b.reps)
+        if getattr(scene, "_wsb_checked", None) != sig:
+            for b in scene.bodies:
+                for r in b.reps:
+                    if not isinstance(r, SurfaceRep):
+                        raise NotImplementedError(f"FusedWall: {type(r).__name__} is not built (surface loops only)")
+                    if r._triangle:
+                        raise NotImplementedError("FusedWall: a conditioned single-triangle SurfaceRep takes the sliver "
+                                                  "quadrature, which is not built; use SurfaceRep(..., "
+                                                  "conditioned=False)")
+            scene._wsb_checked = sig
         self.res = []
         alloc = torch.empty if route == "fused" else torch.zeros     # the fused route assigns every row of a body
+        if outs is not None and (route != "fused" or len(self.groups) != 1):
+            raise ValueError("FusedWall: caller-owned outputs serve the fused route with one kernel group")
         for g in self.groups:
-            out = {"lam": alloc((B, N), dtype=F64, device=self.dev),
-                   "G": alloc((B, N, 2), dtype=F64, device=self.dev),
-                   "Cov": alloc((B, N, 2, 2), dtype=F64, device=self.dev),
-                   "m1": alloc((B, N, 2), dtype=F64, device=self.dev),
-                   "m2": alloc((B, N, 2, 2), dtype=F64, device=self.dev)}
+            if outs is not None:
+                out = outs                                             # caller-owned [B, N, ...] float64 buffers
+            else:
+                out = {"lam": alloc((B, N), dtype=F64, device=self.dev),
+                       "G": alloc((B, N, 2), dtype=F64, device=self.dev),
+                       "Cov": alloc((B, N, 2, 2), dtype=F64, device=self.dev),
+                       "m1": alloc((B, N, 2), dtype=F64, device=self.dev),
+                       "m2": alloc((B, N, 2, 2), dtype=F64, device=self.dev)}
             kid = KERNEL_IDS[g.kernel]
             if route == "fused":
                 self._fused(pos, sup, allowed, kid, out)
@@ -122,7 +133,11 @@ class FusedWall(WallAggregate):
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
             for ri, rep in enumerate(body.reps):
                 ns = rep.native(self.support, self.dev)
-                ws, need = ns.workspace(N)
+                if self.workspaces is not None:
+                    ws = self.workspaces[id(rep)]
+                    need = ws.numel()
+                else:
+                    ws, need = ns.workspace(N)
                 mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)     # the first surface of a body assigns
                 check(lib.wsb_aggregate(ns.handle, kid, _PREC[self.precision], ptr(pos), ptr(sup), ptr(al), N,
                                         ptr(pose), obb, int(body.unbounded()), mode, ptr(out["lam"][bi]),

@@ -76,12 +76,15 @@ class NativeSurface:
         self._ws = {}
 
     def workspace(self, n):
-        """cached workspace tensor for n rows (the library allocates nothing per call)."""
+        """the workspace for n rows on the current stream: one buffer per stream, grown geometrically and reused for
+        any smaller row count (the library carves it per call and allocates nothing itself)."""
         need = int(lib.wsb_aggregate_workspace_size(self.handle, int(n)))
-        ws = self._ws.get(n)
+        key = torch.cuda.current_stream(self.device).cuda_stream
+        ws = self._ws.get(key)
         if ws is None or ws.numel() < need:
-            ws = torch.empty(max(need, 1), dtype=torch.uint8, device=self.device)
-            self._ws[n] = ws
+            ws = torch.empty(max(need, int(1.5 * ws.numel()) if ws is not None else need, 1), dtype=torch.uint8,
+                             device=self.device)
+            self._ws[key] = ws
         return ws, need
 
     def cells(self):

@@ -1,0 +1,400 @@
+"""Continuous-batching request loop for boundary queries from many simulations.
+
+    srv = BoundaryServer(device="cuda:0")
+    srv.register("tank-3", scene, support=0.02)                 # geometry, cell grid, indicator cache resident
+    rid = srv.submit("tank-3", positions, supports, "w4", grad=False)    # positions / supports: device tensors
+    srv.run()                                                    # or srv.poll() from the caller's own loop
+    res = srv.result(rid)        # {"lam": [B, n], "G": [B, n, 2], "Cov": [B, n, 2, 2], "m1": [B, n, 2], "m2": [B, n, 2, 2]
+                                 #  (+ "d_pos": [n, 2] with grad=True: the adjoint of sum(lam))}
+
+Scheduling (one host thread, the caller's):
+* requests queue per (scene, kernel, grad); a batch takes the oldest requests of one queue up to `max_batch_rows`
+  rows and is admitted while the device memory it reserves (inputs, outputs, workspace) fits `hbm_budget`;
+* a batch is ONE fused launch family over the concatenated rows of its requests.  Rows are independent (each row's
+  pairs are summed in its own fixed order), so a request's result is bit-identical alone and in any mix;
+* batches run on `streams` CUDA streams at once, so requests that arrive while others are on the GPU are admitted as
+  stream slots and memory free up, and their work overlaps on the device;
+* batches of at most `graph_max_rows` rows replay a CUDA graph captured per (stream, bucket, scene, kernel) over
+  static buffers padded to a power-of-two bucket (padding rows are masked out), removing launch overhead for small
+  requests; a key is captured once it has been launched `graph_after_uses` times, so one-off keys stay eager;
+* nothing is allocated per batch: a request's outputs are allocated when it is submitted (on the caller's stream),
+  a single-request batch writes straight into them, a multi-request batch into persistent per-stream buffers that are
+  then copied into each request's outputs;
+* admission: a batch is launched while the device memory it reserves fits `hbm_budget`, and `submit` blocks (it
+  keeps polling) while the outputs of queued and in-flight requests would exceed it -- back-pressure instead of an
+  unbounded queue;
+* latency of a request = completion (its batch's end event observed) - arrival; `stats()` reports p50 / p99.
+"""
+import itertools
+import time
+from dataclasses import dataclass
+from typing import Dict, List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr
+from .kernels import KERNEL_IDS
+from .provider import FusedGroup, FusedWall
+from .scene import SurfaceRep
+from .shim import ParticleState, kernelName
+
+F64 = torch.float64
+OUT_KEYS = ("lam", "G", "Cov", "m1", "m2")
+_TAIL = {"lam": (), "G": (2,), "Cov": (2, 2), "m1": (2,), "m2": (2, 2)}
+
+
+@dataclass
+class Request:
+    rid: int
+    scene_id: str
+    kernel: str
+    pos: torch.Tensor
+    sup: torch.Tensor
+    grad: bool
+    arrival: float
+    result: Optional[dict] = None
+    done: Optional[float] = None
+    flat: Optional[torch.Tensor] = None
+    nbytes: int = 0
+
+
+@dataclass
+class _Batch:
+    reqs: List[Request]
+    rows: int
+    reserved: int
+    event: torch.cuda.Event
+
+
+class _Slot:
+    """one stream, its persistent batch buffers and its static graph buffers."""
+
+    def __init__(self, device):
+        self.device = device
+        self.stream = torch.cuda.Stream(device=device)
+        self.busy = None
+        self.static = {}              # bucket -> (pos, sup, allowed)
+        self.cap = 0
+        self.B = 0
+        self.buf = None
+
+    def workspace(self, nbytes):
+        """the persistent workspace of this stream (one batch at a time uses it)."""
+        if getattr(self, "ws", None) is None or self.ws.numel() < nbytes:
+            with torch.cuda.stream(self.stream):
+                self.ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
+        return self.ws
+
+    def buffers(self, rows, B):
+        """persistent batch buffers for `rows` rows of a B-body scene (grown geometrically, allocated on this stream)."""
+        if self.buf is None or rows > self.cap or B > self.B:
+            cap = max(rows, int(1.5 * self.cap), 1 << 16)
+            self.B = max(B, self.B)
+            with torch.cuda.stream(self.stream):
+                self.buf = {"pos": torch.empty((cap, 2), dtype=F64, device=self.device),
+                            "sup": torch.empty(cap, dtype=F64, device=self.device),
+                            "one": torch.ones(cap, dtype=F64, device=self.device),
+                            **{k: torch.empty((self.B, cap) + _TAIL[k], dtype=F64, device=self.device)
+                               for k in OUT_KEYS}}
+            self.cap = cap
+        return self.buf
+
+
+class BoundaryServer:
+    def __init__(self, device="cuda:0", streams=4, max_batch_rows=1 << 20, hbm_budget=None, use_graphs=True,
+                 graph_max_rows=1 << 16, precision="fp64", graph_after_uses=4, pool_limit=None):
+        self.device = torch.device(device)
+        self.scenes: Dict[str, tuple] = {}
+        self.queues: Dict[tuple, List[Request]] = {}
+        self.slots = [_Slot(self.device) for _ in range(streams)]
+        self.max_batch_rows = int(max_batch_rows)
+        free, total = torch.cuda.mem_get_info(self.device)
+        self.hbm_budget = int(hbm_budget if hbm_budget is not None else 0.25 * free)
+        self.reserved = 0
+        self.use_graphs = use_graphs
+        self.graph_max_rows = int(graph_max_rows)
+        self.graph_after_uses = int(graph_after_uses)
+        self.precision = precision
+        self.graphs = {}
+        self.uses = {}
+        self.requests: Dict[int, Request] = {}
+        self._ids = itertools.count()
+        self.completed: List[Request] = []
+        self.n_queued = 0
+        self.n_inflight = 0
+        self.t_first = None
+        self.t_last = None
+        self.plans = {}
+        self.ws_bytes = 0
+        self.pool = {}                      # size class -> free output buffers
+        self.pooled_bytes = 0
+        self.pool_limit = int(pool_limit if pool_limit is not None else 0.1 * free)
+        self.held_bytes = 0                 # outputs of queued and in-flight requests
+
+    # ------------------------------------------------------------------ scenes
+    def register(self, scene_id, scene, support):
+        """keep `scene` resident: its surfaces' static structures are built now for `support`, with the launch plan
+        (pose, body box, surface handles) resolved once."""
+        for b in scene.bodies:
+            for r in b.reps:
+                if not isinstance(r, SurfaceRep) or r._triangle:
+                    raise NotImplementedError("BoundaryServer: surface loops only (no conditioned single triangles)")
+        plan = []
+        for b in scene.bodies:
+            reps = [r.native(float(support), self.device) for r in b.reps]
+            plan.append((b.pose_tensor(self.device), (_lib.ctypes.c_double * 4)(*b.obb()), int(b.unbounded()), reps))
+            for ns in reps:
+                self.ws_bytes = max(self.ws_bytes, int(lib.wsb_aggregate_workspace_size(ns.handle, self.max_batch_rows)))
+        self.scenes[scene_id] = (scene, float(support))
+        self.plans[scene_id] = plan
+
+    # ------------------------------------------------------------------ requests
+    def submit(self, scene_id, positions, supports, kernel, grad=False, arrival=None):
+        """queue a request; its outputs are allocated here, on the caller's stream."""
+        if scene_id not in self.scenes:
+            raise KeyError(f"unknown scene {scene_id!r}")
+        kname = kernelName(kernel)
+        pos = positions.to(self.device, F64).contiguous()
+        sup = supports if torch.is_tensor(supports) else torch.full((len(pos),), float(supports), dtype=F64,
+                                                                      device=self.device)
+        sup = sup.to(self.device, F64).contiguous()
+        r = Request(next(self._ids), scene_id, kname, pos, sup, bool(grad),
+                    time.perf_counter() if arrival is None else arrival)
+        B, n = len(self.scenes[scene_id][0].bodies), len(pos)
+        nbytes = 8 * (13 * B * n + (2 * n if r.grad else 0))
+        # back-pressure: a full server makes the caller wait (polling) instead of queueing without bound
+        while self.held_bytes + nbytes > self.hbm_budget and (self.n_queued or self.n_inflight):
+            self.poll()
+        self.held_bytes += nbytes
+        r.nbytes = nbytes
+        flat = self._take(13 * B * n + (2 * n if r.grad else 0))          # one buffer, from the pool when possible
+        r.flat = flat
+        r.result, off = {}, 0
+        for k in OUT_KEYS:
+            size = B * n * int(np.prod(_TAIL[k], dtype=np.int64))
+            r.result[k] = flat[off:off + size].view((B, n) + _TAIL[k])
+            off += size
+        if r.grad:
+            r.result["d_pos"] = flat[off:off + 2 * n].view(n, 2)
+            r.result["d_pos"].zero_()
+        self.requests[r.rid] = r
+        self.queues.setdefault((scene_id, kname, r.grad), []).append(r)
+        self.n_queued += 1
+        return r.rid
+
+    def result(self, rid):
+        """the outputs of a request (owned by the request; complete once `poll` has retired its batch)."""
+        return self.requests[rid].result
+
+    def release(self, rid):
+        """hand a finished request's output buffer back to the pool (its result tensors must not be used after)."""
+        r = self.requests.pop(rid)
+        if r.done is None:
+            raise ValueError("release: the request has not completed")
+        flat = getattr(r, "flat", None)
+        if flat is not None and self.pooled_bytes + 8 * flat.numel() <= self.pool_limit:
+            self.pool.setdefault(flat.numel(), []).append(flat)
+            self.pooled_bytes += 8 * flat.numel()
+        r.result = None
+        r.flat = None
+
+    def _take(self, n):
+        """a float64 buffer of at least n elements: pooled size classes (powers of two) avoid allocator calls in the
+        steady state."""
+        cls = max(1 << 12, 1 << (int(n) - 1).bit_length())
+        lst = self.pool.get(cls)
+        if lst:
+            self.pooled_bytes -= 8 * cls
+            return lst.pop()
+        return torch.empty(cls, dtype=F64, device=self.device)
+
+    # ------------------------------------------------------------------ bytes a batch holds on the device
+    def _bytes(self, scene, support, rows, grad):
+        B = len(scene.bodies)
+        ws = 0
+        for b in scene.bodies:
+            for r in b.reps:
+                ws = max(ws, int(lib.wsb_aggregate_workspace_size(r.native(support, self.device).handle, rows)))
+        return (8 * 13 * B + 24 + (16 if grad else 0)) * rows + ws
+
+    # ------------------------------------------------------------------ the loop
+    def _next_batch(self):
+        """the queue whose oldest request arrived first; its oldest requests up to max_batch_rows rows."""
+        best = None
+        for key, q in self.queues.items():
+            if q and (best is None or q[0].arrival < self.queues[best][0].arrival):
+                best = key
+        if best is None:
+            return None
+        q = self.queues[best]
+        take, rows = [], 0
+        while q and (not take or rows + len(q[0].pos) <= self.max_batch_rows):
+            r = q.pop(0)
+            take.append(r)
+            rows += len(r.pos)
+        self.n_queued -= len(take)
+        return take, rows
+
+    def poll(self):
+        """retire finished batches, then launch queued work while stream slots and memory allow.  Returns the number
+        of requests still queued plus batches in flight."""
+        for s in self.slots:
+            b = s.busy
+            if b is not None and b.event.query():
+                # the caller's stream owns the requests' tensors: order it after this batch so their memory is only
+                # reused once the batch is done (the event has completed: this wait costs nothing)
+                torch.cuda.current_stream(self.device).wait_event(b.event)
+                t = time.perf_counter()
+                for r in b.reqs:
+                    r.done = t
+                    self.completed.append(r)
+                    self.held_bytes -= r.nbytes
+                self.reserved -= b.reserved
+                s.busy = None
+                self.n_inflight -= 1
+                self.t_last = t
+        while self.n_queued:
+            si = next((i for i, s in enumerate(self.slots) if s.busy is None), None)
+            if si is None:
+                break
+            reqs, rows = self._next_batch()
+            scene, support = self.scenes[reqs[0].scene_id]
+            need = self._bytes(scene, support, rows, reqs[0].grad)
+            if self.reserved and self.reserved + need > self.hbm_budget:
+                q = self.queues[(reqs[0].scene_id, reqs[0].kernel, reqs[0].grad)]
+                q[:0] = reqs                        # not admitted yet: back to the head of its queue
+                self.n_queued += len(reqs)
+                break
+            self.reserved += need
+            self._launch(si, reqs, rows, scene, support, need)
+            self.n_inflight += 1
+        return self.n_queued + self.n_inflight
+
+    def run(self):
+        while self.poll():
+            time.sleep(0)
+
+    # ------------------------------------------------------------------ launches
+    def _launch(self, si, reqs, rows, scene, support, need):
+        slot = self.slots[si]
+        kname, grad = reqs[0].kernel, reqs[0].grad
+        B = len(scene.bodies)
+        plan = self.plans[reqs[0].scene_id]
+        if self.t_first is None:
+            self.t_first = time.perf_counter()
+        slot.stream.wait_stream(torch.cuda.current_stream(self.device))   # inputs and outputs come from the caller
+        with torch.cuda.stream(slot.stream):
+            single = len(reqs) == 1
+            if single:
+                pos, sup, outs = reqs[0].pos, reqs[0].sup, reqs[0].result
+            else:
+                buf = slot.buffers(rows, B)
+                pos, sup = buf["pos"][:rows], buf["sup"][:rows]
+                off = 0
+                for r in reqs:
+                    n = len(r.pos)
+                    pos[off:off + n].copy_(r.pos)
+                    sup[off:off + n].copy_(r.sup)
+                    off += n
+                outs = {k: buf[k][:B, :rows] for k in OUT_KEYS}
+            gkey = None
+            if self.use_graphs and not grad and rows <= self.graph_max_rows:
+                gkey = (si, self._bucket(rows), reqs[0].scene_id, kname)
+                self.uses[gkey] = self.uses.get(gkey, 0) + 1
+                if gkey not in self.graphs and self.uses[gkey] < self.graph_after_uses:
+                    gkey = None
+            if gkey is not None:
+                self._graph_run(slot, gkey, plan, support, kname, pos, sup, rows, outs)
+            else:
+                self._aggregate(plan, kname, pos, sup, None, rows, outs, slot.workspace(self.ws_bytes),
+                                slot.stream)
+            if grad:
+                d_pos = reqs[0].result["d_pos"] if single else torch.zeros((rows, 2), dtype=F64, device=self.device)
+                self._adjoint(plan, support, kname, pos, sup, d_pos, slot)
+            if not single:
+                off = 0
+                for r in reqs:
+                    n = len(r.pos)
+                    for k in OUT_KEYS:
+                        r.result[k].copy_(outs[k][:, off:off + n])
+                    if grad:
+                        r.result["d_pos"].copy_(d_pos[off:off + n])
+                    off += n
+            ev = torch.cuda.Event()
+            ev.record(slot.stream)
+        slot.busy = _Batch(reqs, rows, need, ev)
+
+    def _aggregate(self, plan, kname, pos, sup, allowed, n, outs, ws, stream):
+        """the fused aggregate of every body and surface of a resolved scene into `outs` (the first surface of a body
+        assigns its rows, the others add)."""
+        kid = KERNEL_IDS[kname]
+        prec = _lib.PREC_MIXED if self.precision == "mixed" else _lib.PREC_FP64
+        st = _lib.ctypes.c_void_p(stream.cuda_stream)
+        for bi, (pose, obb, unbounded, reps) in enumerate(plan):
+            o = [ptr(outs[k][bi]) for k in OUT_KEYS]
+            for ri, ns in enumerate(reps):
+                mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)
+                check(lib.wsb_aggregate(ns.handle, kid, prec, ptr(pos), ptr(sup), ptr(allowed), n, ptr(pose), obb,
+                                        unbounded, mode, *o, ptr(ws), ws.numel(), None, st), "wsb_aggregate")
+
+    def _adjoint(self, plan, support, kname, pos, sup, d_pos, slot):
+        """adds d(sum lam)/dpos of every body and surface into d_pos (the gradient-flagged requests)."""
+        N = len(pos)
+        g_lam = slot.buffers(N, len(plan))["one"][:N]
+        ws = slot.workspace(self.ws_bytes)
+        kid = KERNEL_IDS[kname]
+        for pose, obb, unbounded, reps in plan:
+            for ns in reps:
+                check(lib.wsb_aggregate_backward(ns.handle, kid, ptr(pos), ptr(sup), None, N, ptr(pose), obb,
+                                                 unbounded, ptr(g_lam), None, None, ptr(d_pos), None, ptr(ws),
+                                                 ws.numel(), _lib.ctypes.c_void_p(slot.stream.cuda_stream)),
+                      "wsb_aggregate_backward")
+
+    @staticmethod
+    def _bucket(rows):
+        return max(1024, 1 << (int(rows) - 1).bit_length())
+
+    def _graph_run(self, slot, key, plan, support, kname, pos, sup, rows, outs):
+        bucket = key[1]
+        B = len(plan)
+        st = slot.static.get(bucket)
+        if st is None:
+            st = (torch.zeros((bucket, 2), dtype=F64, device=self.device),
+                  torch.full((bucket,), support, dtype=F64, device=self.device),
+                  torch.zeros(bucket, dtype=torch.int32, device=self.device))
+            slot.static[bucket] = st
+        spos, ssup, sall = st
+        g = self.graphs.get(key)
+        if g is None:
+            sall.fill_(1)
+            # graph-owned workspace and outputs: a captured graph keeps its pointers, so they are never freed
+            need = max(int(lib.wsb_aggregate_workspace_size(ns.handle, bucket)) for _, _, _, reps in plan for ns in reps)
+            ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+            gout = {k: torch.empty((B, bucket) + _TAIL[k], dtype=F64, device=self.device) for k in OUT_KEYS}
+            self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)     # eager warm-up
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=slot.stream):
+                self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)
+            g = (graph, gout, ws)
+            self.graphs[key] = g
+        graph, gout, _ = g
+        spos[:rows].copy_(pos)
+        ssup[:rows].copy_(sup)
+        sall[:rows].fill_(1)
+        sall[rows:].fill_(0)
+        graph.replay()
+        for k in OUT_KEYS:
+            outs[k].copy_(gout[k][:, :rows])
+
+    # ------------------------------------------------------------------ statistics
+    def stats(self):
+        lat = np.array([(r.done - r.arrival) * 1e3 for r in self.completed])
+        out = {"requests": len(self.completed)}
+        if len(lat):
+            out.update(p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
+                       mean_ms=float(lat.mean()), max_ms=float(lat.max()))
+        if self.t_first is not None and self.t_last is not None:
+            out["wall_s"] = self.t_last - self.t_first
+        return out
