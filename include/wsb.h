@@ -40,8 +40,12 @@ enum {
 /* arithmetic of the fused aggregate */
 enum {
   WSB_PREC_FP64 = 0,   /* every step in float64 */
-  WSB_PREC_MIXED = 1   /* float32 special functions where the per-pair error bound allows, float64 guards and sums */
+  WSB_PREC_MIXED = 1,  /* float32 special functions where the per-pair error bound allows, float64 guards and sums */
+  WSB_PREC_FP32 = 2    /* every step in float32 (wsb_radial_channels only) */
 };
+
+/* solid kinds of wsb_radial_channels */
+enum { WSB_RADIAL_PLANE = 0, WSB_RADIAL_SPHERE = 1 };
 
 /* output selection bits of wsb_aggregate */
 enum { WSB_OUT_LAM = 1, WSB_OUT_G = 2, WSB_OUT_COV = 4, WSB_OUT_M1 = 8, WSB_OUT_M2 = 16, WSB_OUT_ALL = 31,
@@ -155,6 +159,21 @@ int wsb_signed_distance(const wsb_surface* s, const double* lpos, int64_t m, dou
  * (src/warpSPHBoundaries/scene/scene.py:1155-1225) and Body.velocityAt / accelerationAt (scene.py:934-939, 1063-1067). */
 int wsb_kinematics(const double* bodies, int32_t n_bodies, const double* x, int64_t n, double* rel, double* local,
                    double* velocity, double* acceleration, void* stream);
+
+/* Solid half-space (kind WSB_RADIAL_PLANE) or solid sphere (WSB_RADIAL_SPHERE) in 3-D, one query per row: from the
+ * signed outward distance distances [n] (sphere: |x - c| - R, >= -R), radii [n] (sphere only; NULL for a plane), unit
+ * outward normals [n*3] and supports [n] (all device, float64), the nine axial invariants (lam, m1_axial, m2_tangent,
+ * m2_axial, G_axial, g1_tangent, g1_axial, H_tangent, H_axial) in physical units into invariants [n*9] (may be NULL)
+ * and the Cartesian channel of each request row (degree, i, j, order) of the host array requests [n_requests*4]
+ * (n_requests <= 28; the 28-row baseline lists value moments |alpha| <= 2, first kernel-derivative moments |alpha| <= 1
+ * and the symmetric kernel Hessian) into out [n*n_requests].  Kernels cubic, w2, w4, w6; precision WSB_PREC_FP64 or
+ * WSB_PREC_FP32.  Rows with invalid input (support <= 0, non-finite values, sphere radius <= 0 or distance < -radius)
+ * get NaN and status [n] = 1 (status may be NULL), others 0.  Replaces fluxbridge's RadialEvaluator batch, the native
+ * element and select (src/warpSPHBoundaries/fluxbridge/radial.py:20-71, 200-215;
+ * src/warpSPHBoundaries/fluxbridge/_radial_code.py:43-148). */
+int wsb_radial_channels(int kind, int kernel, int precision, const double* distances, const double* radii,
+                        const double* normals, const double* supports, int64_t n, const int32_t* requests,
+                        int n_requests, double* out, double* invariants, int32_t* status, void* stream);
 
 #ifdef __cplusplus
 }

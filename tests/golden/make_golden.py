@@ -13,6 +13,9 @@ Writes
                               (edge/np2d.py, whole polygon) for cubic, w2, w4, w6
   torch2d_grad.npz            gradients of lam and the moments with respect to particle positions and polygon
                               vertices from torch autograd through the reference's edge/torch2d.py (star polygon, w4)
+  radial_golden.json          solid half-spaces and spheres, 3-D: the nine radial invariants and the 28 baseline
+                              channels of the reference's 70-digit fixtures (tests/fixtures/fluxbridge-radial-v1.json,
+                              and the baseline requests of tests/fixtures/fluxbridge-sphere-v1.json)
 
 The reference package is imported with a stub parent package because its
 `__init__` needs the GPU stack (warp, warpSPHCore), which the CPU modules used
@@ -148,9 +151,34 @@ def torch2d_grads(torch2d, seed=0, n_pts=96):
     np.savez_compressed(HERE / "torch2d_grad.npz", polygon=P, particles=X, h=h, **res)
 
 
+def radial_golden(root):
+    fx = Path(root) / "tests" / "fixtures"
+    rad = json.loads((fx / "fluxbridge-radial-v1.json").read_text())
+    out = {"meta": {"source": "tests/fixtures/fluxbridge-radial-v1.json and fluxbridge-sphere-v1.json of the reference",
+                    "dps": rad["dps"], "support": "1 (distances and radii in units of the support)",
+                    "invariants": "lam, m1_axial, m2_tangent, m2_axial, G_axial, g1_tangent, g1_axial, H_tangent, "
+                                  "H_axial", "values": "the 28 baseline channels in request order"},
+           "radial": [], "sphere": []}
+    for c in rad["cases"]:
+        out["radial"].append({k: c[k] for k in ("kind", "kernel", "distance", "radius", "normal", "invariants",
+                                                "values")})
+    sph = json.loads((fx / "fluxbridge-sphere-v1.json").read_text())
+    for c in sph["cases"]:
+        vals = {}
+        for req, v in zip(c["requests"], c["values"]):
+            if sum(req["alpha"]) + len(req["derivative"]) <= 2 and (len(req["derivative"]) == 0 or
+                                                                   sum(req["alpha"]) + len(req["derivative"]) <= 2):
+                vals[json.dumps([req["alpha"], req["derivative"]])] = v
+        out["sphere"].append({"label": c["label"], "kernel": c["kernel"], "distance": c["distance"],
+                              "radius": c["radius"], "normal": c["normal"], "values": vals})
+    (HERE / "radial_golden.json").write_text(json.dumps(out, indent=1))
+    print("radial_golden.json:", len(out["radial"]), "radial cases,", len(out["sphere"]), "sphere cases")
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     np2d, torch2d = load_reference(root)
     golden_subset(root)
     np2d_c1(np2d)
     torch2d_grads(torch2d)
+    radial_golden(root)

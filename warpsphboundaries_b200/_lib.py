@@ -12,7 +12,8 @@ from pathlib import Path
 LIB_PATH = Path(os.environ.get("WSB_LIB", Path(__file__).resolve().parent / "_build" / "libwsb.so"))
 
 WSB_OK, WSB_ERR_ARG, WSB_ERR_CUDA, WSB_ERR_UNSUPPORTED, WSB_ERR_SIZE, WSB_ERR_DEVICE = 0, -1, -2, -3, -4, -5
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP32 = 0, 1, 2
+RADIAL_PLANE, RADIAL_SPHERE = 0, 1
 OUT_LAM, OUT_G, OUT_COV, OUT_M1, OUT_M2, OUT_ALL, OUT_ASSIGN = 1, 2, 4, 8, 16, 31, 32
 
 EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_destroy", "wsb_surface_info_get",
@@ -20,7 +21,7 @@ EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_d
            "wsb_aggregate_workspace_size", "wsb_aggregate", "wsb_aggregate_prepare", "wsb_aggregate_evaluate",
            "wsb_aggregate_noalloc",
            "wsb_aggregate_backward", "wsb_signed_distance",
-           "wsb_kinematics"]
+           "wsb_kinematics", "wsb_radial_channels"]
 
 
 class SurfaceInfo(ctypes.Structure):
@@ -56,6 +57,7 @@ def _load():
         "wsb_aggregate_backward": (c_int, [P, c_int, P, P, P, c_int64, P, D, c_int, P, P, P, P, P, P, c_size_t, P]),
         "wsb_signed_distance": (c_int, [P, P, c_int64, c_double, P, P, P, P, P]),
         "wsb_kinematics": (c_int, [P, c_int32, P, c_int64, P, P, P, P, P]),
+        "wsb_radial_channels": (c_int, [c_int, c_int, c_int, P, P, P, P, c_int64, I32P, c_int, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -533,4 +533,114 @@ static const int kPlanCn[kPlanCoeffs] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 
 static const double kPlanCc[kPlanCoeffs] = {5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05};
 static const double kPlanRadii[kPlanNumRadii] = {1.0, 0.5, 1.0, 1.0, 1.0, 1.0, 0.6, 0.2, 1.0, 0.6666666666666666, 0.3333333333333333, 1.0};
 
+// ---- 3-D radial family (solid half-space / sphere), unit support; W = c3*pi * shape, L = W'/r, dL = L'
+template <int K, typename T>
+__host__ __device__ __forceinline__ T ipow(T x) {
+  T y = x;
+#pragma unroll
+  for (int i = 1; i < K; ++i) y *= x;
+  return y;
+}
+__host__ __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+__host__ __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+constexpr int kRadialGauss = 12;
+static __device__ const double kRadialGx[kRadialGauss] = {-0.9815606342467192, -0.9041172563704748, -0.7699026741943047, -0.5873179542866175, -0.3678314989981802, -0.1252334085114689, 0.1252334085114689, 0.3678314989981802, 0.5873179542866175, 0.7699026741943047, 0.9041172563704748, 0.9815606342467192};
+static __device__ const double kRadialGw[kRadialGauss] = {0.04717533638651141, 0.10693932599531907, 0.16007832854334642, 0.20316742672306573, 0.2334925365383546, 0.2491470458134027, 0.2491470458134027, 0.2334925365383546, 0.20316742672306573, 0.16007832854334642, 0.10693932599531907, 0.04717533638651141};
+struct Rad_cubic {   // c3*pi = 16
+  static constexpr int kPieces = 2;
+  static constexpr double kLo[kPieces] = {0.0, 0.5};
+  static constexpr double kHi[kPieces] = {0.5, 1.0};
+  template <typename T> __host__ __device__ static __forceinline__ void full(T* v) {
+    v[0] = T(1.0); v[1] = T(0.0); v[2] = T(0.075); v[3] = T(0.075); v[4] = T(0.0); v[5] = T(1.0); v[6] = T(1.0); v[7] = T(0.0); v[8] = T(0.0);
+  }
+  template <int P, typename T> __host__ __device__ static __forceinline__ void eval(T r, T& w, T& l, T& dl);
+};
+template <> __host__ __device__ __forceinline__ void Rad_cubic::eval<0, double>(double r, double& w, double& l, double& dl) {
+  using T = double;
+  w = (fma_t((fma_t(T(48.0), r, T(-48.0)) * r), r, T(8.0)));
+  l = (fma_t(T(144.0), r, T(-96.0)));
+  dl = (T(144.0));
+}
+template <> __host__ __device__ __forceinline__ void Rad_cubic::eval<0, float>(float r, float& w, float& l, float& dl) {
+  using T = float;
+  w = (fma_t((fma_t(T(48.0), r, T(-48.0)) * r), r, T(8.0)));
+  l = (fma_t(T(144.0), r, T(-96.0)));
+  dl = (T(144.0));
+}
+template <> __host__ __device__ __forceinline__ void Rad_cubic::eval<1, double>(double r, double& w, double& l, double& dl) {
+  using T = double;
+  w = (T(16.0)) * ipow<3>(T(1.0) - r);
+  l = (T(-48.0)) * ipow<2>(T(1.0) - r) * (T(1) / ipow<1>(r));
+  dl = (fma_t(T(48.0), r, T(48.0))) * ipow<1>(T(1.0) - r) * (T(1) / ipow<2>(r));
+}
+template <> __host__ __device__ __forceinline__ void Rad_cubic::eval<1, float>(float r, float& w, float& l, float& dl) {
+  using T = float;
+  w = (T(16.0)) * ipow<3>(T(1.0) - r);
+  l = (T(-48.0)) * ipow<2>(T(1.0) - r) * (T(1) / ipow<1>(r));
+  dl = (fma_t(T(48.0), r, T(48.0))) * ipow<1>(T(1.0) - r) * (T(1) / ipow<2>(r));
+}
+struct Rad_w2 {   // c3*pi = 21/2
+  static constexpr int kPieces = 1;
+  static constexpr double kLo[kPieces] = {0.0};
+  static constexpr double kHi[kPieces] = {1.0};
+  template <typename T> __host__ __device__ static __forceinline__ void full(T* v) {
+    v[0] = T(1.0); v[1] = T(0.0); v[2] = T(0.06666666666666667); v[3] = T(0.06666666666666667); v[4] = T(0.0); v[5] = T(1.0); v[6] = T(1.0); v[7] = T(0.0); v[8] = T(0.0);
+  }
+  template <int P, typename T> __host__ __device__ static __forceinline__ void eval(T r, T& w, T& l, T& dl);
+};
+template <> __host__ __device__ __forceinline__ void Rad_w2::eval<0, double>(double r, double& w, double& l, double& dl) {
+  using T = double;
+  w = (fma_t(T(42.0), r, T(10.5))) * ipow<4>(T(1.0) - r);
+  l = (T(-210.0)) * ipow<3>(T(1.0) - r);
+  dl = (T(630.0)) * ipow<2>(T(1.0) - r);
+}
+template <> __host__ __device__ __forceinline__ void Rad_w2::eval<0, float>(float r, float& w, float& l, float& dl) {
+  using T = float;
+  w = (fma_t(T(42.0), r, T(10.5))) * ipow<4>(T(1.0) - r);
+  l = (T(-210.0)) * ipow<3>(T(1.0) - r);
+  dl = (T(630.0)) * ipow<2>(T(1.0) - r);
+}
+struct Rad_w4 {   // c3*pi = 495/32
+  static constexpr int kPieces = 1;
+  static constexpr double kLo[kPieces] = {0.0};
+  static constexpr double kHi[kPieces] = {1.0};
+  template <typename T> __host__ __device__ static __forceinline__ void full(T* v) {
+    v[0] = T(1.0); v[1] = T(0.0); v[2] = T(0.05128205128205128); v[3] = T(0.05128205128205128); v[4] = T(0.0); v[5] = T(1.0); v[6] = T(1.0); v[7] = T(0.0); v[8] = T(0.0);
+  }
+  template <int P, typename T> __host__ __device__ static __forceinline__ void eval(T r, T& w, T& l, T& dl);
+};
+template <> __host__ __device__ __forceinline__ void Rad_w4::eval<0, double>(double r, double& w, double& l, double& dl) {
+  using T = double;
+  w = (fma_t(fma_t(T(180.46875), r, T(92.8125)), r, T(15.46875))) * ipow<6>(T(1.0) - r);
+  l = (fma_t(T(-1443.75), r, T(-288.75))) * ipow<5>(T(1.0) - r);
+  dl = (T(8662.5)) * ipow<4>(T(1.0) - r) * ipow<1>(r);
+}
+template <> __host__ __device__ __forceinline__ void Rad_w4::eval<0, float>(float r, float& w, float& l, float& dl) {
+  using T = float;
+  w = (fma_t(fma_t(T(180.46875), r, T(92.8125)), r, T(15.46875))) * ipow<6>(T(1.0) - r);
+  l = (fma_t(T(-1443.75), r, T(-288.75))) * ipow<5>(T(1.0) - r);
+  dl = (T(8662.5)) * ipow<4>(T(1.0) - r) * ipow<1>(r);
+}
+struct Rad_w6 {   // c3*pi = 1365/64
+  static constexpr int kPieces = 1;
+  static constexpr double kLo[kPieces] = {0.0};
+  static constexpr double kHi[kPieces] = {1.0};
+  template <typename T> __host__ __device__ static __forceinline__ void full(T* v) {
+    v[0] = T(1.0); v[1] = T(0.0); v[2] = T(0.041666666666666664); v[3] = T(0.041666666666666664); v[4] = T(0.0); v[5] = T(1.0); v[6] = T(1.0); v[7] = T(0.0); v[8] = T(0.0);
+  }
+  template <int P, typename T> __host__ __device__ static __forceinline__ void eval(T r, T& w, T& l, T& dl);
+};
+template <> __host__ __device__ __forceinline__ void Rad_w6::eval<0, double>(double r, double& w, double& l, double& dl) {
+  using T = double;
+  w = (fma_t(fma_t(fma_t(T(682.5), r, T(533.203125)), r, T(170.625)), r, T(21.328125))) * ipow<8>(T(1.0) - r);
+  l = (fma_t(fma_t(T(-7507.5), r, T(-3284.53125)), r, T(-469.21875))) * ipow<7>(T(1.0) - r);
+  dl = (fma_t(T(67567.5), r, T(11261.25))) * ipow<6>(T(1.0) - r) * ipow<1>(r);
+}
+template <> __host__ __device__ __forceinline__ void Rad_w6::eval<0, float>(float r, float& w, float& l, float& dl) {
+  using T = float;
+  w = (fma_t(fma_t(fma_t(T(682.5), r, T(533.203125)), r, T(170.625)), r, T(21.328125))) * ipow<8>(T(1.0) - r);
+  l = (fma_t(fma_t(T(-7507.5), r, T(-3284.53125)), r, T(-469.21875))) * ipow<7>(T(1.0) - r);
+  dl = (fma_t(T(67567.5), r, T(11261.25))) * ipow<6>(T(1.0) - r) * ipow<1>(r);
+}
+
 }  // namespace wsb

@@ -416,6 +416,7 @@ def emit_header() -> str:
     out.append("static const double kPlanCc[kPlanCoeffs] = {" + ", ".join(_lit(x) for x in CC) + "};")
     out.append("static const double kPlanRadii[kPlanNumRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
     out.append("")
+    out.extend(emit_radial())
     out.append("}  // namespace wsb")
     out.append("")
     return "\n".join(out)
@@ -427,6 +428,156 @@ def plane_channels(name):
     k = kernel(name)
     m, p2 = float(k.mass), float(k.plane2)
     return [m, 0.0, 0.0, 0.0, 0.0, m, 0.0, 0.0, m, p2, 0.0, p2]
+
+
+# ------------------------------------------------------------------ 3-D radial profiles (solid half-space / sphere)
+RADIAL_KERNELS = ("cubic", "w2", "w4", "w6")
+_PUBLISHED_C3PI = {"cubic": F(16), "w2": F(21, 2), "w4": F(495, 32), "w6": F(1365, 64)}
+# Gauss-Legendre order of every radial sub-interval: exact for polynomial integrands up to degree 2 * 12 - 1 = 23
+# (the highest is r^4 W a_t of w6, degree 18); cubic's outer Laurent piece lives on r >= 1/2, where 12 nodes leave a
+# relative error below 1e-17.
+RADIAL_GAUSS = 12
+
+
+@dataclass(frozen=True)
+class RadialProfile:
+    """f(r) = r^p (hi - r)^k g(r) with g a polynomial; exact rational coefficients."""
+    p: int
+    k: int
+    g: Tuple[F, ...]
+
+    def __call__(self, r: F) -> F:
+        return F(r) ** self.p * (self.hi - F(r)) ** self.k * _peval(list(self.g), F(r)) if self.k else \
+            F(r) ** self.p * _peval(list(self.g), F(r))
+
+
+def _factor_laurent(terms, hi):
+    """{n: c} (n may be negative) -> (p, k, g) with f = r^p (hi - r)^k g(r), (hi - r) divided out while g(hi) = 0."""
+    terms = {n: c for n, c in terms.items() if c}
+    p = min(terms)
+    g = [F(0)] * (max(terms) - p + 1)
+    for n, c in terms.items():
+        g[n - p] = c
+    k = 0
+    while len(g) > 1 and _peval(g, hi) == 0:
+        # synthetic division by (hi - r) = -(r - hi): g = (r - hi) q  ->  g = (hi - r) (-q)
+        q = [F(0)] * (len(g) - 1)
+        acc = F(0)
+        for i in range(len(g) - 1, 0, -1):
+            acc = acc * hi + g[i]
+            q[i - 1] = acc
+        g = [-x for x in q]
+        k += 1
+    return p, k, tuple(_trim(g))
+
+
+@lru_cache(maxsize=None)
+def radial(name: str):
+    """the 3-D radial tables of `name` (unit support): [(lo, hi, W, L, dL)] with W = c3pi * shape (the 3-D kernel
+    times pi), L = W'/r and dL = L' as RadialProfile in r, and c3pi (checked against the published constant)."""
+    if name not in RADIAL_KERNELS:
+        raise KeyError(f"radial family: kernel {name!r} not in {RADIAL_KERNELS}")
+    raw = _pieces(name)
+    tot = F(0)
+    for lo, hi, c in raw:
+        P = [F(0)] * 3 + [x / (i + 3) for i, x in enumerate(c)]
+        tot += _peval(P, hi) - _peval(P, lo)
+    c3pi = 1 / (4 * tot)
+    if c3pi != _PUBLISHED_C3PI[name]:
+        raise AssertionError(f"3-D normalisation of {name}: {c3pi} != published {_PUBLISHED_C3PI[name]}")
+    out = []
+    for lo, hi, c in raw:
+        w = {n: c3pi * x for n, x in enumerate(c)}
+        ell = {n - 2: n * x for n, x in w.items() if n >= 1}
+        dell = {n - 1: n * x for n, x in ell.items() if n != 0}
+        out.append((lo, hi, *(RadialProfile(*_factor_laurent(t, hi)) for t in (w, ell, dell))))
+    return tuple(out), c3pi
+
+
+def _radial_eval(prof, var, hi_lit, T):
+    """C++ expression of a RadialProfile at `var` in type T."""
+    g = list(prof.g)
+    expr = f"T({_lit(g[-1])})"
+    for x in reversed(g[:-1]):
+        expr = f"fma_t({expr}, {var}, T({_lit(x)}))" if x != 0 else f"({expr} * {var})"
+    fac = []
+    if prof.k:
+        fac.append(f"ipow<{prof.k}>(T({hi_lit}) - {var})")
+    if prof.p > 0:
+        fac.append(f"ipow<{prof.p}>({var})")
+    if prof.p < 0:
+        fac.append(f"(T(1) / ipow<{-prof.p}>({var}))")
+    return " * ".join([f"({expr})"] + fac)
+
+
+def emit_radial() -> list:
+    """generated device code of the radial family: per kernel the pieces and W, W'/r, (W'/r)' in factored form."""
+    import numpy as np
+    xg, wg = np.polynomial.legendre.leggauss(RADIAL_GAUSS)
+    out = ["// ---- 3-D radial family (solid half-space / sphere), unit support; W = c3*pi * shape, L = W'/r, dL = L'",
+           "template <int K, typename T>",
+           "__host__ __device__ __forceinline__ T ipow(T x) {",
+           "  T y = x;",
+           "#pragma unroll",
+           "  for (int i = 1; i < K; ++i) y *= x;",
+           "  return y;",
+           "}",
+           "__host__ __device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }",
+           "__host__ __device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }",
+           f"constexpr int kRadialGauss = {RADIAL_GAUSS};",
+           "static __device__ const double kRadialGx[kRadialGauss] = {" + ", ".join(repr(float(x)) for x in xg) + "};",
+           "static __device__ const double kRadialGw[kRadialGauss] = {" + ", ".join(repr(float(x)) for x in wg) + "};"]
+    for name in RADIAL_KERNELS:
+        pcs, c3pi = radial(name)
+        out.append(f"struct Rad_{name} {{   // c3*pi = {c3pi}")
+        out.append(f"  static constexpr int kPieces = {len(pcs)};")
+        out.append("  static constexpr double kLo[kPieces] = {" + ", ".join(_lit(p[0]) for p in pcs) + "};")
+        out.append("  static constexpr double kHi[kPieces] = {" + ", ".join(_lit(p[1]) for p in pcs) + "};")
+        # whole-support constants (the region of the support inside the solid is the full ball)
+        full = _radial_full(name)
+        out.append("  template <typename T> __host__ __device__ static __forceinline__ void full(T* v) {")
+        out.append("    " + " ".join(f"v[{j}] = T({_lit(x)});" for j, x in enumerate(full)))
+        out.append("  }")
+        out.append("  template <int P, typename T> __host__ __device__ static __forceinline__ void eval(T r, T& w, T& l, T& dl);")
+        out.append("};")
+        for i, (lo, hi, W, L, dL) in enumerate(pcs):
+            out.append(f"template <> __host__ __device__ __forceinline__ void Rad_{name}::eval<{i}, double>(double r, double& w, double& l, double& dl) {{")
+            out.append("  using T = double;")
+            for var, prof in (("w", W), ("l", L), ("dl", dL)):
+                out.append(f"  {var} = {_radial_eval(prof, 'r', _lit(hi), 'T')};")
+            out.append("}")
+            out.append(f"template <> __host__ __device__ __forceinline__ void Rad_{name}::eval<{i}, float>(float r, float& w, float& l, float& dl) {{")
+            out.append("  using T = float;")
+            for var, prof in (("w", W), ("l", L), ("dl", dL)):
+                out.append(f"  {var} = {_radial_eval(prof, 'r', _lit(hi), 'T')};")
+            out.append("}")
+    out.append("")
+    return out
+
+
+def _radial_full(name):
+    """the nine invariants (unit support, /pi folded) of a query whose whole support lies inside the solid."""
+    pcs, _ = radial(name)
+    def integral(prof_idx, power):
+        tot = F(0)
+        for lo, hi, *profs in pcs:
+            prof = profs[prof_idx]
+            # exact integral of r^power * prof over [lo, hi] by expanding prof into a Laurent polynomial
+            poly = list(prof.g)
+            if prof.k:
+                poly = _pmul(poly, _ppow([hi, F(-1)], prof.k))
+            for n, c in enumerate(poly):
+                e = n + prof.p + power
+                if c == 0:
+                    continue
+                if e == -1:
+                    raise AssertionError("log term in a whole-support constant")
+                tot += c * (hi ** (e + 1) - lo ** (e + 1)) / (e + 1)
+        return tot
+    w2, w4 = integral(0, 2), integral(0, 4)
+    l4, l2, dl3 = integral(1, 4), integral(1, 2), integral(2, 3)
+    return [4 * w2, F(0), F(4, 3) * w4, F(4, 3) * w4, F(0), -F(4, 3) * l4, -F(4, 3) * l4,
+            4 * l2 + F(4, 3) * dl3, 4 * l2 + F(4, 3) * dl3]
 
 
 if __name__ == "__main__":       # python -m warpsphboundaries_b200.kernels  -> regenerate the header
