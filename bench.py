@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
-    p.add_argument("--serve-requests", type=int, default=2000,
+    p.add_argument("--serve-requests", type=int, default=10000,
                    help="requests of the serving stream measured after the main workload (0: skip)")
     return p.parse_args()
 
@@ -163,7 +163,7 @@ class Clocks:
 
 
 # ----------------------------------------------------------------------------------------------- serving stream
-def serving_run(n_requests, dev, pair_density, seed=0, load=0.6):
+def serving_run(n_requests, dev, pair_density, seed=0, load=0.7):
     """Poisson stream of boundary queries over 32 resident scenes of the large 2-D kind (64 star polygons each,
     h = 0.02), particle counts log-uniform in [1e3, 1e6] (positions uniform in [0, 4]^2, produced on the device at
     arrival), kernels uniform in {w2, w4, w6}, 25 % of the requests with the adjoint.  The arrival rate is `load` times
@@ -194,7 +194,7 @@ def serving_run(n_requests, dev, pair_density, seed=0, load=0.6):
 
     # saturation probes (every request submitted as soon as the previous submit returns, polling in between, as in the
     # stream): the first warms graphs and workspaces, the second measures the sustainable capacity in rows/s
-    burst = specs[: min(300, n_requests)]
+    burst = specs[: min(600, n_requests)]
     for rep in range(2):
         t0 = time.perf_counter()
         for sid, rows, k, g in burst:
@@ -211,8 +211,7 @@ def serving_run(n_requests, dev, pair_density, seed=0, load=0.6):
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
     for r in list(srv.completed):
         srv.release(r.rid)
-    srv.completed.clear()
-    srv.t_first = srv.t_last = None
+    srv.reset_stats()
     start = time.perf_counter()
     i = 0
     released = [0]
@@ -233,12 +232,54 @@ def serving_run(n_requests, dev, pair_density, seed=0, load=0.6):
     return {"requests": n_requests, "scenes": 32, "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
             "mean_ms": st.get("mean_ms"), "arrival_rate_per_s": rate, "wall_s": wall,
             "rows_per_s": rows_total / wall, "pairs_per_s_est": rows_total * pair_density / wall,
-            "capacity_rows_per_s": cap_rows, "offered_load": load,
+            "capacity_rows_per_s": cap_rows, "offered_load": load, "gpu_busy": st.get("gpu_busy"),
             "note": "pairs estimated from the mean neighbour-pair density of the 2^20-particle scene; all 32 scenes "
                     "2-D (the 3-D mesh scenes of the serving mix are not built)"}
 
 
 # ----------------------------------------------------------------------------------------------- our arm
+def radial_run(dev, stream, flush, n=1 << 21, steps=10, kernel="w4"):
+    """solid spheres in 3-D: 2^21 (query, sphere) shell rows, h = 0.03, radii exp U(ln 0.2h, ln 50h), signed
+    distances U(-1.2h, 1.2h) (clipped at -R), all 28 baseline channels, float64, inputs resident."""
+    import ctypes
+
+    import torch
+    from warpsphboundaries_b200 import _lib
+    from warpsphboundaries_b200.kernels import KERNEL_IDS
+    from warpsphboundaries_b200.radial import RadialEvaluator
+    rng = np.random.default_rng(11)
+    h = 0.03
+    R = np.exp(rng.uniform(np.log(0.2 * h), np.log(50 * h), n))
+    d = np.maximum(rng.uniform(-1.2 * h, 1.2 * h, n), -R)
+    nv = rng.normal(size=(n, 3))
+    nv /= np.linalg.norm(nv, axis=1, keepdims=True)
+    ev = RadialEvaluator("sphere", kernel=kernel)
+    b = ev.prepare(d, nv, h, radii=R)
+    meta = ev.metadata
+    args = (_lib.RADIAL_SPHERE, KERNEL_IDS[kernel], _lib.PREC_FP64, _lib.ptr(b.distances), _lib.ptr(b.radii),
+            _lib.ptr(b.normals), _lib.ptr(b.supports), n, meta.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            len(ev.requests), _lib.ptr(b.values), None, None, ctypes.c_void_p(stream.cuda_stream))
+    for _ in range(3):
+        _lib.check(_lib.lib.wsb_radial_channels(*args))
+    tot = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(_lib.lib.wsb_radial_channels(*args))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    ms = tot / steps
+    byts = n * (6 * 8 + 28 * 8)
+    shell = float(np.mean(np.abs(d) < h))
+    return {"workload": f"{n} sphere rows, h=0.03, R in [0.2h, 50h], d in [-1.2h, 1.2h], {kernel}, 28 channels, f64",
+            "ms": ms, "rows_per_s": n / (ms * 1e-3), "hbm_gbs": byts / (ms * 1e-3) / 1e9,
+            "bytes_per_row": 6 * 8 + 28 * 8, "shell_fraction": shell, "kernel": "k_radial"}
+
+
 def our_arm(args):
     import torch
     import torch.distributed as dist
@@ -421,6 +462,8 @@ def our_arm(args):
                "h2d_bytes_per_step": N * 3 * 8, "d2h_bytes_per_step": len(KERNELS) * N * 7 * 8,
                "ms_per_step": float(t.item()) / args.steps}
 
+    radial = radial_run(dev, stream, flush) if world == 1 else None
+
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:
         serving = serving_run(args.serve_requests, dev, P / N)
@@ -447,7 +490,7 @@ def our_arm(args):
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
                 "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
                 "gpu_launches": args.steps * (4 + 2 * len(KERNELS)),
-                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving,
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial,
                 **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -14,12 +14,14 @@ Scheduling (one host thread, the caller's):
   pairs are summed in its own fixed order), so a request's result is bit-identical alone and in any mix;
 * batches run on `streams` CUDA streams at once, so requests that arrive while others are on the GPU are admitted as
   stream slots and memory free up, and their work overlaps on the device;
-* batches of at most `graph_max_rows` rows replay a CUDA graph captured per (stream, bucket, scene, kernel) over
-  static buffers padded to a power-of-two bucket (padding rows are masked out), removing launch overhead for small
-  requests; a key is captured once it has been launched `graph_after_uses` times, so one-off keys stay eager;
-* nothing is allocated per batch: a request's outputs are allocated when it is submitted (on the caller's stream),
-  a single-request batch writes straight into them, a multi-request batch into persistent per-stream buffers that are
-  then copied into each request's outputs;
+* with `use_graphs=True`, batches of at most `graph_max_rows` rows replay a CUDA graph captured per (stream, bucket,
+  scene, kernel) over static buffers padded to a power-of-two bucket (padding rows are masked out); a key is captured
+  once it has been launched `graph_after_uses` times, so one-off keys stay eager.  Off by default: a batch is seven
+  launches per surface, and each capture holds its own padded outputs and workspace;
+* nothing is allocated per batch: a request's outputs come from a pool of power-of-two buffers when it is submitted
+  (on the caller's stream), a scalar support is a view of a resident vector, a single-request batch writes straight
+  into the request's outputs, a multi-request batch into persistent per-stream buffers that are then copied into each
+  request's outputs;
 * admission: a batch is launched while the device memory it reserves fits `hbm_budget`, and `submit` blocks (it
   keeps polling) while the outputs of queued and in-flight requests would exceed it -- back-pressure instead of an
   unbounded queue;
@@ -66,6 +68,7 @@ class _Batch:
     rows: int
     reserved: int
     event: torch.cuda.Event
+    start: Optional[torch.cuda.Event] = None
 
 
 class _Slot:
@@ -96,6 +99,7 @@ class _Slot:
                 self.buf = {"pos": torch.empty((cap, 2), dtype=F64, device=self.device),
                             "sup": torch.empty(cap, dtype=F64, device=self.device),
                             "one": torch.ones(cap, dtype=F64, device=self.device),
+                            "d_pos": torch.empty((cap, 2), dtype=F64, device=self.device),
                             **{k: torch.empty((self.B, cap) + _TAIL[k], dtype=F64, device=self.device)
                                for k in OUT_KEYS}}
             self.cap = cap
@@ -103,7 +107,7 @@ class _Slot:
 
 
 class BoundaryServer:
-    def __init__(self, device="cuda:0", streams=4, max_batch_rows=1 << 20, hbm_budget=None, use_graphs=True,
+    def __init__(self, device="cuda:0", streams=4, max_batch_rows=1 << 20, hbm_budget=None, use_graphs=False,
                  graph_max_rows=1 << 16, precision="fp64", graph_after_uses=4, pool_limit=None):
         self.device = torch.device(device)
         self.scenes: Dict[str, tuple] = {}
@@ -132,6 +136,8 @@ class BoundaryServer:
         self.pooled_bytes = 0
         self.pool_limit = int(pool_limit if pool_limit is not None else 0.1 * free)
         self.held_bytes = 0                 # outputs of queued and in-flight requests
+        self.support_vecs = {}              # support value -> resident vector filled with it
+        self.intervals = []                 # (start, end) events of retired batches (device busy time)
 
     # ------------------------------------------------------------------ scenes
     def register(self, scene_id, scene, support):
@@ -157,9 +163,10 @@ class BoundaryServer:
             raise KeyError(f"unknown scene {scene_id!r}")
         kname = kernelName(kernel)
         pos = positions.to(self.device, F64).contiguous()
-        sup = supports if torch.is_tensor(supports) else torch.full((len(pos),), float(supports), dtype=F64,
-                                                                      device=self.device)
-        sup = sup.to(self.device, F64).contiguous()
+        if torch.is_tensor(supports):
+            sup = supports.to(self.device, F64).contiguous()
+        else:
+            sup = self._support_vec(float(supports), len(pos))
         r = Request(next(self._ids), scene_id, kname, pos, sup, bool(grad),
                     time.perf_counter() if arrival is None else arrival)
         B, n = len(self.scenes[scene_id][0].bodies), len(pos)
@@ -199,6 +206,15 @@ class BoundaryServer:
             self.pooled_bytes += 8 * flat.numel()
         r.result = None
         r.flat = None
+
+    def _support_vec(self, value, n):
+        """a view of n copies of `value` from a resident vector (grown geometrically; no allocation per request)."""
+        v = self.support_vecs.get(value)
+        if v is None or v.numel() < n:
+            v = torch.full((max(n, self.max_batch_rows, 2 * (0 if v is None else v.numel())),), value, dtype=F64,
+                           device=self.device)
+            self.support_vecs[value] = v
+        return v[:n]
 
     def _take(self, n):
         """a float64 buffer of at least n elements: pooled size classes (powers of two) avoid allocator calls in the
@@ -252,6 +268,7 @@ class BoundaryServer:
                     self.completed.append(r)
                     self.held_bytes -= r.nbytes
                 self.reserved -= b.reserved
+                self.intervals.append((b.start, b.event))
                 s.busy = None
                 self.n_inflight -= 1
                 self.t_last = t
@@ -285,6 +302,8 @@ class BoundaryServer:
         if self.t_first is None:
             self.t_first = time.perf_counter()
         slot.stream.wait_stream(torch.cuda.current_stream(self.device))   # inputs and outputs come from the caller
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev0.record(slot.stream)
         with torch.cuda.stream(slot.stream):
             single = len(reqs) == 1
             if single:
@@ -311,7 +330,11 @@ class BoundaryServer:
                 self._aggregate(plan, kname, pos, sup, None, rows, outs, slot.workspace(self.ws_bytes),
                                 slot.stream)
             if grad:
-                d_pos = reqs[0].result["d_pos"] if single else torch.zeros((rows, 2), dtype=F64, device=self.device)
+                if single:
+                    d_pos = reqs[0].result["d_pos"]
+                else:
+                    d_pos = slot.buffers(rows, B)["d_pos"][:rows]
+                    d_pos.zero_()
                 self._adjoint(plan, support, kname, pos, sup, d_pos, slot)
             if not single:
                 off = 0
@@ -322,9 +345,9 @@ class BoundaryServer:
                     if grad:
                         r.result["d_pos"].copy_(d_pos[off:off + n])
                     off += n
-            ev = torch.cuda.Event()
+            ev = torch.cuda.Event(enable_timing=True)
             ev.record(slot.stream)
-        slot.busy = _Batch(reqs, rows, need, ev)
+        slot.busy = _Batch(reqs, rows, need, ev, ev0)
 
     def _aggregate(self, plan, kname, pos, sup, allowed, n, outs, ws, stream):
         """the fused aggregate of every body and surface of a resolved scene into `outs` (the first surface of a body
@@ -375,8 +398,15 @@ class BoundaryServer:
             gout = {k: torch.empty((B, bucket) + _TAIL[k], dtype=F64, device=self.device) for k in OUT_KEYS}
             self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)     # eager warm-up
             graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(graph, stream=slot.stream):
-                self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)
+            # captured directly on the slot's stream: torch.cuda.graph() would also empty the allocator's cache, and
+            # every later allocation would then go back to the driver
+            slot.stream.synchronize()
+            with torch.cuda.stream(slot.stream):
+                graph.capture_begin(capture_error_mode="thread_local")
+                try:
+                    self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)
+                finally:
+                    graph.capture_end()
             g = (graph, gout, ws)
             self.graphs[key] = g
         graph, gout, _ = g
@@ -397,4 +427,24 @@ class BoundaryServer:
                        mean_ms=float(lat.mean()), max_ms=float(lat.max()))
         if self.t_first is not None and self.t_last is not None:
             out["wall_s"] = self.t_last - self.t_first
+        if self.intervals:
+            # device busy fraction: the union of the batches' [start, end] intervals over the span they cover
+            ref = self.intervals[0][0]
+            iv = sorted((ref.elapsed_time(a), ref.elapsed_time(b)) for a, b in self.intervals)
+            busy, cur0, cur1 = 0.0, iv[0][0], iv[0][1]
+            for a, b in iv[1:]:
+                if a > cur1:
+                    busy += cur1 - cur0
+                    cur0, cur1 = a, b
+                else:
+                    cur1 = max(cur1, b)
+            busy += cur1 - cur0
+            span = max(b for _, b in iv) - min(a for a, _ in iv)
+            out["gpu_busy"] = busy / span if span > 0 else None
         return out
+
+    def reset_stats(self):
+        """forget completed requests' latencies and the busy intervals (e.g. after a warm-up)."""
+        self.completed.clear()
+        self.intervals.clear()
+        self.t_first = self.t_last = None
