@@ -388,7 +388,7 @@ def our_arm(args):
     flops = {k: P * pair_work(k)["flops"] for k in KERNELS}
     achieved = sum(flops.values()) / (sum(eval_ms.values()) * 1e-3) / 1e12
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "agg_main_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "k_agg_pairs_traffic.json")
     if os.path.exists(tp):
         try:
             traffic = json.load(open(tp)).get("bytes_per_launch")
