@@ -173,7 +173,12 @@ __global__ void k_agg_rows(const double* __restrict__ sup, const double* __restr
 // together.  The G partial sums are combined by an xor butterfly (the same additions on every lane, commutative, so
 // the result is deterministic and identical on the G lanes).
 template <class KT, int PREC, int G>
-__global__ void __launch_bounds__(kThreads) k_agg_pairs(SurfView S, const double* __restrict__ sup,
+// 6 resident CTAs of 128 threads per SM (at most 80 registers a thread): measured 13 % faster on B200 than the
+// unconstrained 92-94 registers (5 CTAs); 8 CTAs (64 registers) spills
+#ifndef WSB_PAIRS_MIN_BLOCKS
+#define WSB_PAIRS_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(SurfView S, const double* __restrict__ sup,
                                                        const int32_t* __restrict__ key,
                                                        const double* __restrict__ lpos,
                                                        const int32_t* __restrict__ order,

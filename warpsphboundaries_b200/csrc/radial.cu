@@ -129,65 +129,85 @@ __device__ __forceinline__ void radial_invariants(T d, T R, bool sphere, Inv9<T>
   static_assert(KR::kPieces <= 2, "radial kernels have at most two pieces");
 }
 
+constexpr int kRadialThreads = 128;
+
+__device__ __forceinline__ double pick3(int i, double x, double y, double z) { return i == 0 ? x : (i == 1 ? y : z); }
+
+// one thread per row; the block's rows are contiguous, so their outputs [row0 .. row0 + 128) x n_requests are one
+// contiguous range: each thread writes its row into shared memory, then the block stores the range coalesced
 template <class KR, typename T>
-__global__ void __launch_bounds__(128) k_radial(const double* __restrict__ dist, const double* __restrict__ radii,
-                                                const double* __restrict__ normals,
-                                                const double* __restrict__ supports, int64_t n, int sphere,
-                                                RadialRequests req, double* __restrict__ out,
-                                                double* __restrict__ inv_out, int32_t* __restrict__ status) {
-  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n) return;
-  const double h = supports[row], dd = dist[row];
-  const double Rr = sphere ? radii[row] : 0.0;
-  const double nx = normals[3 * row], ny = normals[3 * row + 1], nz = normals[3 * row + 2];
-  const bool ok = h > 0.0 && isfinite(h) && isfinite(dd) && isfinite(nx) && isfinite(ny) && isfinite(nz) &&
-                  (!sphere || (Rr > 0.0 && isfinite(Rr) && dd >= -Rr));
-  Inv9<T> acc;
-  double inv[9];
-  if (ok) {
-    radial_invariants<KR, T>(T(dd / h), T(Rr / h), sphere != 0, acc);
-    const double ih = 1.0 / h;
-    const double scale[9] = {1.0, h, h * h, h * h, ih, 1.0, 1.0, ih * ih, ih * ih};
+__global__ void __launch_bounds__(kRadialThreads, 6) k_radial(const double* __restrict__ dist,
+                                                              const double* __restrict__ radii,
+                                                              const double* __restrict__ normals,
+                                                              const double* __restrict__ supports, int64_t n,
+                                                              int sphere, RadialRequests req,
+                                                              double* __restrict__ out, double* __restrict__ inv_out,
+                                                              int32_t* __restrict__ status) {
+  __shared__ double stage[kRadialThreads * 28];
+  const int64_t row0 = (int64_t)blockIdx.x * kRadialThreads;
+  const int64_t row = row0 + threadIdx.x;
+  const int nreq = req.n;
+  if (row < n) {
+    const double h = supports[row], dd = dist[row];
+    const double Rr = sphere ? radii[row] : 0.0;
+    const double nx = normals[3 * row], ny = normals[3 * row + 1], nz = normals[3 * row + 2];
+    const bool ok = h > 0.0 && isfinite(h) && isfinite(dd) && isfinite(nx) && isfinite(ny) && isfinite(nz) &&
+                    (!sphere || (Rr > 0.0 && isfinite(Rr) && dd >= -Rr));
+    Inv9<T> acc;
+    double inv[9];
+    if (ok) {
+      radial_invariants<KR, T>(T(dd / h), T(Rr / h), sphere != 0, acc);
+      const double ih = 1.0 / h;
+      const double scale[9] = {1.0, h, h * h, h * h, ih, 1.0, 1.0, ih * ih, ih * ih};
 #pragma unroll
-    for (int j = 0; j < 9; ++j) inv[j] = (double)acc.v[j] * scale[j];
-  } else {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) inv[j] = __longlong_as_double(0x7ff8000000000000LL);
-  }
-  if (status) status[row] = ok ? 0 : 1;
-  if (inv_out) {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) inv_out[row * 9 + j] = inv[j];
-  }
-  const double nv[3] = {nx, ny, nz};
-  for (int c = 0; c < req.n; ++c) {
-    const int degree = req.meta[c][0], i = req.meta[c][1], j = req.meta[c][2], order = req.meta[c][3];
-    double v;
-    if (degree == 0 && order == 0) {
-      v = inv[0];
-    } else if (degree == 1 && order == 0) {
-      v = inv[1] * nv[i];
-    } else if (degree == 0 && order == 1) {
-      v = inv[4] * nv[i];
+      for (int j = 0; j < 9; ++j) inv[j] = (double)acc.v[j] * scale[j];
     } else {
-      const int t = order == 0 ? 2 : (order == 1 ? 5 : 7);
-      v = (inv[t + 1] - inv[t]) * nv[i] * nv[j];
-      if (i == j) v += inv[t];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) inv[j] = __longlong_as_double(0x7ff8000000000000LL);
     }
-    out[row * req.n + c] = v;
+    if (status) status[row] = ok ? 0 : 1;
+    if (inv_out) {
+#pragma unroll
+      for (int j = 0; j < 9; ++j) inv_out[row * 9 + j] = inv[j];
+    }
+#pragma unroll 4
+    for (int c = 0; c < nreq; ++c) {
+      const int degree = req.meta[c][0], i = req.meta[c][1], j = req.meta[c][2], order = req.meta[c][3];
+      const double ni = pick3(i, nx, ny, nz), nj = pick3(j, nx, ny, nz);
+      double v;
+      if (degree == 0 && order == 0) {
+        v = inv[0];
+      } else if (degree == 1 && order == 0) {
+        v = inv[1] * ni;
+      } else if (degree == 0 && order == 1) {
+        v = inv[4] * ni;
+      } else {
+        // tangent / axial pair of the second-order entry: m2 (2, 3), g1 (5, 6), Hessian (7, 8)
+        const double tan = order == 0 ? inv[2] : (order == 1 ? inv[5] : inv[7]);
+        const double axi = order == 0 ? inv[3] : (order == 1 ? inv[6] : inv[8]);
+        v = (axi - tan) * ni * nj + (i == j ? tan : 0.0);
+      }
+      stage[threadIdx.x * nreq + c] = v;
+    }
   }
+  __syncthreads();
+  const int64_t rows_here = n - row0 < kRadialThreads ? n - row0 : kRadialThreads;
+  const int count = (int)rows_here * nreq;
+  double* dst = out + row0 * nreq;
+  for (int k = threadIdx.x; k < count; k += kRadialThreads) dst[k] = stage[k];
 }
 
 template <typename T>
 int launch_radial(int kernel, const double* d, const double* r, const double* nrm, const double* h, int64_t n,
                   int sphere, const RadialRequests& req, double* out, double* inv, int32_t* status,
                   cudaStream_t st) {
-  const unsigned grid = (unsigned)((n + 127) / 128);
+  const unsigned grid = (unsigned)((n + kRadialThreads - 1) / kRadialThreads);
+  constexpr int B = kRadialThreads;
   switch (kernel) {
-    case WSB_KERNEL_CUBIC: k_radial<Rad_cubic, T><<<grid, 128, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
-    case WSB_KERNEL_W2: k_radial<Rad_w2, T><<<grid, 128, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
-    case WSB_KERNEL_W4: k_radial<Rad_w4, T><<<grid, 128, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
-    case WSB_KERNEL_W6: k_radial<Rad_w6, T><<<grid, 128, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
+    case WSB_KERNEL_CUBIC: k_radial<Rad_cubic, T><<<grid, B, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
+    case WSB_KERNEL_W2: k_radial<Rad_w2, T><<<grid, B, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
+    case WSB_KERNEL_W4: k_radial<Rad_w4, T><<<grid, B, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
+    case WSB_KERNEL_W6: k_radial<Rad_w6, T><<<grid, B, 0, st>>>(d, r, nrm, h, n, sphere, req, out, inv, status); break;
     default: return fail(WSB_ERR_UNSUPPORTED, "wsb_radial_channels: the radial family serves cubic, w2, w4, w6");
   }
   WSB_CUDA(cudaGetLastError());
