@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--particles", type=int, default=1 << 20)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-mesh", action="store_true", help="skip the 3-D closed-surface leg")
     p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
     p.add_argument("--serve-requests", type=int, default=10000,
                    help="requests of the serving stream measured after the main workload (0: skip)")
@@ -280,6 +281,43 @@ def radial_run(dev, stream, flush, n=1 << 21, steps=10, kernel="w4"):
             "bytes_per_row": 6 * 8 + 28 * 8, "shell_fraction": shell, "kernel": "k_radial"}
 
 
+def mesh_run(dev, stream, flush, steps=5, kernel="w4"):
+    """the 3-D scene: 2^21 particles uniform in [-1, 1]^3, h = 0.03, a jittered icosphere of 20480 faces (radius 0.6),
+    the 28 baseline channels of every particle, float64, inputs resident; CUDA events around wsb_mesh_channels."""
+    import ctypes
+
+    import torch
+    from warpsphboundaries_b200 import workloads
+    from warpsphboundaries_b200.mesh3d import ClosedMesh
+    V, Fc, X, h = workloads.c3()
+    n = len(X)
+    m = ClosedMesh(V, Fc, h, dev)
+    pos = torch.tensor(X, dtype=torch.float64, device=dev)
+    sup = torch.full((n,), h, dtype=torch.float64, device=dev)
+    out = torch.empty((n, 28), dtype=torch.float64, device=dev)
+    for _ in range(2):
+        m.channels(pos, sup, kernel, out=out, stream=stream)
+    torch.cuda.synchronize()
+    nwork = int(m._ws[2 * ((4 * n + 255) // 256 * 256):][:4].view(torch.int32).item())
+    tot = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        m.channels(pos, sup, kernel, out=out, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    ms = tot / steps
+    inside = float(out[:, 0].mean().item())
+    return {"workload": f"c3: {n} particles in [-1,1]^3, h=0.03, icosphere {len(Fc)} faces (r 0.6, 5% jitter), "
+                        f"{kernel}, 28 channels, f64", "ms": ms, "particles_per_s": n / (ms * 1e-3),
+            "surface_rows": nwork, "surface_rows_per_s": nwork / (ms * 1e-3), "mean_lambda": inside,
+            "kernels": ["k_mesh_rowinfo", "k_mesh_rows", "k_mesh_eval"], "launches_per_step": 3}
+
+
 def our_arm(args):
     import torch
     import torch.distributed as dist
@@ -463,6 +501,7 @@ def our_arm(args):
                "ms_per_step": float(t.item()) / args.steps}
 
     radial = radial_run(dev, stream, flush) if world == 1 else None
+    mesh = mesh_run(dev, stream, flush) if world == 1 and not args.no_mesh else None
 
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:
@@ -490,7 +529,7 @@ def our_arm(args):
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
                 "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
                 "gpu_launches": args.steps * (4 + 2 * len(KERNELS)),
-                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial,
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh,
                 **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -175,6 +175,37 @@ int wsb_radial_channels(int kind, int kernel, int precision, const double* dista
                         const double* normals, const double* supports, int64_t n, const int32_t* requests,
                         int n_requests, double* out, double* invariants, int32_t* status, void* stream);
 
+/* ---- closed triangle surfaces (3-D) ----
+ * A watertight, consistently oriented triangle surface with outward normals (positive signed volume): verts
+ * [n_verts*3] and faces [n_faces*3] (vertex ids) on the host, copied to `device` with a cell grid of faces (cell =
+ * support_max) and (x, y) columns of faces for the inside test.  Invalid surfaces (open, inconsistently oriented,
+ * negative volume, zero-area faces) return WSB_ERR_ARG.  Replaces fluxbridge's Geometry.closed_surface with its
+ * whole-element search tree (src/warpSPHBoundaries/fluxbridge/geometry.py:75-170, device_search.py:125-212) and the
+ * surface checks of mesh3d ClosedSurface (src/warpSPHBoundaries/mesh3d/reference.py:221-244). */
+typedef struct wsb_mesh wsb_mesh;
+int wsb_mesh_create(const double* verts, int64_t n_verts, const int32_t* faces, int64_t n_faces, double support_max,
+                    int device, wsb_mesh** out);
+int wsb_mesh_destroy(wsb_mesh* m);
+
+/* bytes of the workspace wsb_mesh_channels needs for n queries */
+size_t wsb_mesh_workspace_size(const wsb_mesh* m, int64_t n);
+
+/* 1 where the query pos [n*3] (device) lies inside the solid, else 0 (parity of a vertical ray's crossings with
+ * exact tie rules on shared edges).  Replaces the solid-angle winding sum of fluxbridge's closed-surface element
+ * (src/warpSPHBoundaries/fluxbridge/wp_func.py:231-253). */
+int wsb_mesh_inside(const wsb_mesh* m, const double* pos, int64_t n, int32_t* inside, void* stream);
+
+/* The 28 baseline channels of every query (pos [n*3], supports sup [n] <= support_max, device) into out [n*28]
+ * (device, float64, physical units, overwritten): value moments int_solid y^alpha W for alpha = 000 100 010 001 200
+ * 110 101 020 011 002 (y = point - query), kernel-gradient moments int y^alpha dW/dx_j for alpha = 000 100 010 001 and
+ * j = 0..2, and the kernel Hessian int d2W/dx_i dx_j (00 01 02 11 12 22).  `inside` [n] (may be NULL) receives the
+ * inside test (-1 for a row with support above support_max, support <= 0 or a non-finite position: its outputs are
+ * NaN).  Kernels cubic, w2, w4, w6.  Replaces fluxbridge's Evaluator over Geometry.closed_surface with the baseline
+ * requests: Batch.launch, wp_func.element / output / batch and Batch.reduce
+ * (src/warpSPHBoundaries/fluxbridge/evaluate.py:11-187, src/warpSPHBoundaries/fluxbridge/wp_func.py:119-369). */
+int wsb_mesh_channels(const wsb_mesh* m, int kernel, const double* pos, const double* sup, int64_t n, double* out,
+                      int32_t* inside, void* workspace, size_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

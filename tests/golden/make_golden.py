@@ -16,6 +16,10 @@ Writes
   radial_golden.json          solid half-spaces and spheres, 3-D: the nine radial invariants and the 28 baseline
                               channels of the reference's 70-digit fixtures (tests/fixtures/fluxbridge-radial-v1.json,
                               and the baseline requests of tests/fixtures/fluxbridge-sphere-v1.json)
+  mesh3d_golden.json          closed triangle surfaces, 3-D: the 28 baseline channels (value moments |alpha| <= 2,
+                              kernel-gradient moments |alpha| <= 1, kernel Hessian) from the reference's exact
+                              face-to-edge reductions in mpmath (mesh3d/reference.py ClosedSurface), 40 digits, for an
+                              icosahedron, a jittered once-subdivided icosphere, a box and a notched (non-convex) block
 
 The reference package is imported with a stub parent package because its
 `__init__` needs the GPU stack (warp, warpSPHCore), which the CPU modules used
@@ -175,6 +179,104 @@ def radial_golden(root):
     print("radial_golden.json:", len(out["radial"]), "radial cases,", len(out["sphere"]), "sphere cases")
 
 
+def _icosahedron(radius):
+    t = (1 + 5 ** 0.5) / 2
+    V = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+                  [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], float)
+    F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    return V / np.linalg.norm(V[0]) * radius, F
+
+
+def _subdivide(V, F):
+    V = [tuple(v) for v in V]
+    mid = {}
+
+    def m(a, b):
+        key = (min(a, b), max(a, b))
+        if key not in mid:
+            mid[key] = len(V)
+            V.append(tuple((np.array(V[a]) + np.array(V[b])) / 2))
+        return mid[key]
+    out = []
+    for a, b, c in F:
+        ab, bc, ca = m(a, b), m(b, c), m(c, a)
+        out += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+    return np.array(V), out
+
+
+def _box_faces(lo, hi):
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    V = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0], [x0, y0, z1], [x1, y0, z1], [x1, y1, z1],
+                  [x0, y1, z1]], float)
+    F = [(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4), (1, 2, 6), (1, 6, 5), (2, 3, 7), (2, 7, 6),
+         (3, 0, 4), (3, 4, 7)]
+    return V, F
+
+
+def _notched_block():
+    """an L-shaped prism (non-convex): the square [0,0.8]^2 minus [0.4,0.8]x[0.4,0.8], extruded over z in [0, 0.5]."""
+    P = [(0, 0), (0.8, 0), (0.8, 0.4), (0.4, 0.4), (0.4, 0.8), (0, 0.8)]
+    n = len(P)
+    V = [(x, y, 0.0) for x, y in P] + [(x, y, 0.5) for x, y in P]
+    F = [(0, 3, 1), (1, 3, 2), (0, 5, 3), (3, 5, 4)]                 # bottom (outward -z), fan of the L
+    F += [(n + a, n + c, n + b) for a, b, c in F]                      # top, reversed
+    for i in range(n):
+        j = (i + 1) % n
+        F += [(i, j, n + j), (i, n + j, n + i)]
+    return np.array(V), F
+
+
+def mesh3d_golden(root, dps=40):
+    ref = importlib.import_module("warpSPHBoundaries.mesh3d.reference")
+    import mpmath as mp
+    rng = np.random.default_rng(31)
+    meshes = {}
+    meshes["icosahedron"] = _icosahedron(0.6)
+    V2, F2 = _subdivide(*_icosahedron(0.6))
+    V2 = V2 / np.linalg.norm(V2, axis=1, keepdims=True) * 0.6 * (1 + 0.05 * rng.uniform(-1, 1, (len(V2), 1)))
+    meshes["icosphere1_jitter"] = (V2, F2)
+    meshes["cube"] = _box_faces((-0.3, -0.25, -0.2), (0.35, 0.3, 0.25))
+    meshes["notched"] = _notched_block()
+    base = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0), (1, 1, 0), (1, 0, 1), (0, 2, 0), (0, 1, 1), (0, 0, 2)]
+    g_alpha = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)]
+    cases = []
+    queries = {
+        "icosahedron": [((0.1, 0.2, 0.35), 0.3), ((0.0, 0.0, 0.0), 0.2), ((0.05, -0.1, 0.62), 0.25),
+                        ((0.3, 0.3, 0.3), 0.7), ((0.55, 0.0, 0.1), 0.15)],
+        "icosphere1_jitter": [((0.1, -0.2, 0.4), 0.3), ((0.4, 0.35, -0.1), 0.2), ((-0.2, 0.1, -0.63), 0.15)],
+        "cube": [((0.0, 0.0, 0.0), 0.15), ((0.3, 0.25, 0.2), 0.2), ((0.33, 0.0, 0.0), 0.1), ((0.5, 0.4, 0.3), 0.3),
+                 ((0.02, -0.03, 0.1), 0.6)],
+        "notched": [((0.5, 0.5, 0.25), 0.2), ((0.38, 0.42, 0.1), 0.15), ((0.2, 0.2, 0.45), 0.3),
+                    ((0.6, 0.2, 0.25), 0.12)],
+    }
+    for name, (V, F) in meshes.items():
+        for q, h in queries[name]:
+            for k in KERNELS:
+                with mp.workdps(dps):
+                    cs = ref.ClosedSurface([tuple(float(x) for x in v) for v in V], F, q)
+                    vals = [cs.moment(k, a, h) for a in base]
+                    for a in g_alpha:
+                        vals.extend(cs.kernel_gradient(k, a, h))
+                    H = cs.kernel_hessian(k, (0, 0, 0), h)
+                    vals.extend(H[i][j] for i in range(3) for j in range(i, 3))
+                    cases.append({"mesh": name, "kernel": k, "h": h, "query": list(q),
+                                  "values": [mp.nstr(v, 30) for v in vals]})
+            print("mesh3d", name, q, "done", flush=True)
+    out = {"meta": {"source": "mesh3d/reference.py ClosedSurface of the reference (mpmath, %d digits)" % dps,
+                    "values": "28 baseline channels in the request order of the 3-D contract: value moments "
+                              "alpha in (000,100,010,001,200,110,101,020,011,002), kernel-gradient moments "
+                              "(alpha, j) for alpha in (000,100,010,001), j = 0..2, Hessian (00,01,02,11,12,22); "
+                              "physical units (y = vertex - query, support h)"},
+           "meshes": {n: {"vertices": [[float(x) for x in v] for v in V], "faces": [list(map(int, f)) for f in F]}
+                      for n, (V, F) in meshes.items()},
+           "cases": cases}
+    (HERE / "mesh3d_golden.json").write_text(json.dumps(out, indent=1))
+    print("mesh3d_golden.json:", len(cases), "cases")
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     np2d, torch2d = load_reference(root)
@@ -182,3 +284,4 @@ if __name__ == "__main__":
     np2d_c1(np2d)
     torch2d_grads(torch2d)
     radial_golden(root)
+    mesh3d_golden(root)

@@ -1,0 +1,74 @@
+"""Host logic of the closed-surface family (no GPU): surface validation in the C ABI, request mapping, argument
+checks."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from warpsphboundaries_b200 import _lib
+from warpsphboundaries_b200.mesh3d import Evaluator, Geometry, _column
+from warpsphboundaries_b200.radial import Request, baseline
+
+
+def _tet():
+    V = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float)
+    F = np.array([[0, 2, 1], [0, 1, 3], [0, 3, 2], [1, 2, 3]], np.int32)
+    return V, F
+
+
+def _create(V, F, smax=0.1):
+    V = np.ascontiguousarray(V, np.float64)
+    F = np.ascontiguousarray(F, np.int32)
+    h = ctypes.c_void_p()
+    rc = _lib.lib.wsb_mesh_create(V.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(V),
+                                  F.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(F), smax, 0, ctypes.byref(h))
+    return rc, h
+
+
+def test_surface_checks_run_before_any_device_work():
+    V, F = _tet()
+    assert _create(V, F[:3])[0] == _lib.WSB_ERR_ARG                   # open (3 faces)
+    assert _create(V, F[:, ::-1])[0] == _lib.WSB_ERR_ARG              # inward normals: negative volume
+    bad = F.copy()
+    bad[0] = bad[0][::-1]
+    assert _create(V, bad)[0] == _lib.WSB_ERR_ARG                     # one face flipped: inconsistent orientation
+    bad = F.copy()
+    bad[1, 2] = 7
+    assert _create(V, bad)[0] == _lib.WSB_ERR_ARG                     # index out of range
+    assert _create(V, F, smax=0.0)[0] == _lib.WSB_ERR_ARG
+    Vd = V.copy()
+    Vd[3] = [0.5, 0.5, 0.0]                                           # flat: zero volume, degenerate faces
+    assert _create(Vd, F)[0] == _lib.WSB_ERR_ARG
+    assert "mesh_create" in _lib.last_error()
+
+
+def test_channel_abi_argument_errors():
+    f = _lib.lib.wsb_mesh_channels
+    assert f(None, 2, None, None, 4, None, None, None, 0, None) == _lib.WSB_ERR_ARG
+    assert _lib.lib.wsb_mesh_workspace_size(None, 10) == 0
+    assert _lib.lib.wsb_mesh_inside(None, None, 3, None, None) == _lib.WSB_ERR_ARG
+
+
+def test_request_columns():
+    b = baseline(3)
+    assert [_column(r) for r in b] == list(range(28))
+    assert _column(Request((0, 0, 0), (2, 0))) == _column(Request((0, 0, 0), (0, 2)))
+    assert _column(Request((1, 1, 0), (0,))) is None
+
+
+def test_evaluator_arguments():
+    V, F = _tet()
+    g = Geometry.closed_surface(V, F)
+    with pytest.raises(ValueError):
+        Evaluator(g, kernel="quintic")
+    with pytest.raises(NotImplementedError):
+        Evaluator(g, precision="float32")
+    with pytest.raises(NotImplementedError):
+        Evaluator(g, [Request((1, 1, 0), (0,))])
+    with pytest.raises(RuntimeError):
+        Evaluator(g, device="cpu")
+    ev = Evaluator(g)
+    with pytest.raises(ValueError):
+        ev.prepare([[0.1, 0.1, 0.1]], 0.0)
+    with pytest.raises(ValueError):
+        ev.prepare([[np.nan, 0.1, 0.1]], 0.1)

@@ -21,7 +21,8 @@ EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_d
            "wsb_aggregate_workspace_size", "wsb_aggregate", "wsb_aggregate_prepare", "wsb_aggregate_evaluate",
            "wsb_aggregate_noalloc",
            "wsb_aggregate_backward", "wsb_signed_distance",
-           "wsb_kinematics", "wsb_radial_channels"]
+           "wsb_kinematics", "wsb_radial_channels", "wsb_mesh_create", "wsb_mesh_destroy",
+           "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels"]
 
 
 class SurfaceInfo(ctypes.Structure):
@@ -58,6 +59,11 @@ def _load():
         "wsb_signed_distance": (c_int, [P, P, c_int64, c_double, P, P, P, P, P]),
         "wsb_kinematics": (c_int, [P, c_int32, P, c_int64, P, P, P, P, P]),
         "wsb_radial_channels": (c_int, [c_int, c_int, c_int, P, P, P, P, c_int64, I32P, c_int, P, P, P, P]),
+        "wsb_mesh_create": (c_int, [D, c_int64, I32P, c_int64, c_double, c_int, POINTER(c_void_p)]),
+        "wsb_mesh_destroy": (c_int, [P]),
+        "wsb_mesh_workspace_size": (c_size_t, [P, c_int64]),
+        "wsb_mesh_inside": (c_int, [P, P, c_int64, P, P]),
+        "wsb_mesh_channels": (c_int, [P, c_int, P, P, c_int64, P, P, P, c_size_t, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

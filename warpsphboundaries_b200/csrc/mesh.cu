@@ -1,0 +1,790 @@
+// Closed triangle surfaces in 3-D: the 28 baseline kernel integrals over the part of each query's support inside the
+// solid (value moments |alpha| <= 2, kernel-gradient moments |alpha| <= 1, the kernel Hessian).
+//
+// Reference: the closed-surface element of src/warpSPHBoundaries/fluxbridge/wp_func.py:119-333 (face -> edge
+// reductions, solid-angle term summed over every face), its exact mpmath counterpart
+// src/warpSPHBoundaries/mesh3d/reference.py:221-311 (ClosedSurface), the whole-element search of
+// fluxbridge/geometry.py:86-170 / device_search.py:158-212 and the per-query reduction of
+// fluxbridge/evaluate.py:177-187.
+//
+// Reduction (unit support: y = (vertex - query) / h, W~ = pi W):
+//  * volume -> faces.  For |alpha| = k, y y^alpha G_k(r) with (r^(3+k) G_k)' = r^(2+k) W~ has divergence y^alpha W~;
+//    splitting off the homogeneous field y y^alpha Q_k(1) / r^(3+k), whose flux through the closed surface is
+//    ind * int_{S^2} yhat^alpha (ind = 1 inside the solid), leaves the compact profile
+//    K_k = (Q_k(r) - Q_k(1)) / r^(3+k):   M_alpha = sum_faces z_f int_f y^alpha K_k dS + ind Q_k(1) int yhat^alpha.
+//    Kernel-gradient moments are -sum_f N_j int_f y^alpha W~ dS (+ alpha_j M_(alpha - e_j)); the Hessian is
+//    sum_f N_i int_f y_j W~'/r dS.  Only faces within the support contribute: no solid-angle sum over all faces.
+//  * face -> edges.  With y = z N + u (u in the face plane, r^2 = z^2 + |u|^2) and the compact potential
+//    A_F(r) = -int_r^1 t F(t) dt of a profile F:   int_f F = sum_e w_e int_e (A_F(r) - A_F(|z|)) / (r^2 - z^2) ds,
+//    int_f u F = sum_e mu_e int_e A_F ds,  int_f u u^T F = sum_e mu_e (x) int_e u A_F ds - P int_f A_F
+//    (w_e: signed distance of the foot point to the edge line, mu_e: in-plane outward edge normal, P = I - N N^T).
+//  * edges.  Beyond the support the first integrand is -A_F(|z|) / rho^2: an angle.  Inside, every integrand is a
+//    smooth function of s along the edge (a divided difference of a Laurent polynomial in r = sqrt(c^2 + s^2)); it is
+//    integrated by 12-node Gauss-Legendre on panels split at the foot of the perpendicular, at the kernel's knot and
+//    at distances c 2^k from the foot (the dyadic grading of the reference's stable route, edge/warpbc.py:522-575),
+//    which keeps the branch points s = +-ic of r away from every panel: relative error below 1e-12.
+//    Powers z^p multiply the profiles whose potentials hold r^-m (m <= p) so that every face term stays bounded as
+//    the query approaches the face plane.
+// The exact rational potentials are generated by warpsphboundaries_b200/kernels.py (mesh_tables, emit_mesh).
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <vector>
+
+#include "common.cuh"
+
+namespace wsb {
+
+struct Mesh {
+  int device = 0;
+  int64_t n_verts = 0, n_faces = 0;
+  double support_max = 0;
+  double lo[3] = {0, 0, 0};
+  double cell = 1;
+  int32_t nx = 1, ny = 1, nz = 1;
+  int64_t n_items = 0, n_col_items = 0;
+  double* fdata = nullptr;     // [n_faces * kFaceDoubles]
+  int32_t* fcell = nullptr;    // [n_faces * 3] lowest cell of the face's box
+  int32_t* fvid = nullptr;     // [n_faces * 3] vertex ids
+  int32_t* cstart = nullptr;   // [nx*ny*nz + 1]
+  int32_t* citems = nullptr;   // faces per cell
+  int32_t* colstart = nullptr; // [nx*ny + 1] faces per (x, y) column
+  int32_t* colitems = nullptr;
+};
+
+// per face: v0 v1 v2 (9), unit normal N (3), edge tangents t0 t1 t2 (9), edge normals mu_e = t_e x N (9),
+// edge lengths (3), box lo (3), box hi (3)
+constexpr int kFaceDoubles = 39;
+enum { kFV = 0, kFN = 9, kFT = 12, kFMU = 21, kFLEN = 30, kFLO = 33, kFHI = 36 };
+
+struct MeshView {
+  const double* fdata;
+  const int32_t* fcell;
+  const int32_t* fvid;
+  const int32_t* cstart;
+  const int32_t* citems;
+  const int32_t* colstart;
+  const int32_t* colitems;
+  double lo0, lo1, lo2, cell;
+  int32_t nx, ny, nz;
+};
+
+namespace {
+
+MeshView view_of(const Mesh* m) {
+  return MeshView{m->fdata, m->fcell, m->fvid, m->cstart, m->citems, m->colstart, m->colitems,
+                  m->lo[0], m->lo[1], m->lo[2], m->cell, m->nx, m->ny, m->nz};
+}
+
+__device__ __forceinline__ int cell_coord(double x, double lo, double cell, int n) {
+  const double f = floor((x - lo) / cell);
+  return f < -1.0 ? -2 : (f > (double)n ? n + 1 : (int)f);
+}
+
+// ------------------------------------------------------------------------------------------ inside indicator
+// Parity of the crossings of the vertical ray {(x, y, t): t > z} with the surface.  A face's projection owns the
+// point when every edge function is positive, or zero on an edge that the ownership rule gives to this side: edge
+// functions are evaluated with the edge's vertices in id order (so the two faces of an edge see exactly opposite
+// values) and an edge with zero value belongs to the face for which its counter-clockwise direction d has
+// d.y > 0 or (d.y == 0 and d.x < 0) -- exactly one of the two faces of a shared edge.
+// rounded products and differences (never contracted into an fma): a query on a vertex gives exactly 0, and the
+// two faces of an edge compute bit-identical values
+__device__ __forceinline__ double edge_fn(double ax, double ay, double bx, double by, double qx, double qy) {
+  return __dsub_rn(__dmul_rn(__dsub_rn(bx, ax), __dsub_rn(qy, ay)), __dmul_rn(__dsub_rn(by, ay), __dsub_rn(qx, ax)));
+}
+
+__device__ int mesh_inside(const MeshView& M, double x, double y, double z) {
+  const int ix = cell_coord(x, M.lo0, M.cell, M.nx), iy = cell_coord(y, M.lo1, M.cell, M.ny);
+  if (ix < 0 || iy < 0 || ix >= M.nx || iy >= M.ny) return 0;
+  const int col = iy * M.nx + ix;
+  int parity = 0;
+  for (int k = M.colstart[col]; k < M.colstart[col + 1]; ++k) {
+    const int f = M.colitems[k];
+    const double* F = M.fdata + (int64_t)f * kFaceDoubles;
+    const double nzf = F[kFN + 2];
+    if (nzf == 0.0) continue;                         // vertical face: its projection has no interior
+    const int* vid = M.fvid + 3 * f;
+    const double sgn = nzf > 0.0 ? 1.0 : -1.0;        // counter-clockwise projection for N.z > 0
+    bool in = true;
+    for (int e = 0; e < 3 && in; ++e) {
+      const int a = e, b = (e + 1) % 3;
+      const bool fwd = vid[a] < vid[b];
+      const double* A = F + kFV + 3 * (fwd ? a : b);
+      const double* B = F + kFV + 3 * (fwd ? b : a);
+      double E = edge_fn(A[0], A[1], B[0], B[1], x, y);
+      if (!fwd) E = -E;
+      E *= sgn;
+      if (E < 0.0) {
+        in = false;
+      } else if (E == 0.0) {
+        const double* P0 = F + kFV + 3 * a;
+        const double* P1 = F + kFV + 3 * b;
+        const double dx = (P1[0] - P0[0]) * sgn, dy = (P1[1] - P0[1]) * sgn;
+        if (!(dy > 0.0 || (dy == 0.0 && dx < 0.0))) in = false;
+      }
+    }
+    if (!in) continue;
+    const double zt = F[kFV + 2] - (F[kFN] * (x - F[kFV]) + F[kFN + 1] * (y - F[kFV + 1])) / nzf;
+    if (zt > z) parity ^= 1;
+  }
+  return parity;
+}
+
+// ------------------------------------------------------------------------------------------ candidate faces
+// The faces of the 27 cells around the query's cell whose box comes within h of the query; a face listed in several
+// of those cells is taken in one of them only (the lowest corner of its box inside the 27-cell block).
+template <class Visit>
+__device__ __forceinline__ void for_candidates(const MeshView& M, const double q[3], double h, Visit&& visit) {
+  const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
+            cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
+  const int x0 = max(cx - 1, 0), x1 = min(cx + 1, M.nx - 1), y0 = max(cy - 1, 0), y1 = min(cy + 1, M.ny - 1),
+            z0 = max(cz - 1, 0), z1 = min(cz + 1, M.nz - 1);
+  const double h2 = h * h;
+  for (int k = z0; k <= z1; ++k)
+    for (int j = y0; j <= y1; ++j)
+      for (int i = x0; i <= x1; ++i) {
+        const int c = (k * M.ny + j) * M.nx + i;
+        for (int it = M.cstart[c]; it < M.cstart[c + 1]; ++it) {
+          const int f = M.citems[it];
+          const int* fc = M.fcell + 3 * f;
+          if (max(fc[0], cx - 1) != i || max(fc[1], cy - 1) != j || max(fc[2], cz - 1) != k) continue;
+          const double* F = M.fdata + (int64_t)f * kFaceDoubles;
+          double d2 = 0.0;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const double dl = F[kFLO + a] - q[a], dh = q[a] - F[kFHI + a];
+            const double d = fmax(0.0, fmax(dl, dh));
+            d2 = fma(d, d, d2);
+          }
+          if (d2 < h2) visit(f);
+        }
+      }
+}
+
+// ------------------------------------------------------------------------------------------ profiles
+template <class M, int Fn>
+__device__ __forceinline__ double fpoly(int p, double x) {
+  if constexpr (M::kPieces > 1) {
+    if (p) return MeshFn<M, Fn>::poly1(x);
+  }
+  return MeshFn<M, Fn>::poly0(x);
+}
+template <class M, int Fn>
+__device__ __forceinline__ double fdd(int p, double x, double a) {
+  if constexpr (M::kPieces > 1) {
+    if (p) return MeshFn<M, Fn>::dd1(x, a);
+  }
+  return MeshFn<M, Fn>::dd0(x, a);
+}
+template <class M, int Fn>
+__device__ __forceinline__ double fnu(int p) {
+  if constexpr (M::kPieces > 1) {
+    if (p) return MeshFn<M, Fn>::kNu1;
+  }
+  return MeshFn<M, Fn>::kNu0;
+}
+template <int K>
+__device__ __forceinline__ double zpow(double z) {
+  if constexpr (K == 0) return 1.0;
+  else if constexpr (K == 1) return z;
+  else if constexpr (K == 2) return z * z;
+  else return z * z * z;
+}
+// sum_{i < m} x^i a^(m-1-i)
+template <int m>
+__device__ __forceinline__ double smix(double x, double a) {
+  if constexpr (m == 1) return 1.0;
+  else if constexpr (m == 2) return x + a;
+  else return fma(x, x + a, a * a);
+}
+template <class M>
+__device__ __forceinline__ int piece(double x) {
+  if constexpr (M::kPieces > 1) return x < M::kBreak ? 0 : 1;
+  return 0;
+}
+
+// A_F(r) (r inside the support)
+template <class M, int Fn>
+__device__ __forceinline__ double aval(double r) {
+  constexpr int m = MeshFn<M, Fn>::kNeg;
+  const int p = piece<M>(r);
+  double v = fpoly<M, Fn>(p, r);
+  if constexpr (m > 0) v += fnu<M, Fn>(p) / zpow<m>(r);
+  return v;
+}
+
+// z^ZP A_F(|z|), |z| = a (0 outside the support); sg = sign(z)
+template <class M, int Fn, int ZP>
+__device__ __forceinline__ double aval_a(double a, double z, double sg) {
+  constexpr int m = MeshFn<M, Fn>::kNeg;
+  static_assert(ZP >= m, "z power must absorb the negative power");
+  if (a >= 1.0) return 0.0;
+  const int p = piece<M>(a);
+  double v = fpoly<M, Fn>(p, a) * zpow<ZP>(z);
+  if constexpr (m > 0) v += fnu<M, Fn>(p) * zpow<ZP - m>(z) * zpow<m>(sg);
+  return v;
+}
+
+// z^ZP (A_F(r) - A_F(a)) / (r^2 - a^2) for a = |z| < r < 1; rpa = r + a, rma = r - a (from rho^2 / (r + a))
+template <class M, int Fn, int ZP>
+__device__ __forceinline__ double dd2(double r, double a, double z, double sg, double rpa, double rma) {
+  constexpr int m = MeshFn<M, Fn>::kNeg;
+  static_assert(ZP >= m, "z power must absorb the negative power");
+  const int pa = piece<M>(a);
+  double x1 = r;
+  bool split = false;
+  if constexpr (M::kPieces > 1) {
+    if (pa == 0 && r > M::kBreak) {
+      x1 = M::kBreak;
+      split = true;
+    }
+  }
+  double d0 = fdd<M, Fn>(pa, x1, a) * zpow<ZP>(z);
+  if constexpr (m > 0) d0 -= fnu<M, Fn>(pa) * smix<m>(x1, a) / zpow<m>(x1) * zpow<ZP - m>(z) * zpow<m>(sg);
+  if (!split) return d0 / rpa;
+  const double B = M::kBreak;
+  double d1 = fdd<M, Fn>(1, r, B);
+  if constexpr (m > 0) d1 -= fnu<M, Fn>(1) * smix<m>(r, B) / (zpow<m>(r) * zpow<m>(B));
+  d1 *= zpow<ZP>(z);
+  return ((B - a) * d0 + (r - B) * d1) / (rma * rpa);
+}
+
+__device__ __forceinline__ double angle_between(double w, double x0, double x1) {
+  return atan2(w * (x1 - x0), fma(w, w, x0 * x1));
+}
+
+// the 28 accumulators of one row (W~ units, unit support): M0, M1[3], M2[6] (00 01 02 11 12 22), G0[3],
+// G1[9] (i-major), H[6]
+enum { kAM0 = 0, kAM1 = 1, kAM2 = 4, kAG0 = 10, kAG1 = 13, kAH = 22 };
+struct Acc28 {
+  double v[28];
+};
+
+__device__ __forceinline__ void acc_zero(Acc28& A) {
+#pragma unroll
+  for (int i = 0; i < 28; ++i) A.v[i] = 0.0;
+}
+
+// symmetric index of (i, j), i <= j: 00 01 02 11 12 22
+__host__ __device__ constexpr int sym(int i, int j) { return i == 0 ? j : (i == 1 ? 2 + j : 5); }
+
+// per-edge integrals accumulated over the panels of one side of the foot point
+struct EdgeSums {
+  double J[6];   // w int z^p DD_F ds for A_K0 (p1) A_K1 (p2) A_K2 (p3) A_W A_L A2_K2 (p1)
+  double LK1, LK2, LK2b, TK2, LW, LL;   // int z A_K1, int z^2 A_K2, int z A_K2, int s z A_K2, int A_W, int A_L
+};
+
+template <class M>
+__device__ __forceinline__ void edge_panel(double x0, double x1, double sgn_side, double c2, double a, double z,
+                                           double sg, double w, EdgeSums& S) {
+  // x0 < x1 are distances |s| from the foot; s = sgn_side * u
+  const double hc = 0.5 * (x1 - x0), mc = 0.5 * (x1 + x0);
+#pragma unroll 2
+  for (int g = 0; g < kRadialGauss; ++g) {
+    const double u = fma(hc, kRadialGx[g], mc), wt = kRadialGw[g] * hc, s = sgn_side * u;
+    const double rho2 = fma(u, u, w * w);
+    const double r = sqrt(fma(u, u, c2));
+    const double rpa = r + a, rma = rho2 / rpa;
+    if (w != 0.0) {
+      const double ww = w * wt;
+      S.J[0] = fma(ww, dd2<M, 0, 1>(r, a, z, sg, rpa, rma), S.J[0]);
+      S.J[1] = fma(ww, dd2<M, 1, 2>(r, a, z, sg, rpa, rma), S.J[1]);
+      S.J[2] = fma(ww, dd2<M, 2, 3>(r, a, z, sg, rpa, rma), S.J[2]);
+      S.J[3] = fma(ww, dd2<M, 3, 0>(r, a, z, sg, rpa, rma), S.J[3]);
+      S.J[4] = fma(ww, dd2<M, 4, 0>(r, a, z, sg, rpa, rma), S.J[4]);
+      S.J[5] = fma(ww, dd2<M, 5, 1>(r, a, z, sg, rpa, rma), S.J[5]);
+    }
+    const double k1 = aval<M, 1>(r) * z, k2 = aval<M, 2>(r) * z;
+    S.LK1 = fma(wt, k1, S.LK1);
+    S.LK2b = fma(wt, k2, S.LK2b);
+    S.LK2 = fma(wt, k2 * z, S.LK2);
+    S.TK2 = fma(wt * s, k2, S.TK2);
+    S.LW = fma(wt, aval<M, 3>(r), S.LW);
+    S.LL = fma(wt, aval<M, 4>(r), S.LL);
+  }
+}
+
+// panels of [u0, u1] (distances from the foot on one side): split at the knot and at base * 2^k
+template <class M>
+__device__ __forceinline__ void edge_side(double u0, double u1, double sgn_side, double c, double c2, double a,
+                                          double z, double sg, double w, EdgeSums& S) {
+  if (!(u1 > u0)) return;
+  double knot = -1.0;
+  if constexpr (M::kPieces > 1) {
+    if (c < M::kBreak) knot = sqrt((M::kBreak - c) * (M::kBreak + c));
+  }
+  const double base = fmax(c, 1.0 / 16777216.0);
+  double d = base;
+  for (int it = 0; it < 64 && d <= u0; ++it) d *= 2.0;
+  double u = u0;
+  for (int it = 0; it < 96 && u < u1; ++it) {
+    double nxt = fmin(u1, d);
+    if (knot > u && knot < nxt) nxt = knot;
+    edge_panel<M>(u, nxt, sgn_side, c2, a, z, sg, w, S);
+    if (nxt >= d) d *= 2.0;
+    u = nxt;
+  }
+}
+
+// the contribution of face f to the row's accumulators; q in world units, ih = 1 / support
+template <class M>
+__device__ void face_contrib(const MeshView& Mv, int f, const double q[3], double ih, Acc28& A) {
+  const double* F = Mv.fdata + (int64_t)f * kFaceDoubles;
+  double P[3][3];
+#pragma unroll
+  for (int v = 0; v < 3; ++v)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) P[v][k] = (F[kFV + 3 * v + k] - q[k]) * ih;
+  const double N[3] = {F[kFN], F[kFN + 1], F[kFN + 2]};
+  const double z = N[0] * P[0][0] + N[1] * P[0][1] + N[2] * P[0][2];
+  const double a = fabs(z), sg = z > 0.0 ? 1.0 : (z < 0.0 ? -1.0 : 0.0);
+  double J[6] = {0, 0, 0, 0, 0, 0};
+  double I1K1[3] = {0, 0, 0}, I1K2[3] = {0, 0, 0}, I1W[3] = {0, 0, 0}, I1L[3] = {0, 0, 0};
+  double I2[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int e = 0; e < 3; ++e) {
+    const double t[3] = {F[kFT + 3 * e], F[kFT + 3 * e + 1], F[kFT + 3 * e + 2]};
+    const double mu[3] = {F[kFMU + 3 * e], F[kFMU + 3 * e + 1], F[kFMU + 3 * e + 2]};
+    const double len = F[kFLEN + e] * ih;
+    const double w = mu[0] * P[e][0] + mu[1] * P[e][1] + mu[2] * P[e][2];
+    const double lo = t[0] * P[e][0] + t[1] * P[e][1] + t[2] * P[e][2], hi = lo + len;
+    const double c2 = fma(z, z, w * w), c = sqrt(c2);
+    double s0 = 0.0, s1 = 0.0;
+    if (c < 1.0) {
+      const double L = sqrt((1.0 - c) * (1.0 + c));
+      s0 = fmax(lo, -L);
+      s1 = fmin(hi, L);
+    }
+    EdgeSums S;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) S.J[i] = 0.0;
+    S.LK1 = S.LK2 = S.LK2b = S.TK2 = S.LW = S.LL = 0.0;
+    if (w != 0.0) {
+      double out = 0.0;
+      if (s1 > s0) {
+        if (lo < s0) out += angle_between(w, lo, s0);
+        if (s1 < hi) out += angle_between(w, s1, hi);
+      } else {
+        out = angle_between(w, lo, hi);
+      }
+      if (out != 0.0) {
+        S.J[0] -= aval_a<M, 0, 1>(a, z, sg) * out;
+        S.J[1] -= aval_a<M, 1, 2>(a, z, sg) * out;
+        S.J[2] -= aval_a<M, 2, 3>(a, z, sg) * out;
+        S.J[3] -= aval_a<M, 3, 0>(a, z, sg) * out;
+        S.J[4] -= aval_a<M, 4, 0>(a, z, sg) * out;
+        S.J[5] -= aval_a<M, 5, 1>(a, z, sg) * out;
+      }
+    }
+    if (s1 > s0) {
+      // negative side: s in [s0, min(s1, 0)] -> u = -s in [max(-s1, 0), -s0]; positive side: s in [max(s0, 0), s1]
+      if (s0 < 0.0) edge_side<M>(fmax(-s1, 0.0), -s0, -1.0, c, c2, a, z, sg, w, S);
+      if (s1 > 0.0) edge_side<M>(fmax(s0, 0.0), s1, 1.0, c, c2, a, z, sg, w, S);
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) J[i] += S.J[i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      I1K1[k] = fma(mu[k], S.LK1, I1K1[k]);
+      I1K2[k] = fma(mu[k], S.LK2, I1K2[k]);
+      I1W[k] = fma(mu[k], S.LW, I1W[k]);
+      I1L[k] = fma(mu[k], S.LL, I1L[k]);
+    }
+    const double wl = w * S.LK2b;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) I2[3 * i + j] = fma(mu[i], fma(mu[j], wl, t[j] * S.TK2), I2[3 * i + j]);
+  }
+  // assembly (W~ units):  M0 = z I0[K0];  M1 = z^2 N I0[K1] + z I1[K1];
+  // M2 = z^3 N N^T I0[K2] + z^2 (N I1[K2]^T + I1[K2] N^T) + z I2[K2] - (I - N N^T) z I0[A_K2];
+  // S0 = I0[W~], S1 = z N I0[W~] + I1[W~]:  G0_j -= N_j S0,  G1_ij -= S1_i N_j;  H_ij += N_i (z N_j I0[L] + I1_j[L])
+  A.v[kAM0] += J[0];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) A.v[kAM1 + i] += N[i] * J[1] + I1K1[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) {
+      const double Pij = (i == j ? 1.0 : 0.0) - N[i] * N[j];
+      const double v = N[i] * N[j] * J[2] + N[i] * I1K2[j] + I1K2[i] * N[j] + 0.5 * (I2[3 * i + j] + I2[3 * j + i]) -
+                       Pij * J[5];
+      A.v[kAM2 + sym(i, j)] += v;
+    }
+  double S1[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    S1[i] = z * N[i] * J[3] + I1W[i];
+    A.v[kAG0 + i] -= N[i] * J[3];
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) A.v[kAG1 + 3 * i + j] -= S1[i] * N[j];
+  double HL[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) HL[j] = z * N[j] * J[4] + I1L[j];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) A.v[kAH + sym(i, j)] += 0.5 * (N[i] * HL[j] + N[j] * HL[i]);
+}
+
+// ------------------------------------------------------------------------------------------ kernels
+constexpr int kMeshThreads = 128;
+
+// per query: the inside test and whether any face is within the support; rows with faces are appended to `work`
+__global__ void __launch_bounds__(kMeshThreads) k_mesh_rowinfo(MeshView M, const double* __restrict__ pos,
+                                                              const double* __restrict__ sup, int64_t n,
+                                                              int32_t* __restrict__ ind, int32_t* __restrict__ work,
+                                                              int32_t* __restrict__ nwork) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool has = false;
+  if (row < n) {
+    const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
+    const double h = sup[row];
+    // a support above the grid cell would reach faces outside the 27-cell block: such rows (and non-finite input)
+    // are marked -1 and come back as NaN
+    const bool ok = h > 0.0 && h <= M.cell && isfinite(q[0]) && isfinite(q[1]) && isfinite(q[2]);
+    if (ok) {
+      ind[row] = mesh_inside(M, q[0], q[1], q[2]);
+      int cnt = 0;
+      for_candidates(M, q, h, [&](int) { ++cnt; });
+      has = cnt > 0;
+    } else {
+      ind[row] = -1;
+    }
+  }
+  // warp-aggregated append of the rows with candidate faces (their order is irrelevant: each row is computed alone)
+  const unsigned mask = __ballot_sync(0xffffffffu, has);
+  if (mask) {
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(nwork, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (has) work[base + __popc(mask & ((1u << lane) - 1))] = (int32_t)row;
+  }
+}
+
+template <class M>
+__device__ __forceinline__ void write_row(double* __restrict__ out, int64_t row, const Acc28& A, double ind, double h) {
+  const double ip = kInvPi;
+  const double M0 = A.v[kAM0] * ip + ind * 4.0 * M::kQ0;
+  const double m2c = ind * (4.0 / 3.0) * M::kQ2;
+  const double h2 = h * h, ih = 1.0 / h, ih2 = ih * ih;
+  double* o = out + row * 28;
+  o[0] = M0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) o[1 + i] = A.v[kAM1 + i] * ip * h;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) o[4 + k] = (A.v[kAM2 + k] * ip + (k == 0 || k == 3 || k == 5 ? m2c : 0.0)) * h2;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) o[10 + i] = A.v[kAG0 + i] * ip * ih;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) o[13 + 3 * i + j] = A.v[kAG1 + 3 * i + j] * ip + (i == j ? M0 : 0.0);
+#pragma unroll
+  for (int k = 0; k < 6; ++k) o[22 + k] = A.v[kAH + k] * ip * ih2;
+}
+
+// rows without faces in their support: whole-support constants inside, zeros outside, NaN for invalid rows
+template <class M>
+__global__ void __launch_bounds__(kMeshThreads) k_mesh_rows(const double* __restrict__ sup, int64_t n,
+                                                           const int32_t* __restrict__ ind, double* __restrict__ out) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  if (ind[row] < 0) {
+    for (int k = 0; k < 28; ++k) out[row * 28 + k] = __longlong_as_double(0x7ff8000000000000LL);
+    return;
+  }
+  Acc28 A;
+  acc_zero(A);
+  write_row<M>(out, row, A, (double)ind[row], sup[row]);
+}
+
+// G lanes per work row; lane k takes the row's candidate faces k, k + G, ...; the lanes' sums are combined by a
+// fixed butterfly, so a row's result does not depend on the launch
+template <class M, int G>
+__global__ void __launch_bounds__(kMeshThreads) k_mesh_eval(MeshView Mv, const double* __restrict__ pos,
+                                                           const double* __restrict__ sup,
+                                                           const int32_t* __restrict__ ind,
+                                                           const int32_t* __restrict__ work,
+                                                           const int32_t* __restrict__ nwork,
+                                                           double* __restrict__ out) {
+  const int lane = threadIdx.x % G;
+  const int64_t slot = ((int64_t)blockIdx.x * kMeshThreads + threadIdx.x) / G;
+  const int64_t nw = *nwork;
+  const bool active = slot < nw;
+  Acc28 A;
+  acc_zero(A);
+  int64_t row = 0;
+  double h = 1.0;
+  if (active) {
+    row = work[slot];
+    const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
+    h = sup[row];
+    const double ih = 1.0 / h;
+    int k = 0;
+    for_candidates(Mv, q, h, [&](int f) {
+      if (k % G == lane) face_contrib<M>(Mv, f, q, ih, A);
+      ++k;
+    });
+  }
+  // butterfly over the G lanes of the row (every lane of the warp takes part)
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+#pragma unroll
+    for (int i = 0; i < 28; ++i) A.v[i] += __shfl_xor_sync(0xffffffffu, A.v[i], off, G);
+  }
+  if (active && lane == 0) write_row<M>(out, row, A, (double)ind[row], h);
+}
+
+__global__ void k_mesh_inside_only(MeshView M, const double* __restrict__ pos, int64_t n, int32_t* __restrict__ ind) {
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  ind[row] = mesh_inside(M, pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]);
+}
+
+template <typename T>
+int upload_vec(T** dst, const std::vector<T>& src) {
+  const size_t bytes = std::max<size_t>(src.size(), 1) * sizeof(T);
+  WSB_CUDA(cudaMalloc((void**)dst, bytes));
+  if (!src.empty()) WSB_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return WSB_OK;
+}
+
+void free_mesh(Mesh* m) {
+  void* ptrs[] = {m->fdata, m->fcell, m->fvid, m->cstart, m->citems, m->colstart, m->colitems};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+}
+
+inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <class M>
+int launch_mesh(const Mesh* m, const double* pos, const double* sup, int64_t n, double* out, int32_t* ind,
+                int32_t* work, int32_t* nwork, cudaStream_t st) {
+  const MeshView v = view_of(m);
+  const unsigned grid = (unsigned)((n + kMeshThreads - 1) / kMeshThreads);
+  WSB_CUDA(cudaMemsetAsync(nwork, 0, sizeof(int32_t), st));
+  k_mesh_rowinfo<<<grid, kMeshThreads, 0, st>>>(v, pos, sup, n, ind, work, nwork);
+  WSB_CUDA(cudaGetLastError());
+  k_mesh_rows<M><<<grid, kMeshThreads, 0, st>>>(sup, n, ind, out);
+  WSB_CUDA(cudaGetLastError());
+  constexpr int G = 4;
+  const unsigned egrid = (unsigned)((n * G + kMeshThreads - 1) / kMeshThreads);
+  k_mesh_eval<M, G><<<egrid, kMeshThreads, 0, st>>>(v, pos, sup, ind, work, nwork, out);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+}  // namespace
+}  // namespace wsb
+
+using namespace wsb;
+
+struct wsb_mesh : public Mesh {};
+
+extern "C" int wsb_mesh_create(const double* verts, int64_t n_verts, const int32_t* faces, int64_t n_faces,
+                               double support_max, int device, wsb_mesh** out) {
+  if (!out) return fail(WSB_ERR_ARG, "wsb_mesh_create: NULL handle pointer");
+  *out = nullptr;
+  if (!verts || !faces || n_verts < 3 || n_faces < 4)
+    return fail(WSB_ERR_ARG, "wsb_mesh_create: a closed surface needs >= 3 vertices and >= 4 faces");
+  if (n_faces > (int64_t)(INT32_MAX / 8)) return fail(WSB_ERR_SIZE, "wsb_mesh_create: too many faces");
+  if (!(support_max > 0.0) || !std::isfinite(support_max))
+    return fail(WSB_ERR_ARG, "wsb_mesh_create: support_max must be positive and finite");
+  for (int64_t i = 0; i < 3 * n_verts; ++i)
+    if (!std::isfinite(verts[i])) return fail(WSB_ERR_ARG, "wsb_mesh_create: non-finite vertex");
+  // watertight, consistently oriented 2-manifold: every undirected edge twice, once in each direction
+  std::map<std::pair<int32_t, int32_t>, int> dir;
+  for (int64_t f = 0; f < n_faces; ++f) {
+    const int32_t* v = faces + 3 * f;
+    for (int k = 0; k < 3; ++k)
+      if (v[k] < 0 || v[k] >= n_verts) return fail(WSB_ERR_ARG, "wsb_mesh_create: face index out of range");
+    if (v[0] == v[1] || v[1] == v[2] || v[0] == v[2]) return fail(WSB_ERR_ARG, "wsb_mesh_create: repeated vertex");
+    for (int k = 0; k < 3; ++k) {
+      const int32_t a = v[k], b = v[(k + 1) % 3];
+      const auto key = std::make_pair(std::min(a, b), std::max(a, b));
+      const int bit = a < b ? 1 : 2;
+      int& d = dir[key];
+      if (d & bit) return fail(WSB_ERR_ARG, "wsb_mesh_create: surface must be watertight and consistently oriented");
+      d |= bit;
+    }
+  }
+  for (const auto& kv : dir)
+    if (kv.second != 3) return fail(WSB_ERR_ARG, "wsb_mesh_create: surface must be watertight and consistently oriented");
+  // face records, box, signed volume (relative to the first vertex: outward normals give a positive volume)
+  double vol6 = 0.0;
+  const double* o = verts;
+  std::vector<double> hf((size_t)n_faces * kFaceDoubles);
+  std::vector<int32_t> hvid((size_t)n_faces * 3);
+  double blo[3] = {INFINITY, INFINITY, INFINITY}, bhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t f = 0; f < n_faces; ++f) {
+    const int32_t* v = faces + 3 * f;
+    double P[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int k = 0; k < 3; ++k) P[i][k] = verts[3 * v[i] + k];
+    const double a[3] = {P[0][0] - o[0], P[0][1] - o[1], P[0][2] - o[2]};
+    const double b[3] = {P[1][0] - o[0], P[1][1] - o[1], P[1][2] - o[2]};
+    const double c[3] = {P[2][0] - o[0], P[2][1] - o[1], P[2][2] - o[2]};
+    vol6 += a[0] * (b[1] * c[2] - b[2] * c[1]) - a[1] * (b[0] * c[2] - b[2] * c[0]) + a[2] * (b[0] * c[1] - b[1] * c[0]);
+    double* F = hf.data() + f * kFaceDoubles;
+    for (int i = 0; i < 3; ++i)
+      for (int k = 0; k < 3; ++k) F[kFV + 3 * i + k] = P[i][k];
+    const double e1[3] = {P[1][0] - P[0][0], P[1][1] - P[0][1], P[1][2] - P[0][2]};
+    const double e2[3] = {P[2][0] - P[0][0], P[2][1] - P[0][1], P[2][2] - P[0][2]};
+    const double N[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    const double nl = std::sqrt(N[0] * N[0] + N[1] * N[1] + N[2] * N[2]);
+    if (!(nl > 0.0)) return fail(WSB_ERR_ARG, "wsb_mesh_create: degenerate (zero-area) face");
+    for (int k = 0; k < 3; ++k) F[kFN + k] = N[k] / nl;
+    for (int e = 0; e < 3; ++e) {
+      const double* A = P[e];
+      const double* B = P[(e + 1) % 3];
+      double t[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
+      const double len = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+      for (int k = 0; k < 3; ++k) t[k] /= len;
+      const double* n = F + kFN;
+      const double mu[3] = {t[1] * n[2] - t[2] * n[1], t[2] * n[0] - t[0] * n[2], t[0] * n[1] - t[1] * n[0]};
+      for (int k = 0; k < 3; ++k) {
+        F[kFT + 3 * e + k] = t[k];
+        F[kFMU + 3 * e + k] = mu[k];
+      }
+      F[kFLEN + e] = len;
+    }
+    for (int k = 0; k < 3; ++k) {
+      F[kFLO + k] = std::min(P[0][k], std::min(P[1][k], P[2][k]));
+      F[kFHI + k] = std::max(P[0][k], std::max(P[1][k], P[2][k]));
+      blo[k] = std::min(blo[k], F[kFLO + k]);
+      bhi[k] = std::max(bhi[k], F[kFHI + k]);
+      hvid[3 * f + k] = v[k];
+    }
+  }
+  if (!(vol6 > 0.0)) return fail(WSB_ERR_ARG, "wsb_mesh_create: surface must have positive signed volume");
+  // cell grid over the box grown by one cell; the cell is support_max, enlarged if the grid would pass 2^26 cells
+  double cell = support_max;
+  int64_t nx = 0, ny = 0, nz = 0;
+  double lo[3] = {0, 0, 0};
+  for (int tries = 0; tries < 64; ++tries) {
+    for (int k = 0; k < 3; ++k) lo[k] = blo[k] - cell;
+    nx = (int64_t)std::floor((bhi[0] + cell - lo[0]) / cell) + 1;
+    ny = (int64_t)std::floor((bhi[1] + cell - lo[1]) / cell) + 1;
+    nz = (int64_t)std::floor((bhi[2] + cell - lo[2]) / cell) + 1;
+    if (nx * ny * nz <= ((int64_t)1 << 26)) break;
+    cell *= 1.5;
+  }
+  const int64_t n3[3] = {nx, ny, nz};
+  auto cidx = [&](double x, int k) {
+    const int64_t i = (int64_t)std::floor((x - lo[k]) / cell);
+    return std::min<int64_t>(std::max<int64_t>(i, 0), n3[k] - 1);
+  };
+  const int64_t ncell = nx * ny * nz, ncol = nx * ny;
+  std::vector<int64_t> cnt(ncell + 1, 0), ccnt(ncol + 1, 0);
+  std::vector<int32_t> fcell((size_t)n_faces * 3);
+  std::vector<int64_t> range((size_t)n_faces * 6);
+  for (int64_t f = 0; f < n_faces; ++f) {
+    const double* F = hf.data() + f * kFaceDoubles;
+    for (int k = 0; k < 3; ++k) {
+      range[6 * f + 2 * k] = cidx(F[kFLO + k], k);
+      range[6 * f + 2 * k + 1] = cidx(F[kFHI + k], k);
+      fcell[3 * f + k] = (int32_t)range[6 * f + 2 * k];
+    }
+    for (int64_t kz = range[6 * f + 4]; kz <= range[6 * f + 5]; ++kz)
+      for (int64_t jy = range[6 * f + 2]; jy <= range[6 * f + 3]; ++jy)
+        for (int64_t ix = range[6 * f]; ix <= range[6 * f + 1]; ++ix) ++cnt[(kz * ny + jy) * nx + ix + 1];
+    for (int64_t jy = range[6 * f + 2]; jy <= range[6 * f + 3]; ++jy)
+      for (int64_t ix = range[6 * f]; ix <= range[6 * f + 1]; ++ix) ++ccnt[jy * nx + ix + 1];
+  }
+  for (int64_t c = 0; c < ncell; ++c) cnt[c + 1] += cnt[c];
+  for (int64_t c = 0; c < ncol; ++c) ccnt[c + 1] += ccnt[c];
+  if (cnt[ncell] > INT32_MAX || ccnt[ncol] > INT32_MAX)
+    return fail(WSB_ERR_SIZE, "wsb_mesh_create: cell lists exceed 2^31 items");
+  std::vector<int32_t> items((size_t)cnt[ncell]), citems((size_t)ccnt[ncol]);
+  std::vector<int32_t> start(cnt.begin(), cnt.end()), cstart(ccnt.begin(), ccnt.end());
+  {
+    std::vector<int64_t> cur(cnt.begin(), cnt.end() - 1), ccur(ccnt.begin(), ccnt.end() - 1);
+    for (int64_t f = 0; f < n_faces; ++f) {
+      for (int64_t kz = range[6 * f + 4]; kz <= range[6 * f + 5]; ++kz)
+        for (int64_t jy = range[6 * f + 2]; jy <= range[6 * f + 3]; ++jy)
+          for (int64_t ix = range[6 * f]; ix <= range[6 * f + 1]; ++ix)
+            items[cur[(kz * ny + jy) * nx + ix]++] = (int32_t)f;
+      for (int64_t jy = range[6 * f + 2]; jy <= range[6 * f + 3]; ++jy)
+        for (int64_t ix = range[6 * f]; ix <= range[6 * f + 1]; ++ix) citems[ccur[jy * nx + ix]++] = (int32_t)f;
+    }
+  }
+  WSB_CUDA(cudaSetDevice(device));
+  Mesh* m = new wsb_mesh();
+  m->device = device;
+  m->n_verts = n_verts;
+  m->n_faces = n_faces;
+  m->support_max = support_max;
+  for (int k = 0; k < 3; ++k) m->lo[k] = lo[k];
+  m->cell = cell;
+  m->nx = (int32_t)nx;
+  m->ny = (int32_t)ny;
+  m->nz = (int32_t)nz;
+  m->n_items = (int64_t)items.size();
+  m->n_col_items = (int64_t)citems.size();
+  int rc;
+  if ((rc = upload_vec(&m->fdata, hf)) || (rc = upload_vec(&m->fcell, fcell)) || (rc = upload_vec(&m->fvid, hvid)) ||
+      (rc = upload_vec(&m->cstart, start)) || (rc = upload_vec(&m->citems, items)) ||
+      (rc = upload_vec(&m->colstart, cstart)) || (rc = upload_vec(&m->colitems, citems))) {
+    free_mesh(m);
+    delete m;
+    return rc;
+  }
+  *out = static_cast<wsb_mesh*>(m);
+  return WSB_OK;
+}
+
+extern "C" int wsb_mesh_destroy(wsb_mesh* m) {
+  if (!m) return WSB_OK;
+  cudaSetDevice(m->device);
+  free_mesh(m);
+  delete m;
+  return WSB_OK;
+}
+
+extern "C" size_t wsb_mesh_workspace_size(const wsb_mesh* m, int64_t n) {
+  if (!m || n < 0) return 0;
+  return al256(sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)) * 2 + 256;
+}
+
+extern "C" int wsb_mesh_inside(const wsb_mesh* m, const double* pos, int64_t n, int32_t* inside, void* stream) {
+  if (!m) return fail(WSB_ERR_ARG, "wsb_mesh_inside: NULL mesh");
+  if (n < 0) return fail(WSB_ERR_ARG, "wsb_mesh_inside: negative size");
+  if (n == 0) return WSB_OK;
+  if (!pos || !inside) return fail(WSB_ERR_ARG, "wsb_mesh_inside: NULL array");
+  WSB_CUDA(cudaSetDevice(m->device));
+  k_mesh_inside_only<<<(unsigned)((n + kMeshThreads - 1) / kMeshThreads), kMeshThreads, 0, (cudaStream_t)stream>>>(
+      view_of(m), pos, n, inside);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+extern "C" int wsb_mesh_channels(const wsb_mesh* m, int kernel, const double* pos, const double* sup, int64_t n,
+                                 double* out, int32_t* inside, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!m) return fail(WSB_ERR_ARG, "wsb_mesh_channels: NULL mesh");
+  if (n < 0) return fail(WSB_ERR_ARG, "wsb_mesh_channels: negative size");
+  if (kernel < 0 || kernel > WSB_KERNEL_W6)
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_mesh_channels: closed surfaces serve cubic, w2, w4, w6");
+  if (n == 0) return WSB_OK;
+  if (!pos || !sup || !out || !workspace) return fail(WSB_ERR_ARG, "wsb_mesh_channels: NULL array");
+  if (n > (int64_t)INT32_MAX / 8) return fail(WSB_ERR_SIZE, "wsb_mesh_channels: more than 2^28 queries");
+  if (workspace_bytes < wsb_mesh_workspace_size(m, n))
+    return fail(WSB_ERR_SIZE, "wsb_mesh_channels: workspace smaller than wsb_mesh_workspace_size");
+  WSB_CUDA(cudaSetDevice(m->device));
+  char* base = (char*)workspace;
+  const size_t s = al256(sizeof(int32_t) * (size_t)n);
+  int32_t* work = (int32_t*)base;
+  int32_t* ind = inside ? inside : (int32_t*)(base + s);
+  int32_t* nwork = (int32_t*)(base + 2 * s);
+  cudaStream_t st = (cudaStream_t)stream;
+  switch (kernel) {
+    case WSB_KERNEL_CUBIC: return launch_mesh<Mesh_cubic>(m, pos, sup, n, out, ind, work, nwork, st);
+    case WSB_KERNEL_W2: return launch_mesh<Mesh_w2>(m, pos, sup, n, out, ind, work, nwork, st);
+    case WSB_KERNEL_W4: return launch_mesh<Mesh_w4>(m, pos, sup, n, out, ind, work, nwork, st);
+    default: return launch_mesh<Mesh_w6>(m, pos, sup, n, out, ind, work, nwork, st);
+  }
+}

@@ -417,6 +417,7 @@ def emit_header() -> str:
     out.append("static const double kPlanRadii[kPlanNumRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
     out.append("")
     out.extend(emit_radial())
+    out.extend(emit_mesh())
     out.append("}  // namespace wsb")
     out.append("")
     return "\n".join(out)
@@ -492,6 +493,129 @@ def radial(name: str):
         dell = {n - 1: n * x for n, x in ell.items() if n != 0}
         out.append((lo, hi, *(RadialProfile(*_factor_laurent(t, hi)) for t in (w, ell, dell))))
     return tuple(out), c3pi
+
+
+# ------------------------------------------------------------------ 3-D closed surfaces (face -> edge reductions)
+MESH_FUNCS = ("A_K0", "A_K1", "A_K2", "A_W", "A_L", "A2_K2")
+
+
+def _leval(d, x):
+    """value of the Laurent polynomial {exponent: coefficient} at x (x > 0 wherever a negative exponent is used)."""
+    return sum((c * F(x) ** e for e, c in d.items() if c), F(0))
+
+
+def _compact_potential(bounds, fp):
+    """per piece the Laurent polynomial A_p with A' = r f and A(r) = -int_r^1 t f(t) dt (zero from r = 1 on)."""
+    prims = []
+    for f in fp:
+        prim = {}
+        for n, c in f.items():
+            if n + 2 == 0:
+                raise AssertionError("logarithmic term in a compact potential")
+            prim[n + 2] = prim.get(n + 2, F(0)) + c / (n + 2)
+        prims.append(prim)
+    out = []
+    for p, ((lo, hi), prim) in enumerate(zip(bounds, prims)):
+        tail = sum((_leval(prims[q], bounds[q][1]) - _leval(prims[q], bounds[q][0]) for q in range(p + 1, len(bounds))),
+                   F(0))
+        d = dict(prim)
+        d[0] = d.get(0, F(0)) - _leval(prim, hi) - tail
+        out.append({e: c for e, c in d.items() if c})
+    return out
+
+
+@lru_cache(maxsize=None)
+def mesh_tables(name: str):
+    """exact tables of the closed-surface reduction of `name` (unit support, W~ = c3*pi * shape = pi * W):
+    {"bounds": [(lo, hi)] per piece, "Q": (Q0(1), Q1(1), Q2(1)) with Q_k(r) = int_0^r t^(2+k) W~ dt,
+     "funcs": {name: [Laurent dict per piece]} for the compact potentials
+        A_K0, A_K1, A_K2  of K_k(r) = (Q_k(r) - Q_k(1)) / r^(3+k)   (volume potentials of the value moments),
+        A_W, A_L          of W~ and L = W~'/r,
+        A2_K2             of r -> A_K2(r) (the trace term of the in-plane second moment)}."""
+    raw = _pieces(name)
+    c3pi = radial(name)[1]
+    bounds = [(lo, hi) for lo, hi, _ in raw]
+    Wp = [{n: c3pi * c for n, c in enumerate(co) if c} for _, _, co in raw]
+    Lp = [{n - 2: n * c for n, c in w.items() if n >= 1} for w in Wp]
+    Q, K = [], []
+    for k in range(3):
+        pieces, acc = [], F(0)
+        for (lo, hi), w in zip(bounds, Wp):
+            prim = {n + 3 + k: c / (n + 3 + k) for n, c in w.items()}
+            d = dict(prim)
+            d[0] = d.get(0, F(0)) + acc - _leval(prim, lo)
+            pieces.append(d)
+            acc += _leval(prim, hi) - _leval(prim, lo)
+        Q.append(acc)
+        Kk = []
+        for d in pieces:
+            kd = {}
+            for e, c in d.items():
+                kd[e - 3 - k] = kd.get(e - 3 - k, F(0)) + c
+            kd[-3 - k] = kd.get(-3 - k, F(0)) - acc
+            Kk.append({e: c for e, c in kd.items() if c})
+        K.append(Kk)
+    funcs = {"A_K0": _compact_potential(bounds, K[0]), "A_K1": _compact_potential(bounds, K[1]),
+             "A_K2": _compact_potential(bounds, K[2]), "A_W": _compact_potential(bounds, Wp),
+             "A_L": _compact_potential(bounds, Lp)}
+    funcs["A2_K2"] = _compact_potential(bounds, funcs["A_K2"])
+    for fname, pcs in funcs.items():
+        negs = {e for d in pcs for e in d if e < 0}
+        if len(negs) > 1:
+            raise AssertionError(f"{name} {fname}: more than one negative power {negs}")
+    return {"bounds": bounds, "Q": tuple(Q), "funcs": funcs}
+
+
+def mesh_negative_power(name, fname):
+    pcs = mesh_tables(name)["funcs"][fname]
+    negs = {e for d in pcs for e in d if e < 0}
+    return -min(negs) if negs else 0
+
+
+def _emit_dd(coeffs, x, a):
+    """C++ statements computing (P(x) - P(a)) / (x - a) into `dd` for P = sum coeffs[n] x^n (n >= 0): the synthetic
+    division by (x - a) evaluated by Horner's rule, no cancellation between P(x) and P(a)."""
+    cs = list(coeffs)
+    while len(cs) > 1 and cs[-1] == 0:
+        cs.pop()
+    D = len(cs) - 1
+    if D < 1:
+        return ["dd = 0.0;"]
+    out = [f"double b = {_lit(cs[D])}; dd = b;"]
+    for j in range(D - 2, -1, -1):
+        out.append(f"b = fma({a}, b, {_lit(cs[j + 1])}); dd = fma(dd, {x}, b);")
+    return out
+
+
+def emit_mesh() -> list:
+    """generated device code of the closed-surface family: per kernel and compact potential the polynomial part's value
+    and divided difference per piece, the negative power and its coefficient."""
+    out = ["// ---- 3-D closed surfaces: compact potentials (unit support, W~ = c3*pi * shape); function ids:",
+           "//      0 A_K0, 1 A_K1, 2 A_K2, 3 A_W, 4 A_L, 5 A2_K2",
+           "template <class M, int Fn> struct MeshFn;"]
+    for name in RADIAL_KERNELS:
+        t = mesh_tables(name)
+        bounds = t["bounds"]
+        out.append(f"struct Mesh_{name} {{")
+        out.append(f"  static constexpr int kPieces = {len(bounds)};")
+        out.append(f"  static constexpr double kBreak = {_lit(bounds[0][1]) if len(bounds) > 1 else '2.0'};   // end of the inner piece")
+        out.append(f"  static constexpr double kQ0 = {_lit(t['Q'][0])}, kQ1 = {_lit(t['Q'][1])}, kQ2 = {_lit(t['Q'][2])};")
+        out.append("};")
+        for fi, fname in enumerate(MESH_FUNCS):
+            pcs = t["funcs"][fname]
+            m = mesh_negative_power(name, fname)
+            out.append(f"template <> struct MeshFn<Mesh_{name}, {fi}> {{   // {fname}")
+            out.append(f"  static constexpr int kNeg = {m};")
+            for p, d in enumerate(pcs):
+                poly = [d.get(n, F(0)) for n in range(max([e for e in d if e >= 0], default=0) + 1)]
+                nu = d.get(-m, F(0)) if m else F(0)
+                out.append(f"  static constexpr double kNu{p} = {_lit(nu)};")
+                out.append(f"  __host__ __device__ static __forceinline__ double poly{p}(double x) {{ return {_horner(poly, 'x')}; }}")
+                body = " ".join(_emit_dd(poly, "x", "a"))
+                out.append(f"  __host__ __device__ static __forceinline__ double dd{p}(double x, double a) {{ double dd; {body} return dd; }}")
+            out.append("};")
+    out.append("")
+    return out
 
 
 def _radial_eval(prof, var, hi_lit, T):

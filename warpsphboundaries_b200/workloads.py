@@ -94,3 +94,55 @@ def edges_of(loops):
         E.append(np.stack([off + np.arange(n), off + (np.arange(n) + 1) % n], 1))
         off += n
     return np.concatenate(V), np.concatenate(E)
+
+
+# ------------------------------------------------------------------ 3-D closed surfaces
+def icosphere(subdivisions, radius=0.6, jitter=0.0, seed=0):
+    """(vertices [V, 3], faces [F, 3]) of an icosahedron subdivided `subdivisions` times (20 * 4^k outward faces),
+    projected to the sphere of `radius`, each vertex radius then scaled by (1 + jitter U(-1, 1)) (seeded)."""
+    t = (1 + 5 ** 0.5) / 2
+    V = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    V = [tuple(np.asarray(v, float) / np.linalg.norm(v)) for v in V]
+    Fc = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+          (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+          (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        mid = {}
+
+        def m(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                p = (np.asarray(V[a]) + np.asarray(V[b])) / 2
+                mid[key] = len(V)
+                V.append(tuple(p / np.linalg.norm(p)))
+            return mid[key]
+        out = []
+        for a, b, c in Fc:
+            ab, bc, ca = m(a, b), m(b, c), m(c, a)
+            out += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        Fc = out
+    V = np.asarray(V) * radius
+    if jitter:
+        rng = np.random.default_rng(seed)
+        V = V * (1 + jitter * rng.uniform(-1, 1, (len(V), 1)))
+    return V, np.asarray(Fc, dtype=np.int32)
+
+
+def box_mesh(lo, hi):
+    """(vertices, faces) of an axis-aligned box, two outward triangles per side."""
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    V = np.array([[x0, y0, z0], [x1, y0, z0], [x1, y1, z0], [x0, y1, z0], [x0, y0, z1], [x1, y0, z1], [x1, y1, z1],
+                  [x0, y1, z1]], float)
+    Fc = np.array([(0, 2, 1), (0, 3, 2), (4, 5, 6), (4, 6, 7), (0, 1, 5), (0, 5, 4), (1, 2, 6), (1, 6, 5), (2, 3, 7),
+                   (2, 7, 6), (3, 0, 4), (3, 4, 7)], dtype=np.int32)
+    return V, Fc
+
+
+def c3(n_particles=1 << 21, seed=0, h=0.03, subdivisions=5):
+    """the 3-D scene: 2^21 particles uniform in [-1, 1]^3, h = 0.03, an icosphere of 20 * 4^5 = 20480 faces, radius
+    0.6, vertex radii jittered by 5 % (seeded)."""
+    V, Fc = icosphere(subdivisions, 0.6, 0.05, seed + 21)
+    rng = np.random.default_rng(seed + 22)
+    return V, Fc, rng.uniform(-1.0, 1.0, size=(n_particles, 3)), h
