@@ -646,6 +646,8 @@ template <> __host__ __device__ __forceinline__ void Rad_w6::eval<0, float>(floa
 // ---- 3-D closed surfaces: compact potentials (unit support, W~ = c3*pi * shape); function ids:
 //      0 A_K0, 1 A_K1, 2 A_K2, 3 A_W, 4 A_L, 5 A2_K2
 template <class M, int Fn> struct MeshFn;
+static __device__ const double kMeshGx8[8] = {-0.9602898564975362, -0.7966664774136267, -0.525532409916329, -0.18343464249564978, 0.18343464249564978, 0.525532409916329, 0.7966664774136267, 0.9602898564975362};
+static __device__ const double kMeshGw8[8] = {0.10122853629037706, 0.22238103445337443, 0.3137066458778869, 0.36268378337836166, 0.36268378337836166, 0.3137066458778869, 0.22238103445337443, 0.10122853629037706};
 struct Mesh_cubic {
   static constexpr int kPieces = 2;
   static constexpr double kBreak = 0.5;   // end of the inner piece

@@ -590,9 +590,13 @@ def _emit_dd(coeffs, x, a):
 def emit_mesh() -> list:
     """generated device code of the closed-surface family: per kernel and compact potential the polynomial part's value
     and divided difference per piece, the negative power and its coefficient."""
+    import numpy as np
+    x8, w8 = np.polynomial.legendre.leggauss(8)
     out = ["// ---- 3-D closed surfaces: compact potentials (unit support, W~ = c3*pi * shape); function ids:",
            "//      0 A_K0, 1 A_K1, 2 A_K2, 3 A_W, 4 A_L, 5 A2_K2",
-           "template <class M, int Fn> struct MeshFn;"]
+           "template <class M, int Fn> struct MeshFn;",
+           "static __device__ const double kMeshGx8[8] = {" + ", ".join(repr(float(x)) for x in x8) + "};",
+           "static __device__ const double kMeshGw8[8] = {" + ", ".join(repr(float(x)) for x in w8) + "};"]
     for name in RADIAL_KERNELS:
         t = mesh_tables(name)
         bounds = t["bounds"]
