@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-mesh", action="store_true", help="skip the 3-D closed-surface leg")
+    p.add_argument("--leg", choices=["all", "radial", "mesh3d"], default="all",
+                   help="run one side leg alone (prints its JSON object; for profiling)")
+    p.add_argument("--mesh-particles", type=int, default=1 << 21, help="particles of the 3-D closed-surface leg")
     p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
     p.add_argument("--serve-requests", type=int, default=10000,
                    help="requests of the serving stream measured after the main workload (0: skip)")
@@ -281,7 +284,7 @@ def radial_run(dev, stream, flush, n=1 << 21, steps=10, kernel="w4"):
             "bytes_per_row": 6 * 8 + 28 * 8, "shell_fraction": shell, "kernel": "k_radial"}
 
 
-def mesh_run(dev, stream, flush, steps=5, kernel="w4"):
+def mesh_run(dev, stream, flush, steps=5, kernel="w4", n_particles=1 << 21):
     """the 3-D scene: 2^21 particles uniform in [-1, 1]^3, h = 0.03, a jittered icosphere of 20480 faces (radius 0.6),
     the 28 baseline channels of every particle, float64, inputs resident; CUDA events around wsb_mesh_channels."""
     import ctypes
@@ -289,7 +292,7 @@ def mesh_run(dev, stream, flush, steps=5, kernel="w4"):
     import torch
     from warpsphboundaries_b200 import workloads
     from warpsphboundaries_b200.mesh3d import ClosedMesh
-    V, Fc, X, h = workloads.c3()
+    V, Fc, X, h = workloads.c3(n_particles=n_particles)
     n = len(X)
     m = ClosedMesh(V, Fc, h, dev)
     pos = torch.tensor(X, dtype=torch.float64, device=dev)
@@ -501,7 +504,7 @@ def our_arm(args):
                "ms_per_step": float(t.item()) / args.steps}
 
     radial = radial_run(dev, stream, flush) if world == 1 else None
-    mesh = mesh_run(dev, stream, flush) if world == 1 and not args.no_mesh else None
+    mesh = mesh_run(dev, stream, flush, n_particles=args.mesh_particles) if world == 1 and not args.no_mesh else None
 
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:
@@ -537,9 +540,25 @@ def our_arm(args):
         dist.destroy_process_group()
 
 
+def side_leg(args):
+    """one side leg alone on cuda:0 (the 3-D sphere rows or the 3-D closed surface), its JSON object printed."""
+    import torch
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    if args.leg == "radial":
+        res = radial_run(dev, stream, flush, steps=args.steps)
+    else:
+        res = mesh_run(dev, stream, flush, steps=args.steps, n_particles=args.mesh_particles)
+    print(json.dumps({"leg": args.leg, **res}), flush=True)
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.leg != "all" and args.impl != "reference":
+        side_leg(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         our_arm(args)
