@@ -161,6 +161,31 @@ __device__ __forceinline__ void for_candidates(const MeshView& M, const double q
       }
 }
 
+// whether any face box comes within h of the query (the loops of for_candidates, stopping at the first)
+__device__ __forceinline__ bool has_candidate(const MeshView& M, const double q[3], double h) {
+  const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
+            cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
+  const int x0 = max(cx - 1, 0), x1 = min(cx + 1, M.nx - 1), y0 = max(cy - 1, 0), y1 = min(cy + 1, M.ny - 1),
+            z0 = max(cz - 1, 0), z1 = min(cz + 1, M.nz - 1);
+  const double h2 = h * h;
+  for (int k = z0; k <= z1; ++k)
+    for (int j = y0; j <= y1; ++j)
+      for (int i = x0; i <= x1; ++i) {
+        const int c = (k * M.ny + j) * M.nx + i;
+        for (int it = M.cstart[c]; it < M.cstart[c + 1]; ++it) {
+          const double* F = M.fdata + (int64_t)M.citems[it] * kFaceDoubles;
+          double d2 = 0.0;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            const double d = fmax(0.0, fmax(F[kFLO + a] - q[a], q[a] - F[kFHI + a]));
+            d2 = fma(d, d, d2);
+          }
+          if (d2 < h2) return true;
+        }
+      }
+  return false;
+}
+
 // ------------------------------------------------------------------------------------------ profiles
 template <class M, int Fn>
 __device__ __forceinline__ double fpoly(int p, double x) {
@@ -403,13 +428,47 @@ __device__ __forceinline__ double tri_dist2(const double P[3][3]) {
   return cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2];
 }
 
-// the contribution of face f to the row's accumulators, computed by the whole warp: the geometry and the assembly
-// are the same in every lane, the quadrature nodes of an edge (12 per panel) are spread over the lanes and their
-// sums reduced by a fixed butterfly.  Everything is linear in the per-edge integrals.  Faces that do not meet the
+// assembly (W~ units), per edge:  M0 += J0;  M1 += N J1 + mu LK1;
+// M2 += N N^T J2 + N (mu LK2)^T + (mu LK2) N^T + sym(mu (x) (w mu LK2b + t TK2)) - (I - N N^T) J5;
+// G0 -= N J3;  G1_ij -= (z N_i J3 + mu_i LW) N_j;  H += sym(N (x) (z N J4 + mu LL))
+__device__ __forceinline__ void edge_assemble(double* __restrict__ Av, const double N[3], double z, const double t[3],
+                                              const double mu[3], double w, const EdgeSums& S) {
+  Av[kAM0] += S.J[0];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) Av[kAM1 + i] += N[i] * S.J[1] + mu[i] * S.LK1;
+  const double wl = w * S.LK2b;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) {
+      const double Pij = (i == j ? 1.0 : 0.0) - N[i] * N[j];
+      const double v = N[i] * N[j] * S.J[2] + (N[i] * mu[j] + mu[i] * N[j]) * S.LK2 + mu[i] * mu[j] * wl +
+                       0.5 * (mu[i] * t[j] + mu[j] * t[i]) * S.TK2 - Pij * S.J[5];
+      Av[kAM2 + sym(i, j)] += v;
+    }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    Av[kAG0 + i] -= N[i] * S.J[3];
+    const double S1 = z * N[i] * S.J[3] + mu[i] * S.LW;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) Av[kAG1 + 3 * i + j] -= S1 * N[j];
+  }
+  double HL[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) HL[j] = z * N[j] * S.J[4] + mu[j] * S.LL;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = i; j < 3; ++j) Av[kAH + sym(i, j)] += 0.5 * (N[i] * HL[j] + N[j] * HL[i]);
+}
+
+// the contribution of face f to the row's accumulators (the warp's shared array Av), computed by the whole warp: the
+// geometry is the same in every lane, the quadrature nodes of an edge (12 per panel) are spread over the lanes and
+// their sums reduced by a fixed butterfly, lane 0 adds the edge's terms to Av.  Everything is linear in the per-edge integrals.  Faces that do not meet the
 // support contribute exactly nothing: skipped.  q in world units, ih = 1 / support.
 template <class M>
 __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], double ih, PanelList& PL, int lane,
-                                  Acc28& A) {
+                                  double* __restrict__ Av) {
   const double* F = Mv.fdata + (int64_t)f * kFaceDoubles;
   double P[3][3];
 #pragma unroll
@@ -475,36 +534,9 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
         S.J[5] -= aval_a<M, 5, 1>(a, z, sg) * out;
       }
     }
-    // assembly (W~ units), per edge:  M0 += J0;  M1 += N J1 + mu LK1;
-    // M2 += N N^T J2 + N (mu LK2)^T + (mu LK2) N^T + sym(mu (x) (w mu LK2b + t TK2)) - (I - N N^T) J5;
-    // G0 -= N J3;  G1_ij -= (z N_i J3 + mu_i LW) N_j;  H += sym(N (x) (z N J4 + mu LL))
-    A.v[kAM0] += S.J[0];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) A.v[kAM1 + i] += N[i] * S.J[1] + mu[i] * S.LK1;
-    const double wl = w * S.LK2b;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = i; j < 3; ++j) {
-        const double Pij = (i == j ? 1.0 : 0.0) - N[i] * N[j];
-        const double v = N[i] * N[j] * S.J[2] + (N[i] * mu[j] + mu[i] * N[j]) * S.LK2 + mu[i] * mu[j] * wl +
-                         0.5 * (mu[i] * t[j] + mu[j] * t[i]) * S.TK2 - Pij * S.J[5];
-        A.v[kAM2 + sym(i, j)] += v;
-      }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      A.v[kAG0 + i] -= N[i] * S.J[3];
-      const double S1 = z * N[i] * S.J[3] + mu[i] * S.LW;
-#pragma unroll
-      for (int j = 0; j < 3; ++j) A.v[kAG1 + 3 * i + j] -= S1 * N[j];
-    }
-    double HL[3];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) HL[j] = z * N[j] * S.J[4] + mu[j] * S.LL;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = i; j < 3; ++j) A.v[kAH + sym(i, j)] += 0.5 * (N[i] * HL[j] + N[j] * HL[i]);
+    // assembly into the warp's shared accumulators, by lane 0 (keeping 28 accumulators out of every lane's registers)
+    if (lane == 0) edge_assemble(Av, N, z, t, mu, w, S);
+    __syncwarp();
   }
 }
 
@@ -526,9 +558,7 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_rowinfo(MeshView M, const
     const bool ok = h > 0.0 && h <= M.cell && isfinite(q[0]) && isfinite(q[1]) && isfinite(q[2]);
     if (ok) {
       ind[row] = mesh_inside(M, q[0], q[1], q[2]);
-      int cnt = 0;
-      for_candidates(M, q, h, [&](int) { ++cnt; });
-      has = cnt > 0;
+      has = has_candidate(M, q, h);
     } else {
       ind[row] = -1;
     }
@@ -597,6 +627,7 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
                                                            const int32_t* __restrict__ nwork,
                                                            int32_t* __restrict__ grab, double* __restrict__ out) {
   __shared__ PanelList pl[kMeshThreads / 32];
+  __shared__ double acc[kMeshThreads / 32][28];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int nw = *nwork;
   for (int it = 0; it < (1 << 30); ++it) {
@@ -607,10 +638,16 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
     const int64_t row = work[slot];
     const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
     const double h = sup[row], ih = 1.0 / h;
-    Acc28 A;
-    acc_zero(A);
-    for_candidates(Mv, q, h, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], lane, A); });
-    if (lane == 0) write_row<M>(out, row, A, (double)ind[row], h);
+    if (lane < 28) acc[wib][lane] = 0.0;
+    __syncwarp();
+    for_candidates(Mv, q, h, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], lane, acc[wib]); });
+    if (lane == 0) {
+      Acc28 A;
+#pragma unroll
+      for (int i = 0; i < 28; ++i) A.v[i] = acc[wib][i];
+      write_row<M>(out, row, A, (double)ind[row], h);
+    }
+    __syncwarp();
   }
 }
 
