@@ -175,6 +175,30 @@ int wsb_radial_channels(int kind, int kernel, int precision, const double* dista
                         const double* normals, const double* supports, int64_t n, const int32_t* requests,
                         int n_requests, double* out, double* invariants, int32_t* status, void* stream);
 
+/* ---- conditioned single triangles (2-D) ----
+ * Float64 area quadrature of a solid triangle for the rows where the closed form would lose digits: the triangle is
+ * small (longest edge <= 0.02 h) or a sliver (2 area <= 0.01 longest edge^2); the other rows get status 0 and zero
+ * values (they keep the closed form).  tri [6] (host): the vertices v0 v1 v2 in the rule's order (v2 - v0 the shortest
+ * edge), area2 = 2 area, sign +1 for a counter-clockwise solid triangle (-1 clockwise), background 1 for an unbounded
+ * solid.  lpos [n*2] body-frame positions, sup [n], valid [n] (may be NULL), all device.  Writes values [n*12]
+ * (support-normalised units, body frame, order lam m1x m1y Gx Gy g1xx g1xy g1yx g1yy m20 m11 m02), estimate [n*12]
+ * (may be NULL; empirical quadrature differences, NaN where status is 0) and status [n]: 0 closed form, 1 converged,
+ * -1 panel budget exhausted (values NaN).  Kernels with at most two radii (cubic, w2, w4, w6, poly6).  Replaces
+ * warptriangle.channels / prepare (src/warpSPHBoundaries/edge/warptriangle.py:126-201, 258-310). */
+int wsb_triangle_channels(const double* tri, double area2, double sign, int background, int kernel, const double* lpos,
+                          const double* sup, const int32_t* valid, int64_t n, double tolerance, int max_panels,
+                          double* values, double* estimate, int32_t* status, void* stream);
+
+/* The per-row override of a conditioned triangle: rows with status != 0 take values (rotated into the world frame by
+ * pose [4] = (cx, cy, cos, sin) and scaled by the support: m1 h, G 1/h, m2 h^2), the others the closed-form outputs
+ * clam [n], cG [n*2], ccov [n*4], cm1 [n*2], cm2 [n*4]; the result is assigned (add = 0) or added into lam, G, cov, m1,
+ * m2 (all device).  Replaces the quadrature override of the contraction (src/warpSPHBoundaries/scene/fused.py:556-564,
+ * src/warpSPHBoundaries/scene/scene.py:405-409). */
+int wsb_triangle_combine(const double* values, const int32_t* status, const double* sup, const double* pose, int64_t n,
+                         int add, const double* clam, const double* cG, const double* ccov, const double* cm1,
+                         const double* cm2, double* lam, double* G, double* cov, double* m1, double* m2,
+                         void* stream);
+
 /* ---- closed triangle surfaces (3-D) ----
  * A watertight, consistently oriented triangle surface with outward normals (positive signed volume): verts
  * [n_verts*3] and faces [n_faces*3] (vertex ids) on the host, copied to `device` with a cell grid of faces (cell =

@@ -16,6 +16,9 @@ Writes
   radial_golden.json          solid half-spaces and spheres, 3-D: the nine radial invariants and the 28 baseline
                               channels of the reference's 70-digit fixtures (tests/fixtures/fluxbridge-radial-v1.json,
                               and the baseline requests of tests/fixtures/fluxbridge-sphere-v1.json)
+  triangle_golden.json        conditioned single triangles (2-D): the reference's adversarial triangle cases (tiny, needle
+                              angles, slivers; validation/adversarial.py polygon_cases) at its deterministic probes, with
+                              the twelve channels (w4) of its 70-digit analytic reference (precision_polygon_reference)
   mesh3d_golden.json          closed triangle surfaces, 3-D: the 28 baseline channels (value moments |alpha| <= 2,
                               kernel-gradient moments |alpha| <= 1, kernel Hessian) from the reference's exact
                               face-to-edge reductions in mpmath (mesh3d/reference.py ClosedSurface), 40 digits, for an
@@ -277,6 +280,23 @@ def mesh3d_golden(root, dps=40):
     print("mesh3d_golden.json:", len(cases), "cases")
 
 
+def triangle_golden(root, names=("triangle-size-1e-09", "triangle-size-0.01", "triangle-size-1e-05",
+                                 "triangle-angle-0.1", "triangle-angle-179", "sliver-1e-07", "sliver-0.001")):
+    adv = importlib.import_module("warpSPHBoundaries.validation.adversarial")
+    out = {"meta": {"source": "validation/adversarial.py of the reference: polygon_cases, probes, "
+                              "precision_polygon_reference (70 digits), kernel w4, support 1",
+                    "channels": "m00 m10 m01 m20 m11 m02 Gx Gy g1xx g1xy g1yx g1yy"}, "cases": []}
+    for c in adv.polygon_cases():
+        if c.name not in names:
+            continue
+        pts = c.probes()
+        target = adv.precision_polygon_reference(c.vertices, pts, "w4")
+        out["cases"].append({"name": c.name, "vertices": c.vertices.tolist(), "points": pts.tolist(),
+                             "target": [[repr(float(v)) for v in row] for row in target]})
+        print("triangle", c.name, len(pts), "probes", flush=True)
+    (HERE / "triangle_golden.json").write_text(json.dumps(out, indent=1))
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     np2d, torch2d = load_reference(root)
@@ -285,3 +305,4 @@ if __name__ == "__main__":
     torch2d_grads(torch2d)
     radial_golden(root)
     mesh3d_golden(root)
+    triangle_golden(root)

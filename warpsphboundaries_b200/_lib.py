@@ -22,7 +22,8 @@ EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_d
            "wsb_aggregate_noalloc",
            "wsb_aggregate_backward", "wsb_signed_distance",
            "wsb_kinematics", "wsb_radial_channels", "wsb_mesh_create", "wsb_mesh_destroy",
-           "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels"]
+           "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels", "wsb_triangle_channels",
+           "wsb_triangle_combine"]
 
 
 class SurfaceInfo(ctypes.Structure):
@@ -64,6 +65,9 @@ def _load():
         "wsb_mesh_workspace_size": (c_size_t, [P, c_int64]),
         "wsb_mesh_inside": (c_int, [P, P, c_int64, P, P]),
         "wsb_mesh_channels": (c_int, [P, c_int, P, P, c_int64, P, P, P, c_size_t, P]),
+        "wsb_triangle_channels": (c_int, [D, c_double, c_double, c_int, c_int, P, P, P, c_int64, c_double, c_int, P, P,
+                                          P, P]),
+        "wsb_triangle_combine": (c_int, [P, P, P, P, c_int64, c_int, P, P, P, P, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

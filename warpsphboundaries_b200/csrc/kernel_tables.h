@@ -831,4 +831,70 @@ template <> struct MeshFn<Mesh_w6, 5> {   // A2_K2
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.21875; dd = b; b = fma(a, b, -1.955078125); dd = fma(dd, x, b); b = fma(a, b, 7.5); dd = fma(dd, x, b); b = fma(a, b, -15.791015625); dd = fma(dd, x, b); b = fma(a, b, 18.958333333333332); dd = fma(dd, x, b); b = fma(a, b, -11.197265625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 3.2584635416666665); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -1.396484375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 0.533203125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -0.15950520833333334); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
 };
 
+// ---- 2-D conditioned triangles: pi W and rho = -pi W'/r per piece (unit support)
+static __device__ const double kTriGx16[16] = {-0.9894009349916499, -0.9445750230732326, -0.8656312023878318, -0.755404408355003, -0.6178762444026438, -0.45801677765722737, -0.2816035507792589, -0.09501250983763744, 0.09501250983763744, 0.2816035507792589, 0.45801677765722737, 0.6178762444026438, 0.755404408355003, 0.8656312023878318, 0.9445750230732326, 0.9894009349916499};
+static __device__ const double kTriGw16[16] = {0.027152459411754176, 0.062253523938647456, 0.0951585116824926, 0.12462897125553407, 0.1495959888165767, 0.16915651939500265, 0.18260341504492364, 0.18945061045506864, 0.18945061045506864, 0.18260341504492364, 0.16915651939500265, 0.1495959888165767, 0.12462897125553407, 0.0951585116824926, 0.062253523938647456, 0.027152459411754176};
+static __device__ const double kTriGx8[8] = {-0.9602898564975362, -0.7966664774136267, -0.525532409916329, -0.18343464249564978, 0.18343464249564978, 0.525532409916329, 0.7966664774136267, 0.9602898564975362};
+static __device__ const double kTriGw8[8] = {0.10122853629037706, 0.22238103445337443, 0.3137066458778869, 0.36268378337836166, 0.36268378337836166, 0.3137066458778869, 0.22238103445337443, 0.10122853629037706};
+struct Tri_cubic {
+  static constexpr int kPieces = 2;
+  static constexpr double kPlane2 = 0.07908163265306123;   // int_plane y_x^2 W
+  static constexpr double kKnot = 0.5;   // end of the inner piece
+  template <int P> __host__ __device__ static __forceinline__ void eval(double r, double& w, double& rho);
+};
+template <> __host__ __device__ __forceinline__ void Tri_cubic::eval<0>(double r, double& w, double& rho) {
+  using T = double;
+  w = (fma_t((fma_t(T(34.285714285714285), r, T(-34.285714285714285)) * r), r, T(5.714285714285714)));
+  rho = (fma_t(T(-102.85714285714286), r, T(68.57142857142857)));
+}
+template <> __host__ __device__ __forceinline__ void Tri_cubic::eval<1>(double r, double& w, double& rho) {
+  using T = double;
+  w = (T(11.428571428571429)) * ipow<3>(T(1.0) - r);
+  rho = (T(34.285714285714285)) * ipow<2>(T(1.0) - r) * (T(1) / ipow<1>(r));
+}
+struct Tri_w2 {
+  static constexpr int kPieces = 1;
+  static constexpr double kPlane2 = 0.06944444444444445;   // int_plane y_x^2 W
+  static constexpr double kKnot = 2.0;   // end of the inner piece
+  template <int P> __host__ __device__ static __forceinline__ void eval(double r, double& w, double& rho);
+};
+template <> __host__ __device__ __forceinline__ void Tri_w2::eval<0>(double r, double& w, double& rho) {
+  using T = double;
+  w = (fma_t(T(28.0), r, T(7.0))) * ipow<4>(T(1.0) - r);
+  rho = (T(140.0)) * ipow<3>(T(1.0) - r);
+}
+struct Tri_w4 {
+  static constexpr int kPieces = 1;
+  static constexpr double kPlane2 = 0.05303030303030303;   // int_plane y_x^2 W
+  static constexpr double kKnot = 2.0;   // end of the inner piece
+  template <int P> __host__ __device__ static __forceinline__ void eval(double r, double& w, double& rho);
+};
+template <> __host__ __device__ __forceinline__ void Tri_w4::eval<0>(double r, double& w, double& rho) {
+  using T = double;
+  w = (fma_t(fma_t(T(105.0), r, T(54.0)), r, T(9.0))) * ipow<6>(T(1.0) - r);
+  rho = (fma_t(T(840.0), r, T(168.0))) * ipow<5>(T(1.0) - r);
+}
+struct Tri_w6 {
+  static constexpr int kPieces = 1;
+  static constexpr double kPlane2 = 0.04285714285714286;   // int_plane y_x^2 W
+  static constexpr double kKnot = 2.0;   // end of the inner piece
+  template <int P> __host__ __device__ static __forceinline__ void eval(double r, double& w, double& rho);
+};
+template <> __host__ __device__ __forceinline__ void Tri_w6::eval<0>(double r, double& w, double& rho) {
+  using T = double;
+  w = (fma_t(fma_t(fma_t(T(356.57142857142856), r, T(278.57142857142856)), r, T(89.14285714285714)), r, T(11.142857142857142))) * ipow<8>(T(1.0) - r);
+  rho = (fma_t(fma_t(T(3922.285714285714), r, T(1716.0)), r, T(245.14285714285714))) * ipow<7>(T(1.0) - r);
+}
+struct Tri_poly6 {
+  static constexpr int kPieces = 1;
+  static constexpr double kPlane2 = 0.1;   // int_plane y_x^2 W
+  static constexpr double kKnot = 2.0;   // end of the inner piece
+  template <int P> __host__ __device__ static __forceinline__ void eval(double r, double& w, double& rho);
+};
+template <> __host__ __device__ __forceinline__ void Tri_poly6::eval<0>(double r, double& w, double& rho) {
+  using T = double;
+  w = (fma_t(fma_t(fma_t(T(4.0), r, T(12.0)), r, T(12.0)), r, T(4.0))) * ipow<3>(T(1.0) - r);
+  rho = (fma_t(fma_t(T(24.0), r, T(48.0)), r, T(24.0))) * ipow<2>(T(1.0) - r);
+}
+
 }  // namespace wsb

@@ -418,6 +418,7 @@ def emit_header() -> str:
     out.append("")
     out.extend(emit_radial())
     out.extend(emit_mesh())
+    out.extend(emit_triangle())
     out.append("}  // namespace wsb")
     out.append("")
     return "\n".join(out)
@@ -636,6 +637,51 @@ def _radial_eval(prof, var, hi_lit, T):
     if prof.p < 0:
         fac.append(f"(T(1) / ipow<{-prof.p}>({var}))")
     return " * ".join([f"({expr})"] + fac)
+
+
+# ------------------------------------------------------------------ 2-D conditioned triangles (area quadrature)
+TRIANGLE_KERNELS = ("cubic", "w2", "w4", "w6", "poly6")
+
+
+def triangle_profiles(name):
+    """per piece of the 2-D kernel (pi W, unit support): (lo, hi, W, rho) with rho = -W'/r, both as RadialProfile
+    r^p (hi - r)^k g(r) (exact factors keep the values accurate where W is small)."""
+    if name not in TRIANGLE_KERNELS:
+        raise KeyError(f"conditioned triangles: kernel {name!r} not in {TRIANGLE_KERNELS} (at most two radii)")
+    out = []
+    for lo, hi, co in kernel(name).pieces:
+        w = {n: c for n, c in enumerate(co) if c}
+        rho = {n - 2: -n * c for n, c in w.items() if n >= 1}
+        out.append((lo, hi, RadialProfile(*_factor_laurent(w, hi)), RadialProfile(*_factor_laurent(rho, hi))))
+    return out
+
+
+def emit_triangle() -> list:
+    """generated device code of the conditioned-triangle quadrature: per kernel the pieces and W, -W'/r."""
+    import numpy as np
+    x16, w16 = np.polynomial.legendre.leggauss(16)
+    x8, w8 = np.polynomial.legendre.leggauss(8)
+    out = ["// ---- 2-D conditioned triangles: pi W and rho = -pi W'/r per piece (unit support)",
+           "static __device__ const double kTriGx16[16] = {" + ", ".join(repr(float(x)) for x in x16) + "};",
+           "static __device__ const double kTriGw16[16] = {" + ", ".join(repr(float(x)) for x in w16) + "};",
+           "static __device__ const double kTriGx8[8] = {" + ", ".join(repr(float(x)) for x in x8) + "};",
+           "static __device__ const double kTriGw8[8] = {" + ", ".join(repr(float(x)) for x in w8) + "};"]
+    for name in TRIANGLE_KERNELS:
+        pcs = triangle_profiles(name)
+        out.append(f"struct Tri_{name} {{")
+        out.append(f"  static constexpr int kPieces = {len(pcs)};")
+        out.append(f"  static constexpr double kPlane2 = {_lit(kernel(name).plane2)};   // int_plane y_x^2 W")
+        out.append(f"  static constexpr double kKnot = {_lit(pcs[0][1]) if len(pcs) > 1 else '2.0'};   // end of the inner piece")
+        out.append("  template <int P> __host__ __device__ static __forceinline__ void eval(double r, double& w, double& rho);")
+        out.append("};")
+        for i, (lo, hi, W, rho) in enumerate(pcs):
+            out.append(f"template <> __host__ __device__ __forceinline__ void Tri_{name}::eval<{i}>(double r, double& w, double& rho) {{")
+            out.append("  using T = double;")
+            out.append(f"  w = {_radial_eval(W, 'r', _lit(hi), 'T')};")
+            out.append(f"  rho = {_radial_eval(rho, 'r', _lit(hi), 'T')};")
+            out.append("}")
+    out.append("")
+    return out
 
 
 def emit_radial() -> list:

@@ -93,12 +93,12 @@ class FusedWall(WallAggregate):
                 for r in b.reps:
                     if not isinstance(r, SurfaceRep):
                         raise NotImplementedError(f"FusedWall: {type(r).__name__} is not built (surface loops only)")
-                    if r._triangle:
-                        raise NotImplementedError("FusedWall: a conditioned single-triangle SurfaceRep takes the sliver "
-                                                  "quadrature, which is not built; use SurfaceRep(..., "
-                                                  "conditioned=False)")
+                    if r._triangle is not None and route != "fused":
+                        raise NotImplementedError("FusedWall: conditioned single triangles take the fused route")
             scene._wsb_checked = sig
         self.res = []
+        self.qstatus = {}                      # (group, body, rep) -> [N] int32 of conditioned triangles
+        self.estimates = {}                    # (group, body, rep) -> [N, 12] quadrature estimates
         alloc = torch.empty if route == "fused" else torch.zeros     # the fused route assigns every row of a body
         if outs is not None and (route != "fused" or len(self.groups) != 1):
             raise ValueError("FusedWall: caller-owned outputs serve the fused route with one kernel group")
@@ -112,6 +112,7 @@ class FusedWall(WallAggregate):
                        "m1": alloc((B, N, 2), dtype=F64, device=self.dev),
                        "m2": alloc((B, N, 2, 2), dtype=F64, device=self.dev)}
             kid = KERNEL_IDS[g.kernel]
+            self._group = len(self.res)
             if route == "fused":
                 self._fused(pos, sup, allowed, kid, out)
             elif route == "plain":
@@ -139,10 +140,41 @@ class FusedWall(WallAggregate):
                 else:
                     ws, need = ns.workspace(N)
                 mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)     # the first surface of a body assigns
+                tgt = {k: out[k][bi] for k in ("lam", "G", "Cov", "m1", "m2")}
+                if rep._triangle is not None:
+                    # closed form into scratch, then the rows the quadrature takes are overridden while combining
+                    tgt = {k: torch.empty_like(out[k][bi]) for k in ("lam", "G", "Cov", "m1", "m2")}
+                    mode = _lib.OUT_ALL | _lib.OUT_ASSIGN
                 check(lib.wsb_aggregate(ns.handle, kid, _PREC[self.precision], ptr(pos), ptr(sup), ptr(al), N,
-                                        ptr(pose), obb, int(body.unbounded()), mode, ptr(out["lam"][bi]),
-                                        ptr(out["G"][bi]), ptr(out["Cov"][bi]), ptr(out["m1"][bi]),
-                                        ptr(out["m2"][bi]), ptr(ws), need, None, _stream()), "wsb_aggregate")
+                                        ptr(pose), obb, int(body.unbounded()), mode, ptr(tgt["lam"]),
+                                        ptr(tgt["G"]), ptr(tgt["Cov"]), ptr(tgt["m1"]),
+                                        ptr(tgt["m2"]), ptr(ws), need, None, _stream()), "wsb_aggregate")
+                if rep._triangle is not None:
+                    self._conditioned(body, bi, ri, rep, pos, sup, al, kid, pose, tgt, out)
+
+    def _conditioned(self, body, bi, ri, rep, pos, sup, al, kid, pose, closed, out, tolerance=2e-12,
+                     max_panels=4096):
+        """the conditioned area quadrature of a single-triangle rep on its small / sliver rows, combined with the
+        closed form of the other rows (warptriangle.py:126-201, fused.py:556-564)."""
+        N = self.N
+        tri, area2, sign = rep._triangle
+        state = torch.tensor([body.state_row()], dtype=F64, device=self.dev)
+        local = torch.empty((N, 2), dtype=F64, device=self.dev)
+        check(lib.wsb_kinematics(ptr(state), 1, ptr(pos), N, None, ptr(local), None, None, _stream()),
+              "wsb_kinematics")
+        vals = torch.empty((N, 12), dtype=F64, device=self.dev)
+        est = torch.empty((N, 12), dtype=F64, device=self.dev)
+        st = torch.empty(N, dtype=torch.int32, device=self.dev)
+        check(lib.wsb_triangle_channels(_lib.dptr(tri), area2, sign, rep.background, kid, ptr(local), ptr(sup),
+                                        ptr(al), N, tolerance, max_panels, ptr(vals), ptr(est), ptr(st), _stream()),
+              "wsb_triangle_channels")
+        check(lib.wsb_triangle_combine(ptr(vals), ptr(st), ptr(sup), ptr(pose), N, int(ri > 0), ptr(closed["lam"]),
+                                       ptr(closed["G"]), ptr(closed["Cov"]), ptr(closed["m1"]), ptr(closed["m2"]),
+                                       ptr(out["lam"][bi]), ptr(out["G"][bi]), ptr(out["Cov"][bi]),
+                                       ptr(out["m1"][bi]), ptr(out["m2"][bi]), _stream()), "wsb_triangle_combine")
+        key = (self._group, bi, ri)
+        self.qstatus[key] = st
+        self.estimates[key] = est
 
     def _plain(self, ps, kid, out):
         props = OperationProperties(operationMode=OperationDirection.BoundaryToFluid)

@@ -116,9 +116,31 @@ class SurfaceRep:
         self.vertices = torch.as_tensor(vertices, dtype=F64)
         self.edges = torch.as_tensor(edges, dtype=torch.int32)
         self.background = int(background)
-        # single-triangle reps would take the reference's conditioned sliver quadrature (warptriangle.py:126-201)
-        self._triangle = (len(self.vertices) == 3 and len(self.edges) == 3) if conditioned else False
+        # a single triangle takes the conditioned area quadrature on its small / sliver rows (warptriangle.py:126-201)
+        self._triangle = self._triangle_meta() if conditioned else None
         self._native = {}
+
+    def _triangle_meta(self):
+        """(ordered vertices [6], 2 area, sign) of a single-triangle loop, or None (warptriangle.py:290-310): the
+        vertices in the loop's order, the exact signed area, the rule's order with the shortest edge last."""
+        if len(self.vertices) != 3 or len(self.edges) != 3:
+            return None
+        v = self.vertices.detach().cpu().numpy()
+        e = {tuple(int(x) for x in pair) for pair in self.edges.detach().cpu().tolist()}
+        if e == {(0, 1), (1, 2), (2, 0)}:
+            loop = [0, 1, 2]
+        elif e == {(0, 2), (2, 1), (1, 0)}:
+            loop = [0, 2, 1]
+        else:
+            return None
+        a, b, c = [[Fraction(float(x)) for x in v[i]] for i in loop]
+        signed = (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])
+        if not signed:
+            return None
+        short = int(np.argmin([float(((v[(i + 1) % 3] - v[i]) ** 2).sum()) for i in range(3)]))
+        order = [short, (short + 2) % 3, (short + 1) % 3]
+        return (np.ascontiguousarray(v[order].reshape(-1), dtype=np.float64), float(abs(signed)),
+                1.0 if signed > 0 else -1.0)
 
     @staticmethod
     def _orient(P, solid):
