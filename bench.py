@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-mesh", action="store_true", help="skip the 3-D closed-surface leg")
-    p.add_argument("--leg", choices=["all", "radial", "mesh3d"], default="all",
+    p.add_argument("--leg", choices=["all", "radial", "mesh3d", "serving"], default="all",
                    help="run one side leg alone (prints its JSON object; for profiling)")
     p.add_argument("--mesh-particles", type=int, default=1 << 21, help="particles of the 3-D closed-surface leg")
     p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
@@ -168,33 +168,50 @@ class Clocks:
 
 # ----------------------------------------------------------------------------------------------- serving stream
 def serving_run(n_requests, dev, pair_density, seed=0, load=0.8):
-    """Poisson stream of boundary queries over 32 resident scenes of the large 2-D kind (64 star polygons each,
-    h = 0.02), particle counts log-uniform in [1e3, 1e6] (positions uniform in [0, 4]^2, produced on the device at
-    arrival), kernels uniform in {w2, w4, w6}, 25 % of the requests with the adjoint.  The arrival rate is `load` times
-    the capacity measured on a saturating run.  Returns p50 / p99 latency and rates."""
+    """Poisson stream of boundary queries over 32 resident scenes: 16 of the large 2-D kind (64 star polygons each,
+    h = 0.02) and 16 of the 3-D kind (closed icospheres of 5120 faces, radius U(0.3, 0.8), 5 % jitter, h = 0.03).
+    Particle counts log-uniform in [1e3, 1e6] (positions uniform in [0, 4]^2 or [-1, 1]^3, slices of resident
+    rings), kernels uniform in {w2, w4, w6}, 25 % of the 2-D requests with the adjoint.  The arrival rate is `load`
+    times the capacity measured on a saturating run.  Returns p50 / p99 latency, rates and the device busy fraction."""
     import torch
     from warpsphboundaries_b200 import workloads
     from warpsphboundaries_b200.scene import Body, Scene, SurfaceRep
     from warpsphboundaries_b200.serve import BoundaryServer
-    h = 0.02
+    h, h3 = 0.02, 0.03
     rng = np.random.default_rng(seed + 77)
-    scenes = {f"scene{k}": Scene([Body(reps=[SurfaceRep.loops(workloads.stars(64, (32, 512), seed=100 + k))])], dev)
-              for k in range(32)}
     srv = BoundaryServer(dev, streams=4)
-    for sid, sc in scenes.items():
-        srv.register(sid, sc, h)
-    specs = [(f"scene{rng.integers(0, 32)}", int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))),
-              ["w2", "w4", "w6"][rng.integers(0, 3)], bool(rng.uniform() < 0.25)) for _ in range(n_requests)]
+    for k in range(16):
+        sc = Scene([Body(reps=[SurfaceRep.loops(workloads.stars(64, (32, 512), seed=100 + k))])], dev)
+        srv.register(f"scene{k}", sc, h)
+    for k in range(16):
+        V, Fc = workloads.icosphere(4, float(rng.uniform(0.3, 0.8)), 0.05, seed=200 + k)
+        srv.register_mesh(f"mesh{k}", V, Fc, h3)
+    names = [f"scene{k}" for k in range(16)] + [f"mesh{k}" for k in range(16)]
+    specs = []
+    for _ in range(n_requests):
+        sid = names[rng.integers(0, 32)]
+        rows = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e6)))))
+        kern = ["w2", "w4", "w6"][rng.integers(0, 3)]
+        grad = bool(rng.uniform() < 0.25) and sid.startswith("scene")
+        specs.append((sid, rows, kern, grad))
     gen = torch.Generator(device=dev)
     gen.manual_seed(seed)
-    # the clients' particle positions: slices of a resident ring of positions (a simulation's state is resident)
-    ring = torch.rand((1 << 22, 2), dtype=torch.float64, device=dev, generator=gen) * 4.0
-    cursor = [0]
+    # the clients' particle positions: slices of resident rings of positions (a simulation's state is resident)
+    ring2 = torch.rand((1 << 22, 2), dtype=torch.float64, device=dev, generator=gen) * 4.0
+    ring3 = torch.rand((1 << 22, 3), dtype=torch.float64, device=dev, generator=gen) * 2.0 - 1.0
+    cursor = [0, 0]
 
-    def make(rows):
-        start = cursor[0] if cursor[0] + rows <= len(ring) else 0
-        cursor[0] = start + rows
-        return ring[start:start + rows]
+    def make(sid, rows):
+        three = sid.startswith("mesh")
+        ring = ring3 if three else ring2
+        c = cursor[int(three)]
+        start = c if c + rows <= len(ring) else 0
+        cursor[int(three)] = start + rows
+        return ring[start:start + rows], (h3 if three else h)
+
+    def submit(sid, rows, k, g, arrival=None):
+        p, hh = make(sid, rows)
+        return srv.submit(sid, p, hh, k, grad=g, arrival=arrival)
 
     # saturation probes (every request submitted as soon as the previous submit returns, polling in between, as in the
     # stream): the first warms graphs and workspaces, the second measures the sustainable capacity in rows/s
@@ -202,7 +219,7 @@ def serving_run(n_requests, dev, pair_density, seed=0, load=0.8):
     for rep in range(2):
         t0 = time.perf_counter()
         for sid, rows, k, g in burst:
-            srv.submit(sid, make(rows), h, k, grad=g)
+            submit(sid, rows, k, g)
             srv.poll()
         srv.run()
         torch.cuda.synchronize()
@@ -223,7 +240,7 @@ def serving_run(n_requests, dev, pair_density, seed=0, load=0.8):
         now = time.perf_counter() - start
         while i < n_requests and arrivals[i] <= now:
             sid, rows, k, g = specs[i]
-            srv.submit(sid, make(rows), h, k, grad=g, arrival=start + arrivals[i])
+            submit(sid, rows, k, g, arrival=start + arrivals[i])
             i += 1
         srv.poll()
         while released[0] < len(srv.completed):               # the clients take their results and free them
@@ -233,12 +250,14 @@ def serving_run(n_requests, dev, pair_density, seed=0, load=0.8):
     wall = time.perf_counter() - start
     st = srv.stats()
     rows_total = sum(r for _, r, _, _ in specs)
+    rows_2d = sum(r for sid, r, _, _ in specs if sid.startswith("scene"))
     return {"requests": n_requests, "scenes": 32, "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
             "mean_ms": st.get("mean_ms"), "arrival_rate_per_s": rate, "wall_s": wall,
-            "rows_per_s": rows_total / wall, "pairs_per_s_est": rows_total * pair_density / wall,
+            "rows_per_s": rows_total / wall, "pairs_per_s_est": rows_2d * pair_density / wall,
+            "rows_3d_per_s": (rows_total - rows_2d) / wall,
             "capacity_rows_per_s": cap_rows, "offered_load": load, "gpu_busy": st.get("gpu_busy"),
-            "note": "pairs estimated from the mean neighbour-pair density of the 2^20-particle scene; all 32 scenes "
-                    "2-D (the 3-D mesh scenes of the serving mix are not built)"}
+            "note": "16 2-D scenes (64 star polygons) + 16 closed 3-D surfaces (5120 faces); pairs estimated from the "
+                    "mean neighbour-pair density of the 2^20-particle 2-D scene for the 2-D rows only"}
 
 
 # ----------------------------------------------------------------------------------------------- our arm
@@ -561,6 +580,8 @@ def side_leg(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     if args.leg == "radial":
         res = radial_run(dev, stream, flush, steps=args.steps)
+    elif args.leg == "serving":
+        res = serving_run(args.serve_requests, dev, 2.09)
     else:
         res = mesh_run(dev, stream, flush, steps=args.steps, n_particles=args.mesh_particles)
     print(json.dumps({"leg": args.leg, **res}), flush=True)

@@ -77,3 +77,43 @@ def test_server_result_equals_provider():
                    (FusedGroup("w4"),))
     for key in OUT_KEYS:
         assert torch.equal(srv.result(rid)[key], fw.res[0][key])
+
+
+def test_closed_surfaces_in_the_mix():
+    """3-D closed-surface scenes served next to 2-D ones: each request's channels equal a direct wsb_mesh_channels
+    call on its own positions, bit for bit, however the requests were batched."""
+    from warpsphboundaries_b200.mesh3d import ClosedMesh
+    h = 0.05
+    meshes = {f"m{k}": workloads.icosphere(2, 0.5 + 0.1 * k, 0.05, seed=k) for k in range(2)}
+    srv = BoundaryServer(DEV, streams=3, max_batch_rows=40000)
+    for sid, (V, Fc) in meshes.items():
+        srv.register_mesh(sid, V, Fc, h)
+    srv.register("s0", _scenes()["s0"], 0.02)
+    rng = np.random.default_rng(3)
+    reqs = []
+    for i in range(24):
+        if i % 3 == 2:
+            reqs.append(("s0", "w4", int(rng.integers(500, 5000)), int(rng.integers(0, 1 << 30))))
+        else:
+            reqs.append((f"m{rng.integers(0, 2)}", ["w2", "w4", "w6", "cubic"][rng.integers(0, 4)],
+                         int(rng.integers(300, 8000)), int(rng.integers(0, 1 << 30))))
+
+    def pos3(rows, seed):
+        g = torch.Generator(device=DEV)
+        g.manual_seed(seed)
+        return torch.rand((rows, 3), dtype=torch.float64, device=DEV, generator=g) * 1.6 - 0.8
+
+    ids = [srv.submit(sid, pos3(rows, seed) if sid.startswith("m") else _positions(rows, seed),
+                      h if sid.startswith("m") else 0.02, k) for sid, k, rows, seed in reqs]
+    srv.run()
+    torch.cuda.synchronize()
+    direct = {sid: ClosedMesh(V, Fc, h, DEV) for sid, (V, Fc) in meshes.items()}
+    for (sid, k, rows, seed), rid in zip(reqs, ids):
+        if not sid.startswith("m"):
+            continue
+        p = pos3(rows, seed)
+        ref = direct[sid].channels(p, torch.full((rows,), h, dtype=torch.float64, device=DEV), k)
+        torch.cuda.synchronize()
+        assert torch.equal(srv.result(rid)["channels"], ref), (sid, k, rows)
+    with pytest.raises(NotImplementedError):
+        srv.submit("m0", pos3(10, 1), h, "w4", grad=True)

@@ -3,9 +3,11 @@
     srv = BoundaryServer(device="cuda:0")
     srv.register("tank-3", scene, support=0.02)                 # geometry, cell grid, indicator cache resident
     rid = srv.submit("tank-3", positions, supports, "w4", grad=False)    # positions / supports: device tensors
+    srv.register_mesh("hull-1", vertices, faces, support=0.03)    # 3-D: a closed triangle surface
     srv.run()                                                    # or srv.poll() from the caller's own loop
     res = srv.result(rid)        # {"lam": [B, n], "G": [B, n, 2], "Cov": [B, n, 2, 2], "m1": [B, n, 2], "m2": [B, n, 2, 2]
                                  #  (+ "d_pos": [n, 2] with grad=True: the adjoint of sum(lam))}
+                                 # closed surfaces: {"channels": [n, 28]} (wsb_mesh_channels order)
 
 Scheduling (one host thread, the caller's):
 * requests queue per (scene, kernel, grad); a batch takes the oldest requests of one queue up to `max_batch_rows`
@@ -90,6 +92,17 @@ class _Slot:
                 self.ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
         return self.ws
 
+    def buffers3(self, rows):
+        """persistent buffers of a closed-surface batch: positions [cap, 3], supports, channels [cap, 28]."""
+        if getattr(self, "buf3", None) is None or rows > self.cap3:
+            cap = max(rows, int(1.5 * getattr(self, "cap3", 0)), 1 << 16)
+            with torch.cuda.stream(self.stream):
+                self.buf3 = {"pos": torch.empty((cap, 3), dtype=F64, device=self.device),
+                             "sup": torch.empty(cap, dtype=F64, device=self.device),
+                             "chan": torch.empty((cap, 28), dtype=F64, device=self.device)}
+            self.cap3 = cap
+        return self.buf3
+
     def buffers(self, rows, B):
         """persistent batch buffers for `rows` rows of a B-body scene (grown geometrically, allocated on this stream)."""
         if self.buf is None or rows > self.cap or B > self.B:
@@ -156,6 +169,18 @@ class BoundaryServer:
         self.scenes[scene_id] = (scene, float(support))
         self.plans[scene_id] = plan
 
+    def register_mesh(self, scene_id, vertices, faces, support):
+        """keep a closed triangle surface resident (3-D): requests on it return the 28 baseline channels per row
+        ("channels" [n, 28], the order of wsb_mesh_channels)."""
+        from .mesh3d import ClosedMesh
+        mesh = ClosedMesh(vertices, faces, float(support), self.device)
+        self.scenes[scene_id] = (mesh, float(support))
+        self.plans[scene_id] = None
+        self.ws_bytes = max(self.ws_bytes, int(lib.wsb_mesh_workspace_size(mesh.handle, self.max_batch_rows)))
+
+    def _is_mesh(self, scene_id):
+        return self.plans.get(scene_id, ()) is None
+
     # ------------------------------------------------------------------ requests
     def submit(self, scene_id, positions, supports, kernel, grad=False, arrival=None):
         """queue a request; its outputs are allocated here, on the caller's stream."""
@@ -169,6 +194,8 @@ class BoundaryServer:
             sup = self._support_vec(float(supports), len(pos))
         r = Request(next(self._ids), scene_id, kname, pos, sup, bool(grad),
                     time.perf_counter() if arrival is None else arrival)
+        if self._is_mesh(scene_id):
+            return self._submit_mesh(r)
         B, n = len(self.scenes[scene_id][0].bodies), len(pos)
         nbytes = 8 * (13 * B * n + (2 * n if r.grad else 0))
         # back-pressure: a full server makes the caller wait (polling) instead of queueing without bound
@@ -188,6 +215,24 @@ class BoundaryServer:
             r.result["d_pos"].zero_()
         self.requests[r.rid] = r
         self.queues.setdefault((scene_id, kname, r.grad), []).append(r)
+        self.n_queued += 1
+        return r.rid
+
+    def _submit_mesh(self, r):
+        if r.grad:
+            raise NotImplementedError("BoundaryServer: closed surfaces serve the channels, not the adjoint")
+        if r.pos.dim() != 2 or r.pos.shape[1] != 3:
+            raise ValueError("BoundaryServer: closed-surface requests take positions [n, 3]")
+        n = len(r.pos)
+        nbytes = 8 * 28 * n
+        while self.held_bytes + nbytes > self.hbm_budget and (self.n_queued or self.n_inflight):
+            self.poll()
+        self.held_bytes += nbytes
+        r.nbytes = nbytes
+        r.flat = self._take(28 * n)
+        r.result = {"channels": r.flat[:28 * n].view(n, 28)}
+        self.requests[r.rid] = r
+        self.queues.setdefault((r.scene_id, r.kernel, False), []).append(r)
         self.n_queued += 1
         return r.rid
 
@@ -228,6 +273,8 @@ class BoundaryServer:
 
     # ------------------------------------------------------------------ bytes a batch holds on the device
     def _bytes(self, scene, support, rows, grad):
+        if not hasattr(scene, "bodies"):                              # a closed surface
+            return (8 * 28 + 32) * rows + int(lib.wsb_mesh_workspace_size(scene.handle, rows))
         B = len(scene.bodies)
         ws = 0
         for b in scene.bodies:
@@ -294,7 +341,42 @@ class BoundaryServer:
             time.sleep(0)
 
     # ------------------------------------------------------------------ launches
+    def _launch_mesh(self, si, reqs, rows, mesh, need):
+        slot = self.slots[si]
+        if self.t_first is None:
+            self.t_first = time.perf_counter()
+        slot.stream.wait_stream(torch.cuda.current_stream(self.device))
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev0.record(slot.stream)
+        with torch.cuda.stream(slot.stream):
+            if len(reqs) == 1:
+                pos, sup, out = reqs[0].pos, reqs[0].sup, reqs[0].result["channels"]
+            else:
+                buf = slot.buffers3(rows)
+                pos, sup, out = buf["pos"][:rows], buf["sup"][:rows], buf["chan"][:rows]
+                off = 0
+                for r in reqs:
+                    n = len(r.pos)
+                    pos[off:off + n].copy_(r.pos)
+                    sup[off:off + n].copy_(r.sup)
+                    off += n
+            ws = slot.workspace(self.ws_bytes)
+            check(lib.wsb_mesh_channels(mesh.handle, KERNEL_IDS[reqs[0].kernel], ptr(pos), ptr(sup), rows, ptr(out),
+                                        None, ptr(ws), ws.numel(), _lib.ctypes.c_void_p(slot.stream.cuda_stream)),
+                  "wsb_mesh_channels")
+            if len(reqs) > 1:
+                off = 0
+                for r in reqs:
+                    n = len(r.pos)
+                    r.result["channels"].copy_(out[off:off + n])
+                    off += n
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(slot.stream)
+        slot.busy = _Batch(reqs, rows, need, ev, ev0)
+
     def _launch(self, si, reqs, rows, scene, support, need):
+        if self._is_mesh(reqs[0].scene_id):
+            return self._launch_mesh(si, reqs, rows, scene, need)
         slot = self.slots[si]
         kname, grad = reqs[0].kernel, reqs[0].grad
         B = len(scene.bodies)
