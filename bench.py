@@ -58,11 +58,11 @@ def parse():
 
 
 def workload(n, rank):
-    from warpsphboundaries_b200 import workloads
+    """the rank's shard of the 2-D workload: the c2 geometry on every rank, rank 0 the c2 particles, the other ranks
+    their own seeded particle sets of the same size (weak scaling)."""
+    from warpsphboundaries_b200 import shard, workloads
     loops, X, h = workloads.c2(n_particles=n, seed=0)
-    if rank:
-        X = np.random.default_rng(1000 + rank).uniform(0, 4.0, size=X.shape)
-    return loops, X, h
+    return loops, shard.rank_particles(len(X), rank, X), h
 
 
 # ----------------------------------------------------------------------------------------------- reference (CPU) arm
@@ -430,12 +430,11 @@ def our_arm(args):
     clocks.start(local)
     total_ms, eval_ms, prep_ms = timed(args.precision, args.steps, args.warmup)
     clk = clocks.stop()
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
-    pairs_step = P * len(KERNELS)
-    value = pairs_step * args.steps * world / (total_ms * 1e-3)
+    from warpsphboundaries_b200 import shard
+    total_ms = shard.max_over_ranks(total_ms, dev)             # the slowest rank's device time
+    pairs_step = P * len(KERNELS)                              # this rank's pairs per step
+    job_pairs_step = shard.sum_over_ranks(pairs_step, dev)     # all ranks' pairs per step
+    value = job_pairs_step * args.steps / (total_ms * 1e-3)
 
     # ---- roofline of the dominant kernel (the fused evaluate pass): algorithmic float64 flops per launch
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
@@ -527,12 +526,10 @@ def our_arm(args):
             b.record(stream)
             torch.cuda.synchronize()
             tot += a.elapsed_time(b)
-        t = torch.tensor([tot], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = {"value": pairs_step * args.steps * world / (float(t.item()) * 1e-3), "unit": UNIT,
+        tot = shard.max_over_ranks(tot, dev)
+        e2e = {"value": job_pairs_step * args.steps / (tot * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": N * 3 * 8, "d2h_bytes_per_step": len(KERNELS) * N * 7 * 8,
-               "ms_per_step": float(t.item()) / args.steps}
+               "ms_per_step": tot / args.steps}
 
     radial = radial_run(dev, stream, flush) if world == 1 else None
     mesh = mesh_run(dev, stream, flush, n_particles=args.mesh_particles) if world == 1 and not args.no_mesh else None
