@@ -72,3 +72,5 @@ def test_evaluator_arguments():
         ev.prepare([[0.1, 0.1, 0.1]], 0.0)
     with pytest.raises(ValueError):
         ev.prepare([[np.nan, 0.1, 0.1]], 0.1)
+    with pytest.raises(ValueError):                                    # element < 1e-4 of the support
+        Evaluator(Geometry.closed_surface(V * 1e-5, F)).prepare([[0.1, 0.1, 0.1]], 1.0)

@@ -159,6 +159,10 @@ class Evaluator:
         h = torch.broadcast_to(h, (len(q),)).contiguous()
         if not torch.isfinite(q).all() or not torch.isfinite(h).all() or bool((h <= 0).any()):
             raise ValueError("queries and supports must be finite with positive supports")
+        # the reference's conservative domain (evaluate.py:96-114): an element spanning less than 1e-4 of a support
+        span = float(np.ptp(self.geometry.vertices, axis=0).max())
+        if len(h) and span / float(h.max()) < 1e-4:
+            raise ValueError("tiny element relative to support: use the arbitrary-precision reference")
         return Batch(self, q.to(self.device).contiguous(), h.to(self.device))
 
     def evaluate(self, queries, supports):
