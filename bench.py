@@ -477,6 +477,34 @@ def our_arm(args):
         del ab
         torch.cuda.empty_cache()
 
+    # ---- the adjoint (d sum(lam) / dx of every particle, w4): prepare + backward per call, timed alone
+    adjoint = None
+    if world == 1:
+        g_lam = torch.ones(N, dtype=torch.float64, device=dev)
+        d_pos = torch.zeros((N, 2), dtype=torch.float64, device=dev)
+
+        def back():
+            _lib.check(_lib.lib.wsb_aggregate_backward(ns.handle, KERNEL_IDS["w4"], _lib.ptr(pos), _lib.ptr(sup), None,
+                                                       N, _lib.ptr(pose), obb, 0, _lib.ptr(g_lam), None, None,
+                                                       _lib.ptr(d_pos), None, _lib.ptr(ws), need, _stream()),
+                       "backward")
+        for _ in range(3):
+            back()
+        torch.cuda.synchronize()
+        tb = 0.0
+        for _ in range(5):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            back()
+            a1.record(stream)
+            torch.cuda.synchronize()
+            tb += a0.elapsed_time(a1)
+        adjoint = {"what": "d sum(lam)/dx of every particle, w4, prepare + k_agg_backward", "ms": tb / 5,
+                   "pairs_per_s": P / (tb / 5 * 1e-3)}
+
     # ---- end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
@@ -560,7 +588,7 @@ def our_arm(args):
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
                 "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
                 "gpu_launches": args.steps * (4 + 2 * len(KERNELS)),
-                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh,
+                "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh, "adjoint": adjoint,
                 **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -283,7 +283,9 @@ __device__ __forceinline__ void adj_blocks(const PairGeo& g, AdjSums& tot) {
   }
 }
 
-template <class KT>
+// G lanes per work row split its cell's candidates (lane g takes g, g + G, ...; the float-prefiltered predicate, exact
+// where the float decision is within its margin); their d_pos partial sums are combined by a fixed xor butterfly
+template <class KT, int G>
 __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const double* __restrict__ sup,
                                                           const int32_t* __restrict__ key,
                                                           const double* __restrict__ lpos,
@@ -295,21 +297,22 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
                                                           const double* __restrict__ g_m1,
                                                           const double* __restrict__ g_m2, double* d_pos,
                                                           double* d_verts) {
-  const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (w >= n || w >= (int64_t)offs[0]) return;        // work rows only (rows with neighbour pairs; offs = counter)
-  const int32_t i = order[work[w]];
-  const int32_t b = key[i];
-  const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
+  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
+  const int sub = threadIdx.x % G;
+  const bool ok = w < n && w < (int64_t)offs[0];      // work rows only (rows with neighbour pairs; offs = counter)
+  const int32_t i = ok ? order[work[w]] : 0;
+  const int32_t b = ok ? key[i] : 0;
+  const double lx = ok ? lpos[2 * i] : 0.0, ly = ok ? lpos[2 * i + 1] : 0.0, h = ok ? sup[i] : 1.0;
   const double c = pose[2], s = pose[3];
   // upstream gradients in the body frame and in channel units: m1_world = R m1, m2_world = R m2 R^T
-  const double gl = g_lam ? g_lam[i] : 0.0;
+  const double gl = g_lam && ok ? g_lam[i] : 0.0;
   double g10 = 0.0, g01 = 0.0, g20 = 0.0, g11 = 0.0, g02 = 0.0;
-  if (g_m1) {
+  if (g_m1 && ok) {
     const double wx = g_m1[2 * i], wy = g_m1[2 * i + 1];
     g10 = c * wx + s * wy;
     g01 = -s * wx + c * wy;
   }
-  if (g_m2) {
+  if (g_m2 && ok) {
     const double a = g_m2[4 * i], bb = g_m2[4 * i + 1], cc = g_m2[4 * i + 2], d = g_m2[4 * i + 3];
     // GL = R^T Gw R with R = [[c, -s], [s, c]]
     const double t00 = c * a + s * cc, t01 = c * bb + s * d, t10 = -s * a + c * cc, t11 = -s * bb + c * d;
@@ -321,9 +324,10 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
   // physical units: d m_alpha = h^(|alpha| - 1) / pi * (unit integral)
   const double u0 = gl / h, u1x = g10, u1y = g01, u2x = g20 * h, u2m = g11 * h, u2y = g02 * h;
   double dx = 0.0, dy = 0.0;
-  for (int k = S.cstart[b]; k < S.cstart[b + 1]; ++k) {
+  const int kend = ok ? S.cstart[b + 1] : 0;
+  for (int k = ok ? S.cstart[b] + sub : 0; k < kend; k += G) {
     const double4 e = S.crec[k];
-    if (!seg_within(lx, ly, e.x, e.y, e.z, e.w, h)) continue;
+    if (!seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) continue;
     PairGeo g;
     if (!pair_geo_row(lx, ly, h, 1.0 / h, e, g)) continue;
     AdjSums W = {0.0, 0.0, 0.0, 0.0};
@@ -350,6 +354,12 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
       atomicAdd(&d_verts[2 * v1 + 1], kInvPi * g.n1 * a1);
     }
   }
+#pragma unroll
+  for (int off = 1; off < G; off <<= 1) {
+    dx += __shfl_xor_sync(0xffffffffu, dx, off);
+    dy += __shfl_xor_sync(0xffffffffu, dy, off);
+  }
+  if (!ok || sub != 0) return;
   dx *= kInvPi;
   dy *= kInvPi;
   // world frame: x_local = R^T (x - c)  =>  dL/dx = R dL/dx_local
@@ -620,11 +630,12 @@ extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const d
   rc = sort_rows(s, pos, sup, allowed, n, pose, obb, unbounded, w, st);
   if (rc) return rc;
   const SurfView v = view_of(s);
-  const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
+  constexpr int G = 2;
+  const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads);
   rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
-    k_agg_backward<KT><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.nwork, w.order, w.work, n, pose, g_lam, g_m1,
-                                                  g_m2, d_pos, d_verts);
+    k_agg_backward<KT, G><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.nwork, w.order, w.work, n, pose, g_lam,
+                                                     g_m1, g_m2, d_pos, d_verts);
     return 0;
   });
   if (rc) return rc;
