@@ -57,6 +57,10 @@ def parse():
     return p.parse_args()
 
 
+WORKLOAD = ("c2: 2^20 particles uniform in [0,4]^2, h=0.02, 64 star polygons (32-512 vertices, one multi-loop "
+            "surface), kernels cubic/w2/w4/w6, lambda + 12 moments")
+
+
 def workload(n, rank):
     """the rank's shard of the 2-D workload: the c2 geometry on every rank, rank 0 the c2 particles, the other ranks
     their own seeded particle sets of the same size (weak scaling)."""
@@ -93,6 +97,7 @@ def cpu_reference(loops, X, h, seconds=15.0, procs=None):
             if time.perf_counter() - t0 > seconds:
                 break
     dt = time.perf_counter() - t0
+    cpu_reference.density = pairs / (done * chunk)                     # neighbour pairs per particle of the sample
     return pairs / dt, procs, f"{done} chunks of {chunk} random particles of the scene, kernels cycled; {pairs} pairs in {dt:.1f} s"
 
 
@@ -110,11 +115,13 @@ def reference_arm(args):
         v, procs, sample = cpu_reference(loops, X, h, seconds=8.0, procs=procs)
         steps.append(v)
     value = float(statistics.mean(steps))
+    # one full step (4 kernels over all particles) at the sample's rate and pair density
+    step_ms = len(KERNELS) * cpu_reference.density * len(X) / value * 1e3
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": "c2: 2^20 particles in [0,4]^2, h=0.02, 64 star polygons (32-512 vertices), "
-                                   "kernels cubic/w2/w4/w6", "sample": sample},
+            "config": {"workload": WORKLOAD, "sample": sample,
+                       "ms_per_step": "extrapolated from the sample: 4 kernels x pairs of the full scene / rate"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -576,8 +583,7 @@ def our_arm(args):
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
                 "data": "synthetic (seeded)",
-                "config": {"workload": "c2: 2^20 particles uniform in [0,4]^2, h=0.02, 64 star polygons (32-512 "
-                                       "vertices, one multi-loop surface), kernels cubic/w2/w4/w6, lambda + 12 moments",
+                "config": {"workload": WORKLOAD,
                            "pairs_per_kernel": P, "particles_per_gpu": N, "route": args.route,
                            "precision": args.precision, "l2": "flushed between steps (256 MiB write, untimed)"},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
