@@ -126,9 +126,13 @@ def test_routes_agree_and_error_paths():
         fused.evaluate([WallOutput("L", 0, "lap")])
     with pytest.raises(NotImplementedError):
         AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Gaussian, lean=True)
+    # a conditioned single triangle is served on the fused route (its small / sliver rows by the area quadrature),
+    # not on the plain one
     tri = Scene([Body(reps=[SurfaceRep.polygon([(0, 0), (0.01, 0), (0, 0.01)])])], DEV)
+    fw_tri = AnalyticBoundary(tri).aggregate(ps, h, kernel=KernelFunctions.Wendland2, lean=True)
+    assert torch.isfinite(fw_tri.out["lam"]).all()
     with pytest.raises(NotImplementedError):
-        AnalyticBoundary(tri).aggregate(ps, h, kernel=KernelFunctions.Wendland2, lean=True)
+        AnalyticBoundary(tri, route="plain").aggregate(ps, h, kernel=KernelFunctions.Wendland2, lean=True)
     # copy_from carries a new position set into the buffers of an existing aggregate
     X2 = X + 0.003
     ps2 = ParticleState(torch.tensor(X2, device=DEV), ps.supports)

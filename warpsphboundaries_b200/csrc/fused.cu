@@ -96,6 +96,12 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
 
 // Per sorted row: its number of neighbour pairs (float-prefiltered exact predicate over its cell's candidates) as a
 // radix key, and its winding indicator -- both kernel independent, computed once per position set.
+// a 32-byte record through the read-only data path (two 16-byte loads)
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return make_double4(a.x, a.y, b.x, b.y);
+}
+
 __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const int32_t* __restrict__ key,
                               const double* __restrict__ lpos, const int32_t* __restrict__ offs,
                               const int32_t* __restrict__ order, int64_t n, double* __restrict__ ind,
@@ -120,8 +126,11 @@ __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const 
         const double ry = __dadd_rn(S.lo_y, __dmul_rn(__dadd_rn((double)cy, 0.5), S.cell));
         bool degenerate = S.cok[b] == 0;
         int cross = 0;
-        for (int k = S.cstart[b]; k < S.cstart[b + 1]; ++k) {
-          const double4 e = S.crec[k];
+        const int k0 = S.cstart[b], k1 = S.cstart[b + 1];
+        double4 nxt = k0 < k1 ? ldg4(S.crec + k0) : make_double4(0.0, 0.0, 0.0, 0.0);
+        for (int k = k0; k < k1; ++k) {
+          const double4 e = nxt;
+          if (k + 1 < k1) nxt = ldg4(S.crec + k + 1);               // one record ahead
           cnt += seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h) ? 1 : 0;
           if (!degenerate) cross += segment_crossing(rx, ry, lx, ly, e, &degenerate);
         }
@@ -209,12 +218,15 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
   double acc[12];
 #pragma unroll
   for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+  // the next candidate's record is loaded one step ahead, so its latency hides behind the current pair's closed form
+  double4 nxt = k < e1 ? ldg4(S.crec + k) : make_double4(0.0, 0.0, 0.0, 0.0);
   while (__any_sync(0xffffffffu, k < e1)) {
     double4 e = make_double4(0.0, 0.0, 0.0, 0.0);
     bool have = false;
     while (k < e1) {
-      e = S.crec[k];
+      e = nxt;
       k += G;
+      if (k < e1) nxt = ldg4(S.crec + k);
       if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
         have = true;
         break;

@@ -87,7 +87,7 @@ class FusedWall(WallAggregate):
             if g.kernel not in KERNEL_IDS:
                 raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} (wall-operator layout: cover / "
                                           f"Laplacian / tensile) is not built; use the lean layout")
-        sig = tuple(id(r) for b in scene.bodies for r in b.reps)
+        sig = (route,) + tuple(id(r) for b in scene.bodies for r in b.reps)
         if getattr(scene, "_wsb_checked", None) != sig:
             for b in scene.bodies:
                 for r in b.reps:
