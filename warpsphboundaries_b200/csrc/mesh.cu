@@ -336,15 +336,19 @@ __device__ __forceinline__ void node_eval(double u, double wt, double sgn_side, 
 }
 
 // the panels of one edge (both sides of the foot of the perpendicular): [u0, u1] of distances from the foot, split
-// at the kernel's knot and at c 2^k; at most 26 panels a side (c 2^k runs from 2^-24 to 1)
+// at the kernel's knot and at c 2^k (k >= 1); at most 26 panels a side (c 2^k runs from 2^-24 to 1).  A panel that
+// starts within 2c of the foot (the branch points of r sit at distance c from the foot) takes 16 Gauss-Legendre
+// nodes (relative error below 2e-15 on [0, 2c]), the graded ones further out 12 (below 1e-18 on [2^k c, 2^(k+1) c]).
+// A typical edge (side lengths up to 2c) is then 32 nodes: one round of the warp's lanes.
 constexpr int kMaxPanels = 64;
 struct PanelList {
   double lo[kMaxPanels], hi[kMaxPanels], sg[kMaxPanels];
+  int off[kMaxPanels + 1];    // first node of each panel; off[np] = all nodes
 };
 
 template <class M>
 __device__ int build_panels(PanelList& PL, double s0, double s1, double c) {
-  int np = 0;
+  int np = 0, nodes = 0;
   double knot = -1.0;
   if constexpr (M::kPieces > 1) {
     if (c < M::kBreak) knot = sqrt((M::kBreak - c) * (M::kBreak + c));
@@ -355,7 +359,7 @@ __device__ int build_panels(PanelList& PL, double s0, double s1, double c) {
     const double u0 = side == 0 ? fmax(-s1, 0.0) : fmax(s0, 0.0);
     const double u1 = side == 0 ? -s0 : s1;
     if (!(u1 > u0)) continue;
-    double d = base;
+    double d = 2.0 * base;
     for (int it = 0; it < 64 && d <= u0; ++it) d *= 2.0;
     double u = u0;
     for (int it = 0; it < 96 && u < u1 && np < kMaxPanels; ++it) {
@@ -364,11 +368,14 @@ __device__ int build_panels(PanelList& PL, double s0, double s1, double c) {
       PL.lo[np] = u;
       PL.hi[np] = nxt;
       PL.sg[np] = sgn;
+      PL.off[np] = nodes;
+      nodes += u < 2.0 * base ? 16 : 12;
       ++np;
       if (nxt >= d) d *= 2.0;
       u = nxt;
     }
   }
+  PL.off[np] = nodes;
   return np;
 }
 
@@ -463,7 +470,7 @@ __device__ __forceinline__ void edge_assemble(double* __restrict__ Av, const dou
 }
 
 // the contribution of face f to the row's accumulators (the warp's shared array Av), computed by the whole warp: the
-// geometry is the same in every lane, the quadrature nodes of an edge (12 per panel) are spread over the lanes and
+// geometry is the same in every lane, the quadrature nodes of an edge (12 or 16 per panel) are spread over the lanes and
 // their sums reduced by a fixed butterfly, lane 0 adds the edge's terms to Av.  Everything is linear in the per-edge integrals.  Faces that do not meet the
 // support contribute exactly nothing: skipped.  q in world units, ih = 1 / support.
 template <class M>
@@ -501,11 +508,15 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
       if (lane == 0) np = build_panels<M>(PL, s0, s1, c);
       np = __shfl_sync(0xffffffffu, np, 0);
       __syncwarp();
-      for (int k = lane; k < 12 * np; k += 32) {
-        const int p = k / 12, g = k - 12 * p;
+      int p = 0;
+      for (int k = lane; k < PL.off[np]; k += 32) {
+        while (k >= PL.off[p + 1]) ++p;
+        const int g = k - PL.off[p];
+        const bool n16 = PL.off[p + 1] - PL.off[p] == 16;
+        const double xg = n16 ? kTriGx16[g] : kRadialGx[g], wg = n16 ? kTriGw16[g] : kRadialGw[g];
         const double x0 = PL.lo[p], x1 = PL.hi[p];
         const double hc = 0.5 * (x1 - x0);
-        node_eval<M>(fma(hc, kRadialGx[g], 0.5 * (x1 + x0)), kRadialGw[g] * hc, PL.sg[p], c2, a, z, sg, w, S);
+        node_eval<M>(fma(hc, xg, 0.5 * (x1 + x0)), wg * hc, PL.sg[p], c2, a, z, sg, w, S);
       }
 #pragma unroll
       for (int i = 0; i < 6; ++i) S.J[i] = warp_sum(S.J[i]);
