@@ -460,30 +460,59 @@ __global__ void k_kinematics(const double* __restrict__ bodies, int32_t nb, cons
   }
 }
 
-// exclusive prefix sums of m counts in one block: each thread scans a contiguous chunk, the chunk totals are
-// scanned across the block (the bucket counts of the row sort: one cell grid's worth of entries)
+// exclusive prefix sums of m counts in one block, tile by tile: a tile of kScanThreads x kScanItems counts is loaded
+// coalesced into shared memory (padded one word every 32 against bank conflicts), each thread scans its kScanItems
+// consecutive counts, the thread totals are scanned with warp shuffles, and the tile is written back coalesced with
+// the running total of the earlier tiles added (the bucket counts of the row sort: one cell grid's worth of entries)
 constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+__device__ __forceinline__ int scan_pad(int k) { return k + (k >> 5); }
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_block(const int32_t* __restrict__ in, int32_t* __restrict__ out,
                                                             int64_t m) {
-  __shared__ int32_t s_tot[kScanThreads];
-  const int t = threadIdx.x;
-  const int64_t chunk = (m + kScanThreads - 1) / kScanThreads;
-  const int64_t a = min((int64_t)t * chunk, m), b = min(a + chunk, m);
-  int32_t sum = 0;
-  for (int64_t i = a; i < b; ++i) sum += in[i];
-  s_tot[t] = sum;
-  __syncthreads();
-  for (int d = 1; d < kScanThreads; d <<= 1) {       // inclusive Hillis-Steele scan of the chunk totals
-    const int32_t v = t >= d ? s_tot[t - d] : 0;
+  __shared__ int32_t s_data[kScanTile + kScanTile / 32];
+  __shared__ int32_t s_warp[kScanThreads / 32];
+  __shared__ int32_t s_carry;
+  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+  if (t == 0) s_carry = 0;
+  for (int64_t base = 0; base < m; base += kScanTile) {
+    const int tile = (int)min((int64_t)kScanTile, m - base);
+    for (int k = t; k < kScanTile; k += kScanThreads) s_data[scan_pad(k)] = k < tile ? in[base + k] : 0;
     __syncthreads();
-    s_tot[t] += v;
+    int32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) sum += s_data[scan_pad(t * kScanItems + i)];
+    int32_t x = sum;                                   // inclusive scan of the thread totals within the warp
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int32_t y = __shfl_up_sync(0xffffffffu, x, d);
+      if (lane >= d) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
     __syncthreads();
-  }
-  int32_t run = t ? s_tot[t - 1] : 0;
-  for (int64_t i = a; i < b; ++i) {
-    const int32_t v = in[i];
-    out[i] = run;
-    run += v;
+    if (wid == 0) {                                    // inclusive scan of the 32 warp totals
+      int32_t v = s_warp[lane];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, v, d);
+        if (lane >= d) v += y;
+      }
+      s_warp[lane] = v;
+    }
+    __syncthreads();
+    int32_t run = s_carry + (wid ? s_warp[wid - 1] : 0) + (x - sum);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+      const int p = scan_pad(t * kScanItems + i);
+      const int32_t v = s_data[p];
+      s_data[p] = run;
+      run += v;
+    }
+    __syncthreads();
+    if (t == kScanThreads - 1) s_carry = run;          // the total of this and the earlier tiles
+    for (int k = t; k < tile; k += kScanThreads) out[base + k] = s_data[scan_pad(k)];
+    __syncthreads();
   }
 }
 
