@@ -593,7 +593,7 @@ def our_arm(args):
                              "peak_source": "measured: libwsbpeak FP64 FMA stream (this GPU, this run)",
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
                 "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
-                "gpu_launches": args.steps * (5 + 2 * len(KERNELS)),   # prepare: 5 kernels; per kernel: rows + pairs
+                "gpu_launches": args.steps * (5 + len(KERNELS)),   # prepare: 5 kernels; per kernel: one pair kernel
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh, "adjoint": adjoint,
                 **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)

@@ -160,14 +160,12 @@ __device__ __forceinline__ void finish_row(double acc[12], double ind, double ma
   write_outputs(acc, h, rot, i, lam, G, cov, m1, m2, assign);
 }
 
-// rows without neighbour pairs: the indicator times the whole-plane channels (or zeros for non-candidates when the
-// outputs are assigned), coalesced over the row index
+// a row without neighbour pairs: the indicator times the whole-plane channels (or zeros for a non-candidate when the
+// outputs are assigned); the tail blocks of k_agg_pairs run these coalesced over the row index
 template <class KT>
-__global__ void k_agg_rows(const double* __restrict__ sup, const double* __restrict__ ind,
-                           const int32_t* __restrict__ flag, int64_t n, const double* __restrict__ pose, bool assign,
-                           double* lam, double* G, double* cov, double* m1, double* m2) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ __forceinline__ void constant_row(int64_t i, const double* __restrict__ sup, const double* __restrict__ ind,
+                                             const int32_t* __restrict__ flag, const double* __restrict__ pose,
+                                             bool assign, double* lam, double* G, double* cov, double* m1, double* m2) {
   const int32_t f = flag[i];
   if (f == 2 || (f == 0 && !assign)) return;
   double acc[12];
@@ -176,8 +174,11 @@ __global__ void k_agg_rows(const double* __restrict__ sup, const double* __restr
   finish_row(acc, f == 1 ? ind[i] : 0.0, KT::kMass, KT::kPlane2, sup[i], pose, i, assign, lam, G, cov, m1, m2);
 }
 
-// Rows with neighbour pairs only (compacted, cell order).  A group of G adjacent lanes owns one row and splits its
-// cell's candidates (lane g takes candidates g, g + G, ...).  Each iteration every lane first advances, with the cheap
+// Rows with neighbour pairs (compacted, cell order), then the rows without: the first ceil(nwork G / kThreads) blocks
+// take the work rows, the next ceil(n / kThreads) blocks the constant rows (one row a thread, coalesced), so the
+// constant rows' stores overlap the last wave of pair blocks instead of running as a launch of their own; the grid
+// is sized for nwork = n and blocks past both ranges return.  A group of G adjacent lanes owns one work row and
+// splits its cell's candidates (lane g takes candidates g, g + G, ...).  Each iteration every lane first advances, with the cheap
 // float-prefiltered predicate, to its next neighbour edge; then all lanes that found one evaluate the closed form
 // together.  The G partial sums are combined by an xor butterfly (the same additions on every lane, commutative, so
 // the result is deterministic and identical on the G lanes).
@@ -193,12 +194,18 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
                                                        const int32_t* __restrict__ order,
                                                        const int32_t* __restrict__ work,
                                                        const int32_t* __restrict__ nwork_p, int64_t n,
-                                                       const double* __restrict__ ind, const double* __restrict__ pose,
+                                                       const double* __restrict__ ind,
+                                                       const int32_t* __restrict__ flag, const double* __restrict__ pose,
                                                        bool assign, double* lam, double* G_, double* cov, double* m1,
                                                        double* m2) {
   static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "lanes per row");
   const int64_t nwork = *nwork_p;
-  if ((int64_t)blockIdx.x * (blockDim.x / G) >= nwork) return;     // whole CTA past the work rows
+  const int64_t wblocks = (nwork + kThreads / G - 1) / (kThreads / G);
+  if ((int64_t)blockIdx.x >= wblocks) {                             // a tail block: constant rows
+    const int64_t i = ((int64_t)blockIdx.x - wblocks) * kThreads + threadIdx.x;
+    if (i < n) constant_row<KT>(i, sup, ind, flag, pose, assign, lam, G_, cov, m1, m2);
+    return;
+  }
   const int64_t w = (int64_t)blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
   const int sub = threadIdx.x % G;
   const bool ok = w < nwork;
@@ -264,10 +271,10 @@ template <class KT, int PREC>
 static void launch_pairs(const SurfView& v, const double* sup, const Workspace& w, int64_t n, const double* pose,
                          bool assign, double* L, double* Gp, double* C, double* M1, double* M2, cudaStream_t st) {
   const int G = lanes_per_row();
-  const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads);
+  const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads + (n + kThreads - 1) / kThreads);
 #define WSB_PAIRS(GG)                                                                                          \
   k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.order, w.work, w.nwork, n, w.ind, \
-                                                       pose, assign, L, Gp, C, M1, M2)
+                                                       w.flag, pose, assign, L, Gp, C, M1, M2)
   switch (G) {
     case 8: WSB_PAIRS(8); break;
     case 1: WSB_PAIRS(1); break;
@@ -618,11 +625,9 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   double* M1 = (out_mask & WSB_OUT_M1) ? m1 : nullptr;
   double* M2 = (out_mask & WSB_OUT_M2) ? m2 : nullptr;
   const SurfView v = view_of(s);
-  const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
   const bool assign = (out_mask & WSB_OUT_ASSIGN) != 0;
   int rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
-    k_agg_rows<KT><<<grid, kThreads, 0, st>>>(sup, w.ind, w.flag, n, pose, assign, L, Gp, C, M1, M2);
     if (precision == WSB_PREC_MIXED)
       launch_pairs<KT, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, L, Gp, C, M1, M2, st);
     else
