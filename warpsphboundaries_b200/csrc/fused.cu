@@ -24,6 +24,7 @@ struct Workspace {
   double* ind;       // [n] indicator of a row (by row index)
   int32_t* flag;     // [n] 0 not a candidate, 1 candidate without neighbour pairs, 2 row with pairs (by row index)
   int32_t* rkey;     // [n] count key of a sorted row: 63 - min(pairs, 63) for rows with pairs, 64 otherwise
+  uint64_t* mask;    // [2n] by sorted row: bit k set when candidate k (< kMaskBits) of the row's cell is a neighbour
   int32_t* khist;    // [kKeys] rows per key   } zeroed together
   int32_t* kcur;     // [kKeys] fill cursors   }
   int32_t* work;     // [n] rows with pairs first, by decreasing pair count
@@ -49,6 +50,7 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
   w.ind = (double*)take(sizeof(double) * std::max<int64_t>(n, 1));
   w.flag = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
   w.rkey = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.mask = (uint64_t*)take(sizeof(uint64_t) * 2 * std::max<int64_t>(n, 1));
   w.khist = (int32_t*)take(sizeof(int32_t) * 2 * kKeys);
   w.kcur = w.khist + kKeys;
   w.work = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
@@ -97,6 +99,25 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
 // Per sorted row: its number of neighbour pairs (float-prefiltered exact predicate over its cell's candidates) as a
 // radix key, and its winding indicator -- both kernel independent, computed once per position set.
 // a 32-byte record through the read-only data path (two 16-byte loads)
+// the neighbour mask of a row covers the first kMaskBits candidates of its cell; later candidates (cells holding more
+// edges) are found again by the predicate in the pair kernel
+constexpr int kMaskBits = 128;
+
+// index of the lowest set bit of the 128-bit mask (m0 low word), cleared; -1 when the mask is empty
+__device__ __forceinline__ int pop_bit(uint64_t& m0, uint64_t& m1) {
+  if (m0) {
+    const int b = __ffsll((long long)m0) - 1;
+    m0 &= m0 - 1;
+    return b;
+  }
+  if (m1) {
+    const int b = 63 + __ffsll((long long)m1);
+    m1 &= m1 - 1;
+    return b;
+  }
+  return -1;
+}
+
 __device__ __forceinline__ double4 ldg4(const double4* p) {
   const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
   return make_double4(a.x, a.y, b.x, b.y);
@@ -105,7 +126,8 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
 __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const int32_t* __restrict__ key,
                               const double* __restrict__ lpos, const int32_t* __restrict__ offs,
                               const int32_t* __restrict__ order, int64_t n, double* __restrict__ ind,
-                              int32_t* __restrict__ flag, int32_t* __restrict__ rkey, int32_t* __restrict__ khist) {
+                              int32_t* __restrict__ flag, int32_t* __restrict__ rkey, uint64_t* __restrict__ mask,
+                              int32_t* __restrict__ khist) {
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   int cnt = 0;
   if (j < n) {
@@ -126,14 +148,23 @@ __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const 
         const double ry = __dadd_rn(S.lo_y, __dmul_rn(__dadd_rn((double)cy, 0.5), S.cell));
         bool degenerate = S.cok[b] == 0;
         int cross = 0;
+        uint64_t m0 = 0, m1 = 0;
         const int k0 = S.cstart[b], k1 = S.cstart[b + 1];
         double4 nxt = k0 < k1 ? ldg4(S.crec + k0) : make_double4(0.0, 0.0, 0.0, 0.0);
         for (int k = k0; k < k1; ++k) {
           const double4 e = nxt;
           if (k + 1 < k1) nxt = ldg4(S.crec + k + 1);               // one record ahead
-          cnt += seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h) ? 1 : 0;
+          if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
+            ++cnt;
+            const int r = k - k0;
+            if (r < 64)
+              m0 |= 1ull << r;
+            else if (r < kMaskBits)
+              m1 |= 1ull << (r - 64);
+          }
           if (!degenerate) cross += segment_crossing(rx, ry, lx, ly, e, &degenerate);
         }
+        reinterpret_cast<ulonglong2*>(mask)[j] = make_ulonglong2(m0, m1);
         w = degenerate ? indicator_at(S, lx, ly, h, true, b) : S.cind[b] + (double)cross;
       }
       ind[i] = w;
@@ -178,10 +209,12 @@ __device__ __forceinline__ void constant_row(int64_t i, const double* __restrict
 // take the work rows, the next ceil(n / kThreads) blocks the constant rows (one row a thread, coalesced), so the
 // constant rows' stores overlap the last wave of pair blocks instead of running as a launch of their own; the grid
 // is sized for nwork = n and blocks past both ranges return.  A group of G adjacent lanes owns one work row and
-// splits its cell's candidates (lane g takes candidates g, g + G, ...).  Each iteration every lane first advances, with the cheap
-// float-prefiltered predicate, to its next neighbour edge; then all lanes that found one evaluate the closed form
-// together.  The G partial sums are combined by an xor butterfly (the same additions on every lane, commutative, so
-// the result is deterministic and identical on the G lanes).
+// splits its neighbours: the row's neighbour mask (set by k_agg_rowinfo) lists them among the first kMaskBits
+// candidates of its cell, and lane g takes those of rank g, g + G, ... in candidate order; candidates past the mask
+// are split g, g + G, ... and found by the float-prefiltered predicate.  Work rows are sorted by pair count, so the
+// lanes of a warp evaluate nearly the same number of closed forms.  The G partial sums are combined by an xor
+// butterfly (the same additions on every lane, commutative, so the result is deterministic and identical on the G
+// lanes); with G = 1 a row's pairs are summed in candidate order.
 template <class KT, int PREC, int G>
 // 6 resident CTAs of 128 threads per SM (at most 80 registers a thread): measured 13 % faster on B200 than the
 // unconstrained 92-94 registers (5 CTAs); 8 CTAs (64 registers) spills
@@ -193,7 +226,8 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
                                                        const double* __restrict__ lpos,
                                                        const int32_t* __restrict__ order,
                                                        const int32_t* __restrict__ work,
-                                                       const int32_t* __restrict__ nwork_p, int64_t n,
+                                                       const int32_t* __restrict__ nwork_p,
+                                                       const uint64_t* __restrict__ mask, int64_t n,
                                                        const double* __restrict__ ind,
                                                        const int32_t* __restrict__ flag, const double* __restrict__ pose,
                                                        bool assign, double* lam, double* G_, double* cov, double* m1,
@@ -210,33 +244,56 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
   const int sub = threadIdx.x % G;
   const bool ok = w < nwork;
   int32_t i = 0;
-  int k = 0, e1 = 0;
+  int kb = 0, kt = 0, e1 = 0;
+  uint64_t mk0 = 0, mk1 = 0;
   double lx = 0.0, ly = 0.0, h = 1.0;
   if (ok) {
-    i = order[work[w]];
+    const int32_t j = work[w];
+    i = order[j];
     const int32_t b = key[i];
     lx = lpos[2 * i];
     ly = lpos[2 * i + 1];
     h = sup[i];
-    k = S.cstart[b] + sub;
+    kb = S.cstart[b];
     e1 = S.cstart[b + 1];
+    kt = kb + kMaskBits + sub;                                      // past the mask: lane sub scans kt, kt + G, ...
+    const ulonglong2 mm = __ldg(reinterpret_cast<const ulonglong2*>(mask) + j);
+    mk0 = mm.x;
+    mk1 = mm.y;
   }
+  // lane sub takes the neighbours of rank sub, sub + G, ... of the mask (in candidate order), then its share of the
+  // candidates past the mask by the predicate
+  for (int s = 0; s < sub; ++s) pop_bit(mk0, mk1);
+  int nb = pop_bit(mk0, mk1);
   const double ih = 1.0 / h;
   double acc[12];
 #pragma unroll
   for (int c = 0; c < 12; ++c) acc[c] = 0.0;
-  // the next candidate's record is loaded one step ahead, so its latency hides behind the current pair's closed form
-  double4 nxt = k < e1 ? ldg4(S.crec + k) : make_double4(0.0, 0.0, 0.0, 0.0);
-  while (__any_sync(0xffffffffu, k < e1)) {
-    double4 e = make_double4(0.0, 0.0, 0.0, 0.0);
+  // the next neighbour's (or tail candidate's) record is loaded one step ahead, so its latency hides behind the
+  // current pair's closed form
+  const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
+  double4 nxt = nb >= 0 ? ldg4(S.crec + kb + nb) : (kt < e1 ? ldg4(S.crec + kt) : zero);
+  while (__any_sync(0xffffffffu, nb >= 0 || kt < e1)) {
+    double4 e = zero;
     bool have = false;
-    while (k < e1) {
+    if (nb >= 0) {
       e = nxt;
-      k += G;
-      if (k < e1) nxt = ldg4(S.crec + k);
-      if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
-        have = true;
-        break;
+      have = true;
+      for (int s = 1; s < G; ++s) pop_bit(mk0, mk1);
+      nb = pop_bit(mk0, mk1);
+      if (nb >= 0)
+        nxt = ldg4(S.crec + kb + nb);
+      else if (kt < e1)
+        nxt = ldg4(S.crec + kt);
+    } else {
+      while (kt < e1) {
+        e = nxt;
+        kt += G;
+        if (kt < e1) nxt = ldg4(S.crec + kt);
+        if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
+          have = true;
+          break;
+        }
       }
     }
     __syncwarp();
@@ -273,8 +330,8 @@ static void launch_pairs(const SurfView& v, const double* sup, const Workspace& 
   const int G = lanes_per_row();
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads + (n + kThreads - 1) / kThreads);
 #define WSB_PAIRS(GG)                                                                                          \
-  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.order, w.work, w.nwork, n, w.ind, \
-                                                       w.flag, pose, assign, L, Gp, C, M1, M2)
+  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.order, w.work, w.nwork, w.mask, n, \
+                                                       w.ind, w.flag, pose, assign, L, Gp, C, M1, M2)
   switch (G) {
     case 8: WSB_PAIRS(8); break;
     case 1: WSB_PAIRS(1); break;
@@ -563,7 +620,8 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
                                         unbounded, w.key, w.lpos, w.counts);
   k_scan_block<<<1, kScanThreads, 0, st>>>(w.counts, w.offs, nbk + 1);
   k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
-  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.khist);
+  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.mask,
+                                            w.khist);
   k_key_scatter<<<grid, kThreads, 0, st>>>(w.rkey, n, w.khist, w.kcur, w.work, w.nwork);
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
