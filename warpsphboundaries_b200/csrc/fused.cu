@@ -359,15 +359,17 @@ __device__ __forceinline__ void adj_blocks(const PairGeo& g, AdjSums& tot) {
   }
 }
 
-// G lanes per work row split its cell's candidates (lane g takes g, g + G, ...; the float-prefiltered predicate, exact
-// where the float decision is within its margin); their d_pos partial sums are combined by a fixed xor butterfly
+// G lanes per work row split its neighbours (lane g takes the neighbours of rank g, g + G, ... of the row's mask, then
+// candidates past the mask g, g + G, ... by the float-prefiltered predicate, exact where the float decision is within
+// its margin); their d_pos partial sums are combined by a fixed xor butterfly
 template <class KT, int G>
 __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const double* __restrict__ sup,
                                                           const int32_t* __restrict__ key,
                                                           const double* __restrict__ lpos,
                                                           const int32_t* __restrict__ offs,
                                                           const int32_t* __restrict__ order,
-                                                          const int32_t* __restrict__ work, int64_t n,
+                                                          const int32_t* __restrict__ work,
+                                                          const uint64_t* __restrict__ mask, int64_t n,
                                                           const double* __restrict__ pose,
                                                           const double* __restrict__ g_lam,
                                                           const double* __restrict__ g_m1,
@@ -376,7 +378,8 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
   const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
   const int sub = threadIdx.x % G;
   const bool ok = w < n && w < (int64_t)offs[0];      // work rows only (rows with neighbour pairs; offs = counter)
-  const int32_t i = ok ? order[work[w]] : 0;
+  const int32_t j = ok ? work[w] : 0;
+  const int32_t i = ok ? order[j] : 0;
   const int32_t b = ok ? key[i] : 0;
   const double lx = ok ? lpos[2 * i] : 0.0, ly = ok ? lpos[2 * i + 1] : 0.0, h = ok ? sup[i] : 1.0;
   const double c = pose[2], s = pose[3];
@@ -400,10 +403,35 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
   // physical units: d m_alpha = h^(|alpha| - 1) / pi * (unit integral)
   const double u0 = gl / h, u1x = g10, u1y = g01, u2x = g20 * h, u2m = g11 * h, u2y = g02 * h;
   double dx = 0.0, dy = 0.0;
-  const int kend = ok ? S.cstart[b + 1] : 0;
-  for (int k = ok ? S.cstart[b] + sub : 0; k < kend; k += G) {
+  // the row's neighbours: lane sub takes ranks sub, sub + G, ... of the neighbour mask, then its share of the
+  // candidates past the mask by the predicate
+  const int kb = ok ? S.cstart[b] : 0, kend = ok ? S.cstart[b + 1] : 0;
+  int kt = kb + kMaskBits + sub;
+  uint64_t mk0 = 0, mk1 = 0;
+  if (ok) {
+    const ulonglong2 mm = __ldg(reinterpret_cast<const ulonglong2*>(mask) + j);
+    mk0 = mm.x;
+    mk1 = mm.y;
+  }
+  for (int r = 0; r < sub; ++r) pop_bit(mk0, mk1);
+  for (;;) {
+    int k = pop_bit(mk0, mk1);
+    if (k >= 0) {
+      k += kb;
+      for (int r = 1; r < G; ++r) pop_bit(mk0, mk1);
+    } else {
+      while (kt < kend) {
+        const double4 c4 = S.crec[kt];
+        const int kk = kt;
+        kt += G;
+        if (seg_within_fast(lx, ly, c4.x, c4.y, c4.z, c4.w, h)) {
+          k = kk;
+          break;
+        }
+      }
+      if (k < 0) break;
+    }
     const double4 e = S.crec[k];
-    if (!seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) continue;
     PairGeo g;
     if (!pair_geo_row(lx, ly, h, 1.0 / h, e, g)) continue;
     AdjSums W = {0.0, 0.0, 0.0, 0.0};
@@ -738,8 +766,8 @@ extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const d
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads);
   rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
-    k_agg_backward<KT, G><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.nwork, w.order, w.work, n, pose, g_lam,
-                                                     g_m1, g_m2, d_pos, d_verts);
+    k_agg_backward<KT, G><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.nwork, w.order, w.work, w.mask, n, pose,
+                                                     g_lam, g_m1, g_m2, d_pos, d_verts);
     return 0;
   });
   if (rc) return rc;
