@@ -2,6 +2,7 @@
 // body-frame position, runs the float64 neighbour predicate over the row's cell and accumulates the closed-form
 // channels of every neighbour pair in registers, then adds the indicator, scales and rotates.  Also the adjoint of the
 // moments, signed distance and rigid-body kinematics.
+#include <cstddef>
 #include <cstdlib>
 #include <mutex>
 
@@ -13,6 +14,22 @@ constexpr int kThreads = 128;
 constexpr int kKeys = 65;          // count keys: 0..63 rows with pairs (63 - min(pairs, 63)), 64 rows without
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// the neighbour mask of a row covers the first kMaskBits candidates of its cell; later candidates (cells holding more
+// edges) are found again by the predicate in the pair kernel
+constexpr int kMaskBits = 128;
+
+// one work row (a row with neighbour pairs) as the pair and adjoint kernels read it: one coalesced 64-byte load
+struct __align__(16) WorkRec {
+  double lx, ly;           // [0, 16)  body-frame position
+  double h;                // [16, 24) support
+  int32_t row, kb;         // [24, 32) row index, first candidate of the row's cell
+  uint64_t m0, m1;         // [32, 48) neighbour mask of the first kMaskBits candidates
+  int32_t ke, pad[3];      // [48, 64) end of the cell's candidates
+};
+static_assert(sizeof(WorkRec) == 64 && offsetof(WorkRec, h) == 16 && offsetof(WorkRec, row) == 24 &&
+                  offsetof(WorkRec, kb) == 28 && offsetof(WorkRec, m0) == 32 && offsetof(WorkRec, ke) == 48,
+              "work record layout");
 
 struct Workspace {
   int32_t* key;      // [n] bucket of a row: cell id, ncells = outside the grid, ncells + 1 = not a candidate
@@ -27,7 +44,7 @@ struct Workspace {
   uint64_t* mask;    // [2n] by sorted row: bit k set when candidate k (< kMaskBits) of the row's cell is a neighbour
   int32_t* khist;    // [kKeys] rows per key   } zeroed together
   int32_t* kcur;     // [kKeys] fill cursors   }
-  int32_t* work;     // [n] rows with pairs first, by decreasing pair count
+  WorkRec* wrec;     // [n] work rows by decreasing pair count (slots < nwork used)
   int32_t* nwork;    // [1] number of rows with pairs
   size_t total;
 };
@@ -53,7 +70,7 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
   w.mask = (uint64_t*)take(sizeof(uint64_t) * 2 * std::max<int64_t>(n, 1));
   w.khist = (int32_t*)take(sizeof(int32_t) * 2 * kKeys);
   w.kcur = w.khist + kKeys;
-  w.work = (int32_t*)take(sizeof(int32_t) * std::max<int64_t>(n, 1));
+  w.wrec = (WorkRec*)take(sizeof(WorkRec) * std::max<int64_t>(n, 1));
   w.nwork = (int32_t*)take(sizeof(int32_t));
   w.total = off;
   return w;
@@ -99,10 +116,6 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
 // Per sorted row: its number of neighbour pairs (float-prefiltered exact predicate over its cell's candidates) as a
 // radix key, and its winding indicator -- both kernel independent, computed once per position set.
 // a 32-byte record through the read-only data path (two 16-byte loads)
-// the neighbour mask of a row covers the first kMaskBits candidates of its cell; later candidates (cells holding more
-// edges) are found again by the predicate in the pair kernel
-constexpr int kMaskBits = 128;
-
 // index of the lowest set bit of the 128-bit mask (m0 low word), cleared; -1 when the mask is empty
 __device__ __forceinline__ int pop_bit(uint64_t& m0, uint64_t& m1) {
   if (m0) {
@@ -116,6 +129,23 @@ __device__ __forceinline__ int pop_bit(uint64_t& m0, uint64_t& m1) {
     return b;
   }
   return -1;
+}
+
+// a work record by three 16-byte loads and one 4-byte load through the read-only path
+__device__ __forceinline__ WorkRec load_workrec(const WorkRec* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+  const longlong2 b = __ldg(reinterpret_cast<const longlong2*>(p) + 1);
+  const ulonglong2 m = __ldg(reinterpret_cast<const ulonglong2*>(p) + 2);
+  WorkRec r;
+  r.lx = a.x;
+  r.ly = a.y;
+  r.h = __longlong_as_double(b.x);
+  r.row = (int32_t)(uint32_t)((unsigned long long)b.y & 0xffffffffull);
+  r.kb = (int32_t)(uint32_t)((unsigned long long)b.y >> 32);
+  r.m0 = m.x;
+  r.m1 = m.y;
+  r.ke = __ldg(reinterpret_cast<const int32_t*>(p) + 12);
+  return r;
 }
 
 __device__ __forceinline__ double4 ldg4(const double4* p) {
@@ -222,12 +252,8 @@ template <class KT, int PREC, int G>
 #define WSB_PAIRS_MIN_BLOCKS 6
 #endif
 __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(SurfView S, const double* __restrict__ sup,
-                                                       const int32_t* __restrict__ key,
-                                                       const double* __restrict__ lpos,
-                                                       const int32_t* __restrict__ order,
-                                                       const int32_t* __restrict__ work,
-                                                       const int32_t* __restrict__ nwork_p,
-                                                       const uint64_t* __restrict__ mask, int64_t n,
+                                                       const WorkRec* __restrict__ wrec,
+                                                       const int32_t* __restrict__ nwork_p, int64_t n,
                                                        const double* __restrict__ ind,
                                                        const int32_t* __restrict__ flag, const double* __restrict__ pose,
                                                        bool assign, double* lam, double* G_, double* cov, double* m1,
@@ -248,18 +274,16 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
   uint64_t mk0 = 0, mk1 = 0;
   double lx = 0.0, ly = 0.0, h = 1.0;
   if (ok) {
-    const int32_t j = work[w];
-    i = order[j];
-    const int32_t b = key[i];
-    lx = lpos[2 * i];
-    ly = lpos[2 * i + 1];
-    h = sup[i];
-    kb = S.cstart[b];
-    e1 = S.cstart[b + 1];
+    const WorkRec r = load_workrec(wrec + w);
+    i = r.row;
+    lx = r.lx;
+    ly = r.ly;
+    h = r.h;
+    kb = r.kb;
+    e1 = r.ke;
     kt = kb + kMaskBits + sub;                                      // past the mask: lane sub scans kt, kt + G, ...
-    const ulonglong2 mm = __ldg(reinterpret_cast<const ulonglong2*>(mask) + j);
-    mk0 = mm.x;
-    mk1 = mm.y;
+    mk0 = r.m0;
+    mk1 = r.m1;
   }
   // lane sub takes the neighbours of rank sub, sub + G, ... of the mask (in candidate order), then its share of the
   // candidates past the mask by the predicate
@@ -330,8 +354,8 @@ static void launch_pairs(const SurfView& v, const double* sup, const Workspace& 
   const int G = lanes_per_row();
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads + (n + kThreads - 1) / kThreads);
 #define WSB_PAIRS(GG)                                                                                          \
-  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.order, w.work, w.nwork, w.mask, n, \
-                                                       w.ind, w.flag, pose, assign, L, Gp, C, M1, M2)
+  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, L, \
+                                                       Gp, C, M1, M2)
   switch (G) {
     case 8: WSB_PAIRS(8); break;
     case 1: WSB_PAIRS(1); break;
@@ -364,12 +388,8 @@ __device__ __forceinline__ void adj_blocks(const PairGeo& g, AdjSums& tot) {
 // its margin); their d_pos partial sums are combined by a fixed xor butterfly
 template <class KT, int G>
 __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const double* __restrict__ sup,
-                                                          const int32_t* __restrict__ key,
-                                                          const double* __restrict__ lpos,
-                                                          const int32_t* __restrict__ offs,
-                                                          const int32_t* __restrict__ order,
-                                                          const int32_t* __restrict__ work,
-                                                          const uint64_t* __restrict__ mask, int64_t n,
+                                                          const WorkRec* __restrict__ wrec,
+                                                          const int32_t* __restrict__ nwork_p, int64_t n,
                                                           const double* __restrict__ pose,
                                                           const double* __restrict__ g_lam,
                                                           const double* __restrict__ g_m1,
@@ -377,11 +397,11 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
                                                           double* d_verts) {
   const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) / G;
   const int sub = threadIdx.x % G;
-  const bool ok = w < n && w < (int64_t)offs[0];      // work rows only (rows with neighbour pairs; offs = counter)
-  const int32_t j = ok ? work[w] : 0;
-  const int32_t i = ok ? order[j] : 0;
-  const int32_t b = ok ? key[i] : 0;
-  const double lx = ok ? lpos[2 * i] : 0.0, ly = ok ? lpos[2 * i + 1] : 0.0, h = ok ? sup[i] : 1.0;
+  const bool ok = w < n && w < (int64_t)*nwork_p;    // work rows only (rows with neighbour pairs)
+  WorkRec r{};
+  if (ok) r = load_workrec(wrec + w);
+  const int32_t i = ok ? r.row : 0;
+  const double lx = ok ? r.lx : 0.0, ly = ok ? r.ly : 0.0, h = ok ? r.h : 1.0;
   const double c = pose[2], s = pose[3];
   // upstream gradients in the body frame and in channel units: m1_world = R m1, m2_world = R m2 R^T
   const double gl = g_lam && ok ? g_lam[i] : 0.0;
@@ -405,14 +425,9 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
   double dx = 0.0, dy = 0.0;
   // the row's neighbours: lane sub takes ranks sub, sub + G, ... of the neighbour mask, then its share of the
   // candidates past the mask by the predicate
-  const int kb = ok ? S.cstart[b] : 0, kend = ok ? S.cstart[b + 1] : 0;
+  const int kb = ok ? r.kb : 0, kend = ok ? r.ke : 0;
   int kt = kb + kMaskBits + sub;
-  uint64_t mk0 = 0, mk1 = 0;
-  if (ok) {
-    const ulonglong2 mm = __ldg(reinterpret_cast<const ulonglong2*>(mask) + j);
-    mk0 = mm.x;
-    mk1 = mm.y;
-  }
+  uint64_t mk0 = ok ? r.m0 : 0, mk1 = ok ? r.m1 : 0;
   for (int r = 0; r < sub; ++r) pop_bit(mk0, mk1);
   for (;;) {
     int k = pop_bit(mk0, mk1);
@@ -611,8 +626,11 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_block(const int32_t* __re
 // rows with pairs into `work`, grouped by count key (decreasing pair count): the prefix of the key histogram per
 // block, then warp-aggregated cursor atomics (the order inside a key group is arbitrary; every row's result is
 // independent of it)
-__global__ void k_key_scatter(const int32_t* __restrict__ rkey, int64_t n, const int32_t* __restrict__ khist,
-                              int32_t* __restrict__ kcur, int32_t* __restrict__ work, int32_t* __restrict__ nwork) {
+__global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int64_t n, const int32_t* __restrict__ khist,
+                              int32_t* __restrict__ kcur, const int32_t* __restrict__ order,
+                              const int32_t* __restrict__ bucket, const double* __restrict__ lpos,
+                              const double* __restrict__ sup, const uint64_t* __restrict__ mask,
+                              WorkRec* __restrict__ wrec, int32_t* __restrict__ nwork) {
   __shared__ int32_t s_pre[kKeys + 1];
   if (threadIdx.x == 0) {
     int32_t run = 0;
@@ -633,7 +651,23 @@ __global__ void k_key_scatter(const int32_t* __restrict__ rkey, int64_t n, const
   int base = 0;
   if (mine && lane == leader) base = atomicAdd(&kcur[key], __popc(peers));
   base = __shfl_sync(0xffffffffu, base, leader);
-  if (mine) work[s_pre[key] + base + __popc(peers & ((1u << lane) - 1))] = (int32_t)j;
+  if (mine) {
+    // gather the row's record once here, so the evaluations read one coalesced record per work row
+    const int32_t i = order[j];
+    const int32_t b = bucket[i];
+    const ulonglong2 mm = reinterpret_cast<const ulonglong2*>(mask)[j];
+    WorkRec r;
+    r.lx = lpos[2 * i];
+    r.ly = lpos[2 * i + 1];
+    r.h = sup[i];
+    r.row = i;
+    r.kb = S.cstart[b];
+    r.ke = S.cstart[b + 1];
+    r.pad[0] = r.pad[1] = r.pad[2] = 0;
+    r.m0 = mm.x;
+    r.m1 = mm.y;
+    wrec[s_pre[key] + base + __popc(peers & ((1u << lane) - 1))] = r;
+  }
 }
 
 // shared front half of the aggregate and its adjoint: body frame, broadphase, counting sort of the rows by cell
@@ -650,7 +684,8 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
   k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
   k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.mask,
                                             w.khist);
-  k_key_scatter<<<grid, kThreads, 0, st>>>(w.rkey, n, w.khist, w.kcur, w.work, w.nwork);
+  k_key_scatter<<<grid, kThreads, 0, st>>>(v, w.rkey, n, w.khist, w.kcur, w.order, w.key, w.lpos, sup, w.mask, w.wrec,
+                                           w.nwork);
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }
@@ -766,8 +801,8 @@ extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const d
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads);
   rc = dispatch_kernel(kernel, [&](auto kt) {
     using KT = decltype(kt);
-    k_agg_backward<KT, G><<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.nwork, w.order, w.work, w.mask, n, pose,
-                                                     g_lam, g_m1, g_m2, d_pos, d_verts);
+    k_agg_backward<KT, G><<<grid, kThreads, 0, st>>>(v, sup, w.wrec, w.nwork, n, pose, g_lam, g_m1, g_m2, d_pos,
+                                                     d_verts);
     return 0;
   });
   if (rc) return rc;
