@@ -290,8 +290,8 @@ __device__ __forceinline__ void special_fns(double lo, double hi, double rlo, do
 // A_n = int_lo^hi r^n ds by the parity recurrence, the six chord sums of the block and their contribution to the twelve
 // channels (before the common 1/pi).  acc layout: 0 lam, 1-2 m1, 3-4 G, 5-8 g1 (g(1,0)_x, g(1,0)_y, g(0,1)_x,
 // g(0,1)_y), 9-11 m20, m11, m02 -- the per-edge values of the reference plan (warpbc.py:98-117, 970-991).
-template <class KT, int B, int PREC>
-__device__ __forceinline__ void block_channels(const PairGeo& g, double acc[12]) {
+template <class KT, int B, int PREC, class Acc>
+__device__ __forceinline__ void block_channels(const PairGeo& g, Acc acc) {
   constexpr double R = KT::kR[B];
   constexpr int NA = KT::kNA[B];
   const double az = fabs(g.z);
@@ -335,8 +335,9 @@ __device__ __forceinline__ void block_channels(const PairGeo& g, double acc[12])
   acc[11] += g.n1 * Z1 - Vp;
 }
 
-template <class KT, int B, int PREC>
-__device__ __forceinline__ void all_blocks(const PairGeo& g, double acc[12]) {
+// acc: a double* or any type whose operator[] gives the channel's accumulator by reference
+template <class KT, int B, int PREC, class Acc>
+__device__ __forceinline__ void all_blocks(const PairGeo& g, Acc acc) {
   if constexpr (B < KT::kBlocks) {
     block_channels<KT, B, PREC>(g, acc);
     all_blocks<KT, B + 1, PREC>(g, acc);

@@ -131,6 +131,12 @@ __device__ __forceinline__ int pop_bit(uint64_t& m0, uint64_t& m1) {
   return -1;
 }
 
+// one thread's channel accumulators in a [12][kThreads] shared array
+struct SmemAcc {
+  double* p;
+  __device__ __forceinline__ double& operator[](int c) const { return p[c * kThreads]; }
+};
+
 // a work record by three 16-byte loads and one 4-byte load through the read-only path
 __device__ __forceinline__ WorkRec load_workrec(const WorkRec* p) {
   const double2 a = __ldg(reinterpret_cast<const double2*>(p));
@@ -246,10 +252,11 @@ __device__ __forceinline__ void constant_row(int64_t i, const double* __restrict
 // butterfly (the same additions on every lane, commutative, so the result is deterministic and identical on the G
 // lanes); with G = 1 a row's pairs are summed in candidate order.
 template <class KT, int PREC, int G>
-// 6 resident CTAs of 128 threads per SM (at most 80 registers a thread): measured 13 % faster on B200 than the
-// unconstrained 92-94 registers (5 CTAs); 8 CTAs (64 registers) spills
+// 7 resident CTAs of 128 threads per SM (at most 72 registers a thread, channel sums in shared memory): measured on
+// B200 on the 2^20-particle scene 12.2e9 pairs/s against 12.0e9 with 6 or 8 CTAs and 11.6e9 with the sums in
+// registers (6 CTAs, 80 registers and spills)
 #ifndef WSB_PAIRS_MIN_BLOCKS
-#define WSB_PAIRS_MIN_BLOCKS 6
+#define WSB_PAIRS_MIN_BLOCKS 7
 #endif
 __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(SurfView S, const double* __restrict__ sup,
                                                        const WorkRec* __restrict__ wrec,
@@ -290,9 +297,11 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
   for (int s = 0; s < sub; ++s) pop_bit(mk0, mk1);
   int nb = pop_bit(mk0, mk1);
   const double ih = 1.0 / h;
-  double acc[12];
+  // the twelve channel sums live in shared memory: 24 registers fewer a thread, no spills at 72 registers
+  __shared__ double s_acc[12 * kThreads];
+  const SmemAcc acc_s{s_acc + threadIdx.x};
 #pragma unroll
-  for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+  for (int c = 0; c < 12; ++c) acc_s[c] = 0.0;
   // the next neighbour's (or tail candidate's) record is loaded one step ahead, so its latency hides behind the
   // current pair's closed form
   const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -323,9 +332,12 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
     __syncwarp();
     if (have) {
       PairGeo g;
-      if (pair_geo_row(lx, ly, h, ih, e, g)) all_blocks<KT, 0, PREC>(g, acc);
+      if (pair_geo_row(lx, ly, h, ih, e, g)) all_blocks<KT, 0, PREC>(g, acc_s);
     }
   }
+  double acc[12];
+#pragma unroll
+  for (int c = 0; c < 12; ++c) acc[c] = acc_s[c];
 #pragma unroll
   for (int off = 1; off < G; off <<= 1) {
 #pragma unroll
@@ -338,7 +350,7 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
 }
 
 // lanes per row of k_agg_pairs: 2 unless WSB_LANES_PER_ROW (1, 2, 4, 8) says otherwise (a tuning knob, read once;
-// 2 measured fastest on the 2^20-particle scene: 1 / 2 / 4 lanes give 6.4 / 8.2 / 7.7e9 pairs/s)
+// 2 measured fastest on the 2^20-particle scene: 1 / 2 lanes give 10.4 / 11.3e9 pairs/s with the neighbour masks)
 static int lanes_per_row() {
   static int v = [] {
     const char* e = getenv("WSB_LANES_PER_ROW");
