@@ -286,6 +286,26 @@ __device__ __forceinline__ void special_fns(double lo, double hi, double rlo, do
   dang = (y == 0.0 && x == 0.0) ? 0.0 : atan2(y, x);
 }
 
+// The chord [s0, s1] of the edge line clipped to the circle r <= R around the row, with one square root per end: an
+// end outside the circle moves to -+L = -+sqrt(R^2 - z^2), where its radius is R; an end inside keeps its radius
+// sqrt(s^2 + z^2).  False when the clipped chord is empty.
+__device__ __forceinline__ bool clip_chord(const PairGeo& g, const double R, double& lo, double& hi, double& rlo,
+                                           double& rhi, double& zz) {
+  const double az = fabs(g.z);
+  if (!(az < R)) return false;
+  zz = g.z * g.z;
+  const double LL = fmax((R - az) * (R + az), 0.0);
+  const double q0 = g.s0 * g.s0 + zz, q1 = g.s1 * g.s1 + zz;
+  const bool c0 = g.s0 < 0.0 && q0 > R * R, c1 = g.s1 > 0.0 && q1 > R * R;
+  const double t0 = sqrt(c0 ? LL : q0), t1 = sqrt(c1 ? LL : q1);
+  lo = c0 ? -t0 : g.s0;
+  hi = c1 ? t1 : g.s1;
+  if (!(lo < hi)) return false;
+  rlo = c0 ? R : t0;
+  rhi = c1 ? R : t1;
+  return true;
+}
+
 // One kernel block (truncated monomial profile on r <= R_B) of one pair: the chord, the monomial chord integrals
 // A_n = int_lo^hi r^n ds by the parity recurrence, the six chord sums of the block and their contribution to the twelve
 // channels (before the common 1/pi).  acc layout: 0 lam, 1-2 m1, 3-4 G, 5-8 g1 (g(1,0)_x, g(1,0)_y, g(0,1)_x,
@@ -294,13 +314,8 @@ template <class KT, int B, int PREC, class Acc>
 __device__ __forceinline__ void block_channels(const PairGeo& g, Acc acc) {
   constexpr double R = KT::kR[B];
   constexpr int NA = KT::kNA[B];
-  const double az = fabs(g.z);
-  if (!(az < R)) return;
-  const double L = sqrt(fmax((R - az) * (R + az), 0.0));
-  const double lo = fmax(g.s0, -L), hi = fmin(g.s1, L);
-  if (!(lo < hi)) return;
-  const double zz = g.z * g.z;
-  const double rlo = sqrt(lo * lo + zz), rhi = sqrt(hi * hi + zz);
+  double lo, hi, rlo, rhi, zz;
+  if (!clip_chord(g, R, lo, hi, rlo, rhi, zz)) return;
   double dasinh, dang;
   special_fns<PREC>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
   double A[NA];
@@ -349,13 +364,8 @@ template <class KT, int B>
 __device__ __forceinline__ bool block_adjoint(const PairGeo& g, AdjSums& o) {
   constexpr double R = KT::kR[B];
   constexpr int NA = KT::kNAadj[B];
-  const double az = fabs(g.z);
-  if (!(az < R)) return false;
-  const double L = sqrt(fmax((R - az) * (R + az), 0.0));
-  const double lo = fmax(g.s0, -L), hi = fmin(g.s1, L);
-  if (!(lo < hi)) return false;
-  const double zz = g.z * g.z;
-  const double rlo = sqrt(lo * lo + zz), rhi = sqrt(hi * hi + zz);
+  double lo, hi, rlo, rhi, zz;
+  if (!clip_chord(g, R, lo, hi, rlo, rhi, zz)) return false;
   double dasinh, dang;
   special_fns<WSB_PREC_FP64>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
   double A[NA];
