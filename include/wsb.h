@@ -126,9 +126,9 @@ int wsb_aggregate_evaluate(const wsb_surface* s, int kernel, int precision, cons
 
 /* wsb_aggregate without a caller workspace, for hosts that cannot allocate device memory for this library (their
  * allocator owns the GPU's memory, or their step loop may not call cudaMalloc / cudaFree, which synchronise the
- * device).  No counterpart in the reference: it exists for such C-ABI callers.  The scratch is a static 8 MiB device
+ * device).  No counterpart in the reference: it exists for such C-ABI callers.  The scratch is a static 16 MiB device
  * array inside libwsb.so (per GPU, held until the library is unloaded); the call allocates nothing.  It serves about
- * 52 bytes per row plus 12 bytes per cell of the surface's grid, e.g. 131072 rows over a 256 x 256 grid; larger
+ * 120 bytes per row plus 12 bytes per cell of the surface's grid, e.g. 131072 rows over a 256 x 256 grid; larger
  * requests fail with WSB_ERR_SIZE.  The first call on a device looks the scratch address up (make that first call
  * before any stream capture).  All calls share the one array: calls that overlap on the GPU (other streams, other
  * threads) race and must be serialised by the caller; each call clears the counters it needs. */

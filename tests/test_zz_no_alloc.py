@@ -79,3 +79,27 @@ def test_noalloc_refuses_requests_beyond_its_scratch():
                                         *[_lib.ptr(t) for t in out], None, None)
     assert rc == _lib.WSB_ERR_SIZE
     assert "scratch" in _lib.last_error()
+
+
+def test_noalloc_serves_its_documented_capacity():
+    """131072 rows over a grid of at most 256 x 256 cells fit the built-in scratch, and the call runs."""
+    from warpsphboundaries_b200 import _lib, workloads
+    from warpsphboundaries_b200.scene import Body, SurfaceRep, _stream
+
+    dev = torch.device("cuda", 0)
+    h = 0.004
+    rep = SurfaceRep.loops(workloads.stars(3, (32, 64), seed=2, box=1.0))
+    body = Body(reps=[rep])
+    ns = rep.native(h, dev)
+    assert ns.info.nx <= 256 and ns.info.ny <= 256
+    n = 131072
+    assert _lib.lib.wsb_aggregate_workspace_size(ns.handle, n) <= 16 << 20
+    pos = torch.rand((n, 2), dtype=torch.float64, device=dev)
+    sup = torch.full((n,), h, dtype=torch.float64, device=dev)
+    out = _outputs(n, dev)
+    obb = (ctypes.c_double * 4)(*body.obb())
+    _lib.check(_lib.lib.wsb_aggregate_noalloc(ns.handle, 2, _lib.PREC_FP64, _lib.ptr(pos), _lib.ptr(sup), None, n,
+                                              _lib.ptr(body.pose_tensor(dev)), obb, 0, _lib.OUT_ALL,
+                                              *[_lib.ptr(t) for t in out], None, _stream()), "wsb_aggregate_noalloc")
+    torch.cuda.synchronize()
+    assert torch.isfinite(out[0]).all()

@@ -856,7 +856,7 @@ extern "C" int wsb_kinematics(const double* bodies, int32_t n_bodies, const doub
 // long as the library is loaded.  The address of that array is looked up once per device (cudaGetSymbolAddress with
 // the device current) on the first call for that device; host code must never pass the array's own name to a kernel,
 // since on the host that name only stands in for the device symbol.
-constexpr size_t kNoAllocScratchBytes = (size_t)8 << 20;
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 static void* g_noalloc_addr[64] = {nullptr};
 static std::mutex g_noalloc_mu;
