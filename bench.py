@@ -363,7 +363,7 @@ def our_arm(args):
     from warpsphboundaries_b200 import _lib
     from warpsphboundaries_b200.fixedadj import fixed_topology
     from warpsphboundaries_b200.kernels import KERNEL_IDS, pair_work
-    from warpsphboundaries_b200.provider import AnalyticBoundary, WallOutput
+    from warpsphboundaries_b200.provider import AnalyticBoundary, FusedGroup, FusedWall, WallOutput
     from warpsphboundaries_b200.scene import Body, Scene, SurfaceRep, _stream
     from warpsphboundaries_b200.shim import KernelFunctions, ParticleState
 
@@ -390,7 +390,11 @@ def our_arm(args):
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def step(precision, timers=None):
+    kids = _lib.int32s([KERNEL_IDS[k] for k in KERNELS])
+    gout = [_lib.ptrs([outs[k][j] for k in KERNELS]) for j in range(5)]
+
+    def step(precision, timers=None, grouped=True):
+        """prepare, then the four kernel groups: one grouped pass (the FusedWall path), or one pass per kernel"""
         ev = []
         e0 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -399,6 +403,19 @@ def our_arm(args):
         e1 = torch.cuda.Event(enable_timing=True)
         e1.record(stream)
         ev.append(("prepare", e0, e1))
+        if grouped:
+            a = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _lib.check(_lib.lib.wsb_aggregate_evaluate_groups(ns.handle, len(KERNELS), kids, prec[precision],
+                                                              _lib.ptr(sup), N, _lib.ptr(pose),
+                                                              _lib.OUT_ALL | _lib.OUT_ASSIGN, *gout, _lib.ptr(ws),
+                                                              need, _stream()), "evaluate_groups")
+            b = torch.cuda.Event(enable_timing=True)
+            b.record(stream)
+            ev.append(("groups", a, b))
+            if timers is not None:
+                timers.append(ev)
+            return
         for k in KERNELS:
             o = outs[k]
             a = torch.cuda.Event(enable_timing=True)
@@ -413,9 +430,9 @@ def our_arm(args):
         if timers is not None:
             timers.append(ev)
 
-    def timed(precision, steps, warmup):
+    def timed(precision, steps, warmup, grouped=True):
         for _ in range(warmup):
-            step(precision)
+            step(precision, grouped=grouped)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -423,13 +440,13 @@ def our_arm(args):
         for _ in range(steps):
             flush.fill_(1)
             torch.cuda.synchronize()
-            step(precision, timers)
+            step(precision, timers, grouped=grouped)
             torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         step_ms = [ev[0][1].elapsed_time(ev[-1][2]) for ev in timers]
-        eval_ms = {k: statistics.mean(e[i + 1][1].elapsed_time(e[i + 1][2]) for e in timers)
-                   for i, k in enumerate(KERNELS)}
+        eval_ms = {name: statistics.mean(e[i][1].elapsed_time(e[i][2]) for e in timers)
+                   for i, (name, _, _) in enumerate(timers[0]) if i > 0}
         prep_ms = statistics.mean(e[0][1].elapsed_time(e[0][2]) for e in timers)
         return sum(step_ms), eval_ms, prep_ms
 
@@ -437,6 +454,11 @@ def our_arm(args):
     clocks.start(local)
     total_ms, eval_ms, prep_ms = timed(args.precision, args.steps, args.warmup)
     clk = clocks.stop()
+    # the same four kernels as four single-kernel passes over the prepared rows (reported beside the grouped pass)
+    sep_ms = None
+    if world == 1:
+        ms_s, ev_s, pr_s = timed(args.precision, max(3, args.steps // 2), 1, grouped=False)
+        sep_ms = {**ev_s, "prepare": pr_s, "step": ms_s / max(3, args.steps // 2)}
     from warpsphboundaries_b200 import shard
     total_ms = shard.max_over_ranks(total_ms, dev)             # the slowest rank's device time
     pairs_step = P * len(KERNELS)                              # this rank's pairs per step
@@ -515,7 +537,6 @@ def our_arm(args):
     # ---- end to end through the public API with host buffers
     e2e = None
     if not args.no_e2e:
-        ab = AnalyticBoundary(scene, route="fused", precision=args.precision)
         hpos = torch.tensor(X, dtype=torch.float64).pin_memory()
         hsup = torch.full((N,), h, dtype=torch.float64).pin_memory()
         dpos = torch.empty_like(pos)
@@ -523,29 +544,17 @@ def our_arm(args):
         host_out = {k: [torch.empty((1, N), dtype=torch.float64).pin_memory(),
                         torch.empty((1, N, 2), dtype=torch.float64).pin_memory(),
                         torch.empty((1, N, 2, 2), dtype=torch.float64).pin_memory()] for k in KERNELS}
-        kf = {"cubic": KernelFunctions.CubicSpline, "w2": KernelFunctions.Wendland2, "w4": KernelFunctions.Wendland4,
-              "w6": KernelFunctions.Wendland6}
-
-        copy_stream = torch.cuda.Stream(device=dev)
+        groups = tuple(FusedGroup(k) for k in KERNELS)
 
         def e2e_step():
-            # inputs up, then each kernel's results down on a second stream while the next kernel computes (the
-            # results of a step stay referenced until the step has synchronised)
+            # inputs up, the four kernel groups of the scene in one FusedWall (fused.py:506-547), results down
             dpos.copy_(hpos, non_blocking=True)
             dsup.copy_(hsup, non_blocking=True)
-            ps = ParticleState(dpos, dsup)
-            keep = []
-            for k in KERNELS:
-                fw = ab.aggregate(ps, h, kernel=kf[k], lean=True)
-                keep.append(fw)
-                done = torch.cuda.Event()
-                done.record(stream)
-                copy_stream.wait_event(done)
-                with torch.cuda.stream(copy_stream):
-                    for dst, name in zip(host_out[k], ("lam", "G", "Cov")):
-                        dst.copy_(fw.out[name], non_blocking=True)
-            stream.wait_stream(copy_stream)
-            return keep
+            fw = FusedWall(scene, ParticleState(dpos, dsup), h, groups, precision=args.precision)
+            for gi, k in enumerate(KERNELS):
+                for dst, name in zip(host_out[k], ("lam", "G", "Cov")):
+                    dst.copy_(fw.res[gi][name], non_blocking=True)
+            return fw
 
         for _ in range(args.warmup):
             e2e_step()
@@ -588,12 +597,13 @@ def our_arm(args):
                            "precision": args.precision, "l2": "flushed between steps (256 MiB write, untimed)"},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                              "frac": achieved / fp64_peak, "traffic": traffic,
-                             "kernel": "k_agg_pairs (wsb_aggregate_evaluate)",
+                             "kernel": "k_agg_pairs<KPack<cubic, w2, w4, w6>> (wsb_aggregate_evaluate_groups)",
                              "flops_per_pair": {k: pair_work(k)["flops"] for k in KERNELS},
                              "peak_source": "measured: libwsbpeak FP64 FMA stream (this GPU, this run)",
                              "fp32_peak_tflops": fp32_peak, "hbm_gbs_measured_peaks": peaks.get("hbm_gbs")},
                 "kernel_ms": {**{k: v for k, v in eval_ms.items()}, "prepare": prep_ms},
-                "gpu_launches": args.steps * (5 + len(KERNELS)),   # prepare: 5 kernels; per kernel: one pair kernel
+                "kernel_ms_separate": sep_ms,
+                "gpu_launches": args.steps * (5 + 1),   # prepare: 5 kernels; one pair kernel for the four groups
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh, "adjoint": adjoint,
                 **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)

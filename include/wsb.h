@@ -124,6 +124,25 @@ int wsb_aggregate_evaluate(const wsb_surface* s, int kernel, int precision, cons
                            const double* pose, int out_mask, double* lam, double* G, double* cov, double* m1,
                            double* m2, const void* workspace, size_t workspace_bytes, void* stream);
 
+/* Several kernel groups over one position set, as FusedWall evaluates its tuple of groups in one launch family
+ * (src/warpSPHBoundaries/scene/fused.py:506-547; edge/warpfused.py:58-109 FusedPlan and :190 fused_channels).
+ * kernels [n_groups] (host) lists the groups' kernel ids; lam, G, cov, m1, m2 are HOST arrays of n_groups device
+ * pointers each (the array, or an entry, may be NULL when out_mask leaves that output out); group g is written as
+ * wsb_aggregate_evaluate with kernels[g] would write it.  When the groups are exactly {cubic, w2, w4, w6} or
+ * {w2, w4, w6} (any order) one pass over the neighbour pairs evaluates them all, sharing each pair's chord, special
+ * functions and monomial integrals between kernel blocks of equal support radius; other sets run one pass per group.
+ * At most WSB_MAX_GROUPS groups.  _groups = _prepare + _evaluate_groups. */
+enum { WSB_MAX_GROUPS = 8 };
+int wsb_aggregate_evaluate_groups(const wsb_surface* s, int n_groups, const int32_t* kernels, int precision,
+                                  const double* sup, int64_t n, const double* pose, int out_mask, double* const* lam,
+                                  double* const* G, double* const* cov, double* const* m1, double* const* m2,
+                                  const void* workspace, size_t workspace_bytes, void* stream);
+int wsb_aggregate_groups(const wsb_surface* s, int n_groups, const int32_t* kernels, int precision, const double* pos,
+                         const double* sup, const int32_t* allowed, int64_t n, const double* pose, const double* obb,
+                         int unbounded, int out_mask, double* const* lam, double* const* G, double* const* cov,
+                         double* const* m1, double* const* m2, void* workspace, size_t workspace_bytes,
+                         void* stream);
+
 /* wsb_aggregate without a caller workspace, for hosts that cannot allocate device memory for this library (their
  * allocator owns the GPU's memory, or their step loop may not call cudaMalloc / cudaFree, which synchronise the
  * device).  No counterpart in the reference: it exists for such C-ABI callers.  The scratch is a static 16 MiB device

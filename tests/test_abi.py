@@ -45,3 +45,15 @@ def test_errors_without_device_are_raised_not_silent():
     with pytest.raises(ValueError):
         _lib.check(rc, "wsb_fixed_topology")
     assert _lib.lib.wsb_version() >= 100
+
+
+def test_grouped_aggregate_checks_its_arguments_without_a_device():
+    """the grouped entry points refuse a NULL surface before touching a device."""
+    from warpsphboundaries_b200 import _lib
+    none5 = [_lib.ptrs([None]) for _ in range(5)]
+    rc = _lib.lib.wsb_aggregate_evaluate_groups(None, 1, _lib.int32s([2]), _lib.PREC_FP64, None, 4, None,
+                                                _lib.OUT_ALL, *none5, None, 0, None)
+    assert rc == _lib.WSB_ERR_ARG
+    rc = _lib.lib.wsb_aggregate_groups(None, 1, _lib.int32s([2]), _lib.PREC_FP64, None, None, None, 4, None, None, 0,
+                                       _lib.OUT_ALL, *none5, None, 0, None)
+    assert rc == _lib.WSB_ERR_ARG

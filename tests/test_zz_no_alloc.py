@@ -87,8 +87,10 @@ def test_noalloc_serves_its_documented_capacity():
     from warpsphboundaries_b200.scene import Body, SurfaceRep, _stream
 
     dev = torch.device("cuda", 0)
-    h = 0.004
-    rep = SurfaceRep.loops(workloads.stars(3, (32, 64), seed=2, box=1.0))
+    loops = workloads.stars(3, (32, 64), seed=2, box=1.0)
+    V = np.concatenate(loops)
+    h = float((V.max(0) - V.min(0)).max()) / 250.0          # the grid spans the extent + 2 h in cells of h
+    rep = SurfaceRep.loops(loops)
     body = Body(reps=[rep])
     ns = rep.native(h, dev)
     assert ns.info.nx <= 256 and ns.info.ny <= 256

@@ -19,7 +19,7 @@ OUT_LAM, OUT_G, OUT_COV, OUT_M1, OUT_M2, OUT_ALL, OUT_ASSIGN = 1, 2, 4, 8, 16, 3
 EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_destroy", "wsb_surface_info_get",
            "wsb_surface_cells", "wsb_fixed_topology", "wsb_slot_channels_plain", "wsb_contract",
            "wsb_aggregate_workspace_size", "wsb_aggregate", "wsb_aggregate_prepare", "wsb_aggregate_evaluate",
-           "wsb_aggregate_noalloc",
+           "wsb_aggregate_evaluate_groups", "wsb_aggregate_groups", "wsb_aggregate_noalloc",
            "wsb_aggregate_backward", "wsb_signed_distance",
            "wsb_kinematics", "wsb_radial_channels", "wsb_mesh_create", "wsb_mesh_destroy",
            "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels", "wsb_triangle_channels",
@@ -38,7 +38,7 @@ def _load():
         raise RuntimeError(f"{LIB_PATH} is not built: run `python -m warpsphboundaries_b200.build` "
                            "(this package has no CPU fallback)")
     lib = ctypes.CDLL(str(LIB_PATH))
-    P, D, I32P = c_void_p, POINTER(c_double), POINTER(c_int32)
+    P, D, I32P, PP = c_void_p, POINTER(c_double), POINTER(c_int32), POINTER(c_void_p)
     sig = {
         "wsb_last_error": (c_char_p, []),
         "wsb_version": (c_int, []),
@@ -54,6 +54,10 @@ def _load():
                                   P, P]),
         "wsb_aggregate_prepare": (c_int, [P, P, P, P, c_int64, P, D, c_int, P, c_size_t, P]),
         "wsb_aggregate_evaluate": (c_int, [P, c_int, c_int, P, c_int64, P, c_int, P, P, P, P, P, P, c_size_t, P]),
+        "wsb_aggregate_evaluate_groups": (c_int, [P, c_int, I32P, c_int, P, c_int64, P, c_int, PP, PP, PP, PP, PP, P,
+                                                  c_size_t, P]),
+        "wsb_aggregate_groups": (c_int, [P, c_int, I32P, c_int, P, P, P, c_int64, P, D, c_int, c_int, PP, PP, PP, PP,
+                                         PP, P, c_size_t, P]),
         "wsb_aggregate_noalloc": (c_int, [P, c_int, c_int, P, P, P, c_int64, P, D, c_int, c_int, P, P, P, P, P, P,
                                           P]),
         "wsb_aggregate_backward": (c_int, [P, c_int, P, P, P, c_int64, P, D, c_int, P, P, P, P, P, P, c_size_t, P]),
@@ -99,6 +103,16 @@ def check(rc, what=""):
 def ptr(t):
     """device (or host) address of a tensor, None -> NULL."""
     return None if t is None else c_void_p(t.data_ptr())
+
+
+def ptrs(tensors):
+    """a host array of device addresses (None -> NULL), for the per-group output arguments."""
+    return (c_void_p * len(tensors))(*[None if t is None else t.data_ptr() for t in tensors])
+
+
+def int32s(values):
+    """a host int32 array."""
+    return (c_int32 * len(values))(*values)
 
 
 def dptr(a):

@@ -306,19 +306,11 @@ __device__ __forceinline__ bool clip_chord(const PairGeo& g, const double R, dou
   return true;
 }
 
-// One kernel block (truncated monomial profile on r <= R_B) of one pair: the chord, the monomial chord integrals
-// A_n = int_lo^hi r^n ds by the parity recurrence, the six chord sums of the block and their contribution to the twelve
-// channels (before the common 1/pi).  acc layout: 0 lam, 1-2 m1, 3-4 G, 5-8 g1 (g(1,0)_x, g(1,0)_y, g(0,1)_x,
-// g(0,1)_y), 9-11 m20, m11, m02 -- the per-edge values of the reference plan (warpbc.py:98-117, 970-991).
-template <class KT, int B, int PREC, class Acc>
-__device__ __forceinline__ void block_channels(const PairGeo& g, Acc acc) {
-  constexpr double R = KT::kR[B];
-  constexpr int NA = KT::kNA[B];
-  double lo, hi, rlo, rhi, zz;
-  if (!clip_chord(g, R, lo, hi, rlo, rhi, zz)) return;
-  double dasinh, dang;
-  special_fns<PREC>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
-  double A[NA];
+// The monomial chord integrals A_n = int_lo^hi r^n ds, n < NA, by the parity recurrence: A_0 = hi - lo, A_1 through
+// the asinh difference, A_n = (hi rhi^n - lo rlo^n + n z^2 A_{n-2}) / (n + 1).
+template <int NA>
+__device__ __forceinline__ void chord_monomials(double lo, double hi, double rlo, double rhi, double zz, double dasinh,
+                                                double* A) {
   A[0] = hi - lo;
   if (NA > 1) A[1] = 0.5 * (hi * rhi - lo * rlo + zz * dasinh);
   double ph = rhi, pl = rlo;
@@ -328,8 +320,14 @@ __device__ __forceinline__ void block_channels(const PairGeo& g, Acc acc) {
     pl *= rlo;
     A[n] = (hi * ph - lo * pl + (double)n * zz * A[n - 2]) * (1.0 / (double)(n + 1));
   }
-  BlockSums S;
-  KT::template sums<B>(A, rlo, rhi, S);
+}
+
+// The contribution of one block's chord sums S (chord angle dang) to the twelve channels (before the common 1/pi).
+// acc layout: 0 lam, 1-2 m1, 3-4 G, 5-8 g1 (g(1,0)_x, g(1,0)_y, g(0,1)_x, g(0,1)_y), 9-11 m20, m11, m02 -- the
+// per-edge values of the reference plan (warpbc.py:98-117, 970-991).  acc: a double* or any type whose operator[]
+// gives the channel's accumulator by reference.
+template <class Acc>
+__device__ __forceinline__ void add_block(const PairGeo& g, const BlockSums& S, double dang, Acc acc) {
   const double Vl = g.z * S.Lreg - S.Mhat * dang;
   const double Vp = g.z * S.Preg - S.MPhat * dang;
   acc[0] += Vl;
@@ -350,13 +348,21 @@ __device__ __forceinline__ void block_channels(const PairGeo& g, Acc acc) {
   acc[11] += g.n1 * Z1 - Vp;
 }
 
-// acc: a double* or any type whose operator[] gives the channel's accumulator by reference
+// One kernel block (truncated monomial profile on r <= R_B) of one pair: the clipped chord, its monomial integrals,
+// the six chord sums of the block and their contribution to the twelve channels.
 template <class KT, int B, int PREC, class Acc>
-__device__ __forceinline__ void all_blocks(const PairGeo& g, Acc acc) {
-  if constexpr (B < KT::kBlocks) {
-    block_channels<KT, B, PREC>(g, acc);
-    all_blocks<KT, B + 1, PREC>(g, acc);
-  }
+__device__ __forceinline__ void block_channels(const PairGeo& g, Acc acc) {
+  constexpr double R = KT::kR[B];
+  constexpr int NA = KT::kNA[B];
+  double lo, hi, rlo, rhi, zz;
+  if (!clip_chord(g, R, lo, hi, rlo, rhi, zz)) return;
+  double dasinh, dang;
+  special_fns<PREC>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
+  double A[NA];
+  chord_monomials<NA>(lo, hi, rlo, rhi, zz, dasinh, A);
+  BlockSums S;
+  KT::template sums<B>(A, rlo, rhi, S);
+  add_block(g, S, dang, acc);
 }
 
 // the adjoint chord sums of one block: int s^j P ds, j = 0..3 (units of h, pi-free)
@@ -369,15 +375,7 @@ __device__ __forceinline__ bool block_adjoint(const PairGeo& g, AdjSums& o) {
   double dasinh, dang;
   special_fns<WSB_PREC_FP64>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
   double A[NA];
-  A[0] = hi - lo;
-  if (NA > 1) A[1] = 0.5 * (hi * rhi - lo * rlo + zz * dasinh);
-  double ph = rhi, pl = rlo;
-#pragma unroll
-  for (int n = 2; n < NA; ++n) {
-    ph *= rhi;
-    pl *= rlo;
-    A[n] = (hi * ph - lo * pl + (double)n * zz * A[n - 2]) * (1.0 / (double)(n + 1));
-  }
+  chord_monomials<NA>(lo, hi, rlo, rhi, zz, dasinh, A);
   KT::template adj<B>(A, rlo, rhi, zz, o);
   return true;
 }

@@ -5,6 +5,7 @@
 #include <cstddef>
 #include <cstdlib>
 #include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 
@@ -227,50 +228,175 @@ __device__ __forceinline__ void finish_row(double acc[12], double ind, double ma
   write_outputs(acc, h, rot, i, lam, G, cov, m1, m2, assign);
 }
 
-// a row without neighbour pairs: the indicator times the whole-plane channels (or zeros for a non-candidate when the
-// outputs are assigned); the tail blocks of k_agg_pairs run these coalesced over the row index
-template <class KT>
-__device__ __forceinline__ void constant_row(int64_t i, const double* __restrict__ sup, const double* __restrict__ ind,
-                                             const int32_t* __restrict__ flag, const double* __restrict__ pose,
-                                             bool assign, double* lam, double* G, double* cov, double* m1, double* m2) {
-  const int32_t f = flag[i];
-  if (f == 2 || (f == 0 && !assign)) return;
-  double acc[12];
-#pragma unroll
-  for (int c = 0; c < 12; ++c) acc[c] = 0.0;
-  finish_row(acc, f == 1 ? ind[i] : 0.0, KT::kMass, KT::kPlane2, sup[i], pose, i, assign, lam, G, cov, m1, m2);
+// ------------------------------------------------------------------------------------------------ kernel packs
+// A pack of kernel tables is evaluated in one pass over the neighbour pairs: the kernel groups of one aggregate, as
+// FusedWall evaluates a tuple of groups in one launch family (src/warpSPHBoundaries/scene/fused.py:506-547,
+// warpfused.fused_channels over every group).  The blocks of all the pack's kernels are grouped by support radius R;
+// per pair the clipped chord, its special functions and its monomial integrals are formed once per distinct R (up to
+// the highest power any block of that radius needs), then every (kernel, block) of that radius adds its chord sums
+// into the kernel's own accumulators.  A pack of one kernel is the single-kernel evaluation.
+template <int M>
+struct PackRadii {
+  double r[M];   // distinct block radii in first-seen order (pack order, then block order)
+  int na[M];     // monomial integrals formed at each radius: the most any block of that radius uses
+  int n;
+};
+
+template <int M>
+constexpr void pack_radii_add(PackRadii<M>& a, const double* r, const int* na, int nb) {
+  for (int b = 0; b < nb; ++b) {
+    int d = 0;
+    while (d < a.n && a.r[d] != r[b]) ++d;
+    if (d == a.n) {
+      a.r[d] = r[b];
+      a.na[d] = na[b];
+      ++a.n;
+    } else if (na[b] > a.na[d]) {
+      a.na[d] = na[b];
+    }
+  }
 }
 
-// Rows with neighbour pairs (compacted, cell order), then the rows without: the first ceil(nwork G / kThreads) blocks
-// take the work rows, the next ceil(n / kThreads) blocks the constant rows (one row a thread, coalesced), so the
-// constant rows' stores overlap the last wave of pair blocks instead of running as a launch of their own; the grid
-// is sized for nwork = n and blocks past both ranges return.  A group of G adjacent lanes owns one work row and
-// splits its neighbours: the row's neighbour mask (set by k_agg_rowinfo) lists them among the first kMaskBits
-// candidates of its cell, and lane g takes those of rank g, g + G, ... in candidate order; candidates past the mask
-// are split g, g + G, ... and found by the float-prefiltered predicate.  Work rows are sorted by pair count, so the
-// lanes of a warp evaluate nearly the same number of closed forms.  The G partial sums are combined by an xor
+template <class... KTs>
+constexpr PackRadii<(KTs::kBlocks + ...)> pack_radii() {
+  PackRadii<(KTs::kBlocks + ...)> a{};
+  (pack_radii_add(a, KTs::kR, KTs::kNA, KTs::kBlocks), ...);
+  return a;
+}
+
+template <class... KTs>
+struct KPack {
+  static constexpr int kN = sizeof...(KTs);
+  static constexpr auto kRadii = pack_radii<KTs...>();
+  template <int K>
+  using Kern = std::tuple_element_t<K, std::tuple<KTs...>>;
+};
+
+constexpr int kMaxPack = 4;
+
+// output pointers of the pack's kernels, by pack position (NULL: not written)
+struct PackOut {
+  double* lam[kMaxPack];
+  double* G[kMaxPack];
+  double* cov[kMaxPack];
+  double* m1[kMaxPack];
+  double* m2[kMaxPack];
+};
+
+// resident CTAs of 128 threads per SM for a pack of n kernels: the 12 n float64 channel sums of a thread live in shared
+// memory (12 KiB a kernel per CTA), at most 7 CTAs (measured on B200 with one kernel on the 2^20-particle scene:
+// 12.2e9 pairs/s with 7 CTAs at 72 registers, 12.0e9 with 6 or 8, 11.6e9 with the sums in registers at 6 CTAs)
+constexpr int pack_min_blocks(int n) {
+  const int by_smem = (227 * 1024) / (12 * n * kThreads * 8 + 1024);
+  return by_smem < 7 ? by_smem : 7;
+}
+
+// every (kernel, block) of the pack whose radius is the D-th distinct radius: its chord sums into its accumulators
+template <class Pack, int D, int K, int B>
+__device__ __forceinline__ void pack_blocks_at(const PairGeo& g, const double* A, double rlo, double rhi, double dang,
+                                               double* acc_t) {
+  if constexpr (K < Pack::kN) {
+    using KT = typename Pack::template Kern<K>;
+    if constexpr (B < KT::kBlocks) {
+      if constexpr (KT::kR[B] == Pack::kRadii.r[D]) {
+        BlockSums S;
+        KT::template sums<B>(A, rlo, rhi, S);
+        add_block(g, S, dang, SmemAcc{acc_t + K * 12 * kThreads});
+      }
+      pack_blocks_at<Pack, D, K, B + 1>(g, A, rlo, rhi, dang, acc_t);
+    } else {
+      pack_blocks_at<Pack, D, K + 1, 0>(g, A, rlo, rhi, dang, acc_t);
+    }
+  }
+}
+
+// one pair, every kernel of the pack: per distinct radius the clipped chord, special functions and monomials once
+template <class Pack, int PREC, int D>
+__device__ __forceinline__ void pack_pair(const PairGeo& g, double* acc_t) {
+  if constexpr (D < Pack::kRadii.n) {
+    constexpr double R = Pack::kRadii.r[D];
+    constexpr int NA = Pack::kRadii.na[D];
+    double lo, hi, rlo, rhi, zz;
+    if (clip_chord(g, R, lo, hi, rlo, rhi, zz)) {
+      double dasinh, dang;
+      special_fns<PREC>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
+      double A[NA];
+      chord_monomials<NA>(lo, hi, rlo, rhi, zz, dasinh, A);
+      pack_blocks_at<Pack, D, 0, 0>(g, A, rlo, rhi, dang, acc_t);
+    }
+    pack_pair<Pack, PREC, D + 1>(g, acc_t);
+  }
+}
+
+// a row without neighbour pairs, every kernel of the pack: the indicator w times the whole-plane channels (w = 0 for
+// a non-candidate when the outputs are assigned)
+template <class Pack, int K>
+__device__ __forceinline__ void pack_constant_row(int64_t i, double w, double h, const double* pose, bool assign,
+                                                  const PackOut& o) {
+  if constexpr (K < Pack::kN) {
+    using KT = typename Pack::template Kern<K>;
+    double acc[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+    finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+    pack_constant_row<Pack, K + 1>(i, w, h, pose, assign, o);
+  }
+}
+
+// a work row, every kernel of the pack: the G lanes' sums combined by an xor butterfly (every lane of the warp takes
+// part), then the lane that writes adds the indicator terms and stores the outputs
+template <class Pack, int G, int K>
+__device__ __forceinline__ void pack_finish(const double* acc_t, bool write, int64_t i, double w, double h,
+                                            const double* pose, bool assign, const PackOut& o) {
+  if constexpr (K < Pack::kN) {
+    using KT = typename Pack::template Kern<K>;
+    double acc[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) acc[c] = acc_t[(K * 12 + c) * kThreads];
+#pragma unroll
+    for (int off = 1; off < G; off <<= 1) {
+#pragma unroll
+      for (int c = 0; c < 12; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+    }
+    if (write) {
+#pragma unroll
+      for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
+      finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+    }
+    pack_finish<Pack, G, K + 1>(acc_t, write, i, w, h, pose, assign, o);
+  }
+}
+
+// Rows with neighbour pairs (compacted, by decreasing pair count), then the rows without: the first
+// ceil(nwork G / kThreads) blocks take the work rows, the next ceil(n / kThreads) blocks the constant rows (one row a
+// thread, coalesced), so the constant rows' stores overlap the last wave of pair blocks instead of running as a launch
+// of their own; the grid is sized for nwork = n and blocks past both ranges return.  A group of G adjacent lanes owns
+// one work row and splits its neighbours: the row's neighbour mask (set by k_agg_rowinfo) lists them among the first
+// kMaskBits candidates of its cell, and lane g takes those of rank g, g + G, ... in candidate order; candidates past
+// the mask are split g, g + G, ... and found by the float-prefiltered predicate.  Work rows are sorted by pair count,
+// so the lanes of a warp evaluate nearly the same number of closed forms.  The G partial sums are combined by an xor
 // butterfly (the same additions on every lane, commutative, so the result is deterministic and identical on the G
-// lanes); with G = 1 a row's pairs are summed in candidate order.
-template <class KT, int PREC, int G>
-// 7 resident CTAs of 128 threads per SM (at most 72 registers a thread, channel sums in shared memory): measured on
-// B200 on the 2^20-particle scene 12.2e9 pairs/s against 12.0e9 with 6 or 8 CTAs and 11.6e9 with the sums in
-// registers (6 CTAs, 80 registers and spills)
-#ifndef WSB_PAIRS_MIN_BLOCKS
-#define WSB_PAIRS_MIN_BLOCKS 7
-#endif
-__global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(SurfView S, const double* __restrict__ sup,
-                                                       const WorkRec* __restrict__ wrec,
-                                                       const int32_t* __restrict__ nwork_p, int64_t n,
-                                                       const double* __restrict__ ind,
-                                                       const int32_t* __restrict__ flag, const double* __restrict__ pose,
-                                                       bool assign, double* lam, double* G_, double* cov, double* m1,
-                                                       double* m2) {
+// lanes).  The channel sums live in shared memory ([kernel][channel][thread]), which keeps the registers for the
+// closed form.
+template <class Pack, int PREC, int G, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const double* __restrict__ sup,
+                                                             const WorkRec* __restrict__ wrec,
+                                                             const int32_t* __restrict__ nwork_p, int64_t n,
+                                                             const double* __restrict__ ind,
+                                                             const int32_t* __restrict__ flag,
+                                                             const double* __restrict__ pose, bool assign,
+                                                             const PackOut out) {
   static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "lanes per row");
+  static_assert(Pack::kN >= 1 && Pack::kN <= kMaxPack, "pack size");
+  __shared__ double s_acc[Pack::kN * 12 * kThreads];
   const int64_t nwork = *nwork_p;
   const int64_t wblocks = (nwork + kThreads / G - 1) / (kThreads / G);
   if ((int64_t)blockIdx.x >= wblocks) {                             // a tail block: constant rows
     const int64_t i = ((int64_t)blockIdx.x - wblocks) * kThreads + threadIdx.x;
-    if (i < n) constant_row<KT>(i, sup, ind, flag, pose, assign, lam, G_, cov, m1, m2);
+    if (i < n) {
+      const int32_t f = flag[i];
+      if (f == 1 || (f == 0 && assign)) pack_constant_row<Pack, 0>(i, f == 1 ? ind[i] : 0.0, sup[i], pose, assign, out);
+    }
     return;
   }
   const int64_t w = (int64_t)blockIdx.x * (blockDim.x / G) + threadIdx.x / G;
@@ -297,11 +423,9 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
   for (int s = 0; s < sub; ++s) pop_bit(mk0, mk1);
   int nb = pop_bit(mk0, mk1);
   const double ih = 1.0 / h;
-  // the twelve channel sums live in shared memory: 24 registers fewer a thread, no spills at 72 registers
-  __shared__ double s_acc[12 * kThreads];
-  const SmemAcc acc_s{s_acc + threadIdx.x};
+  double* const acc_t = s_acc + threadIdx.x;
 #pragma unroll
-  for (int c = 0; c < 12; ++c) acc_s[c] = 0.0;
+  for (int c = 0; c < Pack::kN * 12; ++c) acc_t[c * kThreads] = 0.0;
   // the next neighbour's (or tail candidate's) record is loaded one step ahead, so its latency hides behind the
   // current pair's closed form
   const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -332,49 +456,22 @@ __global__ void __launch_bounds__(kThreads, WSB_PAIRS_MIN_BLOCKS) k_agg_pairs(Su
     __syncwarp();
     if (have) {
       PairGeo g;
-      if (pair_geo_row(lx, ly, h, ih, e, g)) all_blocks<KT, 0, PREC>(g, acc_s);
+      if (pair_geo_row(lx, ly, h, ih, e, g)) pack_pair<Pack, PREC, 0>(g, acc_t);
     }
   }
-  double acc[12];
-#pragma unroll
-  for (int c = 0; c < 12; ++c) acc[c] = acc_s[c];
-#pragma unroll
-  for (int off = 1; off < G; off <<= 1) {
-#pragma unroll
-    for (int c = 0; c < 12; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
-  }
-  if (!ok || sub != 0) return;
-#pragma unroll
-  for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
-  finish_row(acc, ind[i], KT::kMass, KT::kPlane2, h, pose, i, assign, lam, G_, cov, m1, m2);
+  const bool write = ok && sub == 0;
+  pack_finish<Pack, G, 0>(acc_t, write, i, write ? ind[i] : 0.0, h, pose, assign, out);
 }
 
-// lanes per row of k_agg_pairs: 2 unless WSB_LANES_PER_ROW (1, 2, 4, 8) says otherwise (a tuning knob, read once;
-// 2 measured fastest on the 2^20-particle scene: 1 / 2 lanes give 10.4 / 11.3e9 pairs/s with the neighbour masks)
-static int lanes_per_row() {
-  static int v = [] {
-    const char* e = getenv("WSB_LANES_PER_ROW");
-    const int x = e ? atoi(e) : 2;
-    return (x == 1 || x == 2 || x == 4 || x == 8) ? x : 2;
-  }();
-  return v;
-}
-
-template <class KT, int PREC>
-static void launch_pairs(const SurfView& v, const double* sup, const Workspace& w, int64_t n, const double* pose,
-                         bool assign, double* L, double* Gp, double* C, double* M1, double* M2, cudaStream_t st) {
-  const int G = lanes_per_row();
+// the pair kernel of a pack over a prepared workspace (two lanes per work row: measured fastest on the 2^20-particle
+// scene, 1 / 2 lanes give 10.4 / 11.3e9 pairs/s with the neighbour masks)
+template <class Pack, int PREC>
+static void launch_pack(const SurfView& v, const double* sup, const Workspace& w, int64_t n, const double* pose,
+                        bool assign, const PackOut& out, cudaStream_t st) {
+  constexpr int G = 2;
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads + (n + kThreads - 1) / kThreads);
-#define WSB_PAIRS(GG)                                                                                          \
-  k_agg_pairs<KT, PREC, GG><<<grid, kThreads, 0, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, L, \
-                                                       Gp, C, M1, M2)
-  switch (G) {
-    case 8: WSB_PAIRS(8); break;
-    case 1: WSB_PAIRS(1); break;
-    case 4: WSB_PAIRS(4); break;
-    default: WSB_PAIRS(2); break;
-  }
-#undef WSB_PAIRS
+  k_agg_pairs<Pack, PREC, G, pack_min_blocks(Pack::kN)><<<grid, kThreads, 0, st>>>(v, sup, w.wrec, w.nwork, n, w.ind,
+                                                                                  w.flag, pose, assign, out);
 }
 
 // ------------------------------------------------------------------------------------------------ adjoint
@@ -759,15 +856,103 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   double* M2 = (out_mask & WSB_OUT_M2) ? m2 : nullptr;
   const SurfView v = view_of(s);
   const bool assign = (out_mask & WSB_OUT_ASSIGN) != 0;
+  PackOut o{};
+  o.lam[0] = L;
+  o.G[0] = Gp;
+  o.cov[0] = C;
+  o.m1[0] = M1;
+  o.m2[0] = M2;
   int rc = dispatch_kernel(kernel, [&](auto kt) {
-    using KT = decltype(kt);
+    using P1 = KPack<decltype(kt)>;
     if (precision == WSB_PREC_MIXED)
-      launch_pairs<KT, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, L, Gp, C, M1, M2, st);
+      launch_pack<P1, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
     else
-      launch_pairs<KT, WSB_PREC_FP64>(v, sup, w, n, pose, assign, L, Gp, C, M1, M2, st);
+      launch_pack<P1, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
     return 0;
   });
   if (rc) return rc;
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+// the kernel sets evaluated in one pass (as a set: the groups may come in any order); other sets run one pass per group
+static const int32_t kPackCW[4] = {WSB_KERNEL_CUBIC, WSB_KERNEL_W2, WSB_KERNEL_W4, WSB_KERNEL_W6};
+static const int32_t kPackW[3] = {WSB_KERNEL_W2, WSB_KERNEL_W4, WSB_KERNEL_W6};
+
+// perm[p] = the group holding pack kernel p when the groups are exactly the pack's kernels, each once
+static bool match_pack(const int32_t* kernels, int n_groups, const int32_t* pack, int m, int* perm) {
+  if (n_groups != m) return false;
+  for (int p = 0; p < m; ++p) {
+    perm[p] = -1;
+    for (int g = 0; g < n_groups; ++g)
+      if (kernels[g] == pack[p]) {
+        if (perm[p] >= 0) return false;
+        perm[p] = g;
+      }
+    if (perm[p] < 0) return false;
+  }
+  return true;
+}
+
+extern "C" int wsb_aggregate_evaluate_groups(const wsb_surface* s_, int n_groups, const int32_t* kernels,
+                                             int precision, const double* sup, int64_t n, const double* pose,
+                                             int out_mask, double* const* lam, double* const* G, double* const* cov,
+                                             double* const* m1, double* const* m2, const void* workspace,
+                                             size_t workspace_bytes, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate_groups: NULL surface");
+  if (n_groups < 1 || n_groups > WSB_MAX_GROUPS || !kernels)
+    return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate_groups: 1 to " + std::to_string(WSB_MAX_GROUPS) +
+                                 " kernel groups expected");
+  for (int g = 0; g < n_groups; ++g)
+    if (kernels[g] < 0 || kernels[g] >= kNumKernels)
+      return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate_groups: unknown kernel id");
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate_groups: unknown precision mode");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate_groups: row count out of range");
+  if (n == 0) return WSB_OK;
+  if (!sup || !pose) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate_groups: NULL array");
+  auto pick = [&](double* const* a, int g, int bit) { return (a && (out_mask & bit)) ? a[g] : nullptr; };
+  int perm[kMaxPack];
+  const bool cw = match_pack(kernels, n_groups, kPackCW, 4, perm);
+  const bool wn = !cw && match_pack(kernels, n_groups, kPackW, 3, perm);
+  if (!cw && !wn) {                                                 // one pass per group
+    for (int g = 0; g < n_groups; ++g) {
+      const int rc = wsb_aggregate_evaluate(s_, kernels[g], precision, sup, n, pose, out_mask, pick(lam, g, WSB_OUT_LAM),
+                                            pick(G, g, WSB_OUT_G), pick(cov, g, WSB_OUT_COV), pick(m1, g, WSB_OUT_M1),
+                                            pick(m2, g, WSB_OUT_M2), workspace, workspace_bytes, stream);
+      if (rc) return rc;
+    }
+    return WSB_OK;
+  }
+  const Workspace w = carve(s, n, const_cast<void*>(workspace));
+  if (!workspace || workspace_bytes < w.total)
+    return fail(WSB_ERR_SIZE, "wsb_aggregate_evaluate_groups: workspace too small");
+  WSB_CUDA(cudaSetDevice(s->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const SurfView v = view_of(s);
+  const bool assign = (out_mask & WSB_OUT_ASSIGN) != 0;
+  PackOut o{};
+  for (int p = 0; p < (cw ? 4 : 3); ++p) {
+    o.lam[p] = pick(lam, perm[p], WSB_OUT_LAM);
+    o.G[p] = pick(G, perm[p], WSB_OUT_G);
+    o.cov[p] = pick(cov, perm[p], WSB_OUT_COV);
+    o.m1[p] = pick(m1, perm[p], WSB_OUT_M1);
+    o.m2[p] = pick(m2, perm[p], WSB_OUT_M2);
+  }
+  using PCW = KPack<Kern_cubic, Kern_w2, Kern_w4, Kern_w6>;
+  using PW = KPack<Kern_w2, Kern_w4, Kern_w6>;
+  if (cw) {
+    if (precision == WSB_PREC_MIXED)
+      launch_pack<PCW, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
+    else
+      launch_pack<PCW, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
+  } else {
+    if (precision == WSB_PREC_MIXED)
+      launch_pack<PW, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
+    else
+      launch_pack<PW, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
+  }
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }
@@ -790,6 +975,28 @@ extern "C" int wsb_aggregate(const wsb_surface* s_, int kernel, int precision, c
   if (rc) return rc;
   return wsb_aggregate_evaluate(s_, kernel, precision, sup, n, pose, out_mask, lam, G, cov, m1, m2, workspace,
                                 workspace_bytes, stream);
+}
+
+extern "C" int wsb_aggregate_groups(const wsb_surface* s_, int n_groups, const int32_t* kernels, int precision,
+                                    const double* pos, const double* sup, const int32_t* allowed, int64_t n,
+                                    const double* pose, const double* obb, int unbounded, int out_mask,
+                                    double* const* lam, double* const* G, double* const* cov, double* const* m1,
+                                    double* const* m2, void* workspace, size_t workspace_bytes, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  int rc = check_common(s, 0, pos, sup, n, pose, obb, "wsb_aggregate_groups");
+  if (rc) return rc;
+  if (n_groups < 1 || n_groups > WSB_MAX_GROUPS || !kernels)
+    return fail(WSB_ERR_ARG, "wsb_aggregate_groups: 1 to " + std::to_string(WSB_MAX_GROUPS) + " kernel groups expected");
+  for (int g = 0; g < n_groups; ++g)
+    if (kernels[g] < 0 || kernels[g] >= kNumKernels)
+      return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_groups: unknown kernel id");
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_groups: unknown precision mode");
+  if (n == 0) return WSB_OK;
+  rc = wsb_aggregate_prepare(s_, pos, sup, allowed, n, pose, obb, unbounded, workspace, workspace_bytes, stream);
+  if (rc) return rc;
+  return wsb_aggregate_evaluate_groups(s_, n_groups, kernels, precision, sup, n, pose, out_mask, lam, G, cov, m1, m2,
+                                       workspace, workspace_bytes, stream);
 }
 
 extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const double* pos, const double* sup,

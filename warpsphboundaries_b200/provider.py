@@ -111,24 +111,29 @@ class FusedWall(WallAggregate):
                        "Cov": alloc((B, N, 2, 2), dtype=F64, device=self.dev),
                        "m1": alloc((B, N, 2), dtype=F64, device=self.dev),
                        "m2": alloc((B, N, 2, 2), dtype=F64, device=self.dev)}
-            kid = KERNEL_IDS[g.kernel]
-            self._group = len(self.res)
-            if route == "fused":
-                self._fused(pos, sup, allowed, kid, out)
-            elif route == "plain":
-                self._plain(ps, kid, out)
-            else:
-                raise ValueError(f"unknown route {route!r}")
             self.res.append(out)
+        kids = [KERNEL_IDS[g.kernel] for g in self.groups]
+        if route == "fused":
+            self._fused(pos, sup, allowed, kids, self.res)
+        elif route == "plain":
+            for gi, kid in enumerate(kids):
+                self._plain(ps, kid, self.res[gi])
+        else:
+            raise ValueError(f"unknown route {route!r}")
         self.out = {}
 
-    def _fused(self, pos, sup, allowed, kid, out):
+    def _fused(self, pos, sup, allowed, kids, outs):
+        """every group of every (body, surface) at once: one wsb_aggregate_groups call per surface (the groups share
+        the prepared rows and, for the kernel sets the library packs, the pass over the neighbour pairs:
+        fused.py:506-547); a conditioned single triangle runs per group, its quadrature rows combined in."""
         N = self.N
         al = None if allowed is None else allowed.to(torch.int32).contiguous()
+        names = ("lam", "G", "Cov", "m1", "m2")
         for bi, body in enumerate(self.scene.bodies):
             if not body.reps:
-                for t in out.values():
-                    t[bi].zero_()
+                for out in outs:
+                    for t in out.values():
+                        t[bi].zero_()
                 continue
             pose = body.pose_tensor(self.dev)
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
@@ -140,17 +145,23 @@ class FusedWall(WallAggregate):
                 else:
                     ws, need = ns.workspace(N)
                 mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)     # the first surface of a body assigns
-                tgt = {k: out[k][bi] for k in ("lam", "G", "Cov", "m1", "m2")}
-                if rep._triangle is not None:
+                if rep._triangle is None:
+                    tgt = {k: _lib.ptrs([out[k][bi] for out in outs]) for k in names}
+                    check(lib.wsb_aggregate_groups(ns.handle, len(kids), _lib.int32s(kids), _PREC[self.precision],
+                                                   ptr(pos), ptr(sup), ptr(al), N, ptr(pose), obb,
+                                                   int(body.unbounded()), mode, tgt["lam"], tgt["G"], tgt["Cov"],
+                                                   tgt["m1"], tgt["m2"], ptr(ws), need, _stream()),
+                          "wsb_aggregate_groups")
+                    continue
+                for gi, kid in enumerate(kids):
                     # closed form into scratch, then the rows the quadrature takes are overridden while combining
-                    tgt = {k: torch.empty_like(out[k][bi]) for k in ("lam", "G", "Cov", "m1", "m2")}
-                    mode = _lib.OUT_ALL | _lib.OUT_ASSIGN
-                check(lib.wsb_aggregate(ns.handle, kid, _PREC[self.precision], ptr(pos), ptr(sup), ptr(al), N,
-                                        ptr(pose), obb, int(body.unbounded()), mode, ptr(tgt["lam"]),
-                                        ptr(tgt["G"]), ptr(tgt["Cov"]), ptr(tgt["m1"]),
-                                        ptr(tgt["m2"]), ptr(ws), need, None, _stream()), "wsb_aggregate")
-                if rep._triangle is not None:
-                    self._conditioned(body, bi, ri, rep, pos, sup, al, kid, pose, tgt, out)
+                    self._group = gi
+                    tgt = {k: torch.empty_like(outs[gi][k][bi]) for k in names}
+                    check(lib.wsb_aggregate(ns.handle, kid, _PREC[self.precision], ptr(pos), ptr(sup), ptr(al), N,
+                                            ptr(pose), obb, int(body.unbounded()), _lib.OUT_ALL | _lib.OUT_ASSIGN,
+                                            ptr(tgt["lam"]), ptr(tgt["G"]), ptr(tgt["Cov"]), ptr(tgt["m1"]),
+                                            ptr(tgt["m2"]), ptr(ws), need, None, _stream()), "wsb_aggregate")
+                    self._conditioned(body, bi, ri, rep, pos, sup, al, kid, pose, tgt, outs[gi])
 
     def _conditioned(self, body, bi, ri, rep, pos, sup, al, kid, pose, closed, out, tolerance=2e-12,
                      max_panels=4096):
