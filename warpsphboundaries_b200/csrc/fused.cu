@@ -114,9 +114,6 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
   order[offs[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
 }
 
-// Per sorted row: its number of neighbour pairs (float-prefiltered exact predicate over its cell's candidates) as a
-// radix key, and its winding indicator -- both kernel independent, computed once per position set.
-// a 32-byte record through the read-only data path (two 16-byte loads)
 // index of the lowest set bit of the 128-bit mask (m0 low word), cleared; -1 when the mask is empty
 __device__ __forceinline__ int pop_bit(uint64_t& m0, uint64_t& m1) {
   if (m0) {
@@ -155,11 +152,15 @@ __device__ __forceinline__ WorkRec load_workrec(const WorkRec* p) {
   return r;
 }
 
+// a 32-byte record through the read-only data path (two 16-byte loads)
 __device__ __forceinline__ double4 ldg4(const double4* p) {
   const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
+// Per sorted row: its number of neighbour pairs (float-prefiltered exact predicate over its cell's candidates) as a
+// radix key with the neighbour mask, and its winding indicator -- both kernel independent, computed once per position
+// set.
 __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const int32_t* __restrict__ key,
                               const double* __restrict__ lpos, const int32_t* __restrict__ offs,
                               const int32_t* __restrict__ order, int64_t n, double* __restrict__ ind,
@@ -464,7 +465,8 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
 }
 
 // the pair kernel of a pack over a prepared workspace (two lanes per work row: measured fastest on the 2^20-particle
-// scene, 1 / 2 lanes give 10.4 / 11.3e9 pairs/s with the neighbour masks)
+// scene, 1 / 2 lanes give 10.4 / 11.3e9 pairs/s with one kernel, 1 / 2 / 4 lanes 0.448 / 0.421 / 0.471 ms for the
+// four-kernel pack, which also beat the four kernels as two two-kernel packs, 0.426 ms)
 template <class Pack, int PREC>
 static void launch_pack(const SurfView& v, const double* sup, const Workspace& w, int64_t n, const double* pose,
                         bool assign, const PackOut& out, cudaStream_t st) {
