@@ -130,3 +130,41 @@ def test_group_count_and_kernel_ids_are_checked(c2s):
                                            _lib.ptr(sup), None, n, _lib.ptr(body.pose_tensor(DEV)), obb, 0,
                                            _lib.OUT_ALL, *outs, _lib.ptr(ws), need, _stream())
         assert rc == code, (count, ids, rc)
+
+
+def _single_into(c2s, kernel, views, mode):
+    loops, X, h = c2s
+    scene, rep, body = make_scene(loops)
+    ns = rep.native(h, DEV)
+    n = len(X)
+    pos = torch.tensor(X, dtype=torch.float64, device=DEV)
+    sup = torch.full((n,), h, dtype=torch.float64, device=DEV)
+    ws, need = ns.workspace(n)
+    obb = (_lib.ctypes.c_double * 4)(*body.obb())
+    _lib.check(_lib.lib.wsb_aggregate(ns.handle, KERNEL_IDS[kernel], _lib.PREC_MIXED, _lib.ptr(pos), _lib.ptr(sup),
+                                      None, n, _lib.ptr(body.pose_tensor(DEV)), obb, 0, mode,
+                                      *[_lib.ptr(views[name]) for name in NAMES], _lib.ptr(ws), need, None,
+                                      _stream()), "wsb_aggregate")
+    torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("kernel", ["cubic", "w4"])
+def test_misaligned_outputs_and_the_add_mode(c2s, kernel):
+    """outputs that are not 16 / 32-byte aligned (views one element into a buffer) get the same values as aligned
+    ones, in both the assign and the add mode (the add mode on top of the first result doubles it exactly)."""
+    n = len(c2s[1])
+    widths = {"lam": 1, "G": 2, "Cov": 4, "m1": 2, "m2": 4}
+    aligned = {k: torch.zeros(n * w, dtype=torch.float64, device=DEV) for k, w in widths.items()}
+    raw = {k: torch.zeros(n * w + 1, dtype=torch.float64, device=DEV) for k, w in widths.items()}
+    shifted = {k: raw[k][1:] for k in widths}
+    assert shifted["G"].data_ptr() % 16 != 0
+    for views in (aligned, shifted):
+        _single_into(c2s, kernel, views, _lib.OUT_ALL | _lib.OUT_ASSIGN)
+    for k in widths:
+        assert torch.equal(aligned[k], shifted[k]), k
+    first = {k: aligned[k].clone() for k in widths}
+    for views in (aligned, shifted):
+        _single_into(c2s, kernel, views, _lib.OUT_ALL)              # add a second time on top
+    for k in widths:
+        assert torch.equal(aligned[k], shifted[k]), k
+        assert torch.equal(aligned[k], first[k] + first[k]), k
