@@ -158,24 +158,60 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
   return make_double4(a.x, a.y, b.x, b.y);
 }
 
+constexpr int kStageRecs = 768;   // candidate records a row-info block stages in shared memory (24 KiB)
+
 // Per sorted row: its number of neighbour pairs (float-prefiltered exact predicate over its cell's candidates) as a
 // radix key with the neighbour mask, and its winding indicator -- both kernel independent, computed once per position
 // set.
-__global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const int32_t* __restrict__ key,
-                              const double* __restrict__ lpos, const int32_t* __restrict__ offs,
-                              const int32_t* __restrict__ order, int64_t n, double* __restrict__ ind,
-                              int32_t* __restrict__ flag, int32_t* __restrict__ rkey, uint64_t* __restrict__ mask,
-                              int32_t* __restrict__ khist) {
+
+__global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const double* __restrict__ sup,
+                                                         const int32_t* __restrict__ key,
+                                                         const double* __restrict__ lpos,
+                                                         const int32_t* __restrict__ offs,
+                                                         const int32_t* __restrict__ order, int64_t n,
+                                                         double* __restrict__ ind, int32_t* __restrict__ flag,
+                                                         int32_t* __restrict__ rkey, uint64_t* __restrict__ mask,
+                                                         int32_t* __restrict__ khist) {
+  // The block's rows are consecutive in cell order, so the candidates of all their cells are one contiguous range of
+  // the cell-list records: it is staged in shared memory with coalesced loads when it fits, and every row's pass
+  // over its cell's candidates reads it there.
+  __shared__ double4 s_rec[kStageRecs];
+  __shared__ int32_t s_lo, s_hi;
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int32_t ncells = S.nx * S.ny;
+  if (threadIdx.x == 0) {
+    s_lo = INT32_MAX;
+    s_hi = -1;
+  }
+  int32_t i = 0, b = ncells + 1;
+  bool cand = false;
+  if (j < n) {
+    i = order[j];
+    cand = j < (int64_t)offs[ncells + 1];
+    if (cand) b = key[i];
+  }
+  __syncthreads();
+  if (cand && b < ncells) {
+    atomicMin(&s_lo, b);
+    atomicMax(&s_hi, b);
+  }
+  __syncthreads();
+  int r0 = 0;
+  bool staged = false;
+  if (s_hi >= 0) {
+    r0 = S.cstart[s_lo];
+    const int r1 = S.cstart[s_hi + 1];
+    staged = r1 - r0 <= kStageRecs;
+    if (staged)
+      for (int k = threadIdx.x; k < r1 - r0; k += kThreads) s_rec[k] = ldg4(S.crec + r0 + k);
+  }
+  __syncthreads();
   int cnt = 0;
   if (j < n) {
-    const int32_t ncells = S.nx * S.ny;
-    const int32_t i = order[j];
-    if (j >= (int64_t)offs[ncells + 1]) {      // not a candidate of this body
+    if (!cand) {                               // not a candidate of this body
       flag[i] = 0;
       ind[i] = 0.0;
     } else {
-      const int32_t b = key[i];
       const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
       double w = S.background;
       if (b < ncells) {
@@ -188,10 +224,8 @@ __global__ void k_agg_rowinfo(SurfView S, const double* __restrict__ sup, const 
         int cross = 0;
         uint64_t m0 = 0, m1 = 0;
         const int k0 = S.cstart[b], k1 = S.cstart[b + 1];
-        double4 nxt = k0 < k1 ? ldg4(S.crec + k0) : make_double4(0.0, 0.0, 0.0, 0.0);
         for (int k = k0; k < k1; ++k) {
-          const double4 e = nxt;
-          if (k + 1 < k1) nxt = ldg4(S.crec + k + 1);               // one record ahead
+          const double4 e = staged ? s_rec[k - r0] : ldg4(S.crec + k);
           if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
             ++cnt;
             const int r = k - k0;
