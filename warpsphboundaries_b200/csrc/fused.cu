@@ -81,7 +81,7 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
 __global__ void k_agg_prep(SurfView S, const double* __restrict__ pos, const double* __restrict__ sup,
                            const int32_t* __restrict__ allowed, int64_t n, const double* __restrict__ pose,
                            double4 obb, int unbounded, int32_t* __restrict__ key, double* __restrict__ lpos,
-                           int32_t* __restrict__ counts) {
+                           int32_t* __restrict__ counts, double* __restrict__ ind, int32_t* __restrict__ flag) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double lx, ly;
@@ -102,8 +102,16 @@ __global__ void k_agg_prep(SurfView S, const double* __restrict__ pos, const dou
     int32_t cid;
     b = cell_of(S, lx, ly, cid) ? cid : ncells;
   }
-  key[i] = b;
-  atomicAdd(&counts[b], 1);
+  if (b < ncells && S.cempty[b] == 0) {        // a cell with candidates: the row is sorted and row info takes it
+    key[i] = b;
+    atomicAdd(&counts[b], 1);
+    return;
+  }
+  // no candidates: not a candidate of the body (flag 0), outside the grid (the background), or an edge-free cell, whose
+  // cached centre winding is the indicator of all its points; these rows never enter the sort
+  key[i] = -1;
+  flag[i] = b == ncells + 1 ? 0 : 1;
+  ind[i] = b == ncells + 1 ? 0.0 : (b == ncells ? S.background : S.cind[b]);
 }
 
 __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const int32_t* __restrict__ offs,
@@ -111,7 +119,7 @@ __global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const 
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t b = key[i];
-  order[offs[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
+  if (b >= 0) order[offs[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
 }
 
 // index of the lowest set bit of the 128-bit mask (m0 low word), cleared; -1 when the mask is empty
@@ -183,15 +191,15 @@ __global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const doub
     s_lo = INT32_MAX;
     s_hi = -1;
   }
-  int32_t i = 0, b = ncells + 1;
-  bool cand = false;
-  if (j < n) {
+  // sorted rows: the rows in cells with candidates (k_agg_prep settles all others)
+  int32_t i = 0, b = 0;
+  const bool cand = j < (int64_t)offs[ncells];
+  if (cand) {
     i = order[j];
-    cand = j < (int64_t)offs[ncells + 1];
-    if (cand) b = key[i];
+    b = key[i];
   }
   __syncthreads();
-  if (cand && b < ncells) {
+  if (cand) {
     atomicMin(&s_lo, b);
     atomicMax(&s_hi, b);
   }
@@ -208,37 +216,31 @@ __global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const doub
   __syncthreads();
   int cnt = 0;
   if (j < n) {
-    if (!cand) {                               // not a candidate of this body
-      flag[i] = 0;
-      ind[i] = 0.0;
-    } else {
+    if (cand) {
       const double lx = lpos[2 * i], ly = lpos[2 * i + 1], h = sup[i];
-      double w = S.background;
-      if (b < ncells) {
-        // one pass over the cell's candidates: the neighbour count and the signed crossings of the segment from the
-        // cell centre (whose exact winding is stored) to the row; an uncertain orientation falls back to the ray cast
-        const int64_t cx = b / S.ny, cy = b % S.ny;
-        const double rx = __dadd_rn(S.lo_x, __dmul_rn(__dadd_rn((double)cx, 0.5), S.cell));
-        const double ry = __dadd_rn(S.lo_y, __dmul_rn(__dadd_rn((double)cy, 0.5), S.cell));
-        bool degenerate = S.cok[b] == 0;
-        int cross = 0;
-        uint64_t m0 = 0, m1 = 0;
-        const int k0 = S.cstart[b], k1 = S.cstart[b + 1];
-        for (int k = k0; k < k1; ++k) {
-          const double4 e = staged ? s_rec[k - r0] : ldg4(S.crec + k);
-          if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
-            ++cnt;
-            const int r = k - k0;
-            if (r < 64)
-              m0 |= 1ull << r;
-            else if (r < kMaskBits)
-              m1 |= 1ull << (r - 64);
-          }
-          if (!degenerate) cross += segment_crossing(rx, ry, lx, ly, e, &degenerate);
+      // one pass over the cell's candidates: the neighbour count and the signed crossings of the segment from the
+      // cell centre (whose exact winding is stored) to the row; an uncertain orientation falls back to the ray cast
+      const int64_t cx = b / S.ny, cy = b % S.ny;
+      const double rx = __dadd_rn(S.lo_x, __dmul_rn(__dadd_rn((double)cx, 0.5), S.cell));
+      const double ry = __dadd_rn(S.lo_y, __dmul_rn(__dadd_rn((double)cy, 0.5), S.cell));
+      bool degenerate = S.cok[b] == 0;
+      int cross = 0;
+      uint64_t m0 = 0, m1 = 0;
+      const int k0 = S.cstart[b], k1 = S.cstart[b + 1];
+      for (int k = k0; k < k1; ++k) {
+        const double4 e = staged ? s_rec[k - r0] : ldg4(S.crec + k);
+        if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
+          ++cnt;
+          const int r = k - k0;
+          if (r < 64)
+            m0 |= 1ull << r;
+          else if (r < kMaskBits)
+            m1 |= 1ull << (r - 64);
         }
-        reinterpret_cast<ulonglong2*>(mask)[j] = make_ulonglong2(m0, m1);
-        w = degenerate ? indicator_at(S, lx, ly, h, true, b) : S.cind[b] + (double)cross;
+        if (!degenerate) cross += segment_crossing(rx, ry, lx, ly, e, &degenerate);
       }
+      reinterpret_cast<ulonglong2*>(mask)[j] = make_ulonglong2(m0, m1);
+      const double w = degenerate ? indicator_at(S, lx, ly, h, true, b) : S.cind[b] + (double)cross;
       ind[i] = w;
       flag[i] = cnt > 0 ? 2 : 1;
     }
@@ -824,7 +826,7 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
   const SurfView v = view_of(s);
   const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
   k_agg_prep<<<grid, kThreads, 0, st>>>(v, pos, sup, allowed, n, pose, make_double4(obb[0], obb[1], obb[2], obb[3]),
-                                        unbounded, w.key, w.lpos, w.counts);
+                                        unbounded, w.key, w.lpos, w.counts, w.ind, w.flag);
   k_scan_block<<<1, kScanThreads, 0, st>>>(w.counts, w.offs, nbk + 1);
   k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
   k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.mask,
