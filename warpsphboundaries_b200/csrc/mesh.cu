@@ -296,9 +296,6 @@ __device__ __forceinline__ void acc_zero(Acc28& A) {
   for (int i = 0; i < 28; ++i) A.v[i] = 0.0;
 }
 
-// symmetric index of (i, j), i <= j: 00 01 02 11 12 22
-__host__ __device__ constexpr int sym(int i, int j) { return i == 0 ? j : (i == 1 ? 2 + j : 5); }
-
 // per-edge integrals accumulated over the panels of one side of the foot point
 struct EdgeSums {
   double J[6];   // w int z^p DD_F ds for A_K0 (p1) A_K1 (p2) A_K2 (p3) A_W A_L A2_K2 (p1)
@@ -435,47 +432,57 @@ __device__ __forceinline__ double tri_dist2(const double P[3][3]) {
   return cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2];
 }
 
-// assembly (W~ units), per edge:  M0 += J0;  M1 += N J1 + mu LK1;
-// M2 += N N^T J2 + N (mu LK2)^T + (mu LK2) N^T + sym(mu (x) (w mu LK2b + t TK2)) - (I - N N^T) J5;
-// G0 -= N J3;  G1_ij -= (z N_i J3 + mu_i LW) N_j;  H += sym(N (x) (z N J4 + mu LL))
-__device__ __forceinline__ void edge_assemble(double* __restrict__ Av, const double N[3], double z, const double t[3],
-                                              const double mu[3], double w, const EdgeSums& S) {
-  Av[kAM0] += S.J[0];
-#pragma unroll
-  for (int i = 0; i < 3; ++i) Av[kAM1 + i] += N[i] * S.J[1] + mu[i] * S.LK1;
-  const double wl = w * S.LK2b;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = i; j < 3; ++j) {
-      const double Pij = (i == j ? 1.0 : 0.0) - N[i] * N[j];
-      const double v = N[i] * N[j] * S.J[2] + (N[i] * mu[j] + mu[i] * N[j]) * S.LK2 + mu[i] * mu[j] * wl +
-                       0.5 * (mu[i] * t[j] + mu[j] * t[i]) * S.TK2 - Pij * S.J[5];
-      Av[kAM2 + sym(i, j)] += v;
-    }
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    Av[kAG0 + i] -= N[i] * S.J[3];
-    const double S1 = z * N[i] * S.J[3] + mu[i] * S.LW;
-#pragma unroll
-    for (int j = 0; j < 3; ++j) Av[kAG1 + 3 * i + j] -= S1 * N[j];
-  }
-  double HL[3];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) HL[j] = z * N[j] * S.J[4] + mu[j] * S.LL;
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = i; j < 3; ++j) Av[kAH + sym(i, j)] += 0.5 * (N[i] * HL[j] + N[j] * HL[i]);
+// Assembly (W~ units), per edge:  M0 += J0;  M1_i += N_i J1 + mu_i LK1;
+// M2_ij += N_i N_j (J2 + J5) + (N_i mu_j + mu_i N_j) LK2 + mu_i mu_j w LK2b + (mu_i t_j + mu_j t_i) TK2 / 2 - d_ij J5;
+// G0_i -= N_i J3;  G1_ij -= z N_i N_j J3 + mu_i N_j LW;  H_ij += z N_i N_j J4 + (N_i mu_j + mu_i N_j) LL / 2.
+// Lane k < 28 adds the term of accumulator k: every term is one bilinear form in the edge vectors N, mu, t whose
+// coefficients a lane selects by its accumulator's type, so all lanes run the same instructions.
+enum { kTM0, kTM1, kTM2, kTG0, kTG1, kTH, kTNone };
+struct AccSlot {
+  int type, i, j;
+};
+
+__device__ __forceinline__ AccSlot acc_slot(int k) {
+  auto sym_i = [](int x) { return x < 3 ? 0 : (x < 5 ? 1 : 2); };
+  auto sym_j = [](int x) { return x < 3 ? x : (x < 5 ? x - 2 : 2); };
+  if (k == kAM0) return {kTM0, 0, 0};
+  if (k < kAM2) return {kTM1, k - kAM1, 0};
+  if (k < kAG0) return {kTM2, sym_i(k - kAM2), sym_j(k - kAM2)};
+  if (k < kAG1) return {kTG0, k - kAG0, 0};
+  if (k < kAH) return {kTG1, (k - kAG1) / 3, (k - kAG1) % 3};
+  if (k < 28) return {kTH, sym_i(k - kAH), sym_j(k - kAH)};
+  return {kTNone, 0, 0};
+}
+
+__device__ __forceinline__ double pick3(const double v[3], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
+
+__device__ __forceinline__ double edge_term(const AccSlot& sl, const double N[3], double z, const double t[3],
+                                            const double mu[3], double w, const EdgeSums& S) {
+  const double Ni = pick3(N, sl.i), Nj = pick3(N, sl.j), mi = pick3(mu, sl.i), mj = pick3(mu, sl.j);
+  const double ti = pick3(t, sl.i), tj = pick3(t, sl.j);
+  const double NN = Ni * Nj, X = Ni * mj + mi * Nj, MN = mi * Nj, MM = mi * mj, MT = 0.5 * (mi * tj + mj * ti);
+  const double dij = sl.i == sl.j ? 1.0 : 0.0;
+  const int ty = sl.type;
+  const double cC = ty == kTM0 ? S.J[0] : 0.0;
+  const double cNi = ty == kTM1 ? S.J[1] : (ty == kTG0 ? -S.J[3] : 0.0);
+  const double cMi = ty == kTM1 ? S.LK1 : 0.0;
+  const double cNN = ty == kTM2 ? S.J[2] + S.J[5] : (ty == kTG1 ? -z * S.J[3] : (ty == kTH ? z * S.J[4] : 0.0));
+  const double cX = ty == kTM2 ? S.LK2 : (ty == kTH ? 0.5 * S.LL : 0.0);
+  const double cMN = ty == kTG1 ? -S.LW : 0.0;
+  const double cMM = ty == kTM2 ? w * S.LK2b : 0.0;
+  const double cMT = ty == kTM2 ? S.TK2 : 0.0;
+  const double cD = ty == kTM2 ? -S.J[5] : 0.0;
+  return cC + Ni * cNi + mi * cMi + NN * cNN + X * cX + MN * cMN + MM * cMM + MT * cMT + dij * cD;
 }
 
 // the contribution of face f to the row's accumulators (the warp's shared array Av), computed by the whole warp: the
 // geometry is the same in every lane, the quadrature nodes of an edge (12 or 16 per panel) are spread over the lanes and
-// their sums reduced by a fixed butterfly, lane 0 adds the edge's terms to Av.  Everything is linear in the per-edge integrals.  Faces that do not meet the
-// support contribute exactly nothing: skipped.  q in world units, ih = 1 / support.
+// their sums reduced by a fixed butterfly, then lane k adds the edge's term of accumulator k (slot: this lane's).
+// Everything is linear in the per-edge integrals.  Faces that do not meet the support contribute exactly nothing:
+// skipped.  q in world units, ih = 1 / support.
 template <class M>
 __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], double ih, PanelList& PL, int lane,
-                                  double* __restrict__ Av) {
+                                  const AccSlot& slot, double* __restrict__ Av) {
   const double* F = Mv.fdata + (int64_t)f * kFaceDoubles;
   double P[3][3];
 #pragma unroll
@@ -545,8 +552,8 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
         S.J[5] -= aval_a<M, 5, 1>(a, z, sg) * out;
       }
     }
-    // assembly into the warp's shared accumulators, by lane 0 (keeping 28 accumulators out of every lane's registers)
-    if (lane == 0) edge_assemble(Av, N, z, t, mu, w, S);
+    // assembly into the warp's shared accumulators, accumulator k by lane k (the sums are in every lane)
+    if (lane < 28) Av[lane] += edge_term(slot, N, z, t, mu, w, S);
     __syncwarp();
   }
 }
@@ -640,6 +647,7 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
   __shared__ PanelList pl[kMeshThreads / 32];
   __shared__ double acc[kMeshThreads / 32][28];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const AccSlot aslot = acc_slot(lane);                  // the accumulator this lane assembles
   const int nw = *nwork;
   for (int it = 0; it < (1 << 30); ++it) {
     int slot = 0;
@@ -651,7 +659,7 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
     const double h = sup[row], ih = 1.0 / h;
     if (lane < 28) acc[wib][lane] = 0.0;
     __syncwarp();
-    for_candidates(Mv, q, h, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], lane, acc[wib]); });
+    for_candidates(Mv, q, h, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], lane, aslot, acc[wib]); });
     if (lane == 0) {
       Acc28 A;
 #pragma unroll
