@@ -376,10 +376,32 @@ __device__ int build_panels(PanelList& PL, double s0, double s1, double c) {
   return np;
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
+// the warp's sums of twelve values, in every lane: lanes 16 apart swap six values and keep the sums of the other six,
+// lanes 8 apart swap three, a butterfly over the last three lane bits completes each group of eight lanes' three sums,
+// and each total is broadcast from its group (a fixed order: deterministic)
+__device__ __forceinline__ void warp_sum12(double v[12]) {
+  const int lane = threadIdx.x & 31;
+  const bool up = (lane >> 4) & 1, b3 = (lane >> 3) & 1;
+  double a[6];
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  return v;
+  for (int k = 0; k < 6; ++k) {
+    const double give = up ? v[k] : v[k + 6];
+    const double keep = up ? v[k + 6] : v[k];
+    a[k] = keep + __shfl_xor_sync(0xffffffffu, give, 16);
+  }
+  double b[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const double give = b3 ? a[k] : a[k + 3];
+    const double keep = b3 ? a[k + 3] : a[k];
+    b[k] = keep + __shfl_xor_sync(0xffffffffu, give, 8);
+  }
+#pragma unroll
+  for (int off = 4; off > 0; off >>= 1)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) b[k] += __shfl_xor_sync(0xffffffffu, b[k], off);
+#pragma unroll
+  for (int x = 0; x < 12; ++x) v[x] = __shfl_sync(0xffffffffu, b[x % 3], 8 * (x / 3));
 }
 
 // squared distance from the origin to the triangle P (unit coordinates relative to the query)
@@ -525,14 +547,16 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
         const double hc = 0.5 * (x1 - x0);
         node_eval<M>(fma(hc, xg, 0.5 * (x1 + x0)), wg * hc, PL.sg[p], c2, a, z, sg, w, S);
       }
+      double v[12] = {S.J[0], S.J[1], S.J[2], S.J[3], S.J[4], S.J[5], S.LK1, S.LK2, S.LK2b, S.TK2, S.LW, S.LL};
+      warp_sum12(v);
 #pragma unroll
-      for (int i = 0; i < 6; ++i) S.J[i] = warp_sum(S.J[i]);
-      S.LK1 = warp_sum(S.LK1);
-      S.LK2 = warp_sum(S.LK2);
-      S.LK2b = warp_sum(S.LK2b);
-      S.TK2 = warp_sum(S.TK2);
-      S.LW = warp_sum(S.LW);
-      S.LL = warp_sum(S.LL);
+      for (int i = 0; i < 6; ++i) S.J[i] = v[i];
+      S.LK1 = v[6];
+      S.LK2 = v[7];
+      S.LK2b = v[8];
+      S.TK2 = v[9];
+      S.LW = v[10];
+      S.LL = v[11];
       __syncwarp();                                   // the list is rebuilt for the next edge
     }
     if (w != 0.0) {
