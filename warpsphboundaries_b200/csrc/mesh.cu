@@ -639,19 +639,31 @@ __device__ __forceinline__ void write_row(double* __restrict__ out, int64_t row,
   for (int k = 0; k < 6; ++k) o[22 + k] = A.v[kAH + k] * ip * ih2;
 }
 
-// rows without faces in their support: whole-support constants inside, zeros outside, NaN for invalid rows
+// rows without faces in their support: whole-support constants inside, zeros outside, NaN for invalid rows.  Each
+// thread builds its row in shared memory (stride 29 doubles against bank conflicts) and the block writes its
+// contiguous slab of 128 x 28 outputs coalesced.
+constexpr int kRowStride = 29;
+
 template <class M>
 __global__ void __launch_bounds__(kMeshThreads) k_mesh_rows(const double* __restrict__ sup, int64_t n,
                                                            const int32_t* __restrict__ ind, double* __restrict__ out) {
-  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= n) return;
-  if (ind[row] < 0) {
-    for (int k = 0; k < 28; ++k) out[row * 28 + k] = __longlong_as_double(0x7ff8000000000000LL);
-    return;
+  __shared__ double s_rows[kMeshThreads * kRowStride];
+  const int64_t row0 = (int64_t)blockIdx.x * kMeshThreads;
+  const int64_t row = row0 + threadIdx.x;
+  double* const mine = s_rows + threadIdx.x * kRowStride;
+  if (row < n) {
+    if (ind[row] < 0) {
+      for (int k = 0; k < 28; ++k) mine[k] = __longlong_as_double(0x7ff8000000000000LL);
+    } else {
+      Acc28 A;
+      acc_zero(A);
+      write_row<M>(mine, 0, A, (double)ind[row], sup[row]);
+    }
   }
-  Acc28 A;
-  acc_zero(A);
-  write_row<M>(out, row, A, (double)ind[row], sup[row]);
+  __syncthreads();
+  const int rows = (int)min((int64_t)kMeshThreads, n - row0);
+  for (int k = threadIdx.x; k < rows * 28; k += kMeshThreads)
+    out[row0 * 28 + k] = s_rows[(k / 28) * kRowStride + k % 28];
 }
 
 // one warp per work row; warps take rows from a counter (rows differ in their number of faces), and the row's
