@@ -50,7 +50,13 @@ struct Mesh {
   int32_t* citems = nullptr;   // faces per cell
   int32_t* colstart = nullptr; // [nx*ny + 1] faces per (x, y) column
   int32_t* colitems = nullptr;
+  uint8_t* cflag = nullptr;    // [nx*ny*nz] kCellEmpty | kCellInside | kCellNear
 };
+
+// per-cell flags: no face box meets the cell (so the surface does not cross it and every point of it has the inside
+// status of its centre); that status; a face box meets one of the 27 cells around it (a query in the cell may have
+// candidate faces)
+enum : uint8_t { kCellEmpty = 1, kCellInside = 2, kCellNear = 4 };
 
 // per face: v0 v1 v2 (9), unit normal N (3), edge tangents t0 t1 t2 (9), edge normals mu_e = t_e x N (9),
 // edge lengths (3), box lo (3), box hi (3)
@@ -65,6 +71,7 @@ struct MeshView {
   const int32_t* citems;
   const int32_t* colstart;
   const int32_t* colitems;
+  const uint8_t* cflag;
   double lo0, lo1, lo2, cell;
   int32_t nx, ny, nz;
 };
@@ -72,7 +79,7 @@ struct MeshView {
 namespace {
 
 MeshView view_of(const Mesh* m) {
-  return MeshView{m->fdata, m->fcell, m->fvid, m->cstart, m->citems, m->colstart, m->colitems,
+  return MeshView{m->fdata, m->fcell, m->fvid, m->cstart, m->citems, m->colstart, m->colitems, m->cflag,
                   m->lo[0], m->lo[1], m->lo[2], m->cell, m->nx, m->ny, m->nz};
 }
 
@@ -585,25 +592,92 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
 // ------------------------------------------------------------------------------------------ kernels
 constexpr int kMeshThreads = 128;
 
-// per query: the inside test and whether any face is within the support; rows with faces are appended to `work`
+// the per-cell flags, once per mesh: emptiness, the inside status of an empty cell's centre (the column parity test),
+// whether any of the 27 cells around holds a face
+__global__ void k_mesh_cellflags(MeshView M, uint8_t* __restrict__ flags) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nxy = (int64_t)M.nx * M.ny;
+  if (c >= nxy * M.nz) return;
+  const int i = (int)(c % M.nx), j = (int)((c / M.nx) % M.ny), k = (int)(c / nxy);
+  uint8_t f = 0;
+  if (M.cstart[c] == M.cstart[c + 1]) {
+    f |= kCellEmpty;
+    const double x = M.lo0 + (i + 0.5) * M.cell, y = M.lo1 + (j + 0.5) * M.cell, z = M.lo2 + (k + 0.5) * M.cell;
+    if (mesh_inside(M, x, y, z)) f |= kCellInside;
+  }
+  for (int dk = -1; dk <= 1; ++dk)
+    for (int dj = -1; dj <= 1; ++dj)
+      for (int di = -1; di <= 1; ++di) {
+        const int a = i + di, b = j + dj, e = k + dk;
+        if (a < 0 || b < 0 || e < 0 || a >= M.nx || b >= M.ny || e >= M.nz) continue;
+        const int64_t n = ((int64_t)e * M.ny + b) * M.nx + a;
+        if (M.cstart[n] != M.cstart[n + 1]) f |= kCellNear;
+      }
+  flags[c] = f;
+}
+
+// Per query, first pass: the cell's flags settle the rows away from the surface (inside status of an empty cell, no
+// faces within the support when no face box meets the 27 cells around); the others are appended to `near`, so the
+// second pass runs the parity walk and the face search on full warps of such rows.  Invalid rows (a support above the
+// grid cell would reach faces outside the 27-cell block, non-finite input) are marked -1 and come back as NaN.
 __global__ void __launch_bounds__(kMeshThreads) k_mesh_rowinfo(MeshView M, const double* __restrict__ pos,
                                                               const double* __restrict__ sup, int64_t n,
-                                                              int32_t* __restrict__ ind, int32_t* __restrict__ work,
-                                                              int32_t* __restrict__ nwork) {
+                                                              int32_t* __restrict__ ind, int32_t* __restrict__ near,
+                                                              int32_t* __restrict__ nnear) {
   const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  bool has = false;
+  bool listed = false;
   if (row < n) {
     const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
     const double h = sup[row];
-    // a support above the grid cell would reach faces outside the 27-cell block: such rows (and non-finite input)
-    // are marked -1 and come back as NaN
     const bool ok = h > 0.0 && h <= M.cell && isfinite(q[0]) && isfinite(q[1]) && isfinite(q[2]);
-    if (ok) {
-      ind[row] = mesh_inside(M, q[0], q[1], q[2]);
-      has = has_candidate(M, q, h);
-    } else {
+    if (!ok) {
       ind[row] = -1;
+    } else {
+      const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
+                cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
+      const bool in_grid = cx >= 0 && cy >= 0 && cz >= 0 && cx < M.nx && cy < M.ny && cz < M.nz;
+      const uint8_t f = in_grid ? M.cflag[((int64_t)cz * M.ny + cy) * M.nx + cx] : (uint8_t)kCellNear;
+      if (!(f & kCellNear)) {
+        ind[row] = (f & kCellInside) ? 1 : 0;     // no face box in the 27 cells: the cell is empty as well
+      } else {
+        listed = true;
+      }
     }
+  }
+  const unsigned mask = __ballot_sync(0xffffffffu, listed);
+  if (mask) {
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(nnear, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (listed) near[base + __popc(mask & ((1u << lane) - 1))] = (int32_t)row;
+  }
+}
+
+// Second pass over the listed rows: the inside test (the cell's flag where the cell is empty, the parity walk
+// otherwise) and whether any face is within the support; rows with faces are appended to `work`
+__global__ void __launch_bounds__(kMeshThreads) k_mesh_rownear(MeshView M, const double* __restrict__ pos,
+                                                              const double* __restrict__ sup,
+                                                              const int32_t* __restrict__ near,
+                                                              const int32_t* __restrict__ nnear,
+                                                              int32_t* __restrict__ ind, int32_t* __restrict__ work,
+                                                              int32_t* __restrict__ nwork) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t m = *nnear;
+  if ((int64_t)blockIdx.x * blockDim.x >= m) return;            // whole block past the listed rows
+  bool has = false;
+  int32_t row = 0;
+  if (t < m) {
+    row = near[t];
+    const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
+    const double h = sup[row];
+    const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
+              cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
+    const bool in_grid = cx >= 0 && cy >= 0 && cz >= 0 && cx < M.nx && cy < M.ny && cz < M.nz;
+    const uint8_t f = in_grid ? M.cflag[((int64_t)cz * M.ny + cy) * M.nx + cx] : (uint8_t)0;
+    ind[row] = (f & kCellEmpty) ? ((f & kCellInside) ? 1 : 0) : mesh_inside(M, q[0], q[1], q[2]);
+    has = has_candidate(M, q, h);
   }
   // warp-aggregated append of the rows with candidate faces (their order is irrelevant: each row is computed alone)
   const unsigned mask = __ballot_sync(0xffffffffu, has);
@@ -613,7 +687,7 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_rowinfo(MeshView M, const
     int base = 0;
     if (lane == leader) base = atomicAdd(nwork, __popc(mask));
     base = __shfl_sync(0xffffffffu, base, leader);
-    if (has) work[base + __popc(mask & ((1u << lane) - 1))] = (int32_t)row;
+    if (has) work[base + __popc(mask & ((1u << lane) - 1))] = row;
   }
 }
 
@@ -721,7 +795,7 @@ int upload_vec(T** dst, const std::vector<T>& src) {
 }
 
 void free_mesh(Mesh* m) {
-  void* ptrs[] = {m->fdata, m->fcell, m->fvid, m->cstart, m->citems, m->colstart, m->colitems};
+  void* ptrs[] = {m->fdata, m->fcell, m->fvid, m->cstart, m->citems, m->colstart, m->colitems, m->cflag};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -730,11 +804,13 @@ inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 template <class M>
 int launch_mesh(const Mesh* m, const double* pos, const double* sup, int64_t n, double* out, int32_t* ind,
-                int32_t* work, int32_t* nwork, cudaStream_t st) {
+                int32_t* work, int32_t* nwork, int32_t* near, cudaStream_t st) {
   const MeshView v = view_of(m);
   const unsigned grid = (unsigned)((n + kMeshThreads - 1) / kMeshThreads);
-  WSB_CUDA(cudaMemsetAsync(nwork, 0, 2 * sizeof(int32_t), st));
-  k_mesh_rowinfo<<<grid, kMeshThreads, 0, st>>>(v, pos, sup, n, ind, work, nwork);
+  WSB_CUDA(cudaMemsetAsync(nwork, 0, 3 * sizeof(int32_t), st));      // work rows, grab counter, listed rows
+  k_mesh_rowinfo<<<grid, kMeshThreads, 0, st>>>(v, pos, sup, n, ind, near, nwork + 2);
+  WSB_CUDA(cudaGetLastError());
+  k_mesh_rownear<<<grid, kMeshThreads, 0, st>>>(v, pos, sup, near, nwork + 2, ind, work, nwork);
   WSB_CUDA(cudaGetLastError());
   k_mesh_rows<M><<<grid, kMeshThreads, 0, st>>>(sup, n, ind, out);
   WSB_CUDA(cudaGetLastError());
@@ -896,10 +972,20 @@ extern "C" int wsb_mesh_create(const double* verts, int64_t n_verts, const int32
   int rc;
   if ((rc = upload_vec(&m->fdata, hf)) || (rc = upload_vec(&m->fcell, fcell)) || (rc = upload_vec(&m->fvid, hvid)) ||
       (rc = upload_vec(&m->cstart, start)) || (rc = upload_vec(&m->citems, items)) ||
-      (rc = upload_vec(&m->colstart, cstart)) || (rc = upload_vec(&m->colitems, citems))) {
+      (rc = upload_vec(&m->colstart, cstart)) || (rc = upload_vec(&m->colitems, citems)) ||
+      (rc = upload_vec(&m->cflag, std::vector<uint8_t>((size_t)m->nx * m->ny * m->nz, 0)))) {
     free_mesh(m);
     delete m;
     return rc;
+  }
+  const int64_t ncells = (int64_t)m->nx * m->ny * m->nz;
+  k_mesh_cellflags<<<(unsigned)((ncells + 255) / 256), 256>>>(view_of(m), m->cflag);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    free_mesh(m);
+    delete m;
+    return cuda_fail(e, "wsb_mesh_create: cell flags");
   }
   *out = static_cast<wsb_mesh*>(m);
   return WSB_OK;
@@ -915,7 +1001,7 @@ extern "C" int wsb_mesh_destroy(wsb_mesh* m) {
 
 extern "C" size_t wsb_mesh_workspace_size(const wsb_mesh* m, int64_t n) {
   if (!m || n < 0) return 0;
-  return al256(sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)) * 2 + 256;
+  return al256(sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)) * 3 + 256;
 }
 
 extern "C" int wsb_mesh_inside(const wsb_mesh* m, const double* pos, int64_t n, int32_t* inside, void* stream) {
@@ -946,12 +1032,13 @@ extern "C" int wsb_mesh_channels(const wsb_mesh* m, int kernel, const double* po
   const size_t s = al256(sizeof(int32_t) * (size_t)n);
   int32_t* work = (int32_t*)base;
   int32_t* ind = inside ? inside : (int32_t*)(base + s);
-  int32_t* nwork = (int32_t*)(base + 2 * s);
+  int32_t* nwork = (int32_t*)(base + 2 * s);     // [3]: work rows, grab counter, listed rows
+  int32_t* near = (int32_t*)(base + 2 * s + 256);
   cudaStream_t st = (cudaStream_t)stream;
   switch (kernel) {
-    case WSB_KERNEL_CUBIC: return launch_mesh<Mesh_cubic>(m, pos, sup, n, out, ind, work, nwork, st);
-    case WSB_KERNEL_W2: return launch_mesh<Mesh_w2>(m, pos, sup, n, out, ind, work, nwork, st);
-    case WSB_KERNEL_W4: return launch_mesh<Mesh_w4>(m, pos, sup, n, out, ind, work, nwork, st);
-    default: return launch_mesh<Mesh_w6>(m, pos, sup, n, out, ind, work, nwork, st);
+    case WSB_KERNEL_CUBIC: return launch_mesh<Mesh_cubic>(m, pos, sup, n, out, ind, work, nwork, near, st);
+    case WSB_KERNEL_W2: return launch_mesh<Mesh_w2>(m, pos, sup, n, out, ind, work, nwork, near, st);
+    case WSB_KERNEL_W4: return launch_mesh<Mesh_w4>(m, pos, sup, n, out, ind, work, nwork, near, st);
+    default: return launch_mesh<Mesh_w6>(m, pos, sup, n, out, ind, work, nwork, near, st);
   }
 }
