@@ -54,6 +54,8 @@ struct Surface {
   double* cind = nullptr;       // [nx*ny] winding + background at the cell centre
   int32_t* cok = nullptr;       // [nx*ny] 1 where the centre's winding is certain (clear of every edge line it tests)
   int32_t* cempty = nullptr;    // [nx*ny]
+  int32_t* ccompact = nullptr;  // [nx*ny] index of a cell among the cells with edges (cell order), -1 for an empty one
+  int32_t n_nonempty = 0;       // cells with edges
   int32_t* bstart = nullptr;    // [nb+1]
   int32_t* bitems = nullptr;    // [n_bitems]
   double4* erec = nullptr;      // [n_edges] (ax, ay, bx, by) by edge id
@@ -124,11 +126,12 @@ struct SurfView {        // the device pointers and scalars a kernel needs (pass
   const double* cind;
   const int32_t* cok;
   const int32_t* cempty;
+  const int32_t* ccompact;
   const int32_t* bstart;
   const int32_t* bitems;
   const double4* brec;
   const double4* erec;
-  int32_t nx, ny, nb, K;
+  int32_t nx, ny, nb, K, nne;
   double lo_x, lo_y, cell, y0, dy;
   double background;
 };

@@ -33,9 +33,9 @@ static_assert(sizeof(WorkRec) == 64 && offsetof(WorkRec, h) == 16 && offsetof(Wo
               "work record layout");
 
 struct Workspace {
-  int32_t* key;      // [n] bucket of a row: cell id, ncells = outside the grid, ncells + 1 = not a candidate
+  int32_t* key;      // [n] cell of a row in a cell with edges (sorted by it), -1 for rows settled by k_agg_prep
   double* lpos;      // [2n] body-frame positions
-  int32_t* counts;   // [nbk + 1]   } zeroed together
+  int32_t* counts;   // [nbk + 1]   } zeroed together (buckets: the cells with edges, by compact index)
   int32_t* cursor;   // [nbk]       }
   int32_t* offs;     // [nbk + 1] exclusive prefix sums of counts
   int32_t* order;    // [n] rows sorted by bucket
@@ -52,7 +52,7 @@ struct Workspace {
 
 static Workspace carve(const Surface* s, int64_t n, void* base) {
   Workspace w{};
-  const int64_t nbk = (int64_t)s->nx * s->ny + 2;
+  const int64_t nbk = (int64_t)s->n_nonempty + 2;   // buckets: the cells with edges
   size_t off = 0;
   auto take = [&](size_t bytes) {
     size_t o = off;
@@ -104,7 +104,7 @@ __global__ void k_agg_prep(SurfView S, const double* __restrict__ pos, const dou
   }
   if (b < ncells && S.cempty[b] == 0) {        // a cell with candidates: the row is sorted and row info takes it
     key[i] = b;
-    atomicAdd(&counts[b], 1);
+    atomicAdd(&counts[S.ccompact[b]], 1);        // bucketed by the cell's index among the cells with edges
     return;
   }
   // no candidates: not a candidate of the body (flag 0), outside the grid (the background), or an edge-free cell, whose
@@ -114,12 +114,15 @@ __global__ void k_agg_prep(SurfView S, const double* __restrict__ pos, const dou
   ind[i] = b == ncells + 1 ? 0.0 : (b == ncells ? S.background : S.cind[b]);
 }
 
-__global__ void k_agg_scatter(const int32_t* __restrict__ key, int64_t n, const int32_t* __restrict__ offs,
+__global__ void k_agg_scatter(SurfView S, const int32_t* __restrict__ key, int64_t n, const int32_t* __restrict__ offs,
                               int32_t* __restrict__ cursor, int32_t* __restrict__ order) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t b = key[i];
-  if (b >= 0) order[offs[b] + atomicAdd(&cursor[b], 1)] = (int32_t)i;
+  if (b >= 0) {
+    const int32_t c = S.ccompact[b];
+    order[offs[c] + atomicAdd(&cursor[c], 1)] = (int32_t)i;
+  }
 }
 
 // index of the lowest set bit of the 128-bit mask (m0 low word), cleared; -1 when the mask is empty
@@ -186,14 +189,13 @@ __global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const doub
   __shared__ double4 s_rec[kStageRecs];
   __shared__ int32_t s_lo, s_hi;
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int32_t ncells = S.nx * S.ny;
   if (threadIdx.x == 0) {
     s_lo = INT32_MAX;
     s_hi = -1;
   }
   // sorted rows: the rows in cells with candidates (k_agg_prep settles all others)
   int32_t i = 0, b = 0;
-  const bool cand = j < (int64_t)offs[ncells];
+  const bool cand = j < (int64_t)offs[S.nne];
   if (cand) {
     i = order[j];
     b = key[i];
@@ -820,7 +822,7 @@ __global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int6
 // shared front half of the aggregate and its adjoint: body frame, broadphase, counting sort of the rows by cell
 static int sort_rows(const Surface* s, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
                      const double* pose, const double* obb, int unbounded, const Workspace& w, cudaStream_t st) {
-  const int64_t nbk = (int64_t)s->nx * s->ny + 2;
+  const int64_t nbk = (int64_t)s->n_nonempty + 2;   // buckets: the cells with edges
   WSB_CUDA(cudaMemsetAsync(w.counts, 0, sizeof(int32_t) * (2 * nbk + 1), st));
   WSB_CUDA(cudaMemsetAsync(w.khist, 0, sizeof(int32_t) * 2 * kKeys, st));
   const SurfView v = view_of(s);
@@ -828,7 +830,7 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
   k_agg_prep<<<grid, kThreads, 0, st>>>(v, pos, sup, allowed, n, pose, make_double4(obb[0], obb[1], obb[2], obb[3]),
                                         unbounded, w.key, w.lpos, w.counts, w.ind, w.flag);
   k_scan_block<<<1, kScanThreads, 0, st>>>(w.counts, w.offs, nbk + 1);
-  k_agg_scatter<<<grid, kThreads, 0, st>>>(w.key, n, w.offs, w.cursor, w.order);
+  k_agg_scatter<<<grid, kThreads, 0, st>>>(v, w.key, n, w.offs, w.cursor, w.order);
   k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.mask,
                                             w.khist);
   k_key_scatter<<<grid, kThreads, 0, st>>>(v, w.rkey, n, w.khist, w.kcur, w.order, w.key, w.lpos, sup, w.mask, w.wrec,

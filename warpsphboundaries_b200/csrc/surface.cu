@@ -35,6 +35,8 @@ SurfView view_of(const Surface* s) {
   v.cind = s->cind;
   v.cok = s->cok;
   v.cempty = s->cempty;
+  v.ccompact = s->ccompact;
+  v.nne = s->n_nonempty;
   v.bstart = s->bstart;
   v.bitems = s->bitems;
   v.brec = s->brec;
@@ -100,7 +102,7 @@ static int upload(T** dst, const std::vector<T>& src) {
 }
 
 static void free_surface(Surface* s) {
-  void* ptrs[] = {s->verts, s->edges, s->cstart, s->citems, s->crec, s->cind, s->cempty, s->bstart, s->bitems, s->erec,
+  void* ptrs[] = {s->verts, s->edges, s->cstart, s->citems, s->crec, s->cind, s->cempty, s->ccompact, s->bstart, s->bitems, s->erec,
                   s->brec, s->cok};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -184,6 +186,9 @@ extern "C" int wsb_surface_create(const double* verts, int64_t n_verts, const in
   for (int64_t i = 0; i < n_items; ++i) crec[i] = erec[items[i]];
   std::vector<int32_t> cempty(ncells);
   for (int64_t c = 0; c < ncells; ++c) cempty[c] = (start[c + 1] == start[c]) ? 1 : 0;
+  std::vector<int32_t> ccompact(ncells);
+  int32_t nne = 0;
+  for (int64_t c = 0; c < ncells; ++c) ccompact[c] = cempty[c] ? -1 : nne++;
   // ---- y bins (scene.py:297-314)
   const int32_t nb = std::max<int32_t>(1, (int32_t)std::sqrt((double)n_edges) * 2);
   double ylo_min = INFINITY, yhi_max = -INFINITY;
@@ -213,6 +218,7 @@ extern "C" int wsb_surface_create(const double* verts, int64_t n_verts, const in
   s->lo_y = gmin[1];
   s->cell = cell;
   s->K = K;
+  s->n_nonempty = nne;
   s->n_items = n_items;
   s->nb = nb;
   s->y0 = y0;
@@ -227,7 +233,7 @@ extern "C" int wsb_surface_create(const double* verts, int64_t n_verts, const in
   int rc = WSB_OK;
   if ((rc = upload(&s->verts, hv)) || (rc = upload(&s->edges, he)) || (rc = upload(&s->cstart, start)) ||
       (rc = upload(&s->citems, items)) || (rc = upload(&s->crec, crec)) || (rc = upload(&s->cind, cind)) ||
-      (rc = upload(&s->cempty, cempty)) || (rc = upload(&s->bstart, bstart)) || (rc = upload(&s->bitems, bitems)) ||
+      (rc = upload(&s->cempty, cempty)) || (rc = upload(&s->ccompact, ccompact)) || (rc = upload(&s->bstart, bstart)) || (rc = upload(&s->bitems, bitems)) ||
       (rc = upload(&s->erec, erec)) || (rc = upload(&s->brec, brec)) ||
       (rc = upload(&s->cok, std::vector<int32_t>(ncells, 0)))) {
     free_surface(s);
