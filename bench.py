@@ -241,9 +241,7 @@ def serving_run(n_requests, dev, pair_density, seed=0, loads=(0.8, 0.9, 0.95)):
     def stream(load):
         rate = load * cap_rows / mean_rows                     # requests per second
         arrivals = np.cumsum(unit / rate)
-        for r in list(srv.completed):
-            srv.release(r.rid)
-        srv.completed.clear()
+        srv.completed.clear()                                  # every request of an earlier stream is released
         srv.reset_stats()
         start = time.perf_counter()
         i = 0
@@ -259,7 +257,12 @@ def serving_run(n_requests, dev, pair_density, seed=0, loads=(0.8, 0.9, 0.95)):
                 srv.release(srv.completed[released[0]].rid)
                 released[0] += 1
         torch.cuda.synchronize()
-        return rate, time.perf_counter() - start, srv.stats()
+        wall = time.perf_counter() - start
+        st = srv.stats()
+        while released[0] < len(srv.completed):               # the ones completed by the last poll
+            srv.release(srv.completed[released[0]].rid)
+            released[0] += 1
+        return rate, wall, st
 
     tried = []
     for load in loads:
