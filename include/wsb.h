@@ -34,7 +34,11 @@ enum {
 /* kernel ids (warpsphboundaries_b200/kernels.py: KERNEL_IDS) */
 enum {
   WSB_KERNEL_CUBIC = 0, WSB_KERNEL_W2 = 1, WSB_KERNEL_W4 = 2, WSB_KERNEL_W6 = 3,
-  WSB_KERNEL_QUARTIC = 4, WSB_KERNEL_QUINTIC = 5, WSB_KERNEL_POLY6 = 6
+  WSB_KERNEL_QUARTIC = 4, WSB_KERNEL_QUINTIC = 5, WSB_KERNEL_POLY6 = 6,
+  /* the wall-operator kernels of the non-lean provider layout: cone (1 - q), whose G channels are the free-surface
+   * cover vector (edge/kernels.py:179-181, scene/cover.py); lw2 / lw4, W'/r of the Wendland C2 / C4 kernels, whose
+   * 2 lam - tr Cov is the wall Laplacian (scene/viscosity.py:48-61, scene/fused.py:11) */
+  WSB_KERNEL_CONE = 7, WSB_KERNEL_LW2 = 8, WSB_KERNEL_LW4 = 9
 };
 
 /* arithmetic of the fused aggregate */

@@ -70,6 +70,12 @@ def blocks(name):
         pieces = [(F(1), [C * x for x in _pmul(_ppow(om, n), poly)])]
     elif name == "poly6":
         pieces = [(F(1), [F(4) * x for x in [F(1), F(0), F(-3), F(0), F(3), F(0), F(-1)]])]
+    elif name in ("cone", "lw2", "lw4"):
+        # the wall-operator kernels: cone 3 (1 - r) (edge/kernels.py:179-181); W'/r of w2 / w4 registered as
+        # 10 (1 - r)^3 and 28/3 (6 u^5 - 5 u^6), u = 1 - r (scene/viscosity.py:48-61; normalisation of edge/kernels.py:141-156)
+        shape, C = {"cone": (om, F(3)), "lw2": (_ppow(om, 3), F(10)),
+                    "lw4": (_padd([6 * x for x in _ppow(om, 5)], [-5 * x for x in _ppow(om, 6)]), F(28, 3))}[name]
+        pieces = [(F(1), [C * x for x in shape])]
     else:
         terms, C = {"quartic": ([(1, F(1), 4), (-5, F(3, 5), 4), (10, F(1, 5), 4)], F(46875, 2398)),
                     "quintic": ([(1, F(1), 5), (-6, F(2, 3), 5), (15, F(1, 3), 5)], F(15309, 478))}[name]

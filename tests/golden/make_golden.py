@@ -297,6 +297,45 @@ def triangle_golden(root, names=("triangle-size-1e-09", "triangle-size-0.01", "t
     (HERE / "triangle_golden.json").write_text(json.dumps(out, indent=1))
 
 
+WALL_KERNELS = ["cone", "lw2", "lw4"]
+
+
+def wall_kernel_golden(root, dps=40):
+    """the wall-operator kernels -- cone (the kernel of the free-surface cover vector) and lw2 / lw4 (W'/r of the wall
+    Laplacian, registered by scene/viscosity.py:_register) -- on the element cases of the 2-D golden subset: value,
+    moments |alpha| <= 2, gradient and moment gradients by the reference's own mpmath edge reduction
+    (edge/core.py:219-262), 40 digits; with the reference's registered normalisation and block coefficients."""
+    import mpmath as mp
+    core = importlib.import_module("warpSPHBoundaries.edge.core")
+    kernels = importlib.import_module("warpSPHBoundaries.edge.kernels")
+    visc = importlib.import_module("warpSPHBoundaries.scene.viscosity")
+    for fam in ("w2", "w4"):
+        visc._register(fam)
+    sub = json.loads((HERE / "edge2d_golden_subset.json").read_text())
+    moms = [(1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]
+    grads = [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]
+    s = lambda v: mp.nstr(v, 36)
+    out = {"meta": {"source": "edge/core.py value / gradient / moment / moment_gradient of the reference, 40 digits, "
+                              "on the element cases of edge2d_golden_subset.json", "kernels": WALL_KERNELS},
+           "kernels": {k: {"c2_pi": str(kernels.KERNELS[k].c2_pi),
+                           "blocks": [[str(b.R), [str(c) for c in b.coeffs]] for b in kernels.KERNELS[k].blocks]}
+                       for k in WALL_KERNELS},
+           "cases": []}
+    for c in sub["cases"]:
+        P, x, h = c["polygon"], c["x"], c["h"]
+        rec = {"id": c["id"], "kernels": {}}
+        for k in WALL_KERNELS:
+            e = {"value": s(core.value(P, x, k, h=h, dps=dps)),
+                 "grad": [s(g) for g in core.gradient(P, x, k, h=h, dps=dps)],
+                 "moments": {f"{a},{b}": s(core.moment(P, x, k, (a, b), h=h, dps=dps)) for a, b in moms},
+                 "moment_grad": {f"{a},{b}": [s(g) for g in core.moment_gradient(P, x, k, (a, b), h=h, dps=dps)]
+                                 for a, b in grads}}
+            rec["kernels"][k] = e
+        out["cases"].append(rec)
+    (HERE / "edge2d_wall_kernels.json").write_text(json.dumps(out, indent=1))
+    print("edge2d_wall_kernels.json:", len(out["cases"]), "cases")
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     np2d, torch2d = load_reference(root)
@@ -306,3 +345,4 @@ if __name__ == "__main__":
     radial_golden(root)
     mesh3d_golden(root)
     triangle_golden(root)
+    wall_kernel_golden(root)

@@ -168,3 +168,27 @@ def test_misaligned_outputs_and_the_add_mode(c2s, kernel):
     for k in widths:
         assert torch.equal(aligned[k], shifted[k]), k
         assert torch.equal(aligned[k], first[k] + first[k]), k
+
+
+def test_wall_operator_groups_cover_vector_and_laplacian(c2s):
+    """FusedWall with the delta+ groups it serves -- the smoothing kernel, lw2 (W'/r of w2) and cone: the 'lap' output
+    (2 lam - tr Cov of the lw2 group, the wall Laplacian before the scheme's factor) and the cover vector (G of the cone
+    group) against the oracle, and every group equal to its one-group FusedWall."""
+    from helpers import oracle_outputs
+    from warpsphboundaries_b200.provider import WallOutput
+    loops, X, h = c2s
+    scene, rep, body = make_scene(loops, center=(0.01, 0.02), angle=-0.4)
+    ps = ParticleState(torch.tensor(X, dtype=torch.float64, device=DEV),
+                       torch.full((len(X),), h, dtype=torch.float64, device=DEV))
+    groups = (FusedGroup("w2"), FusedGroup("lw2"), FusedGroup("cone", (3, 4)))
+    fw = FusedWall(scene, ps, h, groups)
+    out = fw.evaluate([WallOutput("lap", 1, "lap"), WallOutput("cover", 2, "g0")])
+    ref_l = oracle_outputs(loops, X, h, "lw2", h, center=(0.01, 0.02), angle=-0.4)
+    ref_c = oracle_outputs(loops, X, h, "cone", h, center=(0.01, 0.02), angle=-0.4)
+    lap_ref = 2.0 * ref_l["lam"] - (ref_l["Cov"][:, 0, 0] + ref_l["Cov"][:, 1, 1])
+    assert np.abs(out["lap"][0].cpu().numpy() - lap_ref).max() < 1e-10
+    assert np.abs((out["cover"][0].cpu().numpy() - ref_c["G"]) * h).max() < 1e-10
+    for gi, g in enumerate(groups):
+        one = FusedWall(scene, ps, h, (g,))
+        for name in NAMES:
+            assert torch.equal(fw.res[gi][name], one.res[0][name]), (g.kernel, name)

@@ -122,8 +122,8 @@ def test_routes_agree_and_error_paths():
         AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Wendland2)          # the delta+ layout
     with pytest.raises(NotImplementedError):
         fused.cone_area(torch.zeros((len(X), 2), device=DEV), 0.5)
-    with pytest.raises(NotImplementedError):
-        fused.evaluate([WallOutput("L", 0, "lap")])
+    with pytest.raises(ValueError):
+        fused.evaluate([WallOutput("L", 0, "lap")])                  # 'lap' needs an lw2 / lw4 group
     with pytest.raises(NotImplementedError):
         AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Gaussian, lean=True)
     # a conditioned single triangle is served on the fused route (its small / sliver rows by the area quadrature),

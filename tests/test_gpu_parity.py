@@ -18,7 +18,7 @@ from warpsphboundaries_b200 import workloads
 from warpsphboundaries_b200.fixedadj import fixed_topology
 
 pytestmark = pytest.mark.gpu
-KERNELS = ["cubic", "w2", "w4", "w6", "quartic", "quintic", "poly6"]
+KERNELS = ["cubic", "w2", "w4", "w6", "quartic", "quintic", "poly6", "cone", "lw2", "lw4"]
 TOL64 = 1e-10
 TOL_MIXED = 1e-6
 
@@ -82,7 +82,7 @@ def test_fp64_routes_match_oracle_c2(c2s, kernel, route):
     assert max(err.values()) < TOL64, err
 
 
-@pytest.mark.parametrize("kernel", ["cubic", "w2", "w4", "w6"])
+@pytest.mark.parametrize("kernel", ["cubic", "w2", "w4", "w6", "cone", "lw2", "lw4"])
 def test_mixed_route_within_1e6(c2s, kernel):
     loops, X, h = c2s
     scene, rep, body = make_scene(loops)

@@ -79,3 +79,44 @@ def test_plane_constants():
     for k, (m, p2) in {"w4": (1, F(7, 132)), "w2": (1, F(5, 72)), "w6": (1, F(3, 70)), "cubic": (1, F(31, 392))}.items():
         mass, plane2 = O.kernel_mass_and_plane(k)
         assert mass == m and plane2 == p2
+
+
+WALL = json.loads((G / "edge2d_wall_kernels.json").read_text())
+
+
+def test_wall_kernel_tables_equal_the_reference_registration():
+    """cone, lw2, lw4: the normalisation and block coefficients the reference registers (edge/kernels.py, scene/
+    viscosity.py) equal the exact tables of the library and of the oracle."""
+    from warpsphboundaries_b200 import kernels as K
+    for k, ref in WALL["kernels"].items():
+        assert K.kernel(k).c2pi == F(ref["c2_pi"])
+        ours = [(b.R, [F(x) for x in b.c]) for b in K.kernel(k).blocks]
+        theirs = [(F(R), [F(x) for x in cs]) for R, cs in ref["blocks"]]
+        assert len(ours) == len(theirs)
+        for (r0, c0), (r1, c1) in zip(ours, theirs):
+            assert r0 == r1
+            n = max(len(c0), len(c1))
+            assert c0 + [F(0)] * (n - len(c0)) == c1 + [F(0)] * (n - len(c1)), k
+        orc = O.blocks(k)
+        assert [(R, [P.get(i, F(0)) for i in range(len(cs))]) for (R, P), (_, cs) in zip(orc, theirs)] == theirs
+
+
+@pytest.mark.parametrize("case", WALL["cases"], ids=[c["id"] for c in WALL["cases"]])
+def test_oracle_matches_wall_kernel_golden_vectors(case):
+    """the wall-operator kernels (cone, lw2, lw4) on every golden element: value, moments |alpha| <= 2, gradient and
+    moment gradients against the reference's 40-digit evaluation, absolute error <= 1e-11 (1 + |ref|)."""
+    geo = next(c for c in GOLD["cases"] if c["id"] == case["id"])
+    P, x, h = _case(geo)
+    for k, e in case["kernels"].items():
+        r = O.polygon_moments(P, x, h, k)
+        pairs = [(r[(0, 0)], e["value"])]
+        for al in [(1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]:
+            pairs.append((r[al], e["moments"][f"{al[0]},{al[1]}"]))
+        pairs += [(r["G"][0], e["grad"][0]), (r["G"][1], e["grad"][1])]
+        for al in [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]:
+            g = O.moment_gradient(P, x, h, k, al)
+            ref = e["moment_grad"][f"{al[0]},{al[1]}"]
+            pairs += [(g[0], ref[0]), (g[1], ref[1])]
+        for got, ref in pairs:
+            ref = float(ref)
+            assert abs(got - ref) <= 1e-11 * (1 + abs(ref)), (case["id"], k, got, ref)

@@ -435,6 +435,9 @@ inline int dispatch_kernel(int kernel, F&& f) {
     case WSB_KERNEL_QUARTIC: return f(Kern_quartic{});
     case WSB_KERNEL_QUINTIC: return f(Kern_quintic{});
     case WSB_KERNEL_POLY6: return f(Kern_poly6{});
+    case WSB_KERNEL_CONE: return f(Kern_cone{});
+    case WSB_KERNEL_LW2: return f(Kern_lw2{});
+    case WSB_KERNEL_LW4: return f(Kern_lw4{});
     default: return fail(WSB_ERR_UNSUPPORTED, "unknown kernel id " + std::to_string(kernel));
   }
 }

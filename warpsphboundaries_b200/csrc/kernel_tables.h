@@ -4,7 +4,7 @@
 
 namespace wsb {
 
-constexpr int kNumKernels = 7;
+constexpr int kNumKernels = 10;
 constexpr int kMaxA = 14;   // A_n, n = 0 .. kMaxA-1
 
 struct BlockSums {      // per (pair, block) chord sums, before the 1/pi and the edge frame
@@ -325,13 +325,106 @@ template <> __host__ __device__ __forceinline__ void Kern_poly6::adj<0>(const do
   o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
 }
 
+// ---- cone: C2*pi = 3, plane second moment 3/20
+struct Kern_cone {
+  static constexpr int kId = 7;
+  static constexpr int kBlocks = 1;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.15;
+  static constexpr double kR[kBlocks] = {1.0};
+  static constexpr int kNA[kBlocks] = {4};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {4};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_cone::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['3', '-3']
+  o.W0 = 3.0*A[0] + -3.0*A[1];
+  o.W1 = (((fma(-1.0, rhi, 1.5))*rhi)*rhi) - (((fma(-1.0, rlo, 1.5))*rlo)*rlo);
+  o.P0 = -0.5*A[0] + 1.5*A[2] + -1.0*A[3];
+  o.P1 = (((fma(fma(fma(-0.2, rhi, 0.375), rhi, 0.0), rhi, -0.25))*rhi)*rhi) - (((fma(fma(fma(-0.2, rlo, 0.375), rlo, 0.0), rlo, -0.25))*rlo)*rlo);
+  o.Lreg = 1.5*A[0] + -1.0*A[1];
+  o.Preg = -0.25*A[0] + 0.375*A[2] + -0.2*A[3];
+  o.Mhat = 0.5;
+  o.MPhat = -0.075;
+}
+template <> __host__ __device__ __forceinline__ void Kern_cone::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 3.0*A[0] + -3.0*A[1];
+  const double a2 = 3.0*A[2] + -3.0*A[3];
+  const double m1 = (((fma(-1.0, rhi, 1.5))*rhi)*rhi) - (((fma(-1.0, rlo, 1.5))*rlo)*rlo);
+  const double m3 = (((((fma(-0.6, rhi, 0.75))*rhi)*rhi)*rhi)*rhi) - (((((fma(-0.6, rlo, 0.75))*rlo)*rlo)*rlo)*rlo);
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- lw2: C2*pi = 10, plane second moment 1/14
+struct Kern_lw2 {
+  static constexpr int kId = 8;
+  static constexpr int kBlocks = 1;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.07142857142857142;
+  static constexpr double kR[kBlocks] = {1.0};
+  static constexpr int kNA[kBlocks] = {6};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {6};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_lw2::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['10', '-30', '30', '-10']
+  o.W0 = 10.0*A[0] + -30.0*A[1] + 30.0*A[2] + -10.0*A[3];
+  o.W1 = (((fma(fma(fma(-2.0, rhi, 7.5), rhi, -10.0), rhi, 5.0))*rhi)*rhi) - (((fma(fma(fma(-2.0, rlo, 7.5), rlo, -10.0), rlo, 5.0))*rlo)*rlo);
+  o.P0 = -0.5*A[0] + 5.0*A[2] + -10.0*A[3] + 7.5*A[4] + -2.0*A[5];
+  o.P1 = (((fma(fma(fma(fma(fma(-0.2857142857142857, rhi, 1.25), rhi, -2.0), rhi, 1.25), rhi, 0.0), rhi, -0.25))*rhi)*rhi) - (((fma(fma(fma(fma(fma(-0.2857142857142857, rlo, 1.25), rlo, -2.0), rlo, 1.25), rlo, 0.0), rlo, -0.25))*rlo)*rlo);
+  o.Lreg = 5.0*A[0] + -10.0*A[1] + 7.5*A[2] + -2.0*A[3];
+  o.Preg = -0.25*A[0] + 1.25*A[2] + -2.0*A[3] + 1.25*A[4] + -0.2857142857142857*A[5];
+  o.Mhat = 0.5;
+  o.MPhat = -0.03571428571428571;
+}
+template <> __host__ __device__ __forceinline__ void Kern_lw2::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 10.0*A[0] + -30.0*A[1] + 30.0*A[2] + -10.0*A[3];
+  const double a2 = 10.0*A[2] + -30.0*A[3] + 30.0*A[4] + -10.0*A[5];
+  const double m1 = (((fma(fma(fma(-2.0, rhi, 7.5), rhi, -10.0), rhi, 5.0))*rhi)*rhi) - (((fma(fma(fma(-2.0, rlo, 7.5), rlo, -10.0), rlo, 5.0))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(-1.4285714285714286, rhi, 5.0), rhi, -6.0), rhi, 2.5))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(-1.4285714285714286, rlo, 5.0), rlo, -6.0), rlo, 2.5))*rlo)*rlo)*rlo)*rlo);
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
+// ---- lw4: C2*pi = 28/3, plane second moment 1/18
+struct Kern_lw4 {
+  static constexpr int kId = 9;
+  static constexpr int kBlocks = 1;
+  static constexpr double kMass = 1.0;
+  static constexpr double kPlane2 = 0.05555555555555555;
+  static constexpr double kR[kBlocks] = {1.0};
+  static constexpr int kNA[kBlocks] = {9};   // A_0..A_{kNA-1} for the forward sums
+  static constexpr int kNAadj[kBlocks] = {9};   // for the adjoint sums
+  template <int B> __host__ __device__ static __forceinline__ void sums(const double* A, double rlo, double rhi, BlockSums& o);
+  template <int B> __host__ __device__ static __forceinline__ void adj(const double* A, double rlo, double rhi, double zz, AdjSums& o);
+};
+template <> __host__ __device__ __forceinline__ void Kern_lw4::sums<0>(const double* A, double rlo, double rhi, BlockSums& o) {
+  // block R = 1: P = ['28/3', '0', '-140', '1120/3', '-420', '224', '-140/3']
+  o.W0 = 9.333333333333334*A[0] + -140.0*A[2] + 373.3333333333333*A[3] + -420.0*A[4] + 224.0*A[5] + -46.666666666666664*A[6];
+  o.W1 = (((fma(fma(fma(fma(fma(fma(-5.833333333333333, rhi, 32.0), rhi, -70.0), rhi, 74.66666666666667), rhi, -35.0), rhi, 0.0), rhi, 4.666666666666667))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(-5.833333333333333, rlo, 32.0), rlo, -70.0), rlo, 74.66666666666667), rlo, -35.0), rlo, 0.0), rlo, 4.666666666666667))*rlo)*rlo);
+  o.P0 = -0.5*A[0] + 4.666666666666667*A[2] + -35.0*A[4] + 74.66666666666667*A[5] + -70.0*A[6] + 32.0*A[7] + -5.833333333333333*A[8];
+  o.P1 = (((fma(fma(fma(fma(fma(fma(fma(fma(-0.5833333333333334, rhi, 3.5555555555555554), rhi, -8.75), rhi, 10.666666666666666), rhi, -5.833333333333333), rhi, 0.0), rhi, 1.1666666666666667), rhi, 0.0), rhi, -0.25))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(fma(fma(-0.5833333333333334, rlo, 3.5555555555555554), rlo, -8.75), rlo, 10.666666666666666), rlo, -5.833333333333333), rlo, 0.0), rlo, 1.1666666666666667), rlo, 0.0), rlo, -0.25))*rlo)*rlo);
+  o.Lreg = 4.666666666666667*A[0] + -35.0*A[2] + 74.66666666666667*A[3] + -70.0*A[4] + 32.0*A[5] + -5.833333333333333*A[6];
+  o.Preg = -0.25*A[0] + 1.1666666666666667*A[2] + -5.833333333333333*A[4] + 10.666666666666666*A[5] + -8.75*A[6] + 3.5555555555555554*A[7] + -0.5833333333333334*A[8];
+  o.Mhat = 0.5;
+  o.MPhat = -0.027777777777777776;
+}
+template <> __host__ __device__ __forceinline__ void Kern_lw4::adj<0>(const double* A, double rlo, double rhi, double zz, AdjSums& o) {
+  const double a0 = 9.333333333333334*A[0] + -140.0*A[2] + 373.3333333333333*A[3] + -420.0*A[4] + 224.0*A[5] + -46.666666666666664*A[6];
+  const double a2 = 9.333333333333334*A[2] + -140.0*A[4] + 373.3333333333333*A[5] + -420.0*A[6] + 224.0*A[7] + -46.666666666666664*A[8];
+  const double m1 = (((fma(fma(fma(fma(fma(fma(-5.833333333333333, rhi, 32.0), rhi, -70.0), rhi, 74.66666666666667), rhi, -35.0), rhi, 0.0), rhi, 4.666666666666667))*rhi)*rhi) - (((fma(fma(fma(fma(fma(fma(-5.833333333333333, rlo, 32.0), rlo, -70.0), rlo, 74.66666666666667), rlo, -35.0), rlo, 0.0), rlo, 4.666666666666667))*rlo)*rlo);
+  const double m3 = (((((fma(fma(fma(fma(fma(fma(-4.666666666666667, rhi, 24.88888888888889), rhi, -52.5), rhi, 53.333333333333336), rhi, -23.333333333333332), rhi, 0.0), rhi, 2.3333333333333335))*rhi)*rhi)*rhi)*rhi) - (((((fma(fma(fma(fma(fma(fma(-4.666666666666667, rlo, 24.88888888888889), rlo, -52.5), rlo, 53.333333333333336), rlo, -23.333333333333332), rlo, 0.0), rlo, 2.3333333333333335))*rlo)*rlo)*rlo)*rlo);
+  o.W0 = a0; o.W1 = m1; o.W2 = a2 - zz * a0; o.W3 = m3 - zz * m1;
+}
+
 // ---- reference term plans (plain FP64 interpreter): per kernel offsets into flat tables
-constexpr int kPlanEdgeTerms = 132;
-constexpr int kPlanValueTerms = 60;
-constexpr int kPlanCoeffs = 1140;
-constexpr int kPlanNumRadii = 12;
+constexpr int kPlanEdgeTerms = 165;
+constexpr int kPlanValueTerms = 75;
+constexpr int kPlanCoeffs = 1353;
+constexpr int kPlanNumRadii = 15;
 struct PlanOffsets { int e0, e1, v0, v1; };
-static const PlanOffsets kPlanOffsets[kNumKernels] = {{0, 22, 0, 10}, {22, 33, 10, 15}, {33, 44, 15, 20}, {44, 55, 20, 25}, {55, 88, 25, 40}, {88, 121, 40, 55}, {121, 132, 55, 60}};
+static const PlanOffsets kPlanOffsets[kNumKernels] = {{0, 22, 0, 10}, {22, 33, 10, 15}, {33, 44, 15, 20}, {44, 55, 20, 25}, {55, 88, 25, 40}, {88, 121, 40, 55}, {121, 132, 55, 60}, {132, 143, 60, 65}, {143, 154, 65, 70}, {154, 165, 70, 75}};
 static const int kPlanE[kPlanEdgeTerms][7] = {   // ch, i, a, b, radius index, c0, c1
   {1, 0, 0, 0, 0, 8, 13},
   {1, 0, 0, 0, 1, 13, 18},
@@ -465,6 +558,39 @@ static const int kPlanE[kPlanEdgeTerms][7] = {   // ch, i, a, b, radius index, c
   {9, 0, 1, 0, 11, 1115, 1120},
   {10, 0, 0, 1, 11, 1125, 1130},
   {11, 1, 0, 1, 11, 1130, 1135},
+  {1, 0, 0, 0, 12, 1142, 1145},
+  {2, 1, 0, 0, 12, 1145, 1148},
+  {3, 0, 0, 0, 12, 1148, 1150},
+  {4, 1, 0, 0, 12, 1150, 1152},
+  {5, 0, 1, 0, 12, 1152, 1154},
+  {6, 1, 1, 0, 12, 1156, 1158},
+  {7, 0, 0, 1, 12, 1158, 1160},
+  {8, 1, 0, 1, 12, 1160, 1162},
+  {9, 0, 1, 0, 12, 1164, 1167},
+  {10, 0, 0, 1, 12, 1170, 1173},
+  {11, 1, 0, 1, 12, 1173, 1176},
+  {1, 0, 0, 0, 13, 1183, 1188},
+  {2, 1, 0, 0, 13, 1188, 1193},
+  {3, 0, 0, 0, 13, 1193, 1197},
+  {4, 1, 0, 0, 13, 1197, 1201},
+  {5, 0, 1, 0, 13, 1201, 1205},
+  {6, 1, 1, 0, 13, 1209, 1213},
+  {7, 0, 0, 1, 13, 1213, 1217},
+  {8, 1, 0, 1, 13, 1217, 1221},
+  {9, 0, 1, 0, 13, 1225, 1230},
+  {10, 0, 0, 1, 13, 1235, 1240},
+  {11, 1, 0, 1, 13, 1240, 1245},
+  {1, 0, 0, 0, 14, 1256, 1263},
+  {2, 1, 0, 0, 14, 1263, 1270},
+  {3, 0, 0, 0, 14, 1270, 1276},
+  {4, 1, 0, 0, 14, 1276, 1282},
+  {5, 0, 1, 0, 14, 1282, 1288},
+  {6, 1, 1, 0, 14, 1294, 1300},
+  {7, 0, 0, 1, 14, 1300, 1306},
+  {8, 1, 0, 1, 14, 1306, 1312},
+  {9, 0, 1, 0, 14, 1318, 1325},
+  {10, 0, 0, 1, 14, 1332, 1339},
+  {11, 1, 0, 1, 14, 1339, 1346},
 };
 static const int kPlanVi[kPlanValueTerms][4] = {   // ch, radius index, c0, c1
   {0, 0, 0, 4},
@@ -527,11 +653,26 @@ static const int kPlanVi[kPlanValueTerms][4] = {   // ch, radius index, c0, c1
   {8, 11, 1111, 1115},
   {9, 11, 1120, 1125},
   {11, 11, 1135, 1140},
+  {0, 12, 1140, 1142},
+  {5, 12, 1154, 1156},
+  {8, 12, 1162, 1164},
+  {9, 12, 1167, 1170},
+  {11, 12, 1176, 1179},
+  {0, 13, 1179, 1183},
+  {5, 13, 1205, 1209},
+  {8, 13, 1221, 1225},
+  {9, 13, 1230, 1235},
+  {11, 13, 1245, 1250},
+  {0, 14, 1250, 1256},
+  {5, 14, 1288, 1294},
+  {8, 14, 1312, 1318},
+  {9, 14, 1325, 1332},
+  {11, 14, 1346, 1353},
 };
-static const double kPlanVmR[kPlanValueTerms] = {0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.04081632653061224, -0.0012755102040816326, 0.04081632653061224, -0.0012755102040816326, 0.5, 0.5, 0.5, 0.034722222222222224, 0.034722222222222224, 0.5, 0.5, 0.5, 0.026515151515151516, 0.026515151515151516, 0.5, 0.5, 0.5, 0.02142857142857143, 0.02142857142857143, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.5, 0.5, 0.5, 0.05, 0.05};
-static const int kPlanCn[kPlanCoeffs] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8};
-static const double kPlanCc[kPlanCoeffs] = {5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05};
-static const double kPlanRadii[kPlanNumRadii] = {1.0, 0.5, 1.0, 1.0, 1.0, 1.0, 0.6, 0.2, 1.0, 0.6666666666666666, 0.3333333333333333, 1.0};
+static const double kPlanVmR[kPlanValueTerms] = {0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.5714285714285714, -0.07142857142857142, 0.04081632653061224, -0.0012755102040816326, 0.04081632653061224, -0.0012755102040816326, 0.5, 0.5, 0.5, 0.034722222222222224, 0.034722222222222224, 0.5, 0.5, 0.5, 0.026515151515151516, 0.026515151515151516, 0.5, 0.5, 0.5, 0.02142857142857143, 0.02142857142857143, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.6515846538782318, -0.15200166805671392, 0.0004170141784820684, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.03490632074347671, -0.0029314607410937687, 8.936018110330037e-07, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.7625523012552301, -0.26778242677824265, 0.005230125523012552, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.03177301255230126, -0.004958933829226716, 2.4213544088021077e-05, 0.5, 0.5, 0.5, 0.05, 0.05, 0.5, 0.5, 0.5, 0.075, 0.075, 0.5, 0.5, 0.5, 0.03571428571428571, 0.03571428571428571, 0.5, 0.5, 0.5, 0.027777777777777776, 0.027777777777777776};
+static const int kPlanCn[kPlanCoeffs] = {0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 7, 8, 9, 10, 11, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 2, 4, 6, 8, 9, 10, 11, 12, 13, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 1, 2, 3, 4, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 1, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 3, 4, 5, 6, 7, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 2, 4, 6, 8, 0, 1, 0, 2, 3, 0, 2, 3, 0, 1, 0, 1, 0, 1, 0, 1, 0, 1, 0, 1, 0, 1, 0, 1, 0, 2, 3, 0, 2, 3, 0, 2, 3, 0, 2, 3, 0, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 1, 2, 3, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 0, 2, 3, 4, 5, 6, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 3, 4, 5, 6, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8, 0, 2, 4, 5, 6, 7, 8};
+static const double kPlanCc[kPlanCoeffs] = {5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, -11.428571428571429, 34.285714285714285, -34.285714285714285, 11.428571428571429, 5.714285714285714, -34.285714285714285, 68.57142857142857, -45.714285714285715, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, -0.5714285714285714, 5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.07142857142857142, -2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.2857142857142857, -1.4285714285714286, 2.2857142857142856, -1.4285714285714286, 0.32653061224489793, -0.03571428571428571, 0.7142857142857143, -2.2857142857142856, 2.857142857142857, -1.3061224489795917, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, -7.0, 70.0, -140.0, 105.0, -28.0, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, -0.5, 3.5, -17.5, 28.0, -17.5, 4.0, 0.25, -0.875, 2.9166666666666665, -4.0, 2.1875, -0.4444444444444444, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, -9.0, 84.0, -630.0, 1344.0, -1260.0, 576.0, -105.0, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, -0.5, 4.5, -21.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.25, -1.125, 3.5, -13.125, 21.333333333333332, -15.75, 5.818181818181818, -0.875, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, -11.142857142857142, 122.57142857142857, -735.4285714285714, 5148.0, -11766.857142857143, 12870.0, -7844.571428571428, 2574.0, -356.57142857142856, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, -0.5, 5.571428571428571, -30.642857142857142, 122.57142857142857, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.25, -1.3928571428571428, 5.107142857142857, -15.321428571428571, 64.35, -118.85714285714286, 107.25, -54.857142857142854, 15.321428571428571, -1.8285714285714285, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, -19.547539616346956, 78.19015846538782, -117.28523769808173, 78.19015846538782, -19.547539616346956, 12.666805671392828, -84.44537114261885, 211.11342785654713, -234.57047539616346, 97.73769808173478, -0.3127606338615513, 6.255212677231026, -46.914095079232695, 156.38031693077565, -195.47539616346955, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, -0.6515846538782318, 9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.15200166805671392, -6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, -0.0004170141784820684, 0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.3257923269391159, -2.4434424520433695, 5.212677231025855, -4.886884904086739, 2.2340045275825093, -0.40724040867389494, -0.07600083402835696, 1.5833507089241035, -5.629691409507923, 8.79639282735613, -6.702013582747528, 2.0362020433694745, 0.0002085070892410342, -0.03909507923269391, 0.4170141784820684, -1.9547539616346956, 4.468009055165019, -4.072404086738949, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, -32.02719665271967, 160.13598326359832, -320.27196652719664, 320.27196652719664, -160.13598326359832, 32.02719665271967, 25.305439330543933, -189.7907949790795, 569.3723849372385, -854.0585774058577, 640.5439330543933, -192.163179916318, -1.9769874476987448, 29.65481171548117, -177.92887029288704, 533.7866108786611, -800.6799163179917, 480.407949790795, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, -0.7625523012552301, 16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.26778242677824265, -12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, -0.005230125523012552, 0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.38127615062761505, -4.003399581589958, 10.675732217573222, -13.344665271966527, 9.150627615062762, -3.3361663179916317, 0.5083682008368201, -0.13389121338912133, 3.1631799163179917, -12.652719665271967, 23.723849372384937, -24.401673640167363, 13.344665271966527, -3.0502092050209204, 0.002615062761506276, -0.2471234309623431, 1.9769874476987448, -7.4137029288702925, 15.251046025104603, -16.68083158995816, 7.625523012552302, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, -4.0, 12.0, -12.0, 4.0, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05, -0.5, 2.0, -3.0, 2.0, -0.5, -0.5, 2.0, -3.0, 2.0, -0.5, 0.25, -0.5, 0.5, -0.25, 0.05, 1.5, -1.0, -0.5, 1.5, -1.0, -0.5, 1.5, -1.0, -3.0, 3.0, -3.0, 3.0, -3.0, 3.0, 1.5, -1.0, -3.0, 3.0, -3.0, 3.0, -3.0, 3.0, 1.5, -1.0, -0.5, 1.5, -1.0, 0.25, -0.375, 0.2, -0.5, 1.5, -1.0, -0.5, 1.5, -1.0, 0.25, -0.375, 0.2, 5.0, -10.0, 7.5, -2.0, -0.5, 5.0, -10.0, 7.5, -2.0, -0.5, 5.0, -10.0, 7.5, -2.0, -10.0, 30.0, -30.0, 10.0, -10.0, 30.0, -30.0, 10.0, -10.0, 30.0, -30.0, 10.0, 5.0, -10.0, 7.5, -2.0, -10.0, 30.0, -30.0, 10.0, -10.0, 30.0, -30.0, 10.0, -10.0, 30.0, -30.0, 10.0, 5.0, -10.0, 7.5, -2.0, -0.5, 5.0, -10.0, 7.5, -2.0, 0.25, -1.25, 2.0, -1.25, 0.2857142857142857, -0.5, 5.0, -10.0, 7.5, -2.0, -0.5, 5.0, -10.0, 7.5, -2.0, 0.25, -1.25, 2.0, -1.25, 0.2857142857142857, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, -0.5, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, -0.5, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, -9.333333333333334, 140.0, -373.3333333333333, 420.0, -224.0, 46.666666666666664, -9.333333333333334, 140.0, -373.3333333333333, 420.0, -224.0, 46.666666666666664, -9.333333333333334, 140.0, -373.3333333333333, 420.0, -224.0, 46.666666666666664, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, -9.333333333333334, 140.0, -373.3333333333333, 420.0, -224.0, 46.666666666666664, -9.333333333333334, 140.0, -373.3333333333333, 420.0, -224.0, 46.666666666666664, -9.333333333333334, 140.0, -373.3333333333333, 420.0, -224.0, 46.666666666666664, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, -0.5, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, 0.25, -1.1666666666666667, 5.833333333333333, -10.666666666666666, 8.75, -3.5555555555555554, 0.5833333333333334, -0.5, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, -0.5, 4.666666666666667, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, 0.25, -1.1666666666666667, 5.833333333333333, -10.666666666666666, 8.75, -3.5555555555555554, 0.5833333333333334};
+static const double kPlanRadii[kPlanNumRadii] = {1.0, 0.5, 1.0, 1.0, 1.0, 1.0, 0.6, 0.2, 1.0, 0.6666666666666666, 0.3333333333333333, 1.0, 1.0, 1.0, 1.0};
 
 // ---- 3-D radial family (solid half-space / sphere), unit support; W = c3*pi * shape, L = W'/r, dL = L'
 template <int K, typename T>

@@ -38,13 +38,19 @@ from math import comb
 from typing import Dict, List, Tuple
 
 # kernel ids of the C ABI (include/wsb.h: WSB_KERNEL_*); order is part of the ABI
-KERNEL_IDS = {"cubic": 0, "w2": 1, "w4": 2, "w6": 3, "quartic": 4, "quintic": 5, "poly6": 6}
+KERNEL_IDS = {"cubic": 0, "w2": 1, "w4": 2, "w6": 3, "quartic": 4, "quintic": 5, "poly6": 6, "cone": 7, "lw2": 8,
+              "lw4": 9}
 KERNEL_NAMES = {v: k for k, v in KERNEL_IDS.items()}
 
 # published 2-D normalisations C2 * pi (src/warpSPHBoundaries/curvbound/kernels.py:5-13,
 # src/warpSPHBoundaries/edge/kernels.py:183-185); only used to check the recomputed ones
 _PUBLISHED_C2PI = {"cubic": F(80, 7), "w2": F(7), "w4": F(9), "w6": F(78, 7),
-                   "quartic": F(46875, 2398), "quintic": F(15309, 478), "poly6": F(4)}
+                   "quartic": F(46875, 2398), "quintic": F(15309, 478), "poly6": F(4),
+                   # the wall-operator kernels: cone (1 - q), the cover vector's kernel, normalisation 3
+                   # (src/warpSPHBoundaries/edge/kernels.py:179-181); lw2 (1 - q)^3 and lw4 6 u^5 - 5 u^6 (u = 1 - q),
+                   # the kernels W'/r of the wall Laplacian (src/warpSPHBoundaries/scene/viscosity.py:48-61), normalised
+                   # by the same rule C = 1 / (2 int_0^1 r shape dr)
+                   "cone": F(3), "lw2": F(10), "lw4": F(28, 3)}
 
 
 # ------------------------------------------------------------------ polynomial helpers (ascending coefficient lists)
@@ -106,6 +112,12 @@ def _pieces(name):
         return [(F(0), F(1), _pmul(_ppow(one_minus, n), poly))]
     if name == "poly6":
         return [(F(0), F(1), [F(1), F(0), F(-3), F(0), F(3), F(0), F(-1)])]
+    if name == "cone":
+        return [(F(0), F(1), one_minus)]
+    if name == "lw2":
+        return [(F(0), F(1), _ppow(one_minus, 3))]
+    if name == "lw4":
+        return [(F(0), F(1), _padd([6 * x for x in _ppow(one_minus, 5)], [-5 * x for x in _ppow(one_minus, 6)]))]
     terms = {"quartic": [(1, F(1), 4), (-5, F(3, 5), 4), (10, F(1, 5), 4)],
              "quintic": [(1, F(1), 5), (-6, F(2, 3), 5), (15, F(1, 3), 5)]}.get(name)
     if terms is None:

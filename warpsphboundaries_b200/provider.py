@@ -14,8 +14,10 @@ Routes:
   plain  the reference's structure on the GPU: fixed-capacity slots (wsb_fixed_topology), the per-slot plan
          interpreter (wsb_slot_channels_plain) writing c[N*K, 12], and the per-row contraction (wsb_contract).
 
-Outputs that belong to kernels this build does not tabulate (the delta+ layout's cover vector `cone`, wall Laplacian
-`lw2`/`lw4`, tensile `w2p5`/`w4p5`) and `cone_area` / `dir_extreme` raise NotImplementedError; they never return zeros.
+Kernel groups: the smoothing kernels (cubic, w2, w4, w6, quartic, quintic, poly6) and the wall-operator kernels of the
+delta+ layout, `cone` (its G is the free-surface cover vector) and `lw2` / `lw4` (W'/r; the `lap` output kind is
+2 lam - tr Cov, the wall Laplacian before the scheme's factor).  The tensile group (`w2p5` / `w4p5`), and with it the
+full delta+ layout, and `cone_area` / `dir_extreme` raise NotImplementedError; they never return zeros.
 """
 from dataclasses import dataclass
 from typing import Optional, Protocol, runtime_checkable
@@ -85,8 +87,8 @@ class FusedWall(WallAggregate):
         B = len(scene.bodies)
         for g in self.groups:
             if g.kernel not in KERNEL_IDS:
-                raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} (wall-operator layout: cover / "
-                                          f"Laplacian / tensile) is not built; use the lean layout")
+                raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} is not built (the tensile "
+                                          f"groups w2p5 / w4p5 of the delta+ layout among them)")
         sig = (route,) + tuple(id(r) for b in scene.bodies for r in b.reps)
         if getattr(scene, "_wsb_checked", None) != sig:
             for b in scene.bodies:
@@ -228,9 +230,14 @@ class FusedWall(WallAggregate):
                 if a1 is None:
                     raise ValueError("FusedWall.evaluate: a1 [B, N, 2] is required for 'a1g1' outputs")
                 res[o.name] = torch.einsum("bnd,bndj->bnj", a1.to(self.dev, F64), r["Cov"])
+            elif o.kind == "lap":
+                # the wall Laplacian of the registered W'/r kernel (lw2 / lw4): 2 lam - tr g1, the indicator cancels
+                # (fused.py:11); the trace is the same in the body and the world frame
+                if self.groups[o.group].kernel not in ("lw2", "lw4"):
+                    raise ValueError("FusedWall.evaluate: 'lap' outputs come from an lw2 / lw4 group")
+                res[o.name] = 2.0 * r["lam"] - (r["Cov"][..., 0, 0] + r["Cov"][..., 1, 1])
             else:
-                raise NotImplementedError("FusedWall.evaluate: the wall Laplacian ('lap', kernels lw2 / lw4) is not "
-                                          "built")
+                raise ValueError(f"FusedWall.evaluate: unknown output kind {o.kind!r}")
         return res
 
     def _tensors(self):
@@ -294,9 +301,12 @@ class AnalyticBoundary:
                                    operationMode=OperationDirection.BoundaryToFluid)
 
     def layout(self, kernel, laplacian, fixedAdjacency=True):
-        """the delta+ layout (kernel, cone, [lw], wp5) of provider.py:73-87: its wall-operator kernels are not built."""
-        raise NotImplementedError("AnalyticBoundary.layout: the delta+ wall-operator kernels (cover vector 'cone', "
-                                  "wall Laplacian, tensile) are not built; call aggregate(..., lean=True)")
+        """the delta+ layout (kernel, cone, [lw], wp5) of provider.py:73-87: its tensile group (w2p5 / w4p5) is not
+        built, so the layout is refused; the cover vector ('cone') and the wall Laplacian ('lw2' / 'lw4') groups are
+        available to FusedWall directly."""
+        self.family(kernel)
+        raise NotImplementedError("AnalyticBoundary.layout: the delta+ tensile group (w2p5 / w4p5) is not built; "
+                                  "call aggregate(..., lean=True), or FusedWall with the cone / lw2 / lw4 groups")
 
     def aggregate(self, ps, support, kernel=KernelFunctions.Wendland2, laplacian=False, fixedAdjacency=True,
                   lean=False):
