@@ -38,7 +38,12 @@ enum {
   /* the wall-operator kernels of the non-lean provider layout: cone (1 - q), whose G channels are the free-surface
    * cover vector (edge/kernels.py:179-181, scene/cover.py); lw2 / lw4, W'/r of the Wendland C2 / C4 kernels, whose
    * 2 lam - tr Cov is the wall Laplacian (scene/viscosity.py:48-61, scene/fused.py:11) */
-  WSB_KERNEL_CONE = 7, WSB_KERNEL_LW2 = 8, WSB_KERNEL_LW4 = 9
+  WSB_KERNEL_CONE = 7, WSB_KERNEL_LW2 = 8, WSB_KERNEL_LW4 = 9,
+  /* the tensile group of the delta+ layout: W^5 of Wendland C2 / C4 (scene/tensile.py, edge/kernels.py:214-232),
+   * polynomials of degree 25 / 40 integrated along each chord by graded Gauss-Legendre panels.  Fused aggregate only
+   * (wsb_aggregate, _evaluate, _groups, _noalloc); only the G output is defined (the others are written as NaN); no
+   * adjoint, no plain route */
+  WSB_KERNEL_W2P5 = 10, WSB_KERNEL_W4P5 = 11
 };
 
 /* arithmetic of the fused aggregate */

@@ -490,3 +490,88 @@ def shape_gradient(P, x, h, name, alpha):
         out[:, comp] += nrm * (a0 - a1) + np.roll(nrm * a1, 1)
     k = alpha[0] + alpha[1]
     return out * INV_PI * h ** (k - 1)
+
+
+# ----------------------------------------------------------------------------- powered kernels (tensile group)
+# pi*W = C u^p B(u)^5, u = 1 - r: the 5th power of the Wendland C2 / C4 shape (edge/kernels.py:214-232, registered by
+# scene/tensile.py:40-47), normalised by C = 1 / (2 int_0^1 r shape^5 dr) (edge/kernels.py:141-156)
+_POWERED = {"w2p5": (4, [F(5), F(-4)]), "w4p5": (6, [F(56, 3), F(-88, 3), F(35, 3)])}
+
+
+@lru_cache(maxsize=None)
+def powered(name):
+    """(C, p, base coefficients in u) of a powered kernel, C exact."""
+    p0, base = _POWERED[name]
+    shape = {"w2p5": _pmul(_ppow([F(1), F(-1)], 4), [F(1), F(4)]),
+             "w4p5": _pmul(_ppow([F(1), F(-1)], 6), [F(1), F(6), F(35, 3)])}[name]
+    s5 = [F(1)]
+    for _ in range(5):
+        s5 = _pmul(s5, shape)
+    integral = sum(c / (n + 2) for n, c in enumerate(s5))      # int_0^1 r shape^5 dr
+    return 1 / (2 * integral), 5 * p0, base
+
+
+def powered_pi_w(name, r):
+    C, p, base = powered(name)
+    u = 1.0 - np.minimum(r, 1.0)
+    b = sum(float(c) * u ** k for k, c in enumerate(base))
+    return float(C) * u ** p * b ** 5
+
+
+def _powered_chord(name, lo, hi, z):
+    """int_lo^hi pi*W(sqrt(s^2 + z^2)) ds by adaptive Gauss-Kronrod (QUADPACK), split at the foot s = 0."""
+    from scipy.integrate import quad
+    f = lambda s: powered_pi_w(name, np.sqrt(s * s + z * z))
+    pts = [0.0] if lo < 0.0 < hi else None
+    return quad(f, lo, hi, points=pts, epsabs=1e-15, epsrel=1e-13, limit=400)[0]
+
+
+def powered_gradient(P, x, h, name):
+    """grad_x int_solid W dA' of a powered kernel at x = -(1 / (pi h)) sum_e n_e int_chord pi*W ds (chord in units of
+    h, clipped to the support): the G channels of the tensile group, physical units [2]."""
+    P = np.asarray(P, dtype=np.float64)
+    a2 = np.sum(P[:, 0] * np.roll(P[:, 1], -1) - np.roll(P[:, 0], -1) * P[:, 1])
+    if a2 < 0:
+        P = P[::-1].copy()
+    x = np.asarray(x, dtype=np.float64).reshape(1, 2)
+    p = (P - x) / h
+    q = (np.roll(P, -1, 0) - x) / h
+    ok, t0, t1, n0, n1, z, s0, s1 = pair_geometry(p, q)
+    g = np.zeros(2)
+    for e in range(len(p)):
+        az = abs(z[e])
+        if not ok[e] or az >= 1.0:
+            continue
+        L = np.sqrt((1.0 - az) * (1.0 + az))
+        lo, hi = max(s0[e], -L), min(s1[e], L)
+        if lo < hi:
+            w = _powered_chord(name, lo, hi, z[e])
+            g -= np.array([n0[e], n1[e]]) * w
+    return g * INV_PI / h
+
+
+def powered_gradient_local(V, E, lpos, h, name):
+    """powered_gradient of every body-frame position lpos [N, 2] over the edges E of vertices V (the whole surface,
+    one call per particle over the edges within the support), [N, 2]."""
+    a, b = V[E[:, 0]], V[E[:, 1]]
+    out = np.zeros((len(lpos), 2))
+    for i, xq in enumerate(np.asarray(lpos, dtype=np.float64)):
+        d = b - a
+        t = np.clip(((xq - a) * d).sum(1) / np.maximum((d * d).sum(1), 1e-300), 0.0, 1.0)
+        dist = np.linalg.norm(a + t[:, None] * d - xq, axis=1)
+        near = np.flatnonzero(dist < h)
+        if len(near) == 0:
+            continue
+        p = (a[near] - xq) / h
+        q = (b[near] - xq) / h
+        ok, t0, t1, n0, n1, z, s0, s1 = pair_geometry(p, q)
+        for e in range(len(near)):
+            az = abs(z[e])
+            if not ok[e] or az >= 1.0:
+                continue
+            L = np.sqrt((1.0 - az) * (1.0 + az))
+            lo, hi = max(s0[e], -L), min(s1[e], L)
+            if lo < hi:
+                w = _powered_chord(name, lo, hi, z[e])
+                out[i] -= np.array([n0[e], n1[e]]) * w
+    return out * INV_PI / h

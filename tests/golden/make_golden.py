@@ -298,6 +298,7 @@ def triangle_golden(root, names=("triangle-size-1e-09", "triangle-size-0.01", "t
 
 
 WALL_KERNELS = ["cone", "lw2", "lw4"]
+POWERED_KERNELS = ["w2p5", "w4p5"]
 
 
 def wall_kernel_golden(root, dps=40):
@@ -311,6 +312,8 @@ def wall_kernel_golden(root, dps=40):
     visc = importlib.import_module("warpSPHBoundaries.scene.viscosity")
     for fam in ("w2", "w4"):
         visc._register(fam)
+        # the tensile kernel W^5, registered as scene/tensile.py:_register does (its warpbc import needs warp)
+        kernels.KERNELS[fam + "p5"] = kernels._from_terms(fam + "p5", kernels.power_terms(5, fam))
     sub = json.loads((HERE / "edge2d_golden_subset.json").read_text())
     moms = [(1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]
     grads = [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]
@@ -319,7 +322,7 @@ def wall_kernel_golden(root, dps=40):
                               "on the element cases of edge2d_golden_subset.json", "kernels": WALL_KERNELS},
            "kernels": {k: {"c2_pi": str(kernels.KERNELS[k].c2_pi),
                            "blocks": [[str(b.R), [str(c) for c in b.coeffs]] for b in kernels.KERNELS[k].blocks]}
-                       for k in WALL_KERNELS},
+                       for k in WALL_KERNELS + POWERED_KERNELS},
            "cases": []}
     for c in sub["cases"]:
         P, x, h = c["polygon"], c["x"], c["h"]
@@ -331,6 +334,8 @@ def wall_kernel_golden(root, dps=40):
                  "moment_grad": {f"{a},{b}": [s(g) for g in core.moment_gradient(P, x, k, (a, b), h=h, dps=dps)]
                                  for a, b in grads}}
             rec["kernels"][k] = e
+        # the tensile kernels: the gradient only (their group's G channels)
+        rec["powered_grad"] = {k: [s(g) for g in core.gradient(P, x, k, h=h, dps=dps)] for k in POWERED_KERNELS}
         out["cases"].append(rec)
     (HERE / "edge2d_wall_kernels.json").write_text(json.dumps(out, indent=1))
     print("edge2d_wall_kernels.json:", len(out["cases"]), "cases")

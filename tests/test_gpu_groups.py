@@ -192,3 +192,52 @@ def test_wall_operator_groups_cover_vector_and_laplacian(c2s):
         one = FusedWall(scene, ps, h, (g,))
         for name in NAMES:
             assert torch.equal(fw.res[gi][name], one.res[0][name]), (g.kernel, name)
+
+
+@pytest.mark.parametrize("kernel", ["w2p5", "w4p5"])
+def test_tensile_group_gradient_matches_oracle(c2s, kernel):
+    """the tensile group (W^5 of Wendland C2 / C4, chord quadrature): its G against the oracle's adaptive quadrature
+    (pinned to the reference's 40-digit values), 1e-10 in units of 1/h; its other outputs are NaN, not numbers."""
+    from oracle import edge2d as O
+    loops, X, h = c2s
+    X = X[:1500]
+    scene, rep, body = make_scene(loops)
+    ps = ParticleState(torch.tensor(X, dtype=torch.float64, device=DEV),
+                       torch.full((len(X),), h, dtype=torch.float64, device=DEV))
+    fw = FusedWall(scene, ps, h, (FusedGroup(kernel, (3, 4)),))
+    from helpers import workloads
+    V, E = workloads.edges_of(loops)
+    ref = O.powered_gradient_local(V, E, X, h, kernel)
+    got = fw.res[0]["G"][0].cpu().numpy()
+    assert np.abs((got - ref) * h).max() < 1e-10
+    assert np.abs(ref).max() > 1.0
+    assert torch.isnan(fw.res[0]["lam"]).all()
+    with pytest.raises(ValueError):
+        from warpsphboundaries_b200.provider import WallOutput
+        fw.evaluate([WallOutput("x", 0, "lam")])
+
+
+def test_delta_plus_layout_aggregate(c2s):
+    """AnalyticBoundary.aggregate without `lean`: the delta+ layout (w2, cone, lw2, w2p5) -- lam, G, Cov of the scheme
+    kernel, the cover vector, the wall Laplacian and the tensile vector -- against the oracle."""
+    from oracle import edge2d as O
+    from helpers import oracle_outputs, workloads
+    from warpsphboundaries_b200.provider import AnalyticBoundary
+    from warpsphboundaries_b200.shim import KernelFunctions
+    loops, X, h = c2s
+    X = X[:1500]
+    scene, rep, body = make_scene(loops)
+    ps = ParticleState(torch.tensor(X, dtype=torch.float64, device=DEV),
+                       torch.full((len(X),), h, dtype=torch.float64, device=DEV))
+    fw = AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Wendland2, laplacian=True)
+    assert set(fw.out) == {"lam", "G", "Cov", "cover", "lap", "tens"}
+    w = oracle_outputs(loops, X, h, "w2", h)
+    assert np.abs(fw.out["lam"][0].cpu().numpy() - w["lam"]).max() < 1e-10
+    c = oracle_outputs(loops, X, h, "cone", h)
+    assert np.abs((fw.out["cover"][0].cpu().numpy() - c["G"]) * h).max() < 1e-10
+    lw = oracle_outputs(loops, X, h, "lw2", h)
+    lap = 2.0 * lw["lam"] - (lw["Cov"][:, 0, 0] + lw["Cov"][:, 1, 1])
+    assert np.abs(fw.out["lap"][0].cpu().numpy() - lap).max() < 1e-10
+    V, E = workloads.edges_of(loops)
+    t = O.powered_gradient_local(V, E, X, h, "w2p5")
+    assert np.abs((fw.out["tens"][0].cpu().numpy() - t) * h).max() < 1e-10

@@ -118,8 +118,10 @@ def test_routes_agree_and_error_paths():
     plain = AnalyticBoundary(scene, route="plain").aggregate(ps, h, kernel=KernelFunctions.Wendland6, lean=True)
     for k in ("lam", "G", "Cov"):
         assert (fused.out[k] - plain.out[k]).abs().max().item() < 1e-9
+    dp = AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Wendland2)      # the delta+ layout
+    assert set(dp.out) == {"lam", "G", "Cov", "cover", "tens"}
     with pytest.raises(NotImplementedError):
-        AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Wendland2)          # the delta+ layout
+        AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Wendland6)          # C2 / C4 only
     with pytest.raises(NotImplementedError):
         fused.cone_area(torch.zeros((len(X), 2), device=DEV), 0.5)
     with pytest.raises(ValueError):

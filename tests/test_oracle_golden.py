@@ -88,7 +88,8 @@ def test_wall_kernel_tables_equal_the_reference_registration():
     """cone, lw2, lw4: the normalisation and block coefficients the reference registers (edge/kernels.py, scene/
     viscosity.py) equal the exact tables of the library and of the oracle."""
     from warpsphboundaries_b200 import kernels as K
-    for k, ref in WALL["kernels"].items():
+    for k in ("cone", "lw2", "lw4"):
+        ref = WALL["kernels"][k]
         assert K.kernel(k).c2pi == F(ref["c2_pi"])
         ours = [(b.R, [F(x) for x in b.c]) for b in K.kernel(k).blocks]
         theirs = [(F(R), [F(x) for x in cs]) for R, cs in ref["blocks"]]
@@ -120,3 +121,28 @@ def test_oracle_matches_wall_kernel_golden_vectors(case):
         for got, ref in pairs:
             ref = float(ref)
             assert abs(got - ref) <= 1e-11 * (1 + abs(ref)), (case["id"], k, got, ref)
+
+
+def test_powered_kernel_normalisation_equals_the_reference_registration():
+    """w2p5 / w4p5 (W^5 of Wendland C2 / C4, the tensile group): the reference's normalisation equals ours and the
+    oracle's; its block is the expanded polynomial of C u^p B(u)^5."""
+    from warpsphboundaries_b200 import kernels as K
+    for k in ("w2p5", "w4p5"):
+        ref = WALL["kernels"][k]
+        assert K.quad_kernel(k)[0] == F(ref["c2_pi"]) == O.powered(k)[0]
+        (R, cs), = ref["blocks"]
+        r = F(3, 7)
+        assert sum(F(c) * r ** n for n, c in enumerate(cs)) == K.pi_w_quad(k, r)
+
+
+@pytest.mark.parametrize("case", WALL["cases"], ids=[c["id"] for c in WALL["cases"]])
+def test_oracle_tensile_gradient_matches_golden(case):
+    """the tensile kernels' gradient (adaptive quadrature along each chord) against the reference's 40-digit exact
+    edge reduction on every golden element: absolute error <= 1e-11 (1 + |ref|)."""
+    geo = next(c for c in GOLD["cases"] if c["id"] == case["id"])
+    P, x, h = _case(geo)
+    for k, ref in case["powered_grad"].items():
+        got = O.powered_gradient(P, x, h, k)
+        for a, b in zip(got, ref):
+            b = float(b)
+            assert abs(a - b) <= 1e-11 * (1 + abs(b)), (case["id"], k, a, b)

@@ -351,6 +351,39 @@ __device__ __forceinline__ void add_block(const PairGeo& g, const BlockSums& S, 
   acc[11] += g.n1 * Z1 - Vp;
 }
 
+// int_lo^hi pi*W(sqrt(s^2 + z^2)) ds of a quadrature kernel (KT::poly = pi*W on r <= 1), the chord [lo, hi] already
+// clipped to the support: Gauss-Legendre panels on both sides of the foot s = 0, graded from it -- the first up to
+// 2 max(|z|, 2^-24), then doubling.  pi*W is analytic except through r, whose branch points s = +-iz lie a panel's
+// half-length away from the first panel (Bernstein parameter ~2.9: the 24-node rule is below 1e-15 there) and ever
+// further from the doubled ones; the 24 nodes integrate the polynomial part (degree <= 47) exactly.
+template <class KT>
+__device__ __forceinline__ double quad_chord(double lo, double hi, double z) {
+  const double zz = z * z, base = fmax(fabs(z), 0x1p-24);
+  double sum = 0.0;
+  for (int side = 0; side < 2; ++side) {
+    const double u0 = side == 0 ? fmax(-hi, 0.0) : fmax(lo, 0.0);
+    const double u1 = side == 0 ? -lo : hi;
+    if (!(u1 > u0)) continue;
+    double d = 2.0 * base;
+    for (int it = 0; it < 64 && d <= u0; ++it) d *= 2.0;
+    double u = u0;
+    for (int it = 0; it < 64 && u < u1; ++it) {
+      const double nxt = fmin(u1, d);
+      const double hc = 0.5 * (nxt - u), mc = 0.5 * (nxt + u);
+      double ps = 0.0;
+#pragma unroll
+      for (int k = 0; k < kQuadGauss; ++k) {
+        const double x = fma(hc, kQuadGx[k], mc);
+        ps = fma(kQuadGw[k], KT::poly(fmin(sqrt(fma(x, x, zz)), 1.0)), ps);
+      }
+      sum = fma(hc, ps, sum);
+      if (nxt >= d) d *= 2.0;
+      u = nxt;
+    }
+  }
+  return sum;
+}
+
 // One kernel block (truncated monomial profile on r <= R_B) of one pair: the clipped chord, its monomial integrals,
 // the six chord sums of the block and their contribution to the twelve channels.
 template <class KT, int B, int PREC, class Acc>

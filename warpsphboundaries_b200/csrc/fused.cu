@@ -332,19 +332,28 @@ constexpr int pack_min_blocks(int n) {
 
 // every (kernel, block) of the pack whose radius is the D-th distinct radius: its chord sums into its accumulators
 template <class Pack, int D, int K, int B>
-__device__ __forceinline__ void pack_blocks_at(const PairGeo& g, const double* A, double rlo, double rhi, double dang,
-                                               double* acc_t) {
+__device__ __forceinline__ void pack_blocks_at(const PairGeo& g, double lo, double hi, const double* A, double rlo,
+                                               double rhi, double dang, double* acc_t) {
   if constexpr (K < Pack::kN) {
     using KT = typename Pack::template Kern<K>;
     if constexpr (B < KT::kBlocks) {
       if constexpr (KT::kR[B] == Pack::kRadii.r[D]) {
-        BlockSums S;
-        KT::template sums<B>(A, rlo, rhi, S);
-        add_block(g, S, dang, SmemAcc{acc_t + K * 12 * kThreads});
+        if constexpr (KT::kQuad) {
+          // a quadrature kernel contributes its gradient channels only: G = -n int W ds (no indicator term, W and
+          // W' vanish at the support edge)
+          const double W0 = quad_chord<KT>(lo, hi, g.z);
+          const SmemAcc a{acc_t + K * 12 * kThreads};
+          a[3] -= g.n0 * W0;
+          a[4] -= g.n1 * W0;
+        } else {
+          BlockSums S;
+          KT::template sums<B>(A, rlo, rhi, S);
+          add_block(g, S, dang, SmemAcc{acc_t + K * 12 * kThreads});
+        }
       }
-      pack_blocks_at<Pack, D, K, B + 1>(g, A, rlo, rhi, dang, acc_t);
+      pack_blocks_at<Pack, D, K, B + 1>(g, lo, hi, A, rlo, rhi, dang, acc_t);
     } else {
-      pack_blocks_at<Pack, D, K + 1, 0>(g, A, rlo, rhi, dang, acc_t);
+      pack_blocks_at<Pack, D, K + 1, 0>(g, lo, hi, A, rlo, rhi, dang, acc_t);
     }
   }
 }
@@ -361,9 +370,31 @@ __device__ __forceinline__ void pack_pair(const PairGeo& g, double* acc_t) {
       special_fns<PREC>(lo, hi, rlo, rhi, g.z, zz, dasinh, dang);
       double A[NA];
       chord_monomials<NA>(lo, hi, rlo, rhi, zz, dasinh, A);
-      pack_blocks_at<Pack, D, 0, 0>(g, A, rlo, rhi, dang, acc_t);
+      pack_blocks_at<Pack, D, 0, 0>(g, lo, hi, A, rlo, rhi, dang, acc_t);
     }
     pack_pair<Pack, PREC, D + 1>(g, acc_t);
+  }
+}
+
+// the outputs of a row of a quadrature kernel: its gradient channels G (scaled, rotated); the other outputs are not
+// defined for it and are written as NaN
+__device__ __forceinline__ void finish_row_quad(const double acc[12], double h, const double* pose, int64_t i,
+                                                bool assign, double* lam, double* G, double* cov, double* m1,
+                                                double* m2) {
+  const double c = pose[2], s = pose[3], nan = __longlong_as_double(0x7ff8000000000000LL);
+  if (lam) put(&lam[i], nan, assign);
+  if (G) {
+    const double vx = acc[3] / h, vy = acc[4] / h;
+    put(&G[2 * i], c * vx - s * vy, assign);
+    put(&G[2 * i + 1], s * vx + c * vy, assign);
+  }
+  for (int k = 0; k < 4; ++k) {
+    if (cov) put(&cov[4 * i + k], nan, assign);
+    if (m2) put(&m2[4 * i + k], nan, assign);
+  }
+  if (m1) {
+    put(&m1[2 * i], nan, assign);
+    put(&m1[2 * i + 1], nan, assign);
   }
 }
 
@@ -377,7 +408,10 @@ __device__ __forceinline__ void pack_constant_row(int64_t i, double w, double h,
     double acc[12];
 #pragma unroll
     for (int c = 0; c < 12; ++c) acc[c] = 0.0;
-    finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+    if constexpr (KT::kQuad)
+      finish_row_quad(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+    else
+      finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
     pack_constant_row<Pack, K + 1>(i, w, h, pose, assign, o);
   }
 }
@@ -400,7 +434,10 @@ __device__ __forceinline__ void pack_finish(const double* acc_t, bool write, int
     if (write) {
 #pragma unroll
       for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
-      finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+      if constexpr (KT::kQuad)
+        finish_row_quad(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+      else
+        finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
     }
     pack_finish<Pack, G, K + 1>(acc_t, write, i, w, h, pose, assign, o);
   }
@@ -839,10 +876,14 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
   return WSB_OK;
 }
 
+// kernel ids the fused aggregate serves: the exact-table kernels and the quadrature kernels (the tensile group)
+static bool is_quad_kernel(int k) { return k == Kern_w2p5::kId || k == Kern_w4p5::kId; }
+static bool aggregate_kernel_ok(int k) { return (k >= 0 && k < kNumKernels) || is_quad_kernel(k); }
+
 static int check_common(const Surface* s, int kernel, const double* pos, const double* sup, int64_t n,
                         const double* pose, const double* obb, const char* who) {
   if (!s) return fail(WSB_ERR_ARG, std::string(who) + ": NULL surface");
-  if (kernel < 0 || kernel >= kNumKernels) return fail(WSB_ERR_UNSUPPORTED, std::string(who) + ": unknown kernel id");
+  if (!aggregate_kernel_ok(kernel)) return fail(WSB_ERR_UNSUPPORTED, std::string(who) + ": unknown kernel id");
   if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, std::string(who) + ": row count out of range");
   if (n > 0 && (!pos || !sup || !pose || !obb)) return fail(WSB_ERR_ARG, std::string(who) + ": NULL array");
   return WSB_OK;
@@ -879,7 +920,7 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
                                       void* stream) {
   const Surface* s = reinterpret_cast<const Surface*>(s_);
   if (!s) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: NULL surface");
-  if (kernel < 0 || kernel >= kNumKernels) return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate: unknown kernel id");
+  if (!aggregate_kernel_ok(kernel)) return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate: unknown kernel id");
   if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate: unknown precision mode");
   if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: row count out of range");
@@ -902,14 +943,21 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   o.cov[0] = C;
   o.m1[0] = M1;
   o.m2[0] = M2;
-  int rc = dispatch_kernel(kernel, [&](auto kt) {
+  auto launch1 = [&](auto kt) {
     using P1 = KPack<decltype(kt)>;
     if (precision == WSB_PREC_MIXED)
       launch_pack<P1, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
     else
       launch_pack<P1, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
     return 0;
-  });
+  };
+  int rc = 0;
+  if (kernel == Kern_w2p5::kId)
+    rc = launch1(Kern_w2p5{});
+  else if (kernel == Kern_w4p5::kId)
+    rc = launch1(Kern_w4p5{});
+  else
+    rc = dispatch_kernel(kernel, launch1);
   if (rc) return rc;
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
@@ -945,7 +993,7 @@ extern "C" int wsb_aggregate_evaluate_groups(const wsb_surface* s_, int n_groups
     return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate_groups: 1 to " + std::to_string(WSB_MAX_GROUPS) +
                                  " kernel groups expected");
   for (int g = 0; g < n_groups; ++g)
-    if (kernels[g] < 0 || kernels[g] >= kNumKernels)
+    if (!aggregate_kernel_ok(kernels[g]))
       return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate_groups: unknown kernel id");
   if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate_groups: unknown precision mode");
@@ -1028,7 +1076,7 @@ extern "C" int wsb_aggregate_groups(const wsb_surface* s_, int n_groups, const i
   if (n_groups < 1 || n_groups > WSB_MAX_GROUPS || !kernels)
     return fail(WSB_ERR_ARG, "wsb_aggregate_groups: 1 to " + std::to_string(WSB_MAX_GROUPS) + " kernel groups expected");
   for (int g = 0; g < n_groups; ++g)
-    if (kernels[g] < 0 || kernels[g] >= kNumKernels)
+    if (!aggregate_kernel_ok(kernels[g]))
       return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_groups: unknown kernel id");
   if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_groups: unknown precision mode");
@@ -1047,6 +1095,8 @@ extern "C" int wsb_aggregate_backward(const wsb_surface* s_, int kernel, const d
   const Surface* s = reinterpret_cast<const Surface*>(s_);
   int rc = check_common(s, kernel, pos, sup, n, pose, obb, "wsb_aggregate_backward");
   if (rc) return rc;
+  if (is_quad_kernel(kernel))
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_backward: the quadrature (tensile) kernels have no adjoint");
   if (n == 0) return WSB_OK;
   if (!d_pos) return fail(WSB_ERR_ARG, "wsb_aggregate_backward: d_pos is NULL");
   const Workspace w = carve(s, n, workspace);

@@ -41,6 +41,10 @@ from typing import Dict, List, Tuple
 KERNEL_IDS = {"cubic": 0, "w2": 1, "w4": 2, "w6": 3, "quartic": 4, "quintic": 5, "poly6": 6, "cone": 7, "lw2": 8,
               "lw4": 9}
 KERNEL_NAMES = {v: k for k, v in KERNEL_IDS.items()}
+# the powered kernels W^5 of the Wendland C2 / C4 shapes (the tensile group of the delta+ layout): degree 25 / 40 in r,
+# evaluated by a graded Gauss-Legendre quadrature along the chord instead of the monomial closed form
+QUAD_KERNEL_IDS = {"w2p5": 10, "w4p5": 11}
+QUAD_GAUSS = 24
 
 # published 2-D normalisations C2 * pi (src/warpSPHBoundaries/curvbound/kernels.py:5-13,
 # src/warpSPHBoundaries/edge/kernels.py:183-185); only used to check the recomputed ones
@@ -366,6 +370,7 @@ def emit_header() -> str:
         out.append(f"// ---- {name}: C2*pi = {k.c2pi}, plane second moment {k.plane2}")
         out.append(f"struct Kern_{name} {{")
         out.append(f"  static constexpr int kId = {kid};")
+        out.append("  static constexpr bool kQuad = false;")
         out.append(f"  static constexpr int kBlocks = {len(k.blocks)};")
         out.append(f"  static constexpr double kMass = {_lit(k.mass)};")
         out.append(f"  static constexpr double kPlane2 = {_lit(k.plane2)};")
@@ -428,12 +433,90 @@ def emit_header() -> str:
     out.append("static const double kPlanCc[kPlanCoeffs] = {" + ", ".join(_lit(x) for x in CC) + "};")
     out.append("static const double kPlanRadii[kPlanNumRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
     out.append("")
+    out.extend(emit_quad())
     out.extend(emit_radial())
     out.extend(emit_mesh())
     out.extend(emit_triangle())
     out.append("}  // namespace wsb")
     out.append("")
     return "\n".join(out)
+
+
+# the Wendland C2 / C4 shapes in u = 1 - q (src/warpSPHBoundaries/edge/kernels.py:217-219): u^p0 B(u)
+_POWER_FAMILIES = {"w2": (4, [F(5), F(-4)]), "w4": (6, [F(56, 3), F(-88, 3), F(35, 3)])}
+
+
+@lru_cache(maxsize=None)
+def quad_kernel(name: str):
+    """(C2*pi, p, B) of a powered kernel: `w2p5` / `w4p5` = the 5th power of the Wendland C2 / C4 shape
+    (src/warpSPHBoundaries/edge/kernels.py:214-232, registered by scene/tensile.py:40-47), pi*W = C u^p B(u)^5 with
+    u = 1 - r, p = 5 p0, B the family's base in u; normalised by the rule C = 1 / (2 int_0^1 r shape dr) of
+    edge/kernels.py:141-156.  Every factor is positive on r <= 1, so the factored form is accurate to a few ulp where
+    the monomial expansion (coefficients up to ~1e13 for w4p5) cancels."""
+    if name not in QUAD_KERNEL_IDS:
+        raise KeyError(f"unknown powered kernel {name!r}; expected one of {sorted(QUAD_KERNEL_IDS)}")
+    fam = name[:2]
+    p0, base = _POWER_FAMILIES[fam]
+    (lo, hi, shape), = _pieces(fam)
+    # the u-form equals the q-form of the smoothing kernel's shape: u^p0 B(u) expanded in q
+    u = [F(1), F(-1)]
+    bq = [F(0)]
+    for k, c in enumerate(base):
+        bq = _padd(bq, [c * x for x in _ppow(u, k)])
+    if _trim(_pmul(_ppow(u, p0), bq)) != _trim(list(shape)):
+        raise AssertionError(f"{fam}: the u-form of the shape differs from its q-form")
+    s5 = _ppow(shape, 5)
+    C = 1 / (2 * _shape_integral([(F(0), F(1), s5)]))
+    return C, 5 * p0, tuple(base)
+
+
+def pi_w_quad(name, r: F) -> F:
+    """exact pi * W(r) of a powered kernel (h = 1, r <= 1; tests)."""
+    C, p, base = quad_kernel(name)
+    u = 1 - r
+    return C * u ** p * sum(c * u ** k for k, c in enumerate(base)) ** 5
+
+
+def emit_quad() -> list:
+    """the powered kernels as quadrature kernels: pi*W(r) in the factored form, and the Gauss-Legendre rule of the
+    chord panels."""
+    import numpy as np
+    gx, gw = np.polynomial.legendre.leggauss(QUAD_GAUSS)
+    out = ["// x^N by squaring",
+           "template <int N>",
+           "__host__ __device__ __forceinline__ double qpow(double x) {",
+           "  if constexpr (N == 0) {",
+           "    return 1.0;",
+           "  } else if constexpr (N % 2 == 0) {",
+           "    const double y = qpow<N / 2>(x);",
+           "    return y * y;",
+           "  } else {",
+           "    return x * qpow<N - 1>(x);",
+           "  }",
+           "}",
+           f"constexpr int kQuadGauss = {QUAD_GAUSS};",
+           "static __device__ const double kQuadGx[kQuadGauss] = {" + ", ".join(repr(float(x)) for x in gx) + "};",
+           "static __device__ const double kQuadGw[kQuadGauss] = {" + ", ".join(repr(float(x)) for x in gw) + "};", ""]
+    for name, kid in sorted(QUAD_KERNEL_IDS.items(), key=lambda t: t[1]):
+        C, p, base = quad_kernel(name)
+        out.append(f"// ---- {name}: C2*pi = {C}; pi*W = C u^{p} B(u)^5, u = 1 - r, on r <= 1")
+        out.append(f"struct Kern_{name} {{")
+        out.append(f"  static constexpr int kId = {kid};")
+        out.append("  static constexpr bool kQuad = true;")
+        out.append("  static constexpr int kBlocks = 1;")
+        out.append("  static constexpr double kR[kBlocks] = {1.0};")
+        out.append("  static constexpr int kNA[kBlocks] = {1};")
+        out.append("  static constexpr double kMass = 1.0;")
+        out.append("  static constexpr double kPlane2 = 0.0;")
+        out.append("  __host__ __device__ static __forceinline__ double poly(double r) {")
+        out.append("    const double u = 1.0 - r;")
+        out.append(f"    const double b = {_horner(list(base), 'u')};")
+        out.append("    const double b2 = b * b;")
+        out.append(f"    return {_lit(C)} * qpow<{p}>(u) * (b2 * b2 * b);")
+        out.append("  }")
+        out.append("};")
+        out.append("")
+    return out
 
 
 def plane_channels(name):

@@ -15,9 +15,10 @@ Routes:
          interpreter (wsb_slot_channels_plain) writing c[N*K, 12], and the per-row contraction (wsb_contract).
 
 Kernel groups: the smoothing kernels (cubic, w2, w4, w6, quartic, quintic, poly6) and the wall-operator kernels of the
-delta+ layout, `cone` (its G is the free-surface cover vector) and `lw2` / `lw4` (W'/r; the `lap` output kind is
-2 lam - tr Cov, the wall Laplacian before the scheme's factor).  The tensile group (`w2p5` / `w4p5`), and with it the
-full delta+ layout, and `cone_area` / `dir_extreme` raise NotImplementedError; they never return zeros.
+delta+ layout: `cone` (its G is the free-surface cover vector), `lw2` / `lw4` (W'/r; the `lap` output kind is
+2 lam - tr Cov, the wall Laplacian before the scheme's factor) and the tensile `w2p5` / `w4p5` (W^5, degree 25 / 40,
+by chord quadrature on the fused route; their groups serve G only).  `cone_area` / `dir_extreme` raise
+NotImplementedError; they never return zeros.
 """
 from dataclasses import dataclass
 from typing import Optional, Protocol, runtime_checkable
@@ -27,7 +28,9 @@ import torch
 from . import _lib
 from ._lib import check, lib, ptr
 from .fixedadj import body_candidates, fixed_adjacency
-from .kernels import KERNEL_IDS
+from .kernels import KERNEL_IDS, QUAD_KERNEL_IDS
+
+_GROUP_IDS = {**KERNEL_IDS, **QUAD_KERNEL_IDS}     # every kernel a FusedWall group may name
 from .scene import Scene, SurfaceRep, _stream
 from .shim import (GradientScheme, KernelFunctions, OperationDirection, OperationProperties, WarpOperation, kernelName,
                    queryAllowed)
@@ -86,9 +89,10 @@ class FusedWall(WallAggregate):
         self.N = N = len(pos)
         B = len(scene.bodies)
         for g in self.groups:
-            if g.kernel not in KERNEL_IDS:
-                raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} is not built (the tensile "
-                                          f"groups w2p5 / w4p5 of the delta+ layout among them)")
+            if g.kernel not in _GROUP_IDS:
+                raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} is not built")
+            if g.kernel in QUAD_KERNEL_IDS and route != "fused":
+                raise NotImplementedError(f"FusedWall: the tensile group {g.kernel!r} runs on the fused route only")
         sig = (route,) + tuple(id(r) for b in scene.bodies for r in b.reps)
         if getattr(scene, "_wsb_checked", None) != sig:
             for b in scene.bodies:
@@ -114,7 +118,7 @@ class FusedWall(WallAggregate):
                        "m1": alloc((B, N, 2), dtype=F64, device=self.dev),
                        "m2": alloc((B, N, 2, 2), dtype=F64, device=self.dev)}
             self.res.append(out)
-        kids = [KERNEL_IDS[g.kernel] for g in self.groups]
+        kids = [_GROUP_IDS[g.kernel] for g in self.groups]
         if route == "fused":
             self._fused(pos, sup, allowed, kids, self.res)
         elif route == "plain":
@@ -216,6 +220,9 @@ class FusedWall(WallAggregate):
             if o.kind not in KINDS:
                 raise ValueError(f"unknown output kind {o.kind!r}")
             r = self.res[o.group]
+            if self.groups[o.group].kernel in QUAD_KERNEL_IDS and o.kind != "g0":
+                raise ValueError(f"FusedWall.evaluate: the tensile group {self.groups[o.group].kernel!r} serves 'g0' "
+                                 f"only")
             if o.kind == "lam":
                 res[o.name] = r["lam"]
             elif o.kind == "g0":
@@ -301,25 +308,41 @@ class AnalyticBoundary:
                                    operationMode=OperationDirection.BoundaryToFluid)
 
     def layout(self, kernel, laplacian, fixedAdjacency=True):
-        """the delta+ layout (kernel, cone, [lw], wp5) of provider.py:73-87: its tensile group (w2p5 / w4p5) is not
-        built, so the layout is refused; the cover vector ('cone') and the wall Laplacian ('lw2' / 'lw4') groups are
-        available to FusedWall directly."""
-        self.family(kernel)
-        raise NotImplementedError("AnalyticBoundary.layout: the delta+ tensile group (w2p5 / w4p5) is not built; "
-                                  "call aggregate(..., lean=True), or FusedWall with the cone / lw2 / lw4 groups")
+        """(groups, roles) of the delta+ layout (provider.py:73-87): the scheme kernel ('w'), the cover vector's cone
+        kernel ('cone', G only), the wall Laplacian's W'/r kernel ('lap', when `laplacian`) and the tensile W^5 kernel
+        ('tens', G only); built once per configuration."""
+        key = (kernel, bool(laplacian), bool(fixedAdjacency))
+        if key not in self._layouts:
+            fam = self.family(kernel)
+            groups, idx = [FusedGroup(kernelName(kernel)), FusedGroup("cone", (3, 4))], {"w": 0, "cone": 1}
+            if laplacian:
+                idx["lap"] = len(groups)
+                groups.append(FusedGroup("l" + fam))
+            idx["tens"] = len(groups)
+            groups.append(FusedGroup(fam + "p5", (3, 4)))
+            self._layouts[key] = (tuple(groups), idx)
+        return self._layouts[key]
 
     def aggregate(self, ps, support, kernel=KernelFunctions.Wendland2, laplacian=False, fixedAdjacency=True,
                   lean=False):
         """the wall evaluation at the positions of `ps` (provider.py:89-110): `.out` holds lam, G, Cov per body;
-        `evaluate` serves m1, m2 and a1g1 as well.  `support`: host float >= every support of `ps`."""
-        if not lean:
-            self.layout(kernel, laplacian, fixedAdjacency)
-        groups = (FusedGroup(kernelName(kernel)),)
+        `evaluate` serves m1, m2 and a1g1 as well; without `lean` the delta+ layout adds cover, lap (when `laplacian`)
+        and tens, raw (the scheme applies its factors).  `support`: host float >= every support of `ps`."""
+        if lean:
+            groups, idx = (FusedGroup(kernelName(kernel)),), {"w": 0}
+        else:
+            groups, idx = self.layout(kernel, laplacian, fixedAdjacency)
         allowed = None
         if getattr(ps, "kinds", None) is not None:      # without kinds every query is served: no mask, no host read
             allowed = queryAllowed(ps, self.properties(kernel).operationMode, self.scene.device)
         fw = FusedWall(self.scene, ps, support, groups, route=self.route, precision=self.precision, allowed=allowed)
-        fw.out = fw.evaluate([WallOutput("lam", 0, "lam"), WallOutput("G", 0, "g0"), WallOutput("Cov", 0, "cov")])
+        outs = [WallOutput("lam", 0, "lam"), WallOutput("G", 0, "g0"), WallOutput("Cov", 0, "cov")]
+        if not lean:
+            outs.append(WallOutput("cover", idx["cone"], "g0"))
+            if "lap" in idx:
+                outs.append(WallOutput("lap", idx["lap"], "lap"))
+            outs.append(WallOutput("tens", idx["tens"], "g0"))
+        fw.out = fw.evaluate(outs)
         return fw
 
     def signed_distance(self, x, body=None, supportMax=None, want_body=False):
