@@ -16,6 +16,7 @@ restatement of the reference's numpy path) over a bounded particle sample, all c
 """
 import argparse
 import json
+import math
 import os
 
 # expandable segments: the serving stream allocates buffers of widely varying sizes on several streams; without them
@@ -325,6 +326,53 @@ def radial_run(dev, stream, flush, n=1 << 21, steps=10, kernel="w4"):
             "bytes_per_row": 6 * 8 + 28 * 8, "shell_fraction": shell, "kernel": "k_radial"}
 
 
+def detector_run(ns, pos, sup, pose, obb, ws, need, pairs, stream, flush, steps=5):
+    """the delta+ detector inputs on the c2 rows (2^20 particles, h = 0.02, 64 star polygons): wsb_cone_area (half
+    angle pi/3, seeded axes) and wsb_dir_extreme (the same vectors) on the workspace prepared once for the c2
+    particles, float64, inputs resident; CUDA events around each call, L2 flushed before each."""
+    import ctypes
+
+    import torch
+    from warpsphboundaries_b200 import _lib
+    n = len(pos)
+    gen = torch.Generator(device=pos.device).manual_seed(3)
+    axes = torch.randn((n, 2), dtype=torch.float64, device=pos.device, generator=gen)
+    area = torch.zeros(2 * n, dtype=torch.float64, device=pos.device)
+    dmax = torch.zeros(n, dtype=torch.float64, device=pos.device)
+    st = ctypes.c_void_p(stream.cuda_stream)
+    p = _lib.ptr
+    _lib.check(_lib.lib.wsb_aggregate_prepare(ns.handle, p(pos), p(sup), None, n, p(pose), obb, 0, p(ws), need, st),
+               "wsb_aggregate_prepare")
+
+    def cone():
+        _lib.check(_lib.lib.wsb_cone_area(ns.handle, p(sup), n, p(pose), p(axes), math.pi / 3, p(area), p(ws), need,
+                                          st), "wsb_cone_area")
+
+    def dirx():
+        _lib.check(_lib.lib.wsb_dir_extreme(ns.handle, n, p(pose), p(axes), p(dmax), p(ws), need, st),
+                   "wsb_dir_extreme")
+
+    res = {}
+    for name, fn in (("cone_area", cone), ("dir_extreme", dirx)):
+        for _ in range(3):
+            fn()
+        tot = 0.0
+        for _ in range(steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        ms = tot / steps
+        res[name] = {"ms": ms, "rows_per_s": n / (ms * 1e-3), "pairs_per_s": pairs / (ms * 1e-3)}
+    return {"workload": "c2 rows (2^20 particles, h=0.02, 64 star polygons), prepared once; cone_area half angle "
+                        "pi/3; f64", "pairs": pairs, **res, "kernels": ["k_cone_area", "k_dir_extreme"]}
+
+
 def mesh_run(dev, stream, flush, steps=5, kernel="w4", n_particles=1 << 21):
     """the 3-D scene: 2^21 particles uniform in [-1, 1]^3, h = 0.03, a jittered icosphere of 20480 faces (radius 0.6),
     the 28 baseline channels of every particle, float64, inputs resident; CUDA events around wsb_mesh_channels."""
@@ -631,6 +679,7 @@ def our_arm(args):
                "sequential": {"value": job_pairs_step * args.steps / (seq * 1e-3), "ms_per_step": seq / args.steps}}
 
     radial = radial_run(dev, stream, flush) if world == 1 else None
+    detector = detector_run(ns, pos, sup, pose, obb, ws, need, P, stream, flush) if world == 1 else None
     mesh = mesh_run(dev, stream, flush, n_particles=args.mesh_particles) if world == 1 and not args.no_mesh else None
 
     serving = None
@@ -660,6 +709,7 @@ def our_arm(args):
                 "kernel_ms_separate": sep_ms,
                 "gpu_launches": args.steps * (5 + 1),   # prepare: 5 kernels; one pair kernel for the four groups
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh, "adjoint": adjoint,
+                "detector": detector,
                 **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)
     if world > 1:

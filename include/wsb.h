@@ -152,6 +152,25 @@ int wsb_aggregate_groups(const wsb_surface* s, int n_groups, const int32_t* kern
                          double* const* m1, double* const* m2, void* workspace, size_t workspace_bytes,
                          void* stream);
 
+/* Two detector inputs of the delta+ scheme on a workspace that wsb_aggregate_prepare filled for this surface, pose
+ * and position set (they visit the same neighbour edges as the channel pass, |x - seg| < sup of the row; float64).
+ *
+ * wsb_cone_area ADDS, per row i, the area of (solid cap disk(x_i, sup_i) cap wedge(x_i, axis_i, half_angle)) into area[i]
+ * and the full-disk area of the solid into area[n + i] (area [2n], units length^2; half_angle >= pi = the full disk).
+ * axes [n*2] are world vectors (only their direction matters).  A row outside the broadphase of a surface whose solid
+ * is the unbounded outside (background 1) adds the whole sector.  half_angle must be finite and >= 0 (WSB_ERR_ARG).
+ * Replaces FusedWall.cone_area's polygon launch and its background term (src/warpSPHBoundaries/scene/fused.py:180-246
+ * _cone_area_kernel, :799-835 cone_area); the per-edge closed form it evaluates locally is scene/cone_area.py:20-60.
+ *
+ * wsb_dir_extreme max-accumulates, per row i, into out[i] the largest |cos| between the world vector vecs[i] (vecs
+ * [n*2]) and a direction from x_i to a point of the solid within sup_i: 1 where the line of the vector meets the solid
+ * there (a row inside the solid: 1), 0 for a zero vector or no solid in support.  Replaces FusedWall.dir_extreme's
+ * polygon launch and its background rule (fused.py:248-308 _dir_extreme_kernel, :741-797 dir_extreme). */
+int wsb_cone_area(const wsb_surface* s, const double* sup, int64_t n, const double* pose, const double* axes,
+                  double half_angle, double* area, const void* workspace, size_t workspace_bytes, void* stream);
+int wsb_dir_extreme(const wsb_surface* s, int64_t n, const double* pose, const double* vecs, double* out,
+                    const void* workspace, size_t workspace_bytes, void* stream);
+
 /* wsb_aggregate without a caller workspace, for hosts that cannot allocate device memory for this library (their
  * allocator owns the GPU's memory, or their step loop may not call cudaMalloc / cudaFree, which synchronise the
  * device).  No counterpart in the reference: it exists for such C-ABI callers.  The scratch is a static 16 MiB device

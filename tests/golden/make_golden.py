@@ -19,6 +19,9 @@ Writes
   triangle_golden.json        conditioned single triangles (2-D): the reference's adversarial triangle cases (tiny, needle
                               angles, slivers; validation/adversarial.py polygon_cases) at its deterministic probes, with
                               the twelve channels (w4) of its 70-digit analytic reference (precision_polygon_reference)
+  cone_area_golden.json       the area of solid cap disk(x, H) cap wedge from the reference's vectorised per-edge closed form
+                              (scene/cone_area.py): an L-shape, a thin bar and a tank (background), H 0.5 and 0.23,
+                              half angles pi/6, pi/3, 2 and pi
   mesh3d_golden.json          closed triangle surfaces, 3-D: the 28 baseline channels (value moments |alpha| <= 2,
                               kernel-gradient moments |alpha| <= 1, kernel Hessian) from the reference's exact
                               face-to-edge reductions in mpmath (mesh3d/reference.py ClosedSurface), 40 digits, for an
@@ -29,6 +32,7 @@ The reference package is imported with a stub parent package because its
 here do not.
 """
 import importlib
+import math
 import json
 import sys
 import types
@@ -341,6 +345,46 @@ def wall_kernel_golden(root, dps=40):
     print("edge2d_wall_kernels.json:", len(out["cases"]), "cases")
 
 
+def _cone_reps():
+    """three body-frame polygons (solid on the left): an L-shape with a reflex corner, a thin bar and a tank (the
+    clockwise outline of a box, background 1: the solid is the outside)."""
+    L = np.array([[0.0, 0.0], [2.0, 0.0], [2.0, 0.6], [0.7, 0.6], [0.7, 1.8], [0.0, 1.8]])
+    bar = np.array([[-0.6, -0.05], [0.6, -0.05], [0.6, 0.05], [-0.6, 0.05]])
+    tank = np.array([[-1.0, -0.8], [-1.0, 2.6], [3.1, 2.6], [3.1, -0.8]])
+    out = []
+    for P, bg in ((L, 0), (bar, 0), (tank, 1)):
+        n = len(P)
+        out.append((P, np.stack([np.arange(n), (np.arange(n) + 1) % n], 1), bg))
+    return out
+
+
+def cone_area_golden(root, n=160, seed=11):
+    """cone_area_golden.json: the reference's own vectorised closed form (scene/cone_area.py `cone_area`, float64
+    torch on the CPU) for the three polygons of _cone_reps, seeded points inside / near / far and random axes, at
+    H = 0.5 and H = 0.23 and half angles pi/6, pi/3, 2, pi (the full disk)."""
+    import importlib.util
+    import torch
+    spec = importlib.util.spec_from_file_location(
+        "ref_cone_area", str(Path(root) / "src" / "warpSPHBoundaries" / "scene" / "cone_area.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    rng = np.random.default_rng(seed)
+    reps, cases = [], []
+    for ri, (V, E, bg) in enumerate(_cone_reps()):
+        lo, hi = V.min(0) - 0.6, V.max(0) + 0.6
+        pts = rng.uniform(lo, hi, (n, 2))
+        axes = rng.normal(size=(n, 2))
+        reps.append({"vertices": V.tolist(), "edges": E.tolist(), "background": bg, "points": pts.tolist(),
+                     "axes": axes.tolist()})
+        for H in (0.5, 0.23):
+            for al in (math.pi / 6, math.pi / 3, 2.0, math.pi):
+                val = mod.cone_area(torch.tensor(pts), torch.tensor(axes), al, H, torch.tensor(V), torch.tensor(E), bg)
+                cases.append({"rep": ri, "H": H, "half_angle": al, "value": val.numpy().tolist()})
+    with open(HERE / "cone_area_golden.json", "w") as fh:
+        json.dump({"source": "src/warpSPHBoundaries/scene/cone_area.py cone_area (float64, CPU)", "reps": reps,
+                   "cases": cases}, fh)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     np2d, torch2d = load_reference(root)
@@ -351,3 +395,4 @@ if __name__ == "__main__":
     mesh3d_golden(root)
     triangle_golden(root)
     wall_kernel_golden(root)
+    cone_area_golden(root)

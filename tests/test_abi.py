@@ -57,3 +57,10 @@ def test_grouped_aggregate_checks_its_arguments_without_a_device():
     rc = _lib.lib.wsb_aggregate_groups(None, 1, _lib.int32s([2]), _lib.PREC_FP64, None, None, None, 4, None, None, 0,
                                        _lib.OUT_ALL, *none5, None, 0, None)
     assert rc == _lib.WSB_ERR_ARG
+
+
+def test_detector_inputs_check_their_arguments_without_a_device():
+    """wsb_cone_area / wsb_dir_extreme refuse a NULL surface before touching a device."""
+    from warpsphboundaries_b200 import _lib
+    assert _lib.lib.wsb_cone_area(None, None, 4, None, None, 0.5, None, None, 0, None) == _lib.WSB_ERR_ARG
+    assert _lib.lib.wsb_dir_extreme(None, 4, None, None, None, None, 0, None) == _lib.WSB_ERR_ARG

@@ -122,8 +122,8 @@ def test_routes_agree_and_error_paths():
     assert set(dp.out) == {"lam", "G", "Cov", "cover", "tens"}
     with pytest.raises(NotImplementedError):
         AnalyticBoundary(scene).aggregate(ps, h, kernel=KernelFunctions.Wendland6)          # C2 / C4 only
-    with pytest.raises(NotImplementedError):
-        fused.cone_area(torch.zeros((len(X), 2), device=DEV), 0.5)
+    ax = torch.tensor(np.random.default_rng(8).normal(size=(len(X), 2)), device=DEV)
+    assert torch.equal(fused.cone_area(ax, 0.5), plain.cone_area(ax, 0.5))   # one detector path for both routes
     with pytest.raises(ValueError):
         fused.evaluate([WallOutput("L", 0, "lap")])                  # 'lap' needs an lw2 / lw4 group
     with pytest.raises(NotImplementedError):

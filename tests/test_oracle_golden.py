@@ -146,3 +146,55 @@ def test_oracle_tensile_gradient_matches_golden(case):
         for a, b in zip(got, ref):
             b = float(b)
             assert abs(a - b) <= 1e-11 * (1 + abs(b)), (case["id"], k, a, b)
+
+
+# ------------------------------------------------------------------------------------------------ detector inputs
+CONE = json.loads((G / "cone_area_golden.json").read_text())
+
+
+@pytest.mark.parametrize("case", range(len(CONE["cases"])))
+def test_cone_area_oracle_matches_the_reference_closed_form(case):
+    """oracle/cone_area.py against the reference's own vectorised closed form (scene/cone_area.py) on the golden
+    points: the same per-edge formula in float64, so the tolerance is round-off, 1e-13 H^2."""
+    from oracle import cone_area as C
+    c = CONE["cases"][case]
+    r = CONE["reps"][c["rep"]]
+    got = C.cone_area(r["points"], r["axes"], c["half_angle"], c["H"], r["vertices"], r["edges"], r["background"])
+    assert np.abs(got - np.array(c["value"])).max() <= 1e-13 * c["H"] ** 2
+    assert (np.array(c["value"]) > 1e-3 * c["H"] ** 2).sum() > 10          # the points do see the solid
+
+
+def test_cone_area_oracle_additivity_and_bounds():
+    """two complementary wedges (axis a, half angle al; axis -a, half angle pi - al) tile the disk, so their areas
+    sum to the full-disk area; 0 <= wedge area <= full area <= pi H^2 (round-off 1e-13 H^2)."""
+    from oracle import cone_area as C
+    H = 0.5
+    for r in CONE["reps"]:
+        p, a = np.array(r["points"]), np.array(r["axes"])
+        full = C.cone_area(p, a, np.pi, H, r["vertices"], r["edges"], r["background"])
+        for al in (0.3, 1.0, 2.5):
+            w1 = C.cone_area(p, a, al, H, r["vertices"], r["edges"], r["background"])
+            w2 = C.cone_area(p, -a, np.pi - al, H, r["vertices"], r["edges"], r["background"])
+            assert np.abs(w1 + w2 - full).max() <= 1e-13
+            assert w1.min() >= -1e-13 and (w1 - full).max() <= 1e-13
+        assert full.max() <= np.pi * H * H + 1e-13
+
+
+def test_dir_extreme_local_oracle_matches_the_polar_grid():
+    """the closed-form direction extreme (oracle/cone_area.dir_extreme_local) against the reference test's polar
+    grid oracle with even-odd membership (tests/scene/test_fused_wall.py:207-226): never below it, within its
+    angular resolution (the reference's tolerance 1.5e-2), both near and far points present, a zero vector gives 0."""
+    from oracle import cone_area as C
+    rng = np.random.default_rng(5)
+    H = 0.5
+    for r in CONE["reps"]:
+        V, E, bg = np.array(r["vertices"]), np.array(r["edges"]), r["background"]
+        p = np.array(r["points"])[:40]
+        v = rng.normal(size=(len(p), 2))
+        v[3] = 0.0
+        got = C.dir_extreme_local(p, v, H, V, E, bg)
+        ref = C.dir_extreme_polar(p, v, H, V, E, bg, nr=150, nphi=1440)
+        assert (got >= ref - 1e-9).all(), float((ref - got).max())
+        assert np.abs(got - ref).max() <= 1.5e-2
+        assert got[3] == 0.0
+        assert (got > 0.5).sum() > 3

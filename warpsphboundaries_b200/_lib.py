@@ -20,7 +20,7 @@ EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_d
            "wsb_surface_cells", "wsb_fixed_topology", "wsb_slot_channels_plain", "wsb_contract",
            "wsb_aggregate_workspace_size", "wsb_aggregate", "wsb_aggregate_prepare", "wsb_aggregate_evaluate",
            "wsb_aggregate_evaluate_groups", "wsb_aggregate_groups", "wsb_aggregate_noalloc",
-           "wsb_aggregate_backward", "wsb_signed_distance",
+           "wsb_aggregate_backward", "wsb_cone_area", "wsb_dir_extreme", "wsb_signed_distance",
            "wsb_kinematics", "wsb_radial_channels", "wsb_mesh_create", "wsb_mesh_destroy",
            "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels", "wsb_triangle_channels",
            "wsb_triangle_combine"]
@@ -61,6 +61,8 @@ def _load():
         "wsb_aggregate_noalloc": (c_int, [P, c_int, c_int, P, P, P, c_int64, P, D, c_int, c_int, P, P, P, P, P, P,
                                           P]),
         "wsb_aggregate_backward": (c_int, [P, c_int, P, P, P, c_int64, P, D, c_int, P, P, P, P, P, P, c_size_t, P]),
+        "wsb_cone_area": (c_int, [P, P, c_int64, P, P, c_double, P, P, c_size_t, P]),
+        "wsb_dir_extreme": (c_int, [P, c_int64, P, P, P, P, c_size_t, P]),
         "wsb_signed_distance": (c_int, [P, P, c_int64, c_double, P, P, P, P, P]),
         "wsb_kinematics": (c_int, [P, c_int32, P, c_int64, P, P, P, P, P]),
         "wsb_radial_channels": (c_int, [c_int, c_int, c_int, P, P, P, P, c_int64, I32P, c_int, P, P, P, P]),

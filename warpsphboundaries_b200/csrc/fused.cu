@@ -2,6 +2,7 @@
 // body-frame position, runs the float64 neighbour predicate over the row's cell and accumulates the closed-form
 // channels of every neighbour pair in registers, then adds the indicator, scales and rotates.  Also the adjoint of the
 // moments, signed distance and rigid-body kinematics.
+#include <cmath>
 #include <cstddef>
 #include <cstdlib>
 #include <mutex>
@@ -856,6 +857,189 @@ __global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int6
   }
 }
 
+// ------------------------------------------------------------------------------------------------ cone area, direction
+// Two detector inputs of the delta+ scheme over the prepared rows (src/warpSPHBoundaries/scene/fused.py:155-308,
+// 741-835): the area of the solid inside the support disk and a wedge about a per-row axis, and the largest |cos|
+// between a per-row vector and the directions from the row to the solid within its support.  Both visit the same
+// neighbour edges as the channel pass (the float64 predicate |x - seg| < h over the row's cell candidates), one thread
+// per work row, in float64.
+
+// a - 2 pi round((a + pi) / 2 pi - 1/2): the angle in [-pi, pi)
+__device__ __forceinline__ double wrap_pi(double a) {
+  const double r = a + 0.5 * kTwoPi;
+  return r - kTwoPi * floor(r / kTwoPi) - 0.5 * kTwoPi;
+}
+
+// every neighbour edge of a work row, in candidate order: the candidates the row's mask marks, then those past the
+// mask that pass the predicate
+template <class F>
+__device__ __forceinline__ void for_each_neighbour(const SurfView& S, const WorkRec& r, F&& f) {
+  uint64_t m0 = r.m0, m1 = r.m1;
+  for (int b = pop_bit(m0, m1); b >= 0; b = pop_bit(m0, m1)) f(ldg4(S.crec + r.kb + b));
+  for (int k = r.kb + kMaskBits; k < r.ke; ++k) {
+    const double4 e = ldg4(S.crec + k);
+    if (seg_within_fast(r.lx, r.ly, e.x, e.y, e.z, e.w, r.h)) f(e);
+  }
+}
+
+// The sector of the support disk that an edge a -> b sweeps about the row, seen through its chord: s = the edge's
+// orientation about the row (+1 counter-clockwise), z = the row's distance to the edge line, [lo, hi] = the swept
+// angles (|hi - lo| < pi), pn = the angle of the foot of the perpendicular (on the branch of lo) and be = acos(z / H),
+// the half-angle under which the chord inside the disk is seen.  False for a degenerate edge, a row on the edge line
+// or an edge line that misses the open disk (scene/cone_area.py:20-40 per edge; fused.py:200-225 in the local form).
+struct ConeEdge {
+  double s, z, lo, hi, pn, be;
+};
+
+__device__ __forceinline__ bool cone_edge(double px, double py, double H, const double4& e, ConeEdge& c) {
+  const double ax = e.x - px, ay = e.y - py, bx = e.z - px, by = e.w - py;
+  const double cr = ax * by - ay * bx;
+  const double dx = bx - ax, dy = by - ay;
+  const double L = sqrt(dx * dx + dy * dy);
+  if (!(L > 0.0) || !(fabs(cr) >= 1e-300)) return false;
+  c.z = fabs(cr) / L;
+  if (!(c.z < H)) return false;
+  c.s = cr < 0.0 ? -1.0 : 1.0;
+  const double pa = atan2(ay, ax);
+  const double dphi = wrap_pi(atan2(by, bx) - pa);
+  c.lo = dphi < 0.0 ? pa + dphi : pa;
+  c.hi = dphi < 0.0 ? pa : pa + dphi;
+  const double ux = dx / L, uy = dy / L, t = ax * ux + ay * uy;
+  c.pn = c.lo + wrap_pi(atan2(ay - t * uy, ax - t * ux) - c.lo);
+  c.be = acos(c.z / H);
+  return true;
+}
+
+// What the chord removes from the sector 1/2 H^2 (h - l) of the angles [l, h] (inside [lo, hi]): where the edge is
+// nearer than H -- the copy of (pn - be, pn + be) whose centre is nearest the interval's midpoint -- the ray ends on
+// the edge at z / cos(phi - pn), so the sector 1/2 H^2 dphi gives way to the triangle 1/2 z^2 d tan(phi - pn).
+__device__ __forceinline__ double chord_deficit(double l, double h, const ConeEdge& c, double H) {
+  const double k = floor((0.5 * (l + h) - c.pn) / kTwoPi + 0.5);
+  const double c0 = fmax(l, c.pn + kTwoPi * k - c.be), c1 = fmin(h, c.pn + kTwoPi * k + c.be);
+  if (!(c0 < c1)) return 0.0;
+  return 0.5 * H * H * (c1 - c0) - 0.5 * c.z * c.z * (tan(c1 - c.pn) - tan(c0 - c.pn));
+}
+
+// Per row: area += 1/2 H^2 W ind - sum_e s_e (chord deficit of e inside the wedge) and full += pi H^2 ind - sum_e s_e
+// (chord deficit of e), W = 2 half_angle (2 pi for half_angle >= pi).  The sectors of the edges beyond the disk sum
+// along every ray to the winding indicator, which is why only the neighbour edges enter.  A row outside the
+// broadphase of a surface whose solid is the unbounded outside lies deep in it: the whole sector.  Work blocks first,
+// then tail blocks for the rows without neighbour edges (as the channel pass).
+__global__ void __launch_bounds__(kThreads) k_cone_area(SurfView S, const double* __restrict__ sup,
+                                                       const WorkRec* __restrict__ wrec,
+                                                       const int32_t* __restrict__ nwork_p, int64_t n,
+                                                       const double* __restrict__ ind,
+                                                       const int32_t* __restrict__ flag,
+                                                       const double* __restrict__ pose,
+                                                       const double* __restrict__ axes, double half_angle,
+                                                       double* __restrict__ area) {
+  const int64_t nwork = *nwork_p;
+  const int64_t wblocks = (nwork + kThreads - 1) / kThreads;
+  const bool wedge = half_angle < 0.5 * kTwoPi;
+  const double W = wedge ? 2.0 * half_angle : kTwoPi;
+  if ((int64_t)blockIdx.x >= wblocks) {
+    const int64_t i = ((int64_t)blockIdx.x - wblocks) * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const int32_t f = flag[i];
+    if (f == 2) return;
+    const double w = f == 1 ? ind[i] : S.background;
+    if (w != 0.0) {
+      const double H = sup[i];
+      area[i] += 0.5 * H * H * W * w;
+      area[n + i] += 0.5 * H * H * kTwoPi * w;
+    }
+    return;
+  }
+  const int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (j >= nwork) return;
+  const WorkRec r = load_workrec(wrec + j);
+  const int64_t i = r.row;
+  const double H = r.h;
+  const double ax = axes[2 * i], ay = axes[2 * i + 1], pc = pose[2], ps = pose[3];
+  const double th = atan2(-ps * ax + pc * ay, pc * ax + ps * ay);      // the world axis in the body frame
+  double a_wedge = 0.0, a_full = 0.0;
+  for_each_neighbour(S, r, [&](const double4& e) {
+    ConeEdge c;
+    if (!cone_edge(r.lx, r.ly, H, e, c)) return;
+    a_full += c.s * chord_deficit(c.lo, c.hi, c, H);
+    if (!wedge) return;
+    const double mid = c.lo + wrap_pi(th - c.lo);                     // the wedge centre on the branch of lo
+#pragma unroll
+    for (int k = -1; k <= 1; ++k) {
+      const double l = fmax(c.lo, mid + kTwoPi * k - half_angle), h = fmin(c.hi, mid + kTwoPi * k + half_angle);
+      if (l < h) a_wedge += c.s * chord_deficit(l, h, c, H);
+    }
+  });
+  if (!wedge) a_wedge = a_full;
+  const double w = ind[i];
+  area[i] += 0.5 * H * H * W * w - a_wedge;
+  area[n + i] += 0.5 * H * H * kTwoPi * w - a_full;
+}
+
+// Per row: max |v . x| over the unit directions x from the row to the solid within its support, v the row's world
+// vector in the body frame, normalised; max-accumulated into out[i] (0 for a zero vector or no solid in support).  A
+// row inside the solid sees it in every direction (1).  Otherwise the solid inside the disk is seen under the angular
+// spans of the edge pieces inside it; |cos| peaks where a span contains the line of v (1) or at a span's end (a vertex
+// inside the disk or the edge's crossing of the support circle): fused.py:248-308.
+__device__ __forceinline__ double edge_extreme(double px, double py, double H, const double4& e, double vx,
+                                               double vy) {
+  const double ax = e.x - px, ay = e.y - py, dx = e.z - e.x, dy = e.w - e.y;
+  const double a = dx * dx + dy * dy;
+  if (!(a > 0.0)) return 0.0;
+  const double b = ax * dx + ay * dy;
+  const double disc = b * b - a * (ax * ax + ay * ay - H * H);
+  if (!(disc > 0.0)) return 0.0;
+  const double sq = sqrt(disc);
+  const double t0 = fmax(0.0, (-b - sq) / a), t1 = fmin(1.0, (-b + sq) / a);
+  if (!(t0 < t1)) return 0.0;
+  const double cd = dx * vy - dy * vx;
+  if (fabs(cd) > 0.0) {
+    const double ts = -(ax * vy - ay * vx) / cd;                       // where the line of v crosses the edge
+    if (ts >= t0 && ts <= t1) return 1.0;
+  }
+  double f = 0.0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const double t = k == 0 ? t0 : t1;
+    const double rx = ax + t * dx, ry = ay + t * dy, rr = sqrt(rx * rx + ry * ry);
+    if (rr > 0.0) f = fmax(f, fabs(rx * vx + ry * vy) / rr);
+  }
+  return f;
+}
+
+__global__ void __launch_bounds__(kThreads) k_dir_extreme(SurfView S, const WorkRec* __restrict__ wrec,
+                                                         const int32_t* __restrict__ nwork_p, int64_t n,
+                                                         const double* __restrict__ ind,
+                                                         const int32_t* __restrict__ flag,
+                                                         const double* __restrict__ pose,
+                                                         const double* __restrict__ vecs, double* __restrict__ out) {
+  const int64_t nwork = *nwork_p;
+  const int64_t wblocks = (nwork + kThreads - 1) / kThreads;
+  if ((int64_t)blockIdx.x >= wblocks) {
+    const int64_t i = ((int64_t)blockIdx.x - wblocks) * kThreads + threadIdx.x;
+    if (i >= n) return;
+    const int32_t f = flag[i];
+    if (f == 2) return;
+    const double w = f == 1 ? ind[i] : S.background;
+    if (w > 0.5 && (vecs[2 * i] != 0.0 || vecs[2 * i + 1] != 0.0)) out[i] = 1.0;
+    return;
+  }
+  const int64_t j = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+  if (j >= nwork) return;
+  const WorkRec r = load_workrec(wrec + j);
+  const int64_t i = r.row;
+  const double wx = vecs[2 * i], wy = vecs[2 * i + 1], pc = pose[2], ps = pose[3];
+  double vx = pc * wx + ps * wy, vy = -ps * wx + pc * wy;             // R^T w
+  const double nv = sqrt(vx * vx + vy * vy);
+  if (!(nv > 0.0)) return;
+  vx /= nv;
+  vy /= nv;
+  double best = ind[i] > 0.5 ? 1.0 : 0.0;
+  if (best < 1.0)
+    for_each_neighbour(S, r, [&](const double4& e) { best = fmax(best, edge_extreme(r.lx, r.ly, r.h, e, vx, vy)); });
+  out[i] = fmax(out[i], best);
+}
+
 // shared front half of the aggregate and its adjoint: body frame, broadphase, counting sort of the rows by cell
 static int sort_rows(const Surface* s, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
                      const double* pose, const double* obb, int unbounded, const Workspace& w, cudaStream_t st) {
@@ -1141,6 +1325,55 @@ extern "C" int wsb_kinematics(const double* bodies, int32_t n_bodies, const doub
   const int64_t total = (int64_t)n_bodies * n;
   k_kinematics<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(bodies, n_bodies, x, n, rel, local,
                                                                                   velocity, acceleration);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+// the workspace of a prepared position set, checked against the surface and the row count
+static int prepared(const Surface* s, int64_t n, const void* workspace, size_t workspace_bytes, const char* who,
+                    Workspace* w) {
+  *w = carve(s, n, const_cast<void*>(workspace));
+  if (!workspace || workspace_bytes < w->total)
+    return fail(WSB_ERR_SIZE, std::string(who) + ": workspace of " + std::to_string(workspace_bytes) + " bytes, need " +
+                                  std::to_string(w->total));
+  return WSB_OK;
+}
+
+extern "C" int wsb_cone_area(const wsb_surface* s_, const double* sup, int64_t n, const double* pose,
+                             const double* axes, double half_angle, double* area, const void* workspace,
+                             size_t workspace_bytes, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s) return fail(WSB_ERR_ARG, "wsb_cone_area: NULL surface");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_cone_area: row count out of range");
+  if (!(half_angle >= 0.0) || !std::isfinite(half_angle))
+    return fail(WSB_ERR_ARG, "wsb_cone_area: the half angle must be finite and >= 0");
+  if (n == 0) return WSB_OK;
+  if (!sup || !pose || !axes || !area) return fail(WSB_ERR_ARG, "wsb_cone_area: NULL array");
+  Workspace w;
+  int rc = prepared(s, n, workspace, workspace_bytes, "wsb_cone_area", &w);
+  if (rc) return rc;
+  WSB_CUDA(cudaSetDevice(s->device));
+  const unsigned grid = (unsigned)(2 * ((n + kThreads - 1) / kThreads));   // work blocks (at most n rows), then tails
+  k_cone_area<<<grid, kThreads, 0, (cudaStream_t)stream>>>(view_of(s), sup, w.wrec, w.nwork, n, w.ind, w.flag, pose,
+                                                           axes, half_angle, area);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+extern "C" int wsb_dir_extreme(const wsb_surface* s_, int64_t n, const double* pose, const double* vecs, double* out,
+                               const void* workspace, size_t workspace_bytes, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s) return fail(WSB_ERR_ARG, "wsb_dir_extreme: NULL surface");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_dir_extreme: row count out of range");
+  if (n == 0) return WSB_OK;
+  if (!pose || !vecs || !out) return fail(WSB_ERR_ARG, "wsb_dir_extreme: NULL array");
+  Workspace w;
+  int rc = prepared(s, n, workspace, workspace_bytes, "wsb_dir_extreme", &w);
+  if (rc) return rc;
+  WSB_CUDA(cudaSetDevice(s->device));
+  const unsigned grid = (unsigned)(2 * ((n + kThreads - 1) / kThreads));
+  k_dir_extreme<<<grid, kThreads, 0, (cudaStream_t)stream>>>(view_of(s), w.wrec, w.nwork, n, w.ind, w.flag, pose, vecs,
+                                                             out);
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }

@@ -17,9 +17,11 @@ Routes:
 Kernel groups: the smoothing kernels (cubic, w2, w4, w6, quartic, quintic, poly6) and the wall-operator kernels of the
 delta+ layout: `cone` (its G is the free-surface cover vector), `lw2` / `lw4` (W'/r; the `lap` output kind is
 2 lam - tr Cov, the wall Laplacian before the scheme's factor) and the tensile `w2p5` / `w4p5` (W^5, degree 25 / 40,
-by chord quadrature on the fused route; their groups serve G only).  `cone_area` / `dir_extreme` raise
-NotImplementedError; they never return zeros.
+by chord quadrature on the fused route; their groups serve G only).  `cone_area` (the wedge and full-disk areas of
+the solid in the support) and `dir_extreme` (the largest direction cosine towards the solid) run on the prepared rows of
+every (body, surface): wsb_cone_area / wsb_dir_extreme.
 """
+import math
 from dataclasses import dataclass
 from typing import Optional, Protocol, runtime_checkable
 
@@ -87,6 +89,8 @@ class FusedWall(WallAggregate):
         pos = ps.positions.to(self.dev, F64).contiguous()
         sup = ps.supports.to(self.dev, F64).contiguous()
         self.N = N = len(pos)
+        self._pos, self._sup = pos, sup         # the position set cone_area / dir_extreme prepare again
+        self._allowed = None if allowed is None else allowed.to(self.dev, torch.int32).contiguous()
         B = len(scene.bodies)
         for g in self.groups:
             if g.kernel not in _GROUP_IDS:
@@ -269,11 +273,60 @@ class FusedWall(WallAggregate):
     def reset_derived(self):
         """no lazily derived buffers exist in this implementation (fused.py:721-725)."""
 
+    def _surfaces(self):
+        """(body index, native surface, workspace, bytes, pose) of every (body, surface), each workspace prepared for
+        this position set (wsb_aggregate_prepare: body frame, broadphase, neighbour masks, indicator)."""
+        N = self.N
+        for bi, body in enumerate(self.scene.bodies):
+            if not body.reps:
+                continue
+            pose = body.pose_tensor(self.dev)
+            obb = (_lib.ctypes.c_double * 4)(*body.obb())
+            for rep in body.reps:
+                ns = rep.native(self.support, self.dev)
+                if self.workspaces is not None:
+                    ws = self.workspaces[id(rep)]
+                    need = ws.numel()
+                else:
+                    ws, need = ns.workspace(N)
+                check(lib.wsb_aggregate_prepare(ns.handle, ptr(self._pos), ptr(self._sup), ptr(self._allowed), N,
+                                                ptr(pose), obb, int(body.unbounded()), ptr(ws), need, _stream()),
+                      "wsb_aggregate_prepare")
+                yield bi, ns, ws, need, pose
+
     def cone_area(self, axes, half_angle):
-        raise NotImplementedError("FusedWall.cone_area (wedge area of the solid, fused.py:741-835) is not built")
+        """[2, N] float64 (fused.py:788-835): row 0 the area of solid cap disk(x, H) cap wedge(x, axis, half_angle)
+        (units length^2; half_angle >= pi is the full disk), row 1 the full-disk area of the solid, summed over the
+        bodies; H is each query's support and `axes` [N, 2] are world vectors (only the direction matters).  A query
+        outside the broadphase of a surface whose solid is the outside lies deep in it: the whole sector.  One
+        wsb_aggregate_prepare + wsb_cone_area per (body, surface), float64 whatever the precision of the groups."""
+        ha = float(half_angle)
+        if not math.isfinite(ha) or ha < 0.0:
+            raise ValueError("FusedWall.cone_area: the half angle must be finite and >= 0")
+        N = self.N
+        ax = axes.to(self.dev, F64).contiguous()
+        if tuple(ax.shape) != (N, 2):
+            raise ValueError(f"FusedWall.cone_area: axes of shape {tuple(ax.shape)}, expected ({N}, 2)")
+        out = torch.zeros(2 * N, dtype=F64, device=self.dev)
+        for _, ns, ws, need, pose in self._surfaces():
+            check(lib.wsb_cone_area(ns.handle, ptr(self._sup), N, ptr(pose), ptr(ax), ha, ptr(out), ptr(ws), need,
+                                    _stream()), "wsb_cone_area")
+        return out.reshape(2, N)
 
     def dir_extreme(self, vecs):
-        raise NotImplementedError("FusedWall.dir_extreme (fused.py:662-705) is not built")
+        """[B, N] float64 (fused.py:741-786): for the world vectors `vecs` [B, N, 2] (one per body and query) the
+        largest |cos| between the vector and a direction from the query to a solid point of that body within one
+        support -- 1 where the line of the vector meets the solid there, 0 for a zero vector or no solid in support;
+        the maximum over the body's surfaces.  One wsb_aggregate_prepare + wsb_dir_extreme per (body, surface)."""
+        N, B = self.N, len(self.scene.bodies)
+        v = vecs.to(self.dev, F64).contiguous()
+        if tuple(v.shape) != (B, N, 2):
+            raise ValueError(f"FusedWall.dir_extreme: vecs of shape {tuple(v.shape)}, expected ({B}, {N}, 2)")
+        out = torch.zeros((B, N), dtype=F64, device=self.dev)
+        for bi, ns, ws, need, pose in self._surfaces():
+            check(lib.wsb_dir_extreme(ns.handle, N, ptr(pose), ptr(v[bi]), ptr(out[bi]), ptr(ws), need, _stream()),
+                  "wsb_dir_extreme")
+        return out
 
 
 _FAMILY = {"Wendland2": "w2", "Wendland4": "w4"}
