@@ -22,6 +22,8 @@ Writes
   cone_area_golden.json       the area of solid cap disk(x, H) cap wedge from the reference's vectorised per-edge closed form
                               (scene/cone_area.py): an L-shape, a thin bar and a tank (background), H 0.5 and 0.23,
                               half angles pi/6, pi/3, 2 and pi
+  sdf_contour_golden.json     the zero contours of sampled distances from the reference's marching squares (scene.py):
+                              a disk, a tank, two merging disks (saddles), a ring
   mesh3d_golden.json          closed triangle surfaces, 3-D: the 28 baseline channels (value moments |alpha| <= 2,
                               kernel-gradient moments |alpha| <= 1, kernel Hessian) from the reference's exact
                               face-to-edge reductions in mpmath (mesh3d/reference.py ClosedSurface), 40 digits, for an
@@ -385,6 +387,49 @@ def cone_area_golden(root, n=160, seed=11):
                    "cases": cases}, fh)
 
 
+def sdf_grids():
+    """(name, d [nx, ny], origin, spacing) of the sampled distances of the contour fixture: a disk obstacle, a tank
+    (the outside of a rounded box), two merging disks (saddle cells) and a ring (a hole in the solid)."""
+    sp = 0.05
+    xs = -1.2 + sp * np.arange(49)
+    X, Y = np.meshgrid(xs, xs, indexing="ij")
+    disk = np.hypot(X - 0.03, Y + 0.02) - 0.61
+    qx, qy = np.abs(X) - 0.7, np.abs(Y) - 0.5
+    box = np.hypot(np.maximum(qx, 0), np.maximum(qy, 0)) + np.minimum(np.maximum(qx, qy), 0) - 0.2
+    tank = -box
+    two = np.minimum(np.hypot(X + 0.36, Y) - 0.4, np.hypot(X - 0.36, Y - 0.03) - 0.37)
+    r = np.hypot(X, Y)
+    ring = np.maximum(r - 0.8, 0.35 - r)
+    out = [(n, d, (-1.2, -1.2), sp) for n, d in (("disk", disk), ("tank", tank), ("two_disks", two), ("ring", ring))]
+    for name, a in (("saddle_joined", -0.9), ("saddle_split", -0.3)):      # a diagonal solid pair: the cell mean decides
+        d = np.ones((4, 4))
+        d[1, 1], d[2, 2], d[1, 2], d[2, 1] = a, a, 0.5, 0.45
+        out.append((name, d, (0.0, 0.0), 0.1))
+    return out
+
+
+def sdf_contour_golden(root):
+    """sdf_contour_golden.json: the reference's marching squares (scene/scene.py _marching_squares, read from the
+    source and run on its own with a stand-in SurfaceRep that records vertices / edges / background) on sdf_grids."""
+    import ast
+    src = (Path(root) / "src" / "warpSPHBoundaries" / "scene" / "scene.py").read_text()
+    node = next(n for n in ast.parse(src).body if isinstance(n, ast.FunctionDef) and n.name == "_marching_squares")
+
+    class Recorder:
+        def __init__(self, vertices, edges, background=0):
+            self.vertices, self.edges, self.background = vertices, edges, background
+
+    ns = {"np": np, "SurfaceRep": Recorder}
+    exec(compile(ast.Module(body=[node], type_ignores=[]), "scene.py", "exec"), ns)
+    cases = []
+    for name, d, origin, sp in sdf_grids():
+        rep = ns["_marching_squares"](d, np.asarray(origin), sp)
+        cases.append({"name": name, "vertices": np.asarray(rep.vertices).tolist(),
+                      "edges": np.asarray(rep.edges).tolist(), "background": int(rep.background)})
+    with open(HERE / "sdf_contour_golden.json", "w") as fh:
+        json.dump({"source": "src/warpSPHBoundaries/scene/scene.py _marching_squares", "cases": cases}, fh)
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     np2d, torch2d = load_reference(root)
@@ -396,3 +441,4 @@ if __name__ == "__main__":
     triangle_golden(root)
     wall_kernel_golden(root)
     cone_area_golden(root)
+    sdf_contour_golden(root)

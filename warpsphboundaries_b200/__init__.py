@@ -9,7 +9,7 @@ from .shim import (GradientScheme, KernelFunctions, OperationDirection, Operatio
 
 def __getattr__(name):
     # the GPU-facing modules load libwsb.so on first use, so the exact algebra and the shims import without it
-    if name in ("Scene", "Body", "Pose", "SurfaceRep", "BodyKinematics", "RepMoments", "SurfaceTopology"):
+    if name in ("Scene", "Body", "Pose", "SurfaceRep", "BoxRep", "BodyKinematics", "RepMoments", "SurfaceTopology"):
         from . import scene
         return getattr(scene, name)
     if name in ("AnalyticBoundary", "BoundaryProvider", "FusedWall", "WallAggregate", "WallOutput", "FusedGroup"):

@@ -106,12 +106,9 @@ def fixed_adjacency(scene, queryParticles, operationProperties, supportMax):
     for bi, body in enumerate(scene.bodies):
         lpos = kin.local[bi]
         valid = body_candidates(body, lpos, sup, allowed)
-        reps = []
-        for rep in body.reps:
-            if not isinstance(rep, SurfaceRep):
-                raise NotImplementedError(f"fixed adjacency: {type(rep).__name__} is not built (surface loops only)")
-            reps.append(fixed_topology(rep, lpos, sup, valid, supportMax))
-        bodies.append(BodyAdjacency(body, cand, lpos, sup, reps, valid, list(body.reps)))
+        surfaces = body.fused_reps(supportMax, dev)                  # implicit / sampled shapes as their polygon
+        reps = [fixed_topology(rep, lpos, sup, valid, supportMax) for rep in surfaces]
+        bodies.append(BodyAdjacency(body, cand, lpos, sup, reps, valid, list(surfaces)))
     return SceneAdjacency(N, bodies, {"candidates": None}, queryParticles, float(supportMax))
 
 

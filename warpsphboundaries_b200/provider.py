@@ -97,12 +97,10 @@ class FusedWall(WallAggregate):
                 raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} is not built")
             if g.kernel in QUAD_KERNEL_IDS and route != "fused":
                 raise NotImplementedError(f"FusedWall: the tensile group {g.kernel!r} runs on the fused route only")
-        sig = (route,) + tuple(id(r) for b in scene.bodies for r in b.reps)
+        sig = (route, self.support) + tuple(id(r) for b in scene.bodies for r in b.reps)
         if getattr(scene, "_wsb_checked", None) != sig:
             for b in scene.bodies:
-                for r in b.reps:
-                    if not isinstance(r, SurfaceRep):
-                        raise NotImplementedError(f"FusedWall: {type(r).__name__} is not built (surface loops only)")
+                for r in b.fused_reps(self.support, self.dev):
                     if r._triangle is not None and route != "fused":
                         raise NotImplementedError("FusedWall: conditioned single triangles take the fused route")
             scene._wsb_checked = sig
@@ -147,7 +145,7 @@ class FusedWall(WallAggregate):
                 continue
             pose = body.pose_tensor(self.dev)
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
-            for ri, rep in enumerate(body.reps):
+            for ri, rep in enumerate(body.fused_reps(self.support, self.dev)):
                 ns = rep.native(self.support, self.dev)
                 if self.workspaces is not None:
                     ws = self.workspaces[id(rep)]
@@ -214,7 +212,8 @@ class FusedWall(WallAggregate):
 
     @staticmethod
     def supported(scene, lowering=True):
-        return all(isinstance(r, SurfaceRep) for b in scene.bodies for r in b.reps)
+        return all(b.fusable() for b in scene.bodies) if lowering else \
+            all(isinstance(r, SurfaceRep) for b in scene.bodies for r in b.reps)
 
     def evaluate(self, outputs, a1=None):
         """{name: tensor [B, N, ...]} float64, world frame (fused.py:612-659).  `a1` [B, N, 2]: world vectors of the
@@ -282,7 +281,7 @@ class FusedWall(WallAggregate):
                 continue
             pose = body.pose_tensor(self.dev)
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
-            for rep in body.reps:
+            for rep in body.fused_reps(self.support, self.dev):
                 ns = rep.native(self.support, self.dev)
                 if self.workspaces is not None:
                     ws = self.workspaces[id(rep)]

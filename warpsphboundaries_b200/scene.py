@@ -241,6 +241,220 @@ class SurfaceRep:
         return SurfaceTopology(ft.qi[keep], ft.e[keep], supmax, ft.ind)
 
 
+
+class BoxRep(SurfaceRep):
+    """an axis-aligned rectangle [lo, hi] in the body frame (scene.py:459-510): the solid (`solid='inside'`: an
+    obstacle, a baffle, a floor slab) or the fluid domain (`solid='outside'`: a tank, a channel).  The reference
+    evaluates a box from Chebyshev corner tables (scene/box.py; table error up to 1e-7 on the gradient channels of w2
+    and 1e-6 for lw2) and its exact polygon for the kinked kernels; here every kernel runs the exact closed form of
+    that polygon -- four edges, at most four neighbour pairs a row -- so a box is the SurfaceRep of its outline (a
+    tank: the clockwise outline with background 1), and `surface()` is the box itself."""
+    kind = "box"
+
+    def __init__(self, lo, hi, solid: str = "inside"):
+        if solid not in ("inside", "outside"):
+            raise ValueError("solid must be 'inside' or 'outside'")
+        lo_h = tuple(float(v) for v in torch.as_tensor(lo, dtype=F64).reshape(2))
+        hi_h = tuple(float(v) for v in torch.as_tensor(hi, dtype=F64).reshape(2))
+        if not (hi_h[0] > lo_h[0] and hi_h[1] > lo_h[1]):
+            raise ValueError(f"BoxRep: hi {hi_h} must exceed lo {lo_h} in both coordinates")
+        (x0, y0), (x1, y1) = lo_h, hi_h
+        P = SurfaceRep._orient(np.array([(x0, y0), (x1, y0), (x1, y1), (x0, y1)], dtype=float), solid)
+        super().__init__(np.ascontiguousarray(P), np.array([[0, 1], [1, 2], [2, 3], [3, 0]]),
+                         background=0 if solid == "inside" else 1, conditioned=False)
+        self.solid = solid
+        self.lo_h, self.hi_h = lo_h, hi_h      # host copies: reading a device tensor would synchronise
+        self.lo = torch.tensor(lo_h, dtype=F64)
+        self.hi = torch.tensor(hi_h, dtype=F64)
+
+    def to(self, device):
+        super().to(device)
+        self.lo, self.hi = self.lo.to(device), self.hi.to(device)
+        return self
+
+    def surface(self):
+        return self
+
+    def signed(self, lpos):
+        """(d, n) of body-frame points (scene.py:490-506): the signed distance, positive in the fluid, and the unit
+        normal from the wall into the fluid -- from the closest point of the box outside it, else the normal of the
+        nearest face plane."""
+        lo, hi = self.lo.to(lpos.device), self.hi.to(lpos.device)
+        c, hw = 0.5 * (lo + hi), 0.5 * (hi - lo)
+        r = lpos - c
+        q = r.abs() - hw
+        sd = q.clamp(min=0).norm(dim=1) + q.max(dim=1).values.clamp(max=0)
+        ax = (q[:, 1] > q[:, 0]).long()
+        sgn = torch.where(r.gather(1, ax[:, None])[:, 0] >= 0, 1.0, -1.0).to(F64)
+        face = torch.zeros_like(lpos).scatter_(1, ax[:, None], sgn[:, None])
+        dirv = lpos - torch.minimum(torch.maximum(lpos, lo), hi)
+        dn = dirv.norm(dim=1, keepdim=True)
+        outward = torch.where(dn > 1e-12, dirv / dn.clamp(min=1e-300), face)
+        if self.solid == "inside":
+            return sd, outward
+        return -sd, -face
+
+
+class ImplicitRep:
+    """an analytic primitive in the body frame (scene.py:558-596).  The fused wall path integrates its exact polygon
+    form: a cavity disk (fluid inside the circle) is its area-preserving regular polygon with edges <= the policy's
+    bound times the support (at least 24 edges), integrated exactly like any surface.  A solid disk is the
+    reference's disk element (a table lookup per (query, disk)) and a half plane has no polygon form: both raise
+    NotImplementedError on the fused path."""
+    kind = "implicit"
+
+    def __init__(self, shape, policy=None):
+        from .implicit import TierPolicy
+        self.shape = shape
+        self.policy = policy or TierPolicy()
+        self._fallback = {}
+
+    def to(self, device):
+        for s in self._fallback.values():
+            s.to(device)
+        return self
+
+    def bounds(self):
+        from .implicit import DiskBody
+        s = self.shape
+        if isinstance(s, DiskBody):
+            c = torch.as_tensor(s.center, dtype=F64)
+            return c - s.radius, c + s.radius
+        big = 1e8
+        return torch.full((2,), -big, dtype=F64), torch.full((2,), big, dtype=F64)
+
+    def unbounded(self):
+        """the solid reaches infinity: a half plane or a cavity (scene.py:1036-1046)."""
+        from .implicit import HalfPlaneBody
+        return isinstance(self.shape, HalfPlaneBody) or getattr(self.shape, "solid", None) == "outside"
+
+    def lowered(self, hmin, device):
+        """the exact-integral form for the fused wall evaluation (scene.py:582-588)."""
+        from .implicit import DiskBody
+        if not isinstance(self.shape, DiskBody):
+            raise NotImplementedError("FusedWall: a half plane has no polygon form (the reference serves it by its "
+                                      "per-operation path, not the fused wall)")
+        if self.shape.solid == "inside":
+            raise NotImplementedError("FusedWall: a solid disk is the disk element (DiskArrayRep tables), which is "
+                                      "not built; a polygon SurfaceRep of the disk is served")
+        return self.fallbackSurface(hmin, device)
+
+    def fallbackSurface(self, hmin, device):
+        """the area-preserving regular polygon with n = max(24, ceil(2 pi R / (edge bound * hmin))) edges, cached per
+        n (scene.py:590-596)."""
+        s = self.shape
+        n = max(24, int(np.ceil(2 * np.pi * s.radius / (self.policy.maxPolygonEdgeOverH * float(hmin)))))
+        if n not in self._fallback:
+            self._fallback[n] = SurfaceRep.regularPolygon(s.center, s.radius, n, solid=s.solid)
+        return self._fallback[n].to(device)
+
+    def signed(self, lpos):
+        d, n, _ = self.shape.signed(lpos)
+        return d, n
+
+
+def _marching_squares(d, origin, spacing):
+    """the zero level set of node values d [nx, ny] (d < 0 solid) as a SurfaceRep with the solid on the left of every
+    edge (scene.py:762-805).  Per cell the sign changes along its counter-clockwise boundary are exits (solid ->
+    fluid) and entries; each exit links to the next entry along the boundary, or -- in a saddle cell whose mean
+    value is solid (the solid connects across the cell) -- to the previous one.  A crossing's vertex interpolates d
+    linearly from the first end of the cell side as the cell walks it.  The border nodes must all be fluid (an
+    obstacle, background 0) or all solid (a tank, background 1)."""
+    d = np.asarray(d, dtype=float)
+    nx, ny = d.shape
+    solid = d < 0
+    border = np.concatenate([solid[0], solid[-1], solid[1:-1, 0], solid[1:-1, -1]])
+    if border.any() and not border.all():
+        raise ValueError("SdfRep.contour: the sampled grid must cover the body with a margin (all border nodes "
+                         "fluid, or all solid)")
+    background = 1 if border.all() else 0
+    ox, oy = float(origin[0]), float(origin[1])
+    verts, vid, edges = [], {}, []
+
+    def crossing(a, b):
+        key = (a, b)
+        if key not in vid:
+            t = d[a] / (d[a] - d[b])
+            vid[key] = len(verts)
+            verts.append((ox + spacing * (a[0] + t * (b[0] - a[0])), oy + spacing * (a[1] + t * (b[1] - a[1]))))
+        return vid[key]
+
+    corners = solid[:-1, :-1].astype(np.int8) + solid[1:, :-1] + solid[1:, 1:] + solid[:-1, 1:]
+    for i, j in zip(*np.nonzero((corners > 0) & (corners < 4))):
+        i, j = int(i), int(j)
+        ring = ((i, j), (i + 1, j), (i + 1, j + 1), (i, j + 1))
+        seq = []                                       # (is_exit, vertex) in boundary order
+        for k in range(4):
+            a, b = ring[k], ring[(k + 1) % 4]
+            if solid[a] != solid[b]:
+                seq.append((bool(solid[a]), crossing(a, b)))
+        m = len(seq)
+        step = -1 if (m == 4 and d[i:i + 2, j:j + 2].mean() < 0) else 1
+        for k in range(m):
+            if seq[k][0]:
+                q = (k + step) % m
+                while seq[q][0]:
+                    q = (q + step) % m
+                edges.append((seq[k][1], seq[q][1]))
+    if not edges:
+        raise ValueError("SdfRep.contour: no zero level set in the sampled grid")
+    return SurfaceRep(np.asarray(verts, dtype=float), np.asarray(edges, dtype=np.int32), background=background,
+                      conditioned=False)
+
+
+class SdfRep:
+    """a sampled signed distance in the body frame, positive in the fluid, on a regular grid (scene.py:599-705).
+    The fused wall path integrates its exact polygon form: the given `fallback` surface, else the marching-squares
+    contour of the samples.  The reference's sampled-field tier-3 model belongs to its per-operation path and is
+    not built; the signed distance of the representation is the exact distance to that polygon."""
+    kind = "sdf"
+
+    def __init__(self, values, origin, spacing, fallback: Optional[SurfaceRep] = None, **guards):
+        self.d = torch.as_tensor(values, dtype=F64)
+        self.origin = torch.as_tensor(origin, dtype=F64)
+        self.spacing = float(spacing)
+        if not self.spacing > 0:
+            raise ValueError("SdfRep: the grid spacing must be positive")
+        self.fallback = fallback
+        self.guards = guards           # the reference's tier-3 guard settings, kept for its signature
+        self._contour = None
+
+    @staticmethod
+    def fromFunction(fn, lo, hi, spacing, **kw):
+        """sample fn(points [M, 2]) -> d on the regular grid covering [lo, hi] (scene.py:640-647)."""
+        nx = int(np.ceil((hi[0] - lo[0]) / spacing)) + 1
+        ny = int(np.ceil((hi[1] - lo[1]) / spacing)) + 1
+        X, Y = np.meshgrid(lo[0] + spacing * np.arange(nx), lo[1] + spacing * np.arange(ny), indexing="ij")
+        pts = torch.as_tensor(np.stack([X.ravel(), Y.ravel()], 1), dtype=F64)
+        return SdfRep(fn(pts).reshape(nx, ny), lo, spacing, **kw)
+
+    def to(self, device):
+        self.d, self.origin = self.d.to(device), self.origin.to(device)
+        if self.fallback is not None:
+            self.fallback.to(device)
+        if self._contour is not None:
+            self._contour.to(device)
+        return self
+
+    def contour(self):
+        if self._contour is None:
+            self._contour = _marching_squares(self.d.cpu().numpy(), self.origin.cpu().numpy(),
+                                              self.spacing).to(self.d.device)
+        return self._contour
+
+    def lowered(self, hmin, device):
+        """the given fallback surface, else the contour (scene.py:663-666)."""
+        fb = self.fallback if self.fallback is not None else self.contour()
+        return fb.to(device)
+
+    def unbounded(self):
+        return bool(self.lowered(0.0, self.d.device).background)
+
+    def bounds(self):
+        ext = torch.as_tensor(self.d.shape, dtype=F64) - 1
+        o = self.origin.cpu()
+        return o, o + ext * self.spacing
+
 @dataclass
 class SurfaceTopology:
     """the pair list of one SurfaceRep against a set of queries (scene.py:145-178)."""
@@ -326,7 +540,8 @@ class Body:
         key = tuple(id(r) for r in self.reps)
         c = self.__dict__.get("_obbCache")
         if c is None or c[0] != key:
-            los, his = zip(*[r.bounds() for r in self.reps])
+            # a sampled distance is integrated as its polygon, which a fallback surface may extend past the grid
+            los, his = zip(*[(r.lowered(0.0, r.d.device) if isinstance(r, SdfRep) else r).bounds() for r in self.reps])
             lo = torch.stack([a.cpu() for a in los]).amin(0)
             hi = torch.stack([a.cpu() for a in his]).amax(0)
             c = (key, (float(lo[0]), float(lo[1]), float(hi[0]), float(hi[1])))
@@ -334,10 +549,34 @@ class Body:
         return c[1]
 
     def unbounded(self):
-        return any(isinstance(r, SurfaceRep) and r.background for r in self.reps)
+        """the static exterior-solid broadphase convention (scene.py:1036-1046): a surface with background 1 (a tank
+        outline), a cavity disk or a half plane, a sampled distance whose contour is a tank."""
+        return any((isinstance(r, SurfaceRep) and r.background) or
+                   (isinstance(r, (ImplicitRep, SdfRep)) and r.unbounded()) for r in self.reps)
 
     def fusable(self):
-        return all(isinstance(r, SurfaceRep) for r in self.reps)
+        from .implicit import DiskBody
+        return all(isinstance(r, (SurfaceRep, SdfRep)) or
+                   (isinstance(r, ImplicitRep) and isinstance(r.shape, DiskBody) and r.shape.solid == "outside")
+                   for r in self.reps)
+
+    def fused_reps(self, hmin, device):
+        """the representations as the surfaces the fused wall evaluation integrates exactly (scene.py:970-997):
+        SurfaceRep and BoxRep as they are, ImplicitRep and SdfRep lowered to their polygon; cached per (hmin,
+        device).  NotImplementedError for a representation without that form."""
+        cache = self.__dict__.setdefault("_fusedCache", {})
+        key = (float(hmin), str(device), tuple(id(r) for r in self.reps))
+        if key not in cache:
+            out = []
+            for r in self.reps:
+                if isinstance(r, SurfaceRep):
+                    out.append(r)
+                elif isinstance(r, (ImplicitRep, SdfRep)):
+                    out.append(r.lowered(hmin, device))
+                else:
+                    raise NotImplementedError(f"FusedWall: {type(r).__name__} is not built")
+            cache[key] = out
+        return cache[key]
 
     def pose_tensor(self, device):
         """(cx, cy, cos, sin) on the device, cached while the pose is unchanged."""
@@ -416,6 +655,18 @@ class Scene:
                 continue
             lp = bd.toLocal(pts).contiguous()
             for rep in bd.reps:
+                if isinstance(rep, SdfRep):
+                    rep = rep.lowered(0.0, self.device)        # the exact distance to its polygon form
+                if isinstance(rep, (BoxRep, ImplicitRep)):
+                    # the shape's own closed form and normals (scene.py:1351-1353, 1360-1362)
+                    d, nl = rep.signed(lp)
+                    n = bd.pose.vecToWorld(nl)
+                    better = d < best
+                    best = torch.where(better, d, best)
+                    normal = torch.where(better[:, None], n, normal)
+                    bidx = torch.where(better, torch.full_like(bidx, bi), bidx)
+                    hit |= True
+                    continue
                 if not isinstance(rep, SurfaceRep):
                     continue
                 ns = rep.native(supportMax, self.device) if supportMax is not None else rep._default_native(self.device)
@@ -443,6 +694,10 @@ class Scene:
                 continue
             lp = bd.toLocal(pts)
             for rep in bd.reps:
-                if isinstance(rep, SurfaceRep):
+                if isinstance(rep, SdfRep):
+                    rep = rep.lowered(0.0, self.device)
+                if isinstance(rep, ImplicitRep):
+                    out |= rep.signed(lp)[0] < 0
+                elif isinstance(rep, SurfaceRep):
                     out |= rep.indicator(lp) > 0.5
         return out
