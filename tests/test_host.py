@@ -146,7 +146,8 @@ def test_contour_rejects_bad_grids():
 
 def test_implicit_lowering_host_logic():
     """ImplicitRep (scene.py:558-596): a cavity disk lowers to its area-preserving polygon with
-    max(24, ceil(2 pi R / (h / 16))) edges, cached; solid disks and half planes have no polygon form here."""
+    max(24, ceil(2 pi R / (h / 16))) edges, cached; a solid disk to a one-disk DiskArrayRep; a half plane has no
+    exact form."""
     from warpsphboundaries_b200.implicit import DiskBody, HalfPlaneBody, TierPolicy
     from warpsphboundaries_b200.scene import ImplicitRep
     cav = ImplicitRep(DiskBody((0.2, -0.1), 0.9, solid="outside"))
@@ -159,13 +160,30 @@ def test_implicit_lowering_host_logic():
     assert len(ImplicitRep(DiskBody((0, 0), 0.01, "outside")).lowered(0.1, "cpu").edges) == 24
     assert len(ImplicitRep(DiskBody((0, 0), 0.9, "outside"), TierPolicy(maxPolygonEdgeOverH=0.5)).lowered(
         0.1, "cpu").edges) == int(np.ceil(2 * np.pi * 0.9 / 0.05))
-    for rep in (ImplicitRep(DiskBody((0, 0), 0.5)), ImplicitRep(HalfPlaneBody((0, 0), (0, 1)))):
-        with pytest.raises(NotImplementedError):
-            rep.lowered(0.1, "cpu")
+    from warpsphboundaries_b200.scene import DiskArrayRep
+    solid = ImplicitRep(DiskBody((0.3, 0.1), 0.5)).lowered(0.1, "cpu")
+    assert isinstance(solid, DiskArrayRep) and solid.centres.tolist() == [[0.3, 0.1]] and solid.radii.tolist() == [0.5]
+    with pytest.raises(NotImplementedError):
+        ImplicitRep(HalfPlaneBody((0, 0), (0, 1))).lowered(0.1, "cpu")
     b = Body(reps=[cav])
     assert b.unbounded() and b.fusable()
-    assert not Body(reps=[ImplicitRep(DiskBody((0, 0), 0.5))]).fusable()
+    assert Body(reps=[ImplicitRep(DiskBody((0, 0), 0.5))]).fusable()
+    assert not Body(reps=[ImplicitRep(HalfPlaneBody((0, 0), (0, 1)))]).fusable()
     d, nrm, kap = DiskBody((0.0, 0.0), 1.0).signed(torch.tensor([[2.0, 0.0]], dtype=torch.float64))
     assert float(d[0]) == 1.0 and nrm.tolist() == [[1.0, 0.0]] and kap == 1.0
     d, nrm, _ = HalfPlaneBody((0.0, 1.0), (0.0, 1.0)).signed(torch.tensor([[3.0, 0.5]], dtype=torch.float64))
     assert float(d[0]) == -0.5 and nrm.tolist() == [[0.0, 1.0]]
+
+
+def test_disk_array_host_logic():
+    """DiskArrayRep (scene.py:808-905): bounds, argument checks and the signed distance to the nearest circle."""
+    from warpsphboundaries_b200.scene import DiskArrayRep
+    d = DiskArrayRep([[0.0, 0.0], [3.0, 1.0]], [1.0, 0.5])
+    lo, hi = d.bounds()
+    assert lo.tolist() == [-1.0, -1.0] and hi.tolist() == [3.5, 1.5]
+    sd, n = d.signed(torch.tensor([[2.0, 0.0], [0.5, 0.0], [3.0, 2.0]], dtype=torch.float64))
+    assert np.allclose(sd.numpy(), [np.hypot(1, 1) - 0.5, -0.5, 0.5]) and np.allclose(n.numpy()[1:], [[1, 0], [0, 1]])
+    with pytest.raises(ValueError):
+        DiskArrayRep([[0.0, 0.0]], [1.0, 2.0])
+    with pytest.raises(ValueError):
+        DiskArrayRep([[0.0, 0.0]], [0.0])

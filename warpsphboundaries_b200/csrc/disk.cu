@@ -1,0 +1,332 @@
+// The disk element: the twelve channels of solid disks (fibre bundles, solid disk bodies) at every particle,
+// exactly, in float64 -- the drop-in for the reference's table lookup per (query, disk)
+// (src/warpSPHBoundaries/edge/warpdisk.py:1-199, edge/disktables.py, scene/scene.py:808-905 DiskArrayRep,
+// scene/fixedadj.py:199-246 fixed_disk_topology).
+//
+// Math (h = 1, P = pi W as truncated polynomial blocks).  The channels of the region Omega = disk cap support follow
+// from the divergence theorem with the radial potentials F1(r) = int_0^r t P dt and F2(r) = int_0^r t F1 dt:
+//   lam  = oint F1/r^2 (y.n)        m1 = oint F1 n         G = -oint P n
+//   g1_dj = delta_dj lam - oint y_d P n_j                m2_dj = oint y_d F1 n_j - delta_dj oint F2/r^2 (y.n)
+// over the boundary of Omega: the arc of the disk's circle inside the support and the arc of the support circle
+// inside the disk (r = 1, n = y: closed forms in its half-angle).  In the frame whose x axis points at the disk
+// centre (distance D, radius R) the disk arc is symmetric about the point nearest the particle; with u the angle from
+// that point the integrand is analytic except at u = +-i acosh((D^2 + R^2) / (2 D R)), where r vanishes.  The arc is
+// integrated by 24-node Gauss-Legendre panels graded from u = 0 (the first up to twice that distance, then doubling,
+// as the edge quadrature of the tensile kernels) and split where r crosses a block radius; every quantity that cancels
+// near the particle is formed from sin^2(u/2):  r^2 = (D - R)^2 + 4 D R sin^2(u/2), y.n = (R - D) + 2 D sin^2(u/2).
+// The arc ends and the support arc's half-angle come from the same stable forms.  Near-tangent rows (|D - R| -> 0)
+// take more panels (about log2(pi / |D - R|)), never fewer digits.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace wsb {
+
+struct Disks {
+  int device = 0;
+  int64_t m = 0;
+  double support_max = 0;
+  int32_t nx = 0, ny = 0;
+  double lo_x = 0, lo_y = 0, cell = 1;
+  int64_t n_items = 0;
+  int32_t* cstart = nullptr;   // [nx*ny+1]
+  double4* items = nullptr;    // [n_items] (cx, cy, R, 0) of the disks that reach the cell, cell-list order
+};
+
+constexpr int kDiskThreads = 128;
+
+// the value potential F1/r^2, the second potential F2/r^2 and P at r (sums over the truncated blocks)
+__device__ __forceinline__ void disk_profile(const DiskTable& T, double r, double& P, double& Fl, double& F2l) {
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.0;
+  const double ir2 = 1.0 / (r * r);
+  for (int k = 0; k < T.nb; ++k) {
+    const DiskBlock& b = T.b[k];
+    F2l += 0.5 * b.Mhat;
+    if (r <= b.R) {
+      double p = 0.0, l = 0.0, f = 0.0;
+      for (int j = b.np - 1; j >= 0; --j) p = fma(p, r, b.P[j]);
+      for (int j = b.nl - 1; j >= 0; --j) l = fma(l, r, b.L[j]);
+      for (int j = b.nf - 1; j >= 0; --j) f = fma(f, r, b.F[j]);
+      P += p;
+      Fl += l;
+      F2l += f;
+    } else {
+      Fl += b.Mhat * ir2;
+      F2l += b.MPhat * ir2;
+    }
+  }
+}
+
+// The seven non-zero channels of one disk in its aligned frame (before 1/pi): lam, m1_x, G_x, g1_xx, g1_yy, m2_xx,
+// m2_yy.  D = centre distance, R = radius (h = 1), D < 1 + R.
+__device__ void disk_pair(const DiskTable& T, double D, double R, double out[7]) {
+  double lam = 0.0, m1 = 0.0, G = 0.0, gxx = 0.0, gyy = 0.0, mxx = 0.0, myy = 0.0, SF = 0.0;
+  const double dm = D - R;
+  // the arc of the disk's circle inside the support: u in [0, U] (and its mirror image)
+  if (fabs(dm) < 1.0) {   // (D = 0: a concentric circle, one panel: the singularity distance is infinite)
+    const double U = D + R <= 1.0 ? 0.5 * kTwoPi : 2.0 * asin(fmin(1.0, sqrt((1.0 - dm * dm) / (4.0 * D * R))));
+    const double x = 0.5 * dm * dm / (D * R);                  // acosh(1 + x): the distance of the singularity
+    const double base = fmax(log1p(x + sqrt(x * (x + 2.0))), 0x1p-24);
+    double knots[kDiskMaxBlocks];
+    int nk = 0;
+    for (int k = 0; k < T.nb; ++k) {
+      const double Rb = T.b[k].R;
+      if (Rb < 1.0 && fabs(dm) < Rb && Rb < D + R) {
+        const double kn = 2.0 * asin(fmin(1.0, sqrt((Rb * Rb - dm * dm) / (4.0 * D * R))));
+        if (kn > 0.0 && kn < U) knots[nk++] = kn;
+      }
+    }
+    for (int a = 1; a < nk; ++a)                                   // ascending (at most kDiskMaxBlocks - 1 knots)
+      for (int b = a; b > 0 && knots[b] < knots[b - 1]; --b) {
+        const double t = knots[b];
+        knots[b] = knots[b - 1];
+        knots[b - 1] = t;
+      }
+    double d = 2.0 * base, u = 0.0;
+    int ki = 0;
+    for (int it = 0; it < 160 && u < U; ++it) {
+      double nxt = fmin(U, d);
+      while (ki < nk && knots[ki] <= u) ++ki;
+      if (ki < nk && knots[ki] < nxt) nxt = knots[ki];
+      const double hc = 0.5 * (nxt - u), mc = 0.5 * (nxt + u);
+      for (int q = 0; q < kQuadGauss; ++q) {
+        const double uu = fma(hc, kQuadGx[q], mc);
+        double su, cu;
+        sincos(uu, &su, &cu);
+        const double sh = sin(0.5 * uu), s2 = sh * sh;
+        const double yx = fma(2.0 * R, s2, dm), yy = R * su, nx = -cu, ny = su;
+        const double yn = fma(2.0 * D, s2, -dm);
+        const double r = sqrt(fma(4.0 * D * R, s2, dm * dm));
+        double P, Fl, F2l;
+        disk_profile(T, r, P, Fl, F2l);
+        const double F1 = Fl * r * r;
+        const double w = 2.0 * R * hc * kQuadGw[q];
+        lam = fma(w * Fl, yn, lam);
+        m1 = fma(w * F1, nx, m1);
+        G = fma(-w * P, nx, G);
+        gxx = fma(-w * P * yx, nx, gxx);
+        gyy = fma(-w * P * yy, ny, gyy);
+        mxx = fma(w * F1 * yx, nx, mxx);
+        myy = fma(w * F1 * yy, ny, myy);
+        SF = fma(w * F2l, yn, SF);
+      }
+      if (nxt >= d) d *= 2.0;
+      u = nxt;
+    }
+  }
+  // the arc of the support circle inside the disk: |phi| < beta
+  double beta = -1.0;
+  if (R >= D + 1.0)
+    beta = 0.5 * kTwoPi;
+  else if (fabs(D - 1.0) < R && D > 0.0)
+    beta = 2.0 * asin(fmin(1.0, sqrt((R * R - (D - 1.0) * (D - 1.0)) / (4.0 * D))));
+  if (beta > 0.0) {
+    double P1, Fl1, F2l1;
+    disk_profile(T, 1.0, P1, Fl1, F2l1);
+    const double sb = sin(beta), s2b = sin(2.0 * beta);
+    const double cxx = beta + 0.5 * s2b, cyy = beta - 0.5 * s2b;
+    lam += 2.0 * beta * Fl1;
+    m1 += 2.0 * sb * Fl1;
+    G -= 2.0 * sb * P1;
+    gxx -= P1 * cxx;
+    gyy -= P1 * cyy;
+    mxx += Fl1 * cxx;
+    myy += Fl1 * cyy;
+    SF += 2.0 * beta * F2l1;
+  }
+  out[0] = lam;
+  out[1] = m1;
+  out[2] = G;
+  out[3] = gxx + lam;
+  out[4] = gyy + lam;
+  out[5] = mxx - SF;
+  out[6] = myy - SF;
+}
+
+// one thread per particle: body frame, the particle's cell, every disk of the cell within reach, the channels of each
+// rotated from its aligned frame and summed in cell-list order, then scaled and rotated to the world frame
+__global__ void __launch_bounds__(kDiskThreads) k_disk(const DiskTable T, const int32_t* __restrict__ cstart,
+                                                      const double4* __restrict__ items, int32_t nx, int32_t ny,
+                                                      double lo_x, double lo_y, double cell,
+                                                      const double* __restrict__ pos, const double* __restrict__ sup,
+                                                      const int32_t* __restrict__ allowed, int64_t n,
+                                                      const double* __restrict__ pose, bool assign, double* lam,
+                                                      double* G, double* cov, double* m1, double* m2) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double acc[12];
+#pragma unroll
+  for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+  const double h = sup[i];
+  if (!allowed || allowed[i] != 0) {
+    double lx, ly;
+    to_local_rn(pos[2 * i], pos[2 * i + 1], pose[0], pose[1], pose[2], pose[3], lx, ly);
+    const double fx = floor((lx - lo_x) / cell), fy = floor((ly - lo_y) / cell);
+    if (fx >= 0.0 && fx < (double)nx && fy >= 0.0 && fy < (double)ny) {
+      const int32_t cid = (int32_t)fx * ny + (int32_t)fy;
+      const double ih = 1.0 / h;
+      for (int32_t k = cstart[cid]; k < cstart[cid + 1]; ++k) {
+        const double4 e = items[k];
+        const double vx = (e.x - lx) * ih, vy = (e.y - ly) * ih, R = e.z * ih;
+        const double D = sqrt(vx * vx + vy * vy);
+        if (!(D < 1.0 + R)) continue;
+        double o[7];
+        disk_pair(T, D, R, o);
+        const double ca = D > 0.0 ? vx / D : 1.0, sa = D > 0.0 ? vy / D : 0.0;
+        acc[0] += o[0];
+        acc[1] += ca * o[1];
+        acc[2] += sa * o[1];
+        acc[3] += ca * o[2];
+        acc[4] += sa * o[2];
+        const double dg = o[3] - o[4], dmm = o[5] - o[6];
+        acc[5] += ca * ca * o[3] + sa * sa * o[4];
+        acc[6] += ca * sa * dg;
+        acc[7] += ca * sa * dg;
+        acc[8] += sa * sa * o[3] + ca * ca * o[4];
+        acc[9] += ca * ca * o[5] + sa * sa * o[6];
+        acc[10] += ca * sa * dmm;
+        acc[11] += sa * sa * o[5] + ca * ca * o[6];
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
+  const double c = pose[2], s = pose[3];
+  const double rot[4] = {c, -s, s, c};
+  write_outputs(acc, h, rot, i, lam, G, cov, m1, m2, assign);
+}
+
+}  // namespace wsb
+
+using namespace wsb;
+
+extern "C" int wsb_disks_create(const double* centres, const double* radii, int64_t m, double support_max, int device,
+                                wsb_disks** out) {
+  if (!out) return fail(WSB_ERR_ARG, "wsb_disks_create: NULL output handle");
+  *out = nullptr;
+  if (m < 0 || m > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_disks_create: disk count out of range");
+  if (m > 0 && (!centres || !radii)) return fail(WSB_ERR_ARG, "wsb_disks_create: NULL array");
+  if (!(support_max > 0.0) || !std::isfinite(support_max))
+    return fail(WSB_ERR_ARG, "wsb_disks_create: support_max must be positive and finite");
+  double lo_x = 0, lo_y = 0, hi_x = 0, hi_y = 0;
+  for (int64_t k = 0; k < m; ++k) {
+    const double cx = centres[2 * k], cy = centres[2 * k + 1], R = radii[k];
+    if (!std::isfinite(cx) || !std::isfinite(cy) || !(R > 0.0) || !std::isfinite(R))
+      return fail(WSB_ERR_ARG, "wsb_disks_create: disk " + std::to_string(k) + " has a non-finite centre or a "
+                                   "radius that is not positive");
+    if (k == 0 || cx - R < lo_x) lo_x = cx - R;
+    if (k == 0 || cy - R < lo_y) lo_y = cy - R;
+    if (k == 0 || cx + R > hi_x) hi_x = cx + R;
+    if (k == 0 || cy + R > hi_y) hi_y = cy + R;
+  }
+  Disks* d = new Disks();
+  d->device = device;
+  d->m = m;
+  d->support_max = support_max;
+  // a cell grid over the disks' boxes grown by one support; a disk is listed in every cell whose box comes within
+  // R + support_max of its centre (interior cells included: a particle deep inside still has the disk's plane terms)
+  const double s = support_max;
+  double cell = s;
+  lo_x -= s;
+  lo_y -= s;
+  hi_x += s;
+  hi_y += s;
+  auto dims = [&](double c, int64_t& gx, int64_t& gy) {
+    gx = std::max<int64_t>(1, (int64_t)std::ceil((hi_x - lo_x) / c));
+    gy = std::max<int64_t>(1, (int64_t)std::ceil((hi_y - lo_y) / c));
+  };
+  int64_t gx = 1, gy = 1;
+  if (m > 0) {
+    dims(cell, gx, gy);
+    while (gx * gy > ((int64_t)1 << 22)) {   // at most 4M cells: a coarser grid only lengthens the cell lists
+      cell *= 2.0;
+      dims(cell, gx, gy);
+    }
+  }
+  d->nx = (int32_t)gx;
+  d->ny = (int32_t)gy;
+  d->lo_x = lo_x;
+  d->lo_y = lo_y;
+  d->cell = cell;
+  std::vector<int32_t> counts((size_t)(gx * gy) + 1, 0);
+  auto each = [&](auto&& f) {
+    for (int64_t k = 0; k < m; ++k) {
+      const double cx = centres[2 * k], cy = centres[2 * k + 1], reach = radii[k] + s;
+      const int64_t x0 = std::max<int64_t>(0, (int64_t)std::floor((cx - reach - lo_x) / cell));
+      const int64_t x1 = std::min<int64_t>(gx - 1, (int64_t)std::floor((cx + reach - lo_x) / cell));
+      const int64_t y0 = std::max<int64_t>(0, (int64_t)std::floor((cy - reach - lo_y) / cell));
+      const int64_t y1 = std::min<int64_t>(gy - 1, (int64_t)std::floor((cy + reach - lo_y) / cell));
+      for (int64_t ix = x0; ix <= x1; ++ix)
+        for (int64_t iy = y0; iy <= y1; ++iy) {
+          const double bx0 = lo_x + ix * cell, by0 = lo_y + iy * cell;
+          const double ex = std::max({bx0 - cx, 0.0, cx - (bx0 + cell)});
+          const double ey = std::max({by0 - cy, 0.0, cy - (by0 + cell)});
+          if (std::sqrt(ex * ex + ey * ey) < reach * (1.0 + 1e-12)) f(ix * gy + iy, k);
+        }
+    }
+  };
+  each([&](int64_t c, int64_t) { ++counts[(size_t)c + 1]; });
+  for (size_t c = 1; c < counts.size(); ++c) counts[c] += counts[c - 1];
+  d->n_items = counts.back();
+  std::vector<double4> items((size_t)std::max<int64_t>(d->n_items, 1));
+  std::vector<int32_t> fill(counts.begin(), counts.end() - 1);
+  each([&](int64_t c, int64_t k) {
+    items[(size_t)fill[(size_t)c]++] = make_double4(centres[2 * k], centres[2 * k + 1], radii[k], 0.0);
+  });
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaMalloc(&d->cstart, sizeof(int32_t) * counts.size());
+  if (e == cudaSuccess) e = cudaMalloc(&d->items, sizeof(double4) * items.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpy(d->cstart, counts.data(), sizeof(int32_t) * counts.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d->items, items.data(), sizeof(double4) * items.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d->cstart);
+    cudaFree(d->items);
+    delete d;
+    return cuda_fail(e, "wsb_disks_create");
+  }
+  *out = reinterpret_cast<wsb_disks*>(d);
+  return WSB_OK;
+}
+
+extern "C" int wsb_disks_destroy(wsb_disks* d_) {
+  Disks* d = reinterpret_cast<Disks*>(d_);
+  if (!d) return WSB_OK;
+  cudaSetDevice(d->device);
+  cudaFree(d->cstart);
+  cudaFree(d->items);
+  delete d;
+  return WSB_OK;
+}
+
+extern "C" int wsb_disk_aggregate(const wsb_disks* d_, int kernel, const double* pos, const double* sup,
+                                  const int32_t* allowed, int64_t n, const double* pose, int out_mask, double* lam,
+                                  double* G, double* cov, double* m1, double* m2, void* stream) {
+  const Disks* d = reinterpret_cast<const Disks*>(d_);
+  if (!d) return fail(WSB_ERR_ARG, "wsb_disk_aggregate: NULL disks");
+  if (kernel < 0 || kernel >= kNumKernels)
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_disk_aggregate: kernel id " + std::to_string(kernel) +
+                                         " has no disk element (exact-table kernels only)");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_disk_aggregate: row count out of range");
+  if (n == 0) return WSB_OK;
+  if (!pos || !sup || !pose) return fail(WSB_ERR_ARG, "wsb_disk_aggregate: NULL array");
+  WSB_CUDA(cudaSetDevice(d->device));
+  const bool assign = (out_mask & WSB_OUT_ASSIGN) != 0;
+  double* L = (out_mask & WSB_OUT_LAM) ? lam : nullptr;
+  double* Gp = (out_mask & WSB_OUT_G) ? G : nullptr;
+  double* C = (out_mask & WSB_OUT_COV) ? cov : nullptr;
+  double* M1 = (out_mask & WSB_OUT_M1) ? m1 : nullptr;
+  double* M2 = (out_mask & WSB_OUT_M2) ? m2 : nullptr;
+  const unsigned grid = (unsigned)((n + kDiskThreads - 1) / kDiskThreads);
+  k_disk<<<grid, kDiskThreads, 0, (cudaStream_t)stream>>>(kDiskTables[kernel], d->cstart, d->items, d->nx, d->ny,
+                                                          d->lo_x, d->lo_y, d->cell, pos, sup, allowed, n, pose,
+                                                          assign, L, Gp, C, M1, M2);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}

@@ -434,12 +434,53 @@ def emit_header() -> str:
     out.append("static const double kPlanRadii[kPlanNumRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
     out.append("")
     out.extend(emit_quad())
+    out.extend(emit_disk())
     out.extend(emit_radial())
     out.extend(emit_mesh())
     out.extend(emit_triangle())
     out.append("}  // namespace wsb")
     out.append("")
     return "\n".join(out)
+
+
+DISK_MAX_BLOCKS = 3
+DISK_MAX_COEF = 16
+
+
+def emit_disk() -> list:
+    """the disk element's profile table: per exact kernel id its truncated blocks of pi*W -- radius R, P, the value
+    potential M(r)/r^2 (M = int_0^r t P dt), the second potential MPsi(r)/r^2 and the constants M(R), MPsi(R) that
+    continue them past R -- as literal data for a kernel argument (host-side array, copied by value per launch)."""
+    out = ["// ---- disk element: per kernel id the truncated blocks of pi*W (radius, P, M/r^2, MPsi/r^2, M(R), MPsi(R))",
+           f"constexpr int kDiskMaxBlocks = {DISK_MAX_BLOCKS};", f"constexpr int kDiskMaxCoef = {DISK_MAX_COEF};",
+           "struct DiskBlock {",
+           "  double R, Mhat, MPhat;",
+           "  int np, nl, nf;",
+           "  double P[kDiskMaxCoef], L[kDiskMaxCoef], F[kDiskMaxCoef];",
+           "};",
+           "struct DiskTable {",
+           "  int nb;",
+           "  DiskBlock b[kDiskMaxBlocks];",
+           "};",
+           "static const DiskTable kDiskTables[kNumKernels] = {"]
+
+    def arr(c):
+        c = list(c) + [F(0)] * (DISK_MAX_COEF - len(c))
+        return "{" + ", ".join(_lit(x) for x in c) + "}"
+
+    for kid in range(len(KERNEL_IDS)):
+        k = kernel(KERNEL_NAMES[kid])
+        if len(k.blocks) > DISK_MAX_BLOCKS or any(max(len(b.c), len(b.flam), len(b.fpsi)) > DISK_MAX_COEF
+                                                  for b in k.blocks):
+            raise AssertionError(f"disk table of {k.name} exceeds its bounds")
+        blocks = []
+        for b in k.blocks:
+            blocks.append(f"{{{_lit(b.R)}, {_lit(b.Mhat)}, {_lit(b.MPhat)}, {len(b.c)}, {len(b.flam)}, {len(b.fpsi)}, "
+                          f"{arr(b.c)}, {arr(b.flam)}, {arr(b.fpsi)}}}")
+        out.append(f"  {{{len(k.blocks)}, {{" + ", ".join(blocks) + "}},   // " + k.name)
+    out.append("};")
+    out.append("")
+    return out
 
 
 # the Wendland C2 / C4 shapes in u = 1 - q (src/warpSPHBoundaries/edge/kernels.py:217-219): u^p0 B(u)

@@ -33,7 +33,7 @@ from .fixedadj import body_candidates, fixed_adjacency
 from .kernels import KERNEL_IDS, QUAD_KERNEL_IDS
 
 _GROUP_IDS = {**KERNEL_IDS, **QUAD_KERNEL_IDS}     # every kernel a FusedWall group may name
-from .scene import Scene, SurfaceRep, _stream
+from .scene import DiskArrayRep, Scene, SurfaceRep, _stream
 from .shim import (GradientScheme, KernelFunctions, OperationDirection, OperationProperties, WarpOperation, kernelName,
                    queryAllowed)
 
@@ -101,9 +101,15 @@ class FusedWall(WallAggregate):
         if getattr(scene, "_wsb_checked", None) != sig:
             for b in scene.bodies:
                 for r in b.fused_reps(self.support, self.dev):
-                    if r._triangle is not None and route != "fused":
+                    if isinstance(r, DiskArrayRep):
+                        if route != "fused":
+                            raise NotImplementedError("FusedWall: disk sets take the fused route")
+                    elif r._triangle is not None and route != "fused":
                         raise NotImplementedError("FusedWall: conditioned single triangles take the fused route")
             scene._wsb_checked = sig
+        if any(g.kernel in QUAD_KERNEL_IDS for g in self.groups) and any(
+                isinstance(r, DiskArrayRep) for b in scene.bodies for r in b.fused_reps(self.support, self.dev)):
+            raise NotImplementedError("FusedWall: the tensile groups have no disk element")
         self.res = []
         self.qstatus = {}                      # (group, body, rep) -> [N] int32 of conditioned triangles
         self.estimates = {}                    # (group, body, rep) -> [N, 12] quadrature estimates
@@ -146,13 +152,22 @@ class FusedWall(WallAggregate):
             pose = body.pose_tensor(self.dev)
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
             for ri, rep in enumerate(body.fused_reps(self.support, self.dev)):
+                mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)     # the first representation assigns
+                if isinstance(rep, DiskArrayRep):
+                    nd = rep.native(self.support, self.dev)
+                    for gi, kid in enumerate(kids):
+                        o = outs[gi]
+                        check(lib.wsb_disk_aggregate(nd.handle, kid, ptr(pos), ptr(sup), ptr(al), N, ptr(pose), mode,
+                                                     ptr(o["lam"][bi]), ptr(o["G"][bi]), ptr(o["Cov"][bi]),
+                                                     ptr(o["m1"][bi]), ptr(o["m2"][bi]), _stream()),
+                              "wsb_disk_aggregate")
+                    continue
                 ns = rep.native(self.support, self.dev)
                 if self.workspaces is not None:
                     ws = self.workspaces[id(rep)]
                     need = ws.numel()
                 else:
                     ws, need = ns.workspace(N)
-                mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)     # the first surface of a body assigns
                 if rep._triangle is None:
                     tgt = {k: _lib.ptrs([out[k][bi] for out in outs]) for k in names}
                     check(lib.wsb_aggregate_groups(ns.handle, len(kids), _lib.int32s(kids), _PREC[self.precision],
@@ -282,6 +297,9 @@ class FusedWall(WallAggregate):
             pose = body.pose_tensor(self.dev)
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
             for rep in body.fused_reps(self.support, self.dev):
+                if isinstance(rep, DiskArrayRep):
+                    raise NotImplementedError("FusedWall: the cone area and direction extreme of disk sets "
+                                              "(fused.py:754-785, 801-819) are not built")
                 ns = rep.native(self.support, self.dev)
                 if self.workspaces is not None:
                     ws = self.workspaces[id(rep)]

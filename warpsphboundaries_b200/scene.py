@@ -295,12 +295,81 @@ class BoxRep(SurfaceRep):
         return -sd, -face
 
 
+class NativeDisks:
+    """the device-resident cell grid of a disk set for supports <= support_max (wsb_disks)."""
+
+    def __init__(self, centres, radii, support_max, device):
+        c = np.ascontiguousarray(centres.detach().cpu().numpy(), dtype=np.float64).reshape(-1)
+        r = np.ascontiguousarray(radii.detach().cpu().numpy(), dtype=np.float64).reshape(-1)
+        self.device = torch.device(device)
+        idx = self.device.index if self.device.index is not None else torch.cuda.current_device()
+        h = ctypes.c_void_p()
+        check(lib.wsb_disks_create(c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                   r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r), float(support_max), idx,
+                                   ctypes.byref(h)), "wsb_disks_create")
+        self.handle = h
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and lib is not None:
+            lib.wsb_disks_destroy(h)
+            self.handle = None
+
+
+class DiskArrayRep:
+    """solid disks in the body frame, centres [M, 2] and radii [M] (scene.py:808-905): a fibre bundle moving as one
+    body; the disks must not overlap (their integrals add).  Every (particle, disk) pair within reach is integrated
+    exactly by the disk element (wsb_disk_aggregate) -- no polygon, any radius."""
+    kind = "disks"
+
+    def __init__(self, centres, radii):
+        self.centres = torch.as_tensor(centres, dtype=F64).reshape(-1, 2)
+        self.radii = torch.as_tensor(radii, dtype=F64).reshape(-1)
+        if len(self.centres) != len(self.radii):
+            raise ValueError("DiskArrayRep: centres and radii differ in length")
+        if len(self.radii) and not bool((self.radii > 0).all()):
+            raise ValueError("DiskArrayRep: every radius must be positive")
+        self._native = {}
+
+    def to(self, device):
+        self.centres, self.radii = self.centres.to(device), self.radii.to(device)
+        return self
+
+    def bounds(self):
+        c, r = self.centres.cpu(), self.radii.cpu()[:, None]
+        return (c - r).amin(0), (c + r).amax(0)
+
+    def native(self, supportMax, device) -> NativeDisks:
+        dev = torch.device(device)
+        if dev.type != "cuda":
+            raise RuntimeError("DiskArrayRep: the boundary integrals run on CUDA devices only (no CPU fallback)")
+        key = (float(supportMax), str(dev))
+        nd = self._native.get(key)
+        if nd is None:
+            nd = NativeDisks(self.centres, self.radii, float(supportMax), dev)
+            self._native[key] = nd
+        return nd
+
+    def signed(self, lpos, chunk=1 << 16):
+        """(d, n) of body-frame points: the distance to the nearest circle, negative inside a disk, and the unit
+        normal into the fluid (radially outward from that disk's centre)."""
+        c, r = self.centres.to(lpos.device), self.radii.to(lpos.device)
+        d = torch.empty(len(lpos), dtype=F64, device=lpos.device)
+        n = torch.empty((len(lpos), 2), dtype=F64, device=lpos.device)
+        for k in range(0, len(lpos), chunk):
+            v = lpos[k:k + chunk, None, :] - c[None]
+            dist = v.norm(dim=2)
+            j = (dist - r[None]).argmin(1)
+            rows = torch.arange(len(j), device=lpos.device)
+            d[k:k + chunk] = dist[rows, j] - r[j]
+            n[k:k + chunk] = v[rows, j] / dist[rows, j].clamp(min=1e-300)[:, None]
+        return d, n
+
 class ImplicitRep:
-    """an analytic primitive in the body frame (scene.py:558-596).  The fused wall path integrates its exact polygon
-    form: a cavity disk (fluid inside the circle) is its area-preserving regular polygon with edges <= the policy's
-    bound times the support (at least 24 edges), integrated exactly like any surface.  A solid disk is the
-    reference's disk element (a table lookup per (query, disk)) and a half plane has no polygon form: both raise
-    NotImplementedError on the fused path."""
+    """an analytic primitive in the body frame (scene.py:558-596).  The fused wall path integrates its exact form: a
+    solid disk is a one-disk DiskArrayRep (the disk element), a cavity disk (fluid inside the circle) its
+    area-preserving regular polygon with edges <= the policy's bound times the support (at least 24 edges), integrated
+    exactly like any surface.  A half plane has no such form: NotImplementedError on the fused path."""
     kind = "implicit"
 
     def __init__(self, shape, policy=None):
@@ -335,9 +404,14 @@ class ImplicitRep:
             raise NotImplementedError("FusedWall: a half plane has no polygon form (the reference serves it by its "
                                       "per-operation path, not the fused wall)")
         if self.shape.solid == "inside":
-            raise NotImplementedError("FusedWall: a solid disk is the disk element (DiskArrayRep tables), which is "
-                                      "not built; a polygon SurfaceRep of the disk is served")
+            return self.disks().to(device)
         return self.fallbackSurface(hmin, device)
+
+    def disks(self):
+        """a solid disk as a one-disk DiskArrayRep, cached (scene.py:576-580)."""
+        if getattr(self, "_disks", None) is None:
+            self._disks = DiskArrayRep([self.shape.center], [self.shape.radius])
+        return self._disks
 
     def fallbackSurface(self, hmin, device):
         """the area-preserving regular polygon with n = max(24, ceil(2 pi R / (edge bound * hmin))) edges, cached per
@@ -556,20 +630,20 @@ class Body:
 
     def fusable(self):
         from .implicit import DiskBody
-        return all(isinstance(r, (SurfaceRep, SdfRep)) or
-                   (isinstance(r, ImplicitRep) and isinstance(r.shape, DiskBody) and r.shape.solid == "outside")
-                   for r in self.reps)
+        return all(isinstance(r, (SurfaceRep, SdfRep, DiskArrayRep)) or
+                   (isinstance(r, ImplicitRep) and isinstance(r.shape, DiskBody)) for r in self.reps)
 
     def fused_reps(self, hmin, device):
-        """the representations as the surfaces the fused wall evaluation integrates exactly (scene.py:970-997):
-        SurfaceRep and BoxRep as they are, ImplicitRep and SdfRep lowered to their polygon; cached per (hmin,
-        device).  NotImplementedError for a representation without that form."""
+        """the representations as the fused wall evaluation integrates them exactly (scene.py:970-997): SurfaceRep,
+        BoxRep and DiskArrayRep as they are, ImplicitRep and SdfRep lowered (a solid disk to a disk set, a cavity or
+        a sampled distance to a polygon); cached per (hmin, device).  NotImplementedError for a representation
+        without such a form."""
         cache = self.__dict__.setdefault("_fusedCache", {})
         key = (float(hmin), str(device), tuple(id(r) for r in self.reps))
         if key not in cache:
             out = []
             for r in self.reps:
-                if isinstance(r, SurfaceRep):
+                if isinstance(r, (SurfaceRep, DiskArrayRep)):
                     out.append(r)
                 elif isinstance(r, (ImplicitRep, SdfRep)):
                     out.append(r.lowered(hmin, device))
@@ -657,7 +731,7 @@ class Scene:
             for rep in bd.reps:
                 if isinstance(rep, SdfRep):
                     rep = rep.lowered(0.0, self.device)        # the exact distance to its polygon form
-                if isinstance(rep, (BoxRep, ImplicitRep)):
+                if isinstance(rep, (BoxRep, ImplicitRep, DiskArrayRep)):
                     # the shape's own closed form and normals (scene.py:1351-1353, 1360-1362)
                     d, nl = rep.signed(lp)
                     n = bd.pose.vecToWorld(nl)
@@ -696,7 +770,7 @@ class Scene:
             for rep in bd.reps:
                 if isinstance(rep, SdfRep):
                     rep = rep.lowered(0.0, self.device)
-                if isinstance(rep, ImplicitRep):
+                if isinstance(rep, (ImplicitRep, DiskArrayRep)):
                     out |= rep.signed(lp)[0] < 0
                 elif isinstance(rep, SurfaceRep):
                     out |= rep.indicator(lp) > 0.5
