@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-mesh", action="store_true", help="skip the 3-D closed-surface leg")
-    p.add_argument("--leg", choices=["all", "radial", "mesh3d", "serving"], default="all",
+    p.add_argument("--leg", choices=["all", "radial", "mesh3d", "serving", "disks"], default="all",
                    help="run one side leg alone (prints its JSON object; for profiling)")
     p.add_argument("--mesh-particles", type=int, default=1 << 21, help="particles of the 3-D closed-surface leg")
     p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
@@ -373,6 +373,68 @@ def detector_run(ns, pos, sup, pose, obb, ws, need, pairs, stream, flush, steps=
                         "pi/3; f64", "pairs": pairs, **res, "kernels": ["k_cone_area", "k_dir_extreme"]}
 
 
+def disk_run(dev, stream, flush, steps=5, kernel="w4", n_particles=1 << 20):
+    """a fibre bundle: 1024 non-overlapping solid disks, radii U(0.5h, 5h), in [0, 4]^2, h = 0.02, 2^20 particles
+    uniform in [0, 4]^2, the twelve channels of every particle (wsb_disk_aggregate), float64, inputs resident; CUDA
+    events around the call, L2 flushed before each."""
+    import ctypes
+
+    import torch
+    from warpsphboundaries_b200 import _lib
+    from warpsphboundaries_b200.scene import DiskArrayRep
+    from warpsphboundaries_b200.kernels import KERNEL_IDS
+    rng = np.random.default_rng(31)
+    h = 0.02
+    C, R = [], []
+    grid = {}
+    while len(C) < 1024:                               # rejection sampling on a coarse hash of the centres
+        r = float(rng.uniform(0.5 * h, 5 * h))
+        c = rng.uniform(r, 4.0 - r, 2)
+        key = (int(c[0] / (12 * h)), int(c[1] / (12 * h)))
+        near = [j for dx in (-1, 0, 1) for dy in (-1, 0, 1) for j in grid.get((key[0] + dx, key[1] + dy), ())]
+        if all(math.hypot(*(c - C[j])) > r + R[j] + 0.1 * h for j in near):
+            grid.setdefault(key, []).append(len(C))
+            C.append(c)
+            R.append(r)
+    rep = DiskArrayRep(np.array(C), np.array(R)).to(dev)
+    nd = rep.native(h, dev)
+    n = n_particles
+    X = rng.uniform(0.0, 4.0, (n, 2))
+    pos = torch.tensor(X, dtype=torch.float64, device=dev)
+    sup = torch.full((n,), h, dtype=torch.float64, device=dev)
+    pose = torch.tensor([0.0, 0.0, 1.0, 0.0], dtype=torch.float64, device=dev)
+    out = [torch.empty(n * k, dtype=torch.float64, device=dev) for k in (1, 2, 4, 2, 4)]
+    st = ctypes.c_void_p(stream.cuda_stream)
+    ws, need = nd.workspace(n)
+    args = (nd.handle, KERNEL_IDS[kernel], _lib.ptr(pos), _lib.ptr(sup), None, n, _lib.ptr(pose),
+            _lib.OUT_ALL | _lib.OUT_ASSIGN, *[_lib.ptr(o) for o in out], _lib.ptr(ws), need, st)
+    for _ in range(3):
+        _lib.check(_lib.lib.wsb_disk_aggregate(*args), "wsb_disk_aggregate")
+    tot = 0.0
+    for _ in range(steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(_lib.lib.wsb_disk_aggregate(*args), "wsb_disk_aggregate")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+    ms = tot / steps
+    # (particle, disk) pairs within reach, counted once on the host from a sample
+    Cn, Rn = np.array(C), np.array(R)
+    samp = X[:: max(1, n // 65536)]
+    pairs = 0
+    for k in range(0, len(samp), 4096):
+        D = np.hypot(samp[k:k + 4096, None, 0] - Cn[None, :, 0], samp[k:k + 4096, None, 1] - Cn[None, :, 1])
+        pairs += int((D < Rn[None] + h).sum())
+    pairs = pairs * n / len(samp)
+    return {"workload": f"1024 solid disks (r U(0.5h, 5h)) in [0,4]^2, {n} particles, h=0.02, {kernel}, 12 channels, "
+                        "f64", "ms": ms, "particles_per_s": n / (ms * 1e-3), "pairs_est": pairs,
+            "pairs_per_s": pairs / (ms * 1e-3), "kernels": ["k_disk_rows", "k_disk_warp"]}
+
+
 def mesh_run(dev, stream, flush, steps=5, kernel="w4", n_particles=1 << 21):
     """the 3-D scene: 2^21 particles uniform in [-1, 1]^3, h = 0.03, a jittered icosphere of 20480 faces (radius 0.6),
     the 28 baseline channels of every particle, float64, inputs resident; CUDA events around wsb_mesh_channels."""
@@ -680,6 +742,7 @@ def our_arm(args):
 
     radial = radial_run(dev, stream, flush) if world == 1 else None
     detector = detector_run(ns, pos, sup, pose, obb, ws, need, P, stream, flush) if world == 1 else None
+    disks = disk_run(dev, stream, flush) if world == 1 else None
     mesh = mesh_run(dev, stream, flush, n_particles=args.mesh_particles) if world == 1 and not args.no_mesh else None
 
     serving = None
@@ -709,7 +772,7 @@ def our_arm(args):
                 "kernel_ms_separate": sep_ms,
                 "gpu_launches": args.steps * (5 + 1),   # prepare: 5 kernels; one pair kernel for the four groups
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh, "adjoint": adjoint,
-                "detector": detector,
+                "detector": detector, "disks": disks,
                 **({"extra": extra} if extra else {})}
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -728,6 +791,8 @@ def side_leg(args):
         res = radial_run(dev, stream, flush, steps=args.steps)
     elif args.leg == "serving":
         res = serving_run(args.serve_requests, dev, 2.09)
+    elif args.leg == "disks":
+        res = disk_run(dev, stream, flush, steps=args.steps)
     else:
         res = mesh_run(dev, stream, flush, steps=args.steps, n_particles=args.mesh_particles)
     print(json.dumps({"leg": args.leg, **res}), flush=True)

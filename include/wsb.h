@@ -251,9 +251,10 @@ int wsb_triangle_combine(const double* values, const int32_t* status, const doub
  * on the host, copied to `device` with a cell grid (cell >= support_max) listing every disk that reaches each cell.
  * wsb_disk_aggregate writes the twelve channels of the disks at every particle exactly as wsb_aggregate writes those
  * of a surface (body frame from `pose`, world-frame outputs, out_mask with WSB_OUT_ASSIGN for the first
- * representation of a body; rows outside `allowed` get zeros), for the exact-table kernel ids (0 .. 9).  The
- * integrals are evaluated by graded Gauss-Legendre quadrature along the disk's circle inside the support (float64,
- * ~1e-13), where the reference looks them up in Chebyshev tables (~1e-6 .. 1e-10).  Replaces DiskArrayRep's fixed
+ * representation of a body; rows outside `allowed` get zeros), for the exact-table kernel ids (0 .. 9), on a
+ * caller workspace of wsb_disk_workspace_size bytes (4 bytes per row).  The integrals are evaluated by graded
+ * Gauss-Legendre quadrature along the disk's circle inside the support (float64, ~1e-13), one warp per particle
+ * that reaches a disk, where the reference looks them up in Chebyshev tables (~1e-6 .. 1e-10).  Replaces DiskArrayRep's fixed
  * disk topology and the disk channel launch (src/warpSPHBoundaries/scene/fixedadj.py:199-246,
  * edge/warpdisk.py:1-199, scene/fused.py:566-574); a solid ImplicitRep disk is a one-disk set
  * (scene/scene.py:576-580). */
@@ -261,9 +262,10 @@ typedef struct wsb_disks wsb_disks;
 int wsb_disks_create(const double* centres, const double* radii, int64_t m, double support_max, int device,
                      wsb_disks** out);
 int wsb_disks_destroy(wsb_disks* d);
+size_t wsb_disk_workspace_size(const wsb_disks* d, int64_t n);
 int wsb_disk_aggregate(const wsb_disks* d, int kernel, const double* pos, const double* sup, const int32_t* allowed,
                        int64_t n, const double* pose, int out_mask, double* lam, double* G, double* cov, double* m1,
-                       double* m2, void* stream);
+                       double* m2, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- closed triangle surfaces (3-D) ----
  * A watertight, consistently oriented triangle surface with outward normals (positive signed volume): verts

@@ -23,7 +23,8 @@ EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_d
            "wsb_aggregate_backward", "wsb_cone_area", "wsb_dir_extreme", "wsb_signed_distance",
            "wsb_kinematics", "wsb_radial_channels", "wsb_mesh_create", "wsb_mesh_destroy",
            "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels", "wsb_triangle_channels",
-           "wsb_triangle_combine", "wsb_disks_create", "wsb_disks_destroy", "wsb_disk_aggregate"]
+           "wsb_triangle_combine", "wsb_disks_create", "wsb_disks_destroy", "wsb_disk_workspace_size",
+           "wsb_disk_aggregate"]
 
 
 class SurfaceInfo(ctypes.Structure):
@@ -76,7 +77,8 @@ def _load():
         "wsb_triangle_combine": (c_int, [P, P, P, P, c_int64, c_int, P, P, P, P, P, P, P, P, P, P, P]),
         "wsb_disks_create": (c_int, [D, D, c_int64, c_double, c_int, POINTER(c_void_p)]),
         "wsb_disks_destroy": (c_int, [P]),
-        "wsb_disk_aggregate": (c_int, [P, c_int, P, P, P, c_int64, P, c_int, P, P, P, P, P, P]),
+        "wsb_disk_workspace_size": (c_size_t, [P, c_int64]),
+        "wsb_disk_aggregate": (c_int, [P, c_int, P, P, P, c_int64, P, c_int, P, P, P, P, P, P, c_size_t, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

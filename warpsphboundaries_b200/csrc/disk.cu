@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdint>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -39,33 +40,18 @@ struct Disks {
 
 constexpr int kDiskThreads = 128;
 
-// the value potential F1/r^2, the second potential F2/r^2 and P at r (sums over the truncated blocks)
-__device__ __forceinline__ void disk_profile(const DiskTable& T, double r, double& P, double& Fl, double& F2l) {
-  P = 0.0;
-  Fl = 0.0;
-  F2l = 0.0;
-  const double ir2 = 1.0 / (r * r);
-  for (int k = 0; k < T.nb; ++k) {
-    const DiskBlock& b = T.b[k];
-    F2l += 0.5 * b.Mhat;
-    if (r <= b.R) {
-      double p = 0.0, l = 0.0, f = 0.0;
-      for (int j = b.np - 1; j >= 0; --j) p = fma(p, r, b.P[j]);
-      for (int j = b.nl - 1; j >= 0; --j) l = fma(l, r, b.L[j]);
-      for (int j = b.nf - 1; j >= 0; --j) f = fma(f, r, b.F[j]);
-      P += p;
-      Fl += l;
-      F2l += f;
-    } else {
-      Fl += b.Mhat * ir2;
-      F2l += b.MPhat * ir2;
-    }
-  }
+// the sum over the warp's lanes, in a fixed butterfly order, on every lane
+__device__ __forceinline__ double warp_allsum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
 }
 
 // The seven non-zero channels of one disk in its aligned frame (before 1/pi): lam, m1_x, G_x, g1_xx, g1_yy, m2_xx,
-// m2_yy.  D = centre distance, R = radius (h = 1), D < 1 + R.
-__device__ void disk_pair(const DiskTable& T, double D, double R, double out[7]) {
+// m2_yy.  D = centre distance, R = radius (h = 1), D < 1 + R.  Called by a whole warp with the same (D, R): lane q
+// takes node q of every panel, the eight sums are reduced by a fixed butterfly, every lane returns the totals.
+template <int KID>
+__device__ void disk_pair(double D, double R, int lane, double out[7]) {
   double lam = 0.0, m1 = 0.0, G = 0.0, gxx = 0.0, gyy = 0.0, mxx = 0.0, myy = 0.0, SF = 0.0;
   const double dm = D - R;
   // the arc of the disk's circle inside the support: u in [0, U] (and its mirror image)
@@ -73,16 +59,17 @@ __device__ void disk_pair(const DiskTable& T, double D, double R, double out[7])
     const double U = D + R <= 1.0 ? 0.5 * kTwoPi : 2.0 * asin(fmin(1.0, sqrt((1.0 - dm * dm) / (4.0 * D * R))));
     const double x = 0.5 * dm * dm / (D * R);                  // acosh(1 + x): the distance of the singularity
     const double base = fmax(log1p(x + sqrt(x * (x + 2.0))), 0x1p-24);
-    double knots[kDiskMaxBlocks];
+    double radii[kDiskMaxKnots], knots[kDiskMaxKnots];
+    const int nr = disk_knots<KID>(radii);
     int nk = 0;
-    for (int k = 0; k < T.nb; ++k) {
-      const double Rb = T.b[k].R;
-      if (Rb < 1.0 && fabs(dm) < Rb && Rb < D + R) {
+    for (int k = 0; k < nr; ++k) {
+      const double Rb = radii[k];
+      if (fabs(dm) < Rb && Rb < D + R) {
         const double kn = 2.0 * asin(fmin(1.0, sqrt((Rb * Rb - dm * dm) / (4.0 * D * R))));
         if (kn > 0.0 && kn < U) knots[nk++] = kn;
       }
     }
-    for (int a = 1; a < nk; ++a)                                   // ascending (at most kDiskMaxBlocks - 1 knots)
+    for (int a = 1; a < nk; ++a)                                   // ascending (at most kDiskMaxKnots knots)
       for (int b = a; b > 0 && knots[b] < knots[b - 1]; --b) {
         const double t = knots[b];
         knots[b] = knots[b - 1];
@@ -95,16 +82,16 @@ __device__ void disk_pair(const DiskTable& T, double D, double R, double out[7])
       while (ki < nk && knots[ki] <= u) ++ki;
       if (ki < nk && knots[ki] < nxt) nxt = knots[ki];
       const double hc = 0.5 * (nxt - u), mc = 0.5 * (nxt + u);
-      for (int q = 0; q < kQuadGauss; ++q) {
+      for (int q = lane; q < kQuadGauss; q += 32) {
         const double uu = fma(hc, kQuadGx[q], mc);
-        double su, cu;
-        sincos(uu, &su, &cu);
-        const double sh = sin(0.5 * uu), s2 = sh * sh;
+        double sh, ch;
+        sincos(0.5 * uu, &sh, &ch);                                // one half-angle evaluation per node
+        const double s2 = sh * sh, su = 2.0 * sh * ch, cu = fma(-2.0, s2, 1.0);
         const double yx = fma(2.0 * R, s2, dm), yy = R * su, nx = -cu, ny = su;
         const double yn = fma(2.0 * D, s2, -dm);
         const double r = sqrt(fma(4.0 * D * R, s2, dm * dm));
         double P, Fl, F2l;
-        disk_profile(T, r, P, Fl, F2l);
+        disk_profile<KID>(r, 1.0 / (r * r), P, Fl, F2l);
         const double F1 = Fl * r * r;
         const double w = 2.0 * R * hc * kQuadGw[q];
         lam = fma(w * Fl, yn, lam);
@@ -120,6 +107,14 @@ __device__ void disk_pair(const DiskTable& T, double D, double R, double out[7])
       u = nxt;
     }
   }
+  lam = warp_allsum(lam);
+  m1 = warp_allsum(m1);
+  G = warp_allsum(G);
+  gxx = warp_allsum(gxx);
+  gyy = warp_allsum(gyy);
+  mxx = warp_allsum(mxx);
+  myy = warp_allsum(myy);
+  SF = warp_allsum(SF);
   // the arc of the support circle inside the disk: |phi| < beta
   double beta = -1.0;
   if (R >= D + 1.0)
@@ -128,7 +123,7 @@ __device__ void disk_pair(const DiskTable& T, double D, double R, double out[7])
     beta = 2.0 * asin(fmin(1.0, sqrt((R * R - (D - 1.0) * (D - 1.0)) / (4.0 * D))));
   if (beta > 0.0) {
     double P1, Fl1, F2l1;
-    disk_profile(T, 1.0, P1, Fl1, F2l1);
+    disk_profile<KID>(1.0, 1.0, P1, Fl1, F2l1);
     const double sb = sin(beta), s2b = sin(2.0 * beta);
     const double cxx = beta + 0.5 * s2b, cyy = beta - 0.5 * s2b;
     lam += 2.0 * beta * Fl1;
@@ -149,57 +144,113 @@ __device__ void disk_pair(const DiskTable& T, double D, double R, double out[7])
   out[6] = myy - SF;
 }
 
-// one thread per particle: body frame, the particle's cell, every disk of the cell within reach, the channels of each
-// rotated from its aligned frame and summed in cell-list order, then scaled and rotated to the world frame
-__global__ void __launch_bounds__(kDiskThreads) k_disk(const DiskTable T, const int32_t* __restrict__ cstart,
-                                                      const double4* __restrict__ items, int32_t nx, int32_t ny,
-                                                      double lo_x, double lo_y, double cell,
-                                                      const double* __restrict__ pos, const double* __restrict__ sup,
-                                                      const int32_t* __restrict__ allowed, int64_t n,
-                                                      const double* __restrict__ pose, bool assign, double* lam,
-                                                      double* G, double* cov, double* m1, double* m2) {
+// the body-frame position of particle i and its cell (false outside the grid or outside `allowed`)
+__device__ __forceinline__ bool disk_row(const double* __restrict__ pos, const int32_t* __restrict__ allowed,
+                                         const double* __restrict__ pose, int64_t i, int32_t nx, int32_t ny,
+                                         double lo_x, double lo_y, double cell, double& lx, double& ly, int32_t& cid) {
+  if (allowed && allowed[i] == 0) return false;
+  to_local_rn(pos[2 * i], pos[2 * i + 1], pose[0], pose[1], pose[2], pose[3], lx, ly);
+  const double fx = floor((lx - lo_x) / cell), fy = floor((ly - lo_y) / cell);
+  if (!(fx >= 0.0 && fx < (double)nx && fy >= 0.0 && fy < (double)ny)) return false;
+  cid = (int32_t)fx * ny + (int32_t)fy;
+  return true;
+}
+
+// Pass 1, one thread per particle: a particle that reaches no disk gets its zero channels (when the call assigns);
+// the others are appended to the work list (warp-aggregated).
+__global__ void __launch_bounds__(kDiskThreads) k_disk_rows(const int32_t* __restrict__ cstart,
+                                                           const double4* __restrict__ items, int32_t nx,
+                                                           int32_t ny, double lo_x, double lo_y, double cell,
+                                                           const double* __restrict__ pos,
+                                                           const double* __restrict__ sup,
+                                                           const int32_t* __restrict__ allowed, int64_t n,
+                                                           const double* __restrict__ pose, bool assign,
+                                                           int32_t* __restrict__ work, int32_t* __restrict__ nwork,
+                                                           double* lam, double* G, double* cov, double* m1,
+                                                           double* m2) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double acc[12];
-#pragma unroll
-  for (int c = 0; c < 12; ++c) acc[c] = 0.0;
-  const double h = sup[i];
-  if (!allowed || allowed[i] != 0) {
+  bool has = false;
+  if (i < n) {
     double lx, ly;
-    to_local_rn(pos[2 * i], pos[2 * i + 1], pose[0], pose[1], pose[2], pose[3], lx, ly);
-    const double fx = floor((lx - lo_x) / cell), fy = floor((ly - lo_y) / cell);
-    if (fx >= 0.0 && fx < (double)nx && fy >= 0.0 && fy < (double)ny) {
-      const int32_t cid = (int32_t)fx * ny + (int32_t)fy;
-      const double ih = 1.0 / h;
-      for (int32_t k = cstart[cid]; k < cstart[cid + 1]; ++k) {
+    int32_t cid;
+    if (disk_row(pos, allowed, pose, i, nx, ny, lo_x, lo_y, cell, lx, ly, cid)) {
+      const double ih = 1.0 / sup[i];
+      for (int32_t k = cstart[cid]; k < cstart[cid + 1] && !has; ++k) {
         const double4 e = items[k];
-        const double vx = (e.x - lx) * ih, vy = (e.y - ly) * ih, R = e.z * ih;
-        const double D = sqrt(vx * vx + vy * vy);
-        if (!(D < 1.0 + R)) continue;
-        double o[7];
-        disk_pair(T, D, R, o);
-        const double ca = D > 0.0 ? vx / D : 1.0, sa = D > 0.0 ? vy / D : 0.0;
-        acc[0] += o[0];
-        acc[1] += ca * o[1];
-        acc[2] += sa * o[1];
-        acc[3] += ca * o[2];
-        acc[4] += sa * o[2];
-        const double dg = o[3] - o[4], dmm = o[5] - o[6];
-        acc[5] += ca * ca * o[3] + sa * sa * o[4];
-        acc[6] += ca * sa * dg;
-        acc[7] += ca * sa * dg;
-        acc[8] += sa * sa * o[3] + ca * ca * o[4];
-        acc[9] += ca * ca * o[5] + sa * sa * o[6];
-        acc[10] += ca * sa * dmm;
-        acc[11] += sa * sa * o[5] + ca * ca * o[6];
+        const double vx = (e.x - lx) * ih, vy = (e.y - ly) * ih;
+        has = sqrt(vx * vx + vy * vy) < 1.0 + e.z * ih;
       }
     }
+    if (!has && assign) {
+      double acc[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+      const double c = pose[2], s = pose[3];
+      const double rot[4] = {c, -s, s, c};
+      write_outputs(acc, sup[i], rot, i, lam, G, cov, m1, m2, true);
+    }
   }
+  const unsigned ballot = __ballot_sync(0xffffffffu, has);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && ballot) base = atomicAdd(nwork, __popc(ballot));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (has) work[base + __popc(ballot & ((1u << lane) - 1))] = (int32_t)i;
+}
+
+// Pass 2, one warp per listed particle (grid-stride): every disk of the particle's cell within reach, in cell-list
+// order, integrated by the whole warp, rotated from its aligned frame and summed; lane 0 scales, rotates to the world
+// frame and writes.  Each particle is one warp's work in a fixed order: the result does not depend on the list order.
+template <int KID>
+__global__ void __launch_bounds__(kDiskThreads, 4) k_disk_warp(const int32_t* __restrict__ cstart,
+                                                           const double4* __restrict__ items, int32_t nx,
+                                                           int32_t ny, double lo_x, double lo_y, double cell,
+                                                           const double* __restrict__ pos,
+                                                           const double* __restrict__ sup,
+                                                           const int32_t* __restrict__ work,
+                                                           const int32_t* __restrict__ nwork_p,
+                                                           const double* __restrict__ pose, bool assign, double* lam,
+                                                           double* G, double* cov, double* m1, double* m2) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (kDiskThreads / 32);
+  const int64_t nwork = *nwork_p;
+  for (int64_t j = (int64_t)blockIdx.x * (kDiskThreads / 32) + threadIdx.x / 32; j < nwork; j += warps) {
+    const int64_t i = work[j];
+    double lx, ly;
+    int32_t cid = 0;
+    disk_row(pos, nullptr, pose, i, nx, ny, lo_x, lo_y, cell, lx, ly, cid);   // listed: inside the grid
+    const double h = sup[i], ih = 1.0 / h;
+    double acc[12];
 #pragma unroll
-  for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
-  const double c = pose[2], s = pose[3];
-  const double rot[4] = {c, -s, s, c};
-  write_outputs(acc, h, rot, i, lam, G, cov, m1, m2, assign);
+    for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+    for (int32_t k = cstart[cid]; k < cstart[cid + 1]; ++k) {
+      const double4 e = items[k];
+      const double vx = (e.x - lx) * ih, vy = (e.y - ly) * ih, R = e.z * ih;
+      const double D = sqrt(vx * vx + vy * vy);
+      if (!(D < 1.0 + R)) continue;
+      double o[7];
+      disk_pair<KID>(D, R, lane, o);
+      const double ca = D > 0.0 ? vx / D : 1.0, sa = D > 0.0 ? vy / D : 0.0;
+      acc[0] += o[0];
+      acc[1] += ca * o[1];
+      acc[2] += sa * o[1];
+      acc[3] += ca * o[2];
+      acc[4] += sa * o[2];
+      const double dg = o[3] - o[4], dmm = o[5] - o[6];
+      acc[5] += ca * ca * o[3] + sa * sa * o[4];
+      acc[6] += ca * sa * dg;
+      acc[7] += ca * sa * dg;
+      acc[8] += sa * sa * o[3] + ca * ca * o[4];
+      acc[9] += ca * ca * o[5] + sa * sa * o[6];
+      acc[10] += ca * sa * dmm;
+      acc[11] += sa * sa * o[5] + ca * ca * o[6];
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
+      const double c = pose[2], s = pose[3];
+      const double rot[4] = {c, -s, s, c};
+      write_outputs(acc, h, rot, i, lam, G, cov, m1, m2, assign);
+    }
+  }
 }
 
 }  // namespace wsb
@@ -305,9 +356,17 @@ extern "C" int wsb_disks_destroy(wsb_disks* d_) {
   return WSB_OK;
 }
 
+static inline size_t disk_align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+extern "C" size_t wsb_disk_workspace_size(const wsb_disks* d, int64_t n) {
+  if (!d || n < 0) return 0;
+  return disk_align256(sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1)) + 256;
+}
+
 extern "C" int wsb_disk_aggregate(const wsb_disks* d_, int kernel, const double* pos, const double* sup,
                                   const int32_t* allowed, int64_t n, const double* pose, int out_mask, double* lam,
-                                  double* G, double* cov, double* m1, double* m2, void* stream) {
+                                  double* G, double* cov, double* m1, double* m2, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
   const Disks* d = reinterpret_cast<const Disks*>(d_);
   if (!d) return fail(WSB_ERR_ARG, "wsb_disk_aggregate: NULL disks");
   if (kernel < 0 || kernel >= kNumKernels)
@@ -316,17 +375,46 @@ extern "C" int wsb_disk_aggregate(const wsb_disks* d_, int kernel, const double*
   if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_disk_aggregate: row count out of range");
   if (n == 0) return WSB_OK;
   if (!pos || !sup || !pose) return fail(WSB_ERR_ARG, "wsb_disk_aggregate: NULL array");
+  const size_t need = wsb_disk_workspace_size(d_, n);
+  if (!workspace || workspace_bytes < need)
+    return fail(WSB_ERR_SIZE, "wsb_disk_aggregate: workspace of " + std::to_string(workspace_bytes) +
+                                  " bytes, need " + std::to_string(need));
   WSB_CUDA(cudaSetDevice(d->device));
+  cudaStream_t st = (cudaStream_t)stream;
   const bool assign = (out_mask & WSB_OUT_ASSIGN) != 0;
   double* L = (out_mask & WSB_OUT_LAM) ? lam : nullptr;
   double* Gp = (out_mask & WSB_OUT_G) ? G : nullptr;
   double* C = (out_mask & WSB_OUT_COV) ? cov : nullptr;
   double* M1 = (out_mask & WSB_OUT_M1) ? m1 : nullptr;
   double* M2 = (out_mask & WSB_OUT_M2) ? m2 : nullptr;
+  int32_t* work = static_cast<int32_t*>(workspace);
+  int32_t* nwork = reinterpret_cast<int32_t*>(static_cast<char*>(workspace) + need - 256);
+  WSB_CUDA(cudaMemsetAsync(nwork, 0, sizeof(int32_t), st));
   const unsigned grid = (unsigned)((n + kDiskThreads - 1) / kDiskThreads);
-  k_disk<<<grid, kDiskThreads, 0, (cudaStream_t)stream>>>(kDiskTables[kernel], d->cstart, d->items, d->nx, d->ny,
-                                                          d->lo_x, d->lo_y, d->cell, pos, sup, allowed, n, pose,
-                                                          assign, L, Gp, C, M1, M2);
+  k_disk_rows<<<grid, kDiskThreads, 0, st>>>(d->cstart, d->items, d->nx, d->ny, d->lo_x, d->lo_y, d->cell, pos, sup,
+                                             allowed, n, pose, assign, work, nwork, L, Gp, C, M1, M2);
+  // warps per listed particle, grid-stride: at most 16 blocks of 4 warps per SM, never more warps than particles
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d->device);
+  const int64_t wgrid = std::min<int64_t>((n + 3) / 4, (int64_t)sms * 16);
+  auto launch = [&](auto kid) {
+    k_disk_warp<decltype(kid)::value><<<(unsigned)wgrid, kDiskThreads, 0, st>>>(
+        d->cstart, d->items, d->nx, d->ny, d->lo_x, d->lo_y, d->cell, pos, sup, work, nwork, pose, assign, L, Gp, C,
+        M1, M2);
+  };
+  switch (kernel) {
+    case 0: launch(std::integral_constant<int, 0>{}); break;
+    case 1: launch(std::integral_constant<int, 1>{}); break;
+    case 2: launch(std::integral_constant<int, 2>{}); break;
+    case 3: launch(std::integral_constant<int, 3>{}); break;
+    case 4: launch(std::integral_constant<int, 4>{}); break;
+    case 5: launch(std::integral_constant<int, 5>{}); break;
+    case 6: launch(std::integral_constant<int, 6>{}); break;
+    case 7: launch(std::integral_constant<int, 7>{}); break;
+    case 8: launch(std::integral_constant<int, 8>{}); break;
+    case 9: launch(std::integral_constant<int, 9>{}); break;
+    default: return fail(WSB_ERR_UNSUPPORTED, "wsb_disk_aggregate: unknown kernel id");
+  }
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }

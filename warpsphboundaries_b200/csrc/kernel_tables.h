@@ -734,30 +734,216 @@ struct Kern_w4p5 {
   }
 };
 
-// ---- disk element: per kernel id the truncated blocks of pi*W (radius, P, M/r^2, MPsi/r^2, M(R), MPsi(R))
-constexpr int kDiskMaxBlocks = 3;
-constexpr int kDiskMaxCoef = 16;
-struct DiskBlock {
-  double R, Mhat, MPhat;
-  int np, nl, nf;
-  double P[kDiskMaxCoef], L[kDiskMaxCoef], F[kDiskMaxCoef];
-};
-struct DiskTable {
-  int nb;
-  DiskBlock b[kDiskMaxBlocks];
-};
-static const DiskTable kDiskTables[kNumKernels] = {
-  {2, {{1.0, 0.5714285714285714, -0.04081632653061224, 4, 4, 6, {11.428571428571429, -34.285714285714285, 34.285714285714285, -11.428571428571429, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {5.714285714285714, -11.428571428571429, 8.571428571428571, -2.2857142857142856, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.2857142857142857, 0.0, 1.4285714285714286, -2.2857142857142856, 1.4285714285714286, -0.32653061224489793, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}, {0.5, -0.07142857142857142, 0.0012755102040816326, 4, 4, 6, {-5.714285714285714, 34.285714285714285, -68.57142857142857, 45.714285714285715, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-2.857142857142857, 11.428571428571429, -17.142857142857142, 9.142857142857142, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {0.03571428571428571, 0.0, -0.7142857142857143, 2.2857142857142856, -2.857142857142857, 1.3061224489795917, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // cubic
-  {1, {{1.0, 0.5, -0.034722222222222224, 6, 6, 8, {7.0, 0.0, -70.0, 140.0, -105.0, 28.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {3.5, 0.0, -17.5, 28.0, -17.5, 4.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.25, 0.0, 0.875, 0.0, -2.9166666666666665, 4.0, -2.1875, 0.4444444444444444, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // w2
-  {1, {{1.0, 0.5, -0.026515151515151516, 9, 9, 11, {9.0, 0.0, -84.0, 0.0, 630.0, -1344.0, 1260.0, -576.0, 105.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {4.5, 0.0, -21.0, 0.0, 105.0, -192.0, 157.5, -64.0, 10.5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.25, 0.0, 1.125, 0.0, -3.5, 0.0, 13.125, -21.333333333333332, 15.75, -5.818181818181818, 0.875, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // w4
-  {1, {{1.0, 0.5, -0.02142857142857143, 12, 12, 14, {11.142857142857142, 0.0, -122.57142857142857, 0.0, 735.4285714285714, 0.0, -5148.0, 11766.857142857143, -12870.0, 7844.571428571428, -2574.0, 356.57142857142856, 0.0, 0.0, 0.0, 0.0}, {5.571428571428571, 0.0, -30.642857142857142, 0.0, 122.57142857142857, 0.0, -643.5, 1307.4285714285713, -1287.0, 713.1428571428571, -214.5, 27.428571428571427, 0.0, 0.0, 0.0, 0.0}, {-0.25, 0.0, 1.3928571428571428, 0.0, -5.107142857142857, 0.0, 15.321428571428571, 0.0, -64.35, 118.85714285714286, -107.25, 54.857142857142854, -15.321428571428571, 1.8285714285714285, 0.0, 0.0}}}},   // w6
-  {3, {{1.0, 0.6515846538782318, -0.03490632074347671, 5, 5, 7, {19.547539616346956, -78.19015846538782, 117.28523769808173, -78.19015846538782, 19.547539616346956, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {9.773769808173478, -26.063386155129276, 29.321309424520432, -15.638031693077565, 3.2579232693911595, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.3257923269391159, 0.0, 2.4434424520433695, -5.212677231025855, 4.886884904086739, -2.2340045275825093, 0.40724040867389494, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}, {0.6, -0.15200166805671392, 0.0029314607410937687, 5, 5, 7, {-12.666805671392828, 84.44537114261885, -211.11342785654713, 234.57047539616346, -97.73769808173478, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-6.333402835696414, 28.148457047539615, -52.77835696413678, 46.914095079232695, -16.289616346955796, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {0.07600083402835696, 0.0, -1.5833507089241035, 5.629691409507923, -8.79639282735613, 6.702013582747528, -2.0362020433694745, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}, {0.2, 0.0004170141784820684, -8.936018110330037e-07, 5, 5, 7, {0.3127606338615513, -6.255212677231026, 46.914095079232695, -156.38031693077565, 195.47539616346955, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {0.15638031693077564, -2.085070892410342, 11.728523769808174, -31.27606338615513, 32.57923269391159, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.0002085070892410342, 0.0, 0.03909507923269391, -0.4170141784820684, 1.9547539616346956, -4.468009055165019, 4.072404086738949, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // quartic
-  {3, {{1.0, 0.7625523012552301, -0.03177301255230126, 6, 6, 8, {32.02719665271967, -160.13598326359832, 320.27196652719664, -320.27196652719664, 160.13598326359832, -32.02719665271967, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {16.013598326359833, -53.37866108786611, 80.06799163179916, -64.05439330543933, 26.689330543933053, -4.575313807531381, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.38127615062761505, 0.0, 4.003399581589958, -10.675732217573222, 13.344665271966527, -9.150627615062762, 3.3361663179916317, -0.5083682008368201, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}, {0.6666666666666666, -0.26778242677824265, 0.004958933829226716, 6, 6, 8, {-25.305439330543933, 189.7907949790795, -569.3723849372385, 854.0585774058577, -640.5439330543933, 192.163179916318, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-12.652719665271967, 63.26359832635983, -142.34309623430963, 170.81171548117155, -106.75732217573221, 27.451882845188283, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {0.13389121338912133, 0.0, -3.1631799163179917, 12.652719665271967, -23.723849372384937, 24.401673640167363, -13.344665271966527, 3.0502092050209204, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}, {0.3333333333333333, 0.005230125523012552, -2.4213544088021077e-05, 6, 6, 8, {1.9769874476987448, -29.65481171548117, 177.92887029288704, -533.7866108786611, 800.6799163179917, -480.407949790795, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {0.9884937238493724, -9.884937238493723, 44.48221757322176, -106.75732217573221, 133.44665271966528, -68.6297071129707, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.002615062761506276, 0.0, 0.2471234309623431, -1.9769874476987448, 7.4137029288702925, -15.251046025104603, 16.68083158995816, -7.625523012552302, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // quintic
-  {1, {{1.0, 0.5, -0.05, 7, 7, 9, {4.0, 0.0, -12.0, 0.0, 12.0, 0.0, -4.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {2.0, 0.0, -3.0, 0.0, 2.0, 0.0, -0.5, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.25, 0.0, 0.5, 0.0, -0.5, 0.0, 0.25, 0.0, -0.05, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // poly6
-  {1, {{1.0, 0.5, -0.075, 2, 2, 4, {3.0, -3.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {1.5, -1.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.25, 0.0, 0.375, -0.2, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // cone
-  {1, {{1.0, 0.5, -0.03571428571428571, 4, 4, 6, {10.0, -30.0, 30.0, -10.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {5.0, -10.0, 7.5, -2.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.25, 0.0, 1.25, -2.0, 1.25, -0.2857142857142857, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // lw2
-  {1, {{1.0, 0.5, -0.027777777777777776, 7, 7, 9, {9.333333333333334, 0.0, -140.0, 373.3333333333333, -420.0, 224.0, -46.666666666666664, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {4.666666666666667, 0.0, -35.0, 74.66666666666667, -70.0, 32.0, -5.833333333333333, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, {-0.25, 0.0, 1.1666666666666667, 0.0, -5.833333333333333, 10.666666666666666, -8.75, 3.5555555555555554, -0.5833333333333334, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}}}},   // lw4
-};
+// ---- disk element: pi*W, M/r^2 and the second potential of every exact kernel, summed over its blocks
+template <int KID> __device__ __forceinline__ void disk_profile(double r, double ir2, double& P, double& Fl,
+                                                             double& F2l);
+template <int KID> __device__ __forceinline__ int disk_knots(double* out);
+template <> __device__ __forceinline__ void disk_profile<0>(double r, double ir2, double& P, double& Fl, double& F2l) {   // cubic
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(-11.428571428571429, r, 34.285714285714285), r, -34.285714285714285), r, 11.428571428571429);
+    Fl += fma(fma(fma(-2.2857142857142856, r, 8.571428571428571), r, -11.428571428571429), r, 5.714285714285714);
+    F2l += fma(fma(fma(fma(fma(-0.32653061224489793, r, 1.4285714285714286), r, -2.2857142857142856), r, 1.4285714285714286), r, 0.0), r, -0.2857142857142857);
+  } else {
+    Fl += 0.5714285714285714 * ir2;
+    F2l += -0.04081632653061224 * ir2;
+  }
+  if (r <= 0.5) {
+    P += fma(fma(fma(45.714285714285715, r, -68.57142857142857), r, 34.285714285714285), r, -5.714285714285714);
+    Fl += fma(fma(fma(9.142857142857142, r, -17.142857142857142), r, 11.428571428571429), r, -2.857142857142857);
+    F2l += fma(fma(fma(fma(fma(1.3061224489795917, r, -2.857142857142857), r, 2.2857142857142856), r, -0.7142857142857143), r, 0.0), r, 0.03571428571428571);
+  } else {
+    Fl += -0.07142857142857142 * ir2;
+    F2l += 0.0012755102040816326 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<0>(double* out) {
+  out[0] = 0.5;
+  return 1;
+}
+template <> __device__ __forceinline__ void disk_profile<1>(double r, double ir2, double& P, double& Fl, double& F2l) {   // w2
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(28.0, r, -105.0), r, 140.0), r, -70.0), r, 0.0), r, 7.0);
+    Fl += fma(fma(fma(fma(fma(4.0, r, -17.5), r, 28.0), r, -17.5), r, 0.0), r, 3.5);
+    F2l += fma(fma(fma(fma(fma(fma(fma(0.4444444444444444, r, -2.1875), r, 4.0), r, -2.9166666666666665), r, 0.0), r, 0.875), r, 0.0), r, -0.25);
+  } else {
+    Fl += 0.5 * ir2;
+    F2l += -0.034722222222222224 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<1>(double* out) {
+  return 0;
+}
+template <> __device__ __forceinline__ void disk_profile<2>(double r, double ir2, double& P, double& Fl, double& F2l) {   // w4
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(fma(fma(105.0, r, -576.0), r, 1260.0), r, -1344.0), r, 630.0), r, 0.0), r, -84.0), r, 0.0), r, 9.0);
+    Fl += fma(fma(fma(fma(fma(fma(fma(fma(10.5, r, -64.0), r, 157.5), r, -192.0), r, 105.0), r, 0.0), r, -21.0), r, 0.0), r, 4.5);
+    F2l += fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.875, r, -5.818181818181818), r, 15.75), r, -21.333333333333332), r, 13.125), r, 0.0), r, -3.5), r, 0.0), r, 1.125), r, 0.0), r, -0.25);
+  } else {
+    Fl += 0.5 * ir2;
+    F2l += -0.026515151515151516 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<2>(double* out) {
+  return 0;
+}
+template <> __device__ __forceinline__ void disk_profile<3>(double r, double ir2, double& P, double& Fl, double& F2l) {   // w6
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(356.57142857142856, r, -2574.0), r, 7844.571428571428), r, -12870.0), r, 11766.857142857143), r, -5148.0), r, 0.0), r, 735.4285714285714), r, 0.0), r, -122.57142857142857), r, 0.0), r, 11.142857142857142);
+    Fl += fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(27.428571428571427, r, -214.5), r, 713.1428571428571), r, -1287.0), r, 1307.4285714285713), r, -643.5), r, 0.0), r, 122.57142857142857), r, 0.0), r, -30.642857142857142), r, 0.0), r, 5.571428571428571);
+    F2l += fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.8285714285714285, r, -15.321428571428571), r, 54.857142857142854), r, -107.25), r, 118.85714285714286), r, -64.35), r, 0.0), r, 15.321428571428571), r, 0.0), r, -5.107142857142857), r, 0.0), r, 1.3928571428571428), r, 0.0), r, -0.25);
+  } else {
+    Fl += 0.5 * ir2;
+    F2l += -0.02142857142857143 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<3>(double* out) {
+  return 0;
+}
+template <> __device__ __forceinline__ void disk_profile<4>(double r, double ir2, double& P, double& Fl, double& F2l) {   // quartic
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(19.547539616346956, r, -78.19015846538782), r, 117.28523769808173), r, -78.19015846538782), r, 19.547539616346956);
+    Fl += fma(fma(fma(fma(3.2579232693911595, r, -15.638031693077565), r, 29.321309424520432), r, -26.063386155129276), r, 9.773769808173478);
+    F2l += fma(fma(fma(fma(fma(fma(0.40724040867389494, r, -2.2340045275825093), r, 4.886884904086739), r, -5.212677231025855), r, 2.4434424520433695), r, 0.0), r, -0.3257923269391159);
+  } else {
+    Fl += 0.6515846538782318 * ir2;
+    F2l += -0.03490632074347671 * ir2;
+  }
+  if (r <= 0.6) {
+    P += fma(fma(fma(fma(-97.73769808173478, r, 234.57047539616346), r, -211.11342785654713), r, 84.44537114261885), r, -12.666805671392828);
+    Fl += fma(fma(fma(fma(-16.289616346955796, r, 46.914095079232695), r, -52.77835696413678), r, 28.148457047539615), r, -6.333402835696414);
+    F2l += fma(fma(fma(fma(fma(fma(-2.0362020433694745, r, 6.702013582747528), r, -8.79639282735613), r, 5.629691409507923), r, -1.5833507089241035), r, 0.0), r, 0.07600083402835696);
+  } else {
+    Fl += -0.15200166805671392 * ir2;
+    F2l += 0.0029314607410937687 * ir2;
+  }
+  if (r <= 0.2) {
+    P += fma(fma(fma(fma(195.47539616346955, r, -156.38031693077565), r, 46.914095079232695), r, -6.255212677231026), r, 0.3127606338615513);
+    Fl += fma(fma(fma(fma(32.57923269391159, r, -31.27606338615513), r, 11.728523769808174), r, -2.085070892410342), r, 0.15638031693077564);
+    F2l += fma(fma(fma(fma(fma(fma(4.072404086738949, r, -4.468009055165019), r, 1.9547539616346956), r, -0.4170141784820684), r, 0.03909507923269391), r, 0.0), r, -0.0002085070892410342);
+  } else {
+    Fl += 0.0004170141784820684 * ir2;
+    F2l += -8.936018110330037e-07 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<4>(double* out) {
+  out[0] = 0.2;
+  out[1] = 0.6;
+  return 2;
+}
+template <> __device__ __forceinline__ void disk_profile<5>(double r, double ir2, double& P, double& Fl, double& F2l) {   // quintic
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(-32.02719665271967, r, 160.13598326359832), r, -320.27196652719664), r, 320.27196652719664), r, -160.13598326359832), r, 32.02719665271967);
+    Fl += fma(fma(fma(fma(fma(-4.575313807531381, r, 26.689330543933053), r, -64.05439330543933), r, 80.06799163179916), r, -53.37866108786611), r, 16.013598326359833);
+    F2l += fma(fma(fma(fma(fma(fma(fma(-0.5083682008368201, r, 3.3361663179916317), r, -9.150627615062762), r, 13.344665271966527), r, -10.675732217573222), r, 4.003399581589958), r, 0.0), r, -0.38127615062761505);
+  } else {
+    Fl += 0.7625523012552301 * ir2;
+    F2l += -0.03177301255230126 * ir2;
+  }
+  if (r <= 0.6666666666666666) {
+    P += fma(fma(fma(fma(fma(192.163179916318, r, -640.5439330543933), r, 854.0585774058577), r, -569.3723849372385), r, 189.7907949790795), r, -25.305439330543933);
+    Fl += fma(fma(fma(fma(fma(27.451882845188283, r, -106.75732217573221), r, 170.81171548117155), r, -142.34309623430963), r, 63.26359832635983), r, -12.652719665271967);
+    F2l += fma(fma(fma(fma(fma(fma(fma(3.0502092050209204, r, -13.344665271966527), r, 24.401673640167363), r, -23.723849372384937), r, 12.652719665271967), r, -3.1631799163179917), r, 0.0), r, 0.13389121338912133);
+  } else {
+    Fl += -0.26778242677824265 * ir2;
+    F2l += 0.004958933829226716 * ir2;
+  }
+  if (r <= 0.3333333333333333) {
+    P += fma(fma(fma(fma(fma(-480.407949790795, r, 800.6799163179917), r, -533.7866108786611), r, 177.92887029288704), r, -29.65481171548117), r, 1.9769874476987448);
+    Fl += fma(fma(fma(fma(fma(-68.6297071129707, r, 133.44665271966528), r, -106.75732217573221), r, 44.48221757322176), r, -9.884937238493723), r, 0.9884937238493724);
+    F2l += fma(fma(fma(fma(fma(fma(fma(-7.625523012552302, r, 16.68083158995816), r, -15.251046025104603), r, 7.4137029288702925), r, -1.9769874476987448), r, 0.2471234309623431), r, 0.0), r, -0.002615062761506276);
+  } else {
+    Fl += 0.005230125523012552 * ir2;
+    F2l += -2.4213544088021077e-05 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<5>(double* out) {
+  out[0] = 0.3333333333333333;
+  out[1] = 0.6666666666666666;
+  return 2;
+}
+template <> __device__ __forceinline__ void disk_profile<6>(double r, double ir2, double& P, double& Fl, double& F2l) {   // poly6
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(-4.0, r, 0.0), r, 12.0), r, 0.0), r, -12.0), r, 0.0), r, 4.0);
+    Fl += fma(fma(fma(fma(fma(fma(-0.5, r, 0.0), r, 2.0), r, 0.0), r, -3.0), r, 0.0), r, 2.0);
+    F2l += fma(fma(fma(fma(fma(fma(fma(fma(-0.05, r, 0.0), r, 0.25), r, 0.0), r, -0.5), r, 0.0), r, 0.5), r, 0.0), r, -0.25);
+  } else {
+    Fl += 0.5 * ir2;
+    F2l += -0.05 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<6>(double* out) {
+  return 0;
+}
+template <> __device__ __forceinline__ void disk_profile<7>(double r, double ir2, double& P, double& Fl, double& F2l) {   // cone
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(-3.0, r, 3.0);
+    Fl += fma(-1.0, r, 1.5);
+    F2l += fma(fma(fma(-0.2, r, 0.375), r, 0.0), r, -0.25);
+  } else {
+    Fl += 0.5 * ir2;
+    F2l += -0.075 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<7>(double* out) {
+  return 0;
+}
+template <> __device__ __forceinline__ void disk_profile<8>(double r, double ir2, double& P, double& Fl, double& F2l) {   // lw2
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(-10.0, r, 30.0), r, -30.0), r, 10.0);
+    Fl += fma(fma(fma(-2.0, r, 7.5), r, -10.0), r, 5.0);
+    F2l += fma(fma(fma(fma(fma(-0.2857142857142857, r, 1.25), r, -2.0), r, 1.25), r, 0.0), r, -0.25);
+  } else {
+    Fl += 0.5 * ir2;
+    F2l += -0.03571428571428571 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<8>(double* out) {
+  return 0;
+}
+template <> __device__ __forceinline__ void disk_profile<9>(double r, double ir2, double& P, double& Fl, double& F2l) {   // lw4
+  P = 0.0;
+  Fl = 0.0;
+  F2l = 0.25;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(-46.666666666666664, r, 224.0), r, -420.0), r, 373.3333333333333), r, -140.0), r, 0.0), r, 9.333333333333334);
+    Fl += fma(fma(fma(fma(fma(fma(-5.833333333333333, r, 32.0), r, -70.0), r, 74.66666666666667), r, -35.0), r, 0.0), r, 4.666666666666667);
+    F2l += fma(fma(fma(fma(fma(fma(fma(fma(-0.5833333333333334, r, 3.5555555555555554), r, -8.75), r, 10.666666666666666), r, -5.833333333333333), r, 0.0), r, 1.1666666666666667), r, 0.0), r, -0.25);
+  } else {
+    Fl += 0.5 * ir2;
+    F2l += -0.027777777777777776 * ir2;
+  }
+}
+template <> __device__ __forceinline__ int disk_knots<9>(double* out) {
+  return 0;
+}
+constexpr int kDiskMaxKnots = 2;
 
 // ---- 3-D radial family (solid half-space / sphere), unit support; W = c3*pi * shape, L = W'/r, dL = L'
 template <int K, typename T>

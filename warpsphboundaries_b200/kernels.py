@@ -443,42 +443,39 @@ def emit_header() -> str:
     return "\n".join(out)
 
 
-DISK_MAX_BLOCKS = 3
-DISK_MAX_COEF = 16
-
-
 def emit_disk() -> list:
-    """the disk element's profile table: per exact kernel id its truncated blocks of pi*W -- radius R, P, the value
-    potential M(r)/r^2 (M = int_0^r t P dt), the second potential MPsi(r)/r^2 and the constants M(R), MPsi(R) that
-    continue them past R -- as literal data for a kernel argument (host-side array, copied by value per launch)."""
-    out = ["// ---- disk element: per kernel id the truncated blocks of pi*W (radius, P, M/r^2, MPsi/r^2, M(R), MPsi(R))",
-           f"constexpr int kDiskMaxBlocks = {DISK_MAX_BLOCKS};", f"constexpr int kDiskMaxCoef = {DISK_MAX_COEF};",
-           "struct DiskBlock {",
-           "  double R, Mhat, MPhat;",
-           "  int np, nl, nf;",
-           "  double P[kDiskMaxCoef], L[kDiskMaxCoef], F[kDiskMaxCoef];",
-           "};",
-           "struct DiskTable {",
-           "  int nb;",
-           "  DiskBlock b[kDiskMaxBlocks];",
-           "};",
-           "static const DiskTable kDiskTables[kNumKernels] = {"]
-
-    def arr(c):
-        c = list(c) + [F(0)] * (DISK_MAX_COEF - len(c))
-        return "{" + ", ".join(_lit(x) for x in c) + "}"
-
+    """the disk element's profiles per exact kernel id as literal code: disk_profile<KID>(r) gives P = pi*W, the value
+    potential M(r)/r^2 (M = int_0^r t P dt) and the second potential MPsi(r)/r^2 + sum M(R)/2 summed over the
+    truncated blocks (a block past its radius R continues as M(R)/r^2 and MPsi(R)/r^2), and disk_knots<KID> the
+    block radii below 1 (where the profiles have kinks)."""
+    out = ["// ---- disk element: pi*W, M/r^2 and the second potential of every exact kernel, summed over its blocks",
+           "template <int KID> __device__ __forceinline__ void disk_profile(double r, double ir2, double& P, double& Fl,",
+           "                                                             double& F2l);",
+           "template <int KID> __device__ __forceinline__ int disk_knots(double* out);"]
     for kid in range(len(KERNEL_IDS)):
         k = kernel(KERNEL_NAMES[kid])
-        if len(k.blocks) > DISK_MAX_BLOCKS or any(max(len(b.c), len(b.flam), len(b.fpsi)) > DISK_MAX_COEF
-                                                  for b in k.blocks):
-            raise AssertionError(f"disk table of {k.name} exceeds its bounds")
-        blocks = []
+        half = sum((b.Mhat for b in k.blocks), F(0)) / 2
+        body = [f"template <> __device__ __forceinline__ void disk_profile<{kid}>(double r, double ir2, double& P, "
+                f"double& Fl, double& F2l) {{   // {k.name}",
+                f"  P = 0.0;", f"  Fl = 0.0;", f"  F2l = {_lit(half)};"]
         for b in k.blocks:
-            blocks.append(f"{{{_lit(b.R)}, {_lit(b.Mhat)}, {_lit(b.MPhat)}, {len(b.c)}, {len(b.flam)}, {len(b.fpsi)}, "
-                          f"{arr(b.c)}, {arr(b.flam)}, {arr(b.fpsi)}}}")
-        out.append(f"  {{{len(k.blocks)}, {{" + ", ".join(blocks) + "}},   // " + k.name)
-    out.append("};")
+            body.append(f"  if (r <= {_lit(b.R)}) {{")
+            body.append(f"    P += {_horner(b.c, 'r')};")
+            body.append(f"    Fl += {_horner(b.flam, 'r')};")
+            body.append(f"    F2l += {_horner(b.fpsi, 'r')};")
+            body.append("  } else {")
+            body.append(f"    Fl += {_lit(b.Mhat)} * ir2;")
+            body.append(f"    F2l += {_lit(b.MPhat)} * ir2;")
+            body.append("  }")
+        body.append("}")
+        knots = sorted(b.R for b in k.blocks if b.R < 1)
+        body.append(f"template <> __device__ __forceinline__ int disk_knots<{kid}>(double* out) {{")
+        for j, R in enumerate(knots):
+            body.append(f"  out[{j}] = {_lit(R)};")
+        body.append(f"  return {len(knots)};")
+        body.append("}")
+        out.extend(body)
+    out.append(f"constexpr int kDiskMaxKnots = {max(1, max(sum(1 for b in kernel(n).blocks if b.R < 1) for n in KERNEL_IDS))};")
     out.append("")
     return out
 

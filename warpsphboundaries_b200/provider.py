@@ -155,11 +155,12 @@ class FusedWall(WallAggregate):
                 mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if ri == 0 else 0)     # the first representation assigns
                 if isinstance(rep, DiskArrayRep):
                     nd = rep.native(self.support, self.dev)
+                    dws, dneed = nd.workspace(N)
                     for gi, kid in enumerate(kids):
                         o = outs[gi]
                         check(lib.wsb_disk_aggregate(nd.handle, kid, ptr(pos), ptr(sup), ptr(al), N, ptr(pose), mode,
                                                      ptr(o["lam"][bi]), ptr(o["G"][bi]), ptr(o["Cov"][bi]),
-                                                     ptr(o["m1"][bi]), ptr(o["m2"][bi]), _stream()),
+                                                     ptr(o["m1"][bi]), ptr(o["m2"][bi]), ptr(dws), dneed, _stream()),
                               "wsb_disk_aggregate")
                     continue
                 ns = rep.native(self.support, self.dev)

@@ -308,6 +308,18 @@ class NativeDisks:
                                    r.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(r), float(support_max), idx,
                                    ctypes.byref(h)), "wsb_disks_create")
         self.handle = h
+        self._ws = {}
+
+    def workspace(self, n):
+        """the work-list buffer for n rows on the current stream (one per stream, grown geometrically)."""
+        need = int(lib.wsb_disk_workspace_size(self.handle, int(n)))
+        key = torch.cuda.current_stream(self.device).cuda_stream
+        ws = self._ws.get(key)
+        if ws is None or ws.numel() < need:
+            ws = torch.empty(max(need, int(1.5 * ws.numel()) if ws is not None else need, 1), dtype=torch.uint8,
+                             device=self.device)
+            self._ws[key] = ws
+        return ws, need
 
     def __del__(self):
         h = getattr(self, "handle", None)
