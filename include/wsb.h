@@ -266,6 +266,13 @@ size_t wsb_disk_workspace_size(const wsb_disks* d, int64_t n);
 int wsb_disk_aggregate(const wsb_disks* d, int kernel, const double* pos, const double* sup, const int32_t* allowed,
                        int64_t n, const double* pose, int out_mask, double* lam, double* G, double* cov, double* m1,
                        double* m2, void* workspace, size_t workspace_bytes, void* stream);
+/* The detector inputs of disk sets, as wsb_cone_area / wsb_dir_extreme for surfaces but per call (no prepared
+ * workspace): area [2n] ADDED (wedge, then full disk), out [n] max-accumulated; closed forms per (particle, disk)
+ * (src/warpSPHBoundaries/scene/fused.py:310-475 _disk_cum, _disk_cone_area_kernel, _disk_dir_extreme_kernel). */
+int wsb_disk_cone_area(const wsb_disks* d, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
+                       const double* pose, const double* axes, double half_angle, double* area, void* stream);
+int wsb_disk_dir_extreme(const wsb_disks* d, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
+                         const double* pose, const double* vecs, double* out, void* stream);
 
 /* ---- closed triangle surfaces (3-D) ----
  * A watertight, consistently oriented triangle surface with outward normals (positive signed volume): verts

@@ -112,3 +112,116 @@ def area_preserving_polygon(centre, R, n):
     t = 2 * np.pi * np.arange(n) / n
     return np.stack([centre[0] + rN * np.cos(t), centre[1] + rN * np.sin(t)], 1)
 
+
+
+# ------------------------------------------------------------------------------------------------ detector inputs
+def _ray_span(D, R, phi):
+    """the part of the ray at angle phi (from the centre direction) inside disk cap unit ball: (lo, hi) or None."""
+    sm = D * math.sin(phi)
+    if abs(sm) >= R:
+        return None
+    q = math.sqrt(R * R - sm * sm)
+    t1, t2 = D * math.cos(phi) - q, D * math.cos(phi) + q
+    lo, hi = min(max(t1, 0.0), 1.0), min(max(t2, 0.0), 1.0)
+    return (lo, hi) if hi > lo else None
+
+
+def disk_wedge_area(D, R, g, half_angle, tol=1e-13):
+    """area (support 1) of disk cap unit ball cap the wedge |phi - g| <= half_angle (phi from the centre direction;
+    half_angle >= pi: the whole disk) by adaptive quadrature of 1/2 (hi^2 - lo^2) over the ray angles -- the
+    reference test's independent numerical angular integration (tests/scene/test_disk_array.py:79-97) in
+    adaptive form, split at the tangent rays and the rays through the circle / support-circle crossings."""
+    if half_angle >= math.pi:
+        a, b = -math.pi, math.pi
+    else:
+        a, b = g - half_angle, g + half_angle
+    cuts = []
+    if D >= R and D > 0:
+        t = math.asin(min(R / D, 1.0))
+        cuts += [t, -t]
+    if D > 1e-12:
+        arg = (D * D + 1.0 - R * R) / (2.0 * D)
+        if abs(arg) <= 1.0:
+            t = math.acos(arg)
+            cuts += [t, -t]
+    pts = sorted({c + 2 * math.pi * k for c in cuts for k in (-2, -1, 0, 1, 2) if a < c + 2 * math.pi * k < b})
+
+    def f(phi):
+        s = _ray_span(D, R, phi)
+        return 0.0 if s is None else 0.5 * (s[1] ** 2 - s[0] ** 2)
+    edges = [a] + pts + [b]
+    return sum(integrate.quad(f, x0, x1, limit=400, epsabs=tol, epsrel=tol)[0] for x0, x1 in zip(edges[:-1], edges[1:]))
+
+
+def disks_cone_area(lpos, axes_local, half_angle, H, centres, radii):
+    """[2, N]: wedge and full-disk areas (physical units) of the solid of a disk set at body-frame particles with
+    body-frame axes; H per particle."""
+    lpos = np.asarray(lpos, float)
+    ax = np.asarray(axes_local, float)
+    Hn = np.broadcast_to(np.asarray(H, float), (len(lpos),))
+    out = np.zeros((2, len(lpos)))
+    for i in range(len(lpos)):
+        th = math.atan2(ax[i, 1], ax[i, 0])
+        for c, R in zip(np.asarray(centres, float).reshape(-1, 2), np.asarray(radii, float).reshape(-1)):
+            v = (c - lpos[i]) / Hn[i]
+            D = math.hypot(v[0], v[1])
+            if D >= 1.0 + R / Hn[i]:
+                continue
+            g = th - (math.atan2(v[1], v[0]) if D > 0 else 0.0)
+            out[0, i] += disk_wedge_area(D, R / Hn[i], g, half_angle) * Hn[i] ** 2
+            out[1, i] += disk_wedge_area(D, R / Hn[i], 0.0, math.pi) * Hn[i] ** 2
+    return out
+
+
+def disks_dir_extreme(lpos, vecs_local, H, centres, radii):
+    """max |v_hat . x_hat| over the directions from each body-frame particle to the points of the disks within its
+    support, in closed form per disk (fused.py:440-475): the directions to one disk form [-b, b] about the centre
+    direction, b = asin(R / d) when the tangent points are inside the support, else the angle of the circle's crossing
+    with the support circle; the extreme is cos(max(0, psi - b)), 1 inside the disk; 0 for v = 0."""
+    lpos = np.asarray(lpos, float)
+    w = np.asarray(vecs_local, float)
+    Hn = np.broadcast_to(np.asarray(H, float), (len(lpos),))
+    out = np.zeros(len(lpos))
+    for i in range(len(lpos)):
+        nv = math.hypot(w[i, 0], w[i, 1])
+        if nv == 0:
+            continue
+        best = 0.0
+        for c, R in zip(np.asarray(centres, float).reshape(-1, 2), np.asarray(radii, float).reshape(-1)):
+            cx, cy = c - lpos[i]
+            d = math.hypot(cx, cy)
+            if d <= R:
+                best = 1.0
+            elif d - R < Hn[i]:
+                h = Hn[i]
+                b = (math.asin(min(R / d, 1.0)) if d * d - R * R <= h * h else
+                     math.acos(min(max((d * d + h * h - R * R) / (2 * d * h), -1.0), 1.0)))
+                psi = math.acos(min(abs(cx * w[i, 0] + cy * w[i, 1]) / (d * nv), 1.0))
+                best = max(best, 1.0 if psi <= b else math.cos(psi - b))
+        out[i] = best
+    return out
+
+
+def disks_dir_extreme_polar(lpos, vecs_local, H, centres, radii, nr=150, nphi=1440):
+    """the polar-grid oracle for disk sets: the largest |cos| over the midpoints of a polar grid of the support disk
+    that lie inside a disk (independent of the closed form, accurate to the angular step)."""
+    lpos = np.asarray(lpos, float)
+    w = np.asarray(vecs_local, float)
+    Hn = np.broadcast_to(np.asarray(H, float), (len(lpos),))
+    C = np.asarray(centres, float).reshape(-1, 2)
+    Rr = np.asarray(radii, float).reshape(-1)
+    ph = (np.arange(nphi) + 0.5) / nphi * 2 * np.pi
+    out = np.zeros(len(lpos))
+    for i in range(len(lpos)):
+        if w[i, 0] == 0.0 and w[i, 1] == 0.0:
+            continue
+        rr = (np.arange(nr) + 0.5) / nr * Hn[i]
+        X = lpos[i, 0] + rr[:, None] * np.cos(ph)[None]
+        Y = lpos[i, 1] + rr[:, None] * np.sin(ph)[None]
+        solid = np.zeros(X.shape, bool)
+        for c, R in zip(C, Rr):
+            solid |= (X - c[0]) ** 2 + (Y - c[1]) ** 2 < R * R
+        if solid.any():
+            cosv = np.broadcast_to(np.abs(np.cos(ph - math.atan2(w[i, 1], w[i, 0])))[None], X.shape)
+            out[i] = cosv[solid].max()
+    return out

@@ -253,6 +253,166 @@ __global__ void __launch_bounds__(kDiskThreads, 4) k_disk_warp(const int32_t* __
   }
 }
 
+// ------------------------------------------------------------------------------------------------ detector inputs
+// The cone area and the direction extreme of solid disks (src/warpSPHBoundaries/scene/fused.py:310-475, 741-835):
+// closed forms per (particle, disk), one thread per particle over the disks of its cell.
+
+// the angle in [-pi, pi)
+__device__ __forceinline__ double disk_wrap(double a) {
+  const double r = a + 0.5 * kTwoPi;
+  return r - kTwoPi * floor(r / kTwoPi) - 0.5 * kTwoPi;
+}
+
+// int t^2 dphi along a ray family through the disk: t = D cos(phi) -+ q, q = sqrt(R^2 - D^2 sin^2(phi)), gives
+// t^2 = R^2 + D^2 cos(2 phi) -+ 2 D cos(phi) q, whose antiderivative is R^2 phi + s c -+ (s q + R^2 asin(s / R))
+// (s = D sin(phi), c = D cos(phi)).  q is formed as sqrt((R - D)(R + D) + c^2) and asin(s / R) as atan2(s, q): near
+// the tangent ray s / R -> 1, where asin of a rounded quotient loses half the digits, both stay accurate.
+__device__ __forceinline__ double disk_q(double D, double R, double c) {
+  return sqrt(fmax(fma(c, c, (R - D) * (R + D)), 0.0));
+}
+
+__device__ __forceinline__ double disk_ray_antideriv(double D, double R, double phi, double sign) {
+  double sp, cp;
+  sincos(phi, &sp, &cp);
+  const double s = D * sp, c = D * cp, q = disk_q(D, R, c);
+  return R * R * phi + s * c + sign * (s * q + R * R * atan2(s, q));
+}
+
+// The area of disk cap unit ball swept by the rays from the particle at angles [0, psi] (psi in [0, pi]) from the
+// direction of the centre (distance D, radius R, support 1): 1/2 int (min(t_far, 1)^2 - min(max(t_near, 0), 1)^2)
+// dphi, in closed form on the pieces between the tangent ray asin(R / D) and the rays through the crossings of the
+// disk's circle with the support circle (where a clip switches on or off).
+__device__ double disk_sweep(double D, double R, double psi) {
+  double c[2];
+  int nc = 0;
+  if (D >= R && D > 0.0) {   // (D = R: the particle on the circle; the far end reaches the particle at pi/2)
+    const double a = atan2(R, sqrt((D - R) * (D + R)));   // the tangent ray
+    if (a > 0.0 && a < psi) c[nc++] = a;
+  }
+  if (D > 1e-12) {
+    const double arg = (D * D + 1.0 - R * R) / (2.0 * D);
+    if (fabs(arg) <= 1.0) {
+      const double a = acos(arg);
+      if (a > 0.0 && a < psi) c[nc++] = a;
+    }
+  }
+  if (nc == 2 && c[1] < c[0]) {
+    const double tmp = c[0];
+    c[0] = c[1];
+    c[1] = tmp;
+  }
+  double total = 0.0, lo = 0.0;
+  for (int k = 0; k <= nc; ++k) {
+    const double hi = k < nc ? c[k] : psi;
+    if (hi > lo) {
+      const double m = 0.5 * (lo + hi), sm = D * sin(m);
+      if (fabs(sm) < R) {
+        const double cm = D * cos(m), q = disk_q(D, R, cm), t1 = cm - q, t2 = cm + q;
+        if (t2 > 0.0) {
+          const double far = t2 >= 1.0 ? hi - lo : disk_ray_antideriv(D, R, hi, 1.0) - disk_ray_antideriv(D, R, lo, 1.0);
+          const double near = t1 >= 1.0 ? hi - lo
+                              : t1 > 0.0 ? disk_ray_antideriv(D, R, hi, -1.0) - disk_ray_antideriv(D, R, lo, -1.0)
+                                         : 0.0;
+          total += 0.5 * (far - near);
+        }
+      }
+    }
+    lo = hi;
+  }
+  return total;
+}
+
+// the swept area at any real angle: odd in the angle, and each full turn adds the whole area
+__device__ __forceinline__ double disk_sweep_any(double D, double R, double psi) {
+  const double p0 = disk_wrap(psi);
+  const double k = floor((psi - p0) / kTwoPi + 0.5);
+  double v = disk_sweep(D, R, fabs(p0));
+  if (p0 < 0.0) v = -v;
+  if (k != 0.0) v += k * 2.0 * disk_sweep(D, R, 0.5 * kTwoPi);
+  return v;
+}
+
+// per particle: area[i] += the area of the disks' solid cap disk(x, H) cap wedge(x, axis, half_angle) and
+// area[n + i] += the full-disk area, summed over the disks of its cell within reach
+__global__ void __launch_bounds__(kDiskThreads) k_disk_cone(const int32_t* __restrict__ cstart,
+                                                           const double4* __restrict__ items, int32_t nx, int32_t ny,
+                                                           double lo_x, double lo_y, double cell,
+                                                           const double* __restrict__ pos,
+                                                           const double* __restrict__ sup,
+                                                           const int32_t* __restrict__ allowed, int64_t n,
+                                                           const double* __restrict__ pose,
+                                                           const double* __restrict__ axes, double half_angle,
+                                                           double* __restrict__ area) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double lx, ly;
+  int32_t cid;
+  if (!disk_row(pos, allowed, pose, i, nx, ny, lo_x, lo_y, cell, lx, ly, cid)) return;
+  const double H = sup[i], ih = 1.0 / H;
+  const double ax = axes[2 * i], ay = axes[2 * i + 1], pc = pose[2], ps = pose[3];
+  const double th = atan2(-ps * ax + pc * ay, pc * ax + ps * ay);     // the world axis in the body frame
+  const bool wedge = half_angle < 0.5 * kTwoPi;
+  double a_wedge = 0.0, a_full = 0.0;
+  for (int32_t k = cstart[cid]; k < cstart[cid + 1]; ++k) {
+    const double4 e = items[k];
+    const double vx = (e.x - lx) * ih, vy = (e.y - ly) * ih, R = e.z * ih;
+    const double D = sqrt(vx * vx + vy * vy);
+    if (!(D < 1.0 + R)) continue;
+    const double full = 2.0 * disk_sweep(D, R, 0.5 * kTwoPi);
+    a_full += full;
+    if (wedge) {
+      const double g = disk_wrap(th - atan2(vy, vx));
+      a_wedge += disk_sweep_any(D, R, g + half_angle) - disk_sweep_any(D, R, g - half_angle);
+    } else {
+      a_wedge += full;
+    }
+  }
+  area[i] += a_wedge * H * H;
+  area[n + i] += a_full * H * H;
+}
+
+// per particle: out[i] = max(out[i], the largest |cos| between its world vector and a direction towards a disk point
+// within its support).  The directions to the points of one disk within the support form the interval [-b, b] about
+// the centre direction: b = asin(R / d) when the tangent points lie inside the support, else the angle at which the
+// disk's circle meets the support circle; with psi the angle between the line of the vector and the centre direction
+// the extreme is cos(max(0, psi - b)); a particle inside the disk sees it in every direction.
+__global__ void __launch_bounds__(kDiskThreads) k_disk_dir(const int32_t* __restrict__ cstart,
+                                                          const double4* __restrict__ items, int32_t nx, int32_t ny,
+                                                          double lo_x, double lo_y, double cell,
+                                                          const double* __restrict__ pos,
+                                                          const double* __restrict__ sup,
+                                                          const int32_t* __restrict__ allowed, int64_t n,
+                                                          const double* __restrict__ pose,
+                                                          const double* __restrict__ vecs, double* __restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double lx, ly;
+  int32_t cid;
+  if (!disk_row(pos, allowed, pose, i, nx, ny, lo_x, lo_y, cell, lx, ly, cid)) return;
+  const double wx = vecs[2 * i], wy = vecs[2 * i + 1], pc = pose[2], ps = pose[3];
+  const double bx = pc * wx + ps * wy, by = -ps * wx + pc * wy;      // R^T w
+  const double nb = sqrt(bx * bx + by * by);
+  if (!(nb > 0.0)) return;
+  const double H = sup[i];
+  double best = 0.0;
+  for (int32_t k = cstart[cid]; k < cstart[cid + 1] && best < 1.0; ++k) {
+    const double4 e = items[k];
+    const double cx = e.x - lx, cy = e.y - ly, R = e.z;
+    const double d = sqrt(cx * cx + cy * cy);
+    double f = 0.0;
+    if (d <= R) {
+      f = 1.0;
+    } else if (d - R < H) {
+      const double b = d * d - R * R <= H * H ? asin(fmin(R / d, 1.0))
+                                              : acos(fmin(fmax((d * d + H * H - R * R) / (2.0 * d * H), -1.0), 1.0));
+      const double psi = acos(fmin(fabs(cx * bx + cy * by) / (d * nb), 1.0));
+      f = psi <= b ? 1.0 : cos(psi - b);
+    }
+    best = fmax(best, f);
+  }
+  out[i] = fmax(out[i], best);
+}
+
 }  // namespace wsb
 
 using namespace wsb;
@@ -415,6 +575,37 @@ extern "C" int wsb_disk_aggregate(const wsb_disks* d_, int kernel, const double*
     case 9: launch(std::integral_constant<int, 9>{}); break;
     default: return fail(WSB_ERR_UNSUPPORTED, "wsb_disk_aggregate: unknown kernel id");
   }
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+extern "C" int wsb_disk_cone_area(const wsb_disks* d_, const double* pos, const double* sup, const int32_t* allowed,
+                                  int64_t n, const double* pose, const double* axes, double half_angle, double* area,
+                                  void* stream) {
+  const Disks* d = reinterpret_cast<const Disks*>(d_);
+  if (!d) return fail(WSB_ERR_ARG, "wsb_disk_cone_area: NULL disks");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_disk_cone_area: row count out of range");
+  if (!(half_angle >= 0.0) || !std::isfinite(half_angle))
+    return fail(WSB_ERR_ARG, "wsb_disk_cone_area: the half angle must be finite and >= 0");
+  if (n == 0) return WSB_OK;
+  if (!pos || !sup || !pose || !axes || !area) return fail(WSB_ERR_ARG, "wsb_disk_cone_area: NULL array");
+  WSB_CUDA(cudaSetDevice(d->device));
+  k_disk_cone<<<(unsigned)((n + kDiskThreads - 1) / kDiskThreads), kDiskThreads, 0, (cudaStream_t)stream>>>(
+      d->cstart, d->items, d->nx, d->ny, d->lo_x, d->lo_y, d->cell, pos, sup, allowed, n, pose, axes, half_angle, area);
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
+
+extern "C" int wsb_disk_dir_extreme(const wsb_disks* d_, const double* pos, const double* sup, const int32_t* allowed,
+                                    int64_t n, const double* pose, const double* vecs, double* out, void* stream) {
+  const Disks* d = reinterpret_cast<const Disks*>(d_);
+  if (!d) return fail(WSB_ERR_ARG, "wsb_disk_dir_extreme: NULL disks");
+  if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_disk_dir_extreme: row count out of range");
+  if (n == 0) return WSB_OK;
+  if (!pos || !sup || !pose || !vecs || !out) return fail(WSB_ERR_ARG, "wsb_disk_dir_extreme: NULL array");
+  WSB_CUDA(cudaSetDevice(d->device));
+  k_disk_dir<<<(unsigned)((n + kDiskThreads - 1) / kDiskThreads), kDiskThreads, 0, (cudaStream_t)stream>>>(
+      d->cstart, d->items, d->nx, d->ny, d->lo_x, d->lo_y, d->cell, pos, sup, allowed, n, pose, vecs, out);
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }

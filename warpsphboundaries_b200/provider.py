@@ -289,8 +289,9 @@ class FusedWall(WallAggregate):
         """no lazily derived buffers exist in this implementation (fused.py:721-725)."""
 
     def _surfaces(self):
-        """(body index, native surface, workspace, bytes, pose) of every (body, surface), each workspace prepared for
-        this position set (wsb_aggregate_prepare: body frame, broadphase, neighbour masks, indicator)."""
+        """(body index, native surface or disk set, workspace, bytes, pose) of every (body, representation); a
+        surface's workspace is prepared for this position set (wsb_aggregate_prepare: body frame, broadphase,
+        neighbour masks, indicator), a disk set needs none (None, 0)."""
         N = self.N
         for bi, body in enumerate(self.scene.bodies):
             if not body.reps:
@@ -299,8 +300,8 @@ class FusedWall(WallAggregate):
             obb = (_lib.ctypes.c_double * 4)(*body.obb())
             for rep in body.fused_reps(self.support, self.dev):
                 if isinstance(rep, DiskArrayRep):
-                    raise NotImplementedError("FusedWall: the cone area and direction extreme of disk sets "
-                                              "(fused.py:754-785, 801-819) are not built")
+                    yield bi, rep.native(self.support, self.dev), None, 0, pose
+                    continue
                 ns = rep.native(self.support, self.dev)
                 if self.workspaces is not None:
                     ws = self.workspaces[id(rep)]
@@ -327,6 +328,10 @@ class FusedWall(WallAggregate):
             raise ValueError(f"FusedWall.cone_area: axes of shape {tuple(ax.shape)}, expected ({N}, 2)")
         out = torch.zeros(2 * N, dtype=F64, device=self.dev)
         for _, ns, ws, need, pose in self._surfaces():
+            if ws is None:
+                check(lib.wsb_disk_cone_area(ns.handle, ptr(self._pos), ptr(self._sup), ptr(self._allowed), N,
+                                             ptr(pose), ptr(ax), ha, ptr(out), _stream()), "wsb_disk_cone_area")
+                continue
             check(lib.wsb_cone_area(ns.handle, ptr(self._sup), N, ptr(pose), ptr(ax), ha, ptr(out), ptr(ws), need,
                                     _stream()), "wsb_cone_area")
         return out.reshape(2, N)
@@ -342,6 +347,10 @@ class FusedWall(WallAggregate):
             raise ValueError(f"FusedWall.dir_extreme: vecs of shape {tuple(v.shape)}, expected ({B}, {N}, 2)")
         out = torch.zeros((B, N), dtype=F64, device=self.dev)
         for bi, ns, ws, need, pose in self._surfaces():
+            if ws is None:
+                check(lib.wsb_disk_dir_extreme(ns.handle, ptr(self._pos), ptr(self._sup), ptr(self._allowed), N,
+                                               ptr(pose), ptr(v[bi]), ptr(out[bi]), _stream()), "wsb_disk_dir_extreme")
+                continue
             check(lib.wsb_dir_extreme(ns.handle, N, ptr(pose), ptr(v[bi]), ptr(out[bi]), ptr(ws), need, _stream()),
                   "wsb_dir_extreme")
         return out
