@@ -137,9 +137,10 @@ int wsb_aggregate_evaluate(const wsb_surface* s, int kernel, int precision, cons
  * (src/warpSPHBoundaries/scene/fused.py:506-547; edge/warpfused.py:58-109 FusedPlan and :190 fused_channels).
  * kernels [n_groups] (host) lists the groups' kernel ids; lam, G, cov, m1, m2 are HOST arrays of n_groups device
  * pointers each (the array, or an entry, may be NULL when out_mask leaves that output out); group g is written as
- * wsb_aggregate_evaluate with kernels[g] would write it.  When the groups are exactly {cubic, w2, w4, w6} or
- * {w2, w4, w6} (any order) one pass over the neighbour pairs evaluates them all, sharing each pair's chord, special
- * functions and monomial integrals between kernel blocks of equal support radius; other sets run one pass per group.
+ * wsb_aggregate_evaluate with kernels[g] would write it.  The first of the kernel sets {cubic, w2, w4, w6},
+ * {w2, w4, w6}, {w2, cone, lw2}, {w4, cone, lw4}, {w2, cone}, {w4, cone} that the groups contain (each kernel once,
+ * any order) is evaluated in one pass over the neighbour pairs, sharing each pair's chord, special functions and
+ * monomial integrals between kernel blocks of equal support radius; every other group runs its own pass.
  * At most WSB_MAX_GROUPS groups.  _groups = _prepare + _evaluate_groups. */
 enum { WSB_MAX_GROUPS = 8 };
 int wsb_aggregate_evaluate_groups(const wsb_surface* s, int n_groups, const int32_t* kernels, int precision,

@@ -1,8 +1,9 @@
 """Several kernel groups in one aggregate (wsb_aggregate_groups / FusedWall with a tuple of groups).
 
-The kernel sets {cubic, w2, w4, w6} and {w2, w4, w6} run as one pass over the neighbour pairs that shares each pair's
-chord, special functions and monomial integrals between kernel blocks of equal radius; every other set runs one pass
-per group.  Either way group g must equal the single-kernel aggregate of its kernel: the pack forms the same
+The kernel sets {cubic, w2, w4, w6}, {w2, w4, w6} and the delta+ sets {w2 | w4, cone[, lw2 | lw4]} run as one pass over
+the neighbour pairs that shares each pair's chord, special functions and monomial integrals between kernel blocks of
+equal radius (the first such set contained in the groups; the other groups one pass each); every other set runs one
+pass per group.  Either way group g must equal the single-kernel aggregate of its kernel: the pack forms the same
 quantities by the same operations, so the tolerance is a few ulp of the channel scale (1e-13), far below the 1e-10
 of the oracle comparisons.  The near-tangent scene of the parity tests is used, in both precision routes, with the
 groups in pack order and shuffled, plus a set that no pack covers, the oracle for the float64 pack, and FusedWall.
@@ -71,7 +72,8 @@ def _grouped_and_single(c2s, kernels, precision):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 @pytest.mark.parametrize("kernels", [("cubic", "w2", "w4", "w6"), ("w6", "cubic", "w4", "w2"), ("w2", "w4", "w6"),
-                                     ("w4", "w6", "w2")])
+                                     ("w4", "w6", "w2"), ("w2", "cone", "lw2"), ("lw4", "w4", "cone"), ("cone", "w2"),
+                                     ("w4", "cone", "w6"), ("cubic", "w2", "w4", "w6", "cone")])
 def test_packed_groups_equal_single_kernels(c2s, kernels, precision):
     grouped, single, h = _grouped_and_single(c2s, kernels, precision)
     for k, g, s in zip(kernels, grouped, single):

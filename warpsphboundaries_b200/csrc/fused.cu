@@ -1147,13 +1147,19 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   return WSB_OK;
 }
 
-// the kernel sets evaluated in one pass (as a set: the groups may come in any order); other sets run one pass per group
+// The kernel sets evaluated in one pass over the neighbour pairs, largest first: the smoothing-kernel families, and
+// the exact groups of the delta+ layout (scheme kernel, cone, wall-Laplacian kernel).  The first set contained in the
+// groups (each of its kernels exactly once, any order) runs as one pack; every other group runs its own pass.
 static const int32_t kPackCW[4] = {WSB_KERNEL_CUBIC, WSB_KERNEL_W2, WSB_KERNEL_W4, WSB_KERNEL_W6};
 static const int32_t kPackW[3] = {WSB_KERNEL_W2, WSB_KERNEL_W4, WSB_KERNEL_W6};
+static const int32_t kPackD2L[3] = {WSB_KERNEL_W2, WSB_KERNEL_CONE, WSB_KERNEL_LW2};
+static const int32_t kPackD4L[3] = {WSB_KERNEL_W4, WSB_KERNEL_CONE, WSB_KERNEL_LW4};
+static const int32_t kPackD2[2] = {WSB_KERNEL_W2, WSB_KERNEL_CONE};
+static const int32_t kPackD4[2] = {WSB_KERNEL_W4, WSB_KERNEL_CONE};
 
-// perm[p] = the group holding pack kernel p when the groups are exactly the pack's kernels, each once
+// perm[p] = the group holding pack kernel p when each of the pack's kernels is exactly one of the groups
 static bool match_pack(const int32_t* kernels, int n_groups, const int32_t* pack, int m, int* perm) {
-  if (n_groups != m) return false;
+  if (n_groups < m) return false;
   for (int p = 0; p < m; ++p) {
     perm[p] = -1;
     for (int g = 0; g < n_groups; ++g)
@@ -1186,17 +1192,24 @@ extern "C" int wsb_aggregate_evaluate_groups(const wsb_surface* s_, int n_groups
   if (!sup || !pose) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate_groups: NULL array");
   auto pick = [&](double* const* a, int g, int bit) { return (a && (out_mask & bit)) ? a[g] : nullptr; };
   int perm[kMaxPack];
-  const bool cw = match_pack(kernels, n_groups, kPackCW, 4, perm);
-  const bool wn = !cw && match_pack(kernels, n_groups, kPackW, 3, perm);
-  if (!cw && !wn) {                                                 // one pass per group
-    for (int g = 0; g < n_groups; ++g) {
-      const int rc = wsb_aggregate_evaluate(s_, kernels[g], precision, sup, n, pose, out_mask, pick(lam, g, WSB_OUT_LAM),
-                                            pick(G, g, WSB_OUT_G), pick(cov, g, WSB_OUT_COV), pick(m1, g, WSB_OUT_M1),
-                                            pick(m2, g, WSB_OUT_M2), workspace, workspace_bytes, stream);
-      if (rc) return rc;
+  int which = -1, m = 0;
+  const int32_t* packs[6] = {kPackCW, kPackW, kPackD2L, kPackD4L, kPackD2, kPackD4};
+  const int sizes[6] = {4, 3, 3, 3, 2, 2};
+  for (int k = 0; k < 6 && which < 0; ++k)
+    if (match_pack(kernels, n_groups, packs[k], sizes[k], perm)) {
+      which = k;
+      m = sizes[k];
     }
-    return WSB_OK;
+  bool in_pack[WSB_MAX_GROUPS] = {false};
+  for (int p = 0; p < m; ++p) in_pack[perm[p]] = true;
+  for (int g = 0; g < n_groups; ++g) {                              // the groups outside the pack: one pass each
+    if (in_pack[g]) continue;
+    const int rc = wsb_aggregate_evaluate(s_, kernels[g], precision, sup, n, pose, out_mask, pick(lam, g, WSB_OUT_LAM),
+                                          pick(G, g, WSB_OUT_G), pick(cov, g, WSB_OUT_COV), pick(m1, g, WSB_OUT_M1),
+                                          pick(m2, g, WSB_OUT_M2), workspace, workspace_bytes, stream);
+    if (rc) return rc;
   }
+  if (which < 0) return WSB_OK;
   const Workspace w = carve(s, n, const_cast<void*>(workspace));
   if (!workspace || workspace_bytes < w.total)
     return fail(WSB_ERR_SIZE, "wsb_aggregate_evaluate_groups: workspace too small");
@@ -1205,25 +1218,27 @@ extern "C" int wsb_aggregate_evaluate_groups(const wsb_surface* s_, int n_groups
   const SurfView v = view_of(s);
   const bool assign = (out_mask & WSB_OUT_ASSIGN) != 0;
   PackOut o{};
-  for (int p = 0; p < (cw ? 4 : 3); ++p) {
+  for (int p = 0; p < m; ++p) {
     o.lam[p] = pick(lam, perm[p], WSB_OUT_LAM);
     o.G[p] = pick(G, perm[p], WSB_OUT_G);
     o.cov[p] = pick(cov, perm[p], WSB_OUT_COV);
     o.m1[p] = pick(m1, perm[p], WSB_OUT_M1);
     o.m2[p] = pick(m2, perm[p], WSB_OUT_M2);
   }
-  using PCW = KPack<Kern_cubic, Kern_w2, Kern_w4, Kern_w6>;
-  using PW = KPack<Kern_w2, Kern_w4, Kern_w6>;
-  if (cw) {
+  auto run = [&](auto pack) {
+    using P = decltype(pack);
     if (precision == WSB_PREC_MIXED)
-      launch_pack<PCW, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
+      launch_pack<P, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
     else
-      launch_pack<PCW, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
-  } else {
-    if (precision == WSB_PREC_MIXED)
-      launch_pack<PW, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
-    else
-      launch_pack<PW, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
+      launch_pack<P, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
+  };
+  switch (which) {
+    case 0: run(KPack<Kern_cubic, Kern_w2, Kern_w4, Kern_w6>{}); break;
+    case 1: run(KPack<Kern_w2, Kern_w4, Kern_w6>{}); break;
+    case 2: run(KPack<Kern_w2, Kern_cone, Kern_lw2>{}); break;
+    case 3: run(KPack<Kern_w4, Kern_cone, Kern_lw4>{}); break;
+    case 4: run(KPack<Kern_w2, Kern_cone>{}); break;
+    default: run(KPack<Kern_w4, Kern_cone>{}); break;
   }
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
