@@ -45,6 +45,7 @@ KERNEL_NAMES = {v: k for k, v in KERNEL_IDS.items()}
 # evaluated by a graded Gauss-Legendre quadrature along the chord instead of the monomial closed form
 QUAD_KERNEL_IDS = {"w2p5": 10, "w4p5": 11}
 QUAD_GAUSS = 24
+QUAD_GAUSS_FAR = 12      # panels at least their own length away from the foot (Bernstein parameter >= 5.8)
 
 # published 2-D normalisations C2 * pi (src/warpSPHBoundaries/curvbound/kernels.py:5-13,
 # src/warpSPHBoundaries/edge/kernels.py:183-185); only used to check the recomputed ones
@@ -520,6 +521,7 @@ def emit_quad() -> list:
     chord panels."""
     import numpy as np
     gx, gw = np.polynomial.legendre.leggauss(QUAD_GAUSS)
+    fx, fw = np.polynomial.legendre.leggauss(QUAD_GAUSS_FAR)
     out = ["// x^N by squaring",
            "template <int N>",
            "__host__ __device__ __forceinline__ double qpow(double x) {",
@@ -534,7 +536,11 @@ def emit_quad() -> list:
            "}",
            f"constexpr int kQuadGauss = {QUAD_GAUSS};",
            "static __device__ const double kQuadGx[kQuadGauss] = {" + ", ".join(repr(float(x)) for x in gx) + "};",
-           "static __device__ const double kQuadGw[kQuadGauss] = {" + ", ".join(repr(float(x)) for x in gw) + "};", ""]
+           "static __device__ const double kQuadGw[kQuadGauss] = {" + ", ".join(repr(float(x)) for x in gw) + "};",
+           f"constexpr int kQuadGaussFar = {QUAD_GAUSS_FAR};",
+           "static __device__ const double kQuadFx[kQuadGaussFar] = {" + ", ".join(repr(float(x)) for x in fx) + "};",
+           "static __device__ const double kQuadFw[kQuadGaussFar] = {" + ", ".join(repr(float(x)) for x in fw) + "};",
+           ""]
     for name, kid in sorted(QUAD_KERNEL_IDS.items(), key=lambda t: t[1]):
         C, p, base = quad_kernel(name)
         out.append(f"// ---- {name}: C2*pi = {C}; pi*W = C u^{p} B(u)^5, u = 1 - r, on r <= 1")
