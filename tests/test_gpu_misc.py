@@ -36,6 +36,44 @@ def test_signed_distance_matches_brute_force():
     assert np.abs(np.linalg.norm(nn, axis=1) - 1).max() < 1e-12
 
 
+@pytest.mark.parametrize("support", [0.004, 0.05])
+def test_signed_distance_ring_search_equals_the_scan(support):
+    """wsb_signed_distance searches rings of grid cells around the point (every edge is listed in the cells it
+    crosses): the distance, closest point and edge of every point equal a scan over all edges -- points near and far
+    inside the grid (up to ~100 rings at support 0.004) and outside it (the scan)."""
+    from warpsphboundaries_b200 import _lib
+    from warpsphboundaries_b200.scene import _stream
+    loops = workloads.stars(3, (32, 96), seed=4, box=1.0)
+    rep = SurfaceRep.loops(loops)
+    ns = rep.native(support, DEV)
+    rng = np.random.default_rng(5)
+    P = np.concatenate([rng.uniform(-0.3, 1.3, size=(6000, 2)), rng.uniform(-3.0, 4.0, size=(500, 2))])
+    m = len(P)
+    lp = torch.tensor(P, dtype=torch.float64, device=DEV)
+    d = torch.empty(m, dtype=torch.float64, device=DEV)
+    cp = torch.empty((m, 2), dtype=torch.float64, device=DEV)
+    nl = torch.empty((m, 2), dtype=torch.float64, device=DEV)
+    ed = torch.empty(m, dtype=torch.int32, device=DEV)
+    _lib.check(_lib.lib.wsb_signed_distance(ns.handle, _lib.ptr(lp), m, support, _lib.ptr(d), _lib.ptr(cp),
+                                            _lib.ptr(nl), _lib.ptr(ed), _stream()), "wsb_signed_distance")
+    V, E = rep.vertices.cpu().numpy(), rep.edges.cpu().numpy().astype(np.int64)
+    a, b = V[E[:, 0]], V[E[:, 1]]
+    e = b - a
+    t = np.clip((((P[:, None, :] - a[None]) * e[None]).sum(2)) / (e * e).sum(1)[None], 0, 1)
+    c = a[None] + t[..., None] * e[None]
+    dist = np.linalg.norm(P[:, None, :] - c, axis=2)
+    k = dist.argmin(1)
+    dmin = dist[np.arange(m), k]
+    srt = np.sort(dist, axis=1)
+    unique = srt[:, 1] - srt[:, 0] > 1e-12
+    got = d.cpu().numpy()
+    assert np.abs(np.abs(got) - dmin).max() < 1e-14
+    assert np.array_equal(ed.cpu().numpy()[unique], k[unique])
+    assert np.abs(cp.cpu().numpy()[unique] - c[np.arange(m), k][unique]).max() < 1e-14
+    ins = O.indicator(V, E, 0, P) > 0.5
+    assert np.array_equal(got < 0, ins & (dmin > 0))
+
+
 def test_kinematics_bit_exact():
     bodies = [Body(center=(0.3, -0.2), angle=0.4, linearVelocity=(1.0, -0.5), angularVelocity=2.5,
                    linearAcceleration=(0.1, 0.2), angularAcceleration=-0.7),

@@ -674,6 +674,29 @@ __global__ void __launch_bounds__(kThreads) k_agg_backward(SurfView S, const dou
 }
 
 // ------------------------------------------------------------------------------------------------ signed distance
+// the segment distance of a point to edge record r with the rounding of the reference's brute force; the nearest
+// edge wins, the lower edge id on an exact tie (the order of a scan over all edges)
+__device__ __forceinline__ void nearest_edge(double px, double py, const double4& r, int64_t e, double& best,
+                                             double& bx, double& by, int64_t& be) {
+  const double ex = __dsub_rn(r.z, r.x), ey = __dsub_rn(r.w, r.y);
+  double t = __ddiv_rn(__dadd_rn(__dmul_rn(__dsub_rn(px, r.x), ex), __dmul_rn(__dsub_rn(py, r.y), ey)),
+                       __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)));
+  t = fmin(fmax(t, 0.0), 1.0);
+  const double cx = __dadd_rn(r.x, __dmul_rn(t, ex)), cy = __dadd_rn(r.y, __dmul_rn(t, ey));
+  const double ddx = __dsub_rn(px, cx), ddy = __dsub_rn(py, cy);
+  const double dist = __dsqrt_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)));
+  if (dist < best || (dist == best && e < be)) {
+    best = dist;
+    bx = cx;
+    by = cy;
+    be = e;
+  }
+}
+
+// Signed distance to the nearest edge.  Inside the cell grid the search visits square rings of cells around the
+// point's cell: every edge is listed in each cell it passes through, so after ring k an edge not yet seen is farther
+// than k cells and the search stops once the best distance is below that; outside the grid (farther than one
+// support from every edge) all edges are scanned.  Same distances, closest points and edges as a scan over all edges.
 __global__ void k_signed_distance(SurfView S, const double* __restrict__ lpos, int64_t m, double norm_support,
                                   double* d, double* cp, double* nl, int32_t* edge) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -681,24 +704,30 @@ __global__ void k_signed_distance(SurfView S, const double* __restrict__ lpos, i
   const double px = lpos[2 * i], py = lpos[2 * i + 1];
   double best = INFINITY, bx = 0.0, by = 0.0;
   int64_t be = -1;
-  for (int64_t e = 0; e < S.n_edges; ++e) {
-    const double4 r = S.erec[e];
-    const double ex = __dsub_rn(r.z, r.x), ey = __dsub_rn(r.w, r.y);
-    double t = __ddiv_rn(__dadd_rn(__dmul_rn(__dsub_rn(px, r.x), ex), __dmul_rn(__dsub_rn(py, r.y), ey)),
-                         __dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)));
-    t = fmin(fmax(t, 0.0), 1.0);
-    const double cx = __dadd_rn(r.x, __dmul_rn(t, ex)), cy = __dadd_rn(r.y, __dmul_rn(t, ey));
-    const double ddx = __dsub_rn(px, cx), ddy = __dsub_rn(py, cy);
-    const double dist = __dsqrt_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)));
-    if (dist < best) {
-      best = dist;
-      bx = cx;
-      by = cy;
-      be = e;
-    }
-  }
   int32_t cid;
   const bool in_grid = cell_of(S, px, py, cid);
+  if (in_grid) {
+    const int cx = cid / S.ny, cy = cid % S.ny;
+    const int kmax = max(S.nx, S.ny);
+    auto scan_cell = [&](int x, int y) {
+      const int32_t c = x * S.ny + y;
+      for (int32_t k = S.cstart[c]; k < S.cstart[c + 1]; ++k) nearest_edge(px, py, ldg4(S.crec + k), S.citems[k], best, bx, by, be);
+    };
+    for (int k = 0; k <= kmax; ++k) {
+      const int x0 = max(cx - k, 0), x1 = min(cx + k, S.nx - 1);
+      for (int x = x0; x <= x1; ++x) {
+        if (x == cx - k || x == cx + k) {                  // a full column of the ring
+          for (int y = max(cy - k, 0); y <= min(cy + k, S.ny - 1); ++y) scan_cell(x, y);
+        } else {                                           // its top and bottom cells
+          if (cy - k >= 0) scan_cell(x, cy - k);
+          if (cy + k < S.ny && k > 0) scan_cell(x, cy + k);
+        }
+      }
+      if (best < (double)k * S.cell * (1.0 - 1e-12)) break;
+    }
+  } else {
+    for (int64_t e = 0; e < S.n_edges; ++e) nearest_edge(px, py, S.erec[e], e, best, bx, by, be);
+  }
   const double ind = indicator_at(S, px, py, norm_support > 0.0 ? norm_support : 1.0, in_grid, cid);
   const bool ins = ind > 0.5;
   d[i] = ins ? -best : best;
