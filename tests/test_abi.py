@@ -64,3 +64,25 @@ def test_detector_inputs_check_their_arguments_without_a_device():
     from warpsphboundaries_b200 import _lib
     assert _lib.lib.wsb_cone_area(None, None, 4, None, None, 0.5, None, None, 0, None) == _lib.WSB_ERR_ARG
     assert _lib.lib.wsb_dir_extreme(None, 4, None, None, None, None, 0, None) == _lib.WSB_ERR_ARG
+
+
+def test_disk_entry_points_check_their_arguments_without_a_device():
+    """the disk element refuses bad inputs before touching a device: NULL handles, a non-positive radius, a
+    non-finite centre, a bad support, an unknown kernel id."""
+    import math
+    from warpsphboundaries_b200 import _lib
+    L = _lib.lib
+    D = ctypes.c_double
+    h = ctypes.c_void_p()
+    c = (D * 4)(0.0, 0.0, 1.0, 1.0)
+    for radii, sup in (((D * 2)(0.5, -1.0), 0.1), ((D * 2)(0.5, 0.5), 0.0), ((D * 2)(0.5, 0.5), math.inf)):
+        assert L.wsb_disks_create(c, radii, 2, sup, 0, ctypes.byref(h)) == _lib.WSB_ERR_ARG
+    bad = (D * 4)(0.0, math.nan, 1.0, 1.0)
+    assert L.wsb_disks_create(bad, (D * 2)(0.5, 0.5), 2, 0.1, 0, ctypes.byref(h)) == _lib.WSB_ERR_ARG
+    assert L.wsb_disks_create(c, (D * 2)(0.5, 0.5), 2, 0.1, 0, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_disk_aggregate(None, 1, None, None, None, 4, None, _lib.OUT_ALL, None, None, None, None, None, None,
+                                0, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_disk_cone_area(None, None, None, None, 4, None, None, 0.5, None, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_disk_dir_extreme(None, None, None, None, 4, None, None, None, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_disk_workspace_size(None, 4) == 0
+    assert L.wsb_disks_destroy(None) == _lib.WSB_OK
