@@ -117,3 +117,27 @@ def test_closed_surfaces_in_the_mix():
         assert torch.equal(srv.result(rid)["channels"], ref), (sid, k, rows)
     with pytest.raises(NotImplementedError):
         srv.submit("m0", pos3(10, 1), h, "w4", grad=True)
+
+
+def test_lowered_bodies_are_served():
+    """a box, a cavity disk and a sampled distance are served as the polygons the provider integrates (bit-identical
+    to FusedWall); a disk set is refused."""
+    from warpsphboundaries_b200.implicit import DiskBody
+    from warpsphboundaries_b200.scene import BoxRep, DiskArrayRep, ImplicitRep, SdfRep
+    h = 0.02
+    sdf = SdfRep.fromFunction(lambda p: (p - torch.tensor([0.5, 0.5], dtype=torch.float64)).norm(dim=1) - 0.3,
+                              (0.0, 0.0), (1.0, 1.0), h / 8)
+    scene = Scene([Body(reps=[BoxRep((0.1, 0.1), (0.3, 0.4))]), Body(reps=[sdf]),
+                   Body(center=(0.5, 0.5), reps=[ImplicitRep(DiskBody((0.0, 0.0), 0.7, solid="outside"))])], DEV)
+    srv = BoundaryServer(DEV, streams=2, graph_max_rows=1 << 12)
+    srv.register("low", scene, h)
+    pos = _positions(4000, 9)
+    rid = srv.submit("low", pos, h, "w2")
+    srv.run()
+    torch.cuda.synchronize()
+    fw = FusedWall(scene, ParticleState(pos, torch.full((4000,), h, dtype=torch.float64, device=DEV)), h,
+                   (FusedGroup("w2"),))
+    for key in OUT_KEYS:
+        assert torch.equal(srv.result(rid)[key], fw.res[0][key]), key
+    with pytest.raises(NotImplementedError):
+        srv.register("disks", Scene([Body(reps=[DiskArrayRep([[0.5, 0.5]], [0.1])])], DEV), h)

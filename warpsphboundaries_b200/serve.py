@@ -157,12 +157,13 @@ class BoundaryServer:
         """keep `scene` resident: its surfaces' static structures are built now for `support`, with the launch plan
         (pose, body box, surface handles) resolved once."""
         for b in scene.bodies:
-            for r in b.reps:
+            for r in b.fused_reps(float(support), self.device):     # boxes, cavities, sampled distances: polygons
                 if not isinstance(r, SurfaceRep) or r._triangle:
-                    raise NotImplementedError("BoundaryServer: surface loops only (no conditioned single triangles)")
+                    raise NotImplementedError("BoundaryServer: surface loops only (no disk sets, no conditioned "
+                                              "single triangles)")
         plan = []
         for b in scene.bodies:
-            reps = [r.native(float(support), self.device) for r in b.reps]
+            reps = [r.native(float(support), self.device) for r in b.fused_reps(float(support), self.device)]
             plan.append((b.pose_tensor(self.device), (_lib.ctypes.c_double * 4)(*b.obb()), int(b.unbounded()), reps))
             for ns in reps:
                 self.ws_bytes = max(self.ws_bytes, int(lib.wsb_aggregate_workspace_size(ns.handle, self.max_batch_rows)))
@@ -278,7 +279,7 @@ class BoundaryServer:
         B = len(scene.bodies)
         ws = 0
         for b in scene.bodies:
-            for r in b.reps:
+            for r in b.fused_reps(support, self.device):
                 ws = max(ws, int(lib.wsb_aggregate_workspace_size(r.native(support, self.device).handle, rows)))
         return (8 * 13 * B + 24 + (16 if grad else 0)) * rows + ws
 
