@@ -141,3 +141,33 @@ def test_evaluator_subset_and_physical_units():
     ref = np.array([float(v) for v in c["values"]])
     want = np.array([ref[26], ref[6], ref[0]])
     assert np.abs(got - want).max() < 1e-10 * (1 + np.abs(want).max())
+
+
+def test_tetrahedral_mesh_equals_its_surface():
+    """a tetrahedral mesh (fluxbridge Geometry(elements, 3, 'volume')) is served through the boundary of its union:
+    the fan of a jittered icosphere from its centre equals the icosphere's closed surface, and a cube of five
+    tetrahedra the oracle's box, within 1e-12 (1 + |v|); the reference's tetrahedral method names are accepted."""
+    from warpsphboundaries_b200 import workloads as W
+    from warpsphboundaries_b200.mesh3d import Evaluator, Geometry
+    V, Fc = W.icosphere(2, 0.6, 0.03, seed=5)
+    fan = Geometry.from_elements([np.stack([np.zeros(3), V[a], V[b], V[c]]) for a, b, c in Fc])
+    rng = np.random.default_rng(11)
+    Q = rng.uniform(-0.8, 0.8, (400, 3))
+    h = rng.uniform(0.05, 0.2, len(Q))
+    a = Evaluator(fan, kernel="w4", method="tet_quadrature").evaluate(Q, h)
+    b = Evaluator(Geometry.closed_surface(V, Fc), kernel="w4").evaluate(Q, h)
+    a, b = np.asarray(a), np.asarray(b)
+    assert np.abs(a - b).max() / (1 + np.abs(b).max()) < 1e-12
+    C = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], float) * 0.5 - 0.25
+    i = lambda x, y, z: x * 4 + y * 2 + z
+    tets = [[i(0, 0, 0), i(1, 0, 0), i(0, 1, 0), i(0, 0, 1)], [i(1, 1, 0), i(1, 0, 0), i(0, 1, 0), i(1, 1, 1)],
+            [i(1, 0, 1), i(1, 0, 0), i(1, 1, 1), i(0, 0, 1)], [i(0, 1, 1), i(0, 1, 0), i(0, 0, 1), i(1, 1, 1)],
+            [i(1, 0, 0), i(0, 1, 0), i(0, 0, 1), i(1, 1, 1)]]
+    cube = Geometry.from_elements([C[t] for t in tets])
+    Qc = rng.uniform(-0.4, 0.4, (24, 3))
+    hc = np.full(len(Qc), 0.15)
+    Evaluator(cube, kernel="w2", method="conditioned_boundary").evaluate(Qc, hc)      # the reference's method name
+    got, _ = _run(cube.vertices, cube.faces, Qc, hc, "w2", smax=0.15)
+    for k in range(len(Qc)):
+        ref = M3.channels(cube.vertices, cube.faces, Qc[k], hc[k], "w2")
+        assert np.abs(got[k] - ref).max() / (1 + np.abs(ref).max()) < 1e-8

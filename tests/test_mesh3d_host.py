@@ -5,7 +5,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from warpsphboundaries_b200 import _lib
+from warpsphboundaries_b200 import _lib, workloads
 from warpsphboundaries_b200.mesh3d import Evaluator, Geometry, _column
 from warpsphboundaries_b200.radial import Request, baseline
 
@@ -74,3 +74,36 @@ def test_evaluator_arguments():
         ev.prepare([[np.nan, 0.1, 0.1]], 0.1)
     with pytest.raises(ValueError):                                    # element < 1e-4 of the support
         Evaluator(Geometry.closed_surface(V * 1e-5, F)).prepare([[0.1, 0.1, 0.1]], 1.0)
+
+
+def _cube_tets():
+    C = np.array([[x, y, z] for x in (0, 1) for y in (0, 1) for z in (0, 1)], float)
+    i = lambda x, y, z: x * 4 + y * 2 + z
+    tets = [[i(0, 0, 0), i(1, 0, 0), i(0, 1, 0), i(0, 0, 1)], [i(1, 1, 0), i(1, 0, 0), i(0, 1, 0), i(1, 1, 1)],
+            [i(1, 0, 1), i(1, 0, 0), i(1, 1, 1), i(0, 0, 1)], [i(0, 1, 1), i(0, 1, 0), i(0, 0, 1), i(1, 1, 1)],
+            [i(1, 0, 0), i(0, 1, 0), i(0, 0, 1), i(1, 1, 1)]]
+    return [C[t] for t in tets]
+
+
+def test_tetrahedral_mesh_boundary():
+    """Geometry.from_elements (fluxbridge geometry.py:20-63): a conforming tetrahedral mesh becomes the closed
+    surface of its union -- the shared faces cancel, every boundary face is outward -- for a cube of five tetrahedra
+    (12 faces, volume 1) and a fan of an icosphere from its centre (the icosphere's own 320 faces, same volume);
+    overlapping and degenerate elements and 2-D / surface elements are refused."""
+    from warpsphboundaries_b200.mesh3d import Geometry
+    g = Geometry.from_elements(_cube_tets())
+    vol = lambda V, F: sum(float(np.dot(V[a], np.cross(V[b], V[c]))) for a, b, c in F) / 6
+    assert len(g.faces) == 12 and len(g.vertices) == 8 and abs(vol(g.vertices, g.faces) - 1.0) < 1e-15
+    assert g.from_tets
+    Vs, Fs = workloads.icosphere(2, 0.6, 0.02, seed=3)
+    fan = Geometry.from_elements([np.stack([np.zeros(3), Vs[a], Vs[b], Vs[c]]) for a, b, c in Fs])
+    assert len(fan.faces) == len(Fs) and abs(vol(fan.vertices, fan.faces) - vol(Vs, Fs)) < 1e-14
+    assert {tuple(sorted(map(tuple, fan.vertices[f]))) for f in fan.faces} == \
+        {tuple(sorted(map(tuple, Vs[f]))) for f in Fs}
+    t0 = _cube_tets()[0]
+    with pytest.raises(ValueError):
+        Geometry.from_elements([t0, t0])
+    with pytest.raises(ValueError):
+        Geometry.from_elements([np.array([[0, 0, 0], [1, 0, 0], [2, 0, 0], [0, 1, 0]], float)])
+    with pytest.raises(NotImplementedError):
+        Geometry.from_elements([np.eye(3)], dimension=2)

@@ -98,11 +98,56 @@ class Geometry:
         self.faces = np.ascontiguousarray(np.asarray(faces, dtype=np.int64).reshape(-1, 3))
         if not np.isfinite(self.vertices).all():
             raise ValueError("vertices must be finite")
+        self.from_tets = False
         self._meshes = {}
 
     @classmethod
     def closed_surface(cls, vertices, faces):
         return cls(vertices, faces)
+
+    @classmethod
+    def from_elements(cls, elements, dimension=3, measure="volume"):
+        """the solid of a conforming tetrahedral mesh (fluxbridge geometry.py:20-63: `Geometry(elements, 3,
+        'volume')`, each element a [4, 3] array).  The requests are integrals over the solid, and over a conforming
+        mesh the elements' integrals add up to those of the union, whose boundary the closed-surface path
+        integrates exactly: every face is oriented outward from its tetrahedron (the reference's rule), vertices are
+        welded by exact coordinates, and the faces that two tetrahedra share with opposite orientations cancel.
+        ValueError for a degenerate tetrahedron or a face shared with the same orientation (overlapping elements);
+        NotImplementedError for 2-D elements and surface measure."""
+        if dimension != 3 or measure != "volume":
+            raise NotImplementedError("fluxbridge elements: 3-D volume tetrahedra only (closed_surface for a skin)")
+        index, verts, count = {}, [], {}
+        for el in elements:
+            v = np.asarray(el, dtype=np.float64)
+            if v.shape != (4, 3) or not np.isfinite(v).all():
+                raise ValueError("volume elements must be tetrahedra with finite vertices")
+            ids = []
+            for p in v:
+                key = tuple(float(x) for x in p)
+                if key not in index:
+                    index[key] = len(verts)
+                    verts.append(key)
+                ids.append(index[key])
+            for i in range(4):
+                f = [j for j in range(4) if j != i]
+                p, q, r = v[f]
+                side = float(np.dot(np.cross(q - p, r - p), v[i] - p))
+                if side == 0.0:
+                    raise ValueError("degenerate tetrahedron")
+                if side > 0:                          # the opposite vertex lies on the normal's side: flip outward
+                    f[1], f[2] = f[2], f[1]
+                tri = tuple(ids[j] for j in f)
+                k = min(range(3), key=lambda s: tri[s])
+                tri = tri[k:] + tri[:k]               # rotation with the smallest id first keeps the orientation
+                if tri in count:
+                    raise ValueError("two tetrahedra share a face with the same orientation (overlapping elements)")
+                count[tri] = 1
+        faces = [tri for tri in count if (tri[0], tri[2], tri[1]) not in count]
+        if not faces:
+            raise ValueError("no boundary faces")
+        g = cls(np.array(verts), np.array(faces, dtype=np.int64))
+        g.from_tets = True
+        return g
 
     def native(self, support_max, device):
         """the device copy whose grid serves supports up to `support_max` (rebuilt when a larger one is asked)."""
@@ -122,9 +167,11 @@ class Evaluator:
     """the baseline kernel integrals of a closed surface at queries (fluxbridge evaluate.py:11-187)."""
 
     def __init__(self, geometry, requests=None, *, kernel="w2", precision="float64", device="cuda", compact=False,
-                 method="analytic", search="device"):
+                 method="analytic", search="device", nodes=16, preparation="host"):
         if not isinstance(geometry, Geometry):
-            raise ValueError("geometry must come from Geometry.closed_surface")
+            raise ValueError("geometry must come from Geometry.closed_surface or Geometry.from_elements")
+        if method in ("conditioned_boundary", "tet_quadrature") and geometry.from_tets:
+            method = "analytic"      # the same integrals over the solid, here by the exact boundary reduction
         if kernel not in KERNELS:
             raise ValueError("kernel must be one of " + ", ".join(KERNELS))
         if precision == "float32":
