@@ -75,36 +75,57 @@ __device__ void disk_pair(double D, double R, int lane, double out[7]) {
         knots[b] = knots[b - 1];
         knots[b - 1] = t;
       }
-    double d = 2.0 * base, u = 0.0;
+    auto node = [&](double uu, double wq) {
+      double sh, ch;
+      sincos(0.5 * uu, &sh, &ch);                                  // one half-angle evaluation per node
+      const double s2 = sh * sh, su = 2.0 * sh * ch, cu = fma(-2.0, s2, 1.0);
+      const double yx = fma(2.0 * R, s2, dm), yy = R * su, nx = -cu, ny = su;
+      const double yn = fma(2.0 * D, s2, -dm);
+      const double r = sqrt(fma(4.0 * D * R, s2, dm * dm));
+      double P, Fl, F2l;
+      disk_profile<KID>(r, 1.0 / (r * r), P, Fl, F2l);
+      const double F1 = Fl * r * r;
+      const double w = 2.0 * R * wq;
+      lam = fma(w * Fl, yn, lam);
+      m1 = fma(w * F1, nx, m1);
+      G = fma(-w * P, nx, G);
+      gxx = fma(-w * P * yx, nx, gxx);
+      gyy = fma(-w * P * yy, ny, gyy);
+      mxx = fma(w * F1 * yx, nx, mxx);
+      myy = fma(w * F1 * yy, ny, myy);
+      SF = fma(w * F2l, yn, SF);
+    };
+    // the panel after u: up to the doubling bound d or the next knot, whichever is first
+    double d = 2.0 * base;
     int ki = 0;
-    for (int it = 0; it < 160 && u < U; ++it) {
+    auto next_panel = [&](double u) {
       double nxt = fmin(U, d);
       while (ki < nk && knots[ki] <= u) ++ki;
       if (ki < nk && knots[ki] < nxt) nxt = knots[ki];
-      const double hc = 0.5 * (nxt - u), mc = 0.5 * (nxt + u);
-      for (int q = lane; q < kQuadGauss; q += 32) {
-        const double uu = fma(hc, kQuadGx[q], mc);
-        double sh, ch;
-        sincos(0.5 * uu, &sh, &ch);                                // one half-angle evaluation per node
-        const double s2 = sh * sh, su = 2.0 * sh * ch, cu = fma(-2.0, s2, 1.0);
-        const double yx = fma(2.0 * R, s2, dm), yy = R * su, nx = -cu, ny = su;
-        const double yn = fma(2.0 * D, s2, -dm);
-        const double r = sqrt(fma(4.0 * D * R, s2, dm * dm));
-        double P, Fl, F2l;
-        disk_profile<KID>(r, 1.0 / (r * r), P, Fl, F2l);
-        const double F1 = Fl * r * r;
-        const double w = 2.0 * R * hc * kQuadGw[q];
-        lam = fma(w * Fl, yn, lam);
-        m1 = fma(w * F1, nx, m1);
-        G = fma(-w * P, nx, G);
-        gxx = fma(-w * P * yx, nx, gxx);
-        gyy = fma(-w * P * yy, ny, gyy);
-        mxx = fma(w * F1 * yx, nx, mxx);
-        myy = fma(w * F1 * yy, ny, myy);
-        SF = fma(w * F2l, yn, SF);
-      }
       if (nxt >= d) d *= 2.0;
-      u = nxt;
+      return nxt;
+    };
+    // panels next to the nearest point (start below 2 * base) take 24 nodes on lanes 0-23; farther panels, whose
+    // singularities lie at least their own length away (Bernstein parameter >= 5.8), 12 nodes, two panels at a time
+    // (lanes 0-11 and 12-23)
+    double u = 0.0;
+    for (int it = 0; it < 160 && u < U; ++it) {
+      const double a0 = u, a1 = next_panel(u);
+      if (a0 < 2.0 * base) {
+        const double hc = 0.5 * (a1 - a0), mc = 0.5 * (a1 + a0);
+        if (lane < kQuadGauss) node(fma(hc, kQuadGx[lane], mc), hc * kQuadGw[lane]);
+        u = a1;
+        continue;
+      }
+      const double b1 = a1 < U ? next_panel(a1) : a1;
+      const bool second = lane >= kQuadGaussFar;
+      const double lo = second ? a1 : a0, hi = second ? b1 : a1;
+      const int q = second ? lane - kQuadGaussFar : lane;
+      if (q < kQuadGaussFar && hi > lo) {
+        const double hc = 0.5 * (hi - lo), mc = 0.5 * (hi + lo);
+        node(fma(hc, kQuadFx[q], mc), hc * kQuadFw[q]);
+      }
+      u = b1;
     }
   }
   lam = warp_allsum(lam);
