@@ -354,7 +354,8 @@ __device__ __forceinline__ void add_block(const PairGeo& g, const BlockSums& S, 
 // int_lo^hi pi*W(sqrt(s^2 + z^2)) ds of a quadrature kernel (KT::poly = pi*W on r <= 1), the chord [lo, hi] already
 // clipped to the support: Gauss-Legendre panels on both sides of the foot s = 0, graded from it -- the first up to
 // 2 max(|z|, 2^-24), then doubling.  pi*W is analytic except through r, whose branch points s = +-iz lie a panel's
-// half-length away from the first panel (Bernstein parameter ~2.9: 24 nodes, below 1e-15 there).  A panel [d, 2d]
+// half-length away from the first panel (Bernstein parameter ~2.9: 20 nodes, 2.9^-40 ~ 3e-19 times the polynomial's
+// growth on the ellipse; measured against adaptive quadrature at 1.2e-14 of the chord scale).  A panel [d, 2d]
 // with d >= 2 |z| sees them at least its own length away (parameter >= 3 + sqrt 8 = 5.8: 12 nodes reach 5.8^-24 =
 // 5e-19 times the growth of the degree-25 / 40 polynomial on the ellipse, ~1e3), so those take the 12-node rule.
 template <class KT>
@@ -374,9 +375,9 @@ __device__ __forceinline__ double quad_chord(double lo, double hi, double z) {
       double ps = 0.0;
       if (u < 2.0 * base) {
 #pragma unroll
-        for (int k = 0; k < kQuadGauss; ++k) {
-          const double x = fma(hc, kQuadGx[k], mc);
-          ps = fma(kQuadGw[k], KT::poly(fmin(sqrt(fma(x, x, zz)), 1.0)), ps);
+        for (int k = 0; k < kQuadGaussChord; ++k) {
+          const double x = fma(hc, kQuadCx[k], mc);
+          ps = fma(kQuadCw[k], KT::poly(fmin(sqrt(fma(x, x, zz)), 1.0)), ps);
         }
       } else {
 #pragma unroll

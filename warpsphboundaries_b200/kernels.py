@@ -46,6 +46,7 @@ KERNEL_NAMES = {v: k for k, v in KERNEL_IDS.items()}
 QUAD_KERNEL_IDS = {"w2p5": 10, "w4p5": 11}
 QUAD_GAUSS = 24
 QUAD_GAUSS_FAR = 12      # panels at least their own length away from the foot (Bernstein parameter >= 5.8)
+QUAD_GAUSS_CHORD = 20    # the tensile chord's panel next to the foot (parameter ~2.9: 2.9^-40 ~ 3e-19)
 
 # published 2-D normalisations C2 * pi (src/warpSPHBoundaries/curvbound/kernels.py:5-13,
 # src/warpSPHBoundaries/edge/kernels.py:183-185); only used to check the recomputed ones
@@ -522,6 +523,7 @@ def emit_quad() -> list:
     import numpy as np
     gx, gw = np.polynomial.legendre.leggauss(QUAD_GAUSS)
     fx, fw = np.polynomial.legendre.leggauss(QUAD_GAUSS_FAR)
+    cx, cw = np.polynomial.legendre.leggauss(QUAD_GAUSS_CHORD)
     out = ["// x^N by squaring",
            "template <int N>",
            "__host__ __device__ __forceinline__ double qpow(double x) {",
@@ -540,6 +542,9 @@ def emit_quad() -> list:
            f"constexpr int kQuadGaussFar = {QUAD_GAUSS_FAR};",
            "static __device__ const double kQuadFx[kQuadGaussFar] = {" + ", ".join(repr(float(x)) for x in fx) + "};",
            "static __device__ const double kQuadFw[kQuadGaussFar] = {" + ", ".join(repr(float(x)) for x in fw) + "};",
+           f"constexpr int kQuadGaussChord = {QUAD_GAUSS_CHORD};",
+           "static __device__ const double kQuadCx[kQuadGaussChord] = {" + ", ".join(repr(float(x)) for x in cx) + "};",
+           "static __device__ const double kQuadCw[kQuadGaussChord] = {" + ", ".join(repr(float(x)) for x in cw) + "};",
            ""]
     for name, kid in sorted(QUAD_KERNEL_IDS.items(), key=lambda t: t[1]):
         C, p, base = quad_kernel(name)
