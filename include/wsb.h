@@ -275,6 +275,16 @@ int wsb_disk_cone_area(const wsb_disks* d, const double* pos, const double* sup,
 int wsb_disk_dir_extreme(const wsb_disks* d, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
                          const double* pose, const double* vecs, double* out, void* stream);
 
+/* ---- finite-element pair weights (2-D, P1 triangles) ----
+ * For every (query, element) pair k: w[3k + i] = int_T W_h(x' - x) phi_i(x') dx' and G[6k + 2i + j] =
+ * int_T d/dx_j W_h(x' - x) phi_i(x') dx' (physical units) for the three barycentric functions phi_i of triangle
+ * elems[3 e .. 3 e + 2] (vertex order as given), query pos[2 q], support sup[q]; kernel ids 0 .. 9.  Exact closed
+ * forms of the triangle's channels, or the reference's 8 x 8 far-field Gauss rule for a triangle far from the query
+ * and smooth under the kernel.  All arrays on the device.  Replaces warpbc.pair_weights
+ * (src/warpSPHBoundaries/edge/warpbc.py:226-345, 486-510). */
+int wsb_pair_weights(int kernel, const int32_t* pair_q, const int32_t* pair_e, int64_t n_pairs, const double* pos,
+                     const double* sup, const double* verts, const int32_t* elems, double* w, double* G, void* stream);
+
 /* ---- closed triangle surfaces (3-D) ----
  * A watertight, consistently oriented triangle surface with outward normals (positive signed volume): verts
  * [n_verts*3] and faces [n_faces*3] (vertex ids) on the host, copied to `device` with a cell grid of faces (cell =

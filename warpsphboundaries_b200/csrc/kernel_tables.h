@@ -950,6 +950,111 @@ template <> __device__ __forceinline__ int disk_knots<9>(double* out) {
   return 0;
 }
 constexpr int kDiskMaxKnots = 2;
+// pi*W and its derivative (the far-field rule of the finite-element pair weights)
+template <int KID> __device__ __forceinline__ void pi_w_deriv(double r, double& P, double& dP);
+template <> __device__ __forceinline__ void pi_w_deriv<0>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(-11.428571428571429, r, 34.285714285714285), r, -34.285714285714285), r, 11.428571428571429);
+    dP += fma(fma(-34.285714285714285, r, 68.57142857142857), r, -34.285714285714285);
+  }
+  if (r <= 0.5) {
+    P += fma(fma(fma(45.714285714285715, r, -68.57142857142857), r, 34.285714285714285), r, -5.714285714285714);
+    dP += fma(fma(137.14285714285714, r, -137.14285714285714), r, 34.285714285714285);
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<1>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(28.0, r, -105.0), r, 140.0), r, -70.0), r, 0.0), r, 7.0);
+    dP += (fma(fma(fma(140.0, r, -420.0), r, 420.0), r, -140.0))*r;
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<2>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(fma(fma(105.0, r, -576.0), r, 1260.0), r, -1344.0), r, 630.0), r, 0.0), r, -84.0), r, 0.0), r, 9.0);
+    dP += (fma(fma(fma(fma(fma(fma(840.0, r, -4032.0), r, 7560.0), r, -6720.0), r, 2520.0), r, 0.0), r, -168.0))*r;
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<3>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(356.57142857142856, r, -2574.0), r, 7844.571428571428), r, -12870.0), r, 11766.857142857143), r, -5148.0), r, 0.0), r, 735.4285714285714), r, 0.0), r, -122.57142857142857), r, 0.0), r, 11.142857142857142);
+    dP += (fma(fma(fma(fma(fma(fma(fma(fma(fma(3922.285714285714, r, -25740.0), r, 70601.14285714286), r, -102960.0), r, 82368.0), r, -30888.0), r, 0.0), r, 2941.714285714286), r, 0.0), r, -245.14285714285714))*r;
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<4>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(19.547539616346956, r, -78.19015846538782), r, 117.28523769808173), r, -78.19015846538782), r, 19.547539616346956);
+    dP += fma(fma(fma(78.19015846538782, r, -234.57047539616346), r, 234.57047539616346), r, -78.19015846538782);
+  }
+  if (r <= 0.6) {
+    P += fma(fma(fma(fma(-97.73769808173478, r, 234.57047539616346), r, -211.11342785654713), r, 84.44537114261885), r, -12.666805671392828);
+    dP += fma(fma(fma(-390.9507923269391, r, 703.7114261884905), r, -422.22685571309427), r, 84.44537114261885);
+  }
+  if (r <= 0.2) {
+    P += fma(fma(fma(fma(195.47539616346955, r, -156.38031693077565), r, 46.914095079232695), r, -6.255212677231026), r, 0.3127606338615513);
+    dP += fma(fma(fma(781.9015846538782, r, -469.1409507923269), r, 93.82819015846539), r, -6.255212677231026);
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<5>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(-32.02719665271967, r, 160.13598326359832), r, -320.27196652719664), r, 320.27196652719664), r, -160.13598326359832), r, 32.02719665271967);
+    dP += fma(fma(fma(fma(-160.13598326359832, r, 640.5439330543933), r, -960.81589958159), r, 640.5439330543933), r, -160.13598326359832);
+  }
+  if (r <= 0.6666666666666666) {
+    P += fma(fma(fma(fma(fma(192.163179916318, r, -640.5439330543933), r, 854.0585774058577), r, -569.3723849372385), r, 189.7907949790795), r, -25.305439330543933);
+    dP += fma(fma(fma(fma(960.81589958159, r, -2562.175732217573), r, 2562.175732217573), r, -1138.744769874477), r, 189.7907949790795);
+  }
+  if (r <= 0.3333333333333333) {
+    P += fma(fma(fma(fma(fma(-480.407949790795, r, 800.6799163179917), r, -533.7866108786611), r, 177.92887029288704), r, -29.65481171548117), r, 1.9769874476987448);
+    dP += fma(fma(fma(fma(-2402.039748953975, r, 3202.7196652719667), r, -1601.3598326359834), r, 355.8577405857741), r, -29.65481171548117);
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<6>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(-4.0, r, 0.0), r, 12.0), r, 0.0), r, -12.0), r, 0.0), r, 4.0);
+    dP += (fma(fma(fma(fma(-24.0, r, 0.0), r, 48.0), r, 0.0), r, -24.0))*r;
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<7>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(-3.0, r, 3.0);
+    dP += -3.0;
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<8>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(-10.0, r, 30.0), r, -30.0), r, 10.0);
+    dP += fma(fma(-30.0, r, 60.0), r, -30.0);
+  }
+}
+template <> __device__ __forceinline__ void pi_w_deriv<9>(double r, double& P, double& dP) {
+  P = 0.0;
+  dP = 0.0;
+  if (r <= 1.0) {
+    P += fma(fma(fma(fma(fma(fma(-46.666666666666664, r, 224.0), r, -420.0), r, 373.3333333333333), r, -140.0), r, 0.0), r, 9.333333333333334);
+    dP += (fma(fma(fma(fma(-280.0, r, 1120.0), r, -1680.0), r, 1120.0), r, -280.0))*r;
+  }
+}
+constexpr int kFemGauss = 8;   // nodes per direction of the far-field rule, on [0, 1]
+static __device__ const double kFemGx[kFemGauss] = {0.019855071751231912, 0.10166676129318664, 0.2372337950418355, 0.4082826787521751, 0.5917173212478248, 0.7627662049581645, 0.8983332387068134, 0.9801449282487681};
+static __device__ const double kFemGw[kFemGauss] = {0.05061426814518853, 0.11119051722668721, 0.15685332293894344, 0.18134189168918083, 0.18134189168918083, 0.15685332293894344, 0.11119051722668721, 0.05061426814518853};
 
 // ---- 3-D radial family (solid half-space / sphere), unit support; W = c3*pi * shape, L = W'/r, dL = L'
 template <int K, typename T>

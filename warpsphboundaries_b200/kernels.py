@@ -478,6 +478,24 @@ def emit_disk() -> list:
         body.append("}")
         out.extend(body)
     out.append(f"constexpr int kDiskMaxKnots = {max(1, max(sum(1 for b in kernel(n).blocks if b.R < 1) for n in KERNEL_IDS))};")
+    out.append("// pi*W and its derivative (the far-field rule of the finite-element pair weights)")
+    out.append("template <int KID> __device__ __forceinline__ void pi_w_deriv(double r, double& P, double& dP);")
+    for kid in range(len(KERNEL_IDS)):
+        k = kernel(KERNEL_NAMES[kid])
+        out.append(f"template <> __device__ __forceinline__ void pi_w_deriv<{kid}>(double r, double& P, double& dP) {{")
+        out.append("  P = 0.0;")
+        out.append("  dP = 0.0;")
+        for b in k.blocks:
+            der = [c * (i + 1) for i, c in enumerate(b.c[1:])] or [F(0)]
+            out.append(f"  if (r <= {_lit(b.R)}) {{")
+            out.append(f"    P += {_horner(b.c, 'r')};")
+            out.append(f"    dP += {_horner(der, 'r')};")
+            out.append("  }")
+        out.append("}")
+    gx, gw = __import__("numpy").polynomial.legendre.leggauss(8)
+    out.append("constexpr int kFemGauss = 8;   // nodes per direction of the far-field rule, on [0, 1]")
+    out.append("static __device__ const double kFemGx[kFemGauss] = {" + ", ".join(repr(float((x + 1) / 2)) for x in gx) + "};")
+    out.append("static __device__ const double kFemGw[kFemGauss] = {" + ", ".join(repr(float(w / 2)) for w in gw) + "};")
     out.append("")
     return out
 
