@@ -187,3 +187,20 @@ def test_disk_array_host_logic():
         DiskArrayRep([[0.0, 0.0]], [1.0, 2.0])
     with pytest.raises(ValueError):
         DiskArrayRep([[0.0, 0.0]], [0.0])
+
+
+def test_pair_weights_host_checks():
+    """fem.pair_weights (warpbc.py:486-510 signature) refuses unknown kernels and CPU devices before any launch, and
+    the C entry point refuses NULL arrays and unknown kernel ids without a device."""
+    from warpsphboundaries_b200 import _lib
+    from warpsphboundaries_b200.fem import pair_weights
+    V = np.array([[0.0, 0.0], [1.0, 0.0], [0.0, 1.0]])
+    E = np.array([[0, 1, 2]])
+    with pytest.raises(NotImplementedError):
+        pair_weights([0], [0], [[0.2, 0.2]], [0.5], V, E, "w2p5", device="cuda")
+    with pytest.raises(RuntimeError):
+        pair_weights([0], [0], [[0.2, 0.2]], [0.5], V, E, "w2", device="cpu")
+    L = _lib.lib
+    assert L.wsb_pair_weights(1, None, None, 4, None, None, None, None, None, None, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_pair_weights(10, None, None, 4, None, None, None, None, None, None, None) == _lib.WSB_ERR_UNSUPPORTED
+    assert L.wsb_pair_weights(1, None, None, 0, None, None, None, None, None, None, None) == _lib.WSB_OK
