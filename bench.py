@@ -7,12 +7,16 @@ Workload (one step): lambda + the twelve moments of every particle of the large 
 cubic, w2, w4, w6.  Metric: particle-edge neighbour pairs per second (pairs = pairs passing the float64 neighbour
 predicate, counted once, times the number of kernels).  `value` is measured with inputs resident on the device;
 `e2e` through the public provider API with host buffers (pinned host -> device copy of positions and supports, device
--> host copy of lam, G, Cov of every kernel) inside the timed region.  Between timed steps L2 is flushed by writing a
-256 MiB buffer (outside the events).  Multi-GPU: one process per GPU, each its own particle set of the same size over
-the same geometry (weak scaling, no data-path collective); time = max over ranks.
+-> host copy of lam, G, Cov, m1, m2 of every kernel) inside the timed region.  Between timed steps L2 is flushed by
+writing a 256 MiB buffer (outside the events).  `routes` compares the plain float64 route, the fused float64 pass and
+the fused mixed pass on the same scene.  Multi-GPU: one process per GPU, each its own particle set of the same size
+over the same geometry (weak scaling, no data-path collective); time = max over ranks.
 
 --impl reference times the reference algorithm on the host cores: the oracle port (oracle/edge2d.py, a CPU
-restatement of the reference's numpy path) over a bounded particle sample, all cores in worker processes.
+restatement of the reference's numpy path, with the cell list and y bins built once as the reference caches them) over
+a fixed seeded sample of 2^16 rows per step, the four kernels each, all cores in spawned worker processes; its
+`ms_per_step` is the measured time of that sample (nothing is extrapolated).  `cpu_baseline` of the GPU line is the
+same measurement.
 """
 import argparse
 import json
@@ -25,6 +29,7 @@ os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -52,7 +57,7 @@ def parse():
     p.add_argument("--leg", choices=["all", "radial", "mesh3d", "serving", "disks"], default="all",
                    help="run one side leg alone (prints its JSON object; for profiling)")
     p.add_argument("--mesh-particles", type=int, default=1 << 21, help="particles of the 3-D closed-surface leg")
-    p.add_argument("--extra", action="store_true", help="also time the other precision and the plain route")
+    p.add_argument("--no-routes", action="store_true", help="skip the plain / fused fp64 / mixed comparison")
     p.add_argument("--serve-requests", type=int, default=10000,
                    help="requests of the serving stream measured after the main workload (0: skip)")
     return p.parse_args()
@@ -71,59 +76,86 @@ def workload(n, rank):
 
 
 # ----------------------------------------------------------------------------------------------- reference (CPU) arm
-def _oracle_chunk(args):
-    loops, X, h, kernel = args
+def config(n):
+    """the workload as both arms report it (the reference arm times a fixed sample of it, stated in `cpu_baseline`)."""
+    return {"workload": WORKLOAD, "particles_per_gpu": n, "kernels": KERNELS,
+            "l2": "flushed between steps (256 MiB write, untimed)"}
+
+
+CPU_SAMPLE_ROWS = 1 << 16        # rows of the 2-D scene one reference step evaluates (4 kernels each)
+CPU_CHUNK = 4096                 # rows a worker takes at a time
+
+_CPU = {}
+
+
+def _cpu_init(n):
+    """worker set-up: the scene, its cell list and y bins once per process (the reference caches both per surface
+    and support, scene.py:273-279, 318-336)."""
     from oracle import edge2d as O
     from warpsphboundaries_b200 import workloads
+    loops, X, h = workload(n, 0)
     V, E = workloads.edges_of(loops)
-    out, slots, ind = O.local_twelve(V, E, 0, X, np.full(len(X), h), kernel, h, return_slots=True)
-    return sum(len(s) for s in slots)
+    _CPU.update(X=X, h=h, V=V, E=E, cl=O.build_cell_list(V, E, h), bins=O.ybins(V, E))
 
 
-def cpu_reference(loops, X, h, seconds=15.0, procs=None):
-    """pairs/s of the oracle port over a bounded sample: chunks of near-wall-rich particles across all host cores."""
-    import multiprocessing as mp
-    procs = procs or os.cpu_count() or 1
-    rng = np.random.default_rng(7)
-    chunk = 2048
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
+def _cpu_chunk(rows):
+    """the reference algorithm on one chunk of rows: indicator once, then the four kernels' channels (neighbour slots,
+    per-pair closed forms, fixed-order row sums, indicator times the plane constants, physical scaling)."""
+    from oracle import edge2d as O
+    c = _CPU
+    X, h = c["X"][rows], c["h"]
+    hs = np.full(len(rows), h)
+    ind = O.indicator_binned(c["V"], c["E"], 0, X, hs, c["cl"], c["bins"])
     pairs = 0
-    done = 0
-    with ctx.Pool(procs) as pool:
-        while True:
-            jobs = [(loops, X[rng.choice(len(X), chunk, replace=False)], h, KERNELS[(done + i) % 4]) for i in range(procs)]
-            pairs += sum(pool.map(_oracle_chunk, jobs))
-            done += procs
-            if time.perf_counter() - t0 > seconds:
-                break
-    dt = time.perf_counter() - t0
-    cpu_reference.density = pairs / (done * chunk)                     # neighbour pairs per particle of the sample
-    return pairs / dt, procs, f"{done} chunks of {chunk} random particles of the scene, kernels cycled; {pairs} pairs in {dt:.1f} s"
+    for k in KERNELS:
+        _, slots, _ = O.local_twelve(c["V"], c["E"], 0, X, hs, k, h, ind=ind, cl=c["cl"], return_slots=True)
+        pairs += sum(len(s) for s in slots)
+    return pairs
+
+
+class CpuReference:
+    """the oracle port (oracle/edge2d.py, the reference's numpy algorithm restated) over a fixed seeded sample of the
+    scene's rows, in worker processes on the host cores (spawned before any CUDA work)."""
+
+    def __init__(self, n, procs=None):
+        import multiprocessing as mp
+        self.procs = procs or os.cpu_count() or 1
+        rows = np.sort(np.random.default_rng(7).choice(n, min(CPU_SAMPLE_ROWS, n), replace=False))
+        self.chunks = [rows[i:i + CPU_CHUNK] for i in range(0, len(rows), CPU_CHUNK)]
+        self.pool = mp.get_context("spawn").Pool(self.procs, initializer=_cpu_init, initargs=(n,))
+        self.sample = (f"a fixed seeded sample of {len(rows)} of the {n} rows per step, the four kernels each "
+                       f"({len(self.chunks)} chunks of {CPU_CHUNK} rows over {self.procs} worker processes)")
+
+    def step(self):
+        """(pair evaluations, seconds) of one step."""
+        t0 = time.perf_counter()
+        pairs = sum(self.pool.map(_cpu_chunk, self.chunks, chunksize=1))
+        return pairs, time.perf_counter() - t0
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
 
 
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    loops, X, h = workload(args.particles, 0)
-    steps = []
-    sample = ""
-    procs = os.cpu_count() or 1
+    ref = CpuReference(args.particles)
     for _ in range(args.warmup):
-        cpu_reference(loops, X, h, seconds=1.0, procs=procs)
+        ref.step()
+    pairs, secs = 0, 0.0
     for _ in range(args.steps):
-        v, procs, sample = cpu_reference(loops, X, h, seconds=8.0, procs=procs)
-        steps.append(v)
-    value = float(statistics.mean(steps))
-    # one full step (4 kernels over all particles) at the sample's rate and pair density
-    step_ms = len(KERNELS) * cpu_reference.density * len(X) / value * 1e3
+        p, t = ref.step()
+        pairs += p
+        secs += t
+    ref.close()
+    value = pairs / secs
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD, "sample": sample,
-                       "ms_per_step": "extrapolated from the sample: 4 kernels x pairs of the full scene / rate"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": config(args.particles),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.procs, "kind": "port", "sample": ref.sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -132,7 +164,7 @@ def reference_arm(args):
 class Clocks:
     def __init__(self):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"wsb_clocks_{os.getpid()}.csv")
 
     def start(self, index):
         try:
@@ -479,6 +511,8 @@ def our_arm(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    # the CPU baseline's worker processes, spawned before the first CUDA call
+    cpu_ref = CpuReference(args.particles) if rank == 0 and world == 1 and not args.no_cpu_baseline else None
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     if world > 1:
@@ -608,28 +642,41 @@ def our_arm(args):
         except Exception:
             traffic = None
 
-    extra = {}
-    if args.extra and world == 1:
-        other = "fp64" if args.precision == "mixed" else "mixed"
-        ms_o, ev_o, _ = timed(other, max(3, args.steps // 2), 1)
-        extra[f"fused_{other}_pairs_per_s"] = pairs_step * max(3, args.steps // 2) / (ms_o * 1e-3)
-        # the plain FP64 route (the reference's structure: slots, per-slot plan interpreter, contraction)
+    # ---- the metric's comparison on the same prepared scene: the plain float64 route (the reference's structure:
+    # neighbour slots, the per-slot plan interpreter, the contraction; one aggregate per kernel), the fused float64
+    # pass and the fused mixed pass (four kernels in one pass each)
+    routes = None
+    if world == 1 and not args.no_routes:
+        nr = max(3, args.steps // 2)
+        ms_f, _, _ = timed("fp64", nr, 1)
+        ms_m, _, _ = timed("mixed", nr, 1)
         ab = AnalyticBoundary(scene, route="plain")
         ps = ParticleState(pos, sup)
-        for _ in range(1):
-            ab.aggregate(ps, h, kernel=KernelFunctions.Wendland4, lean=True)
+        kfs = (KernelFunctions.CubicSpline, KernelFunctions.Wendland2, KernelFunctions.Wendland4,
+               KernelFunctions.Wendland6)
+        for kf in kfs:
+            ab.aggregate(ps, h, kernel=kf, lean=True)
         torch.cuda.synchronize()
-        tp0 = time.perf_counter()
+        flush.fill_(1)
+        torch.cuda.synchronize()
         s0 = torch.cuda.Event(enable_timing=True)
         s1 = torch.cuda.Event(enable_timing=True)
         s0.record(stream)
-        for kf in (KernelFunctions.CubicSpline, KernelFunctions.Wendland2, KernelFunctions.Wendland4, KernelFunctions.Wendland6):
+        for kf in kfs:
             ab.aggregate(ps, h, kernel=kf, lean=True)
         s1.record(stream)
         torch.cuda.synchronize()
-        extra["plain_fp64_pairs_per_s"] = pairs_step / (s0.elapsed_time(s1) * 1e-3)
+        plain = pairs_step / (s0.elapsed_time(s1) * 1e-3)
         del ab
         torch.cuda.empty_cache()
+        fused64 = pairs_step * nr / (ms_f * 1e-3)
+        mixed = pairs_step * nr / (ms_m * 1e-3)
+        headline = mixed if args.precision == "mixed" else fused64
+        routes = {"plain_fp64_pairs_per_s": plain, "fused_fp64_pairs_per_s": fused64, "mixed_pairs_per_s": mixed,
+                  "batched_over_plain": headline / plain, "fused_fp64_over_plain": fused64 / plain,
+                  "what": "one step (prepare + the four kernels) per route on the same scene and particles; plain = "
+                          "k_fixed_topology slots + k_slot_channels_plain (the reference's per-slot plan "
+                          "interpreter) + k_contract, one aggregate per kernel"}
 
     # ---- the adjoint (d sum(lam) / dx of every particle, w4): prepare + backward per call, timed alone
     adjoint = None
@@ -666,7 +713,10 @@ def our_arm(args):
         hsup = torch.full((N,), h, dtype=torch.float64).pin_memory()
         dpos = torch.empty_like(pos)
         dsup = torch.empty_like(sup)
+        names = ("lam", "G", "Cov", "m1", "m2")                  # lambda and the twelve moments, every kernel
         host_out = {k: [torch.empty((1, N), dtype=torch.float64).pin_memory(),
+                        torch.empty((1, N, 2), dtype=torch.float64).pin_memory(),
+                        torch.empty((1, N, 2, 2), dtype=torch.float64).pin_memory(),
                         torch.empty((1, N, 2), dtype=torch.float64).pin_memory(),
                         torch.empty((1, N, 2, 2), dtype=torch.float64).pin_memory()] for k in KERNELS}
         groups = tuple(FusedGroup(k) for k in KERNELS)
@@ -677,7 +727,7 @@ def our_arm(args):
             dsup.copy_(hsup, non_blocking=True)
             fw = FusedWall(scene, ParticleState(dpos, dsup), h, groups, precision=args.precision)
             for gi, k in enumerate(KERNELS):
-                for dst, name in zip(host_out[k], ("lam", "G", "Cov")):
+                for dst, name in zip(host_out[k], names):
                     dst.copy_(fw.res[gi][name], non_blocking=True)
             return fw
 
@@ -726,7 +776,7 @@ def our_arm(args):
             down.wait_event(done)
             with torch.cuda.stream(down):
                 for gi, kn in enumerate(KERNELS):
-                    for dst, name in zip(host_out[kn], ("lam", "G", "Cov")):
+                    for dst, name in zip(host_out[kn], names):
                         src = fw.res[gi][name]
                         src.record_stream(down)            # not reused before its download is done
                         dst.copy_(src, non_blocking=True)
@@ -736,7 +786,8 @@ def our_arm(args):
         tot = shard.max_over_ranks(tot, dev)
         seq = shard.max_over_ranks(seq, dev)
         e2e = {"value": job_pairs_step * args.steps / (tot * 1e-3), "unit": UNIT,
-               "h2d_bytes_per_step": N * 3 * 8, "d2h_bytes_per_step": len(KERNELS) * N * 7 * 8,
+               "h2d_bytes_per_step": N * 3 * 8, "d2h_bytes_per_step": len(KERNELS) * N * 13 * 8,
+               "downloads": "lam, G, Cov, m1, m2 of every kernel (13 float64 per particle per kernel)",
                "ms_per_step": tot / args.steps, "pipelined": True,
                "sequential": {"value": job_pairs_step * args.steps / (seq * 1e-3), "ms_per_step": seq / args.steps}}
 
@@ -750,18 +801,24 @@ def our_arm(args):
         serving = serving_run(args.serve_requests, dev, P / N)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, procs, sample = cpu_reference(loops, X, h, seconds=12.0, procs=1)
-        cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": "port", "sample": sample}
+    if cpu_ref is not None:
+        cpu_ref.step()                                             # warm-up
+        pr, sec = 0, 0.0
+        for _ in range(2):
+            p_, t_ = cpu_ref.step()
+            pr += p_
+            sec += t_
+        cpu_ref.close()
+        cpu = {"value": pr / sec, "unit": UNIT, "cores": cpu_ref.procs, "kind": "port", "sample": cpu_ref.sample,
+               "ms_per_step": sec / 2 * 1e3}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
                 "data": "synthetic (seeded)",
-                "config": {"workload": WORKLOAD,
-                           "pairs_per_kernel": P, "particles_per_gpu": N, "route": args.route,
-                           "precision": args.precision, "l2": "flushed between steps (256 MiB write, untimed)"},
+                "config": config(N), "pairs_per_kernel": P, "route": args.route, "precision": args.precision,
+                "routes": routes,
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                              "frac": achieved / fp64_peak, "traffic": traffic,
                              "kernel": "k_agg_pairs<KPack<cubic, w2, w4, w6>> (wsb_aggregate_evaluate_groups)",
@@ -772,8 +829,7 @@ def our_arm(args):
                 "kernel_ms_separate": sep_ms,
                 "gpu_launches": args.steps * (5 + 1),   # prepare: 5 kernels; one pair kernel for the four groups
                 "clocks": clk, "e2e": e2e, "cpu_baseline": cpu, "serving": serving, "radial": radial, "mesh3d": mesh, "adjoint": adjoint,
-                "detector": detector, "disks": disks,
-                **({"extra": extra} if extra else {})}
+                "detector": detector, "disks": disks}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

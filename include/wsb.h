@@ -108,6 +108,17 @@ int wsb_contract(const wsb_surface* s, int kernel, const int32_t* slots, const d
                  const double* lsup, int64_t n, const double* rot, double* lam, double* G, double* cov, double* m1,
                  double* m2, void* stream);
 
+/* Pair-list channels: for every (query, edge) pair k of qi [n_pairs], e [n_pairs] (int32, device) the twelve
+ * edge-local channels c[12k .. 12k + 11] (units of h, the 1/pi applied; 0 lam, 1-2 m1, 3-4 G, 5-8 g1, 9-11 m20 m11
+ * m02) of query row qi[k] (lpos [n_rows*2] body frame, lsup [n_rows]) against edge e[k] by the closed form; kernels
+ * 0 .. 11 (10, 11: the tensile kernels, G channels only, the others NaN); precision WSB_PREC_FP64 or WSB_PREC_MIXED.
+ * An index outside its array gives NaN channels and sets *status (device int32, zeroed by the caller) to 1.
+ * Replaces warpbc.edge_channels + second_channels over a pair list (src/warpSPHBoundaries/edge/warpbc.py:919-991) as
+ * SurfaceRep.moments calls them (src/warpSPHBoundaries/scene/scene.py:384-416). */
+int wsb_pair_channels(const wsb_surface* s, int kernel, int precision, const int32_t* qi, const int32_t* e,
+                      int64_t n_pairs, const double* lpos, const double* lsup, int64_t n_rows, double* c,
+                      int32_t* status, void* stream);
+
 /* Workspace bytes wsb_aggregate needs for n rows. */
 size_t wsb_aggregate_workspace_size(const wsb_surface* s, int64_t n);
 
@@ -280,10 +291,13 @@ int wsb_disk_dir_extreme(const wsb_disks* d, const double* pos, const double* su
  * int_T d/dx_j W_h(x' - x) phi_i(x') dx' (physical units) for the three barycentric functions phi_i of triangle
  * elems[3 e .. 3 e + 2] (vertex order as given), query pos[2 q], support sup[q]; kernel ids 0 .. 9.  Exact closed
  * forms of the triangle's channels, or the reference's 8 x 8 far-field Gauss rule for a triangle far from the query
- * and smooth under the kernel.  All arrays on the device.  Replaces warpbc.pair_weights
- * (src/warpSPHBoundaries/edge/warpbc.py:226-345, 486-510). */
+ * and smooth under the kernel.  All arrays on the device; n_pos rows of pos / sup, n_verts vertices, n_elems elements.
+ * A pair whose query, element or vertex index lies outside its array gets NaN outputs and sets *status (a device
+ * int32 the caller zeroes) to 1; nothing outside the arrays is read.  The launch runs on the device that holds pos.
+ * Replaces warpbc.pair_weights (src/warpSPHBoundaries/edge/warpbc.py:226-345, 486-510). */
 int wsb_pair_weights(int kernel, const int32_t* pair_q, const int32_t* pair_e, int64_t n_pairs, const double* pos,
-                     const double* sup, const double* verts, const int32_t* elems, double* w, double* G, void* stream);
+                     const double* sup, int64_t n_pos, const double* verts, int64_t n_verts, const int32_t* elems,
+                     int64_t n_elems, double* w, double* G, int32_t* status, void* stream);
 
 /* ---- closed triangle surfaces (3-D) ----
  * A watertight, consistently oriented triangle surface with outward normals (positive signed volume): verts

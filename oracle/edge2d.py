@@ -363,15 +363,102 @@ def indicator(verts, edges, background, lpos, lsup=None):
     return out + background
 
 
-# ----------------------------------------------------------------------------- scene composition
-def local_twelve(verts, edges, background, lpos, lsup, name, support_max, valid=None, return_slots=False):
-    """[N, 12] local-frame channels in physical units, summed per row in cell-list slot order, + indicator * plane
-    (scene.py:384-416 / fused.py:69-154): [lam, m10, m01, Gx, Gy, g1xx, g1xy, g1yx, g1yy, m20, m11, m02]."""
+def ybins(verts, edges, nbins=None):
+    """y bins of the edges (scene.py:318-336): bin count 2 floor(sqrt(E)), every edge listed in each bin its y range
+    meets, edge order within a bin.  Returns (y0, dy, nb, start[nb + 1], items)."""
+    a, b = verts[edges[:, 0]], verts[edges[:, 1]]
+    ylo, yhi = np.minimum(a[:, 1], b[:, 1]), np.maximum(a[:, 1], b[:, 1])
+    nb = nbins or max(1, int(np.sqrt(len(edges))) * 2)
+    y0 = float(ylo.min())
+    dy = max(float(yhi.max()) - y0, 1e-300) / nb
+    i0 = np.clip(np.floor((ylo - y0) / dy).astype(np.int64), 0, nb - 1)
+    i1 = np.clip(np.floor((yhi - y0) / dy).astype(np.int64), 0, nb - 1)
+    cnt = i1 - i0 + 1
+    item = np.repeat(np.arange(len(edges)), cnt)
+    st = np.cumsum(cnt) - cnt
+    bins = i0[item] + np.arange(int(cnt.sum())) - np.repeat(st, cnt)
+    order = np.argsort(bins, kind="stable")
+    start = np.concatenate([[0], np.cumsum(np.bincount(bins[order], minlength=nb))])
+    return y0, dy, nb, start, item[order]
+
+
+def indicator_binned(verts, edges, background, lpos, lsup, cl, bins=None):
+    """the reference's fast indicator (scene.py:281-316, 338-396): points in grid cells without edges take the winding
+    of their cell centre (ray cast once per cell), points beyond the grid the background, the others a ray cast over
+    their y bin's edges (half-open crossings; the principal-value angle sum over all edges for points on an edge or a
+    vertex).  Equal to `indicator` (the whole-loop form) wherever the cell cache is exact."""
     verts = np.asarray(verts, dtype=np.float64)
     edges = np.asarray(edges, dtype=np.int64)
     lpos = np.asarray(lpos, dtype=np.float64)
     lsup = np.asarray(lsup, dtype=np.float64)
-    cl = build_cell_list(verts, edges, support_max)
+    lo, cell, (nx, ny), start, _ = cl
+    y0, dy, nb, bstart, bitems = bins if bins is not None else ybins(verts, edges)
+    cnt = np.diff(start)
+    empty = np.nonzero(cnt == 0)[0]
+    cind = np.zeros(nx * ny)
+    if len(empty):
+        centres = lo + (np.stack([empty // ny, empty % ny], 1) + 0.5) * cell
+        cind[empty] = _ray_indicator(verts, edges, centres, None, (y0, dy, nb, bstart, bitems))
+    cx = np.floor((lpos[:, 0] - lo[0]) / cell).astype(np.int64)
+    cy = np.floor((lpos[:, 1] - lo[1]) / cell).astype(np.int64)
+    inside = (cx >= 0) & (cx < nx) & (cy >= 0) & (cy < ny)
+    cid = np.where(inside, cx * ny + cy, 0)
+    fast = inside & (cnt[cid] == 0)
+    out = np.where(fast, cind[cid], 0.0)
+    out = np.where(~inside, float(background), out)
+    slow = np.nonzero(~(fast | ~inside))[0]
+    if len(slow):
+        out[slow] = _ray_indicator(verts, edges, lpos[slow], lsup[slow], (y0, dy, nb, bstart, bitems)) + background
+    out[fast] += background
+    return out
+
+
+def _ray_indicator(verts, edges, p, sup, bins):
+    """winding number by the y-bin ray cast (scene.py:338-396), without the background."""
+    y0, dy, nb, start, items = bins
+    iy = np.floor((p[:, 1] - y0) / dy).astype(np.int64)
+    ok = (iy >= 0) & (iy <= nb)
+    b = np.where(ok, np.minimum(iy, nb - 1), 0)
+    cnt = np.where(ok, start[b + 1] - start[b], 0)
+    q = np.repeat(np.arange(len(p)), cnt)
+    off = np.arange(int(cnt.sum())) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+    e = items[start[b[q]] + off]
+    a, c = verts[edges[e, 0]], verts[edges[e, 1]]
+    x = p[q]
+    ar, cr = a - x, c - x
+    if sup is not None:
+        ar, cr = ar / sup[q, None], cr / sup[q, None]
+    cross = cross2(ar[:, 0], ar[:, 1], cr[:, 0], cr[:, 1])
+    up = (a[:, 1] <= x[:, 1]) & (x[:, 1] < c[:, 1]) & (cross > 0)
+    down = (c[:, 1] <= x[:, 1]) & (x[:, 1] < a[:, 1]) & (cross < 0)
+    wn = np.zeros(len(p))
+    np.add.at(wn, q, up.astype(np.float64) - down.astype(np.float64))
+    on = (cross == 0) & ((ar * cr).sum(1) <= 0)
+    boundary = np.zeros(len(p), dtype=np.int64)
+    np.add.at(boundary, q, on.astype(np.int64))
+    for r in np.nonzero(boundary > 0)[0]:
+        A = verts[edges[:, 0]] - p[r]
+        C = verts[edges[:, 1]] - p[r]
+        if sup is not None:
+            A, C = A / sup[r], C / sup[r]
+        cr2 = cross2(A[:, 0], A[:, 1], C[:, 0], C[:, 1])
+        ang = np.where(cr2 == 0, 0.0, np.arctan2(cr2, (A * C).sum(1)))
+        wn[r] = ang.sum() / (2 * np.pi)
+    return wn
+
+
+# ----------------------------------------------------------------------------- scene composition
+def local_twelve(verts, edges, background, lpos, lsup, name, support_max, valid=None, return_slots=False, ind=None,
+                 cl=None):
+    """[N, 12] local-frame channels in physical units, summed per row in cell-list slot order, + indicator * plane
+    (scene.py:384-416 / fused.py:69-154): [lam, m10, m01, Gx, Gy, g1xx, g1xy, g1yx, g1yy, m20, m11, m02].
+    `ind` / `cl`: a precomputed indicator (before the `valid` mask) and cell list of these rows, reused across
+    kernels."""
+    verts = np.asarray(verts, dtype=np.float64)
+    edges = np.asarray(edges, dtype=np.int64)
+    lpos = np.asarray(lpos, dtype=np.float64)
+    lsup = np.asarray(lsup, dtype=np.float64)
+    cl = build_cell_list(verts, edges, support_max) if cl is None else cl
     slots = fixed_slots(verts, edges, cl, lpos, lsup, valid)
     rows = np.concatenate([np.full(len(s), r, dtype=np.int64) for r, s in enumerate(slots)]) if slots else np.zeros(0, np.int64)
     es = np.concatenate(slots) if slots else np.zeros(0, np.int64)
@@ -383,7 +470,7 @@ def local_twelve(verts, edges, background, lpos, lsup, name, support_max, valid=
         c = edge_channels(p, q, name)
         for k in range(len(es)):                 # fixed order per row: the slot order
             out[rows[k]] += c[k]
-    ind = indicator(verts, edges, background, lpos, lsup)
+    ind = indicator(verts, edges, background, lpos, lsup) if ind is None else np.asarray(ind, dtype=np.float64)
     if valid is not None:
         ind = np.where(valid, ind, 0.0)
     out += ind[:, None] * plane_channels(name)[None, :]

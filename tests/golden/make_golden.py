@@ -164,6 +164,43 @@ def torch2d_grads(torch2d, seed=0, n_pts=96):
     np.savez_compressed(HERE / "torch2d_grad.npz", polygon=P, particles=X, h=h, **res)
 
 
+def torch2d_c4(torch2d, n_pts=256):
+    """the gradient scene at its full size (workloads.c4: 2^18 particles in [0, 4]^2, 16 star polygons of 128
+    vertices, h = 0.02, w4): for 256 seeded particles within 0.95 h of an edge, each moment m_alpha (|alpha| <= 2)
+    summed over the 16 polygons by the reference's torch2d.moment (whole polygons), its autograd gradient per particle
+    and the vertex gradient of sum_i m_alpha(x_i) per polygon."""
+    import torch
+    sys.path.insert(0, str(HERE.parent.parent))
+    from warpsphboundaries_b200 import workloads
+    loops, X, h = workloads.c4()
+    V, E = workloads.edges_of(loops)
+    A, B = V[E[:, 0]], V[E[:, 1]]
+    rng = np.random.default_rng(404)
+    rows = []
+    for i in rng.permutation(len(X)):
+        d = B - A
+        t = np.clip(((X[i] - A) * d).sum(1) / (d * d).sum(1), 0.0, 1.0)
+        if np.linalg.norm(X[i] - (A + t[:, None] * d), axis=1).min() < 0.95 * h:
+            rows.append(int(i))
+            if len(rows) == n_pts:
+                break
+    rows = np.array(rows)
+    P = np.stack(loops)                                                    # [16, 128, 2]
+    res = {}
+    for al in [(0, 0), (1, 0), (0, 1), (2, 0), (1, 1), (0, 2)]:
+        Xt = torch.tensor(X[rows], dtype=torch.float64, requires_grad=True)
+        Vts = [torch.tensor(np.broadcast_to(L, (len(rows), 128, 2)).copy(), dtype=torch.float64, requires_grad=True)
+               for L in P]
+        m = sum(torch2d.moment(Vt, Xt, "w4", al, h) for Vt in Vts)
+        m.sum().backward()
+        key = f"{al[0]}{al[1]}"
+        res[f"m_{key}"] = m.detach().numpy()
+        res[f"dx_{key}"] = Xt.grad.numpy()
+        res[f"dv_{key}"] = np.stack([Vt.grad.numpy().sum(0) for Vt in Vts])
+        print("torch2d c4", al, "done")
+    np.savez_compressed(HERE / "torch2d_c4.npz", rows=rows, particles=X[rows], h=h, **res)
+
+
 def radial_golden(root):
     fx = Path(root) / "tests" / "fixtures"
     rad = json.loads((fx / "fluxbridge-radial-v1.json").read_text())
@@ -431,11 +468,14 @@ def sdf_contour_golden(root):
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the warpSPHBoundaries source tree>")
+    root = sys.argv[1]
     np2d, torch2d = load_reference(root)
     golden_subset(root)
     np2d_c1(np2d)
     torch2d_grads(torch2d)
+    torch2d_c4(torch2d)
     radial_golden(root)
     mesh3d_golden(root)
     triangle_golden(root)

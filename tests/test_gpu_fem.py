@@ -48,11 +48,20 @@ def _pairs(V, E, X, h):
     return np.array(q), np.array(e)
 
 
+def _on_mesh(V, E, rng, n):
+    """queries exactly on mesh vertices and on edge midpoints (the winding indicator's edge and vertex cases)."""
+    vs = V[rng.choice(len(V), n, replace=False)]
+    k = rng.choice(len(E), n, replace=False)
+    j = rng.integers(0, 3, n)
+    mids = (V[E[k, j]] + V[E[k, (j + 1) % 3]]) / 2
+    return np.concatenate([vs, mids])
+
+
 @pytest.mark.parametrize("kernel", ["cubic", "w4", "quintic"])
 def test_pair_weights_match_the_oracle(kernel):
     V, E = _mesh(6, jitter=0.3, seed=1)
     rng = np.random.default_rng(2)
-    X = rng.uniform(-0.1, 1.1, (60, 2))
+    X = np.concatenate([rng.uniform(-0.1, 1.1, (60, 2)), _on_mesh(V, E, rng, 8)])
     h = rng.uniform(0.12, 0.3, len(X))
     q, e = _pairs(V, E, X, h)
     w, G = pair_weights(q, e, X, h, V, E, kernel, device=DEV)
@@ -70,17 +79,78 @@ def test_pair_weights_match_the_oracle(kernel):
 
 
 def test_partition_of_unity_over_a_square():
+    """sum_k w_k and sum_k G_k over all pairs give the square's lam and G (partition of unity), and sum_k (V_k - x) w_k,
+    sum_k (V_k - x)_a G_kj its first moment m1 and Cov (linear reproduction: sum_k V_k phi_k(x') = x'), which checks
+    the barycentric gradient terms g_k of every closed-form pair, at queries on vertices and edge midpoints too."""
     V, E = _mesh(32, jitter=0.25, seed=3)
-    n = 1 << 14
-    X = np.random.default_rng(4).uniform(-0.05, 1.05, (n, 2))
+    rng = np.random.default_rng(4)
+    X = np.concatenate([rng.uniform(-0.05, 1.05, ((1 << 14) - 400, 2)), _on_mesh(V, E, rng, 200)])
+    n = len(X)
     h = np.full(n, 0.05)
     q, e = _pairs(V, E, X, h)
     w, G = pair_weights(q, e, X, h, V, E, "w2", device=DEV, as_torch=True)
     qt = torch.tensor(q, device=DEV, dtype=torch.int64)
     lam = torch.zeros(n, dtype=torch.float64, device=DEV).index_add_(0, qt, w.sum(1))
     grad = torch.zeros((n, 2), dtype=torch.float64, device=DEV).index_add_(0, qt, G.sum(1))
+    Xt = torch.tensor(X, device=DEV)
+    Vt = torch.tensor(V, device=DEV)
+    Et = torch.tensor(E, device=DEV, dtype=torch.int64)
+    et = torch.tensor(e, device=DEV, dtype=torch.int64)
+    m1 = torch.zeros((n, 2), dtype=torch.float64, device=DEV)
+    cov = torch.zeros((n, 2, 2), dtype=torch.float64, device=DEV)
+    for k in range(3):
+        d = Vt[Et[et, k]] - Xt[qt]
+        m1.index_add_(0, qt, d * w[:, k:k + 1])
+        cov.index_add_(0, qt, d[:, :, None] * G[:, k, None, :])
     sq = Scene([Body(reps=[SurfaceRep.box((0.0, 0.0), (1.0, 1.0))])], DEV)
-    fw = FusedWall(sq, ParticleState(torch.tensor(X, device=DEV), torch.tensor(h, device=DEV)), 0.05,
-                   (FusedGroup("w2"),))
-    assert float((lam - fw.res[0]["lam"][0]).abs().max()) <= 1e-10
-    assert float((grad - fw.res[0]["G"][0]).abs().max()) * 0.05 <= 1e-10
+    fw = FusedWall(sq, ParticleState(Xt, torch.tensor(h, device=DEV)), 0.05, (FusedGroup("w2"),))
+    r = fw.res[0]
+    assert float((lam - r["lam"][0]).abs().max()) <= 1e-10
+    assert float((grad - r["G"][0]).abs().max()) * 0.05 <= 1e-10
+    assert float((m1 - r["m1"][0]).abs().max()) / 0.05 <= 1e-10
+    assert float((cov - r["Cov"][0]).abs().max()) <= 1e-10
+
+
+def test_out_of_range_indices_are_refused_without_a_read():
+    """a query, element or vertex index outside its array: the Python call raises ValueError before the launch; the C
+    entry point itself writes NaN for that pair, sets the status word and reads nothing out of range."""
+    from warpsphboundaries_b200 import _lib
+    V, E = _mesh(2)
+    X = np.array([[0.3, 0.3], [0.6, 0.2]])
+    h = np.array([0.5, 0.5])
+    for q, e, EE in (([0, 2], [0, 1], E), ([0, 1], [0, len(E)], E), ([0, 1], [0, 1], np.where(E == 3, 99, E))):
+        with pytest.raises(ValueError):
+            pair_weights(q, e, X, h, V, EE, "w2", device=DEV)
+    dev = torch.device(DEV)
+    q = torch.tensor([0, 1, 5, 1], dtype=torch.int32, device=dev)
+    e = torch.tensor([0, -1, 2, 3], dtype=torch.int32, device=dev)
+    pos = torch.tensor(X, device=dev)
+    sup = torch.tensor(h, device=dev)
+    Vt = torch.tensor(V, device=dev)
+    Et = torch.tensor(E, dtype=torch.int32, device=dev)
+    w = torch.zeros((4, 3), dtype=torch.float64, device=dev)
+    G = torch.zeros((4, 3, 2), dtype=torch.float64, device=dev)
+    st = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(_lib.lib.wsb_pair_weights(2, _lib.ptr(q), _lib.ptr(e), 4, _lib.ptr(pos), _lib.ptr(sup), 2, _lib.ptr(Vt),
+                                         len(V), _lib.ptr(Et), len(E), _lib.ptr(w), _lib.ptr(G), _lib.ptr(st),
+                                         _lib.ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    torch.cuda.synchronize()
+    assert int(st.item()) == 1
+    bad = torch.isnan(w).all(1).cpu().numpy()
+    assert bad.tolist() == [False, True, True, False]
+    rw, _ = pair_weights([0, 1], [0, 3], X, h, V, E, "w2", device=DEV)
+    assert np.allclose(w[[0, 3]].cpu().numpy(), rw, rtol=0, atol=0)
+
+
+@pytest.mark.skipif(not torch.cuda.is_available() or torch.cuda.device_count() < 2, reason="needs two devices")
+def test_pair_weights_on_a_device_that_is_not_current():
+    """device='cuda:1' with device 0 current: the launch runs in device 1's context and device 0 stays current."""
+    V, E = _mesh(4, jitter=0.2, seed=1)
+    X = np.random.default_rng(5).uniform(0.0, 1.0, (50, 2))
+    h = np.full(len(X), 0.2)
+    q, e = _pairs(V, E, X, h)
+    torch.cuda.set_device(0)
+    w1, G1 = pair_weights(q, e, X, h, V, E, "w4", device="cuda:1")
+    assert torch.cuda.current_device() == 0
+    w0, G0 = pair_weights(q, e, X, h, V, E, "w4", device="cuda:0")
+    assert np.array_equal(w0, w1) and np.array_equal(G0, G1)

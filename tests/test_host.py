@@ -201,6 +201,9 @@ def test_pair_weights_host_checks():
     with pytest.raises(RuntimeError):
         pair_weights([0], [0], [[0.2, 0.2]], [0.5], V, E, "w2", device="cpu")
     L = _lib.lib
-    assert L.wsb_pair_weights(1, None, None, 4, None, None, None, None, None, None, None) == _lib.WSB_ERR_ARG
-    assert L.wsb_pair_weights(10, None, None, 4, None, None, None, None, None, None, None) == _lib.WSB_ERR_UNSUPPORTED
-    assert L.wsb_pair_weights(1, None, None, 0, None, None, None, None, None, None, None) == _lib.WSB_OK
+    nul = (None, None, 4, None, None, 1, None, 3, None, 1, None, None, None, None)
+    assert L.wsb_pair_weights(1, *nul) == _lib.WSB_ERR_ARG
+    assert L.wsb_pair_weights(10, *nul) == _lib.WSB_ERR_UNSUPPORTED
+    assert L.wsb_pair_weights(1, None, None, 4, None, None, -1, None, 3, None, 1, None, None, None, None) == \
+        _lib.WSB_ERR_ARG
+    assert L.wsb_pair_weights(1, None, None, 0, None, None, 1, None, 3, None, 1, None, None, None, None) == _lib.WSB_OK

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import edge2d as O
+from warpsphboundaries_b200 import workloads
 
 G = Path(__file__).parent / "golden"
 GOLD = json.loads((G / "edge2d_golden_subset.json").read_text())
@@ -198,3 +199,37 @@ def test_dir_extreme_local_oracle_matches_the_polar_grid():
         assert np.abs(got - ref).max() <= 1.5e-2
         assert got[3] == 0.0
         assert (got > 0.5).sum() > 3
+
+
+def test_binned_indicator_equals_the_whole_loop_indicator():
+    """the oracle's restatement of the reference's fast indicator (cell cache + y-bin ray cast, scene.py:281-396) gives
+    the same value as the whole-loop form, bit for bit, on seeded rows of the large 2-D scene -- including rows exactly
+    on vertices and on edge midpoints (interior-angle fractions) and rows in edge-free cells (the cell cache)."""
+    loops, X, h = workloads.c2(n_particles=1 << 16)
+    V, E = workloads.edges_of(loops)
+    rng = np.random.default_rng(3)
+    sub = X[rng.choice(len(X), 3000, replace=False)]
+    sub[:100] = V[rng.choice(len(V), 100, replace=False)]
+    k = rng.choice(len(E), 100, replace=False)
+    sub[100:200] = (V[E[k, 0]] + V[E[k, 1]]) / 2
+    sup = np.full(len(sub), h)
+    cl = O.build_cell_list(V, E, h)
+    a = O.indicator(V, E, 0, sub, sup)
+    b = O.indicator_binned(V, E, 0, sub, sup, cl)
+    assert np.array_equal(a, b)
+    assert np.any(a[:200] % 1.0 != 0.0)                       # boundary rows took the angle sum
+
+
+def test_oracle_matches_reference_torch2d_on_the_gradient_scene():
+    """on 256 near-wall rows of the full gradient scene (2^18 particles, 16 stars of 128 vertices, h = 0.02, w4) the
+    oracle's six moments equal the reference's torch2d values (tests/golden/torch2d_c4.npz) within 1e-12 in units of
+    h^|alpha|."""
+    g = np.load(Path(__file__).parent / "golden" / "torch2d_c4.npz")
+    loops, X, h = workloads.c4()
+    assert np.array_equal(X[g["rows"]], g["particles"])
+    V, E = workloads.edges_of(loops)
+    Xs = g["particles"]
+    out = O.local_twelve(V, E, 0, Xs, np.full(len(Xs), h), "w4", h)
+    for key, c in {"00": 0, "10": 1, "01": 2, "20": 9, "11": 10, "02": 11}.items():
+        sc = h ** (int(key[0]) + int(key[1]))
+        assert np.abs(out[:, c] - g["m_" + key]).max() / sc < 1e-12, key

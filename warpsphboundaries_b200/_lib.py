@@ -24,7 +24,8 @@ EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_d
            "wsb_kinematics", "wsb_radial_channels", "wsb_mesh_create", "wsb_mesh_destroy",
            "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels", "wsb_triangle_channels",
            "wsb_triangle_combine", "wsb_disks_create", "wsb_disks_destroy", "wsb_disk_workspace_size",
-           "wsb_disk_aggregate", "wsb_disk_cone_area", "wsb_disk_dir_extreme", "wsb_pair_weights"]
+           "wsb_disk_aggregate", "wsb_disk_cone_area", "wsb_disk_dir_extreme", "wsb_pair_weights",
+           "wsb_pair_channels"]
 
 
 class SurfaceInfo(ctypes.Structure):
@@ -81,7 +82,8 @@ def _load():
         "wsb_disk_aggregate": (c_int, [P, c_int, P, P, P, c_int64, P, c_int, P, P, P, P, P, P, c_size_t, P]),
         "wsb_disk_cone_area": (c_int, [P, P, P, P, c_int64, P, P, c_double, P, P]),
         "wsb_disk_dir_extreme": (c_int, [P, P, P, P, c_int64, P, P, P, P]),
-        "wsb_pair_weights": (c_int, [c_int, P, P, c_int64, P, P, P, P, P, P, P]),
+        "wsb_pair_channels": (c_int, [P, c_int, c_int, P, P, c_int64, P, P, c_int64, P, P, P]),
+        "wsb_pair_weights": (c_int, [c_int, P, P, c_int64, P, P, c_int64, P, c_int64, P, c_int64, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -46,13 +46,34 @@ template <class KT>
 __global__ void __launch_bounds__(kFemThreads) k_pair_weights(const int32_t* __restrict__ pair_q,
                                                              const int32_t* __restrict__ pair_e, int64_t n_pairs,
                                                              const double* __restrict__ pos,
-                                                             const double* __restrict__ sup,
-                                                             const double* __restrict__ verts,
-                                                             const int32_t* __restrict__ elems, double* __restrict__ w,
-                                                             double* __restrict__ G) {
+                                                             const double* __restrict__ sup, int64_t n_pos,
+                                                             const double* __restrict__ verts, int64_t n_verts,
+                                                             const int32_t* __restrict__ elems, int64_t n_elems,
+                                                             double* __restrict__ w, double* __restrict__ G,
+                                                             int32_t* __restrict__ bad) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (t >= n_pairs) return;
   const int64_t q = pair_q[t], e = pair_e[t];
+  // an index outside its array: the pair's outputs are NaN and the error word is set, nothing out of range is read
+  bool in_range = q >= 0 && q < n_pos && e >= 0 && e < n_elems;
+  if (in_range) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int32_t v = elems[3 * e + k];
+      in_range = in_range && v >= 0 && v < n_verts;
+    }
+  }
+  if (!in_range) {
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      w[3 * t + k] = nan;
+      G[6 * t + 2 * k] = nan;
+      G[6 * t + 2 * k + 1] = nan;
+    }
+    atomicExch(bad, 1);
+    return;
+  }
   const double h = sup[q], x0 = pos[2 * q], x1 = pos[2 * q + 1];
   double r[3][2];
 #pragma unroll
@@ -154,23 +175,37 @@ __global__ void __launch_bounds__(kFemThreads) k_pair_weights(const int32_t* __r
 
 using namespace wsb;
 
+// The launch runs on the device that holds `pos` (made current for the call, the caller's current device restored
+// afterwards), so a caller whose current device is another one still gets the launch in the right context.
 extern "C" int wsb_pair_weights(int kernel, const int32_t* pair_q, const int32_t* pair_e, int64_t n_pairs,
-                                const double* pos, const double* sup, const double* verts, const int32_t* elems,
-                                double* w, double* G, void* stream) {
+                                const double* pos, const double* sup, int64_t n_pos, const double* verts,
+                                int64_t n_verts, const int32_t* elems, int64_t n_elems, double* w, double* G,
+                                int32_t* status, void* stream) {
   if (n_pairs < 0 || n_pairs > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_pair_weights: pair count out of range");
+  if (n_pos < 0 || n_verts < 0 || n_elems < 0) return fail(WSB_ERR_ARG, "wsb_pair_weights: negative array size");
   if (kernel < 0 || kernel >= kNumKernels)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_pair_weights: kernel id " + std::to_string(kernel) +
                                          " (exact-table kernels only)");
   if (n_pairs == 0) return WSB_OK;
-  if (!pair_q || !pair_e || !pos || !sup || !verts || !elems || !w || !G)
+  if (!pair_q || !pair_e || !pos || !sup || !verts || !elems || !w || !G || !status)
     return fail(WSB_ERR_ARG, "wsb_pair_weights: NULL array");
+  cudaPointerAttributes attr{};
+  WSB_CUDA(cudaPointerGetAttributes(&attr, pos));
+  if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged)
+    return fail(WSB_ERR_ARG, "wsb_pair_weights: positions are not device memory");
+  int prev = 0;
+  WSB_CUDA(cudaGetDevice(&prev));
+  if (prev != attr.device) WSB_CUDA(cudaSetDevice(attr.device));
   const unsigned grid = (unsigned)((n_pairs + kFemThreads - 1) / kFemThreads);
   cudaStream_t st = (cudaStream_t)stream;
   const int rc = dispatch_kernel(kernel, [&](auto kt) {
-    k_pair_weights<decltype(kt)><<<grid, kFemThreads, 0, st>>>(pair_q, pair_e, n_pairs, pos, sup, verts, elems, w, G);
+    k_pair_weights<decltype(kt)><<<grid, kFemThreads, 0, st>>>(pair_q, pair_e, n_pairs, pos, sup, n_pos, verts,
+                                                                 n_verts, elems, n_elems, w, G, status);
     return 0;
   });
+  const cudaError_t launch = cudaGetLastError();
+  if (prev != attr.device) WSB_CUDA(cudaSetDevice(prev));
   if (rc) return rc;
-  WSB_CUDA(cudaGetLastError());
+  WSB_CUDA(launch);
   return WSB_OK;
 }

@@ -217,9 +217,97 @@ __global__ void k_contract(int K, double mass, double plane2, const int32_t* __r
   write_outputs(ch, lsup[r], rot, r, lam, G, cov, m1, m2);
 }
 
+// ------------------------------------------------------------------------------------------------ pair-list channels
+// One thread per (query, edge) pair of a pair list (the (qi, e) lists of SurfaceRep.topology): the pair's twelve
+// edge-local channels, units of h, x 1/pi, by the closed-form chord engine block by block -- the reference's
+// warpbc.edge_channels + second_channels over a pair list (src/warpSPHBoundaries/edge/warpbc.py:919-991), which
+// SurfaceRep.moments sums per query (scene.py:384-416).  A tensile (quadrature) kernel defines its G channels only; the
+// others are NaN.  A query or edge index outside its array gives NaN channels and sets the status word.
+template <class KT, int PREC, int B>
+__device__ __forceinline__ void pair_blocks(const PairGeo& g, double* acc) {
+  if constexpr (B < KT::kBlocks) {
+    block_channels<KT, B, PREC>(g, acc);
+    pair_blocks<KT, PREC, B + 1>(g, acc);
+  }
+}
+
+template <class KT, int PREC>
+__global__ void k_pair_channels(SurfView S, const int32_t* __restrict__ qi, const int32_t* __restrict__ e,
+                                int64_t n_pairs, const double* __restrict__ lpos, const double* __restrict__ lsup,
+                                int64_t n_rows, double* __restrict__ c, int32_t* __restrict__ status) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n_pairs) return;
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  double acc[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+  const int64_t q = qi[t], ei = e[t];
+  if (q < 0 || q >= n_rows || ei < 0 || ei >= S.n_edges) {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) c[12 * t + k] = nan;
+    atomicExch(status, 1);
+    return;
+  }
+  const double h = lsup[q];
+  PairGeo g;
+  if (pair_geo_row(lpos[2 * q], lpos[2 * q + 1], h, 1.0 / h, S.erec[ei], g)) {
+    if constexpr (KT::kQuad) {
+      double lo, hi, rlo, rhi, zz;
+      if (clip_chord(g, 1.0, lo, hi, rlo, rhi, zz)) {
+        const double W0 = quad_chord<KT>(lo, hi, g.z);
+        acc[3] = -g.n0 * W0;
+        acc[4] = -g.n1 * W0;
+      }
+    } else {
+      pair_blocks<KT, PREC, 0>(g, acc);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 12; ++k) {
+    const bool defined = !KT::kQuad || k == 3 || k == 4;
+    c[12 * t + k] = defined ? acc[k] * kInvPi : nan;
+  }
+}
+
 }  // namespace wsb
 
 using namespace wsb;
+
+extern "C" int wsb_pair_channels(const wsb_surface* s_, int kernel, int precision, const int32_t* qi, const int32_t* e,
+                                 int64_t n_pairs, const double* lpos, const double* lsup, int64_t n_rows, double* c,
+                                 int32_t* status, void* stream) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s) return fail(WSB_ERR_ARG, "wsb_pair_channels: NULL surface");
+  if (n_pairs < 0 || n_rows < 0) return fail(WSB_ERR_ARG, "wsb_pair_channels: negative size");
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+    return fail(WSB_ERR_UNSUPPORTED, "wsb_pair_channels: precision " + std::to_string(precision));
+  const bool quad = kernel == Kern_w2p5::kId || kernel == Kern_w4p5::kId;
+  if (!quad && (kernel < 0 || kernel >= kNumKernels)) return fail(WSB_ERR_UNSUPPORTED, "unknown kernel id");
+  if (n_pairs == 0) return WSB_OK;
+  if (!qi || !e || !lpos || !lsup || !c || !status) return fail(WSB_ERR_ARG, "wsb_pair_channels: NULL array");
+  WSB_CUDA(cudaSetDevice(s->device));
+  const unsigned grid = (unsigned)((n_pairs + 127) / 128);
+  cudaStream_t st = (cudaStream_t)stream;
+  const SurfView v = view_of(s);
+  auto launch = [&](auto kt) {
+    using KT = decltype(kt);
+    if (precision == WSB_PREC_MIXED)
+      k_pair_channels<KT, WSB_PREC_MIXED><<<grid, 128, 0, st>>>(v, qi, e, n_pairs, lpos, lsup, n_rows, c, status);
+    else
+      k_pair_channels<KT, WSB_PREC_FP64><<<grid, 128, 0, st>>>(v, qi, e, n_pairs, lpos, lsup, n_rows, c, status);
+    return 0;
+  };
+  int rc;
+  if (kernel == Kern_w2p5::kId)
+    rc = launch(Kern_w2p5{});
+  else if (kernel == Kern_w4p5::kId)
+    rc = launch(Kern_w4p5{});
+  else
+    rc = dispatch_kernel(kernel, launch);
+  if (rc) return rc;
+  WSB_CUDA(cudaGetLastError());
+  return WSB_OK;
+}
 
 static double kernel_plane2(int kernel) {
   double v = 0.0;

@@ -25,18 +25,33 @@ def pair_weights(pair_q, pair_e, positions, supports, vertices, elements, kernel
     dev = torch.device(device)
     if dev.type != "cuda":
         raise RuntimeError("pair_weights runs on a CUDA device (libwsb.so has no CPU path)")
-    q = _dev(pair_q, dev, torch.int32).reshape(-1)
-    e = _dev(pair_e, dev, torch.int32).reshape(-1)
-    if len(q) != len(e):
-        raise ValueError("pair_weights: pair_q and pair_e differ in length")
-    pos = _dev(positions, dev, F64).reshape(-1, 2)
-    sup = _dev(supports, dev, F64).reshape(-1)
-    V = _dev(vertices, dev, F64).reshape(-1, 2)
-    E = _dev(elements, dev, torch.int32).reshape(-1, 3)
-    P = len(q)
-    w = torch.empty((P, 3), dtype=F64, device=dev)
-    G = torch.empty((P, 3, 2), dtype=F64, device=dev)
-    check(lib.wsb_pair_weights(KERNEL_IDS[kernel], ptr(q), ptr(e), P, ptr(pos), ptr(sup), ptr(V), ptr(E), ptr(w),
-                               ptr(G), _lib.ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
-          "wsb_pair_weights")
+    with torch.cuda.device(dev):                    # the launch and the allocations on `device`, whatever is current
+        q = _dev(pair_q, dev, torch.int32).reshape(-1)
+        e = _dev(pair_e, dev, torch.int32).reshape(-1)
+        if len(q) != len(e):
+            raise ValueError("pair_weights: pair_q and pair_e differ in length")
+        pos = _dev(positions, dev, F64).reshape(-1, 2)
+        sup = _dev(supports, dev, F64).reshape(-1)
+        V = _dev(vertices, dev, F64).reshape(-1, 2)
+        E = _dev(elements, dev, torch.int32).reshape(-1, 3)
+        if len(sup) != len(pos):
+            raise ValueError("pair_weights: positions and supports differ in length")
+        P = len(q)
+        if P:
+            # index ranges checked before the launch (the kernel also refuses them: NaN outputs and a status word)
+            lim = torch.stack([q.min(), q.max(), e.min(), e.max(), E.min() if len(E) else q.new_zeros(()),
+                               E.max() if len(E) else q.new_zeros(())]).cpu().tolist()
+            if lim[0] < 0 or lim[1] >= len(pos):
+                raise ValueError(f"pair_weights: query index out of range [0, {len(pos)})")
+            if lim[2] < 0 or lim[3] >= len(E):
+                raise ValueError(f"pair_weights: element index out of range [0, {len(E)})")
+            if lim[4] < 0 or lim[5] >= len(V):
+                raise ValueError(f"pair_weights: vertex index out of range [0, {len(V)})")
+        w = torch.empty((P, 3), dtype=F64, device=dev)
+        G = torch.empty((P, 3, 2), dtype=F64, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        check(lib.wsb_pair_weights(KERNEL_IDS[kernel], ptr(q), ptr(e), P, ptr(pos), ptr(sup), len(pos), ptr(V), len(V),
+                                   ptr(E), len(E), ptr(w), ptr(G), ptr(status),
+                                   _lib.ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)),
+              "wsb_pair_weights")
     return (w, G) if as_torch else (w.cpu().numpy(), G.cpu().numpy())

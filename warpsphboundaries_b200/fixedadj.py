@@ -74,11 +74,28 @@ class BodyAdjacency:
 
 @dataclass
 class SceneAdjacency:
+    """who interacts with whom (scene.py:1083-1108): per body a BodyAdjacency; integers and kernel-independent
+    geometry only, so one adjacency serves every kernel and channel set at these positions."""
     numQueries: int
     bodies: list
-    info: dict = field(default_factory=dict)
+    stats: dict = field(default_factory=dict)
     queryParticles: object = None
     supportMax: float = 0.0
+
+    def restrict(self, index):
+        """the adjacency of the global rows `index` (ascending, distinct) alone, renumbered 0 .. len(index) - 1
+        (scene.py:1090-1108); no search."""
+        dev = index.device
+        newid = torch.full((self.numQueries,), -1, dtype=torch.long, device=dev)
+        newid[index] = torch.arange(len(index), device=dev)
+        out = []
+        for ba in self.bodies:
+            rows = torch.nonzero(newid[ba.cand] >= 0).flatten()
+            rowmap = torch.full((len(ba.cand),), -1, dtype=torch.long, device=dev)
+            rowmap[rows] = torch.arange(len(rows), device=dev)
+            out.append(BodyAdjacency(ba.body, newid[ba.cand[rows]], ba.lpos[rows], ba.lsup[rows],
+                                     [None if t is None else t.restrict(rowmap, rows) for t in ba.reps]))
+        return SceneAdjacency(len(index), out, {"candidates": [len(b.cand) for b in out]}, None, self.supportMax)
 
 
 def body_candidates(body, lpos, sup, allowed):

@@ -95,8 +95,8 @@ class FusedWall(WallAggregate):
         for g in self.groups:
             if g.kernel not in _GROUP_IDS:
                 raise NotImplementedError(f"FusedWall: kernel group {g.kernel!r} is not built")
-            if g.kernel in QUAD_KERNEL_IDS and route != "fused":
-                raise NotImplementedError(f"FusedWall: the tensile group {g.kernel!r} runs on the fused route only")
+            if g.kernel in QUAD_KERNEL_IDS and route == "plain":
+                raise NotImplementedError(f"FusedWall: the tensile group {g.kernel!r} has no plain route")
         sig = (route, self.support) + tuple(id(r) for b in scene.bodies for r in b.reps)
         if getattr(scene, "_wsb_checked", None) != sig:
             for b in scene.bodies:
@@ -104,8 +104,8 @@ class FusedWall(WallAggregate):
                     if isinstance(r, DiskArrayRep):
                         if route != "fused":
                             raise NotImplementedError("FusedWall: disk sets take the fused route")
-                    elif r._triangle is not None and route != "fused":
-                        raise NotImplementedError("FusedWall: conditioned single triangles take the fused route")
+                    elif r._triangle is not None and route == "plain":
+                        raise NotImplementedError("FusedWall: conditioned single triangles have no plain route")
             scene._wsb_checked = sig
         if any(g.kernel in QUAD_KERNEL_IDS for g in self.groups) and any(
                 isinstance(r, DiskArrayRep) for b in scene.bodies for r in b.fused_reps(self.support, self.dev)):
@@ -132,6 +132,8 @@ class FusedWall(WallAggregate):
         elif route == "plain":
             for gi, kid in enumerate(kids):
                 self._plain(ps, kid, self.res[gi])
+        elif route == "scene":
+            self._scene_route(ps, self.res)
         else:
             raise ValueError(f"unknown route {route!r}")
         self.out = {}
@@ -210,6 +212,23 @@ class FusedWall(WallAggregate):
         key = (self._group, bi, ri)
         self.qstatus[key] = st
         self.estimates[key] = est
+
+    def _scene_route(self, ps, outs):
+        """the Scene route (provider.py:89-92 with fixedAdjacency=False): one `Scene.adjacency` (candidates and the
+        pair list of every surface), then per group `Scene.precompute` (per-pair channels, per-query sums, indicator,
+        conditioned triangles) and the world-frame moments added into the [B, N] outputs of the candidate rows."""
+        props = OperationProperties(operationMode=OperationDirection.BoundaryToFluid)
+        adj = self.scene.adjacency(ps, props)
+        for g, out in zip(self.groups, outs):
+            pm = self.scene.precompute(adj, OperationProperties(kernel=g.kernel), precision=self.precision)
+            for bi, ent in enumerate(pm.entries):
+                for m in ent["surface"] + ent["implicit"]:
+                    q = m.q.long()
+                    out["lam"][bi].index_add_(0, q, m.lam)
+                    out["G"][bi].index_add_(0, q, m.g0)
+                    out["Cov"][bi].index_add_(0, q, m.g1)
+                    out["m1"][bi].index_add_(0, q, m.m1)
+                    out["m2"][bi].index_add_(0, q, m.m2)
 
     def _plain(self, ps, kid, out):
         props = OperationProperties(operationMode=OperationDirection.BoundaryToFluid)
@@ -407,7 +426,9 @@ class AnalyticBoundary:
                   lean=False):
         """the wall evaluation at the positions of `ps` (provider.py:89-110): `.out` holds lam, G, Cov per body;
         `evaluate` serves m1, m2 and a1g1 as well; without `lean` the delta+ layout adds cover, lap (when `laplacian`)
-        and tens, raw (the scheme applies its factors).  `support`: host float >= every support of `ps`."""
+        and tens, raw (the scheme applies its factors).  `support`: host float >= every support of `ps`.
+        `fixedAdjacency=False` takes the Scene route (Scene.adjacency + Scene.precompute: pair lists, per-pair
+        channels, per-query sums) instead of the fused pass; the same values within rounding."""
         if lean:
             groups, idx = (FusedGroup(kernelName(kernel)),), {"w": 0}
         else:
@@ -415,7 +436,8 @@ class AnalyticBoundary:
         allowed = None
         if getattr(ps, "kinds", None) is not None:      # without kinds every query is served: no mask, no host read
             allowed = queryAllowed(ps, self.properties(kernel).operationMode, self.scene.device)
-        fw = FusedWall(self.scene, ps, support, groups, route=self.route, precision=self.precision, allowed=allowed)
+        route = self.route if fixedAdjacency else "scene"          # Scene.adjacency + precompute (the oracle path)
+        fw = FusedWall(self.scene, ps, support, groups, route=route, precision=self.precision, allowed=allowed)
         outs = [WallOutput("lam", 0, "lam"), WallOutput("G", 0, "g0"), WallOutput("Cov", 0, "cov")]
         if not lean:
             outs.append(WallOutput("cover", idx["cone"], "g0"))

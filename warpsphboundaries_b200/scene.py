@@ -240,6 +240,73 @@ class SurfaceRep:
         keep = ft.e >= 0
         return SurfaceTopology(ft.qi[keep], ft.e[keep], supmax, ft.ind)
 
+    def moments(self, topo, lpos, lsup, qglobal, kernel, device, channels=None, precision="fp64"):
+        """complete polygon moments of the queries lpos [C, 2] (body frame, supports lsup [C]) from the pair list
+        `topo` (scene.py:384-416): the twelve channels of every pair on the device (wsb_pair_channels), summed per
+        query, plus the indicator times the whole-plane constants; a conditioned single triangle overrides the rows its
+        area quadrature takes; physical units.  Channels 0..8 are the legacy nine, 9..11 m20, m11, m02; None asks for
+        all twelve and an explicit subset zeroes the others.  A tensile kernel (w2p5 / w4p5) defines g0 only.  Returns
+        `RepMoments` in the body frame, q = `qglobal`."""
+        from .kernels import KERNEL_IDS, QUAD_KERNEL_IDS, plane_channels
+        from .shim import kernelName
+        name = kernel if isinstance(kernel, str) and kernel in QUAD_KERNEL_IDS else kernelName(kernel)
+        requested = set(range(12)) if channels is None else {int(k) for k in channels}
+        if not requested <= set(range(12)):
+            raise ValueError("Surface moment channels must be in 0..11")
+        quad = name in QUAD_KERNEL_IDS
+        if name not in KERNEL_IDS and not quad:
+            raise NotImplementedError(f"SurfaceRep.moments: kernel {name!r} is not built")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        if quad and self._triangle is not None:
+            raise NotImplementedError("SurfaceRep.moments: the tensile kernels have no conditioned-triangle route")
+        dev = torch.device(device)
+        lp = lpos.to(dev, F64).contiguous()
+        ls = lsup.to(dev, F64).contiguous()
+        C = len(lp)
+        kid = QUAD_KERNEL_IDS[name] if quad else KERNEL_IDS[name]
+        out = torch.zeros((C, 12), dtype=F64, device=dev)
+        if topo is not None and len(topo.qi):
+            ns = self.native(topo.supMax, dev)
+            P = len(topo.qi)
+            qi = topo.qi.to(dev, torch.int32).contiguous()
+            e = topo.e.to(dev, torch.int32).contiguous()
+            c = torch.empty((P, 12), dtype=F64, device=dev)
+            st = torch.zeros(1, dtype=torch.int32, device=dev)
+            check(lib.wsb_pair_channels(ns.handle, kid, _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64,
+                                        ptr(qi), ptr(e), P, ptr(lp), ptr(ls), C, ptr(c), ptr(st), _stream()),
+                  "wsb_pair_channels")
+            out.index_add_(0, qi.long(), c)
+        estimate = torch.zeros((C, 12), dtype=F64, device=dev)
+        status = torch.zeros(C, dtype=torch.int32, device=dev)
+        if quad:
+            keep = torch.zeros(12, dtype=torch.bool, device=dev)
+            keep[3:5] = True
+            out = torch.where(keep, out, torch.full_like(out, float("nan")))
+        else:
+            ind = topo.indicator(self, lp, ls) if topo is not None else self.indicator(lp, ls)
+            out += ind[:, None] * torch.tensor(plane_channels(name), dtype=F64, device=dev)
+            if self._triangle is not None and C:
+                tri, area2, sign = self._triangle
+                vals = torch.empty((C, 12), dtype=F64, device=dev)
+                check(lib.wsb_triangle_channels(_lib.dptr(tri), area2, sign, self.background, kid, ptr(lp), ptr(ls),
+                                                None, C, 2e-12, 4096, ptr(vals), ptr(estimate), ptr(status), _stream()),
+                      "wsb_triangle_channels")
+                out = torch.where((status != 0)[:, None], vals, out)
+        mask = torch.tensor([float(k in requested) for k in range(12)], dtype=F64, device=dev)
+        one = torch.ones_like(ls)
+        physical = torch.stack([one, ls, ls, 1 / ls, 1 / ls, one, one, one, one, ls * ls, ls * ls, ls * ls], 1)
+        out = out * mask * physical
+        estimate = estimate * mask * physical
+        m2 = (torch.stack([out[:, 9], out[:, 10], out[:, 10], out[:, 11]], 1).reshape(-1, 2, 2)
+              if requested & {9, 10, 11} else None)
+        return RepMoments(qglobal, out[:, 0], out[:, 3:5], out[:, 1:3], out[:, 5:9].reshape(-1, 2, 2), m2, estimate,
+                          status)
+
+    def pairs(self, lpos, lsup, qglobal, kernel, device, channels=None, precision="fp64"):
+        """topology + moments in one call (scene.py:418-422; the fallback surfaces of implicit representations)."""
+        return self.moments(self.topology(lpos, lsup), lpos, lsup, qglobal, kernel, device, channels, precision)
+
 
 
 class BoxRep(SurfaceRep):
@@ -543,7 +610,8 @@ class SdfRep:
 
 @dataclass
 class SurfaceTopology:
-    """the pair list of one SurfaceRep against a set of queries (scene.py:145-178)."""
+    """the pair list of one SurfaceRep against a set of queries (scene.py:145-178): (query row, edge) pairs with the
+    segment closer than the support, rows ascending, a row's edges in cell-list order; the rows' indicator."""
     qi: torch.Tensor
     e: torch.Tensor
     supMax: float
@@ -554,22 +622,55 @@ class SurfaceTopology:
             self._ind = rep.indicator(lpos, lsup)
         return self._ind
 
+    def restrict(self, rowmap, rows):
+        """the pairs of the rows `rows` only, renumbered by `rowmap` (old row -> new row or -1; scene.py:160-178)."""
+        new = rowmap[self.qi.long()]
+        sel = new >= 0
+        return SurfaceTopology(new[sel].to(torch.int32), self.e[sel], self.supMax,
+                               None if self._ind is None else self._ind[rows])
+
 
 @dataclass
 class RepMoments:
-    """per-query moments of one representation in physical units (scene.py:181-210): lam [P], g0 [P,2], m1 [P,2],
-    g1 [P,2,2] = int y (x) grad_x W, m2 [P,2,2]."""
+    """per-query moments of one representation in physical units (scene.py:181-210): lam [P], g0 [P, 2] =
+    int grad_x W, m1 [P, 2] = int y W, g1 [P, 2, 2] = int y_d d_j W, m2 [P, 2, 2] = int y_d y_e W (y = x' - x_i);
+    the conditioned quadrature's estimate [P, 12] and status [P] (0 closed form, 1 refined area, -1 failed)."""
     q: torch.Tensor
     lam: torch.Tensor
     g0: torch.Tensor
     m1: Optional[torch.Tensor] = None
     g1: Optional[torch.Tensor] = None
     m2: Optional[torch.Tensor] = None
+    quadrature_estimate: Optional[torch.Tensor] = None
+    quadrature_status: Optional[torch.Tensor] = None
 
     def toWorld(self, pose: Pose):
-        R = pose.R
+        """the moments rotated to the world frame; error estimates rotated by |R| (bounds stay bounds)."""
+        R = pose.R.to(self.lam.device)
+        est = self.quadrature_estimate
+        if est is not None:
+            A = R.abs()
+            est = est.clone()
+            est[:, 1:3] = est[:, 1:3] @ A.T
+            est[:, 3:5] = est[:, 3:5] @ A.T
+            est[:, 5:9] = (A @ est[:, 5:9].reshape(-1, 2, 2) @ A.T).flatten(1)
+            E = A @ torch.stack([est[:, 9], est[:, 10], est[:, 10], est[:, 11]], 1).reshape(-1, 2, 2) @ A.T
+            est[:, 9], est[:, 10], est[:, 11] = E[:, 0, 0], E[:, 0, 1], E[:, 1, 1]
         return RepMoments(self.q, self.lam, self.g0 @ R.T, None if self.m1 is None else self.m1 @ R.T,
-                          None if self.g1 is None else R @ self.g1 @ R.T, None if self.m2 is None else R @ self.m2 @ R.T)
+                          None if self.g1 is None else R @ self.g1 @ R.T, None if self.m2 is None else R @ self.m2 @ R.T,
+                          est, self.quadrature_status)
+
+
+@dataclass
+class PairMoments:
+    """the per-pair integrals of ONE kernel (and channel set) over an adjacency (scene.py:1111-1120): per body
+    dict(body, cand, surface=[RepMoments world], implicit=[RepMoments world], volume=[]); `channels` None = all
+    twelve."""
+    numQueries: int
+    kernel: str
+    entries: list
+    stats: dict
+    channels: Optional[frozenset] = None
 
 
 # ----------------------------------------------------------------------------------------------------------- bodies
@@ -726,6 +827,81 @@ class Scene:
 
     def kinematics(self, x):
         return BodyKinematics(self.bodies, x) if self.bodies else None
+
+    # ---- the Scene route to the twelve moments: adjacency (integers, kernel independent) then precompute (per kernel)
+    def adjacency(self, queryParticles, operationProperties):
+        """`SceneAdjacency` (scene.py:1400-1416): per body the candidate queries (support circle against the body box;
+        every allowed query of an unbounded body), their body-frame positions and supports, and the pair topology of
+        every SurfaceRep (None for the other representations, whose pairs `precompute` makes).  Only
+        `operationProperties.operationMode` is read; one adjacency serves every kernel and channel set."""
+        from .fixedadj import BodyAdjacency, SceneAdjacency, body_candidates
+        from .shim import queryAllowed
+        dev = self.device
+        pos = queryParticles.positions.to(dev, F64).contiguous()
+        sup = queryParticles.supports.to(dev, F64).contiguous()
+        if pos.shape[1] != 2:
+            raise NotImplementedError("2D only")
+        allowed = queryAllowed(queryParticles, operationProperties.operationMode, dev)
+        kin = self.kinematics(pos)
+        bodies, stats = [], {"candidates": []}
+        for bi, body in enumerate(self.bodies):
+            valid = body_candidates(body, kin.local[bi], sup, allowed)
+            cand = torch.nonzero(valid).flatten()
+            lpos, lsup = kin.local[bi][cand].contiguous(), sup[cand].contiguous()
+            stats["candidates"].append(int(len(cand)))
+            reps = [(r.topology(lpos, lsup) if isinstance(r, SurfaceRep) and len(cand) else None) for r in body.reps]
+            bodies.append(BodyAdjacency(body, cand, lpos, lsup, reps))
+        return SceneAdjacency(len(pos), bodies, stats, queryParticles)
+
+    def precompute(self, adjacency, operationProperties, channels=None, precision="fp64"):
+        """`PairMoments` of one kernel over an adjacency (scene.py:1418-1433): per body the world-frame `RepMoments` of
+        every SurfaceRep on its pair list ('surface'), of implicit and sampled shapes through their exact polygon
+        ('implicit'); channels as in `SurfaceRep.moments`.  Disk sets have no pair-list form here (the fused route
+        integrates them)."""
+        from .shim import kernelName
+        from .kernels import QUAD_KERNEL_IDS
+        k = operationProperties.kernel
+        name = k if isinstance(k, str) and k in QUAD_KERNEL_IDS else kernelName(k)
+        entries, stats = [], {"candidates": list(adjacency.stats.get("candidates") or []), "pairs": 0}
+        for ba in adjacency.bodies:
+            ent = {"body": ba.body, "cand": ba.cand, "surface": [], "implicit": [], "volume": []}
+            if len(ba.cand):
+                pose = ba.body.pose
+                for rep, topo in zip(ba.body.reps, ba.reps):
+                    if isinstance(rep, SurfaceRep):
+                        m = rep.moments(topo, ba.lpos, ba.lsup, ba.cand, name, self.device, channels, precision)
+                        ent["surface"].append(m.toWorld(pose))
+                    elif isinstance(rep, (ImplicitRep, SdfRep)):
+                        surf = rep.lowered(float(ba.lsup.max()), self.device)
+                        if not isinstance(surf, SurfaceRep):
+                            raise NotImplementedError("Scene.precompute: a solid disk has no pair-list form here "
+                                                      "(the fused route integrates it)")
+                        m = surf.pairs(ba.lpos, ba.lsup, ba.cand, name, self.device, channels, precision)
+                        ent["implicit"].append(m.toWorld(pose))
+                    else:
+                        raise NotImplementedError(f"Scene.precompute: {type(rep).__name__} has no pair-list form here "
+                                                  f"(the fused route integrates it)")
+            stats["pairs"] += sum(len(m.q) for m in ent["surface"] + ent["implicit"])
+            entries.append(ent)
+        return PairMoments(adjacency.numQueries, name, entries, stats,
+                           None if channels is None else frozenset(int(c) for c in channels))
+
+    def pairMoments(self, queryParticles, operationProperties, channels=None, precision="fp64"):
+        """adjacency + precompute in one call (scene.py:1435-1437)."""
+        return self.precompute(self.adjacency(queryParticles, operationProperties), operationProperties, channels,
+                               precision)
+
+    def moments(self, source, queryParticles, operationProperties, channels=None, precision="fp64"):
+        """`source` as PairMoments: None builds adjacency + precompute, a SceneAdjacency is precomputed, a PairMoments
+        is returned as it is (scene.py:1439-1446)."""
+        from .fixedadj import SceneAdjacency
+        if source is None:
+            return self.pairMoments(queryParticles, operationProperties, channels, precision)
+        if isinstance(source, SceneAdjacency):
+            return self.precompute(source, operationProperties, channels, precision)
+        if isinstance(source, PairMoments):
+            return source
+        raise TypeError(f"Scene.moments: unsupported source {type(source).__name__}")
 
     def signed_distance(self, points, body=None, supportMax=None, want_body=False):
         """(d [M], n [M, 2], hit [M][, body [M]]) of world points to the nearest body: d > 0 in the fluid, n the unit

@@ -52,8 +52,9 @@ def stars(n_polys, n_vertices, seed, box=4.0, rmin=0.05, rmax=0.4):
     return loops
 
 
-def c2(n_particles=1 << 20, seed=0, h=0.02, n_polys=64, tangent_fraction=0.01):
-    """(loops, particles [N, 2], h) of the large mixed-precision scene."""
+def c2(n_particles=1 << 20, seed=0, h=0.02, n_polys=64, tangent_fraction=0.01, return_special=False):
+    """(loops, particles [N, 2], h) of the large mixed-precision scene; with `return_special` also the row indices of
+    the near-tangent particles and of the particles one support away from a vertex."""
     loops = stars(n_polys, (32, 512), seed)
     rng = np.random.default_rng(seed + 1)
     X = rng.uniform(0, 4.0, size=(n_particles, 2))
@@ -76,6 +77,8 @@ def c2(n_particles=1 << 20, seed=0, h=0.02, n_polys=64, tangent_fraction=0.01):
     slots = rng.choice(n_particles, size=m + mv, replace=False)
     X[slots[:m]] = Xt
     X[slots[m:]] = Xv
+    if return_special:
+        return loops, X, h, {"tangent": slots[:m], "vertex": slots[m:]}
     return loops, X, h
 
 
