@@ -50,7 +50,9 @@ enum {
 enum {
   WSB_PREC_FP64 = 0,   /* every step in float64 */
   WSB_PREC_MIXED = 1,  /* float32 special functions where the per-pair error bound allows, float64 guards and sums */
-  WSB_PREC_FP32 = 2    /* every step in float32 (wsb_radial_channels only) */
+  WSB_PREC_FP32 = 2    /* the float route: 2-D chord sums in float32 (Chebyshev profiles, Gauss-Legendre on panels graded
+                          from the foot point), chord clip, edge frame and row sums in float64; 3-D spheres: every step
+                          in float32 */
 };
 
 /* solid kinds of wsb_radial_channels */
@@ -298,6 +300,56 @@ int wsb_disk_dir_extreme(const wsb_disks* d, const double* pos, const double* su
 int wsb_pair_weights(int kernel, const int32_t* pair_q, const int32_t* pair_e, int64_t n_pairs, const double* pos,
                      const double* sup, int64_t n_pos, const double* verts, int64_t n_verts, const int32_t* elems,
                      int64_t n_elems, double* w, double* G, int32_t* status, void* stream);
+
+/* ---- scenes: several rigid bodies, each with closed surfaces and a pose ----
+ * A scene groups surfaces (wsb_surface handles, which must outlive the scene) into bodies with poses (cx, cy, cos,
+ * sin: world = R local + c), on one device.  wsb_scene_aggregate evaluates every body at once: for each kernel group
+ * g and body b, lam[g] + b*ld, G[g] + 2*b*ld, cov[g] + 4*b*ld, m1[g] + 2*b*ld, m2[g] + 4*b*ld receive that body's
+ * outputs of the n rows (assigned; ld >= n is the row stride per body; a body without surfaces gets zeros), world
+ * frame, as wsb_aggregate_groups per surface (the first surface of a body assigns, the others add).  The workspace
+ * (wsb_scene_workspace_size) is reused surface after surface on the stream.  wsb_scene_set_pose copies the pose on
+ * `stream` and returns when it has arrived.  Replaces the reference's Scene with its bodies and poses
+ * (src/warpSPHBoundaries/scene/scene.py:1230-1300) evaluated by the fused wall over all bodies
+ * (src/warpSPHBoundaries/scene/fused.py:506-547, called from scene/provider.py:89-110). */
+typedef struct wsb_scene wsb_scene;
+int wsb_scene_create(int device, wsb_scene** out);
+int wsb_scene_destroy(wsb_scene* sc);
+int wsb_scene_add_body(wsb_scene* sc, const double* pose, int* body);
+int wsb_scene_add_surface(wsb_scene* sc, int body, const wsb_surface* surface);
+int wsb_scene_set_pose(wsb_scene* sc, int body, const double* pose, void* stream);
+int wsb_scene_info(const wsb_scene* sc, int* n_bodies, int* n_surfaces);
+size_t wsb_scene_workspace_size(const wsb_scene* sc, int64_t n);
+int wsb_scene_aggregate(const wsb_scene* sc, int n_groups, const int32_t* kernels, int precision, const double* pos,
+                        const double* sup, const int32_t* allowed, int64_t n, int64_t ld, double* const* lam,
+                        double* const* G, double* const* cov, double* const* m1, double* const* m2, void* workspace,
+                        size_t workspace_bytes, void* stream);
+
+/* ---- the serving loop: continuous batching of boundary queries over resident scenes ----
+ * wsb_server_create: n_streams stream slots on `device`, batches of at most max_batch_rows rows, persistent device
+ * buffers (inputs, outputs, workspace) grown on demand within hbm_budget bytes.  wsb_serve_submit queues one request
+ * (lambda + the twelve moments of kernel `kernel` at the caller's device arrays pos [n*2], sup [n]; outputs assigned
+ * into the caller's [B, n, ...] arrays lam [B*n], G [B*n*2], cov [B*n*4], m1 [B*n*2], m2 [B*n*4], any may be NULL;
+ * with grad != 0 also d_pos [n*2] = d sum_b lam_b / dx), read once `stream` reaches the point of submission, and
+ * returns its id; it may launch work.  wsb_serve_poll advances the scheduler (retires finished batches, admits queued
+ * requests into free slots: the oldest request and every later one of the same scene, kernel, precision and grad that
+ * fits the batch rows, as one launch family over their concatenated rows; a request of more than max_batch_rows rows
+ * runs in chunks on its own arrays) and sets *done for request_id (for request_id 0: nothing queued or running).
+ * wsb_serve_wait polls until done; wsb_serve_release forgets a completed request.  A request's result is
+ * bit-identical alone and in any batch (rows are independent).  wsb_server_stats: completed requests and the p50 / p99
+ * of their latency (submission to the poll that saw their completion).  One host thread drives a server.  Replaces
+ * the provider call per simulation (src/warpSPHBoundaries/scene/provider.py:38-113) with a shared request loop; the
+ * reference has no server of its own. */
+typedef struct wsb_server wsb_server;
+int wsb_server_create(int device, int n_streams, int64_t max_batch_rows, size_t hbm_budget, wsb_server** out);
+int wsb_server_destroy(wsb_server* srv);
+int wsb_serve_submit(wsb_server* srv, const wsb_scene* scene, int kernel, int precision, int grad, const double* pos,
+                     const double* sup, int64_t n, double* lam, double* G, double* cov, double* m1, double* m2,
+                     double* d_pos, void* stream, int64_t* request_id);
+int wsb_serve_poll(wsb_server* srv, int64_t request_id, int* done);
+int wsb_serve_wait(wsb_server* srv, int64_t request_id);
+int wsb_serve_release(wsb_server* srv, int64_t request_id);
+int wsb_server_stats(const wsb_server* srv, int64_t* completed, double* p50_ms, double* p99_ms,
+                     size_t* reserved_bytes);
 
 /* ---- closed triangle surfaces (3-D) ----
  * A watertight, consistently oriented triangle surface with outward normals (positive signed volume): verts

@@ -201,6 +201,17 @@ def torch2d_c4(torch2d, n_pts=256):
     np.savez_compressed(HERE / "torch2d_c4.npz", rows=rows, particles=X[rows], h=h, **res)
 
 
+def fluxbridge_subset(root):
+    """the single-element cases of the reference's fluxbridge-v1.json (schema 1) -- 2-D triangles and 3-D tetrahedra
+    at five queries, four kernels, with the baseline requests plus two high-degree ones, and the surface triangles --
+    in the same schema, for the interchange-format tests (the full-degree coverage cases are left out for size)."""
+    src = json.loads((Path(root) / "tests" / "fixtures" / "fluxbridge-v1.json").read_text())
+    cases = [c for c in src["cases"] if len(c["requests"]) <= 32]
+    out = {"schema": src["schema"], "dps": src["dps"], "cases": cases}
+    (HERE / "fluxbridge_v1_subset.json").write_text(json.dumps(out, indent=2) + "\n")
+    print("fluxbridge_v1_subset.json:", len(cases), "of", len(src["cases"]), "cases")
+
+
 def radial_golden(root):
     fx = Path(root) / "tests" / "fixtures"
     rad = json.loads((fx / "fluxbridge-radial-v1.json").read_text())
@@ -476,6 +487,7 @@ if __name__ == "__main__":
     np2d_c1(np2d)
     torch2d_grads(torch2d)
     torch2d_c4(torch2d)
+    fluxbridge_subset(root)
     radial_golden(root)
     mesh3d_golden(root)
     triangle_golden(root)

@@ -1,7 +1,7 @@
 """GPU parity on the benchmark scenes at their stated sizes, through the public API and the C ABI.
 
 c2  2^20 particles in [0, 4]^2, 64 star polygons (one multi-loop surface), h = 0.02: the device evaluates every row
-    for cubic, w2, w4 and w6 in one FusedWall (the bench's step), on the float64 and the mixed route; a seeded
+    for cubic, w2, w4 and w6 in one FusedWall (the bench's step), on the float64, mixed and float routes; a seeded
     10 000-row subset -- every near-tangent and endpoint-on-circle particle, 6 000 rows with neighbour pairs, the rest
     uniform -- is compared with the oracle channel by channel, and its neighbour slots bit for bit.
 c3  2^21 particles in [-1, 1]^3 plus 8 planted queries 1e-7 h off vertices, edge midpoints and face centres, the
@@ -76,7 +76,7 @@ def c2_run():
     ps = ParticleState(pos, sup)
     groups = tuple(FusedGroup(k) for k in C2_KERNELS)
     got = {}
-    for prec in ("fp64", "mixed"):
+    for prec in ("fp64", "mixed", "fp32"):
         fw = FusedWall(scene, ps, h, groups, precision=prec)
         got[prec] = [{k: v[0] for k, v in r.items()} for r in fw.res]
     ft = fixed_topology(rep, pos, sup, torch.ones(N, dtype=torch.bool, device=DEV), h)
@@ -120,7 +120,7 @@ def test_c2_neighbour_slots_bit_exact_at_full_size(c2_run):
     assert len(r["special"]) > 200 and (r["npairs"][r["special"]] > 0).mean() > 0.9
 
 
-@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("mixed", 1e-6)])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("mixed", 1e-6), ("fp32", 1e-3)])
 def test_c2_twelve_channels_relative_error_at_full_size(c2_run, prec, tol):
     """lambda and the twelve moments of cubic, w2, w4 and w6 on the 10 000 subset rows of the 2^20-row launch against
     the float64 oracle: the per-channel relative error (floor 1e-3 in natural units) within `tol` for every channel

@@ -3,6 +3,7 @@
 Tolerances (outputs in units of the support h, where every channel is O(1)):
   float64 routes (fused, plain)   <= 1e-10 absolute
   mixed route                     <= 1e-6 absolute (the target bound of the mixed-precision path)
+  float route                     <= 2e-5 absolute (float32 chord sums: a few ulp of each profile's scale)
 """
 import json
 from fractions import Fraction as F
@@ -21,6 +22,7 @@ pytestmark = pytest.mark.gpu
 KERNELS = ["cubic", "w2", "w4", "w6", "quartic", "quintic", "poly6", "cone", "lw2", "lw4"]
 TOL64 = 1e-10
 TOL_MIXED = 1e-6
+TOL_FP32 = 2e-5
 
 
 @pytest.fixture(scope="module")
@@ -90,6 +92,19 @@ def test_mixed_route_within_1e6(c2s, kernel):
     ref = oracle_outputs(loops, X, h, kernel, h)
     err = scaled_errors(got, ref, h)
     assert max(err.values()) < TOL_MIXED, err
+
+
+@pytest.mark.parametrize("kernel", ["cubic", "w2", "w4", "w6", "quartic", "quintic", "poly6", "cone", "lw2", "lw4"])
+def test_fp32_route_within_tolerance(c2s, kernel):
+    """the float route (Chebyshev profiles and graded Gauss-Legendre chord quadrature in float32, float64 clip, edge
+    frame and row sums) against the oracle, near-tangent and on-vertex rows included."""
+    loops, X, h = c2s
+    scene, rep, body = make_scene(loops)
+    got = gpu_outputs(scene, X, h, kernel, h, precision="fp32")
+    ref = oracle_outputs(loops, X, h, kernel, h)
+    err = scaled_errors(got, ref, h)
+    print(f"fp32 {kernel}: " + ", ".join(f"{k} {v:.1e}" for k, v in err.items()))
+    assert max(err.values()) < TOL_FP32, err
 
 
 @pytest.mark.parametrize("kernel", ["cubic", "w2", "w4", "w6"])

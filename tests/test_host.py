@@ -207,3 +207,25 @@ def test_pair_weights_host_checks():
     assert L.wsb_pair_weights(1, None, None, 4, None, None, -1, None, 3, None, 1, None, None, None, None) == \
         _lib.WSB_ERR_ARG
     assert L.wsb_pair_weights(1, None, None, 0, None, None, 1, None, 3, None, 1, None, None, None, None) == _lib.WSB_OK
+
+
+def test_scene_and_server_argument_checks():
+    """the scene and server entry points refuse NULL handles and out-of-range arguments before touching a device."""
+    import ctypes
+    from warpsphboundaries_b200 import _lib
+    L = _lib.lib
+    assert L.wsb_scene_create(0, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_scene_add_body(None, None, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_scene_add_surface(None, 0, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_scene_info(None, None, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_scene_workspace_size(None, 10) == 0
+    assert L.wsb_scene_destroy(None) == _lib.WSB_OK
+    out = ctypes.c_void_p()
+    assert L.wsb_server_create(0, 0, 1024, 1 << 20, ctypes.byref(out)) == _lib.WSB_ERR_ARG      # no streams
+    assert L.wsb_server_create(0, 2, 0, 1 << 20, ctypes.byref(out)) == _lib.WSB_ERR_ARG         # no rows
+    assert L.wsb_server_create(0, 2, 1024, 1 << 20, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_serve_poll(None, 0, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_serve_wait(None, 1) == _lib.WSB_ERR_ARG
+    assert L.wsb_serve_release(None, 1) == _lib.WSB_ERR_ARG
+    assert L.wsb_server_stats(None, None, None, None, None) == _lib.WSB_ERR_ARG
+    assert L.wsb_server_destroy(None) == _lib.WSB_OK

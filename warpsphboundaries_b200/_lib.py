@@ -25,7 +25,10 @@ EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_d
            "wsb_mesh_workspace_size", "wsb_mesh_inside", "wsb_mesh_channels", "wsb_triangle_channels",
            "wsb_triangle_combine", "wsb_disks_create", "wsb_disks_destroy", "wsb_disk_workspace_size",
            "wsb_disk_aggregate", "wsb_disk_cone_area", "wsb_disk_dir_extreme", "wsb_pair_weights",
-           "wsb_pair_channels"]
+           "wsb_pair_channels", "wsb_scene_create", "wsb_scene_destroy", "wsb_scene_add_body", "wsb_scene_add_surface",
+           "wsb_scene_set_pose", "wsb_scene_info", "wsb_scene_workspace_size", "wsb_scene_aggregate",
+           "wsb_server_create", "wsb_server_destroy", "wsb_serve_submit", "wsb_serve_poll", "wsb_serve_wait",
+           "wsb_serve_release", "wsb_server_stats"]
 
 
 class SurfaceInfo(ctypes.Structure):
@@ -84,6 +87,23 @@ def _load():
         "wsb_disk_dir_extreme": (c_int, [P, P, P, P, c_int64, P, P, P, P]),
         "wsb_pair_channels": (c_int, [P, c_int, c_int, P, P, c_int64, P, P, c_int64, P, P, P]),
         "wsb_pair_weights": (c_int, [c_int, P, P, c_int64, P, P, c_int64, P, c_int64, P, c_int64, P, P, P, P]),
+        "wsb_scene_create": (c_int, [c_int, POINTER(c_void_p)]),
+        "wsb_scene_destroy": (c_int, [P]),
+        "wsb_scene_add_body": (c_int, [P, D, POINTER(c_int)]),
+        "wsb_scene_add_surface": (c_int, [P, c_int, P]),
+        "wsb_scene_set_pose": (c_int, [P, c_int, D, P]),
+        "wsb_scene_info": (c_int, [P, POINTER(c_int), POINTER(c_int)]),
+        "wsb_scene_workspace_size": (c_size_t, [P, c_int64]),
+        "wsb_scene_aggregate": (c_int, [P, c_int, I32P, c_int, P, P, P, c_int64, c_int64, PP, PP, PP, PP, PP, P,
+                                        c_size_t, P]),
+        "wsb_server_create": (c_int, [c_int, c_int, c_int64, c_size_t, POINTER(c_void_p)]),
+        "wsb_server_destroy": (c_int, [P]),
+        "wsb_serve_submit": (c_int, [P, P, c_int, c_int, c_int, P, P, c_int64, P, P, P, P, P, P, P,
+                                     POINTER(c_int64)]),
+        "wsb_serve_poll": (c_int, [P, c_int64, POINTER(c_int)]),
+        "wsb_serve_wait": (c_int, [P, c_int64]),
+        "wsb_serve_release": (c_int, [P, c_int64]),
+        "wsb_server_stats": (c_int, [P, POINTER(c_int64), D, D, POINTER(c_size_t)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -19,7 +19,7 @@ from .scene import _stream
 from .shim import kernelName
 
 F64 = torch.float64
-_PREC = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+_PREC = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "fp32": _lib.PREC_FP32}
 
 
 class BoundaryMoments(torch.autograd.Function):

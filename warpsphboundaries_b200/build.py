@@ -14,7 +14,8 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_build"
 LIB = OUT_DIR / "libwsb.so"
-SOURCES = ["surface.cu", "topology.cu", "fused.cu", "radial.cu", "mesh.cu", "triangle.cu", "disk.cu", "fem.cu"]
+SOURCES = ["surface.cu", "topology.cu", "fused.cu", "radial.cu", "mesh.cu", "triangle.cu", "disk.cu", "fem.cu",
+           "serve.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -259,20 +259,24 @@ __device__ __forceinline__ bool pair_geo_row(double px, double py, double h, dou
   return pair_geo(p0, p1, q0, q1, g);
 }
 
-// asinh(hi/|z|) - asinh(lo/|z|) as one logarithm of positive factors (no cancellation of a + sqrt(a^2 + 1) for a < 0)
+// asinh(hi/|z|) - asinh(lo/|z|) as one logarithm of positive factors (no cancellation of a + sqrt(a^2 + 1) for a < 0):
+// the chord on the far side of the foot (lo >= 0), on the near side (hi <= 0), or across it; the factors are selected
+// and one logarithm taken, so a warp whose lanes fall in different cases still evaluates a single log
 template <typename T>
 __device__ __forceinline__ T asinh_diff(T lo, T hi, T rlo, T rhi, T zz) {
-  if (lo >= T(0)) return log((hi + rhi) / (lo + rlo));
-  if (hi <= T(0)) return log((rlo - lo) / (rhi - hi));
-  return log((hi + rhi) * (rlo - lo) / zz);
+  const bool far = lo >= T(0), near = hi <= T(0);
+  const T num = far ? hi + rhi : (near ? rlo - lo : (hi + rhi) * (rlo - lo));
+  const T den = far ? lo + rlo : (near ? rhi - hi : zz);
+  return log(num / den);
 }
 
 // The MIXED route evaluates the chord angle in float.  The angle enters every channel only through M(R) * angle and
-// MPsi(R) * angle with |M(R)| <= 1/2, so float rounding (<= 2.4e-7 absolute for |angle| <= pi) moves lam by < 4e-8.
+// MPsi(R) * angle with |M(R)| <= 1/2, so float rounding (<= 2.4e-7 absolute for |angle| <= pi) moves lam by < 1.2e-7.
 // The logarithm stays in double: its coefficient in the monomial sums reaches 1.7e3 (w6 gradient profile at |z| -> 1),
-// which would amplify float rounding to 1e-4.  Near the foot point (|z| < kMixedGuardZ) the angle is kept in double so
-// its jump across z = 0 stays consistent with the float64 winding indicator.
-constexpr double kMixedGuardZ = 1.0 / 64.0;
+// which would amplify float rounding to 1e-4.  The float angle keeps the sign of y = z (hi - lo), so its jump across
+// z = 0 agrees with the float64 winding indicator; only where y would leave float's normal range (|y| < 2^-100) is
+// the angle taken in double.
+constexpr double kMixedGuardY = 0x1p-100;
 
 template <int PREC>
 __device__ __forceinline__ void special_fns(double lo, double hi, double rlo, double rhi, double z, double zz,
@@ -282,7 +286,7 @@ __device__ __forceinline__ void special_fns(double lo, double hi, double rlo, do
   if (z == 0.0) return;
   const double y = z * (hi - lo), x = zz + lo * hi;
   dasinh = asinh_diff<double>(lo, hi, rlo, rhi, zz);
-  if (PREC == WSB_PREC_MIXED && fabs(z) >= kMixedGuardZ) {
+  if (PREC == WSB_PREC_MIXED && fabs(y) >= kMixedGuardY) {
     dang = (double)atan2f((float)y, (float)x);
     return;
   }

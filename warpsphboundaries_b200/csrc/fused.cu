@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdlib>
+#include <atomic>
 #include <mutex>
 #include <tuple>
 
@@ -163,6 +164,17 @@ __device__ __forceinline__ WorkRec load_workrec(const WorkRec* p) {
   r.ke = __ldg(reinterpret_cast<const int32_t*>(p) + 12);
   return r;
 }
+
+// an asynchronous copy of a 32-byte record into shared memory (two 16-byte cp.async, L1-allocating) and the waits on it:
+// the copy is in flight while the thread computes, without holding registers
+__device__ __forceinline__ void cp_async_rec(double4* dst, const double4* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d + 16), "l"(reinterpret_cast<const char*>(src) + 16)
+               : "memory");
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // a 32-byte record through the read-only data path (two 16-byte loads)
 __device__ __forceinline__ double4 ldg4(const double4* p) {
@@ -327,7 +339,7 @@ struct PackOut {
 // memory (12 KiB a kernel per CTA), at most 7 CTAs (measured on B200 with one kernel on the 2^20-particle scene:
 // 12.2e9 pairs/s with 7 CTAs at 72 registers, 12.0e9 with 6 or 8, 11.6e9 with the sums in registers at 6 CTAs)
 constexpr int pack_min_blocks(int n) {
-  const int by_smem = (227 * 1024) / (12 * n * kThreads * 8 + 1024);
+  const int by_smem = (227 * 1024) / (12 * n * kThreads * 8 + 32 * kThreads + 1024);
   return by_smem < 7 ? by_smem : 7;
 }
 
@@ -374,6 +386,123 @@ __device__ __forceinline__ void pack_pair(const PairGeo& g, double* acc_t) {
       pack_blocks_at<Pack, D, 0, 0>(g, lo, hi, A, rlo, rhi, dang, acc_t);
     }
     pack_pair<Pack, PREC, D + 1>(g, acc_t);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------ the float route
+// WSB_PREC_FP32: per (pair, support radius) the chord is clipped in float64 and its angle taken in float (float64 only
+// where y leaves float's normal range); the four integrated profiles (P, Psi, M/r^2, MPsi/r^2) of every (kernel, block)
+// at that radius are evaluated in float by Clenshaw's recurrence on their Chebyshev series on [0, R] and integrated by
+// 8-node Gauss-Legendre on panels graded from the foot of the perpendicular -- 0, |z|, 2|z|, 4|z|, ... up to the
+// chord end, the reference's stable route (src/warpSPHBoundaries/edge/warpbc.py:519-575) without its cap on the
+// panel count -- the node radius shared by every block of the pack; the odd chord sums come from the potentials M,
+// MPsi at the chord ends; the edge-frame combination and the row sums stay in float64.  The tensile (quadrature)
+// kernels keep their float64 chord quadrature.  Float slot of (kernel K, block B): K * kF32MaxBlocks + B.
+constexpr int kF32MaxBlocks = 3;
+
+template <class Pack, int D, int K, int B>
+__device__ __forceinline__ void f32_node(float x, float w, float* q) {
+  if constexpr (K < Pack::kN) {
+    using KT = typename Pack::template Kern<K>;
+    if constexpr (B < KT::kBlocks) {
+      if constexpr (!KT::kQuad && KT::kR[B] == Pack::kRadii.r[D]) {
+        static_assert(B < kF32MaxBlocks, "blocks per kernel");
+        constexpr int o = 4 * (K * kF32MaxBlocks + B);
+        float P, Psi, Fl, Fp;
+        ChebOf<KT>::template integrands<B>(x, P, Psi, Fl, Fp);
+        q[o] = fmaf(w, P, q[o]);
+        q[o + 1] = fmaf(w, Psi, q[o + 1]);
+        q[o + 2] = fmaf(w, Fl, q[o + 2]);
+        q[o + 3] = fmaf(w, Fp, q[o + 3]);
+      }
+      f32_node<Pack, D, K, B + 1>(x, w, q);
+    } else {
+      f32_node<Pack, D, K + 1, 0>(x, w, q);
+    }
+  }
+}
+
+template <class Pack, int D, int K, int B>
+__device__ __forceinline__ void f32_finish(const PairGeo& g, const float* q, double lo, double hi, double rlo,
+                                           double rhi, double dang, double* acc_t) {
+  if constexpr (K < Pack::kN) {
+    using KT = typename Pack::template Kern<K>;
+    if constexpr (B < KT::kBlocks) {
+      if constexpr (KT::kR[B] == Pack::kRadii.r[D]) {
+        const SmemAcc a{acc_t + K * 12 * kThreads};
+        if constexpr (KT::kQuad) {
+          const double W0 = quad_chord<KT>(lo, hi, g.z);
+          a[3] -= g.n0 * W0;
+          a[4] -= g.n1 * W0;
+        } else {
+          constexpr int o = 4 * (K * kF32MaxBlocks + B);
+          constexpr float s2R = (float)(2.0 / KT::kR[B]);
+          float Mh, MPh, Ml, MPl;
+          ChebOf<KT>::template potentials<B>(fminf(fmaf((float)rhi, s2R, -1.0f), 1.0f), Mh, MPh);
+          ChebOf<KT>::template potentials<B>(fminf(fmaf((float)rlo, s2R, -1.0f), 1.0f), Ml, MPl);
+          BlockSums S;
+          S.W0 = (double)q[o];
+          S.P0 = (double)q[o + 1];
+          S.Lreg = (double)q[o + 2];
+          S.Preg = (double)q[o + 3];
+          S.W1 = (double)Mh - (double)Ml;
+          S.P1 = (double)MPh - (double)MPl;
+          S.Mhat = ChebOf<KT>::kMhat[B];
+          S.MPhat = ChebOf<KT>::kMPhat[B];
+          add_block(g, S, dang, a);
+        }
+      }
+      f32_finish<Pack, D, K, B + 1>(g, q, lo, hi, rlo, rhi, dang, acc_t);
+    } else {
+      f32_finish<Pack, D, K + 1, 0>(g, q, lo, hi, rlo, rhi, dang, acc_t);
+    }
+  }
+}
+
+template <class Pack, int D>
+__device__ __forceinline__ void pack_pair_f32(const PairGeo& g, double* acc_t) {
+  if constexpr (D < Pack::kRadii.n) {
+    constexpr double R = Pack::kRadii.r[D];
+    double lo, hi, rlo, rhi, zz;
+    if (clip_chord(g, R, lo, hi, rlo, rhi, zz)) {
+      double dang = 0.0;
+      if (g.z != 0.0) {
+        const double y = g.z * (hi - lo), x = zz + lo * hi;
+        dang = fabs(y) >= kMixedGuardY ? (double)atan2f((float)y, (float)x)
+                                       : ((y == 0.0 && x == 0.0) ? 0.0 : atan2(y, x));
+      }
+      constexpr int kSlots = 4 * Pack::kN * kF32MaxBlocks;
+      float q[kSlots];
+#pragma unroll
+      for (int i = 0; i < kSlots; ++i) q[i] = 0.0f;
+      const float az = (float)fabs(g.z), zzf = az * az;
+      constexpr float s2R = (float)(2.0 / R);
+      for (int side = 0; side < 2; ++side) {
+        const float u0 = (float)(side == 0 ? fmax(-hi, 0.0) : fmax(lo, 0.0));
+        const float u1 = (float)(side == 0 ? -lo : hi);
+        if (!(u1 > u0)) continue;
+        // panels [0, |z|], [|z|, 2|z|], ... (the first breakpoint at least 2^-30 of the side's length: nearer the foot
+        // the integrand differs from its z = 0 polynomial by O(z^2)); z = 0 integrates a polynomial in s: one panel
+        float d = az > 0.0f ? fmaxf(az, u1 * 0x1p-30f) : u1;
+        for (int it = 0; it < 40 && d <= u0; ++it) d *= 2.0f;
+        float u = u0;
+        for (int it = 0; it < 40 && u < u1; ++it) {
+          const float nxt = fminf(u1, d);
+          const float hc = 0.5f * (nxt - u), mc = 0.5f * (nxt + u);
+#pragma unroll
+          for (int k = 0; k < kF32Gauss; ++k) {
+            const float s = fmaf(hc, kF32Gx[k], mc);
+            const float r = sqrtf(fmaf(s, s, zzf));
+            const float x = fminf(fmaf(r, s2R, -1.0f), 1.0f);
+            f32_node<Pack, D, 0, 0>(x, hc * kF32Gw[k], q);
+          }
+          if (nxt >= d) d *= 2.0f;
+          u = nxt;
+        }
+      }
+      f32_finish<Pack, D, 0, 0>(g, q, lo, hi, rlo, rhi, dang, acc_t);
+    }
+    pack_pair_f32<Pack, D + 1>(g, acc_t);
   }
 }
 
@@ -465,7 +594,10 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
                                                              const PackOut out) {
   static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "lanes per row");
   static_assert(Pack::kN >= 1 && Pack::kN <= kMaxPack, "pack size");
-  __shared__ double s_acc[Pack::kN * 12 * kThreads];
+  // dynamic shared memory: the channel sums [kernel][channel][thread], then each thread's next edge record
+  extern __shared__ double4 s_dyn[];
+  double* const s_acc = reinterpret_cast<double*>(s_dyn + kThreads);
+  double4* const s_next = s_dyn;
   const int64_t nwork = *nwork_p;
   const int64_t wblocks = (nwork + kThreads / G - 1) / (kThreads / G);
   if ((int64_t)blockIdx.x >= wblocks) {                             // a tail block: constant rows
@@ -503,27 +635,33 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
   double* const acc_t = s_acc + threadIdx.x;
 #pragma unroll
   for (int c = 0; c < Pack::kN * 12; ++c) acc_t[c * kThreads] = 0.0;
-  // the next neighbour's (or tail candidate's) record is loaded one step ahead, so its latency hides behind the
-  // current pair's closed form
+  // the next neighbour's (or tail candidate's) record is copied into the thread's shared-memory slot one step ahead
+  // (cp.async), so its latency hides behind the current pair's closed form
   const double4 zero = make_double4(0.0, 0.0, 0.0, 0.0);
-  double4 nxt = nb >= 0 ? ldg4(S.crec + kb + nb) : (kt < e1 ? ldg4(S.crec + kt) : zero);
+  double4* const slot = s_next + threadIdx.x;
+  if (nb >= 0)
+    cp_async_rec(slot, S.crec + kb + nb);
+  else if (kt < e1)
+    cp_async_rec(slot, S.crec + kt);
   while (__any_sync(0xffffffffu, nb >= 0 || kt < e1)) {
     double4 e = zero;
     bool have = false;
     if (nb >= 0) {
-      e = nxt;
+      cp_async_wait_all();
+      e = *slot;
       have = true;
       for (int s = 1; s < G; ++s) pop_bit(mk0, mk1);
       nb = pop_bit(mk0, mk1);
       if (nb >= 0)
-        nxt = ldg4(S.crec + kb + nb);
+        cp_async_rec(slot, S.crec + kb + nb);
       else if (kt < e1)
-        nxt = ldg4(S.crec + kt);
+        cp_async_rec(slot, S.crec + kt);
     } else {
       while (kt < e1) {
-        e = nxt;
+        cp_async_wait_all();
+        e = *slot;
         kt += G;
-        if (kt < e1) nxt = ldg4(S.crec + kt);
+        if (kt < e1) cp_async_rec(slot, S.crec + kt);
         if (seg_within_fast(lx, ly, e.x, e.y, e.z, e.w, h)) {
           have = true;
           break;
@@ -533,7 +671,12 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
     __syncwarp();
     if (have) {
       PairGeo g;
-      if (pair_geo_row(lx, ly, h, ih, e, g)) pack_pair<Pack, PREC, 0>(g, acc_t);
+      if (pair_geo_row(lx, ly, h, ih, e, g)) {
+        if constexpr (PREC == WSB_PREC_FP32)
+          pack_pair_f32<Pack, 0>(g, acc_t);
+        else
+          pack_pair<Pack, PREC, 0>(g, acc_t);
+      }
     }
   }
   const bool write = ok && sub == 0;
@@ -543,13 +686,30 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
 // the pair kernel of a pack over a prepared workspace (two lanes per work row: measured fastest on the 2^20-particle
 // scene, 1 / 2 lanes give 10.4 / 11.3e9 pairs/s with one kernel, 1 / 2 / 4 lanes 0.448 / 0.421 / 0.471 ms for the
 // four-kernel pack, which also beat the four kernels as two two-kernel packs, 0.426 ms)
+template <class Pack>
+constexpr size_t pack_smem_bytes() {
+  return sizeof(double4) * kThreads + sizeof(double) * Pack::kN * 12 * kThreads;
+}
+
 template <class Pack, int PREC>
-static void launch_pack(const SurfView& v, const double* sup, const Workspace& w, int64_t n, const double* pose,
-                        bool assign, const PackOut& out, cudaStream_t st) {
+static int launch_pack(const SurfView& v, const double* sup, const Workspace& w, int64_t n, const double* pose,
+                       bool assign, const PackOut& out, cudaStream_t st) {
   constexpr int G = 2;
+  constexpr size_t smem = pack_smem_bytes<Pack>();
+  auto kern = k_agg_pairs<Pack, PREC, G, pack_min_blocks(Pack::kN)>;
+  if (smem > 48 * 1024) {       // above the default limit: opt in once per device for this instantiation
+    static std::atomic<uint64_t> opted{0};
+    int dev = 0;
+    WSB_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = 1ull << (dev & 63);
+    if (!(opted.load() & bit)) {
+      WSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      opted.fetch_or(bit);
+    }
+  }
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads + (n + kThreads - 1) / kThreads);
-  k_agg_pairs<Pack, PREC, G, pack_min_blocks(Pack::kN)><<<grid, kThreads, 0, st>>>(v, sup, w.wrec, w.nwork, n, w.ind,
-                                                                                  w.flag, pose, assign, out);
+  kern<<<grid, kThreads, smem, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, out);
+  return WSB_OK;
 }
 
 // ------------------------------------------------------------------------------------------------ adjoint
@@ -1134,7 +1294,7 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   const Surface* s = reinterpret_cast<const Surface*>(s_);
   if (!s) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: NULL surface");
   if (!aggregate_kernel_ok(kernel)) return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate: unknown kernel id");
-  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED && precision != WSB_PREC_FP32)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate: unknown precision mode");
   if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: row count out of range");
   if (n == 0) return WSB_OK;
@@ -1158,11 +1318,9 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   o.m2[0] = M2;
   auto launch1 = [&](auto kt) {
     using P1 = KPack<decltype(kt)>;
-    if (precision == WSB_PREC_MIXED)
-      launch_pack<P1, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
-    else
-      launch_pack<P1, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
-    return 0;
+    if (precision == WSB_PREC_MIXED) return launch_pack<P1, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
+    if (precision == WSB_PREC_FP32) return launch_pack<P1, WSB_PREC_FP32>(v, sup, w, n, pose, assign, o, st);
+    return launch_pack<P1, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
   };
   int rc = 0;
   if (kernel == Kern_w2p5::kId)
@@ -1214,7 +1372,7 @@ extern "C" int wsb_aggregate_evaluate_groups(const wsb_surface* s_, int n_groups
   for (int g = 0; g < n_groups; ++g)
     if (!aggregate_kernel_ok(kernels[g]))
       return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate_groups: unknown kernel id");
-  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED && precision != WSB_PREC_FP32)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_evaluate_groups: unknown precision mode");
   if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate_groups: row count out of range");
   if (n == 0) return WSB_OK;
@@ -1256,19 +1414,20 @@ extern "C" int wsb_aggregate_evaluate_groups(const wsb_surface* s_, int n_groups
   }
   auto run = [&](auto pack) {
     using P = decltype(pack);
-    if (precision == WSB_PREC_MIXED)
-      launch_pack<P, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
-    else
-      launch_pack<P, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
+    if (precision == WSB_PREC_MIXED) return launch_pack<P, WSB_PREC_MIXED>(v, sup, w, n, pose, assign, o, st);
+    if (precision == WSB_PREC_FP32) return launch_pack<P, WSB_PREC_FP32>(v, sup, w, n, pose, assign, o, st);
+    return launch_pack<P, WSB_PREC_FP64>(v, sup, w, n, pose, assign, o, st);
   };
+  int rc;
   switch (which) {
-    case 0: run(KPack<Kern_cubic, Kern_w2, Kern_w4, Kern_w6>{}); break;
-    case 1: run(KPack<Kern_w2, Kern_w4, Kern_w6>{}); break;
-    case 2: run(KPack<Kern_w2, Kern_cone, Kern_lw2>{}); break;
-    case 3: run(KPack<Kern_w4, Kern_cone, Kern_lw4>{}); break;
-    case 4: run(KPack<Kern_w2, Kern_cone>{}); break;
-    default: run(KPack<Kern_w4, Kern_cone>{}); break;
+    case 0: rc = run(KPack<Kern_cubic, Kern_w2, Kern_w4, Kern_w6>{}); break;
+    case 1: rc = run(KPack<Kern_w2, Kern_w4, Kern_w6>{}); break;
+    case 2: rc = run(KPack<Kern_w2, Kern_cone, Kern_lw2>{}); break;
+    case 3: rc = run(KPack<Kern_w4, Kern_cone, Kern_lw4>{}); break;
+    case 4: rc = run(KPack<Kern_w2, Kern_cone>{}); break;
+    default: rc = run(KPack<Kern_w4, Kern_cone>{}); break;
   }
+  if (rc) return rc;
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }
@@ -1280,7 +1439,7 @@ extern "C" int wsb_aggregate(const wsb_surface* s_, int kernel, int precision, c
   const Surface* s = reinterpret_cast<const Surface*>(s_);
   int rc = check_common(s, kernel, pos, sup, n, pose, obb, "wsb_aggregate");
   if (rc) return rc;
-  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED && precision != WSB_PREC_FP32)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate: unknown precision mode");
   if (n == 0) return WSB_OK;
   if (status) {
@@ -1306,7 +1465,7 @@ extern "C" int wsb_aggregate_groups(const wsb_surface* s_, int n_groups, const i
   for (int g = 0; g < n_groups; ++g)
     if (!aggregate_kernel_ok(kernels[g]))
       return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_groups: unknown kernel id");
-  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED)
+  if (precision != WSB_PREC_FP64 && precision != WSB_PREC_MIXED && precision != WSB_PREC_FP32)
     return fail(WSB_ERR_UNSUPPORTED, "wsb_aggregate_groups: unknown precision mode");
   if (n == 0) return WSB_OK;
   rc = wsb_aggregate_prepare(s_, pos, sup, allowed, n, pose, obb, unbounded, workspace, workspace_bytes, stream);

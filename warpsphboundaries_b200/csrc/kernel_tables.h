@@ -740,6 +740,1120 @@ struct Kern_w4p5 {
   }
 };
 
+// ---- float Chebyshev tables of the block profiles on [0, R] (x = 2 r / R - 1), Clenshaw in float
+constexpr int kF32Gauss = 8;   // Gauss-Legendre nodes per panel of the float route
+static __device__ const float kF32Gx[kF32Gauss] = {-0.9602898564975362f, -0.7966664774136267f, -0.525532409916329f, -0.18343464249564978f, 0.18343464249564978f, 0.525532409916329f, 0.7966664774136267f, 0.9602898564975362f};
+static __device__ const float kF32Gw[kF32Gauss] = {0.10122853629037706f, 0.22238103445337443f, 0.3137066458778869f, 0.36268378337836166f, 0.36268378337836166f, 0.3137066458778869f, 0.22238103445337443f, 0.10122853629037706f};
+template <class KT> struct ChebOf;   // the float tables of an exact kernel
+struct Cheb_cubic {
+  static constexpr double kMhat[] = {0.5714285714285714, -0.07142857142857142};
+  static constexpr double kMPhat[] = {-0.04081632653061224, 0.0012755102040816326};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_cubic> : Cheb_cubic {};
+template <> __device__ __forceinline__ void Cheb_cubic::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.35714285714285715f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.142857142857143f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.357142857142857f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 3.5714285714285716f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.004464285714285714f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.022321428571428572f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.022321428571428572f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.08928571428571429f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.3125f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.21875f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.07142857142857142f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.6428571428571429f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.5f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 2.5f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0006377551020408163f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0047831632653061226f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.010841836734693877f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.01403061224489796f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.13392857142857142f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.15401785714285715f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_cubic::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.004464285714285714f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.022321428571428572f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.022321428571428572f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.08928571428571429f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.3125f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.35267857142857145f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -3.985969387755102e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00013950892857142856f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00027901785714285713f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.001953125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001953125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.006556919642857143f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.022600446428571428f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.025151466836734693f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_cubic::integrands<1>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.17857142857142858f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.0714285714285714f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.6785714285714284f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, -1.7857142857142858f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0005580357142857143f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0027901785714285715f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0027901785714285715f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.011160714285714286f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0390625f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, 0.02734375f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.03571428571428571f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.32142857142857145f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.25f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, -1.25f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 7.971938775510203e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0005978954081632653f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0013552295918367347f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001753826530612245f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.016741071428571428f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, 0.019252232142857144f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_cubic::potentials<1>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0005580357142857143f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0027901785714285715f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0027901785714285715f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.011160714285714286f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0390625f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, -0.04408482142857143f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.2456154336734693e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.359654017857143e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.719308035714285e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 6.103515625e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.103515625e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00020490373883928572f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0007062639508928571f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, 0.0007859833386479591f - b2);
+  }
+}
+struct Cheb_w2 {
+  static constexpr double kMhat[] = {0.5};
+  static constexpr double kMPhat[] = {-0.034722222222222224};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_w2> : Cheb_w2 {};
+template <> __device__ __forceinline__ void Cheb_w2::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0546875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.2734375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.2734375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.09375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -3.828125f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 2.6796875f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.00048828125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.001708984375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00341796875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.02392578125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.02392578125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.080322265625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.27685546875f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.19189453125f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0078125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.05859375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.1328125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.171875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.640625f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 1.88671875f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 5.425347222222222e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0003085666232638889f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.781684027777778e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.004591200086805556f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.011406792534722222f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.011247422960069444f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.11905924479166667f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.13539632161458334f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_w2::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.00048828125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.001708984375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00341796875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.02392578125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.02392578125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.080322265625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.27685546875f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.30810546875f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 3.3908420138888887e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.7220458984375e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.103515625e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0001678466796875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.000335693359375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00186920166015625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001495361328125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0060577392578125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.019134521484375f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.021711773342556424f - b2);
+  }
+}
+struct Cheb_w4 {
+  static constexpr double kMhat[] = {0.5};
+  static constexpr double kMPhat[] = {-0.026515151515151516};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_w4> : Cheb_w4 {};
+template <> __device__ __forceinline__ void Cheb_w4::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.003204345703125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.01904296875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.015380859375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.15380859375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.4844970703125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.21533203125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.748291015625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.85009765625f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 3.217620849609375f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 2.002716064453125e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.7738037109375e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0001773834228515625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001590728759765625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0014791488647460938f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0095672607421875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.02899932861328125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0112152099609375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.10034751892089844f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.26927947998046875f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.1770153045654297f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0003204345703125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.002685546875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0059814453125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.016357421875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.11456298828125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.185791015625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.3367919921875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.199462890625f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 2.2714691162109375f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.6689300537109375e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.1010603471235795e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.2571161443536931e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00019729498660925663f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0005070440696947502f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0008657050855232008f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0068606174353397255f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.010787154688979641f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.019586288567745323f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.12320899963378906f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.12502527236938477f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_w4::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 2.002716064453125e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.7738037109375e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0001773834228515625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001590728759765625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0014791488647460938f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0095672607421875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.02899932861328125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0112152099609375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.10034751892089844f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.26927947998046875f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.3229846954345703f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.043081283569336e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.7093020352450286e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.205371856689453e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 8.304913838704428e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.4513731002807617e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00010788440704345703f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 7.146596908569336e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0006018877029418945f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0015963166952133179f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00041985511779785156f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.005561232566833496f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.014179468154907227f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.017306370265556103f - b2);
+  }
+}
+struct Cheb_w6 {
+  static constexpr double kMhat[] = {0.5};
+  static constexpr double kMPhat[] = {-0.02142857142857143};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_w6> : Cheb_w6 {};
+template <> __device__ __forceinline__ void Cheb_w6::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.00017002650669642856f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0011689322335379465f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0009351457868303571f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.013559613909040178f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.04395185198102679f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.007714952741350446f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.30859810965401785f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.6452505929129464f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.022443498883928572f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.4627064296177457f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.859623500279018f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 3.7492970057896207f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 8.174351283482142e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.317079271589007e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -7.96999250139509e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 9.431157793317522e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0001018387930733817f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.000752500125340053f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0023670877729143414f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0004821845463344029f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.015108449118477958f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.029658002512795583f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0009935923985072545f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.11313404355730329f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.26185676029750277f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.16634363787514822f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.3078962053571428e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00012138911655970983f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0002795628138950893f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0010667528424944197f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.007101331438337054f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.008967944553920202f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.04006304059709821f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.17900630405970983f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.20514133998325892f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.5587803976876395f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.7741099766322543f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 2.6460268838065013f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 5.4495675223214284e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.0956905909946984e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 3.4059797014508927e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 8.497919355119978e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.4012156895228793e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.825762340000697e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0003787926265171596f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0004723582948957171f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.001957314355032785f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.008439732449395316f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.009108775002615793f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.026254715238298688f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.12499693461826869f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.11738677535738264f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_w6::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 8.174351283482142e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.317079271589007e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -7.96999250139509e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 9.431157793317522e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0001018387930733817f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.000752500125340053f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0023670877729143414f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0004821845463344029f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.015108449118477958f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.029658002512795583f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0009935923985072545f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.11313404355730329f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.26185676029750277f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.3336563621248518f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 3.4059797014508928e-09f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.1974147387913296e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -7.98276492527553e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 3.9967043059212823e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 5.37506171635219e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.849504045077733e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 4.732183047703334e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 4.160723515919277e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.000111939651625497f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.729761609009334e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0007122267569814409f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0012720647667135512f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00017956005675452097f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.004980658047965595f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.011140206030436925f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.014411726806844985f - b2);
+  }
+}
+struct Cheb_quartic {
+  static constexpr double kMhat[] = {0.6515846538782318, -0.15200166805671392, 0.0004170141784820684};
+  static constexpr double kMPhat[] = {-0.03490632074347671, 0.0029314607410937687, -8.936018110330037e-07};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_quartic> : Cheb_quartic {};
+template <> __device__ __forceinline__ void Cheb_quartic::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.1527151532527106f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.2217212260216848f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 4.276024291075896f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.552048582151793f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 5.345030363844871f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.001590782846382402f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.011453636493953295f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.028634091234883235f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.006363131385529608f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.12885341055697455f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.34360909481859886f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.227163790463407f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.025452525542118434f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.28506828607172646f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.445703450792327f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.276024291075896f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 3.7415212546914094f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.00019884785579780026f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0019771158233609855f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.007669845866486581f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.010067382870677202f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.028105724075191938f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.1574875017918578f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.16011229348838876f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quartic::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.001590782846382402f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.011453636493953295f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.028634091234883235f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.006363131385529608f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.12885341055697455f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.34360909481859886f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.4244208634148249f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.2427990987362516e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -7.385777501061152e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 5.9654356739340076e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0005965435673934008f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0018791122372892124f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0008351609943507611f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.006780711882704988f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.018811007158471903f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.022426842364880833f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quartic::integrands<1>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.09895941930775647f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.7916753544620517f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.7708637406171808f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 5.5417274812343615f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, -3.4635796757714763f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.00037109782240408675f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0026719043213094245f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.006679760803273561f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001484391289616347f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.030058923614731024f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.08015712963928273f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, 0.05299276903930358f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.016493236551292745f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.18472424937447873f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.9368158361134279f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.7708637406171808f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, -2.4245057730400332f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -4.6387227800510844e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00046122157927365063f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0017892216437339896f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0023485190760715773f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.006556503312260775f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.03673868441800459f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, 0.03735099582497133f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quartic::potentials<1>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.00037109782240408675f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0026719043213094245f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.006679760803273561f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001484391289616347f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.030058923614731024f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.08015712963928273f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, -0.09900889901741035f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -1.043712625511494e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 6.202635031611164e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.009820602455171e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.009820602455171e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00015780934897733788f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -7.01374884343724e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0005694496084790711f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0015797634299741972f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, 0.0018834241632765842f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quartic::integrands<2>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0024434424520433694f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.019547539616346955f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.06841638865721435f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.1368327773144287f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 0.08552048582151793f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.0181010216847372e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -7.330327356130108e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.832581839032527e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.072404086738949e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.246618275646372e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00021990982068390325f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.00014538482589658048f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0004072404086738949f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.004561092577147623f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.02313125521267723f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.06841638865721435f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 0.059864340075062555f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.2726262771059216e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.2653541269510306e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 4.908701354551412e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.443125037233409e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.7987663408122842e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.000100792001146789f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.0001024718678325688f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quartic::potentials<2>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 1.0181010216847372e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -7.330327356130108e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.832581839032527e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.072404086738949e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.246618275646372e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00021990982068390325f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.0002716293525854879f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 3.181565692764804e-10f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.890759040271655e-09f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.5271515325271059e-09f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.5271515325271058e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.810527327460384e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.1380121455379483e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.735862241972477e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.815617832568808e-07f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -5.741271645409493e-07f - b2);
+  }
+}
+struct Cheb_quintic {
+  static constexpr double kMhat[] = {0.7625523012552301, -0.26778242677824265, 0.005230125523012552};
+  static constexpr double kMPhat[] = {-0.03177301255230126, 0.004958933829226716, -2.4213544088021077e-05};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_quintic> : Cheb_quintic {};
+template <> __device__ __forceinline__ void Cheb_quintic::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0625531184623431f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.6255311846234309f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.814890330805439f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 7.506374215481172f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -13.13615487709205f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 7.88169292625523f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0005585099862709205f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.005212759871861925f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.019547849519482217f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.03127655923117155f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.014335089647620293f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.17202107577144352f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.3870474204857479f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.24574439395920503f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.008936159780334728f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.11914879707112971f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.7357438219142259f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.764252092050209f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.880843030857741f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 5.5046744246861925f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -6.205666514121339e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.000760194147979864f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.003971626569037657f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.010456548076294456f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.007570913147228034f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.044696313067958945f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.1863561654190638f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.17304501074627354f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quintic::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0005585099862709205f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.005212759871861925f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.019547849519482217f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.03127655923117155f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.014335089647620293f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.17202107577144352f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.3870474204857479f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.5168079072960251f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -3.878541571325837e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 3.1997967963438155e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.144937299784257e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.981374828386506e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0008377649794063807f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.001710436832954694f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0069581035789585514f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.01663894334098784f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.02109635724183406f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quintic::integrands<1>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.04942468619246862f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.4942468619246862f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.224110878661088f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.930962343096234f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 10.37918410041841f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, -6.227510460251046f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0001961297071129707f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0018305439330543933f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.006864539748953975f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.010983263598326359f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.005033995815899582f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.06040794979079498f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.1359178870292887f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, 0.08629707112970711f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.007060669456066946f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.09414225941422594f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.5813284518828452f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.1841004184100417f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 5.436715481171548f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, -4.349372384937238f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 2.1792189679218967e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00026695432357043235f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001394700139470014f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.003671983960948396f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.002658647140864714f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.015695824616457462f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.06544194560669456f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, 0.06076752092050209f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quintic::potentials<1>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 0.0001961297071129707f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0018305439330543933f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.006864539748953975f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.010983263598326359f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.005033995815899582f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.06040794979079498f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.1359178870292887f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, -0.18148535564853557f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, 6.053386022005269e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.994043468154347e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.2712110646211065e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.0896094839609484e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0001307531380753138f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00026695432357043235f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0010859774523477453f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0025969026034402603f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, 0.003292587992019216f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quintic::integrands<2>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.003861303608786611f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.03861303608786611f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.1737586623953975f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.4633564330543933f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.8108737578451883f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 0.48652425470711297f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -3.830658342050209e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 3.575281119246862e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00013407304197175733f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0002145168671548117f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 9.83202307792887e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0011798427693514644f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.002654646231040795f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.001685489670502092f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0005516148012552301f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.007354864016736401f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.04541628530334728f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.17063284518828453f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.4247433969665272f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 0.33979471757322177f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -4.2562870467224547e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 5.213951632235007e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.724023709902371e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 7.171843673727336e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.192670197001395e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0003065590745401848f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0012781630001307532f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.0011868656429785565f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_quintic::potentials<2>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -3.830658342050209e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 3.575281119246862e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00013407304197175733f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0002145168671548117f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 9.83202307792887e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0011798427693514644f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.002654646231040795f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.00354463585251046f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -2.9557548935572604e-09f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 2.4384977871847395e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.207085276470246e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -5.320358808403068e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 6.384430570083682e-07f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.3034879080587518e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 5.302624279041725e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.2680188493360647e-05f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -1.6077089804781327e-05f - b2);
+  }
+}
+struct Cheb_poly6 {
+  static constexpr double kMhat[] = {0.5};
+  static constexpr double kMPhat[] = {-0.05};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_poly6> : Cheb_poly6 {};
+template <> __device__ __forceinline__ void Cheb_poly6::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.001953125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0234375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.03515625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.3203125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.158203125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.296875f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 1.87890625f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -1.52587890625e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.000244140625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0008544921875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.003173828125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.01324462890625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.039306640625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0450439453125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.286376953125f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.2173309326171875f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.000244140625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0029296875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00048828125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0712890625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.058349609375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.818359375f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 1.30908203125f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -1.52587890625e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.44140625e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -6.103515625e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0006103515625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001373291015625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0110595703125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00133056640625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.1104736328125f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.15264129638671875f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_poly6::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -1.52587890625e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.000244140625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0008544921875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.003173828125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.01324462890625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.039306640625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0450439453125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.286376953125f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.2826690673828125f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -9.5367431640625e-08f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.9073486328125e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -1.049041748046875e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.33514404296875e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00020933151245117188f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.00013580322265625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.002017974853515625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00347137451171875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.006358146667480469f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.028347015380859375f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.029538917541503906f - b2);
+  }
+}
+struct Cheb_cone {
+  static constexpr double kMhat[] = {0.5};
+  static constexpr double kMPhat[] = {-0.075};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_cone> : Cheb_cone {};
+template <> __device__ __forceinline__ void Cheb_cone::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -1.5f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 1.5f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.03125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.28125f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.25f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.5f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 1.0f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.00625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.009375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.09375f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.171875f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_cone::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.03125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.28125f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.25f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.000390625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0009765625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.005859375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00390625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.04296875f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.0404296875f - b2);
+  }
+}
+struct Cheb_lw2 {
+  static constexpr double kMhat[] = {0.5};
+  static constexpr double kMPhat[] = {-0.03571428571428571};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_lw2> : Cheb_lw2 {};
+template <> __device__ __forceinline__ void Cheb_lw2::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.3125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.6875f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 3.125f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.00390625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.01953125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.01953125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.078125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.2734375f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.19140625f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.5625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.1875f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 2.1875f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0005580357142857143f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.004185267857142857f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.009486607142857142f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.012276785714285714f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.1171875f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.134765625f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_lw2::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.00390625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.01953125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.01953125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.078125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.2734375f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.30859375f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -3.487723214285714e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0001220703125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.000244140625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.001708984375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.001708984375f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0057373046875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.019775390625f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.022007533482142856f - b2);
+  }
+}
+struct Cheb_lw4 {
+  static constexpr double kMhat[] = {0.5};
+  static constexpr double kMPhat[] = {-0.027777777777777776};
+  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, float& Fl, float& Fp);
+  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);
+};
+template <> struct ChebOf<Kern_lw4> : Cheb_lw4 {};
+template <> __device__ __forceinline__ void Cheb_lw4::integrands<0>(float x, float& P, float& Psi, float& Fl, float& Fp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.022786458333333332f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.1640625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.41015625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.09114583333333333f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 1.845703125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -4.921875f - b2); b2 = b1; b1 = t;
+    P = fmaf(x, b1, 3.25390625f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.00017801920572916666f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0010579427083333333f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0008544921875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.008544921875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.02691650390625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.011962890625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.09712727864583333f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.2694498697916667f - b2); b2 = b1; b1 = t;
+    Psi = fmaf(x, b1, -0.1787567138671875f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.0028483072916666665f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0283203125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.10986328125f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.14420572916666666f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.402587890625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -2.255859375f - b2); b2 = b1; b1 = t;
+    Fl = fmaf(x, b1, 2.29345703125f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -1.7801920572916668e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.00014919704861111112f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0003323025173611111f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0009087456597222222f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.006364610460069444f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.010321723090277778f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.018710666232638888f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.1221923828125f - b2); b2 = b1; b1 = t;
+    Fp = fmaf(x, b1, -0.1261927286783854f - b2);
+  }
+}
+template <> __device__ __forceinline__ void Cheb_lw4::potentials<0>(float x, float& M, float& Mp) {
+  const float x2 = 2.0f * x;
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -0.00017801920572916666f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0010579427083333333f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0008544921875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.008544921875f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.02691650390625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.011962890625f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.09712727864583333f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.2694498697916667f - b2); b2 = b1; b1 = t;
+    M = fmaf(x, b1, 0.3212432861328125f - b2);
+  }
+  {
+    float b1 = 0.0f, b2 = 0.0f, t;
+    t = fmaf(x2, b1, -1.1126200358072917e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 4.874335394965277e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 9.854634602864584e-06f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -8.837381998697917e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 8.217493693033855e-05f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0005315144856770834f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.0016110738118489583f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.0006230672200520834f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, 0.005574862162272136f - b2); b2 = b1; b1 = t;
+    t = fmaf(x2, b1, -0.014959971110026041f - b2); b2 = b1; b1 = t;
+    Mp = fmaf(x, b1, -0.017943594190809462f - b2);
+  }
+}
+
 // ---- disk element: pi*W, M/r^2 and the second potential of every exact kernel, summed over its blocks
 template <int KID> __device__ __forceinline__ void disk_profile(double r, double ir2, double& P, double& Fl,
                                                              double& F2l);

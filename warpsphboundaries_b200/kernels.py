@@ -436,6 +436,7 @@ def emit_header() -> str:
     out.append("static const double kPlanRadii[kPlanNumRadii] = {" + ", ".join(_lit(x) for x in RAD) + "};")
     out.append("")
     out.extend(emit_quad())
+    out.extend(emit_cheb32())
     out.extend(emit_disk())
     out.extend(emit_radial())
     out.extend(emit_mesh())
@@ -443,6 +444,91 @@ def emit_header() -> str:
     out.append("}  // namespace wsb")
     out.append("")
     return "\n".join(out)
+
+
+def chebyshev(coeffs, R):
+    """exact Chebyshev coefficients b_k of the polynomial sum_n coeffs[n] r^n on [0, R], x = 2 r / R - 1:
+    p(r) = sum_k b_k T_k(x).  Power basis in x first (r = R (x + 1) / 2), then x^n = 2^(1 - n) sum_j C(n, j) T_(n-2j)
+    with the T_0 term halved."""
+    R = F(R)
+    deg = len(coeffs) - 1
+    px = [F(0)] * (deg + 1)
+    for n, c in enumerate(coeffs):
+        if c:
+            f = F(c) * (R / 2) ** n
+            for k in range(n + 1):
+                px[k] += f * comb(n, k)
+    b = [F(0)] * (deg + 1)
+    for n, a in enumerate(px):
+        if not a:
+            continue
+        for j in range(n // 2 + 1):
+            k = n - 2 * j
+            w = F(1) if n == 0 else F(comb(n, j), 2 ** (n - 1))
+            if k == 0 and n > 0:
+                w /= 2
+            b[k] += a * w
+    return b
+
+
+CHEB_PROFILES = ("c", "psi", "flam", "fpsi", "m", "mpsi")   # the four chord integrands, then the two potentials
+F32_GAUSS = 8                                               # Gauss-Legendre nodes per panel of the float route
+
+
+def emit_cheb32() -> list:
+    """float Chebyshev tables of every exact kernel's block profiles on [0, R] (the float route of the 2-D channels):
+    P, Psi, M/r^2, MPsi/r^2 (integrated along the chord by Gauss-Legendre) and the potentials M, MPsi (whose
+    differences are the odd chord integrals).  Chebyshev coefficients of a bounded profile stay bounded, so Clenshaw's
+    recurrence evaluates them in float to a few ulp of the profile's scale, where the monomial coefficients (up to
+    ~1e4) would cancel."""
+    import numpy as np
+    gx, gw = np.polynomial.legendre.leggauss(F32_GAUSS)
+    out = ["// ---- float Chebyshev tables of the block profiles on [0, R] (x = 2 r / R - 1), Clenshaw in float",
+           f"constexpr int kF32Gauss = {F32_GAUSS};   // Gauss-Legendre nodes per panel of the float route",
+           "static __device__ const float kF32Gx[kF32Gauss] = {" + ", ".join(repr(float(v)) + "f" for v in gx) + "};",
+           "static __device__ const float kF32Gw[kF32Gauss] = {" + ", ".join(repr(float(v)) + "f" for v in gw) + "};",
+           "template <class KT> struct ChebOf;   // the float tables of an exact kernel"]
+
+    def clenshaw(cb, dst):
+        cb = list(cb)
+        while len(cb) > 1 and cb[-1] == 0:
+            cb.pop()
+        lit = lambda v: repr(float(v)) + "f"
+        if len(cb) == 1:
+            return [f"  {dst} = {lit(cb[0])};"]
+        lines = ["  {", "    float b1 = 0.0f, b2 = 0.0f, t;"]
+        for k in range(len(cb) - 1, 0, -1):
+            lines.append(f"    t = fmaf(x2, b1, {lit(cb[k])} - b2); b2 = b1; b1 = t;")
+        lines.append(f"    {dst} = fmaf(x, b1, {lit(cb[0])} - b2);")
+        lines.append("  }")
+        return lines
+
+    for name, kid in sorted(KERNEL_IDS.items(), key=lambda t: t[1]):
+        k = kernel(name)
+        out.append(f"struct Cheb_{name} {{")
+        out.append("  static constexpr double kMhat[] = {" + ", ".join(_lit(b.Mhat) for b in k.blocks) + "};")
+        out.append("  static constexpr double kMPhat[] = {" + ", ".join(_lit(b.MPhat) for b in k.blocks) + "};")
+        out.append("  template <int B> __device__ static __forceinline__ void integrands(float x, float& P, float& Psi, "
+                   "float& Fl, float& Fp);")
+        out.append("  template <int B> __device__ static __forceinline__ void potentials(float x, float& M, float& Mp);")
+        out.append("};")
+        out.append(f"template <> struct ChebOf<Kern_{name}> : Cheb_{name} {{}};")
+        for bi, b in enumerate(k.blocks):
+            cheb = {pn: chebyshev(getattr(b, pn), b.R) for pn in CHEB_PROFILES}
+            out.append(f"template <> __device__ __forceinline__ void Cheb_{name}::integrands<{bi}>(float x, float& P, "
+                       "float& Psi, float& Fl, float& Fp) {")
+            out.append("  const float x2 = 2.0f * x;")
+            for pn, dst in (("c", "P"), ("psi", "Psi"), ("flam", "Fl"), ("fpsi", "Fp")):
+                out.extend(clenshaw(cheb[pn], dst))
+            out.append("}")
+            out.append(f"template <> __device__ __forceinline__ void Cheb_{name}::potentials<{bi}>(float x, float& M, "
+                       "float& Mp) {")
+            out.append("  const float x2 = 2.0f * x;")
+            for pn, dst in (("m", "M"), ("mpsi", "Mp")):
+                out.extend(clenshaw(cheb[pn], dst))
+            out.append("}")
+    out.append("")
+    return out
 
 
 def emit_disk() -> list:

@@ -39,7 +39,7 @@ from .shim import (GradientScheme, KernelFunctions, OperationDirection, Operatio
 
 F64 = torch.float64
 KINDS = {"lam": (0, 1), "g0": (1, 2), "cov": (2, 4), "a1g1": (3, 2), "lap": (4, 1), "m1": (5, 2), "m2": (6, 4)}
-_PREC = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+_PREC = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "fp32": _lib.PREC_FP32}
 
 
 @runtime_checkable

@@ -256,8 +256,10 @@ class SurfaceRep:
         quad = name in QUAD_KERNEL_IDS
         if name not in KERNEL_IDS and not quad:
             raise NotImplementedError(f"SurfaceRep.moments: kernel {name!r} is not built")
+        if precision == "fp32":
+            raise NotImplementedError("SurfaceRep.moments: the float route runs on the fused pass (FusedWall)")
         if precision not in ("fp64", "mixed"):
-            raise ValueError("precision must be 'fp64' or 'mixed'")
+            raise ValueError("precision must be 'fp64', 'mixed' or 'fp32'")
         if quad and self._triangle is not None:
             raise NotImplementedError("SurfaceRep.moments: the tensile kernels have no conditioned-triangle route")
         dev = torch.device(device)
