@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp32"])
     p.add_argument("--route", default="fused", choices=["fused", "plain"])
     p.add_argument("--particles", type=int, default=1 << 20)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -545,7 +545,7 @@ def our_arm(args):
     outs = {k: [torch.zeros(N, dtype=torch.float64, device=dev), torch.zeros((N, 2), dtype=torch.float64, device=dev),
                 torch.zeros((N, 4), dtype=torch.float64, device=dev), torch.zeros((N, 2), dtype=torch.float64, device=dev),
                 torch.zeros((N, 4), dtype=torch.float64, device=dev)] for k in KERNELS}
-    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+    prec = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED, "fp32": _lib.PREC_FP32}
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -650,6 +650,7 @@ def our_arm(args):
         nr = max(3, args.steps // 2)
         ms_f, _, _ = timed("fp64", nr, 1)
         ms_m, _, _ = timed("mixed", nr, 1)
+        ms_32, _, _ = timed("fp32", nr, 1)
         ab = AnalyticBoundary(scene, route="plain")
         ps = ParticleState(pos, sup)
         kfs = (KernelFunctions.CubicSpline, KernelFunctions.Wendland2, KernelFunctions.Wendland4,
@@ -671,8 +672,10 @@ def our_arm(args):
         torch.cuda.empty_cache()
         fused64 = pairs_step * nr / (ms_f * 1e-3)
         mixed = pairs_step * nr / (ms_m * 1e-3)
-        headline = mixed if args.precision == "mixed" else fused64
+        fp32 = pairs_step * nr / (ms_32 * 1e-3)
+        headline = {"mixed": mixed, "fp64": fused64, "fp32": fp32}[args.precision]
         routes = {"plain_fp64_pairs_per_s": plain, "fused_fp64_pairs_per_s": fused64, "mixed_pairs_per_s": mixed,
+                  "fp32_route_pairs_per_s": fp32,
                   "batched_over_plain": headline / plain, "fused_fp64_over_plain": fused64 / plain,
                   "what": "one step (prepare + the four kernels) per route on the same scene and particles; plain = "
                           "k_fixed_topology slots + k_slot_channels_plain (the reference's per-slot plan "
@@ -815,7 +818,8 @@ def our_arm(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f64+f32",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": {"fp64": "f64", "mixed": "f64+f32", "fp32": "f32+f64"}[args.precision],
                 "data": "synthetic (seeded)",
                 "config": config(N), "pairs_per_kernel": P, "route": args.route, "precision": args.precision,
                 "routes": routes,

@@ -123,6 +123,12 @@ int wsb_pair_channels(const wsb_surface* s, int kernel, int precision, const int
 
 /* Workspace bytes wsb_aggregate needs for n rows. */
 size_t wsb_aggregate_workspace_size(const wsb_surface* s, int64_t n);
+/* Optional staging bytes for n rows: a workspace of wsb_aggregate_workspace_size + wsb_aggregate_staging_size bytes
+ * (given to prepare and to every evaluation of that preparation alike) lets the evaluation write each work row's
+ * channel sums to the staging region and then every row's outputs in one coalesced pass, instead of storing the work
+ * rows' outputs scattered by row index.  The results are the same bits either way.  No counterpart in the reference
+ * (a layout choice of this implementation). */
+size_t wsb_aggregate_staging_size(const wsb_surface* s, int64_t n);
 
 /* Fused route: body-frame coordinates (Pose.toLocal), the body broadphase (support circle against the body box
  * [obb_lo, obb_hi]; unbounded != 0 skips it), the fixed-capacity neighbour predicate, the twelve channels of every

@@ -185,3 +185,38 @@ def test_golden_elements_on_gpu():
                 worst = max(worst, err)
                 assert err < 1e-10, (case["id"], k, g, r)
     assert worst < 1e-10
+
+
+@pytest.mark.parametrize("kernels", [("w4",), ("cubic", "w2", "w4", "w6"), ("w2", "cone", "lw2")])
+@pytest.mark.parametrize("assign", [True, False])
+def test_staged_and_direct_evaluation_agree(c2s, kernels, assign):
+    """a workspace with the staging region (work rows' sums staged, every row expanded in one coalesced pass) and one
+    without it (work rows' outputs stored directly) give the same bits, for one kernel and for packs."""
+    import ctypes
+    from warpsphboundaries_b200 import _lib
+    from warpsphboundaries_b200.kernels import KERNEL_IDS
+    from warpsphboundaries_b200.scene import _stream
+    loops, X, h = c2s
+    scene, rep, body = make_scene(loops, center=(0.02, -0.01), angle=0.3)
+    ns = rep.native(h, DEV)
+    n = len(X)
+    pos = torch.tensor(X, dtype=torch.float64, device=DEV)
+    sup = torch.full((n,), h, dtype=torch.float64, device=DEV)
+    base = int(_lib.lib.wsb_aggregate_workspace_size(ns.handle, n))
+    full = base + int(_lib.lib.wsb_aggregate_staging_size(ns.handle, n))
+    kids = _lib.int32s([KERNEL_IDS[k] for k in kernels])
+    obb = (ctypes.c_double * 4)(*body.obb())
+    pose = body.pose_tensor(DEV)
+    mode = _lib.OUT_ALL | (_lib.OUT_ASSIGN if assign else 0)
+    res = []
+    for nbytes in (base, full):
+        ws = torch.empty(nbytes, dtype=torch.uint8, device=DEV)
+        outs = [[torch.full((n * w,), 0.25, dtype=torch.float64, device=DEV) for _ in kernels] for w in (1, 2, 4, 2, 4)]
+        _lib.check(_lib.lib.wsb_aggregate_groups(ns.handle, len(kernels), kids, _lib.PREC_FP64, _lib.ptr(pos),
+                                                 _lib.ptr(sup), None, n, _lib.ptr(pose), obb, 0, mode,
+                                                 *[_lib.ptrs(o) for o in outs], _lib.ptr(ws), nbytes, _stream()))
+        torch.cuda.synchronize()
+        res.append(outs)
+    for a, b in zip(res[0], res[1]):
+        for x, y in zip(a, b):
+            assert torch.equal(x, y)

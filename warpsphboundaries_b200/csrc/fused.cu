@@ -18,6 +18,8 @@ constexpr int kKeys = 65;          // count keys: 0..63 rows with pairs (63 - mi
 
 static inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+constexpr int kMaxPackStaged = 4;   // kernels of the largest pack: channel sums a staged work row holds
+
 // the neighbour mask of a row covers the first kMaskBits candidates of its cell; later candidates (cells holding more
 // edges) are found again by the predicate in the pair kernel
 constexpr int kMaskBits = 128;
@@ -50,6 +52,10 @@ struct Workspace {
   WorkRec* wrec;     // [n] work rows by decreasing pair count (slots < nwork used)
   int32_t* nwork;    // [1] number of rows with pairs
   size_t total;
+  // optional staging region after `total` (a workspace of total + staging bytes): the channel sums of every work row,
+  // [slot][kernel][12], written by the pair pass and expanded to the outputs by k_agg_expand; nullptr without it
+  double* wacc;
+  size_t staging;
 };
 
 static Workspace carve(const Surface* s, int64_t n, void* base) {
@@ -76,7 +82,14 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
   w.wrec = (WorkRec*)take(sizeof(WorkRec) * std::max<int64_t>(n, 1));
   w.nwork = (int32_t*)take(sizeof(int32_t));
   w.total = off;
+  w.staging = align256(sizeof(double) * 12 * kMaxPackStaged * std::max<int64_t>(n, 1));
+  w.wacc = nullptr;
   return w;
+}
+
+// the staging region when the workspace holds it (workspace_bytes >= total + staging)
+static void attach_staging(Workspace& w, void* base, size_t workspace_bytes) {
+  w.wacc = (base && workspace_bytes >= w.total + w.staging) ? (double*)((char*)base + w.total) : nullptr;
 }
 
 // body-frame position (bit-for-bit Pose.toLocal), broadphase (fixedadj.py:257-265) and the bucket of every row
@@ -573,6 +586,27 @@ __device__ __forceinline__ void pack_finish(const double* acc_t, bool write, int
   }
 }
 
+// a work row's channel sums (the G lanes' sums by the xor butterfly, x 1/pi) into its staging slot [kernel][12]
+template <class Pack, int G, int K>
+__device__ __forceinline__ void pack_stage(const double* acc_t, bool write, double* dst) {
+  if constexpr (K < Pack::kN) {
+    double acc[12];
+#pragma unroll
+    for (int c = 0; c < 12; ++c) acc[c] = acc_t[(K * 12 + c) * kThreads];
+#pragma unroll
+    for (int off = 1; off < G; off <<= 1) {
+#pragma unroll
+      for (int c = 0; c < 12; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+    }
+    if (write) {
+      double2* d2 = reinterpret_cast<double2*>(dst + K * 12);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) d2[c] = make_double2(acc[2 * c] * kInvPi, acc[2 * c + 1] * kInvPi);
+    }
+    pack_stage<Pack, G, K + 1>(acc_t, write, dst);
+  }
+}
+
 // Rows with neighbour pairs (compacted, by decreasing pair count), then the rows without: the first
 // ceil(nwork G / kThreads) blocks take the work rows, the next ceil(n / kThreads) blocks the constant rows (one row a
 // thread, coalesced), so the constant rows' stores overlap the last wave of pair blocks instead of running as a launch
@@ -584,14 +618,14 @@ __device__ __forceinline__ void pack_finish(const double* acc_t, bool write, int
 // butterfly (the same additions on every lane, commutative, so the result is deterministic and identical on the G
 // lanes).  The channel sums live in shared memory ([kernel][channel][thread]), which keeps the registers for the
 // closed form.
-template <class Pack, int PREC, int G, int MINB>
+template <class Pack, int PREC, int G, int MINB, bool STAGED>
 __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const double* __restrict__ sup,
                                                              const WorkRec* __restrict__ wrec,
                                                              const int32_t* __restrict__ nwork_p, int64_t n,
                                                              const double* __restrict__ ind,
                                                              const int32_t* __restrict__ flag,
                                                              const double* __restrict__ pose, bool assign,
-                                                             const PackOut out) {
+                                                             const PackOut out, double* __restrict__ wacc) {
   static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "lanes per row");
   static_assert(Pack::kN >= 1 && Pack::kN <= kMaxPack, "pack size");
   // dynamic shared memory: the channel sums [kernel][channel][thread], then each thread's next edge record
@@ -601,6 +635,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
   const int64_t nwork = *nwork_p;
   const int64_t wblocks = (nwork + kThreads / G - 1) / (kThreads / G);
   if ((int64_t)blockIdx.x >= wblocks) {                             // a tail block: constant rows
+    if constexpr (STAGED) return;                                   // (staged: k_agg_expand writes every row)
     const int64_t i = ((int64_t)blockIdx.x - wblocks) * kThreads + threadIdx.x;
     if (i < n) {
       const int32_t f = flag[i];
@@ -680,7 +715,51 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
     }
   }
   const bool write = ok && sub == 0;
-  pack_finish<Pack, G, 0>(acc_t, write, i, write ? ind[i] : 0.0, h, pose, assign, out);
+  if constexpr (STAGED)
+    pack_stage<Pack, G, 0>(acc_t, write, wacc + w * (Pack::kN * 12));
+  else
+    pack_finish<Pack, G, 0>(acc_t, write, i, write ? ind[i] : 0.0, h, pose, assign, out);
+}
+
+// Staged expansion: one thread per row, consecutive rows in consecutive threads, so every output array is written in
+// full coalesced sectors -- a work row's outputs from its staged channel sums (key[i] is its work slot), any other row
+// the indicator times the whole-plane channels.
+template <class Pack, int K>
+__device__ __forceinline__ void pack_expand_row(const double* a, int64_t i, double w, double h, const double* pose,
+                                                bool assign, const PackOut& o) {
+  if constexpr (K < Pack::kN) {
+    using KT = typename Pack::template Kern<K>;
+    double acc[12];
+    const double2* a2 = reinterpret_cast<const double2*>(a + K * 12);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      const double2 v = __ldg(a2 + c);
+      acc[2 * c] = v.x;
+      acc[2 * c + 1] = v.y;
+    }
+    if constexpr (KT::kQuad)
+      finish_row_quad(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+    else
+      finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+    pack_expand_row<Pack, K + 1>(a, i, w, h, pose, assign, o);
+  }
+}
+
+template <class Pack>
+__global__ void __launch_bounds__(kThreads) k_agg_expand(const double* __restrict__ sup,
+                                                         const int32_t* __restrict__ flag,
+                                                         const double* __restrict__ ind,
+                                                         const int32_t* __restrict__ slot,
+                                                         const double* __restrict__ wacc, int64_t n,
+                                                         const double* __restrict__ pose, bool assign,
+                                                         const PackOut out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t f = flag[i];
+  if (f == 2)
+    pack_expand_row<Pack, 0>(wacc + (int64_t)slot[i] * (Pack::kN * 12), i, ind[i], sup[i], pose, assign, out);
+  else if (f == 1 || assign)
+    pack_constant_row<Pack, 0>(i, f == 1 ? ind[i] : 0.0, sup[i], pose, assign, out);
 }
 
 // the pair kernel of a pack over a prepared workspace (two lanes per work row: measured fastest on the 2^20-particle
@@ -696,19 +775,23 @@ static int launch_pack(const SurfView& v, const double* sup, const Workspace& w,
                        bool assign, const PackOut& out, cudaStream_t st) {
   constexpr int G = 2;
   constexpr size_t smem = pack_smem_bytes<Pack>();
-  auto kern = k_agg_pairs<Pack, PREC, G, pack_min_blocks(Pack::kN)>;
+  const bool staged = w.wacc != nullptr;
+  auto kern = staged ? k_agg_pairs<Pack, PREC, G, pack_min_blocks(Pack::kN), true>
+                     : k_agg_pairs<Pack, PREC, G, pack_min_blocks(Pack::kN), false>;
   if (smem > 48 * 1024) {       // above the default limit: opt in once per device for this instantiation
-    static std::atomic<uint64_t> opted{0};
+    static std::atomic<uint64_t> opted[2] = {{0}, {0}};
     int dev = 0;
     WSB_CUDA(cudaGetDevice(&dev));
     const uint64_t bit = 1ull << (dev & 63);
-    if (!(opted.load() & bit)) {
+    if (!(opted[staged].load() & bit)) {
       WSB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      opted.fetch_or(bit);
+      opted[staged].fetch_or(bit);
     }
   }
-  const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads + (n + kThreads - 1) / kThreads);
-  kern<<<grid, kThreads, smem, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, out);
+  const unsigned rows = (unsigned)((n + kThreads - 1) / kThreads);
+  const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads) + (staged ? 0u : rows);
+  kern<<<grid, kThreads, smem, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, out, w.wacc);
+  if (staged) k_agg_expand<Pack><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
   return WSB_OK;
 }
 
@@ -1004,7 +1087,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_block(const int32_t* __re
 // independent of it)
 __global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int64_t n, const int32_t* __restrict__ khist,
                               int32_t* __restrict__ kcur, const int32_t* __restrict__ order,
-                              const int32_t* __restrict__ bucket, const double* __restrict__ lpos,
+                              int32_t* __restrict__ bucket, const double* __restrict__ lpos,
                               const double* __restrict__ sup, const uint64_t* __restrict__ mask,
                               WorkRec* __restrict__ wrec, int32_t* __restrict__ nwork) {
   __shared__ int32_t s_pre[kKeys + 1];
@@ -1042,7 +1125,9 @@ __global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int6
     r.pad[0] = r.pad[1] = r.pad[2] = 0;
     r.m0 = mm.x;
     r.m1 = mm.y;
-    wrec[s_pre[key] + base + __popc(peers & ((1u << lane) - 1))] = r;
+    const int32_t slot = s_pre[key] + base + __popc(peers & ((1u << lane) - 1));
+    wrec[slot] = r;
+    bucket[i] = slot;            // from here on a work row's key is its work slot (read by the staged expansion)
   }
 }
 
@@ -1272,6 +1357,12 @@ extern "C" size_t wsb_aggregate_workspace_size(const wsb_surface* s_, int64_t n)
   return carve(s, n, nullptr).total;
 }
 
+extern "C" size_t wsb_aggregate_staging_size(const wsb_surface* s_, int64_t n) {
+  const Surface* s = reinterpret_cast<const Surface*>(s_);
+  if (!s || n < 0) return 0;
+  return carve(s, n, nullptr).staging;
+}
+
 extern "C" int wsb_aggregate_prepare(const wsb_surface* s_, const double* pos, const double* sup,
                                      const int32_t* allowed, int64_t n, const double* pose, const double* obb,
                                      int unbounded, void* workspace, size_t workspace_bytes, void* stream) {
@@ -1299,7 +1390,8 @@ extern "C" int wsb_aggregate_evaluate(const wsb_surface* s_, int kernel, int pre
   if (n < 0 || n > (int64_t)INT32_MAX) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: row count out of range");
   if (n == 0) return WSB_OK;
   if (!sup || !pose) return fail(WSB_ERR_ARG, "wsb_aggregate_evaluate: NULL array");
-  const Workspace w = carve(s, n, const_cast<void*>(workspace));
+  Workspace w = carve(s, n, const_cast<void*>(workspace));
+  attach_staging(w, const_cast<void*>(workspace), workspace_bytes);
   if (!workspace || workspace_bytes < w.total) return fail(WSB_ERR_SIZE, "wsb_aggregate_evaluate: workspace too small");
   WSB_CUDA(cudaSetDevice(s->device));
   cudaStream_t st = (cudaStream_t)stream;
@@ -1397,7 +1489,8 @@ extern "C" int wsb_aggregate_evaluate_groups(const wsb_surface* s_, int n_groups
     if (rc) return rc;
   }
   if (which < 0) return WSB_OK;
-  const Workspace w = carve(s, n, const_cast<void*>(workspace));
+  Workspace w = carve(s, n, const_cast<void*>(workspace));
+  attach_staging(w, const_cast<void*>(workspace), workspace_bytes);
   if (!workspace || workspace_bytes < w.total)
     return fail(WSB_ERR_SIZE, "wsb_aggregate_evaluate_groups: workspace too small");
   WSB_CUDA(cudaSetDevice(s->device));

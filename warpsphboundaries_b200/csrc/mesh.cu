@@ -309,34 +309,41 @@ struct EdgeSums {
   double LK1, LK2, LK2b, TK2, LW, LL;   // int z A_K1, int z^2 A_K2, int z A_K2, int s z A_K2, int A_W, int A_L
 };
 
-// one quadrature node u (distance from the foot along the edge, s = sgn_side * u) with weight wt
+// one quadrature node u (distance from the foot along the edge, s = sgn_side * u) with weight wt, in two passes over
+// an edge's nodes so that fewer values are live at once: the six divided differences (w != 0 only), then the six
+// potential sums; each pass forms r and 1 / r itself (the same operations, so the sums are those of one pass)
 template <class M>
-__device__ __forceinline__ void node_eval(double u, double wt, double sgn_side, double c2, double a, double z,
-                                          double sg, double w, EdgeSums& S) {
-  const double s = sgn_side * u;
+__device__ __forceinline__ void node_eval_dd(double u, double wt, double c2, double a, double z, double sg, double w,
+                                             EdgeSums& S) {
   const double rho2 = fma(u, u, w * w);
   Node nd;
   nd.r = sqrt(fma(u, u, c2));
   nd.ir = 1.0 / nd.r;
-  if (w != 0.0) {
-    nd.split = M::kPieces > 1 && a < M::kBreak && nd.r > M::kBreak;
-    nd.irpa = 1.0 / (nd.r + a);
-    nd.irho2 = nd.split ? 1.0 / rho2 : 0.0;
-    const double ww = w * wt;
-    S.J[0] = fma(ww, dd2<M, 0, 1>(nd, a, z, sg), S.J[0]);
-    S.J[1] = fma(ww, dd2<M, 1, 2>(nd, a, z, sg), S.J[1]);
-    S.J[2] = fma(ww, dd2<M, 2, 3>(nd, a, z, sg), S.J[2]);
-    S.J[3] = fma(ww, dd2<M, 3, 0>(nd, a, z, sg), S.J[3]);
-    S.J[4] = fma(ww, dd2<M, 4, 0>(nd, a, z, sg), S.J[4]);
-    S.J[5] = fma(ww, dd2<M, 5, 1>(nd, a, z, sg), S.J[5]);
-  }
-  const double k1 = aval<M, 1>(nd.r, nd.ir) * z, k2 = aval<M, 2>(nd.r, nd.ir) * z;
+  nd.split = M::kPieces > 1 && a < M::kBreak && nd.r > M::kBreak;
+  nd.irpa = 1.0 / (nd.r + a);
+  nd.irho2 = nd.split ? 1.0 / rho2 : 0.0;
+  const double ww = w * wt;
+  S.J[0] = fma(ww, dd2<M, 0, 1>(nd, a, z, sg), S.J[0]);
+  S.J[1] = fma(ww, dd2<M, 1, 2>(nd, a, z, sg), S.J[1]);
+  S.J[2] = fma(ww, dd2<M, 2, 3>(nd, a, z, sg), S.J[2]);
+  S.J[3] = fma(ww, dd2<M, 3, 0>(nd, a, z, sg), S.J[3]);
+  S.J[4] = fma(ww, dd2<M, 4, 0>(nd, a, z, sg), S.J[4]);
+  S.J[5] = fma(ww, dd2<M, 5, 1>(nd, a, z, sg), S.J[5]);
+}
+
+template <class M>
+__device__ __forceinline__ void node_eval_pot(double u, double wt, double sgn_side, double c2, double z,
+                                              EdgeSums& S) {
+  const double s = sgn_side * u;
+  const double r = sqrt(fma(u, u, c2));
+  const double ir = 1.0 / r;
+  const double k1 = aval<M, 1>(r, ir) * z, k2 = aval<M, 2>(r, ir) * z;
   S.LK1 = fma(wt, k1, S.LK1);
   S.LK2b = fma(wt, k2, S.LK2b);
   S.LK2 = fma(wt, k2 * z, S.LK2);
   S.TK2 = fma(wt * s, k2, S.TK2);
-  S.LW = fma(wt, aval<M, 3>(nd.r, nd.ir), S.LW);
-  S.LL = fma(wt, aval<M, 4>(nd.r, nd.ir), S.LL);
+  S.LW = fma(wt, aval<M, 3>(r, ir), S.LW);
+  S.LL = fma(wt, aval<M, 4>(r, ir), S.LL);
 }
 
 // the panels of one edge (both sides of the foot of the perpendicular): [u0, u1] of distances from the foot, split
@@ -544,6 +551,18 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
       if (lane == 0) np = build_panels<M>(PL, s0, s1, c);
       np = __shfl_sync(0xffffffffu, np, 0);
       __syncwarp();
+      if (w != 0.0) {
+        int p = 0;
+        for (int k = lane; k < PL.off[np]; k += 32) {
+          while (k >= PL.off[p + 1]) ++p;
+          const int g = k - PL.off[p];
+          const bool n16 = PL.off[p + 1] - PL.off[p] == 16;
+          const double xg = n16 ? kTriGx16[g] : kRadialGx[g], wg = n16 ? kTriGw16[g] : kRadialGw[g];
+          const double x0 = PL.lo[p], x1 = PL.hi[p];
+          const double hc = 0.5 * (x1 - x0);
+          node_eval_dd<M>(fma(hc, xg, 0.5 * (x1 + x0)), wg * hc, c2, a, z, sg, w, S);
+        }
+      }
       int p = 0;
       for (int k = lane; k < PL.off[np]; k += 32) {
         while (k >= PL.off[p + 1]) ++p;
@@ -552,7 +571,7 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
         const double xg = n16 ? kTriGx16[g] : kRadialGx[g], wg = n16 ? kTriGw16[g] : kRadialGw[g];
         const double x0 = PL.lo[p], x1 = PL.hi[p];
         const double hc = 0.5 * (x1 - x0);
-        node_eval<M>(fma(hc, xg, 0.5 * (x1 + x0)), wg * hc, PL.sg[p], c2, a, z, sg, w, S);
+        node_eval_pot<M>(fma(hc, xg, 0.5 * (x1 + x0)), wg * hc, PL.sg[p], c2, z, S);
       }
       double v[12] = {S.J[0], S.J[1], S.J[2], S.J[3], S.J[4], S.J[5], S.LK1, S.LK2, S.LK2b, S.TK2, S.LW, S.LL};
       warp_sum12(v);

@@ -124,7 +124,8 @@ static void scene_bbox(SceneBody& b) {
 static size_t scene_ws_bytes(const wsb_scene* sc, int64_t n) {
   size_t need = 0;
   for (const SceneBody& b : sc->bodies)
-    for (const wsb_surface* s : b.surfaces) need = std::max(need, wsb_aggregate_workspace_size(s, n));
+    for (const wsb_surface* s : b.surfaces)
+      need = std::max(need, wsb_aggregate_workspace_size(s, n) + wsb_aggregate_staging_size(s, n));
   return need;
 }
 

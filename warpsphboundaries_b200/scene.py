@@ -78,7 +78,9 @@ class NativeSurface:
     def workspace(self, n):
         """the workspace for n rows on the current stream: one buffer per stream, grown geometrically and reused for
         any smaller row count (the library carves it per call and allocates nothing itself)."""
-        need = int(lib.wsb_aggregate_workspace_size(self.handle, int(n)))
+        # with the staging region: the evaluations store every row's outputs in one coalesced pass
+        need = int(lib.wsb_aggregate_workspace_size(self.handle, int(n)) +
+                   lib.wsb_aggregate_staging_size(self.handle, int(n)))
         key = torch.cuda.current_stream(self.device).cuda_stream
         ws = self._ws.get(key)
         if ws is None or ws.numel() < need:

@@ -166,7 +166,8 @@ class BoundaryServer:
             reps = [r.native(float(support), self.device) for r in b.fused_reps(float(support), self.device)]
             plan.append((b.pose_tensor(self.device), (_lib.ctypes.c_double * 4)(*b.obb()), int(b.unbounded()), reps))
             for ns in reps:
-                self.ws_bytes = max(self.ws_bytes, int(lib.wsb_aggregate_workspace_size(ns.handle, self.max_batch_rows)))
+                self.ws_bytes = max(self.ws_bytes, int(lib.wsb_aggregate_workspace_size(ns.handle, self.max_batch_rows)) +
+                                    int(lib.wsb_aggregate_staging_size(ns.handle, self.max_batch_rows)))
         self.scenes[scene_id] = (scene, float(support))
         self.plans[scene_id] = plan
 
@@ -280,7 +281,8 @@ class BoundaryServer:
         ws = 0
         for b in scene.bodies:
             for r in b.fused_reps(support, self.device):
-                ws = max(ws, int(lib.wsb_aggregate_workspace_size(r.native(support, self.device).handle, rows)))
+                h_ = r.native(support, self.device).handle
+                ws = max(ws, int(lib.wsb_aggregate_workspace_size(h_, rows)) + int(lib.wsb_aggregate_staging_size(h_, rows)))
         return (8 * 13 * B + 24 + (16 if grad else 0)) * rows + ws
 
     # ------------------------------------------------------------------ the loop
@@ -476,7 +478,8 @@ class BoundaryServer:
         if g is None:
             sall.fill_(1)
             # graph-owned workspace and outputs: a captured graph keeps its pointers, so they are never freed
-            need = max(int(lib.wsb_aggregate_workspace_size(ns.handle, bucket)) for _, _, _, reps in plan for ns in reps)
+            need = max(int(lib.wsb_aggregate_workspace_size(ns.handle, bucket)) + int(lib.wsb_aggregate_staging_size(ns.handle, bucket))
+                       for _, _, _, reps in plan for ns in reps)
             ws = torch.empty(need, dtype=torch.uint8, device=self.device)
             gout = {k: torch.empty((B, bucket) + _TAIL[k], dtype=F64, device=self.device) for k in OUT_KEYS}
             self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)     # eager warm-up
