@@ -209,11 +209,13 @@ class Clocks:
 # ----------------------------------------------------------------------------------------------- serving stream
 def serving_run(n_requests, dev, pair_density, seed=0, loads=(0.8, 0.9, 0.95)):
     """Poisson stream of boundary queries over 32 resident scenes: 16 of the large 2-D kind (64 star polygons each,
-    h = 0.02) and 16 of the 3-D kind (closed icospheres of 5120 faces, radius U(0.3, 0.8), 5 % jitter, h = 0.03).
-    Particle counts log-uniform in [1e3, 1e6] (positions uniform in [0, 4]^2 or [-1, 1]^3, slices of resident
-    rings), kernels uniform in {w2, w4, w6}, 25 % of the 2-D requests with the adjoint.  The arrival rate is a load
-    factor times the capacity measured on a saturating run: the first of `loads` at which the device is at least 80 %
-    busy (every factor tried is reported).  Returns p50 / p99 latency, rates and the device busy fraction."""
+    h = 0.02) and 16 of the 3-D kind, as the 3-D configuration has them: 8 closed icospheres of 20480 faces (radius
+    U(0.3, 0.8), 5 % jitter, h = 0.03) and 8 solid-sphere scenes whose requests are (query, sphere) rows (radii
+    exp U(ln 0.2h, ln 50h), signed distances U(-1.2h, 1.2h) clipped at -R).  Sizes log-uniform in [1e3, 1e6]
+    (particles uniform in [0, 4]^2 or [-1, 1]^3, or sphere rows: slices of resident rings), kernels uniform in
+    {w2, w4, w6}, 25 % of the 2-D requests with the adjoint.  The arrival rate is a load factor times the capacity
+    measured on a saturating run: the first of `loads` at which the device is at least 80 % busy (every factor tried
+    is reported).  Returns p50 / p99 latency overall and per request class, rates and the device busy fraction."""
     import torch
     from warpsphboundaries_b200 import workloads
     from warpsphboundaries_b200.scene import Body, Scene, SurfaceRep
@@ -224,10 +226,12 @@ def serving_run(n_requests, dev, pair_density, seed=0, loads=(0.8, 0.9, 0.95)):
     for k in range(16):
         sc = Scene([Body(reps=[SurfaceRep.loops(workloads.stars(64, (32, 512), seed=100 + k))])], dev)
         srv.register(f"scene{k}", sc, h)
-    for k in range(16):
-        V, Fc = workloads.icosphere(4, float(rng.uniform(0.3, 0.8)), 0.05, seed=200 + k)
+    for k in range(8):
+        V, Fc = workloads.icosphere(5, float(rng.uniform(0.3, 0.8)), 0.05, seed=200 + k)
         srv.register_mesh(f"mesh{k}", V, Fc, h3)
-    names = [f"scene{k}" for k in range(16)] + [f"mesh{k}" for k in range(16)]
+    for k in range(8):
+        srv.register_spheres(f"spheres{k}", h3)
+    names = [f"scene{k}" for k in range(16)] + [f"mesh{k}" for k in range(8)] + [f"spheres{k}" for k in range(8)]
     specs = []
     for _ in range(n_requests):
         sid = names[rng.integers(0, 32)]
@@ -240,15 +244,22 @@ def serving_run(n_requests, dev, pair_density, seed=0, loads=(0.8, 0.9, 0.95)):
     # the clients' particle positions: slices of resident rings of positions (a simulation's state is resident)
     ring2 = torch.rand((1 << 22, 2), dtype=torch.float64, device=dev, generator=gen) * 4.0
     ring3 = torch.rand((1 << 22, 3), dtype=torch.float64, device=dev, generator=gen) * 2.0 - 1.0
-    cursor = [0, 0]
+    rr = np.random.default_rng(seed + 78)
+    ns_ = 1 << 22
+    R = np.exp(rr.uniform(np.log(0.2 * h3), np.log(50 * h3), ns_))
+    nv = rr.normal(size=(ns_, 3))
+    nv /= np.linalg.norm(nv, axis=1, keepdims=True)
+    ringS = torch.tensor(np.concatenate([np.maximum(rr.uniform(-1.2 * h3, 1.2 * h3, ns_), -R)[:, None], nv, R[:, None]],
+                                        1), dtype=torch.float64, device=dev)
+    cursor = [0, 0, 0]
 
     def make(sid, rows):
-        three = sid.startswith("mesh")
-        ring = ring3 if three else ring2
-        c = cursor[int(three)]
+        kind = 2 if sid.startswith("spheres") else int(sid.startswith("mesh"))
+        ring = (ring2, ring3, ringS)[kind]
+        c = cursor[kind]
         start = c if c + rows <= len(ring) else 0
-        cursor[int(three)] = start + rows
-        return ring[start:start + rows], (h3 if three else h)
+        cursor[kind] = start + rows
+        return ring[start:start + rows], (h if kind == 0 else h3)
 
     def submit(sid, rows, k, g, arrival=None):
         p, hh = make(sid, rows)
@@ -301,18 +312,20 @@ def serving_run(n_requests, dev, pair_density, seed=0, loads=(0.8, 0.9, 0.95)):
     for load in loads:
         rate, wall, st = stream(load)
         tried.append({"offered_load": load, "arrival_rate_per_s": rate, "gpu_busy": st.get("gpu_busy"),
-                      "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms")})
+                      "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"), "classes": st.get("classes")})
         if (st.get("gpu_busy") or 0.0) >= 0.8:
             break
     rows_total = sum(r for _, r, _, _ in specs)
     rows_2d = sum(r for sid, r, _, _ in specs if sid.startswith("scene"))
     return {"requests": n_requests, "scenes": 32, "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
+            "classes": st.get("classes"), "graphs": srv.use_graphs,
             "mean_ms": st.get("mean_ms"), "arrival_rate_per_s": rate, "wall_s": wall, "loads_tried": tried,
             "rows_per_s": rows_total / wall, "pairs_per_s_est": rows_2d * pair_density / wall,
             "rows_3d_per_s": (rows_total - rows_2d) / wall,
             "capacity_rows_per_s": cap_rows, "offered_load": load, "gpu_busy": st.get("gpu_busy"),
-            "note": "16 2-D scenes (64 star polygons) + 16 closed 3-D surfaces (5120 faces); pairs estimated from the "
-                    "mean neighbour-pair density of the 2^20-particle 2-D scene for the 2-D rows only"}
+            "note": "16 2-D scenes (64 star polygons) + 8 closed 3-D surfaces (20480 faces) + 8 sphere-row scenes; pairs "
+                    "estimated from the mean neighbour-pair density of the 2^20-particle 2-D scene for the 2-D rows "
+                    "only; rows_3d counts surface queries and sphere rows"}
 
 
 # ----------------------------------------------------------------------------------------------- our arm

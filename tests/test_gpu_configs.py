@@ -100,7 +100,7 @@ def c2_run():
     ref = {k: O.local_twelve(V, E, 0, Xs, hs, k, h, ind=ind, cl=cl) for k in C2_KERNELS}
     ref_slots = O.fixed_slots(V, E, cl, Xs, hs)
     return dict(loops=loops, h=h, rows=rows, special=spec, sub=sub, ref=ref, slots=slots, ref_slots=ref_slots,
-                ind=ind, gpu_ind=ft.ind[rt].cpu().numpy(), npairs=npairs)
+                ind=ind, gpu_ind=ft.ind[rt].cpu().numpy(), npairs=npairs, X=X)
 
 
 def test_c2_neighbour_slots_bit_exact_at_full_size(c2_run):
@@ -251,3 +251,51 @@ def test_c4_gradients_at_full_size():
             Vm[k, c] -= step
             fd = (loss(X, Vp) - loss(X, Vm)) / (2 * step)
             assert abs(fd - gv[k, c]) < 1e-6 * sv, (k, c, fd, gv[k, c])
+
+
+def test_c2_row_sums_agree_with_correctly_rounded_sums(c2_run):
+    """the device sums each row's pair channels in a fixed order without compensation (the reference sums with Kahan /
+    Neumaier compensation, fluxbridge/evaluate.py:177-187, wp_func.py:335-356).  On the 400 subset rows with the
+    most neighbour pairs, the fused float64 pass's channels stay within 4e-15 (natural units) of the correctly
+    rounded sum (math.fsum) of the same closed form's per-pair channels (wsb_pair_channels) plus the indicator term:
+    the uncompensated sum of these bounded terms loses nothing a compensated one would keep."""
+    import ctypes
+    import math
+    from oracle import edge2d as O2
+    from warpsphboundaries_b200 import _lib
+    from warpsphboundaries_b200.kernels import KERNEL_IDS
+    from warpsphboundaries_b200.scene import _stream
+    r = c2_run
+    h = r["h"]
+    counts = np.array([len(s) for s in r["ref_slots"]])
+    top = np.argsort(-counts)[:400]
+    assert counts[top].min() >= 8
+    rep = SurfaceRep.loops(r["loops"])
+    lpos = torch.tensor(r["X"][r["rows"][top]], dtype=torch.float64, device=DEV)
+    lsup = torch.full((len(top),), h, dtype=torch.float64, device=DEV)
+    topo = rep.topology(lpos, lsup)
+    qi = topo.qi.to(torch.int32).contiguous()
+    e = topo.e.to(torch.int32).contiguous()
+    P = len(qi)
+    ns = rep.native(h, DEV)
+    worst = 0.0
+    for gi, k in enumerate(C2_KERNELS):
+        c = torch.empty((P, 12), dtype=torch.float64, device=DEV)
+        st = torch.zeros(1, dtype=torch.int32, device=DEV)
+        _lib.check(_lib.lib.wsb_pair_channels(ns.handle, KERNEL_IDS[k], _lib.PREC_FP64, _lib.ptr(qi), _lib.ptr(e), P,
+                                              _lib.ptr(lpos), _lib.ptr(lsup), len(top), _lib.ptr(c), _lib.ptr(st),
+                                              _stream()))
+        cc = c.cpu().numpy()
+        q = qi.cpu().numpy()
+        plane = np.array(O2.plane_channels(k))
+        phys = np.array([1, h, h, 1 / h, 1 / h, 1, 1, 1, 1, h * h, h * h, h * h])
+        exact = np.zeros((len(top), 12))
+        for t in range(len(top)):
+            sel = cc[q == t]
+            w = r["ind"][top[t]]
+            exact[t] = [math.fsum(list(sel[:, j]) + [w * plane[j]]) * phys[j] for j in range(12)]
+        got = twelve_from_world(r["sub"]["fp64"][gi], h)[top]
+        d = np.abs(got - twelve_from_local(exact, h)).max()
+        worst = max(worst, d)
+        assert d < 4e-15, (k, d)
+    print(f"c2 fp64 vs correctly rounded row sums (400 rows with the most pairs): {worst:.1e}")

@@ -141,3 +141,36 @@ def test_lowered_bodies_are_served():
         assert torch.equal(srv.result(rid)[key], fw.res[0][key]), key
     with pytest.raises(NotImplementedError):
         srv.register("disks", Scene([Body(reps=[DiskArrayRep([[0.5, 0.5]], [0.1])])], DEV), h)
+
+
+def test_sphere_rows_in_the_mix_and_per_class_stats():
+    """sphere-row requests (query, sphere) batched with 2-D requests: each equals RadialEvaluator on its rows bit for
+    bit; the statistics report p50 / p99 per request class."""
+    from warpsphboundaries_b200.radial import RadialEvaluator
+    srv = BoundaryServer(DEV, streams=2, max_batch_rows=30000)
+    srv.register_spheres("sph", 0.03)
+    for sid, sc in _scenes().items():
+        srv.register(sid, sc, 0.03)
+    rng = np.random.default_rng(9)
+    ids, want = [], []
+    for i in range(8):
+        n = int(rng.integers(500, 9000))
+        R = np.exp(rng.uniform(np.log(0.006), np.log(1.5), n))
+        d = np.maximum(rng.uniform(-0.036, 0.036, n), -R)
+        nv = rng.normal(size=(n, 3))
+        nv /= np.linalg.norm(nv, axis=1, keepdims=True)
+        k = ["w2", "w4", "w6"][i % 3]
+        rows = torch.tensor(np.concatenate([d[:, None], nv, R[:, None]], 1), dtype=torch.float64, device=DEV)
+        ids.append(srv.submit("sph", rows, 0.03, k))
+        want.append(RadialEvaluator("sphere", kernel=k, device=DEV).evaluate(d, nv, 0.03, radii=R))
+        ids.append(srv.submit("s0", _positions(1000 + i, i), 0.03, "w4", grad=(i % 2 == 0)))
+        want.append(None)
+    srv.run()
+    torch.cuda.synchronize()
+    for rid, ref in zip(ids, want):
+        if ref is not None:
+            assert np.array_equal(srv.result(rid)["channels"].cpu().numpy(), ref)
+    st = srv.stats()
+    assert set(st["classes"]) == {"3d_spheres", "2d", "2d_grad"}
+    assert st["classes"]["3d_spheres"]["requests"] == 8
+    assert all(v["p50_ms"] <= v["p99_ms"] for v in st["classes"].values())

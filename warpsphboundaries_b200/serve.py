@@ -8,6 +8,7 @@
     res = srv.result(rid)        # {"lam": [B, n], "G": [B, n, 2], "Cov": [B, n, 2, 2], "m1": [B, n, 2], "m2": [B, n, 2, 2]
                                  #  (+ "d_pos": [n, 2] with grad=True: the adjoint of sum(lam))}
                                  # closed surfaces: {"channels": [n, 28]} (wsb_mesh_channels order)
+                                 # sphere rows: {"channels": [n, 28]} (baseline(3) order)
 
 Scheduling (one host thread, the caller's):
 * requests queue per (scene, kernel, grad); a batch takes the oldest requests of one queue up to `max_batch_rows`
@@ -16,10 +17,12 @@ Scheduling (one host thread, the caller's):
   pairs are summed in its own fixed order), so a request's result is bit-identical alone and in any mix;
 * batches run on `streams` CUDA streams at once, so requests that arrive while others are on the GPU are admitted as
   stream slots and memory free up, and their work overlaps on the device;
-* with `use_graphs=True`, batches of at most `graph_max_rows` rows replay a CUDA graph captured per (stream, bucket,
-  scene, kernel) over static buffers padded to a power-of-two bucket (padding rows are masked out); a key is captured
-  once it has been launched `graph_after_uses` times, so one-off keys stay eager.  Off by default: a batch is seven
-  launches per surface, and each capture holds its own padded outputs and workspace;
+* with `use_graphs=True` (the default), batches of at most `graph_max_rows` rows replay a CUDA graph captured per
+  (stream, bucket, scene, kernel) over static buffers padded to a power-of-two bucket (padding rows are masked out); a
+  key is captured once it has been launched `graph_after_uses` times, so one-off keys stay eager (each capture holds
+  its own padded outputs and workspace);
+* solid spheres (`register_spheres`): a request is a set of (query, sphere) rows [n, 5] = (signed distance, outward
+  normal, radius) with supports; a batch is one wsb_radial_channels launch over the concatenated rows;
 * nothing is allocated per batch: a request's outputs come from a pool of power-of-two buffers when it is submitted
   (on the caller's stream), a scalar support is a view of a resident vector, a single-request batch writes straight
   into the request's outputs, a multi-request batch into persistent per-stream buffers that are then copied into each
@@ -103,6 +106,19 @@ class _Slot:
             self.cap3 = cap
         return self.buf3
 
+    def buffers_sph(self, rows):
+        """persistent buffers of a sphere batch: rows [cap, 5], supports, channels [cap, 28], invariants, status."""
+        if getattr(self, "bufs", None) is None or rows > self.caps:
+            cap = max(rows, int(1.5 * getattr(self, "caps", 0)), 1 << 16)
+            with torch.cuda.stream(self.stream):
+                self.bufs = {"rows": torch.empty((cap, 5), dtype=F64, device=self.device),
+                             "sup": torch.empty(cap, dtype=F64, device=self.device),
+                             "chan": torch.empty((cap, 28), dtype=F64, device=self.device),
+                             "work": torch.empty((cap, 9), dtype=F64, device=self.device),
+                             "status": torch.empty(cap, dtype=torch.int32, device=self.device)}
+            self.caps = cap
+        return self.bufs
+
     def buffers(self, rows, B):
         """persistent batch buffers for `rows` rows of a B-body scene (grown geometrically, allocated on this stream)."""
         if self.buf is None or rows > self.cap or B > self.B:
@@ -120,7 +136,7 @@ class _Slot:
 
 
 class BoundaryServer:
-    def __init__(self, device="cuda:0", streams=4, max_batch_rows=1 << 20, hbm_budget=None, use_graphs=False,
+    def __init__(self, device="cuda:0", streams=4, max_batch_rows=1 << 20, hbm_budget=None, use_graphs=True,
                  graph_max_rows=1 << 16, precision="fp64", graph_after_uses=4, pool_limit=None):
         self.device = torch.device(device)
         self.scenes: Dict[str, tuple] = {}
@@ -180,8 +196,26 @@ class BoundaryServer:
         self.plans[scene_id] = None
         self.ws_bytes = max(self.ws_bytes, int(lib.wsb_mesh_workspace_size(mesh.handle, self.max_batch_rows)))
 
+    def register_spheres(self, scene_id, support):
+        """a resident solid-sphere scene (3-D): requests are (query, sphere) rows [n, 5] = (signed outward distance
+        |x - c| - R, unit outward normal, radius R) and return the 28 baseline channels per row
+        (fluxbridge RadialEvaluator("sphere"), float64)."""
+        self.scenes[scene_id] = ("spheres", float(support))
+        self.plans[scene_id] = "spheres"
+
     def _is_mesh(self, scene_id):
         return self.plans.get(scene_id, ()) is None
+
+    def _is_spheres(self, scene_id):
+        return self.plans.get(scene_id, ()) == "spheres"
+
+    def _cls(self, r):
+        """the request class of the per-class latency report."""
+        if self._is_mesh(r.scene_id):
+            return "3d_surface"
+        if self._is_spheres(r.scene_id):
+            return "3d_spheres"
+        return "2d_grad" if r.grad else "2d"
 
     # ------------------------------------------------------------------ requests
     def submit(self, scene_id, positions, supports, kernel, grad=False, arrival=None):
@@ -196,7 +230,7 @@ class BoundaryServer:
             sup = self._support_vec(float(supports), len(pos))
         r = Request(next(self._ids), scene_id, kname, pos, sup, bool(grad),
                     time.perf_counter() if arrival is None else arrival)
-        if self._is_mesh(scene_id):
+        if self._is_mesh(scene_id) or self._is_spheres(scene_id):
             return self._submit_mesh(r)
         B, n = len(self.scenes[scene_id][0].bodies), len(pos)
         nbytes = 8 * (13 * B * n + (2 * n if r.grad else 0))
@@ -222,9 +256,10 @@ class BoundaryServer:
 
     def _submit_mesh(self, r):
         if r.grad:
-            raise NotImplementedError("BoundaryServer: closed surfaces serve the channels, not the adjoint")
-        if r.pos.dim() != 2 or r.pos.shape[1] != 3:
-            raise ValueError("BoundaryServer: closed-surface requests take positions [n, 3]")
+            raise NotImplementedError("BoundaryServer: 3-D scenes serve the channels, not the adjoint")
+        width = 5 if self._is_spheres(r.scene_id) else 3
+        if r.pos.dim() != 2 or r.pos.shape[1] != width:
+            raise ValueError(f"BoundaryServer: this scene's requests take rows [n, {width}]")
         n = len(r.pos)
         nbytes = 8 * 28 * n
         while self.held_bytes + nbytes > self.hbm_budget and (self.n_queued or self.n_inflight):
@@ -275,6 +310,8 @@ class BoundaryServer:
 
     # ------------------------------------------------------------------ bytes a batch holds on the device
     def _bytes(self, scene, support, rows, grad):
+        if isinstance(scene, str):                                    # sphere rows
+            return (8 * 28 + 8 * 6 + 8 * 9 + 4) * rows
         if not hasattr(scene, "bodies"):                              # a closed surface
             return (8 * 28 + 32) * rows + int(lib.wsb_mesh_workspace_size(scene.handle, rows))
         B = len(scene.bodies)
@@ -377,9 +414,52 @@ class BoundaryServer:
             ev.record(slot.stream)
         slot.busy = _Batch(reqs, rows, need, ev, ev0)
 
+    def _launch_spheres(self, si, reqs, rows, support, need):
+        """one wsb_radial_channels launch over the concatenated sphere rows of the batch."""
+        slot = self.slots[si]
+        if self.t_first is None:
+            self.t_first = time.perf_counter()
+        slot.stream.wait_stream(torch.cuda.current_stream(self.device))
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev0.record(slot.stream)
+        with torch.cuda.stream(slot.stream):
+            buf = slot.buffers_sph(rows)
+            off = 0
+            for r in reqs:
+                n = len(r.pos)
+                buf["rows"][off:off + n].copy_(r.pos)
+                buf["sup"][off:off + n].copy_(r.sup)
+                off += n
+            rw = buf["rows"][:rows]
+            d = rw[:, 0].contiguous()
+            nrm = rw[:, 1:4].contiguous()
+            rad = rw[:, 4].contiguous()
+            out = buf["chan"][:rows]
+            check(lib.wsb_radial_channels(_lib.RADIAL_SPHERE, KERNEL_IDS[reqs[0].kernel], _lib.PREC_FP64, ptr(d),
+                                          ptr(rad), ptr(nrm), ptr(buf["sup"]), rows, self._radial_meta(),
+                                          28, ptr(out), ptr(buf["work"]), ptr(buf["status"]),
+                                          _lib.ctypes.c_void_p(slot.stream.cuda_stream)), "wsb_radial_channels")
+            off = 0
+            for r in reqs:
+                n = len(r.pos)
+                r.result["channels"].copy_(out[off:off + n])
+                off += n
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record(slot.stream)
+        slot.busy = _Batch(reqs, rows, need, ev, ev0)
+
+    def _radial_meta(self):
+        if getattr(self, "_meta", None) is None:
+            from .radial import RadialEvaluator
+            self._meta_ev = RadialEvaluator("sphere", kernel="w2", device=self.device)
+            self._meta = self._meta_ev.metadata.ctypes.data_as(_lib.ctypes.POINTER(_lib.ctypes.c_int32))
+        return self._meta
+
     def _launch(self, si, reqs, rows, scene, support, need):
         if self._is_mesh(reqs[0].scene_id):
             return self._launch_mesh(si, reqs, rows, scene, need)
+        if self._is_spheres(reqs[0].scene_id):
+            return self._launch_spheres(si, reqs, rows, support, need)
         slot = self.slots[si]
         kname, grad = reqs[0].kernel, reqs[0].grad
         B = len(scene.bodies)
@@ -511,6 +591,11 @@ class BoundaryServer:
         if len(lat):
             out.update(p50_ms=float(np.percentile(lat, 50)), p99_ms=float(np.percentile(lat, 99)),
                        mean_ms=float(lat.mean()), max_ms=float(lat.max()))
+        classes = {}
+        for r in self.completed:
+            classes.setdefault(self._cls(r), []).append((r.done - r.arrival) * 1e3)
+        out["classes"] = {c: {"requests": len(v), "p50_ms": float(np.percentile(v, 50)),
+                              "p99_ms": float(np.percentile(v, 99))} for c, v in sorted(classes.items())}
         if self.t_first is not None and self.t_last is not None:
             out["wall_s"] = self.t_last - self.t_first
         if self.intervals:
