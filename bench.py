@@ -48,7 +48,8 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64", "fp32"])
+    p.add_argument("--precision", default="fp64", choices=["mixed", "fp64", "fp32"],
+                   help="route of the headline (fp64: the one within 1e-6 relative of the oracle at full size)")
     p.add_argument("--route", default="fused", choices=["fused", "plain"])
     p.add_argument("--particles", type=int, default=1 << 20)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -807,14 +808,24 @@ def our_arm(args):
                "ms_per_step": tot / args.steps, "pipelined": True,
                "sequential": {"value": job_pairs_step * args.steps / (seq * 1e-3), "ms_per_step": seq / args.steps}}
 
-    radial = radial_run(dev, stream, flush) if world == 1 else None
-    detector = detector_run(ns, pos, sup, pose, obb, ws, need, P, stream, flush) if world == 1 else None
-    disks = disk_run(dev, stream, flush) if world == 1 else None
-    mesh = mesh_run(dev, stream, flush, n_particles=args.mesh_particles) if world == 1 and not args.no_mesh else None
+    def side(fn, *a, **k):
+        """a side leg: its result, or its error as one line (a failing side leg never takes the headline line down)"""
+        try:
+            return fn(*a, **k)
+        except Exception as exc:                                   # noqa: BLE001 -- reported in the JSON line
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            return {"error": f"{type(exc).__name__}: {str(exc)[:300]}"}
+
+    radial = side(radial_run, dev, stream, flush) if world == 1 else None
+    detector = side(detector_run, ns, pos, sup, pose, obb, ws, need, P, stream, flush) if world == 1 else None
+    disks = side(disk_run, dev, stream, flush) if world == 1 else None
+    mesh = side(mesh_run, dev, stream, flush, n_particles=args.mesh_particles) if world == 1 and not args.no_mesh \
+        else None
 
     serving = None
     if rank == 0 and world == 1 and args.serve_requests > 0:
-        serving = serving_run(args.serve_requests, dev, P / N)
+        serving = side(serving_run, args.serve_requests, dev, P / N)
 
     cpu = None
     if cpu_ref is not None:

@@ -131,7 +131,7 @@ def test_out_of_range_indices_are_refused_without_a_read():
     w = torch.zeros((4, 3), dtype=torch.float64, device=dev)
     G = torch.zeros((4, 3, 2), dtype=torch.float64, device=dev)
     st = torch.zeros(1, dtype=torch.int32, device=dev)
-    _lib.check(_lib.lib.wsb_pair_weights(2, _lib.ptr(q), _lib.ptr(e), 4, _lib.ptr(pos), _lib.ptr(sup), 2, _lib.ptr(Vt),
+    _lib.check(_lib.lib.wsb_pair_weights(1, _lib.ptr(q), _lib.ptr(e), 4, _lib.ptr(pos), _lib.ptr(sup), 2, _lib.ptr(Vt),
                                          len(V), _lib.ptr(Et), len(E), _lib.ptr(w), _lib.ptr(G), _lib.ptr(st),
                                          _lib.ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
     torch.cuda.synchronize()

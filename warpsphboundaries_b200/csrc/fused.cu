@@ -575,8 +575,9 @@ __device__ __forceinline__ void pack_finish(const double* acc_t, bool write, int
       for (int c = 0; c < 12; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
     }
     if (write) {
+      // a rounded multiply of its own (no contraction with the indicator terms), as the staged path stores the sums
 #pragma unroll
-      for (int c = 0; c < 12; ++c) acc[c] *= kInvPi;
+      for (int c = 0; c < 12; ++c) acc[c] = __dmul_rn(acc[c], kInvPi);
       if constexpr (KT::kQuad)
         finish_row_quad(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
       else
@@ -601,7 +602,7 @@ __device__ __forceinline__ void pack_stage(const double* acc_t, bool write, doub
     if (write) {
       double2* d2 = reinterpret_cast<double2*>(dst + K * 12);
 #pragma unroll
-      for (int c = 0; c < 6; ++c) d2[c] = make_double2(acc[2 * c] * kInvPi, acc[2 * c + 1] * kInvPi);
+      for (int c = 0; c < 6; ++c) d2[c] = make_double2(__dmul_rn(acc[2 * c], kInvPi), __dmul_rn(acc[2 * c + 1], kInvPi));
     }
     pack_stage<Pack, G, K + 1>(acc_t, write, dst);
   }

@@ -12,8 +12,9 @@ tests/fixtures/fluxbridge-v1.json); `load` / `dump` keep every field as written,
   requests: value moments |alpha| <= 2, kernel-gradient moments |alpha| <= 1, the kernel Hessian);
 * a 2-D triangle (volume) through `FusedWall` on the triangle as a polygon (value moments |alpha| <= 2 and the
   kernel-gradient moments |alpha| <= 1: lam, m1, m2, G, Cov);
-and gives NaN for requests outside those sets (higher degrees, the 2-D Hessian); 3-D surface triangles raise
-NotImplementedError (no surface-measure route on the device).
+and gives NaN for requests outside those sets (higher degrees, the 2-D Hessian) and for a tetrahedron whose query lies
+on its boundary (the closed-surface route takes such a query as inside or outside by a ray-parity rule; the reference
+uses the solid-angle fraction); 3-D surface triangles raise NotImplementedError (no surface-measure route).
 """
 import json
 from dataclasses import dataclass, field
@@ -122,11 +123,35 @@ _TWO_D = {((0, 0), ()): ("lam", ()), ((1, 0), ()): ("m1", (0,)), ((0, 1), ()): (
           ((0, 1), (0,)): ("Cov", (1, 0)), ((0, 1), (1,)): ("Cov", (1, 1))}
 
 
+def _on_tet_boundary(case: Case):
+    """the query lies on the tetrahedron's boundary (a face, an edge or a vertex), decided exactly from the file's
+    decimal strings: there the closed-surface route takes the query as inside or outside by its ray-parity rule, where
+    the reference's solid angle gives the fraction of the surrounding sphere inside the solid."""
+    from fractions import Fraction
+    P = [[Fraction(str(x)) for x in v] for v in case.vertices]
+    q = [Fraction(str(x)) for x in case.query]
+
+    def vol(a, b, c, d):
+        u = [b[i] - a[i] for i in range(3)]
+        v = [c[i] - a[i] for i in range(3)]
+        w = [d[i] - a[i] for i in range(3)]
+        return (u[0] * (v[1] * w[2] - v[2] * w[1]) - u[1] * (v[0] * w[2] - v[2] * w[0]) +
+                u[2] * (v[0] * w[1] - v[1] * w[0]))
+    s = []
+    for i in range(4):
+        f = [P[j] for j in range(4) if j != i]
+        ref = vol(*f, P[i])
+        s.append(vol(*f, q) * (1 if ref > 0 else -1))      # >= 0: on the tetrahedron's side of face i
+    return all(x >= 0 for x in s) and any(x == 0 for x in s)
+
+
 def served(case: Case):
     """which of the case's requests the device routes compute (bool per request)."""
     if case.measure != "volume":
         return [False] * len(case.requests)
     if case.dimension == 3:
+        if _on_tet_boundary(case):
+            return [False] * len(case.requests)
         return [c is not None for c in _tet_columns(case.requests)]
     return [(r.alpha, r.derivative) in _TWO_D for r in case.requests]
 
@@ -140,7 +165,7 @@ def evaluate(case: Case, device="cuda"):
     P, x, h = case.points, case.x, case.support
     if case.dimension == 3:
         from .mesh3d import Evaluator, Geometry
-        cols = _tet_columns(case.requests)
+        cols = _tet_columns(case.requests) if not _on_tet_boundary(case) else [None] * len(case.requests)
         g = Geometry.from_elements([P])
         vals = Evaluator(g, None, kernel=case.kernel, device=device).evaluate(x[None], h)[0]
         for i, c in enumerate(cols):

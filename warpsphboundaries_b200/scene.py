@@ -280,7 +280,15 @@ class SurfaceRep:
             check(lib.wsb_pair_channels(ns.handle, kid, _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64,
                                         ptr(qi), ptr(e), P, ptr(lp), ptr(ls), C, ptr(c), ptr(st), _stream()),
                   "wsb_pair_channels")
-            out.index_add_(0, qi.long(), c)
+            # per-query sums in pair order (deterministic, unlike an atomic index_add): the pairs of a query are
+            # contiguous (rows ascending), laid out [query, rank, 12] and reduced over the rank
+            q = qi.long()
+            cnt = torch.bincount(q, minlength=C)
+            start = torch.cumsum(cnt, 0) - cnt
+            rank = torch.arange(P, device=dev) - start[q]
+            pad = torch.zeros((C, int(cnt.max()), 12), dtype=F64, device=dev)
+            pad[q, rank] = c
+            out = pad.sum(1)
         estimate = torch.zeros((C, 12), dtype=F64, device=dev)
         status = torch.zeros(C, dtype=torch.int32, device=dev)
         if quad:

@@ -19,8 +19,8 @@ Scheduling (one host thread, the caller's):
   stream slots and memory free up, and their work overlaps on the device;
 * with `use_graphs=True` (the default), batches of at most `graph_max_rows` rows replay a CUDA graph captured per
   (stream, bucket, scene, kernel) over static buffers padded to a power-of-two bucket (padding rows are masked out); a
-  key is captured once it has been launched `graph_after_uses` times, so one-off keys stay eager (each capture holds
-  its own padded outputs and workspace);
+  key is captured once it has been launched `graph_after_uses` times, so one-off keys stay eager; each capture holds
+  its own padded outputs and workspace, and captures stop once they hold `graph_budget` bytes;
 * solid spheres (`register_spheres`): a request is a set of (query, sphere) rows [n, 5] = (signed distance, outward
   normal, radius) with supports; a batch is one wsb_radial_channels launch over the concatenated rows;
 * nothing is allocated per batch: a request's outputs come from a pool of power-of-two buffers when it is submitted
@@ -137,7 +137,8 @@ class _Slot:
 
 class BoundaryServer:
     def __init__(self, device="cuda:0", streams=4, max_batch_rows=1 << 20, hbm_budget=None, use_graphs=True,
-                 graph_max_rows=1 << 16, precision="fp64", graph_after_uses=4, pool_limit=None):
+                 graph_max_rows=1 << 16, precision="fp64", graph_after_uses=4, pool_limit=None,
+                 graph_budget=2 << 30):
         self.device = torch.device(device)
         self.scenes: Dict[str, tuple] = {}
         self.queues: Dict[tuple, List[Request]] = {}
@@ -151,6 +152,8 @@ class BoundaryServer:
         self.graph_after_uses = int(graph_after_uses)
         self.precision = precision
         self.graphs = {}
+        self.graph_budget = int(graph_budget)  # device bytes all captured graphs may hold (their outputs, workspaces)
+        self.graph_bytes = 0
         self.uses = {}
         self.requests: Dict[int, Request] = {}
         self._ids = itertools.count()
@@ -489,8 +492,8 @@ class BoundaryServer:
                 self.uses[gkey] = self.uses.get(gkey, 0) + 1
                 if gkey not in self.graphs and self.uses[gkey] < self.graph_after_uses:
                     gkey = None
-            if gkey is not None:
-                self._graph_run(slot, gkey, plan, support, kname, pos, sup, rows, outs)
+            if gkey is not None and self._graph_run(slot, gkey, plan, support, kname, pos, sup, rows, outs):
+                pass
             else:
                 self._aggregate(plan, kname, pos, sup, None, rows, outs, slot.workspace(self.ws_bytes),
                                 slot.stream)
@@ -556,10 +559,15 @@ class BoundaryServer:
         spos, ssup, sall = st
         g = self.graphs.get(key)
         if g is None:
-            sall.fill_(1)
-            # graph-owned workspace and outputs: a captured graph keeps its pointers, so they are never freed
+            # graph-owned workspace and outputs: a captured graph keeps its pointers, so they are never freed; a
+            # capture that would take the graphs past `graph_budget` is not made (the batch runs eagerly)
             need = max(int(lib.wsb_aggregate_workspace_size(ns.handle, bucket)) + int(lib.wsb_aggregate_staging_size(ns.handle, bucket))
                        for _, _, _, reps in plan for ns in reps)
+            gbytes = need + 8 * 13 * B * bucket
+            if self.graph_bytes + gbytes > self.graph_budget:
+                return False
+            self.graph_bytes += gbytes
+            sall.fill_(1)
             ws = torch.empty(need, dtype=torch.uint8, device=self.device)
             gout = {k: torch.empty((B, bucket) + _TAIL[k], dtype=F64, device=self.device) for k in OUT_KEYS}
             self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)     # eager warm-up
@@ -583,6 +591,7 @@ class BoundaryServer:
         graph.replay()
         for k in OUT_KEYS:
             outs[k].copy_(gout[k][:, :rows])
+        return True
 
     # ------------------------------------------------------------------ statistics
     def stats(self):
