@@ -129,6 +129,10 @@ size_t wsb_aggregate_workspace_size(const wsb_surface* s, int64_t n);
  * rows' outputs scattered by row index.  The results are the same bits either way.  No counterpart in the reference
  * (a layout choice of this implementation). */
 size_t wsb_aggregate_staging_size(const wsb_surface* s, int64_t n);
+/* Instrumentation: while set, every fused pair pass records `start` (a cudaEvent_t) on its stream right before its pair
+ * kernel and `end` right after it, so a profiler or benchmark can time that kernel alone; NULL, NULL clears them.  The
+ * events are the caller's.  No counterpart in the reference. */
+int wsb_set_pair_events(void* start, void* end);
 
 /* Fused route: body-frame coordinates (Pose.toLocal), the body broadphase (support circle against the body box
  * [obb_lo, obb_hi]; unbounded != 0 skips it), the fixed-capacity neighbour predicate, the twelve channels of every

@@ -55,6 +55,8 @@ def test_device_matches_the_stored_values():
         ref = c.reference()
         ok = np.array(fx.served(c))
         assert np.isnan(got[~ok]).all()
+        if not ok.any():
+            continue
         err = np.abs(got[ok] - ref[ok]) / (1 + np.abs(ref[ok]))
         worst = max(worst, float(err.max()))
         n += int(ok.sum())

@@ -18,7 +18,7 @@ OUT_LAM, OUT_G, OUT_COV, OUT_M1, OUT_M2, OUT_ALL, OUT_ASSIGN = 1, 2, 4, 8, 16, 3
 
 EXPORTS = ["wsb_last_error", "wsb_version", "wsb_surface_create", "wsb_surface_destroy", "wsb_surface_info_get",
            "wsb_surface_cells", "wsb_fixed_topology", "wsb_slot_channels_plain", "wsb_contract",
-           "wsb_aggregate_workspace_size", "wsb_aggregate_staging_size", "wsb_aggregate", "wsb_aggregate_prepare", "wsb_aggregate_evaluate",
+           "wsb_aggregate_workspace_size", "wsb_aggregate_staging_size", "wsb_set_pair_events", "wsb_aggregate", "wsb_aggregate_prepare", "wsb_aggregate_evaluate",
            "wsb_aggregate_evaluate_groups", "wsb_aggregate_groups", "wsb_aggregate_noalloc",
            "wsb_aggregate_backward", "wsb_cone_area", "wsb_dir_extreme", "wsb_signed_distance",
            "wsb_kinematics", "wsb_radial_channels", "wsb_mesh_create", "wsb_mesh_destroy",
@@ -56,6 +56,7 @@ def _load():
         "wsb_contract": (c_int, [P, c_int, P, P, P, P, c_int64, P, P, P, P, P, P, P]),
         "wsb_aggregate_workspace_size": (c_size_t, [P, c_int64]),
         "wsb_aggregate_staging_size": (c_size_t, [P, c_int64]),
+        "wsb_set_pair_events": (c_int, [P, P]),
         "wsb_aggregate": (c_int, [P, c_int, c_int, P, P, P, c_int64, P, D, c_int, c_int, P, P, P, P, P, P, c_size_t,
                                   P, P]),
         "wsb_aggregate_prepare": (c_int, [P, P, P, P, c_int64, P, D, c_int, P, c_size_t, P]),

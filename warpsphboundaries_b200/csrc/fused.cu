@@ -766,6 +766,10 @@ __global__ void __launch_bounds__(kThreads) k_agg_expand(const double* __restric
 // the pair kernel of a pack over a prepared workspace (two lanes per work row: measured fastest on the 2^20-particle
 // scene, 1 / 2 lanes give 10.4 / 11.3e9 pairs/s with one kernel, 1 / 2 / 4 lanes 0.448 / 0.421 / 0.471 ms for the
 // four-kernel pack, which also beat the four kernels as two two-kernel packs, 0.426 ms)
+// instrumentation: events recorded on the launching stream right before and after each fused pair kernel (set by
+// wsb_set_pair_events; NULL: none)
+static cudaEvent_t g_pair_ev[2] = {nullptr, nullptr};
+
 template <class Pack>
 constexpr size_t pack_smem_bytes() {
   return sizeof(double4) * kThreads + sizeof(double) * Pack::kN * 12 * kThreads;
@@ -791,7 +795,9 @@ static int launch_pack(const SurfView& v, const double* sup, const Workspace& w,
   }
   const unsigned rows = (unsigned)((n + kThreads - 1) / kThreads);
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads) + (staged ? 0u : rows);
+  if (g_pair_ev[0]) WSB_CUDA(cudaEventRecord(g_pair_ev[0], st));
   kern<<<grid, kThreads, smem, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, out, w.wacc);
+  if (g_pair_ev[1]) WSB_CUDA(cudaEventRecord(g_pair_ev[1], st));
   if (staged) k_agg_expand<Pack><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
   return WSB_OK;
 }
@@ -1356,6 +1362,13 @@ extern "C" size_t wsb_aggregate_workspace_size(const wsb_surface* s_, int64_t n)
   const Surface* s = reinterpret_cast<const Surface*>(s_);
   if (!s || n < 0) return 0;
   return carve(s, n, nullptr).total;
+}
+
+extern "C" int wsb_set_pair_events(void* start, void* end) {
+  if ((start == nullptr) != (end == nullptr)) return fail(WSB_ERR_ARG, "wsb_set_pair_events: both events or neither");
+  g_pair_ev[0] = (cudaEvent_t)start;
+  g_pair_ev[1] = (cudaEvent_t)end;
+  return WSB_OK;
 }
 
 extern "C" size_t wsb_aggregate_staging_size(const wsb_surface* s_, int64_t n) {
