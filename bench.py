@@ -596,8 +596,8 @@ def our_arm(args):
                 _lib.check(_lib.lib.wsb_set_pair_events(None, None))
             b = torch.cuda.Event(enable_timing=True)
             b.record(stream)
-            ev.append(("groups", a, b))
             ev.append(("pairs", p0, p1))
+            ev.append(("groups", a, b))                     # last: a step ends with the whole evaluation
             if timers is not None:
                 timers.append(ev)
             return

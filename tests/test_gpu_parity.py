@@ -189,9 +189,12 @@ def test_golden_elements_on_gpu():
 
 @pytest.mark.parametrize("kernels", [("w4",), ("cubic", "w2", "w4", "w6"), ("w2", "cone", "lw2")])
 @pytest.mark.parametrize("assign", [True, False])
-def test_staged_and_direct_evaluation_agree(c2s, kernels, assign):
+@pytest.mark.parametrize("offset", [0, 1, 2])
+def test_staged_and_direct_evaluation_agree(c2s, kernels, assign, offset):
     """a workspace with the staging region (work rows' sums staged, every row expanded in one coalesced pass) and one
-    without it (work rows' outputs stored directly) give the same bits, for one kernel and for packs."""
+    without it (work rows' outputs stored directly) give the same bits, for one kernel and for packs; outputs that
+    start 8 bytes off a 16-byte boundary (offset 1) take the expansion's scalar stores, 16 bytes off a 32-byte one
+    (offset 2) its 16-byte stores, aligned ones its 32-byte stores."""
     import ctypes
     from warpsphboundaries_b200 import _lib
     from warpsphboundaries_b200.kernels import KERNEL_IDS
@@ -211,7 +214,8 @@ def test_staged_and_direct_evaluation_agree(c2s, kernels, assign):
     res = []
     for nbytes in (base, full):
         ws = torch.empty(nbytes, dtype=torch.uint8, device=DEV)
-        outs = [[torch.full((n * w,), 0.25, dtype=torch.float64, device=DEV) for _ in kernels] for w in (1, 2, 4, 2, 4)]
+        outs = [[torch.full((n * w + 1,), 0.25, dtype=torch.float64, device=DEV)[offset:offset + n * w]
+                 for _ in kernels] for w in (1, 2, 4, 2, 4)]
         _lib.check(_lib.lib.wsb_aggregate_groups(ns.handle, len(kernels), kids, _lib.PREC_FP64, _lib.ptr(pos),
                                                  _lib.ptr(sup), None, n, _lib.ptr(pose), obb, 0, mode,
                                                  *[_lib.ptrs(o) for o in outs], _lib.ptr(ws), nbytes, _stream()))

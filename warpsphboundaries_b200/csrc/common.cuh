@@ -439,35 +439,73 @@ __device__ __forceinline__ void put(double* p, double v, bool assign) {
     *p += v;
 }
 
+// two consecutive outputs by one 16-byte store (p 16-byte aligned), assigned or added
+__device__ __forceinline__ void put2(double* p, double a, double b, bool assign) {
+  double2* q = reinterpret_cast<double2*>(p);
+  if (assign) {
+    *q = make_double2(a, b);
+  } else {
+    const double2 o = *q;
+    *q = make_double2(o.x + a, o.y + b);
+  }
+}
+
+// four consecutive outputs by one 32-byte store (p 32-byte aligned: st.global.v4.f64, sm_100), assigned or added
+__device__ __forceinline__ void put4(double* p, double a, double b, double c, double d, bool assign) {
+  if (!assign) {
+    const double2 o0 = reinterpret_cast<const double2*>(p)[0], o1 = reinterpret_cast<const double2*>(p)[1];
+    a = o0.x + a;
+    b = o0.y + b;
+    c = o1.x + c;
+    d = o1.y + d;
+  }
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+
+// VEC 0: scalar stores; 1: the pairs of G, m1, cov, m2 as 16-byte stores (pointers 16-byte aligned); 2: also the four
+// values of cov and m2 as one 32-byte store (cov, m2 32-byte aligned), so every store of a warp writes whole sectors.
+// The values are the same in every mode.
+template <int VEC = 0>
 __device__ __forceinline__ void write_outputs(const double ch[12], double h, const double* rot, int64_t r, double* lam,
                                               double* G, double* cov, double* m1, double* m2, bool assign = false) {
   const double R00 = rot[0], R01 = rot[1], R10 = rot[2], R11 = rot[3];
+  auto put_pair = [&](double* p, double a, double b) {
+    if constexpr (VEC > 0) {
+      put2(p, a, b, assign);
+    } else {
+      put(p, a, assign);
+      put(p + 1, b, assign);
+    }
+  };
+  auto put_quad = [&](double* p, double a, double b, double c, double d) {
+    if constexpr (VEC > 1) {
+      put4(p, a, b, c, d, assign);
+    } else {
+      put_pair(p, a, b);
+      put_pair(p + 2, c, d);
+    }
+  };
   if (lam) put(&lam[r], ch[0], assign);
   if (m1) {
     const double vx = h * ch[1], vy = h * ch[2];
-    put(&m1[2 * r], R00 * vx + R01 * vy, assign);
-    put(&m1[2 * r + 1], R10 * vx + R11 * vy, assign);
+    put_pair(&m1[2 * r], R00 * vx + R01 * vy, R10 * vx + R11 * vy);
   }
   if (G) {
     const double vx = ch[3] / h, vy = ch[4] / h;
-    put(&G[2 * r], R00 * vx + R01 * vy, assign);
-    put(&G[2 * r + 1], R10 * vx + R11 * vy, assign);
+    put_pair(&G[2 * r], R00 * vx + R01 * vy, R10 * vx + R11 * vy);
   }
   if (cov) {
     const double a = ch[5], b = ch[6], c = ch[7], d = ch[8];
-    put(&cov[4 * r + 0], R00 * (a * R00 + b * R01) + R01 * (c * R00 + d * R01), assign);
-    put(&cov[4 * r + 1], R00 * (a * R10 + b * R11) + R01 * (c * R10 + d * R11), assign);
-    put(&cov[4 * r + 2], R10 * (a * R00 + b * R01) + R11 * (c * R00 + d * R01), assign);
-    put(&cov[4 * r + 3], R10 * (a * R10 + b * R11) + R11 * (c * R10 + d * R11), assign);
+    put_quad(&cov[4 * r], R00 * (a * R00 + b * R01) + R01 * (c * R00 + d * R01),
+             R00 * (a * R10 + b * R11) + R01 * (c * R10 + d * R11), R10 * (a * R00 + b * R01) + R11 * (c * R00 + d * R01),
+             R10 * (a * R10 + b * R11) + R11 * (c * R10 + d * R11));
   }
   if (m2) {
     const double hh = h * h;
     const double xx = ch[9] * hh, xy = ch[10] * hh, yy = ch[11] * hh;
-    put(&m2[4 * r + 0], R00 * R00 * xx + 2.0 * R00 * R01 * xy + R01 * R01 * yy, assign);
     const double off = R00 * R10 * xx + (R00 * R11 + R01 * R10) * xy + R01 * R11 * yy;
-    put(&m2[4 * r + 1], off, assign);
-    put(&m2[4 * r + 2], off, assign);
-    put(&m2[4 * r + 3], R10 * R10 * xx + 2.0 * R10 * R11 * xy + R11 * R11 * yy, assign);
+    put_quad(&m2[4 * r], R00 * R00 * xx + 2.0 * R00 * R01 * xy + R01 * R01 * yy, off, off,
+             R10 * R10 * xx + 2.0 * R10 * R11 * xy + R11 * R11 * yy);
   }
 }
 

@@ -280,6 +280,7 @@ __global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const doub
   if (ckey >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&khist[ckey], __popc(peers));
 }
 
+template <int VEC = 0>
 __device__ __forceinline__ void finish_row(double acc[12], double ind, double mass, double plane2, double h,
                                            const double* pose, int64_t i, bool assign, double* lam, double* G,
                                            double* cov, double* m1, double* m2) {
@@ -290,7 +291,7 @@ __device__ __forceinline__ void finish_row(double acc[12], double ind, double ma
   acc[11] += ind * plane2;
   const double c = pose[2], s = pose[3];
   const double rot[4] = {c, -s, s, c};
-  write_outputs(acc, h, rot, i, lam, G, cov, m1, m2, assign);
+  write_outputs<VEC>(acc, h, rot, i, lam, G, cov, m1, m2, assign);
 }
 
 // ------------------------------------------------------------------------------------------------ kernel packs
@@ -521,6 +522,7 @@ __device__ __forceinline__ void pack_pair_f32(const PairGeo& g, double* acc_t) {
 
 // the outputs of a row of a quadrature kernel: its gradient channels G (scaled, rotated); the other outputs are not
 // defined for it and are written as NaN
+template <int VEC = 0>
 __device__ __forceinline__ void finish_row_quad(const double acc[12], double h, const double* pose, int64_t i,
                                                 bool assign, double* lam, double* G, double* cov, double* m1,
                                                 double* m2) {
@@ -528,8 +530,12 @@ __device__ __forceinline__ void finish_row_quad(const double acc[12], double h, 
   if (lam) put(&lam[i], nan, assign);
   if (G) {
     const double vx = acc[3] / h, vy = acc[4] / h;
-    put(&G[2 * i], c * vx - s * vy, assign);
-    put(&G[2 * i + 1], s * vx + c * vy, assign);
+    if constexpr (VEC > 0) {
+      put2(&G[2 * i], c * vx - s * vy, s * vx + c * vy, assign);
+    } else {
+      put(&G[2 * i], c * vx - s * vy, assign);
+      put(&G[2 * i + 1], s * vx + c * vy, assign);
+    }
   }
   for (int k = 0; k < 4; ++k) {
     if (cov) put(&cov[4 * i + k], nan, assign);
@@ -543,7 +549,7 @@ __device__ __forceinline__ void finish_row_quad(const double acc[12], double h, 
 
 // a row without neighbour pairs, every kernel of the pack: the indicator w times the whole-plane channels (w = 0 for
 // a non-candidate when the outputs are assigned)
-template <class Pack, int K>
+template <class Pack, int K, int VEC = 0>
 __device__ __forceinline__ void pack_constant_row(int64_t i, double w, double h, const double* pose, bool assign,
                                                   const PackOut& o) {
   if constexpr (K < Pack::kN) {
@@ -552,10 +558,11 @@ __device__ __forceinline__ void pack_constant_row(int64_t i, double w, double h,
 #pragma unroll
     for (int c = 0; c < 12; ++c) acc[c] = 0.0;
     if constexpr (KT::kQuad)
-      finish_row_quad(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+      finish_row_quad<VEC>(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
     else
-      finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
-    pack_constant_row<Pack, K + 1>(i, w, h, pose, assign, o);
+      finish_row<VEC>(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K],
+                      o.m2[K]);
+    pack_constant_row<Pack, K + 1, VEC>(i, w, h, pose, assign, o);
   }
 }
 
@@ -725,7 +732,7 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
 // Staged expansion: one thread per row, consecutive rows in consecutive threads, so every output array is written in
 // full coalesced sectors -- a work row's outputs from its staged channel sums (key[i] is its work slot), any other row
 // the indicator times the whole-plane channels.
-template <class Pack, int K>
+template <class Pack, int K, int VEC>
 __device__ __forceinline__ void pack_expand_row(const double* a, int64_t i, double w, double h, const double* pose,
                                                 bool assign, const PackOut& o) {
   if constexpr (K < Pack::kN) {
@@ -739,14 +746,17 @@ __device__ __forceinline__ void pack_expand_row(const double* a, int64_t i, doub
       acc[2 * c + 1] = v.y;
     }
     if constexpr (KT::kQuad)
-      finish_row_quad(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
+      finish_row_quad<VEC>(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
     else
-      finish_row(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
-    pack_expand_row<Pack, K + 1>(a, i, w, h, pose, assign, o);
+      finish_row<VEC>(acc, w, KT::kMass, KT::kPlane2, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K],
+                      o.m2[K]);
+    pack_expand_row<Pack, K + 1, VEC>(a, i, w, h, pose, assign, o);
   }
 }
 
-template <class Pack>
+// VEC (write_outputs): 2 when G / m1 are 16-byte and cov / m2 32-byte aligned, so every store of a warp writes whole
+// 32-byte sectors (no read-modify-write of partly written sectors); 1 when all are 16-byte aligned; 0 otherwise
+template <class Pack, int VEC>
 __global__ void __launch_bounds__(kThreads) k_agg_expand(const double* __restrict__ sup,
                                                          const int32_t* __restrict__ flag,
                                                          const double* __restrict__ ind,
@@ -758,9 +768,19 @@ __global__ void __launch_bounds__(kThreads) k_agg_expand(const double* __restric
   if (i >= n) return;
   const int32_t f = flag[i];
   if (f == 2)
-    pack_expand_row<Pack, 0>(wacc + (int64_t)slot[i] * (Pack::kN * 12), i, ind[i], sup[i], pose, assign, out);
+    pack_expand_row<Pack, 0, VEC>(wacc + (int64_t)slot[i] * (Pack::kN * 12), i, ind[i], sup[i], pose, assign, out);
   else if (f == 1 || assign)
-    pack_constant_row<Pack, 0>(i, f == 1 ? ind[i] : 0.0, sup[i], pose, assign, out);
+    pack_constant_row<Pack, 0, VEC>(i, f == 1 ? ind[i] : 0.0, sup[i], pose, assign, out);
+}
+
+static int pack_out_vec(const PackOut& o, int n) {
+  auto al = [](const double* p, uintptr_t a) { return p == nullptr || ((uintptr_t)p & (a - 1)) == 0; };
+  bool v16 = true, v32 = true;
+  for (int k = 0; k < n; ++k) {
+    v16 = v16 && al(o.G[k], 16) && al(o.m1[k], 16) && al(o.cov[k], 16) && al(o.m2[k], 16);
+    v32 = v32 && al(o.cov[k], 32) && al(o.m2[k], 32);
+  }
+  return v16 ? (v32 ? 2 : 1) : 0;
 }
 
 // the pair kernel of a pack over a prepared workspace (two lanes per work row: measured fastest on the 2^20-particle
@@ -798,7 +818,15 @@ static int launch_pack(const SurfView& v, const double* sup, const Workspace& w,
   if (g_pair_ev[0]) WSB_CUDA(cudaEventRecord(g_pair_ev[0], st));
   kern<<<grid, kThreads, smem, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, out, w.wacc);
   if (g_pair_ev[1]) WSB_CUDA(cudaEventRecord(g_pair_ev[1], st));
-  if (staged) k_agg_expand<Pack><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
+  if (staged) {
+    const int vec = pack_out_vec(out, Pack::kN);
+    if (vec == 2)
+      k_agg_expand<Pack, 2><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
+    else if (vec == 1)
+      k_agg_expand<Pack, 1><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
+    else
+      k_agg_expand<Pack, 0><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
+  }
   return WSB_OK;
 }
 
