@@ -439,18 +439,20 @@ __device__ __forceinline__ void put(double* p, double v, bool assign) {
     *p += v;
 }
 
+// The vector stores below are streaming (evict-first) stores: they serve output passes that write every row once, so
+// their lines should not push the pass's own inputs out of L2.
 // two consecutive outputs by one 16-byte store (p 16-byte aligned), assigned or added
 __device__ __forceinline__ void put2(double* p, double a, double b, bool assign) {
   double2* q = reinterpret_cast<double2*>(p);
   if (assign) {
-    *q = make_double2(a, b);
+    __stcs(q, make_double2(a, b));
   } else {
     const double2 o = *q;
-    *q = make_double2(o.x + a, o.y + b);
+    __stcs(q, make_double2(o.x + a, o.y + b));
   }
 }
 
-// four consecutive outputs by one 32-byte store (p 32-byte aligned: st.global.v4.f64, sm_100), assigned or added
+// four consecutive outputs by one 32-byte store (p 32-byte aligned: st.global.cs.v4.f64, sm_100), assigned or added
 __device__ __forceinline__ void put4(double* p, double a, double b, double c, double d, bool assign) {
   if (!assign) {
     const double2 o0 = reinterpret_cast<const double2*>(p)[0], o1 = reinterpret_cast<const double2*>(p)[1];
@@ -459,7 +461,12 @@ __device__ __forceinline__ void put4(double* p, double a, double b, double c, do
     c = o1.x + c;
     d = o1.y + d;
   }
-  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+  asm volatile("st.global.cs.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+}
+
+// four consecutive doubles by one 32-byte read-only load (p 32-byte aligned, sm_100)
+__device__ __forceinline__ void ld4_nc(const double* p, double& a, double& b, double& c, double& d) {
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
 }
 
 // VEC 0: scalar stores; 1: the pairs of G, m1, cov, m2 as 16-byte stores (pointers 16-byte aligned); 2: also the four
@@ -485,7 +492,16 @@ __device__ __forceinline__ void write_outputs(const double ch[12], double h, con
       put_pair(p + 2, c, d);
     }
   };
-  if (lam) put(&lam[r], ch[0], assign);
+  if (lam) {
+    if constexpr (VEC > 0) {
+      if (assign)
+        __stcs(&lam[r], ch[0]);
+      else
+        __stcs(&lam[r], lam[r] + ch[0]);
+    } else {
+      put(&lam[r], ch[0], assign);
+    }
+  }
   if (m1) {
     const double vx = h * ch[1], vy = h * ch[2];
     put_pair(&m1[2 * r], R00 * vx + R01 * vy, R10 * vx + R11 * vy);

@@ -87,9 +87,11 @@ static Workspace carve(const Surface* s, int64_t n, void* base) {
   return w;
 }
 
-// the staging region when the workspace holds it (workspace_bytes >= total + staging)
+// the staging region when the workspace holds it (workspace_bytes >= total + staging) and it starts on a 32-byte
+// boundary (the expansion reads it by 32-byte loads); otherwise the evaluation stores its outputs directly
 static void attach_staging(Workspace& w, void* base, size_t workspace_bytes) {
-  w.wacc = (base && workspace_bytes >= w.total + w.staging) ? (double*)((char*)base + w.total) : nullptr;
+  char* p = base ? (char*)base + w.total : nullptr;
+  w.wacc = (p && workspace_bytes >= w.total + w.staging && ((uintptr_t)p & 31u) == 0) ? (double*)p : nullptr;
 }
 
 // body-frame position (bit-for-bit Pose.toLocal), broadphase (fixedadj.py:257-265) and the bucket of every row
@@ -738,13 +740,10 @@ __device__ __forceinline__ void pack_expand_row(const double* a, int64_t i, doub
   if constexpr (K < Pack::kN) {
     using KT = typename Pack::template Kern<K>;
     double acc[12];
-    const double2* a2 = reinterpret_cast<const double2*>(a + K * 12);
+    // three 32-byte loads: each reads one whole sector of the staged sums (a row's slot is 96 B a kernel, 32-byte
+    // aligned), so no sector has to be fetched twice
 #pragma unroll
-    for (int c = 0; c < 6; ++c) {
-      const double2 v = __ldg(a2 + c);
-      acc[2 * c] = v.x;
-      acc[2 * c + 1] = v.y;
-    }
+    for (int c = 0; c < 3; ++c) ld4_nc(a + K * 12 + 4 * c, acc[4 * c], acc[4 * c + 1], acc[4 * c + 2], acc[4 * c + 3]);
     if constexpr (KT::kQuad)
       finish_row_quad<VEC>(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
     else
