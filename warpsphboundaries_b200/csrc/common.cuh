@@ -469,9 +469,13 @@ __device__ __forceinline__ void ld4_nc(const double* p, double& a, double& b, do
   asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
 }
 
+// a*b + c*d with its roundings fixed (one product, then one fused multiply-add): the compiler may not re-contract it,
+// so every instantiation of the row finish -- any store width, any kernel pack, direct or staged -- gives the same bits
+__device__ __forceinline__ double dot2(double a, double b, double c, double d) { return __fma_rn(a, b, __dmul_rn(c, d)); }
+
 // VEC 0: scalar stores; 1: the pairs of G, m1, cov, m2 as 16-byte stores (pointers 16-byte aligned); 2: also the four
 // values of cov and m2 as one 32-byte store (cov, m2 32-byte aligned), so every store of a warp writes whole sectors.
-// The values are the same in every mode.
+// The values are the same in every mode: the rotation to the world frame is written with explicit roundings.
 template <int VEC = 0>
 __device__ __forceinline__ void write_outputs(const double ch[12], double h, const double* rot, int64_t r, double* lam,
                                               double* G, double* cov, double* m1, double* m2, bool assign = false) {
@@ -497,31 +501,35 @@ __device__ __forceinline__ void write_outputs(const double ch[12], double h, con
       if (assign)
         __stcs(&lam[r], ch[0]);
       else
-        __stcs(&lam[r], lam[r] + ch[0]);
+        __stcs(&lam[r], __dadd_rn(lam[r], ch[0]));
     } else {
       put(&lam[r], ch[0], assign);
     }
   }
   if (m1) {
-    const double vx = h * ch[1], vy = h * ch[2];
-    put_pair(&m1[2 * r], R00 * vx + R01 * vy, R10 * vx + R11 * vy);
+    const double vx = __dmul_rn(h, ch[1]), vy = __dmul_rn(h, ch[2]);
+    put_pair(&m1[2 * r], dot2(R00, vx, R01, vy), dot2(R10, vx, R11, vy));
   }
   if (G) {
-    const double vx = ch[3] / h, vy = ch[4] / h;
-    put_pair(&G[2 * r], R00 * vx + R01 * vy, R10 * vx + R11 * vy);
+    const double vx = __ddiv_rn(ch[3], h), vy = __ddiv_rn(ch[4], h);
+    put_pair(&G[2 * r], dot2(R00, vx, R01, vy), dot2(R10, vx, R11, vy));
   }
   if (cov) {
+    // R C R^T with C = [[a, b], [c, d]]: rows of C R^T first, then R times them
     const double a = ch[5], b = ch[6], c = ch[7], d = ch[8];
-    put_quad(&cov[4 * r], R00 * (a * R00 + b * R01) + R01 * (c * R00 + d * R01),
-             R00 * (a * R10 + b * R11) + R01 * (c * R10 + d * R11), R10 * (a * R00 + b * R01) + R11 * (c * R00 + d * R01),
-             R10 * (a * R10 + b * R11) + R11 * (c * R10 + d * R11));
+    const double u00 = dot2(a, R00, b, R01), u01 = dot2(a, R10, b, R11);
+    const double u10 = dot2(c, R00, d, R01), u11 = dot2(c, R10, d, R11);
+    put_quad(&cov[4 * r], dot2(R00, u00, R01, u10), dot2(R00, u01, R01, u11), dot2(R10, u00, R11, u10),
+             dot2(R10, u01, R11, u11));
   }
   if (m2) {
-    const double hh = h * h;
-    const double xx = ch[9] * hh, xy = ch[10] * hh, yy = ch[11] * hh;
-    const double off = R00 * R10 * xx + (R00 * R11 + R01 * R10) * xy + R01 * R11 * yy;
-    put_quad(&m2[4 * r], R00 * R00 * xx + 2.0 * R00 * R01 * xy + R01 * R01 * yy, off, off,
-             R10 * R10 * xx + 2.0 * R10 * R11 * xy + R11 * R11 * yy);
+    // R M R^T with M = [[xx, xy], [xy, yy]] symmetric: the off-diagonal entry written twice
+    const double hh = __dmul_rn(h, h);
+    const double xx = __dmul_rn(ch[9], hh), xy = __dmul_rn(ch[10], hh), yy = __dmul_rn(ch[11], hh);
+    const double u00 = dot2(xx, R00, xy, R01), u01 = dot2(xx, R10, xy, R11);
+    const double u10 = dot2(xy, R00, yy, R01), u11 = dot2(xy, R10, yy, R11);
+    const double off = dot2(R10, u00, R11, u10);
+    put_quad(&m2[4 * r], dot2(R00, u00, R01, u10), off, off, dot2(R10, u01, R11, u11));
   }
 }
 

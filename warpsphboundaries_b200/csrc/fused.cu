@@ -286,11 +286,11 @@ template <int VEC = 0>
 __device__ __forceinline__ void finish_row(double acc[12], double ind, double mass, double plane2, double h,
                                            const double* pose, int64_t i, bool assign, double* lam, double* G,
                                            double* cov, double* m1, double* m2) {
-  acc[0] += ind * mass;
-  acc[5] += ind * mass;
-  acc[8] += ind * mass;
-  acc[9] += ind * plane2;
-  acc[11] += ind * plane2;
+  acc[0] = __fma_rn(ind, mass, acc[0]);
+  acc[5] = __fma_rn(ind, mass, acc[5]);
+  acc[8] = __fma_rn(ind, mass, acc[8]);
+  acc[9] = __fma_rn(ind, plane2, acc[9]);
+  acc[11] = __fma_rn(ind, plane2, acc[11]);
   const double c = pose[2], s = pose[3];
   const double rot[4] = {c, -s, s, c};
   write_outputs<VEC>(acc, h, rot, i, lam, G, cov, m1, m2, assign);
@@ -531,12 +531,12 @@ __device__ __forceinline__ void finish_row_quad(const double acc[12], double h, 
   const double c = pose[2], s = pose[3], nan = __longlong_as_double(0x7ff8000000000000LL);
   if (lam) put(&lam[i], nan, assign);
   if (G) {
-    const double vx = acc[3] / h, vy = acc[4] / h;
+    const double vx = __ddiv_rn(acc[3], h), vy = __ddiv_rn(acc[4], h);
     if constexpr (VEC > 0) {
-      put2(&G[2 * i], c * vx - s * vy, s * vx + c * vy, assign);
+      put2(&G[2 * i], dot2(c, vx, -s, vy), dot2(s, vx, c, vy), assign);
     } else {
-      put(&G[2 * i], c * vx - s * vy, assign);
-      put(&G[2 * i + 1], s * vx + c * vy, assign);
+      put(&G[2 * i], dot2(c, vx, -s, vy), assign);
+      put(&G[2 * i + 1], dot2(s, vx, c, vy), assign);
     }
   }
   for (int k = 0; k < 4; ++k) {
