@@ -144,11 +144,13 @@ def test_lowered_bodies_are_served():
 
 
 def test_sphere_rows_in_the_mix_and_per_class_stats():
-    """sphere-row requests (query, sphere) batched with 2-D requests: each equals RadialEvaluator on its rows bit for
-    bit; the statistics report p50 / p99 per request class."""
+    """sphere-row requests (query, sphere) of two sphere scenes with different supports, batched together and with
+    2-D requests: each equals RadialEvaluator on its rows bit for bit; the statistics report p50 / p99 per request
+    class."""
     from warpsphboundaries_b200.radial import RadialEvaluator
     srv = BoundaryServer(DEV, streams=2, max_batch_rows=30000)
     srv.register_spheres("sph", 0.03)
+    srv.register_spheres("sph2", 0.05)          # another sphere scene: its rows share the launches of "sph"
     for sid, sc in _scenes().items():
         srv.register(sid, sc, 0.03)
     rng = np.random.default_rng(9)
@@ -161,8 +163,9 @@ def test_sphere_rows_in_the_mix_and_per_class_stats():
         nv /= np.linalg.norm(nv, axis=1, keepdims=True)
         k = ["w2", "w4", "w6"][i % 3]
         rows = torch.tensor(np.concatenate([d[:, None], nv, R[:, None]], 1), dtype=torch.float64, device=DEV)
-        ids.append(srv.submit("sph", rows, 0.03, k))
-        want.append(RadialEvaluator("sphere", kernel=k, device=DEV).evaluate(d, nv, 0.03, radii=R))
+        sid, h = ("sph", 0.03) if i % 2 == 0 else ("sph2", 0.05)
+        ids.append(srv.submit(sid, rows, h, k))
+        want.append(RadialEvaluator("sphere", kernel=k, device=DEV).evaluate(d, nv, h, radii=R))
         ids.append(srv.submit("s0", _positions(1000 + i, i), 0.03, "w4", grad=(i % 2 == 0)))
         want.append(None)
     srv.run()

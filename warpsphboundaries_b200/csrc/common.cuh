@@ -461,12 +461,15 @@ __device__ __forceinline__ void put4(double* p, double a, double b, double c, do
     c = o1.x + c;
     d = o1.y + d;
   }
-  asm volatile("st.global.cs.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d) : "memory");
+  // no memory clobber: the stored values depend on any load of the same outputs above, and no other access of this
+  // thread touches them, so the compiler may keep scheduling independent loads across the store
+  asm volatile("st.global.cs.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(a), "d"(b), "d"(c), "d"(d));
 }
 
-// four consecutive doubles by one 32-byte read-only load (p 32-byte aligned, sm_100)
+// four consecutive doubles by one 32-byte read-only load (p 32-byte aligned, sm_100; memory that no thread writes
+// during the kernel, so the load may be hoisted and overlapped freely)
 __device__ __forceinline__ void ld4_nc(const double* p, double& a, double& b, double& c, double& d) {
-  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(a), "=d"(b), "=d"(c), "=d"(d) : "l"(p));
 }
 
 // a*b + c*d with its roundings fixed (one product, then one fused multiply-add): the compiler may not re-contract it,

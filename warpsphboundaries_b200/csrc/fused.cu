@@ -216,11 +216,13 @@ __global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const doub
   // over its cell's candidates reads it there.
   __shared__ double4 s_rec[kStageRecs];
   __shared__ int32_t s_lo, s_hi;
+  __shared__ int32_t s_hist[kKeys - 1];
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (threadIdx.x == 0) {
     s_lo = INT32_MAX;
     s_hi = -1;
   }
+  for (int k = threadIdx.x; k < kKeys - 1; k += kThreads) s_hist[k] = 0;
   // sorted rows: the rows in cells with candidates (k_agg_prep settles all others)
   int32_t i = 0, b = 0;
   const bool cand = j < (int64_t)offs[S.nne];
@@ -276,10 +278,15 @@ __global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const doub
     }
     rkey[j] = cnt > 0 ? 63 - min(cnt, 63) : kKeys - 1;
   }
-  // warp-aggregated histogram of the keys
-  const int ckey = j < n ? (cnt > 0 ? 63 - min(cnt, 63) : kKeys - 1) : -1;
+  // histogram of the keys of the rows with pairs (the rows without are never scattered, so their key is not
+  // counted): warp-aggregated into the block's counts, then one global add per key the block has -- a global atomic
+  // per warp and key would serialise on the few hot keys of millions of rows
+  const int ckey = j < n && cnt > 0 ? 63 - min(cnt, 63) : -1;
   const unsigned peers = __match_any_sync(0xffffffffu, ckey);
-  if (ckey >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&khist[ckey], __popc(peers));
+  if (ckey >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&s_hist[ckey], __popc(peers));
+  __syncthreads();
+  for (int k = threadIdx.x; k < kKeys - 1; k += kThreads)
+    if (s_hist[k]) atomicAdd(&khist[k], s_hist[k]);
 }
 
 template <int VEC = 0>
@@ -733,17 +740,16 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
 
 // Staged expansion: one thread per row, consecutive rows in consecutive threads, so every output array is written in
 // full coalesced sectors -- a work row's outputs from its staged channel sums (key[i] is its work slot), any other row
-// the indicator times the whole-plane channels.
+// the indicator times the whole-plane channels.  A work row's outputs, every kernel of the pack, from its staged sums
+// (already loaded: a[kernel * 12 + c]).
 template <class Pack, int K, int VEC>
 __device__ __forceinline__ void pack_expand_row(const double* a, int64_t i, double w, double h, const double* pose,
                                                 bool assign, const PackOut& o) {
   if constexpr (K < Pack::kN) {
     using KT = typename Pack::template Kern<K>;
     double acc[12];
-    // three 32-byte loads: each reads one whole sector of the staged sums (a row's slot is 96 B a kernel, 32-byte
-    // aligned), so no sector has to be fetched twice
 #pragma unroll
-    for (int c = 0; c < 3; ++c) ld4_nc(a + K * 12 + 4 * c, acc[4 * c], acc[4 * c + 1], acc[4 * c + 2], acc[4 * c + 3]);
+    for (int c = 0; c < 12; ++c) acc[c] = a[K * 12 + c];
     if constexpr (KT::kQuad)
       finish_row_quad<VEC>(acc, h, pose, i, assign, o.lam[K], o.G[K], o.cov[K], o.m1[K], o.m2[K]);
     else
@@ -751,6 +757,16 @@ __device__ __forceinline__ void pack_expand_row(const double* a, int64_t i, doub
                       o.m2[K]);
     pack_expand_row<Pack, K + 1, VEC>(a, i, w, h, pose, assign, o);
   }
+}
+
+// a work row's staged sums, every kernel: 3 Pack::kN 32-byte loads issued together (a row's slot is 96 bytes a
+// kernel, 32-byte aligned: each load reads one whole sector), so their latencies overlap instead of each kernel's
+// loads following the previous kernel's stores (measured on B200, four-kernel pack on the 2^20-particle scene: the
+// expansion from 148 to 140 us)
+template <class Pack>
+__device__ __forceinline__ void load_staged(const double* src, double* a) {
+#pragma unroll
+  for (int c = 0; c < Pack::kN * 3; ++c) ld4_nc(src + 4 * c, a[4 * c], a[4 * c + 1], a[4 * c + 2], a[4 * c + 3]);
 }
 
 // VEC (write_outputs): 2 when G / m1 are 16-byte and cov / m2 32-byte aligned, so every store of a warp writes whole
@@ -766,9 +782,11 @@ __global__ void __launch_bounds__(kThreads) k_agg_expand(const double* __restric
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t f = flag[i];
-  if (f == 2)
-    pack_expand_row<Pack, 0, VEC>(wacc + (int64_t)slot[i] * (Pack::kN * 12), i, ind[i], sup[i], pose, assign, out);
-  else if (f == 1 || assign)
+  if (f == 2) {
+    double a[Pack::kN * 12];
+    load_staged<Pack>(wacc + (int64_t)slot[i] * (Pack::kN * 12), a);
+    pack_expand_row<Pack, 0, VEC>(a, i, ind[i], sup[i], pose, assign, out);
+  } else if (f == 1 || assign)
     pack_constant_row<Pack, 0, VEC>(i, f == 1 ? ind[i] : 0.0, sup[i], pose, assign, out);
 }
 
@@ -1124,26 +1142,48 @@ __global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int6
                               int32_t* __restrict__ bucket, const double* __restrict__ lpos,
                               const double* __restrict__ sup, const uint64_t* __restrict__ mask,
                               WorkRec* __restrict__ wrec, int32_t* __restrict__ nwork) {
-  __shared__ int32_t s_pre[kKeys + 1];
-  if (threadIdx.x == 0) {
-    int32_t run = 0;
-    for (int k = 0; k < kKeys; ++k) {
-      s_pre[k] = run;
-      run += khist[k];
+  constexpr int kWork = kKeys - 1;                                  // keys of rows with pairs: 0 .. 63
+  static_assert(kWork == 64, "two keys a lane in the prefix scan");
+  __shared__ int32_t s_pre[kWork + 1];                              // exclusive prefix of the key counts
+  __shared__ int32_t s_cnt[kWork];                                  // this block's rows per key, then its base
+  if (threadIdx.x < 32) {
+    // the prefix of the 64 key counts by one warp: lane l scans keys l and l + 32
+    const int l = threadIdx.x;
+    const int a = khist[l], b = khist[l + 32];
+    int sa = a, sb = b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ta = __shfl_up_sync(0xffffffffu, sa, o), tb = __shfl_up_sync(0xffffffffu, sb, o);
+      if (l >= o) {
+        sa += ta;
+        sb += tb;
+      }
     }
-    s_pre[kKeys] = run;
-    if (blockIdx.x == 0) *nwork = s_pre[kKeys - 1];          // rows with key < 64
+    const int tot_a = __shfl_sync(0xffffffffu, sa, 31), tot_b = __shfl_sync(0xffffffffu, sb, 31);
+    s_pre[l] = sa - a;
+    s_pre[l + 32] = tot_a + sb - b;
+    if (l == 0) {
+      s_pre[kWork] = tot_a + tot_b;
+      if (blockIdx.x == 0) *nwork = tot_a + tot_b;                  // rows with key < 64
+    }
   }
+  for (int k = threadIdx.x; k < kWork; k += kThreads) s_cnt[k] = 0;
   __syncthreads();
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int key = j < n ? rkey[j] : -1;
-  const bool mine = key >= 0 && key < kKeys - 1;
+  const bool mine = key >= 0 && key < kWork;
+  // the row's rank among the block's rows of its key (warp-aggregated shared atomics), then one global cursor add
+  // per key the block has: the block's base in that key's range
   const unsigned peers = __match_any_sync(0xffffffffu, mine ? key : -1);
   const int lane = threadIdx.x & 31;
   const int leader = __ffs(peers) - 1;
-  int base = 0;
-  if (mine && lane == leader) base = atomicAdd(&kcur[key], __popc(peers));
-  base = __shfl_sync(0xffffffffu, base, leader);
+  int rank = 0;
+  if (mine && lane == leader) rank = atomicAdd(&s_cnt[key], __popc(peers));
+  rank = __shfl_sync(0xffffffffu, rank, leader) + __popc(peers & ((1u << lane) - 1));
+  __syncthreads();
+  for (int k = threadIdx.x; k < kWork; k += kThreads)
+    if (s_cnt[k]) s_cnt[k] = atomicAdd(&kcur[k], s_cnt[k]);
+  __syncthreads();
   if (mine) {
     // gather the row's record once here, so the evaluations read one coalesced record per work row
     const int32_t i = order[j];
@@ -1159,7 +1199,7 @@ __global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int6
     r.pad[0] = r.pad[1] = r.pad[2] = 0;
     r.m0 = mm.x;
     r.m1 = mm.y;
-    const int32_t slot = s_pre[key] + base + __popc(peers & ((1u << lane) - 1));
+    const int32_t slot = s_pre[key] + s_cnt[key] + rank;
     wrec[slot] = r;
     bucket[i] = slot;            // from here on a work row's key is its work slot (read by the staged expansion)
   }

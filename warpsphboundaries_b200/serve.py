@@ -11,18 +11,22 @@
                                  # sphere rows: {"channels": [n, 28]} (baseline(3) order)
 
 Scheduling (one host thread, the caller's):
-* requests queue per (scene, kernel, grad); a batch takes the oldest requests of one queue up to `max_batch_rows`
+* requests queue per (scene, kernel, grad) (sphere rows: per kernel); a batch takes the oldest requests of one queue up to `max_batch_rows`
   rows and is admitted while the device memory it reserves (inputs, outputs, workspace) fits `hbm_budget`;
 * a batch is ONE fused launch family over the concatenated rows of its requests.  Rows are independent (each row's
   pairs are summed in its own fixed order), so a request's result is bit-identical alone and in any mix;
 * batches run on `streams` CUDA streams at once, so requests that arrive while others are on the GPU are admitted as
   stream slots and memory free up, and their work overlaps on the device;
 * with `use_graphs=True` (the default), batches of at most `graph_max_rows` rows replay a CUDA graph captured per
-  (stream, bucket, scene, kernel) over static buffers padded to a power-of-two bucket (padding rows are masked out); a
-  key is captured once it has been launched `graph_after_uses` times, so one-off keys stay eager; each capture holds
-  its own padded outputs and workspace, and captures stop once they hold `graph_budget` bytes;
+  (bucket, scene, kernel) over its own static inputs padded to a power-of-two bucket (padding rows are masked out),
+  outputs and workspace; a key is captured once it has been launched `graph_after_uses` times, so one-off keys stay
+  eager; the capture runs on a stream of its own that never holds work, so it waits for no batch in flight; any stream
+  slot replays a key's graph once the graph's previous replay (with its output copies) has completed, and runs the
+  batch eagerly otherwise; captures stop once they hold `graph_budget` bytes;
 * solid spheres (`register_spheres`): a request is a set of (query, sphere) rows [n, 5] = (signed distance, outward
-  normal, radius) with supports; a batch is one wsb_radial_channels launch over the concatenated rows;
+  normal, radius) with supports; the rows carry their own geometry and support, so the requests of every sphere
+  scene with one kernel share a queue and a batch (one wsb_radial_channels launch over the concatenated rows) serves
+  several scenes;
 * nothing is allocated per batch: a request's outputs come from a pool of power-of-two buffers when it is submitted
   (on the caller's stream), a scalar support is a view of a resident vector, a single-request batch writes straight
   into the request's outputs, a multi-request batch into persistent per-stream buffers that are then copied into each
@@ -76,14 +80,23 @@ class _Batch:
     start: Optional[torch.cuda.Event] = None
 
 
+class _Graph:
+    """a captured batch graph: its static inputs (positions, supports, row mask), workspace and outputs, and the event
+    of its last replay's end (its output copies included)."""
+
+    def __init__(self, pos, sup, allowed, ws, out):
+        self.pos, self.sup, self.allowed, self.ws, self.out = pos, sup, allowed, ws, out
+        self.graph = None
+        self.done = None
+
+
 class _Slot:
-    """one stream, its persistent batch buffers and its static graph buffers."""
+    """one stream and its persistent batch buffers."""
 
     def __init__(self, device):
         self.device = device
         self.stream = torch.cuda.Stream(device=device)
         self.busy = None
-        self.static = {}              # bucket -> (pos, sup, allowed)
         self.cap = 0
         self.B = 0
         self.buf = None
@@ -151,7 +164,8 @@ class BoundaryServer:
         self.graph_max_rows = int(graph_max_rows)
         self.graph_after_uses = int(graph_after_uses)
         self.precision = precision
-        self.graphs = {}
+        self.graphs = {}                    # (bucket, scene, kernel) -> _Graph
+        self.cap_stream = torch.cuda.Stream(self.device) if use_graphs else None    # captures only: never holds work
         self.graph_budget = int(graph_budget)  # device bytes all captured graphs may hold (their outputs, workspaces)
         self.graph_bytes = 0
         self.uses = {}
@@ -170,6 +184,7 @@ class BoundaryServer:
         self.held_bytes = 0                 # outputs of queued and in-flight requests
         self.support_vecs = {}              # support value -> resident vector filled with it
         self.intervals = []                 # (start, end) events of retired batches (device busy time)
+        self.host = {"batches": 0, "requests": 0, "launch_s": 0.0, "captures": 0, "replays": 0, "graph_busy": 0}   # host-side cost of the launches
 
     # ------------------------------------------------------------------ scenes
     def register(self, scene_id, scene, support):
@@ -212,6 +227,14 @@ class BoundaryServer:
     def _is_spheres(self, scene_id):
         return self.plans.get(scene_id, ()) == "spheres"
 
+    def _qkey(self, r):
+        """the queue of a request: requests of one queue run in one launch family.  Sphere rows carry their own
+        geometry and support, so the requests of every sphere scene with one kernel share a queue (one launch serves
+        several scenes); other requests queue per (scene, kernel, adjoint)."""
+        if self._is_spheres(r.scene_id):
+            return ("<spheres>", r.kernel, False)
+        return (r.scene_id, r.kernel, r.grad)
+
     def _cls(self, r):
         """the request class of the per-class latency report."""
         if self._is_mesh(r.scene_id):
@@ -253,7 +276,7 @@ class BoundaryServer:
             r.result["d_pos"] = flat[off:off + 2 * n].view(n, 2)
             r.result["d_pos"].zero_()
         self.requests[r.rid] = r
-        self.queues.setdefault((scene_id, kname, r.grad), []).append(r)
+        self.queues.setdefault(self._qkey(r), []).append(r)
         self.n_queued += 1
         return r.rid
 
@@ -272,7 +295,7 @@ class BoundaryServer:
         r.flat = self._take(28 * n)
         r.result = {"channels": r.flat[:28 * n].view(n, 28)}
         self.requests[r.rid] = r
-        self.queues.setdefault((r.scene_id, r.kernel, False), []).append(r)
+        self.queues.setdefault(self._qkey(r), []).append(r)
         self.n_queued += 1
         return r.rid
 
@@ -370,12 +393,16 @@ class BoundaryServer:
             scene, support = self.scenes[reqs[0].scene_id]
             need = self._bytes(scene, support, rows, reqs[0].grad)
             if self.reserved and self.reserved + need > self.hbm_budget:
-                q = self.queues[(reqs[0].scene_id, reqs[0].kernel, reqs[0].grad)]
+                q = self.queues[self._qkey(reqs[0])]
                 q[:0] = reqs                        # not admitted yet: back to the head of its queue
                 self.n_queued += len(reqs)
                 break
             self.reserved += need
+            t0 = time.perf_counter()
             self._launch(si, reqs, rows, scene, support, need)
+            self.host["launch_s"] += time.perf_counter() - t0
+            self.host["batches"] += 1
+            self.host["requests"] += len(reqs)
             self.n_inflight += 1
         return self.n_queued + self.n_inflight
 
@@ -488,7 +515,7 @@ class BoundaryServer:
                 outs = {k: buf[k][:B, :rows] for k in OUT_KEYS}
             gkey = None
             if self.use_graphs and not grad and rows <= self.graph_max_rows:
-                gkey = (si, self._bucket(rows), reqs[0].scene_id, kname)
+                gkey = (self._bucket(rows), reqs[0].scene_id, kname)
                 self.uses[gkey] = self.uses.get(gkey, 0) + 1
                 if gkey not in self.graphs and self.uses[gkey] < self.graph_after_uses:
                     gkey = None
@@ -548,49 +575,55 @@ class BoundaryServer:
         return max(1024, 1 << (int(rows) - 1).bit_length())
 
     def _graph_run(self, slot, key, plan, support, kname, pos, sup, rows, outs):
-        bucket = key[1]
+        """replay the key's graph for this batch on the slot's stream (capturing it first if the budget allows).
+        False: the batch runs eagerly (over budget, or the graph's previous replay has not completed)."""
+        bucket = key[0]
         B = len(plan)
-        st = slot.static.get(bucket)
-        if st is None:
-            st = (torch.zeros((bucket, 2), dtype=F64, device=self.device),
-                  torch.full((bucket,), support, dtype=F64, device=self.device),
-                  torch.zeros(bucket, dtype=torch.int32, device=self.device))
-            slot.static[bucket] = st
-        spos, ssup, sall = st
         g = self.graphs.get(key)
         if g is None:
-            # graph-owned workspace and outputs: a captured graph keeps its pointers, so they are never freed; a
-            # capture that would take the graphs past `graph_budget` is not made (the batch runs eagerly)
-            need = max(int(lib.wsb_aggregate_workspace_size(ns.handle, bucket)) + int(lib.wsb_aggregate_staging_size(ns.handle, bucket))
+            # graph-owned static inputs, workspace and outputs: a captured graph keeps its pointers, so they are never
+            # freed; a capture that would take the graphs past `graph_budget` is not made
+            need = max(int(lib.wsb_aggregate_workspace_size(ns.handle, bucket)) +
+                       int(lib.wsb_aggregate_staging_size(ns.handle, bucket))
                        for _, _, _, reps in plan for ns in reps)
-            gbytes = need + 8 * 13 * B * bucket
+            gbytes = need + 8 * 13 * B * bucket + 28 * bucket
             if self.graph_bytes + gbytes > self.graph_budget:
                 return False
             self.graph_bytes += gbytes
-            sall.fill_(1)
-            ws = torch.empty(need, dtype=torch.uint8, device=self.device)
-            gout = {k: torch.empty((B, bucket) + _TAIL[k], dtype=F64, device=self.device) for k in OUT_KEYS}
-            self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)     # eager warm-up
-            graph = torch.cuda.CUDAGraph()
-            # captured directly on the slot's stream: torch.cuda.graph() would also empty the allocator's cache, and
-            # every later allocation would then go back to the driver
-            slot.stream.synchronize()
             with torch.cuda.stream(slot.stream):
+                g = _Graph(torch.zeros((bucket, 2), dtype=F64, device=self.device),
+                           torch.full((bucket,), support, dtype=F64, device=self.device),
+                           torch.ones(bucket, dtype=torch.int32, device=self.device),
+                           torch.empty(need, dtype=torch.uint8, device=self.device),
+                           {k: torch.empty((B, bucket) + _TAIL[k], dtype=F64, device=self.device) for k in OUT_KEYS})
+                # eager run on the slot's stream (one-time library setup happens outside the capture; the replay
+                # below is ordered after it on the same stream)
+                self._aggregate(plan, kname, g.pos, g.sup, g.allowed, bucket, g.out, g.ws, slot.stream)
+            # captured on the capture stream, which holds no work: recording launches waits for nothing in flight
+            # (torch.cuda.graph() would also synchronise and empty the allocator's cache)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(self.cap_stream):
                 graph.capture_begin(capture_error_mode="thread_local")
                 try:
-                    self._aggregate(plan, kname, spos, ssup, sall, bucket, gout, ws, slot.stream)
+                    self._aggregate(plan, kname, g.pos, g.sup, g.allowed, bucket, g.out, g.ws, self.cap_stream)
                 finally:
                     graph.capture_end()
-            g = (graph, gout, ws)
+            g.graph = graph
             self.graphs[key] = g
-        graph, gout, _ = g
-        spos[:rows].copy_(pos)
-        ssup[:rows].copy_(sup)
-        sall[:rows].fill_(1)
-        sall[rows:].fill_(0)
-        graph.replay()
+            self.host["captures"] += 1
+        elif g.done is not None and not g.done.query():
+            self.host["graph_busy"] += 1
+            return False                                        # replaying on another slot: this batch runs eagerly
+        g.pos[:rows].copy_(pos)
+        g.sup[:rows].copy_(sup)
+        g.allowed[:rows].fill_(1)
+        g.allowed[rows:].fill_(0)
+        g.graph.replay()
         for k in OUT_KEYS:
-            outs[k].copy_(gout[k][:, :rows])
+            outs[k].copy_(g.out[k][:, :rows])
+        g.done = torch.cuda.Event()
+        g.done.record(slot.stream)
+        self.host["replays"] += 1
         return True
 
     # ------------------------------------------------------------------ statistics
@@ -621,6 +654,14 @@ class BoundaryServer:
             busy += cur1 - cur0
             span = max(b for _, b in iv) - min(a for a, _ in iv)
             out["gpu_busy"] = busy / span if span > 0 else None
+        hb = self.host
+        if hb["batches"]:
+            # host time spent issuing batches (argument setup, copies into batch buffers, launches, graph replays)
+            out["host"] = {"batches": hb["batches"], "requests_per_batch": hb["requests"] / hb["batches"],
+                           "launch_ms_per_batch": 1e3 * hb["launch_s"] / hb["batches"], "captures": hb["captures"],
+                           "graph_replays": hb["replays"], "graph_busy_fallbacks": hb["graph_busy"]}
+            if out.get("wall_s"):
+                out["host"]["launch_fraction"] = hb["launch_s"] / out["wall_s"]
         return out
 
     def reset_stats(self):
@@ -628,3 +669,4 @@ class BoundaryServer:
         self.completed.clear()
         self.intervals.clear()
         self.t_first = self.t_last = None
+        self.host = {"batches": 0, "requests": 0, "launch_s": 0.0, "captures": 0, "replays": 0, "graph_busy": 0}
