@@ -177,3 +177,36 @@ def test_sphere_rows_in_the_mix_and_per_class_stats():
     assert set(st["classes"]) == {"3d_spheres", "2d", "2d_grad"}
     assert st["classes"]["3d_spheres"]["requests"] == 8
     assert all(v["p50_ms"] <= v["p99_ms"] for v in st["classes"].values())
+
+
+def test_light_lane_takes_short_requests():
+    """a short 2-D request submitted after a closed-surface request of several milliseconds runs on the light lane
+    (a high-priority stream) at once instead of waiting for a standard slot; both results equal a server without
+    light lanes, bit for bit."""
+    h = 0.05
+    V, Fc = workloads.icosphere(3, 0.6, 0.05, seed=4)
+
+    def pos3(rows, seed):
+        g = torch.Generator(device=DEV)
+        g.manual_seed(seed)
+        return torch.rand((rows, 3), dtype=torch.float64, device=DEV, generator=g) * 1.6 - 0.8
+
+    out = []
+    for light in (1, 0):
+        srv = BoundaryServer(DEV, streams=1, light_streams=light)
+        srv.register_mesh("m", V, Fc, h)
+        srv.register("s0", _scenes()["s0"], 0.02)
+        heavy = srv.submit("m", pos3(400000, 1), h, "w4")          # estimated 2.6 ms: a standard slot
+        short = srv.submit("s0", _positions(3000, 2), 0.02, "w2")   # estimated 0.02 ms: light
+        srv.poll()
+        on = {s.light: [r.rid for r in s.busy.reqs] for s in srv.slots if s.busy is not None}
+        if light:
+            assert on == {False: [heavy], True: [short]}
+        else:
+            assert on == {False: [heavy]}                           # the short request waits for the slot
+        srv.run()
+        torch.cuda.synchronize()
+        out.append((srv.result(heavy)["channels"].clone(), {k: v.clone() for k, v in srv.result(short).items()}))
+    assert torch.equal(out[0][0], out[1][0])
+    for k in OUT_KEYS:
+        assert torch.equal(out[0][1][k], out[1][1][k]), k

@@ -452,6 +452,14 @@ __device__ __forceinline__ void put2(double* p, double a, double b, bool assign)
   }
 }
 
+// Programmatic dependent launch (sm_90 and later).  A kernel launched with the programmatic-serialization attribute
+// may be scheduled before the preceding kernel of its stream has finished; pdl_wait() blocks until that kernel has
+// completed and its memory operations are visible (at once when there is no such dependency), so it comes before any
+// access to memory the predecessors touch.  pdl_trigger() lets the next such kernel be scheduled as this grid's
+// blocks retire, which overlaps its launch and block start with this grid's tail.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // four consecutive outputs by one 32-byte store (p 32-byte aligned: st.global.cs.v4.f64, sm_100), assigned or added
 __device__ __forceinline__ void put4(double* p, double a, double b, double c, double d, bool assign) {
   if (!assign) {

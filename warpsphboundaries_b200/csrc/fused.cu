@@ -8,6 +8,7 @@
 #include <atomic>
 #include <mutex>
 #include <tuple>
+#include <utility>
 
 #include "common.cuh"
 
@@ -99,6 +100,8 @@ __global__ void k_agg_prep(SurfView S, const double* __restrict__ pos, const dou
                            const int32_t* __restrict__ allowed, int64_t n, const double* __restrict__ pose,
                            double4 obb, int unbounded, int32_t* __restrict__ key, double* __restrict__ lpos,
                            int32_t* __restrict__ counts, double* __restrict__ ind, int32_t* __restrict__ flag) {
+  pdl_wait();      // the preceding kernel of the stream has completed and its writes are visible
+  pdl_trigger();   // the next kernel of the stream may be scheduled into the SMs this grid frees
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double lx, ly;
@@ -133,6 +136,8 @@ __global__ void k_agg_prep(SurfView S, const double* __restrict__ pos, const dou
 
 __global__ void k_agg_scatter(SurfView S, const int32_t* __restrict__ key, int64_t n, const int32_t* __restrict__ offs,
                               int32_t* __restrict__ cursor, int32_t* __restrict__ order) {
+  pdl_wait();      // the preceding kernel of the stream has completed and its writes are visible
+  pdl_trigger();   // the next kernel of the stream may be scheduled into the SMs this grid frees
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t b = key[i];
@@ -211,6 +216,8 @@ __global__ void __launch_bounds__(kThreads) k_agg_rowinfo(SurfView S, const doub
                                                          double* __restrict__ ind, int32_t* __restrict__ flag,
                                                          int32_t* __restrict__ rkey, uint64_t* __restrict__ mask,
                                                          int32_t* __restrict__ khist) {
+  pdl_wait();      // the preceding kernel of the stream has completed and its writes are visible
+  pdl_trigger();   // the next kernel of the stream may be scheduled into the SMs this grid frees
   // The block's rows are consecutive in cell order, so the candidates of all their cells are one contiguous range of
   // the cell-list records: it is staged in shared memory with coalesced loads when it fits, and every row's pass
   // over its cell's candidates reads it there.
@@ -643,6 +650,8 @@ __global__ void __launch_bounds__(kThreads, MINB) k_agg_pairs(SurfView S, const 
                                                              const int32_t* __restrict__ flag,
                                                              const double* __restrict__ pose, bool assign,
                                                              const PackOut out, double* __restrict__ wacc) {
+  pdl_wait();      // the preceding kernel of the stream has completed and its writes are visible
+  pdl_trigger();   // the next kernel of the stream may be scheduled into the SMs this grid frees
   static_assert(G == 1 || G == 2 || G == 4 || G == 8 || G == 16, "lanes per row");
   static_assert(Pack::kN >= 1 && Pack::kN <= kMaxPack, "pack size");
   // dynamic shared memory: the channel sums [kernel][channel][thread], then each thread's next edge record
@@ -771,6 +780,9 @@ __device__ __forceinline__ void load_staged(const double* src, double* a) {
 
 // VEC (write_outputs): 2 when G / m1 are 16-byte and cov / m2 32-byte aligned, so every store of a warp writes whole
 // 32-byte sectors (no read-modify-write of partly written sectors); 1 when all are 16-byte aligned; 0 otherwise
+// (121 registers, 4 CTAs per SM: capping the registers at 5 / 6 / 8 CTAs measured 0.340 / 0.356 / 0.390 ms for the
+// grouped pass on the 2^20-particle scene against 0.306 ms -- the spilled staged sums cost more than the occupancy
+// gains)
 template <class Pack, int VEC>
 __global__ void __launch_bounds__(kThreads) k_agg_expand(const double* __restrict__ sup,
                                                          const int32_t* __restrict__ flag,
@@ -779,15 +791,20 @@ __global__ void __launch_bounds__(kThreads) k_agg_expand(const double* __restric
                                                          const double* __restrict__ wacc, int64_t n,
                                                          const double* __restrict__ pose, bool assign,
                                                          const PackOut out) {
+  pdl_wait();      // the preceding kernel of the stream has completed and its writes are visible
+  pdl_trigger();   // the next kernel of the stream may be scheduled into the SMs this grid frees
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t f = flag[i];
-  if (f == 2) {
-    double a[Pack::kN * 12];
-    load_staged<Pack>(wacc + (int64_t)slot[i] * (Pack::kN * 12), a);
-    pack_expand_row<Pack, 0, VEC>(a, i, ind[i], sup[i], pose, assign, out);
-  } else if (f == 1 || assign)
-    pack_constant_row<Pack, 0, VEC>(i, f == 1 ? ind[i] : 0.0, sup[i], pose, assign, out);
+  if (f == 0 && !assign) return;                                   // not a candidate, outputs added to: nothing
+  // one code path for every row, so a warp issues each of its output stores once (work and constant rows of a warp
+  // in separate branches would store every sector twice with partial masks): a constant row is a work row with zero
+  // sums and the same finish (the indicator terms, w = 0 for a non-candidate)
+  double a[Pack::kN * 12];
+#pragma unroll
+  for (int c = 0; c < Pack::kN * 12; ++c) a[c] = 0.0;
+  if (f == 2) load_staged<Pack>(wacc + (int64_t)slot[i] * (Pack::kN * 12), a);
+  pack_expand_row<Pack, 0, VEC>(a, i, f != 0 ? ind[i] : 0.0, sup[i], pose, assign, out);
 }
 
 static int pack_out_vec(const PackOut& o, int n) {
@@ -833,16 +850,20 @@ static int launch_pack(const SurfView& v, const double* sup, const Workspace& w,
   const unsigned rows = (unsigned)((n + kThreads - 1) / kThreads);
   const unsigned grid = (unsigned)((n * G + kThreads - 1) / kThreads) + (staged ? 0u : rows);
   if (g_pair_ev[0]) WSB_CUDA(cudaEventRecord(g_pair_ev[0], st));
-  kern<<<grid, kThreads, smem, st>>>(v, sup, w.wrec, w.nwork, n, w.ind, w.flag, pose, assign, out, w.wacc);
+  WSB_CUDA(launch_dep(kern, grid, kThreads, smem, st, v, sup, (const WorkRec*)w.wrec, (const int32_t*)w.nwork, n,
+                      (const double*)w.ind, (const int32_t*)w.flag, pose, assign, out, w.wacc));
   if (g_pair_ev[1]) WSB_CUDA(cudaEventRecord(g_pair_ev[1], st));
   if (staged) {
     const int vec = pack_out_vec(out, Pack::kN);
     if (vec == 2)
-      k_agg_expand<Pack, 2><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
+      WSB_CUDA(launch_dep(k_agg_expand<Pack, 2>, rows, kThreads, 0, st, sup, (const int32_t*)w.flag,
+                          (const double*)w.ind, (const int32_t*)w.key, (const double*)w.wacc, n, pose, assign, out));
     else if (vec == 1)
-      k_agg_expand<Pack, 1><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
+      WSB_CUDA(launch_dep(k_agg_expand<Pack, 1>, rows, kThreads, 0, st, sup, (const int32_t*)w.flag,
+                          (const double*)w.ind, (const int32_t*)w.key, (const double*)w.wacc, n, pose, assign, out));
     else
-      k_agg_expand<Pack, 0><<<rows, kThreads, 0, st>>>(sup, w.flag, w.ind, w.key, w.wacc, n, pose, assign, out);
+      WSB_CUDA(launch_dep(k_agg_expand<Pack, 0>, rows, kThreads, 0, st, sup, (const int32_t*)w.flag,
+                          (const double*)w.ind, (const int32_t*)w.key, (const double*)w.wacc, n, pose, assign, out));
   }
   return WSB_OK;
 }
@@ -1089,6 +1110,8 @@ __device__ __forceinline__ int scan_pad(int k) { return k + (k >> 5); }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_block(const int32_t* __restrict__ in, int32_t* __restrict__ out,
                                                             int64_t m) {
+  pdl_wait();      // the preceding kernel of the stream has completed and its writes are visible
+  pdl_trigger();   // the next kernel of the stream may be scheduled into the SMs this grid frees
   __shared__ int32_t s_data[kScanTile + kScanTile / 32];
   __shared__ int32_t s_warp[kScanThreads / 32];
   __shared__ int32_t s_carry;
@@ -1142,6 +1165,8 @@ __global__ void k_key_scatter(SurfView S, const int32_t* __restrict__ rkey, int6
                               int32_t* __restrict__ bucket, const double* __restrict__ lpos,
                               const double* __restrict__ sup, const uint64_t* __restrict__ mask,
                               WorkRec* __restrict__ wrec, int32_t* __restrict__ nwork) {
+  pdl_wait();      // the preceding kernel of the stream has completed and its writes are visible
+  pdl_trigger();   // the next kernel of the stream may be scheduled into the SMs this grid frees
   constexpr int kWork = kKeys - 1;                                  // keys of rows with pairs: 0 .. 63
   static_assert(kWork == 64, "two keys a lane in the prefix scan");
   __shared__ int32_t s_pre[kWork + 1];                              // exclusive prefix of the key counts
@@ -1389,6 +1414,24 @@ __global__ void __launch_bounds__(kThreads) k_dir_extreme(SurfView S, const Work
 }
 
 // shared front half of the aggregate and its adjoint: body frame, broadphase, counting sort of the rows by cell
+// a launch that may start while the preceding kernel of the stream finishes (its kernel calls pdl_wait() before
+// touching memory): the seven kernels of one aggregate (prepare, pair pass, expansion) follow each other this way
+template <class... P, class... A>
+static cudaError_t launch_dep(void (*k)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t st,
+                             A&&... a) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(a)...);
+}
+
 static int sort_rows(const Surface* s, const double* pos, const double* sup, const int32_t* allowed, int64_t n,
                      const double* pose, const double* obb, int unbounded, const Workspace& w, cudaStream_t st) {
   const int64_t nbk = (int64_t)s->n_nonempty + 2;   // buckets: the cells with edges
@@ -1398,12 +1441,14 @@ static int sort_rows(const Surface* s, const double* pos, const double* sup, con
   const unsigned grid = (unsigned)((n + kThreads - 1) / kThreads);
   k_agg_prep<<<grid, kThreads, 0, st>>>(v, pos, sup, allowed, n, pose, make_double4(obb[0], obb[1], obb[2], obb[3]),
                                         unbounded, w.key, w.lpos, w.counts, w.ind, w.flag);
-  k_scan_block<<<1, kScanThreads, 0, st>>>(w.counts, w.offs, nbk + 1);
-  k_agg_scatter<<<grid, kThreads, 0, st>>>(v, w.key, n, w.offs, w.cursor, w.order);
-  k_agg_rowinfo<<<grid, kThreads, 0, st>>>(v, sup, w.key, w.lpos, w.offs, w.order, n, w.ind, w.flag, w.rkey, w.mask,
-                                            w.khist);
-  k_key_scatter<<<grid, kThreads, 0, st>>>(v, w.rkey, n, w.khist, w.kcur, w.order, w.key, w.lpos, sup, w.mask, w.wrec,
-                                           w.nwork);
+  WSB_CUDA(launch_dep(k_scan_block, 1, kScanThreads, 0, st, (const int32_t*)w.counts, w.offs, nbk + 1));
+  WSB_CUDA(launch_dep(k_agg_scatter, grid, kThreads, 0, st, v, (const int32_t*)w.key, n, (const int32_t*)w.offs,
+                      w.cursor, w.order));
+  WSB_CUDA(launch_dep(k_agg_rowinfo, grid, kThreads, 0, st, v, sup, (const int32_t*)w.key, (const double*)w.lpos,
+                      (const int32_t*)w.offs, (const int32_t*)w.order, n, w.ind, w.flag, w.rkey, w.mask, w.khist));
+  WSB_CUDA(launch_dep(k_key_scatter, grid, kThreads, 0, st, v, (const int32_t*)w.rkey, n, (const int32_t*)w.khist,
+                      w.kcur, (const int32_t*)w.order, w.key, (const double*)w.lpos, sup, (const uint64_t*)w.mask,
+                      w.wrec, w.nwork));
   WSB_CUDA(cudaGetLastError());
   return WSB_OK;
 }

@@ -16,7 +16,9 @@ Scheduling (one host thread, the caller's):
 * a batch is ONE fused launch family over the concatenated rows of its requests.  Rows are independent (each row's
   pairs are summed in its own fixed order), so a request's result is bit-identical alone and in any mix;
 * batches run on `streams` CUDA streams at once, so requests that arrive while others are on the GPU are admitted as
-  stream slots and memory free up, and their work overlaps on the device;
+  stream slots and memory free up, and their work overlaps on the device; `light_streams` more streams of higher
+  priority take only batches whose estimated device time (rows x a per-class cost) is below `light_cost_s`, so short
+  requests are not queued behind closed-surface batches of several milliseconds and their blocks are scheduled first;
 * with `use_graphs=True` (the default), batches of at most `graph_max_rows` rows replay a CUDA graph captured per
   (bucket, scene, kernel) over its own static inputs padded to a power-of-two bucket (padding rows are masked out),
   outputs and workspace; a key is captured once it has been launched `graph_after_uses` times, so one-off keys stay
@@ -67,6 +69,7 @@ class Request:
     arrival: float
     result: Optional[dict] = None
     done: Optional[float] = None
+    launched: Optional[float] = None        # host time its batch was issued (queue wait = launched - arrival)
     flat: Optional[torch.Tensor] = None
     nbytes: int = 0
 
@@ -93,9 +96,10 @@ class _Graph:
 class _Slot:
     """one stream and its persistent batch buffers."""
 
-    def __init__(self, device):
+    def __init__(self, device, light=False):
         self.device = device
-        self.stream = torch.cuda.Stream(device=device)
+        self.light = light            # a light-lane slot: high stream priority, batches of small estimated cost only
+        self.stream = torch.cuda.Stream(device=device, priority=-1 if light else 0)
         self.busy = None
         self.cap = 0
         self.B = 0
@@ -151,11 +155,13 @@ class _Slot:
 class BoundaryServer:
     def __init__(self, device="cuda:0", streams=4, max_batch_rows=1 << 20, hbm_budget=None, use_graphs=True,
                  graph_max_rows=1 << 16, precision="fp64", graph_after_uses=4, pool_limit=None,
-                 graph_budget=2 << 30):
+                 graph_budget=2 << 30, light_streams=2, light_cost_s=1e-3):
         self.device = torch.device(device)
         self.scenes: Dict[str, tuple] = {}
         self.queues: Dict[tuple, List[Request]] = {}
-        self.slots = [_Slot(self.device) for _ in range(streams)]
+        self.slots = [_Slot(self.device) for _ in range(streams)] + \
+            [_Slot(self.device, light=True) for _ in range(light_streams)]
+        self.light_cost_s = float(light_cost_s)
         self.max_batch_rows = int(max_batch_rows)
         free, total = torch.cuda.mem_get_info(self.device)
         self.hbm_budget = int(hbm_budget if hbm_budget is not None else 0.25 * free)
@@ -349,20 +355,33 @@ class BoundaryServer:
         return (8 * 13 * B + 24 + (16 if grad else 0)) * rows + ws
 
     # ------------------------------------------------------------------ the loop
-    def _next_batch(self):
-        """the queue whose oldest request arrived first; its oldest requests up to max_batch_rows rows."""
+    # device seconds a row, by request class (measured on B200 at large batches: 2-D one kernel with prepare, the
+    # adjoint about as much again; closed surfaces of the 3-D configuration; sphere rows), for the lane choice only
+    _ROW_COST = {"2d": 2.5e-10, "2d_grad": 5e-10, "3d_surface": 6.5e-9, "3d_spheres": 2.5e-10}
+
+    def _cost(self, r):
+        """the estimated device time of a request (seconds): what sends a batch to the light lanes."""
+        return 2e-5 + len(r.pos) * self._ROW_COST[self._cls(r)]
+
+    def _next_batch(self, light_only=False):
+        """the queue whose oldest request arrived first; its oldest requests up to max_batch_rows rows.  light_only:
+        among the queues whose head is light (estimated cost below light_cost_s), up to that cost."""
         best = None
         for key, q in self.queues.items():
-            if q and (best is None or q[0].arrival < self.queues[best][0].arrival):
+            if not q or (light_only and self._cost(q[0]) >= self.light_cost_s):
+                continue
+            if best is None or q[0].arrival < self.queues[best][0].arrival:
                 best = key
         if best is None:
             return None
         q = self.queues[best]
-        take, rows = [], 0
-        while q and (not take or rows + len(q[0].pos) <= self.max_batch_rows):
+        take, rows, cost = [], 0, 0.0
+        while q and (not take or (rows + len(q[0].pos) <= self.max_batch_rows and
+                                  (not light_only or cost + self._cost(q[0]) < self.light_cost_s))):
             r = q.pop(0)
             take.append(r)
             rows += len(r.pos)
+            cost += self._cost(r)
         self.n_queued -= len(take)
         return take, rows
 
@@ -386,10 +405,19 @@ class BoundaryServer:
                 self.n_inflight -= 1
                 self.t_last = t
         while self.n_queued:
-            si = next((i for i, s in enumerate(self.slots) if s.busy is None), None)
-            if si is None:
+            # a free standard slot takes the oldest queue's batch; with only light slots free, the oldest light batch
+            # (so short requests do not wait behind batches of several milliseconds)
+            free = [i for i, s in enumerate(self.slots) if s.busy is None]
+            if not free:
                 break
-            reqs, rows = self._next_batch()
+            std = [i for i in free if not self.slots[i].light]
+            picked = self._next_batch(light_only=not std)
+            if picked is None:
+                break
+            reqs, rows = picked
+            light = [i for i in free if self.slots[i].light]
+            si = light[0] if light and sum(self._cost(r) for r in reqs) < self.light_cost_s else std[0] if std else \
+                light[0]
             scene, support = self.scenes[reqs[0].scene_id]
             need = self._bytes(scene, support, rows, reqs[0].grad)
             if self.reserved and self.reserved + need > self.hbm_budget:
@@ -399,6 +427,8 @@ class BoundaryServer:
                 break
             self.reserved += need
             t0 = time.perf_counter()
+            for r in reqs:
+                r.launched = t0
             self._launch(si, reqs, rows, scene, support, need)
             self.host["launch_s"] += time.perf_counter() - t0
             self.host["batches"] += 1
@@ -635,9 +665,12 @@ class BoundaryServer:
                        mean_ms=float(lat.mean()), max_ms=float(lat.max()))
         classes = {}
         for r in self.completed:
-            classes.setdefault(self._cls(r), []).append((r.done - r.arrival) * 1e3)
-        out["classes"] = {c: {"requests": len(v), "p50_ms": float(np.percentile(v, 50)),
-                              "p99_ms": float(np.percentile(v, 99))} for c, v in sorted(classes.items())}
+            classes.setdefault(self._cls(r), []).append(((r.done - r.arrival) * 1e3, (r.launched - r.arrival) * 1e3))
+        # per class: latency p50 / p99, and the p99 of the queue wait (arrival to the batch's issue) beside it
+        out["classes"] = {c: {"requests": len(v), "p50_ms": float(np.percentile([x for x, _ in v], 50)),
+                              "p99_ms": float(np.percentile([x for x, _ in v], 99)),
+                              "wait_p99_ms": float(np.percentile([w for _, w in v], 99))}
+                          for c, v in sorted(classes.items())}
         if self.t_first is not None and self.t_last is not None:
             out["wall_s"] = self.t_last - self.t_first
         if self.intervals:
