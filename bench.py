@@ -837,6 +837,8 @@ def our_arm(args):
                "h2d_bytes_per_step": N * 3 * 8, "d2h_bytes_per_step": len(KERNELS) * N * 13 * 8,
                "downloads": "lam, G, Cov, m1, m2 of every kernel (13 float64 per particle per kernel)",
                "ms_per_step": tot / args.steps, "pipelined": True,
+               # the step's bound: its download over the host link (the upload overlaps it on the other direction)
+               "d2h_gbs": len(KERNELS) * N * 13 * 8 * args.steps / (tot * 1e-3) / 1e9,
                "sequential": {"value": job_pairs_step * args.steps / (seq * 1e-3), "ms_per_step": seq / args.steps}}
 
     def side(fn, *a, **k):
