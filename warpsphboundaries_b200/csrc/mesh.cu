@@ -168,16 +168,25 @@ __device__ __forceinline__ void for_candidates(const MeshView& M, const double q
       }
 }
 
-// whether any face box comes within h of the query (the loops of for_candidates, stopping at the first)
+// whether any face box comes within h of the query (the loops of for_candidates, stopping at the first).  A cell
+// whose own box is h or more from the query is skipped: a face box within h of the query has its point nearest to the
+// query in a cell within h, and every cell its box overlaps lists the face.
 __device__ __forceinline__ bool has_candidate(const MeshView& M, const double q[3], double h) {
   const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
             cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
   const int x0 = max(cx - 1, 0), x1 = min(cx + 1, M.nx - 1), y0 = max(cy - 1, 0), y1 = min(cy + 1, M.ny - 1),
             z0 = max(cz - 1, 0), z1 = min(cz + 1, M.nz - 1);
   const double h2 = h * h;
+  // squared distance from the query to the slab of cell index i along one axis
+  auto gap2 = [&](double x, double lo, int i) {
+    const double a = fma((double)i, M.cell, lo), d = fmax(0.0, fmax(a - x, x - (a + M.cell)));
+    return d * d;
+  };
   for (int k = z0; k <= z1; ++k)
     for (int j = y0; j <= y1; ++j)
       for (int i = x0; i <= x1; ++i) {
+        // (a relative margin far above the rounding of the cell boxes: a cell is only skipped when clearly out of reach)
+        if (gap2(q[0], M.lo0, i) + gap2(q[1], M.lo1, j) + gap2(q[2], M.lo2, k) >= h2 * (1.0 + 1e-9)) continue;
         const int c = (k * M.ny + j) * M.nx + i;
         for (int it = M.cstart[c]; it < M.cstart[c + 1]; ++it) {
           const double* F = M.fdata + (int64_t)M.citems[it] * kFaceDoubles;
