@@ -100,48 +100,68 @@ __device__ __forceinline__ double edge_fn(double ax, double ay, double bx, doubl
   return __dsub_rn(__dmul_rn(__dsub_rn(bx, ax), __dsub_rn(qy, ay)), __dmul_rn(__dsub_rn(by, ay), __dsub_rn(qx, ax)));
 }
 
+// whether the vertical ray {(x, y, t): t > z} crosses face f of the column (its projection owns (x, y) and the face
+// lies above z)
+__device__ __forceinline__ bool column_cross(const MeshView& M, int f, double x, double y, double z) {
+  const double* F = M.fdata + (int64_t)f * kFaceDoubles;
+  const double nzf = F[kFN + 2];
+  if (nzf == 0.0) return false;                     // vertical face: its projection has no interior
+  const int* vid = M.fvid + 3 * f;
+  const double sgn = nzf > 0.0 ? 1.0 : -1.0;        // counter-clockwise projection for N.z > 0
+  for (int e = 0; e < 3; ++e) {
+    const int a = e, b = (e + 1) % 3;
+    const bool fwd = vid[a] < vid[b];
+    const double* A = F + kFV + 3 * (fwd ? a : b);
+    const double* B = F + kFV + 3 * (fwd ? b : a);
+    double E = edge_fn(A[0], A[1], B[0], B[1], x, y);
+    if (!fwd) E = -E;
+    E *= sgn;
+    if (E < 0.0) return false;
+    if (E == 0.0) {
+      const double* P0 = F + kFV + 3 * a;
+      const double* P1 = F + kFV + 3 * b;
+      const double dx = (P1[0] - P0[0]) * sgn, dy = (P1[1] - P0[1]) * sgn;
+      if (!(dy > 0.0 || (dy == 0.0 && dx < 0.0))) return false;
+    }
+  }
+  const double zt = F[kFV + 2] - (F[kFN] * (x - F[kFV]) + F[kFN + 1] * (y - F[kFV + 1])) / nzf;
+  return zt > z;
+}
+
 __device__ int mesh_inside(const MeshView& M, double x, double y, double z) {
   const int ix = cell_coord(x, M.lo0, M.cell, M.nx), iy = cell_coord(y, M.lo1, M.cell, M.ny);
   if (ix < 0 || iy < 0 || ix >= M.nx || iy >= M.ny) return 0;
   const int col = iy * M.nx + ix;
   int parity = 0;
-  for (int k = M.colstart[col]; k < M.colstart[col + 1]; ++k) {
-    const int f = M.colitems[k];
-    const double* F = M.fdata + (int64_t)f * kFaceDoubles;
-    const double nzf = F[kFN + 2];
-    if (nzf == 0.0) continue;                         // vertical face: its projection has no interior
-    const int* vid = M.fvid + 3 * f;
-    const double sgn = nzf > 0.0 ? 1.0 : -1.0;        // counter-clockwise projection for N.z > 0
-    bool in = true;
-    for (int e = 0; e < 3 && in; ++e) {
-      const int a = e, b = (e + 1) % 3;
-      const bool fwd = vid[a] < vid[b];
-      const double* A = F + kFV + 3 * (fwd ? a : b);
-      const double* B = F + kFV + 3 * (fwd ? b : a);
-      double E = edge_fn(A[0], A[1], B[0], B[1], x, y);
-      if (!fwd) E = -E;
-      E *= sgn;
-      if (E < 0.0) {
-        in = false;
-      } else if (E == 0.0) {
-        const double* P0 = F + kFV + 3 * a;
-        const double* P1 = F + kFV + 3 * b;
-        const double dx = (P1[0] - P0[0]) * sgn, dy = (P1[1] - P0[1]) * sgn;
-        if (!(dy > 0.0 || (dy == 0.0 && dx < 0.0))) in = false;
-      }
-    }
-    if (!in) continue;
-    const double zt = F[kFV + 2] - (F[kFN] * (x - F[kFV]) + F[kFN + 1] * (y - F[kFV + 1])) / nzf;
-    if (zt > z) parity ^= 1;
-  }
+  for (int k = M.colstart[col]; k < M.colstart[col + 1]; ++k)
+    if (column_cross(M, M.colitems[k], x, y, z)) parity ^= 1;
   return parity;
+}
+
+// mesh_inside for a whole warp (every lane calls it with the same point): the lanes test the column's faces 32 at a
+// time; the parity of the crossings (an integer count) is the same as the serial walk's
+__device__ __forceinline__ int mesh_inside_warp(const MeshView& M, double x, double y, double z, int lane) {
+  const int ix = cell_coord(x, M.lo0, M.cell, M.nx), iy = cell_coord(y, M.lo1, M.cell, M.ny);
+  if (ix < 0 || iy < 0 || ix >= M.nx || iy >= M.ny) return 0;
+  const int col = iy * M.nx + ix;
+  const int e = M.colstart[col + 1];
+  int crossings = 0;
+  for (int base = M.colstart[col]; base < e; base += 32) {
+    const int k = base + lane;
+    crossings += __popc(__ballot_sync(0xffffffffu, k < e && column_cross(M, M.colitems[k], x, y, z)));
+  }
+  return crossings & 1;
 }
 
 // ------------------------------------------------------------------------------------------ candidate faces
 // The faces of the 27 cells around the query's cell whose box comes within h of the query; a face listed in several
-// of those cells is taken in one of them only (the lowest corner of its box inside the 27-cell block).
+// of those cells is taken in one of them only (the lowest corner of its box inside the 27-cell block).  Called by a
+// whole warp with one query: the lanes test 32 items of a cell at a time, and the faces that pass are visited one after
+// the other, warp-uniformly, in cell order and item order within a cell -- a fixed order, so the sums the visits
+// accumulate do not depend on the launch.
 template <class Visit>
-__device__ __forceinline__ void for_candidates(const MeshView& M, const double q[3], double h, Visit&& visit) {
+__device__ __forceinline__ void for_candidates_warp(const MeshView& M, const double q[3], double h, int lane,
+                                                    Visit&& visit) {
   const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
             cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
   const int x0 = max(cx - 1, 0), x1 = min(cx + 1, M.nx - 1), y0 = max(cy - 1, 0), y1 = min(cy + 1, M.ny - 1),
@@ -151,33 +171,47 @@ __device__ __forceinline__ void for_candidates(const MeshView& M, const double q
     for (int j = y0; j <= y1; ++j)
       for (int i = x0; i <= x1; ++i) {
         const int c = (k * M.ny + j) * M.nx + i;
-        for (int it = M.cstart[c]; it < M.cstart[c + 1]; ++it) {
-          const int f = M.citems[it];
-          const int* fc = M.fcell + 3 * f;
-          if (max(fc[0], cx - 1) != i || max(fc[1], cy - 1) != j || max(fc[2], cz - 1) != k) continue;
-          const double* F = M.fdata + (int64_t)f * kFaceDoubles;
-          double d2 = 0.0;
+        const int e = M.cstart[c + 1];
+        for (int base = M.cstart[c]; base < e; base += 32) {
+          const int it = base + lane;
+          int f = -1;
+          bool hit = false;
+          if (it < e) {
+            f = M.citems[it];
+            const int* fc = M.fcell + 3 * f;
+            if (max(fc[0], cx - 1) == i && max(fc[1], cy - 1) == j && max(fc[2], cz - 1) == k) {
+              const double* F = M.fdata + (int64_t)f * kFaceDoubles;
+              double d2 = 0.0;
 #pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const double dl = F[kFLO + a] - q[a], dh = q[a] - F[kFHI + a];
-            const double d = fmax(0.0, fmax(dl, dh));
-            d2 = fma(d, d, d2);
+              for (int a = 0; a < 3; ++a) {
+                const double dl = F[kFLO + a] - q[a], dh = q[a] - F[kFHI + a];
+                const double d = fmax(0.0, fmax(dl, dh));
+                d2 = fma(d, d, d2);
+              }
+              hit = d2 < h2;
+            }
           }
-          if (d2 < h2) visit(f);
+          unsigned m = __ballot_sync(0xffffffffu, hit);
+          while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            visit(__shfl_sync(0xffffffffu, f, b));
+          }
         }
       }
 }
 
-// whether any face box comes within h of the query (the loops of for_candidates, stopping at the first).  A cell
+// whether any face box comes within h of the query (the cells of for_candidates_warp, stopping at the first hit),
+// for a whole warp (every lane calls it with the same query): the items of a cell are tested 32 at a time.  A cell
 // whose own box is h or more from the query is skipped: a face box within h of the query has its point nearest to the
-// query in a cell within h, and every cell its box overlaps lists the face.
-__device__ __forceinline__ bool has_candidate(const MeshView& M, const double q[3], double h) {
+// query in a cell within h, and every cell its box overlaps lists the face (a relative margin far above the rounding
+// of the cell boxes: a cell is only skipped when clearly out of reach).
+__device__ __forceinline__ bool has_candidate_warp(const MeshView& M, const double q[3], double h, int lane) {
   const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
             cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
   const int x0 = max(cx - 1, 0), x1 = min(cx + 1, M.nx - 1), y0 = max(cy - 1, 0), y1 = min(cy + 1, M.ny - 1),
             z0 = max(cz - 1, 0), z1 = min(cz + 1, M.nz - 1);
   const double h2 = h * h;
-  // squared distance from the query to the slab of cell index i along one axis
   auto gap2 = [&](double x, double lo, int i) {
     const double a = fma((double)i, M.cell, lo), d = fmax(0.0, fmax(a - x, x - (a + M.cell)));
     return d * d;
@@ -185,18 +219,23 @@ __device__ __forceinline__ bool has_candidate(const MeshView& M, const double q[
   for (int k = z0; k <= z1; ++k)
     for (int j = y0; j <= y1; ++j)
       for (int i = x0; i <= x1; ++i) {
-        // (a relative margin far above the rounding of the cell boxes: a cell is only skipped when clearly out of reach)
         if (gap2(q[0], M.lo0, i) + gap2(q[1], M.lo1, j) + gap2(q[2], M.lo2, k) >= h2 * (1.0 + 1e-9)) continue;
         const int c = (k * M.ny + j) * M.nx + i;
-        for (int it = M.cstart[c]; it < M.cstart[c + 1]; ++it) {
-          const double* F = M.fdata + (int64_t)M.citems[it] * kFaceDoubles;
-          double d2 = 0.0;
+        const int e = M.cstart[c + 1];
+        for (int base = M.cstart[c]; base < e; base += 32) {
+          const int it = base + lane;
+          bool hit = false;
+          if (it < e) {
+            const double* F = M.fdata + (int64_t)M.citems[it] * kFaceDoubles;
+            double d2 = 0.0;
 #pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            const double d = fmax(0.0, fmax(F[kFLO + a] - q[a], q[a] - F[kFHI + a]));
-            d2 = fma(d, d, d2);
+            for (int a = 0; a < 3; ++a) {
+              const double d = fmax(0.0, fmax(F[kFLO + a] - q[a], q[a] - F[kFHI + a]));
+              d2 = fma(d, d, d2);
+            }
+            hit = d2 < h2;
           }
-          if (d2 < h2) return true;
+          if (__any_sync(0xffffffffu, hit)) return true;
         }
       }
   return false;
@@ -480,8 +519,10 @@ __device__ __forceinline__ double tri_dist2(const double P[3][3]) {
 // Assembly (W~ units), per edge:  M0 += J0;  M1_i += N_i J1 + mu_i LK1;
 // M2_ij += N_i N_j (J2 + J5) + (N_i mu_j + mu_i N_j) LK2 + mu_i mu_j w LK2b + (mu_i t_j + mu_j t_i) TK2 / 2 - d_ij J5;
 // G0_i -= N_i J3;  G1_ij -= z N_i N_j J3 + mu_i N_j LW;  H_ij += z N_i N_j J4 + (N_i mu_j + mu_i N_j) LL / 2.
-// Lane k < 28 adds the term of accumulator k: every term is one bilinear form in the edge vectors N, mu, t whose
-// coefficients a lane selects by its accumulator's type, so all lanes run the same instructions.
+// Lane k < 28 adds the term of accumulator k: every term is one bilinear form in the vectors N, mu, t whose
+// coefficients a lane selects by its accumulator's type, so all lanes run the same instructions.  The J terms multiply
+// face quantities (N, z) only, so they are added once per face with J summed over the face's edges; the LK / TK / LW
+// / LL terms, which carry the edge's mu and t, once per edge.
 enum { kTM0, kTM1, kTM2, kTG0, kTG1, kTH, kTNone };
 struct AccSlot {
   int type, i, j;
@@ -501,33 +542,41 @@ __device__ __forceinline__ AccSlot acc_slot(int k) {
 
 __device__ __forceinline__ double pick3(const double v[3], int i) { return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]); }
 
-__device__ __forceinline__ double edge_term(const AccSlot& sl, const double N[3], double z, const double t[3],
-                                            const double mu[3], double w, const EdgeSums& S) {
+// the terms of accumulator sl with the edge's vectors mu, t (per edge)
+__device__ __forceinline__ double edge_term_mu(const AccSlot& sl, const double N[3], const double t[3],
+                                               const double mu[3], double w, const EdgeSums& S) {
   const double Ni = pick3(N, sl.i), Nj = pick3(N, sl.j), mi = pick3(mu, sl.i), mj = pick3(mu, sl.j);
   const double ti = pick3(t, sl.i), tj = pick3(t, sl.j);
-  const double NN = Ni * Nj, X = Ni * mj + mi * Nj, MN = mi * Nj, MM = mi * mj, MT = 0.5 * (mi * tj + mj * ti);
-  const double dij = sl.i == sl.j ? 1.0 : 0.0;
+  const double X = Ni * mj + mi * Nj, MN = mi * Nj, MM = mi * mj, MT = 0.5 * (mi * tj + mj * ti);
   const int ty = sl.type;
-  const double cC = ty == kTM0 ? S.J[0] : 0.0;
-  const double cNi = ty == kTM1 ? S.J[1] : (ty == kTG0 ? -S.J[3] : 0.0);
   const double cMi = ty == kTM1 ? S.LK1 : 0.0;
-  const double cNN = ty == kTM2 ? S.J[2] + S.J[5] : (ty == kTG1 ? -z * S.J[3] : (ty == kTH ? z * S.J[4] : 0.0));
   const double cX = ty == kTM2 ? S.LK2 : (ty == kTH ? 0.5 * S.LL : 0.0);
   const double cMN = ty == kTG1 ? -S.LW : 0.0;
   const double cMM = ty == kTM2 ? w * S.LK2b : 0.0;
   const double cMT = ty == kTM2 ? S.TK2 : 0.0;
-  const double cD = ty == kTM2 ? -S.J[5] : 0.0;
-  return cC + Ni * cNi + mi * cMi + NN * cNN + X * cX + MN * cMN + MM * cMM + MT * cMT + dij * cD;
+  return mi * cMi + X * cX + MN * cMN + MM * cMM + MT * cMT;
 }
 
-// the contribution of face f to the row's accumulators (the warp's shared array Av), computed by the whole warp: the
-// geometry is the same in every lane, the quadrature nodes of an edge (12 or 16 per panel) are spread over the lanes and
+// the terms of accumulator sl with the J sums (face quantities N, z only: once per face, J summed over its edges)
+__device__ __forceinline__ double face_term_j(const AccSlot& sl, const double N[3], double z, const double J[6]) {
+  const double Ni = pick3(N, sl.i), Nj = pick3(N, sl.j);
+  const double NN = Ni * Nj, dij = sl.i == sl.j ? 1.0 : 0.0;
+  const int ty = sl.type;
+  const double cC = ty == kTM0 ? J[0] : 0.0;
+  const double cNi = ty == kTM1 ? J[1] : (ty == kTG0 ? -J[3] : 0.0);
+  const double cNN = ty == kTM2 ? J[2] + J[5] : (ty == kTG1 ? -z * J[3] : (ty == kTH ? z * J[4] : 0.0));
+  const double cD = ty == kTM2 ? -J[5] : 0.0;
+  return cC + Ni * cNi + NN * cNN + dij * cD;
+}
+
+// the contribution of face f to the row's accumulators (lane k < 28 holds accumulator k in acc), computed by the
+// whole warp: the geometry is the same in every lane, the quadrature nodes of an edge (12 or 16 per panel) are spread over the lanes and
 // their sums reduced by a fixed butterfly, then lane k adds the edge's term of accumulator k (slot: this lane's).
 // Everything is linear in the per-edge integrals.  Faces that do not meet the support contribute exactly nothing:
 // skipped.  q in world units, ih = 1 / support.
 template <class M>
 __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], double ih, PanelList& PL, int lane,
-                                  const AccSlot& slot, double* __restrict__ Av) {
+                                  const AccSlot& slot, double& acc) {
   const double* F = Mv.fdata + (int64_t)f * kFaceDoubles;
   double P[3][3];
 #pragma unroll
@@ -538,6 +587,8 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
   const double N[3] = {F[kFN], F[kFN + 1], F[kFN + 2]};
   const double z = N[0] * P[0][0] + N[1] * P[0][1] + N[2] * P[0][2];
   const double a = fabs(z), sg = z > 0.0 ? 1.0 : (z < 0.0 ? -1.0 : 0.0);
+  double Jf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};          // the face's J sums over its edges
+  double out = 0.0;                                       // the face's summed angles beyond the support
   for (int e = 0; e < 3; ++e) {
     const double t[3] = {F[kFT + 3 * e], F[kFT + 3 * e + 1], F[kFT + 3 * e + 2]};
     const double mu[3] = {F[kFMU + 3 * e], F[kFMU + 3 * e + 1], F[kFMU + 3 * e + 2]};
@@ -595,26 +646,29 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
       __syncwarp();                                   // the list is rebuilt for the next edge
     }
     if (w != 0.0) {
-      double out = 0.0;
       if (s1 > s0) {
         if (lo < s0) out += angle_between(w, lo, s0);
         if (s1 < hi) out += angle_between(w, s1, hi);
       } else {
-        out = angle_between(w, lo, hi);
-      }
-      if (out != 0.0) {
-        S.J[0] -= aval_a<M, 0, 1>(a, z, sg) * out;
-        S.J[1] -= aval_a<M, 1, 2>(a, z, sg) * out;
-        S.J[2] -= aval_a<M, 2, 3>(a, z, sg) * out;
-        S.J[3] -= aval_a<M, 3, 0>(a, z, sg) * out;
-        S.J[4] -= aval_a<M, 4, 0>(a, z, sg) * out;
-        S.J[5] -= aval_a<M, 5, 1>(a, z, sg) * out;
+        out += angle_between(w, lo, hi);
       }
     }
-    // assembly into the warp's shared accumulators, accumulator k by lane k (the sums are in every lane)
-    if (lane < 28) Av[lane] += edge_term(slot, N, z, t, mu, w, S);
-    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 6; ++i) Jf[i] += S.J[i];
+    // assembly of the terms with the edge's vectors: lane k adds its accumulator's (the sums are in every lane)
+    if (lane < 28) acc += edge_term_mu(slot, N, t, mu, w, S);
   }
+  // the J terms multiply face quantities only: the face's three edges summed, with the angle part of the edges
+  // beyond the support (a face constant times the summed angle) taken once
+  if (out != 0.0) {
+    Jf[0] -= aval_a<M, 0, 1>(a, z, sg) * out;
+    Jf[1] -= aval_a<M, 1, 2>(a, z, sg) * out;
+    Jf[2] -= aval_a<M, 2, 3>(a, z, sg) * out;
+    Jf[3] -= aval_a<M, 3, 0>(a, z, sg) * out;
+    Jf[4] -= aval_a<M, 4, 0>(a, z, sg) * out;
+    Jf[5] -= aval_a<M, 5, 1>(a, z, sg) * out;
+  }
+  if (lane < 28) acc += face_term_j(slot, N, z, Jf);
 }
 
 // ------------------------------------------------------------------------------------------ kernels
@@ -691,31 +745,25 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_rownear(MeshView M, const
                                                               const int32_t* __restrict__ nnear,
                                                               int32_t* __restrict__ ind, int32_t* __restrict__ work,
                                                               int32_t* __restrict__ nwork) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // one warp per listed row (the warps of the grid stride over them): the column's faces and the candidate cells'
+  // items are tested 32 at a time
+  const int lane = threadIdx.x & 31;
   const int64_t m = *nnear;
-  if ((int64_t)blockIdx.x * blockDim.x >= m) return;            // whole block past the listed rows
-  bool has = false;
-  int32_t row = 0;
-  if (t < m) {
-    row = near[t];
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x / 32);
+  for (int64_t t = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; t < m; t += warps) {
+    const int32_t row = near[t];
     const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
     const double h = sup[row];
     const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
               cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
     const bool in_grid = cx >= 0 && cy >= 0 && cz >= 0 && cx < M.nx && cy < M.ny && cz < M.nz;
     const uint8_t f = in_grid ? M.cflag[((int64_t)cz * M.ny + cy) * M.nx + cx] : (uint8_t)0;
-    ind[row] = (f & kCellEmpty) ? ((f & kCellInside) ? 1 : 0) : mesh_inside(M, q[0], q[1], q[2]);
-    has = has_candidate(M, q, h);
-  }
-  // warp-aggregated append of the rows with candidate faces (their order is irrelevant: each row is computed alone)
-  const unsigned mask = __ballot_sync(0xffffffffu, has);
-  if (mask) {
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(nwork, __popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (has) work[base + __popc(mask & ((1u << lane) - 1))] = row;
+    const int inside = (f & kCellEmpty) ? ((f & kCellInside) ? 1 : 0) : mesh_inside_warp(M, q[0], q[1], q[2], lane);
+    const bool has = has_candidate_warp(M, q, h, lane);
+    if (lane == 0) {
+      ind[row] = inside;
+      if (has) work[atomicAdd(nwork, 1)] = row;     // (the order is irrelevant: each row is computed alone)
+    }
   }
 }
 
@@ -795,9 +843,10 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
     const int64_t row = work[slot];
     const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
     const double h = sup[row], ih = 1.0 / h;
-    if (lane < 28) acc[wib][lane] = 0.0;
+    double mine = 0.0;                                   // accumulator `lane` of the row (lanes < 28)
+    for_candidates_warp(Mv, q, h, lane, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], lane, aslot, mine); });
+    if (lane < 28) acc[wib][lane] = mine;
     __syncwarp();
-    for_candidates(Mv, q, h, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], lane, aslot, acc[wib]); });
     if (lane == 0) {
       Acc28 A;
 #pragma unroll
@@ -838,7 +887,8 @@ int launch_mesh(const Mesh* m, const double* pos, const double* sup, int64_t n, 
   WSB_CUDA(cudaMemsetAsync(nwork, 0, 3 * sizeof(int32_t), st));      // work rows, grab counter, listed rows
   k_mesh_rowinfo<<<grid, kMeshThreads, 0, st>>>(v, pos, sup, n, ind, near, nwork + 2);
   WSB_CUDA(cudaGetLastError());
-  k_mesh_rownear<<<grid, kMeshThreads, 0, st>>>(v, pos, sup, near, nwork + 2, ind, work, nwork);
+  const unsigned grid_near = (unsigned)std::min<int64_t>((n + kMeshThreads / 32 - 1) / (kMeshThreads / 32), 8192);
+  k_mesh_rownear<<<grid_near, kMeshThreads, 0, st>>>(v, pos, sup, near, nwork + 2, ind, work, nwork);
   WSB_CUDA(cudaGetLastError());
   k_mesh_rows<M><<<grid, kMeshThreads, 0, st>>>(sup, n, ind, out);
   WSB_CUDA(cudaGetLastError());
