@@ -159,6 +159,51 @@ __device__ __forceinline__ int mesh_inside_warp(const MeshView& M, double x, dou
 // whole warp with one query: the lanes test 32 items of a cell at a time, and the faces that pass are visited one after
 // the other, warp-uniformly, in cell order and item order within a cell -- a fixed order, so the sums the visits
 // accumulate do not depend on the launch.
+// The cells of the block x0..x1, y0..y1, z0..z1 (at most 27) for a warp: lane l < number of cells takes cell ordinal
+// l (z outermost, then y, then x -- the order of nested loops) and returns its first item (beg) and the exclusive
+// prefix of the items of the cells before it (pref; a cell `keep` rejects has none).  Returns the block's total.
+template <class Keep>
+__device__ __forceinline__ int block_cells(const MeshView& M, int x0, int x1, int y0, int y1, int z0, int z1, int lane,
+                                           Keep&& keep, int& beg, int& pref) {
+  const int nxr = x1 - x0 + 1, nyr = y1 - y0 + 1, nc = nxr * nyr * (z1 - z0 + 1);
+  int cnt = 0;
+  beg = 0;
+  if (lane < nc) {
+    const int i = x0 + lane % nxr, j = y0 + (lane / nxr) % nyr, k = z0 + lane / (nxr * nyr);
+    if (keep(i, j, k)) {
+      const int c = (k * M.ny + j) * M.nx + i;
+      beg = M.cstart[c];
+      cnt = M.cstart[c + 1] - beg;
+    }
+  }
+  int inc = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  pref = inc - cnt;
+  return __shfl_sync(0xffffffffu, inc, 31);
+}
+
+// the cell ordinal of flattened item t (< total): the last lane whose prefix is <= t (prefixes do not decrease with
+// the lane; an empty cell shares the next cell's prefix, lanes past the cells hold the total), by a binary search over
+// the lanes; every lane of the warp takes part
+__device__ __forceinline__ int cell_ordinal(int pref, int t) {
+  int lo = 0;
+#pragma unroll
+  for (int step = 16; step > 0; step >>= 1) {
+    const int pv = __shfl_sync(0xffffffffu, pref, lo + step);
+    if (pv <= t) lo += step;
+  }
+  return lo;
+}
+
+// The faces of the 27 cells around the query's cell whose box comes within h of the query; a face listed in several
+// of those cells is taken in one of them only (the lowest corner of its box inside the 27-cell block).  Called by a
+// whole warp with one query: the (cell, item) pairs of the block are flattened over the lanes (32 at a time, whatever
+// cell they belong to), and the faces that pass are visited one after the other, warp-uniformly, in cell order and
+// item order within a cell -- a fixed order, so the sums the visits accumulate do not depend on the launch.
 template <class Visit>
 __device__ __forceinline__ void for_candidates_warp(const MeshView& M, const double q[3], double h, int lane,
                                                     Visit&& visit) {
@@ -166,78 +211,80 @@ __device__ __forceinline__ void for_candidates_warp(const MeshView& M, const dou
             cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
   const int x0 = max(cx - 1, 0), x1 = min(cx + 1, M.nx - 1), y0 = max(cy - 1, 0), y1 = min(cy + 1, M.ny - 1),
             z0 = max(cz - 1, 0), z1 = min(cz + 1, M.nz - 1);
+  if (x0 > x1 || y0 > y1 || z0 > z1) return;
   const double h2 = h * h;
-  for (int k = z0; k <= z1; ++k)
-    for (int j = y0; j <= y1; ++j)
-      for (int i = x0; i <= x1; ++i) {
-        const int c = (k * M.ny + j) * M.nx + i;
-        const int e = M.cstart[c + 1];
-        for (int base = M.cstart[c]; base < e; base += 32) {
-          const int it = base + lane;
-          int f = -1;
-          bool hit = false;
-          if (it < e) {
-            f = M.citems[it];
-            const int* fc = M.fcell + 3 * f;
-            if (max(fc[0], cx - 1) == i && max(fc[1], cy - 1) == j && max(fc[2], cz - 1) == k) {
-              const double* F = M.fdata + (int64_t)f * kFaceDoubles;
-              double d2 = 0.0;
+  const int nxr = x1 - x0 + 1, nyr = y1 - y0 + 1;
+  int beg, pref;
+  const int total = block_cells(M, x0, x1, y0, y1, z0, z1, lane, [](int, int, int) { return true; }, beg, pref);
+  for (int base = 0; base < total; base += 32) {
+    const int t = base + lane;
+    const int o = cell_ordinal(pref, t);
+    const int b = __shfl_sync(0xffffffffu, beg, o), p = __shfl_sync(0xffffffffu, pref, o);
+    int f = -1;
+    bool hit = false;
+    if (t < total) {
+      const int i = x0 + o % nxr, j = y0 + (o / nxr) % nyr, k = z0 + o / (nxr * nyr);
+      f = M.citems[b + (t - p)];
+      const int* fc = M.fcell + 3 * f;
+      if (max(fc[0], cx - 1) == i && max(fc[1], cy - 1) == j && max(fc[2], cz - 1) == k) {
+        const double* F = M.fdata + (int64_t)f * kFaceDoubles;
+        double d2 = 0.0;
 #pragma unroll
-              for (int a = 0; a < 3; ++a) {
-                const double dl = F[kFLO + a] - q[a], dh = q[a] - F[kFHI + a];
-                const double d = fmax(0.0, fmax(dl, dh));
-                d2 = fma(d, d, d2);
-              }
-              hit = d2 < h2;
-            }
-          }
-          unsigned m = __ballot_sync(0xffffffffu, hit);
-          while (m) {
-            const int b = __ffs(m) - 1;
-            m &= m - 1;
-            visit(__shfl_sync(0xffffffffu, f, b));
-          }
+        for (int a = 0; a < 3; ++a) {
+          const double dl = F[kFLO + a] - q[a], dh = q[a] - F[kFHI + a];
+          const double d = fmax(0.0, fmax(dl, dh));
+          d2 = fma(d, d, d2);
         }
+        hit = d2 < h2;
       }
+    }
+    unsigned m = __ballot_sync(0xffffffffu, hit);
+    while (m) {
+      const int bl = __ffs(m) - 1;
+      m &= m - 1;
+      visit(__shfl_sync(0xffffffffu, f, bl));
+    }
+  }
 }
 
 // whether any face box comes within h of the query (the cells of for_candidates_warp, stopping at the first hit),
-// for a whole warp (every lane calls it with the same query): the items of a cell are tested 32 at a time.  A cell
-// whose own box is h or more from the query is skipped: a face box within h of the query has its point nearest to the
-// query in a cell within h, and every cell its box overlaps lists the face (a relative margin far above the rounding
-// of the cell boxes: a cell is only skipped when clearly out of reach).
+// for a whole warp (every lane calls it with the same query): the (cell, item) pairs are flattened over the lanes.
+// A cell whose own box is h or more from the query is skipped: a face box within h of the query has its point nearest
+// to the query in a cell within h, and every cell its box overlaps lists the face (a relative margin far above the
+// rounding of the cell boxes: a cell is only skipped when clearly out of reach).
 __device__ __forceinline__ bool has_candidate_warp(const MeshView& M, const double q[3], double h, int lane) {
   const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
             cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
   const int x0 = max(cx - 1, 0), x1 = min(cx + 1, M.nx - 1), y0 = max(cy - 1, 0), y1 = min(cy + 1, M.ny - 1),
             z0 = max(cz - 1, 0), z1 = min(cz + 1, M.nz - 1);
+  if (x0 > x1 || y0 > y1 || z0 > z1) return false;
   const double h2 = h * h;
   auto gap2 = [&](double x, double lo, int i) {
     const double a = fma((double)i, M.cell, lo), d = fmax(0.0, fmax(a - x, x - (a + M.cell)));
     return d * d;
   };
-  for (int k = z0; k <= z1; ++k)
-    for (int j = y0; j <= y1; ++j)
-      for (int i = x0; i <= x1; ++i) {
-        if (gap2(q[0], M.lo0, i) + gap2(q[1], M.lo1, j) + gap2(q[2], M.lo2, k) >= h2 * (1.0 + 1e-9)) continue;
-        const int c = (k * M.ny + j) * M.nx + i;
-        const int e = M.cstart[c + 1];
-        for (int base = M.cstart[c]; base < e; base += 32) {
-          const int it = base + lane;
-          bool hit = false;
-          if (it < e) {
-            const double* F = M.fdata + (int64_t)M.citems[it] * kFaceDoubles;
-            double d2 = 0.0;
+  auto reach = [&](int i, int j, int k) {
+    return gap2(q[0], M.lo0, i) + gap2(q[1], M.lo1, j) + gap2(q[2], M.lo2, k) < h2 * (1.0 + 1e-9);
+  };
+  int beg, pref;
+  const int total = block_cells(M, x0, x1, y0, y1, z0, z1, lane, reach, beg, pref);
+  for (int base = 0; base < total; base += 32) {
+    const int t = base + lane;
+    const int o = cell_ordinal(pref, t);
+    const int b = __shfl_sync(0xffffffffu, beg, o), p = __shfl_sync(0xffffffffu, pref, o);
+    bool hit = false;
+    if (t < total) {
+      const double* F = M.fdata + (int64_t)M.citems[b + (t - p)] * kFaceDoubles;
+      double d2 = 0.0;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              const double d = fmax(0.0, fmax(F[kFLO + a] - q[a], q[a] - F[kFHI + a]));
-              d2 = fma(d, d, d2);
-            }
-            hit = d2 < h2;
-          }
-          if (__any_sync(0xffffffffu, hit)) return true;
-        }
+      for (int a = 0; a < 3; ++a) {
+        const double d = fmax(0.0, fmax(F[kFLO + a] - q[a], q[a] - F[kFHI + a]));
+        d2 = fma(d, d, d2);
       }
+      hit = d2 < h2;
+    }
+    if (__any_sync(0xffffffffu, hit)) return true;
+  }
   return false;
 }
 
