@@ -452,6 +452,14 @@ struct PanelList {
   int off[kMaxPanels + 1];    // first node of each panel; off[np] = all nodes
 };
 
+// an edge of the face being evaluated, relative to the query in units of the support: tangent t and in-plane normal
+// mu, the foot's signed distance w to the edge line, the edge's ends lo, hi along t from the foot, c^2 = z^2 + w^2,
+// the part [s0, s1] inside the support, and its panel count
+struct EdgeGeo {
+  double t[3], mu[3], w, lo, hi, c2, s0, s1;
+  int np;
+};
+
 template <class M>
 __device__ int build_panels(PanelList& PL, double s0, double s1, double c) {
   int np = 0, nodes = 0;
@@ -622,8 +630,8 @@ __device__ __forceinline__ double face_term_j(const AccSlot& sl, const double N[
 // Everything is linear in the per-edge integrals.  Faces that do not meet the support contribute exactly nothing:
 // skipped.  q in world units, ih = 1 / support.
 template <class M>
-__device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], double ih, PanelList& PL, int lane,
-                                  const AccSlot& slot, double& acc) {
+__device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], double ih, PanelList* PL3,
+                                  EdgeGeo* G3, int lane, const AccSlot& slot, double& acc) {
   const double* F = Mv.fdata + (int64_t)f * kFaceDoubles;
   double P[3][3];
 #pragma unroll
@@ -634,30 +642,49 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
   const double N[3] = {F[kFN], F[kFN + 1], F[kFN + 2]};
   const double z = N[0] * P[0][0] + N[1] * P[0][1] + N[2] * P[0][2];
   const double a = fabs(z), sg = z > 0.0 ? 1.0 : (z < 0.0 ? -1.0 : 0.0);
-  double Jf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};          // the face's J sums over its edges
-  double out = 0.0;                                       // the face's summed angles beyond the support
-  for (int e = 0; e < 3; ++e) {
-    const double t[3] = {F[kFT + 3 * e], F[kFT + 3 * e + 1], F[kFT + 3 * e + 2]};
-    const double mu[3] = {F[kFMU + 3 * e], F[kFMU + 3 * e + 1], F[kFMU + 3 * e + 2]};
+  // the three edges' geometry and panel lists, lane e for edge e, side by side (the previous face's lists are read)
+  __syncwarp();
+  if (lane < 3) {
+    const int e = lane;
+    EdgeGeo& ge = G3[e];
+    // the edge's first vertex relative to the query: the same operations as P[e]
+    const double pe[3] = {(F[kFV + 3 * e] - q[0]) * ih, (F[kFV + 3 * e + 1] - q[1]) * ih,
+                          (F[kFV + 3 * e + 2] - q[2]) * ih};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      ge.t[k] = F[kFT + 3 * e + k];
+      ge.mu[k] = F[kFMU + 3 * e + k];
+    }
     const double len = F[kFLEN + e] * ih;
-    const double w = mu[0] * P[e][0] + mu[1] * P[e][1] + mu[2] * P[e][2];
-    const double lo = t[0] * P[e][0] + t[1] * P[e][1] + t[2] * P[e][2], hi = lo + len;
-    const double c2 = fma(z, z, w * w), c = sqrt(c2);
+    ge.w = ge.mu[0] * pe[0] + ge.mu[1] * pe[1] + ge.mu[2] * pe[2];
+    ge.lo = ge.t[0] * pe[0] + ge.t[1] * pe[1] + ge.t[2] * pe[2];
+    ge.hi = ge.lo + len;
+    ge.c2 = fma(z, z, ge.w * ge.w);
+    const double c = sqrt(ge.c2);
     double s0 = 0.0, s1 = 0.0;
     if (c < 1.0) {
       const double L = sqrt((1.0 - c) * (1.0 + c));
-      s0 = fmax(lo, -L);
-      s1 = fmin(hi, L);
+      s0 = fmax(ge.lo, -L);
+      s1 = fmin(ge.hi, L);
     }
+    ge.s0 = s0;
+    ge.s1 = s1;
+    ge.np = s1 > s0 ? build_panels<M>(PL3[e], s0, s1, c) : 0;
+  }
+  __syncwarp();
+  double Jf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};          // the face's J sums over its edges
+  double out = 0.0;                                       // the face's summed angles beyond the support
+  for (int e = 0; e < 3; ++e) {
+    const EdgeGeo& ge = G3[e];
+    const PanelList& PL = PL3[e];
+    const double t[3] = {ge.t[0], ge.t[1], ge.t[2]}, mu[3] = {ge.mu[0], ge.mu[1], ge.mu[2]};
+    const double w = ge.w, lo = ge.lo, hi = ge.hi, c2 = ge.c2, s0 = ge.s0, s1 = ge.s1;
     EdgeSums S;
 #pragma unroll
     for (int i = 0; i < 6; ++i) S.J[i] = 0.0;
     S.LK1 = S.LK2 = S.LK2b = S.TK2 = S.LW = S.LL = 0.0;
     if (s1 > s0) {
-      int np = 0;
-      if (lane == 0) np = build_panels<M>(PL, s0, s1, c);
-      np = __shfl_sync(0xffffffffu, np, 0);
-      __syncwarp();
+      const int np = ge.np;
       if (w != 0.0) {
         int p = 0;
         for (int k = lane; k < PL.off[np]; k += 32) {
@@ -690,7 +717,6 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
       S.TK2 = v[9];
       S.LW = v[10];
       S.LL = v[11];
-      __syncwarp();                                   // the list is rebuilt for the next edge
     }
     if (w != 0.0) {
       if (s1 > s0) {
@@ -877,7 +903,8 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
                                                            const int32_t* __restrict__ work,
                                                            const int32_t* __restrict__ nwork,
                                                            int32_t* __restrict__ grab, double* __restrict__ out) {
-  __shared__ PanelList pl[kMeshThreads / 32];
+  __shared__ PanelList pl[kMeshThreads / 32][3];
+  __shared__ EdgeGeo eg[kMeshThreads / 32][3];
   __shared__ double acc[kMeshThreads / 32][28];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const AccSlot aslot = acc_slot(lane);                  // the accumulator this lane assembles
@@ -891,7 +918,7 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
     const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
     const double h = sup[row], ih = 1.0 / h;
     double mine = 0.0;                                   // accumulator `lane` of the row (lanes < 28)
-    for_candidates_warp(Mv, q, h, lane, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], lane, aslot, mine); });
+    for_candidates_warp(Mv, q, h, lane, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], eg[wib], lane, aslot, mine); });
     if (lane < 28) acc[wib][lane] = mine;
     __syncwarp();
     if (lane == 0) {
