@@ -210,3 +210,4 @@ def test_light_lane_takes_short_requests():
     assert torch.equal(out[0][0], out[1][0])
     for k in OUT_KEYS:
         assert torch.equal(out[0][1][k], out[1][1][k]), k
+

@@ -35,7 +35,8 @@ Scheduling (one host thread, the caller's):
   request's outputs;
 * admission: a batch is launched while the device memory it reserves fits `hbm_budget`, and `submit` blocks (it
   keeps polling) while the outputs of queued and in-flight requests would exceed it -- back-pressure instead of an
-  unbounded queue;
+  unbounded queue; a completed request's outputs are the caller's until it releases them, so a caller should
+  release results as it takes them;
 * latency of a request = completion (its batch's end event observed) - arrival; `stats()` reports p50 / p99.
 """
 import itertools
@@ -265,12 +266,7 @@ class BoundaryServer:
         if self._is_mesh(scene_id) or self._is_spheres(scene_id):
             return self._submit_mesh(r)
         B, n = len(self.scenes[scene_id][0].bodies), len(pos)
-        nbytes = 8 * (13 * B * n + (2 * n if r.grad else 0))
-        # back-pressure: a full server makes the caller wait (polling) instead of queueing without bound
-        while self.held_bytes + nbytes > self.hbm_budget and (self.n_queued or self.n_inflight):
-            self.poll()
-        self.held_bytes += nbytes
-        r.nbytes = nbytes
+        r.nbytes = self._admit(13 * B * n + (2 * n if r.grad else 0))
         flat = self._take(13 * B * n + (2 * n if r.grad else 0))          # one buffer, from the pool when possible
         r.flat = flat
         r.result, off = {}, 0
@@ -293,11 +289,7 @@ class BoundaryServer:
         if r.pos.dim() != 2 or r.pos.shape[1] != width:
             raise ValueError(f"BoundaryServer: this scene's requests take rows [n, {width}]")
         n = len(r.pos)
-        nbytes = 8 * 28 * n
-        while self.held_bytes + nbytes > self.hbm_budget and (self.n_queued or self.n_inflight):
-            self.poll()
-        self.held_bytes += nbytes
-        r.nbytes = nbytes
+        r.nbytes = self._admit(28 * n)
         r.flat = self._take(28 * n)
         r.result = {"channels": r.flat[:28 * n].view(n, 28)}
         self.requests[r.rid] = r
@@ -321,6 +313,22 @@ class BoundaryServer:
         r.result = None
         r.flat = None
 
+    @staticmethod
+    def _size_class(n):
+        """the float64 elements of the pooled buffer that holds n (a power of two, at least 4096)."""
+        return max(1 << 12, 1 << (int(n) - 1).bit_length())
+
+    def _admit(self, n):
+        """back-pressure for a request of n float64 outputs: the outputs of queued and in-flight requests count against
+        hbm_budget; while they would exceed it the caller waits (polling).  A completed request's outputs are the
+        caller's until it releases them (a caller that holds many unreleased results holds that memory).  Returns the
+        bytes counted (the pooled size class)."""
+        nbytes = 8 * self._size_class(n)
+        while self.held_bytes + nbytes > self.hbm_budget and (self.n_queued or self.n_inflight):
+            self.poll()
+        self.held_bytes += nbytes
+        return nbytes
+
     def _support_vec(self, value, n):
         """a view of n copies of `value` from a resident vector (grown geometrically; no allocation per request)."""
         v = self.support_vecs.get(value)
@@ -333,7 +341,7 @@ class BoundaryServer:
     def _take(self, n):
         """a float64 buffer of at least n elements: pooled size classes (powers of two) avoid allocator calls in the
         steady state."""
-        cls = max(1 << 12, 1 << (int(n) - 1).bit_length())
+        cls = self._size_class(n)
         lst = self.pool.get(cls)
         if lst:
             self.pooled_bytes -= 8 * cls
