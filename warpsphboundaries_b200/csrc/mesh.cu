@@ -153,12 +153,57 @@ __device__ __forceinline__ int mesh_inside_warp(const MeshView& M, double x, dou
   return crossings & 1;
 }
 
+// squared distance from the origin to the triangle P (unit coordinates relative to the query)
+__device__ __forceinline__ double tri_dist2(const double P[3][3]) {
+  // closest point by the Voronoi-region tests on the barycentric parameters (vertex, edge or interior region)
+  const double* A = P[0];
+  const double ab[3] = {P[1][0] - A[0], P[1][1] - A[1], P[1][2] - A[2]};
+  const double ac[3] = {P[2][0] - A[0], P[2][1] - A[1], P[2][2] - A[2]};
+  const double ap[3] = {-A[0], -A[1], -A[2]};
+  auto dot = [](const double* x, const double* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+  const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+  double cp[3];
+  auto setp = [&](double v, double w) {
+    for (int k = 0; k < 3; ++k) cp[k] = A[k] + v * ab[k] + w * ac[k];
+  };
+  if (d1 <= 0.0 && d2 <= 0.0) {
+    setp(0.0, 0.0);
+  } else {
+    const double bp[3] = {-P[1][0], -P[1][1], -P[1][2]};
+    const double e3 = dot(ab, bp), e4 = dot(ac, bp);
+    if (e3 >= 0.0 && e4 <= e3) {
+      setp(1.0, 0.0);
+    } else {
+      const double vc = d1 * e4 - e3 * d2;
+      if (vc <= 0.0 && d1 >= 0.0 && e3 <= 0.0) {
+        setp(d1 / (d1 - e3), 0.0);
+      } else {
+        const double cpn[3] = {-P[2][0], -P[2][1], -P[2][2]};
+        const double e5 = dot(ab, cpn), e6 = dot(ac, cpn);
+        if (e6 >= 0.0 && e5 <= e6) {
+          setp(0.0, 1.0);
+        } else {
+          const double vb = e5 * d2 - d1 * e6;
+          if (vb <= 0.0 && d2 >= 0.0 && e6 <= 0.0) {
+            setp(0.0, d2 / (d2 - e6));
+          } else {
+            const double va = e3 * e6 - e5 * e4;
+            if (va <= 0.0 && (e4 - e3) >= 0.0 && (e5 - e6) >= 0.0) {
+              const double t = (e4 - e3) / ((e4 - e3) + (e5 - e6));
+              setp(1.0 - t, t);
+            } else {
+              const double den = 1.0 / (va + vb + vc);
+              setp(vb * den, vc * den);
+            }
+          }
+        }
+      }
+    }
+  }
+  return cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2];
+}
+
 // ------------------------------------------------------------------------------------------ candidate faces
-// The faces of the 27 cells around the query's cell whose box comes within h of the query; a face listed in several
-// of those cells is taken in one of them only (the lowest corner of its box inside the 27-cell block).  Called by a
-// whole warp with one query: the lanes test 32 items of a cell at a time, and the faces that pass are visited one after
-// the other, warp-uniformly, in cell order and item order within a cell -- a fixed order, so the sums the visits
-// accumulate do not depend on the launch.
 // The cells of the block x0..x1, y0..y1, z0..z1 (at most 27) for a warp: lane l < number of cells takes cell ordinal
 // l (z outermost, then y, then x -- the order of nested loops) and returns its first item (beg) and the exclusive
 // prefix of the items of the cells before it (pref; a cell `keep` rejects has none).  Returns the block's total.
@@ -199,9 +244,9 @@ __device__ __forceinline__ int cell_ordinal(int pref, int t) {
   return lo;
 }
 
-// The faces of the 27 cells around the query's cell whose box comes within h of the query; a face listed in several
-// of those cells is taken in one of them only (the lowest corner of its box inside the 27-cell block).  Called by a
-// whole warp with one query: the (cell, item) pairs of the block are flattened over the lanes (32 at a time, whatever
+// The faces of the 27 cells around the query's cell that come within h of the query (box first, then the exact
+// triangle distance, both tested by the lanes in parallel); a face listed in several of those cells is taken in one of
+// them only (the lowest corner of its box inside the 27-cell block).  Called by a whole warp with one query: the (cell, item) pairs of the block are flattened over the lanes (32 at a time, whatever
 // cell they belong to), and the faces that pass are visited one after the other, warp-uniformly, in cell order and
 // item order within a cell -- a fixed order, so the sums the visits accumulate do not depend on the launch.
 template <class Visit>
@@ -235,7 +280,16 @@ __device__ __forceinline__ void for_candidates_warp(const MeshView& M, const dou
           const double d = fmax(0.0, fmax(dl, dh));
           d2 = fma(d, d, d2);
         }
-        hit = d2 < h2;
+        if (d2 < h2) {
+          // the exact triangle distance (unit coordinates relative to the query, the operations of the visit's P)
+          const double ih = 1.0 / h;
+          double P[3][3];
+#pragma unroll
+          for (int v = 0; v < 3; ++v)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) P[v][a] = (F[kFV + 3 * v + a] - q[a]) * ih;
+          hit = tri_dist2(P) < 1.0;
+        }
       }
     }
     unsigned m = __ballot_sync(0xffffffffu, hit);
@@ -522,55 +576,6 @@ __device__ __forceinline__ void warp_sum12(double v[12]) {
   for (int x = 0; x < 12; ++x) v[x] = __shfl_sync(0xffffffffu, b[x % 3], 8 * (x / 3));
 }
 
-// squared distance from the origin to the triangle P (unit coordinates relative to the query)
-__device__ __forceinline__ double tri_dist2(const double P[3][3]) {
-  // closest point by the Voronoi-region tests on the barycentric parameters (vertex, edge or interior region)
-  const double* A = P[0];
-  const double ab[3] = {P[1][0] - A[0], P[1][1] - A[1], P[1][2] - A[2]};
-  const double ac[3] = {P[2][0] - A[0], P[2][1] - A[1], P[2][2] - A[2]};
-  const double ap[3] = {-A[0], -A[1], -A[2]};
-  auto dot = [](const double* x, const double* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
-  const double d1 = dot(ab, ap), d2 = dot(ac, ap);
-  double cp[3];
-  auto setp = [&](double v, double w) {
-    for (int k = 0; k < 3; ++k) cp[k] = A[k] + v * ab[k] + w * ac[k];
-  };
-  if (d1 <= 0.0 && d2 <= 0.0) {
-    setp(0.0, 0.0);
-  } else {
-    const double bp[3] = {-P[1][0], -P[1][1], -P[1][2]};
-    const double e3 = dot(ab, bp), e4 = dot(ac, bp);
-    if (e3 >= 0.0 && e4 <= e3) {
-      setp(1.0, 0.0);
-    } else {
-      const double vc = d1 * e4 - e3 * d2;
-      if (vc <= 0.0 && d1 >= 0.0 && e3 <= 0.0) {
-        setp(d1 / (d1 - e3), 0.0);
-      } else {
-        const double cpn[3] = {-P[2][0], -P[2][1], -P[2][2]};
-        const double e5 = dot(ab, cpn), e6 = dot(ac, cpn);
-        if (e6 >= 0.0 && e5 <= e6) {
-          setp(0.0, 1.0);
-        } else {
-          const double vb = e5 * d2 - d1 * e6;
-          if (vb <= 0.0 && d2 >= 0.0 && e6 <= 0.0) {
-            setp(0.0, d2 / (d2 - e6));
-          } else {
-            const double va = e3 * e6 - e5 * e4;
-            if (va <= 0.0 && (e4 - e3) >= 0.0 && (e5 - e6) >= 0.0) {
-              const double t = (e4 - e3) / ((e4 - e3) + (e5 - e6));
-              setp(1.0 - t, t);
-            } else {
-              const double den = 1.0 / (va + vb + vc);
-              setp(vb * den, vc * den);
-            }
-          }
-        }
-      }
-    }
-  }
-  return cp[0] * cp[0] + cp[1] * cp[1] + cp[2] * cp[2];
-}
 
 // Assembly (W~ units), per edge:  M0 += J0;  M1_i += N_i J1 + mu_i LK1;
 // M2_ij += N_i N_j (J2 + J5) + (N_i mu_j + mu_i N_j) LK2 + mu_i mu_j w LK2b + (mu_i t_j + mu_j t_i) TK2 / 2 - d_ij J5;
@@ -629,7 +634,7 @@ __device__ __forceinline__ double face_term_j(const AccSlot& sl, const double N[
 // whole warp: the geometry is the same in every lane, the quadrature nodes of an edge (12 or 16 per panel) are spread over the lanes and
 // their sums reduced by a fixed butterfly, then lane k adds the edge's term of accumulator k (slot: this lane's).
 // Everything is linear in the per-edge integrals.  Faces that do not meet the support contribute exactly nothing:
-// skipped.  q in world units, ih = 1 / support.
+// the candidate search visits only faces within the support.  q in world units, ih = 1 / support.
 template <class M>
 __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], double ih, PanelList* PL3,
                                   EdgeGeo* G3, int lane, const AccSlot& slot, double& acc) {
@@ -639,7 +644,6 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
   for (int v = 0; v < 3; ++v)
 #pragma unroll
     for (int k = 0; k < 3; ++k) P[v][k] = (F[kFV + 3 * v + k] - q[k]) * ih;
-  if (tri_dist2(P) >= 1.0) return;
   const double N[3] = {F[kFN], F[kFN + 1], F[kFN + 2]};
   const double z = N[0] * P[0][0] + N[1] * P[0][1] + N[2] * P[0][2];
   const double a = fabs(z), sg = z > 0.0 ? 1.0 : (z < 0.0 ? -1.0 : 0.0);
