@@ -886,8 +886,8 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_rows(const double* __rest
 
 // one warp per work row; warps take rows from a counter (rows differ in their number of faces), and the row's
 // result does not depend on which warp computes it
-// 3 resident CTAs per SM (at most 168 registers a thread, some spills) measured 12 % faster on B200 than the
-// unconstrained 255 registers (2 CTAs); 4 CTAs spills more and gains nothing
+// 3 resident CTAs per SM (at most 168 registers a thread, some spills): the c3 leg measured 9.0 ms on B200 against
+// 9.9 ms with 2 CTAs (no cap) and 10.2 ms with 4 (128 registers, more spills)
 #ifndef WSB_MESH_MIN_BLOCKS
 #define WSB_MESH_MIN_BLOCKS 3
 #endif
