@@ -2295,54 +2295,90 @@ template <> struct MeshFn<Mesh_cubic, 0> {   // A_K0
   static constexpr double kNu0 = 0.25;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(1.6, x, -2.4), x, 0.0), x, 1.3333333333333333), x, 0.0), x, -0.7); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 1.6; dd = b; b = fma(a, b, -2.4); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1.3333333333333333); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 5;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 1.6; b[1] = fma(a, b[0], -2.4); b[2] = fma(a, b[1], 0.0); b[3] = fma(a, b[2], 1.3333333333333333); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
   static constexpr double kNu1 = 0.26666666666666666;
   __host__ __device__ static __forceinline__ double poly1(double x) { return fma(fma(fma(fma(fma(-0.5333333333333333, x, 2.4), x, -4.0), x, 2.6666666666666665), x, 0.0), x, -0.8); }
   __host__ __device__ static __forceinline__ double dd1(double x, double a) { double dd; double b = -0.5333333333333333; dd = b; b = fma(a, b, 2.4); dd = fma(dd, x, b); b = fma(a, b, -4.0); dd = fma(dd, x, b); b = fma(a, b, 2.6666666666666665); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD1 = 5;
+  __host__ __device__ static __forceinline__ void ddb1(double a, double* b) { b[0] = -0.5333333333333333; b[1] = fma(a, b[0], 2.4); b[2] = fma(a, b[1], -4.0); b[3] = fma(a, b[2], 2.6666666666666665); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh1(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
 };
 template <> struct MeshFn<Mesh_cubic, 1> {   // A_K1
   static constexpr int kNeg = 2;
   static constexpr double kNu0 = 0.055357142857142855;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(1.3714285714285714, x, -2.0), x, 0.0), x, 1.0), x, 0.0), x, -0.35); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 1.3714285714285714; dd = b; b = fma(a, b, -2.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 5;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 1.3714285714285714; b[1] = fma(a, b[0], -2.0); b[2] = fma(a, b[1], 0.0); b[3] = fma(a, b[2], 1.0); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
   static constexpr double kNu1 = 0.05714285714285714;
   __host__ __device__ static __forceinline__ double poly1(double x) { return fma(fma(fma(fma(fma(-0.45714285714285713, x, 2.0), x, -3.2), x, 2.0), x, 0.0), x, -0.4); }
   __host__ __device__ static __forceinline__ double dd1(double x, double a) { double dd; double b = -0.45714285714285713; dd = b; b = fma(a, b, 2.0); dd = fma(dd, x, b); b = fma(a, b, -3.2); dd = fma(dd, x, b); b = fma(a, b, 2.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD1 = 5;
+  __host__ __device__ static __forceinline__ void ddb1(double a, double* b) { b[0] = -0.45714285714285713; b[1] = fma(a, b[0], 2.0); b[2] = fma(a, b[1], -3.2); b[3] = fma(a, b[2], 2.0); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh1(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
 };
 template <> struct MeshFn<Mesh_cubic, 2> {   // A_K2
   static constexpr int kNeg = 3;
   static constexpr double kNu0 = 0.01875;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(1.2, x, -1.7142857142857142), x, 0.0), x, 0.8), x, 0.0), x, -0.23333333333333334); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 1.2; dd = b; b = fma(a, b, -1.7142857142857142); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 0.8); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 5;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 1.2; b[1] = fma(a, b[0], -1.7142857142857142); b[2] = fma(a, b[1], 0.0); b[3] = fma(a, b[2], 0.8); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
   static constexpr double kNu1 = 0.01904761904761905;
   __host__ __device__ static __forceinline__ double poly1(double x) { return fma(fma(fma(fma(fma(-0.4, x, 1.7142857142857142), x, -2.6666666666666665), x, 1.6), x, 0.0), x, -0.26666666666666666); }
   __host__ __device__ static __forceinline__ double dd1(double x, double a) { double dd; double b = -0.4; dd = b; b = fma(a, b, 1.7142857142857142); dd = fma(dd, x, b); b = fma(a, b, -2.6666666666666665); dd = fma(dd, x, b); b = fma(a, b, 1.6); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD1 = 5;
+  __host__ __device__ static __forceinline__ void ddb1(double a, double* b) { b[0] = -0.4; b[1] = fma(a, b[0], 1.7142857142857142); b[2] = fma(a, b[1], -2.6666666666666665); b[3] = fma(a, b[2], 1.6); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh1(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
 };
 template <> struct MeshFn<Mesh_cubic, 3> {   // A_W
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(9.6, x, -12.0), x, 0.0), x, 4.0), x, 0.0), x, -0.7); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 9.6; dd = b; b = fma(a, b, -12.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 4.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 5;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 9.6; b[1] = fma(a, b[0], -12.0); b[2] = fma(a, b[1], 0.0); b[3] = fma(a, b[2], 4.0); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
   static constexpr double kNu1 = 0.0;
   __host__ __device__ static __forceinline__ double poly1(double x) { return fma(fma(fma(fma(fma(-3.2, x, 12.0), x, -16.0), x, 8.0), x, 0.0), x, -0.8); }
   __host__ __device__ static __forceinline__ double dd1(double x, double a) { double dd; double b = -3.2; dd = b; b = fma(a, b, 12.0); dd = fma(dd, x, b); b = fma(a, b, -16.0); dd = fma(dd, x, b); b = fma(a, b, 8.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD1 = 5;
+  __host__ __device__ static __forceinline__ void ddb1(double a, double* b) { b[0] = -3.2; b[1] = fma(a, b[0], 12.0); b[2] = fma(a, b[1], -16.0); b[3] = fma(a, b[2], 8.0); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh1(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
 };
 template <> struct MeshFn<Mesh_cubic, 4> {   // A_L
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(48.0, x, -48.0), x, 0.0), x, 8.0); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 48.0; dd = b; b = fma(a, b, -48.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 3;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 48.0; b[1] = fma(a, b[0], -48.0); b[2] = fma(a, b[1], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); return dd; }
   static constexpr double kNu1 = 0.0;
   __host__ __device__ static __forceinline__ double poly1(double x) { return fma(fma(fma(-16.0, x, 48.0), x, -48.0), x, 16.0); }
   __host__ __device__ static __forceinline__ double dd1(double x, double a) { double dd; double b = -16.0; dd = b; b = fma(a, b, 48.0); dd = fma(dd, x, b); b = fma(a, b, -48.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD1 = 3;
+  __host__ __device__ static __forceinline__ void ddb1(double a, double* b) { b[0] = -16.0; b[1] = fma(a, b[0], 48.0); b[2] = fma(a, b[1], -48.0); }
+  __host__ __device__ static __forceinline__ double ddh1(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); return dd; }
 };
 template <> struct MeshFn<Mesh_cubic, 5> {   // A2_K2
   static constexpr int kNeg = 1;
   static constexpr double kNu0 = -0.01875;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(0.17142857142857143, x, -0.2857142857142857), x, 0.0), x, 0.2), x, 0.0), x, -0.11666666666666667), x, 0.0), x, 0.055357142857142855); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.17142857142857143; dd = b; b = fma(a, b, -0.2857142857142857); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 0.2); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -0.11666666666666667); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 7;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 0.17142857142857143; b[1] = fma(a, b[0], -0.2857142857142857); b[2] = fma(a, b[1], 0.0); b[3] = fma(a, b[2], 0.2); b[4] = fma(a, b[3], 0.0); b[5] = fma(a, b[4], -0.11666666666666667); b[6] = fma(a, b[5], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); return dd; }
   static constexpr double kNu1 = -0.01904761904761905;
   __host__ __device__ static __forceinline__ double poly1(double x) { return fma(fma(fma(fma(fma(fma(fma(-0.05714285714285714, x, 0.2857142857142857), x, -0.5333333333333333), x, 0.4), x, 0.0), x, -0.13333333333333333), x, 0.0), x, 0.05714285714285714); }
   __host__ __device__ static __forceinline__ double dd1(double x, double a) { double dd; double b = -0.05714285714285714; dd = b; b = fma(a, b, 0.2857142857142857); dd = fma(dd, x, b); b = fma(a, b, -0.5333333333333333); dd = fma(dd, x, b); b = fma(a, b, 0.4); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -0.13333333333333333); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD1 = 7;
+  __host__ __device__ static __forceinline__ void ddb1(double a, double* b) { b[0] = -0.05714285714285714; b[1] = fma(a, b[0], 0.2857142857142857); b[2] = fma(a, b[1], -0.5333333333333333); b[3] = fma(a, b[2], 0.4); b[4] = fma(a, b[3], 0.0); b[5] = fma(a, b[4], -0.13333333333333333); b[6] = fma(a, b[5], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh1(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); return dd; }
 };
 struct Mesh_w2 {
   static constexpr int kPieces = 1;
@@ -2354,36 +2390,54 @@ template <> struct MeshFn<Mesh_w2, 0> {   // A_K0
   static constexpr double kNu0 = 0.25;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(0.75, x, -3.75), x, 7.0), x, -5.25), x, 0.0), x, 1.75), x, 0.0), x, -0.75); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.75; dd = b; b = fma(a, b, -3.75); dd = fma(dd, x, b); b = fma(a, b, 7.0); dd = fma(dd, x, b); b = fma(a, b, -5.25); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1.75); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 7;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 0.75; b[1] = fma(a, b[0], -3.75); b[2] = fma(a, b[1], 7.0); b[3] = fma(a, b[2], -5.25); b[4] = fma(a, b[3], 0.0); b[5] = fma(a, b[4], 1.75); b[6] = fma(a, b[5], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); return dd; }
 };
 template <> struct MeshFn<Mesh_w2, 1> {   // A_K1
   static constexpr int kNeg = 2;
   static constexpr double kNu0 = 0.052083333333333336;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(0.6666666666666666, x, -3.28125), x, 6.0), x, -4.375), x, 0.0), x, 1.3125), x, 0.0), x, -0.375); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.6666666666666666; dd = b; b = fma(a, b, -3.28125); dd = fma(dd, x, b); b = fma(a, b, 6.0); dd = fma(dd, x, b); b = fma(a, b, -4.375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1.3125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 7;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 0.6666666666666666; b[1] = fma(a, b[0], -3.28125); b[2] = fma(a, b[1], 6.0); b[3] = fma(a, b[2], -4.375); b[4] = fma(a, b[3], 0.0); b[5] = fma(a, b[4], 1.3125); b[6] = fma(a, b[5], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); return dd; }
 };
 template <> struct MeshFn<Mesh_w2, 2> {   // A_K2
   static constexpr int kNeg = 3;
   static constexpr double kNu0 = 0.016666666666666666;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(0.6, x, -2.9166666666666665), x, 5.25), x, -3.75), x, 0.0), x, 1.05), x, 0.0), x, -0.25); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.6; dd = b; b = fma(a, b, -2.9166666666666665); dd = fma(dd, x, b); b = fma(a, b, 5.25); dd = fma(dd, x, b); b = fma(a, b, -3.75); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1.05); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 7;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 0.6; b[1] = fma(a, b[0], -2.9166666666666665); b[2] = fma(a, b[1], 5.25); b[3] = fma(a, b[2], -3.75); b[4] = fma(a, b[3], 0.0); b[5] = fma(a, b[4], 1.05); b[6] = fma(a, b[5], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); return dd; }
 };
 template <> struct MeshFn<Mesh_w2, 3> {   // A_W
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(6.0, x, -26.25), x, 42.0), x, -26.25), x, 0.0), x, 5.25), x, 0.0), x, -0.75); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 6.0; dd = b; b = fma(a, b, -26.25); dd = fma(dd, x, b); b = fma(a, b, 42.0); dd = fma(dd, x, b); b = fma(a, b, -26.25); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 5.25); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 7;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 6.0; b[1] = fma(a, b[0], -26.25); b[2] = fma(a, b[1], 42.0); b[3] = fma(a, b[2], -26.25); b[4] = fma(a, b[3], 0.0); b[5] = fma(a, b[4], 5.25); b[6] = fma(a, b[5], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); return dd; }
 };
 template <> struct MeshFn<Mesh_w2, 4> {   // A_L
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(42.0, x, -157.5), x, 210.0), x, -105.0), x, 0.0), x, 10.5); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 42.0; dd = b; b = fma(a, b, -157.5); dd = fma(dd, x, b); b = fma(a, b, 210.0); dd = fma(dd, x, b); b = fma(a, b, -105.0); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 5;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 42.0; b[1] = fma(a, b[0], -157.5); b[2] = fma(a, b[1], 210.0); b[3] = fma(a, b[2], -105.0); b[4] = fma(a, b[3], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); return dd; }
 };
 template <> struct MeshFn<Mesh_w2, 5> {   // A2_K2
   static constexpr int kNeg = 1;
   static constexpr double kNu0 = -0.016666666666666666;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(0.06666666666666667, x, -0.3645833333333333), x, 0.75), x, -0.625), x, 0.0), x, 0.2625), x, 0.0), x, -0.125), x, 0.0), x, 0.052083333333333336); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.06666666666666667; dd = b; b = fma(a, b, -0.3645833333333333); dd = fma(dd, x, b); b = fma(a, b, 0.75); dd = fma(dd, x, b); b = fma(a, b, -0.625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 0.2625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -0.125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 9;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 0.06666666666666667; b[1] = fma(a, b[0], -0.3645833333333333); b[2] = fma(a, b[1], 0.75); b[3] = fma(a, b[2], -0.625); b[4] = fma(a, b[3], 0.0); b[5] = fma(a, b[4], 0.2625); b[6] = fma(a, b[5], 0.0); b[7] = fma(a, b[6], -0.125); b[8] = fma(a, b[7], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); return dd; }
 };
 struct Mesh_w4 {
   static constexpr int kPieces = 1;
@@ -2395,36 +2449,54 @@ template <> struct MeshFn<Mesh_w4, 0> {   // A_K0
   static constexpr double kNu0 = 0.25;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.640625, x, -11.0), x, 30.078125), x, -41.25), x, 25.78125), x, 0.0), x, -7.21875), x, 0.0), x, 2.578125), x, 0.0), x, -0.859375); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 1.640625; dd = b; b = fma(a, b, -11.0); dd = fma(dd, x, b); b = fma(a, b, 30.078125); dd = fma(dd, x, b); b = fma(a, b, -41.25); dd = fma(dd, x, b); b = fma(a, b, 25.78125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -7.21875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 2.578125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 10;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 1.640625; b[1] = fma(a, b[0], -11.0); b[2] = fma(a, b[1], 30.078125); b[3] = fma(a, b[2], -41.25); b[4] = fma(a, b[3], 25.78125); b[5] = fma(a, b[4], 0.0); b[6] = fma(a, b[5], -7.21875); b[7] = fma(a, b[6], 0.0); b[8] = fma(a, b[7], 2.578125); b[9] = fma(a, b[8], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); return dd; }
 };
 template <> struct MeshFn<Mesh_w4, 1> {   // A_K1
   static constexpr int kNeg = 2;
   static constexpr double kNu0 = 0.045572916666666664;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.50390625, x, -10.0), x, 27.0703125), x, -36.666666666666664), x, 22.55859375), x, 0.0), x, -6.015625), x, 0.0), x, 1.93359375), x, 0.0), x, -0.4296875); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 1.50390625; dd = b; b = fma(a, b, -10.0); dd = fma(dd, x, b); b = fma(a, b, 27.0703125); dd = fma(dd, x, b); b = fma(a, b, -36.666666666666664); dd = fma(dd, x, b); b = fma(a, b, 22.55859375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -6.015625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1.93359375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 10;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 1.50390625; b[1] = fma(a, b[0], -10.0); b[2] = fma(a, b[1], 27.0703125); b[3] = fma(a, b[2], -36.666666666666664); b[4] = fma(a, b[3], 22.55859375); b[5] = fma(a, b[4], 0.0); b[6] = fma(a, b[5], -6.015625); b[7] = fma(a, b[6], 0.0); b[8] = fma(a, b[7], 1.93359375); b[9] = fma(a, b[8], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); return dd; }
 };
 template <> struct MeshFn<Mesh_w4, 2> {   // A_K2
   static constexpr int kNeg = 3;
   static constexpr double kNu0 = 0.01282051282051282;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(1.3882211538461537, x, -9.166666666666666), x, 24.609375), x, -33.0), x, 20.052083333333332), x, 0.0), x, -5.15625), x, 0.0), x, 1.546875), x, 0.0), x, -0.2864583333333333); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 1.3882211538461537; dd = b; b = fma(a, b, -9.166666666666666); dd = fma(dd, x, b); b = fma(a, b, 24.609375); dd = fma(dd, x, b); b = fma(a, b, -33.0); dd = fma(dd, x, b); b = fma(a, b, 20.052083333333332); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -5.15625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1.546875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 10;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 1.3882211538461537; b[1] = fma(a, b[0], -9.166666666666666); b[2] = fma(a, b[1], 24.609375); b[3] = fma(a, b[2], -33.0); b[4] = fma(a, b[3], 20.052083333333332); b[5] = fma(a, b[4], 0.0); b[6] = fma(a, b[5], -5.15625); b[7] = fma(a, b[6], 0.0); b[8] = fma(a, b[7], 1.546875); b[9] = fma(a, b[8], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); return dd; }
 };
 template <> struct MeshFn<Mesh_w4, 3> {   // A_W
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(18.046875, x, -110.0), x, 270.703125), x, -330.0), x, 180.46875), x, 0.0), x, -36.09375), x, 0.0), x, 7.734375), x, 0.0), x, -0.859375); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 18.046875; dd = b; b = fma(a, b, -110.0); dd = fma(dd, x, b); b = fma(a, b, 270.703125); dd = fma(dd, x, b); b = fma(a, b, -330.0); dd = fma(dd, x, b); b = fma(a, b, 180.46875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -36.09375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 7.734375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 10;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 18.046875; b[1] = fma(a, b[0], -110.0); b[2] = fma(a, b[1], 270.703125); b[3] = fma(a, b[2], -330.0); b[4] = fma(a, b[3], 180.46875); b[5] = fma(a, b[4], 0.0); b[6] = fma(a, b[5], -36.09375); b[7] = fma(a, b[6], 0.0); b[8] = fma(a, b[7], 7.734375); b[9] = fma(a, b[8], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); return dd; }
 };
 template <> struct MeshFn<Mesh_w4, 4> {   // A_L
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(180.46875, x, -990.0), x, 2165.625), x, -2310.0), x, 1082.8125), x, 0.0), x, -144.375), x, 0.0), x, 15.46875); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 180.46875; dd = b; b = fma(a, b, -990.0); dd = fma(dd, x, b); b = fma(a, b, 2165.625); dd = fma(dd, x, b); b = fma(a, b, -2310.0); dd = fma(dd, x, b); b = fma(a, b, 1082.8125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -144.375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 8;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 180.46875; b[1] = fma(a, b[0], -990.0); b[2] = fma(a, b[1], 2165.625); b[3] = fma(a, b[2], -2310.0); b[4] = fma(a, b[3], 1082.8125); b[5] = fma(a, b[4], 0.0); b[6] = fma(a, b[5], -144.375); b[7] = fma(a, b[6], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); return dd; }
 };
 template <> struct MeshFn<Mesh_w4, 5> {   // A2_K2
   static constexpr int kNeg = 1;
   static constexpr double kNu0 = -0.01282051282051282;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.11568509615384616, x, -0.8333333333333334), x, 2.4609375), x, -3.6666666666666665), x, 2.5065104166666665), x, 0.0), x, -0.859375), x, 0.0), x, 0.38671875), x, 0.0), x, -0.14322916666666666), x, 0.0), x, 0.045572916666666664); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.11568509615384616; dd = b; b = fma(a, b, -0.8333333333333334); dd = fma(dd, x, b); b = fma(a, b, 2.4609375); dd = fma(dd, x, b); b = fma(a, b, -3.6666666666666665); dd = fma(dd, x, b); b = fma(a, b, 2.5065104166666665); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -0.859375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 0.38671875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -0.14322916666666666); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 12;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 0.11568509615384616; b[1] = fma(a, b[0], -0.8333333333333334); b[2] = fma(a, b[1], 2.4609375); b[3] = fma(a, b[2], -3.6666666666666665); b[4] = fma(a, b[3], 2.5065104166666665); b[5] = fma(a, b[4], 0.0); b[6] = fma(a, b[5], -0.859375); b[7] = fma(a, b[6], 0.0); b[8] = fma(a, b[7], 0.38671875); b[9] = fma(a, b[8], 0.0); b[10] = fma(a, b[9], -0.14322916666666666); b[11] = fma(a, b[10], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); dd = fma(dd, x, b[10]); dd = fma(dd, x, b[11]); return dd; }
 };
 struct Mesh_w6 {
   static constexpr int kPieces = 1;
@@ -2436,36 +2508,54 @@ template <> struct MeshFn<Mesh_w6, 0> {   // A_K0
   static constexpr double kNu0 = 0.25;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(3.75, x, -31.58203125), x, 113.75), x, -223.9453125), x, 250.25), x, -136.85546875), x, 0.0), x, 33.515625), x, 0.0), x, -11.73046875), x, 0.0), x, 3.5546875), x, 0.0), x, -0.95703125); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 3.75; dd = b; b = fma(a, b, -31.58203125); dd = fma(dd, x, b); b = fma(a, b, 113.75); dd = fma(dd, x, b); b = fma(a, b, -223.9453125); dd = fma(dd, x, b); b = fma(a, b, 250.25); dd = fma(dd, x, b); b = fma(a, b, -136.85546875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 33.515625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -11.73046875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 3.5546875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 13;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 3.75; b[1] = fma(a, b[0], -31.58203125); b[2] = fma(a, b[1], 113.75); b[3] = fma(a, b[2], -223.9453125); b[4] = fma(a, b[3], 250.25); b[5] = fma(a, b[4], -136.85546875); b[6] = fma(a, b[5], 0.0); b[7] = fma(a, b[6], 33.515625); b[8] = fma(a, b[7], 0.0); b[9] = fma(a, b[8], -11.73046875); b[10] = fma(a, b[9], 0.0); b[11] = fma(a, b[10], 3.5546875); b[12] = fma(a, b[11], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); dd = fma(dd, x, b[10]); dd = fma(dd, x, b[11]); dd = fma(dd, x, b[12]); return dd; }
 };
 template <> struct MeshFn<Mesh_w6, 1> {   // A_K1
   static constexpr int kNeg = 2;
   static constexpr double kNu0 = 0.041015625;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(3.5, x, -29.326171875), x, 105.0), x, -205.283203125), x, 227.5), x, -123.169921875), x, 0.0), x, 29.326171875), x, 0.0), x, -9.775390625), x, 0.0), x, 2.666015625), x, 0.0), x, -0.478515625); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 3.5; dd = b; b = fma(a, b, -29.326171875); dd = fma(dd, x, b); b = fma(a, b, 105.0); dd = fma(dd, x, b); b = fma(a, b, -205.283203125); dd = fma(dd, x, b); b = fma(a, b, 227.5); dd = fma(dd, x, b); b = fma(a, b, -123.169921875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 29.326171875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -9.775390625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 2.666015625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 13;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 3.5; b[1] = fma(a, b[0], -29.326171875); b[2] = fma(a, b[1], 105.0); b[3] = fma(a, b[2], -205.283203125); b[4] = fma(a, b[3], 227.5); b[5] = fma(a, b[4], -123.169921875); b[6] = fma(a, b[5], 0.0); b[7] = fma(a, b[6], 29.326171875); b[8] = fma(a, b[7], 0.0); b[9] = fma(a, b[8], -9.775390625); b[10] = fma(a, b[9], 0.0); b[11] = fma(a, b[10], 2.666015625); b[12] = fma(a, b[11], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); dd = fma(dd, x, b[10]); dd = fma(dd, x, b[11]); dd = fma(dd, x, b[12]); return dd; }
 };
 template <> struct MeshFn<Mesh_w6, 2> {   // A_K2
   static constexpr int kNeg = 3;
   static constexpr double kNu0 = 0.010416666666666666;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(3.28125, x, -27.37109375), x, 97.5), x, -189.4921875), x, 208.54166666666666), x, -111.97265625), x, 0.0), x, 26.067708333333332), x, 0.0), x, -8.37890625), x, 0.0), x, 2.1328125), x, 0.0), x, -0.3190104166666667); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 3.28125; dd = b; b = fma(a, b, -27.37109375); dd = fma(dd, x, b); b = fma(a, b, 97.5); dd = fma(dd, x, b); b = fma(a, b, -189.4921875); dd = fma(dd, x, b); b = fma(a, b, 208.54166666666666); dd = fma(dd, x, b); b = fma(a, b, -111.97265625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 26.067708333333332); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -8.37890625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 2.1328125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 13;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 3.28125; b[1] = fma(a, b[0], -27.37109375); b[2] = fma(a, b[1], 97.5); b[3] = fma(a, b[2], -189.4921875); b[4] = fma(a, b[3], 208.54166666666666); b[5] = fma(a, b[4], -111.97265625); b[6] = fma(a, b[5], 0.0); b[7] = fma(a, b[6], 26.067708333333332); b[8] = fma(a, b[7], 0.0); b[9] = fma(a, b[8], -8.37890625); b[10] = fma(a, b[9], 0.0); b[11] = fma(a, b[10], 2.1328125); b[12] = fma(a, b[11], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); dd = fma(dd, x, b[10]); dd = fma(dd, x, b[11]); dd = fma(dd, x, b[12]); return dd; }
 };
 template <> struct MeshFn<Mesh_w6, 3> {   // A_W
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(52.5, x, -410.56640625), x, 1365.0), x, -2463.3984375), x, 2502.5), x, -1231.69921875), x, 0.0), x, 234.609375), x, 0.0), x, -58.65234375), x, 0.0), x, 10.6640625), x, 0.0), x, -0.95703125); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 52.5; dd = b; b = fma(a, b, -410.56640625); dd = fma(dd, x, b); b = fma(a, b, 1365.0); dd = fma(dd, x, b); b = fma(a, b, -2463.3984375); dd = fma(dd, x, b); b = fma(a, b, 2502.5); dd = fma(dd, x, b); b = fma(a, b, -1231.69921875); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 234.609375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -58.65234375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 10.6640625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 13;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 52.5; b[1] = fma(a, b[0], -410.56640625); b[2] = fma(a, b[1], 1365.0); b[3] = fma(a, b[2], -2463.3984375); b[4] = fma(a, b[3], 2502.5); b[5] = fma(a, b[4], -1231.69921875); b[6] = fma(a, b[5], 0.0); b[7] = fma(a, b[6], 234.609375); b[8] = fma(a, b[7], 0.0); b[9] = fma(a, b[8], -58.65234375); b[10] = fma(a, b[9], 0.0); b[11] = fma(a, b[10], 10.6640625); b[12] = fma(a, b[11], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); dd = fma(dd, x, b[10]); dd = fma(dd, x, b[11]); dd = fma(dd, x, b[12]); return dd; }
 };
 template <> struct MeshFn<Mesh_w6, 4> {   // A_L
   static constexpr int kNeg = 0;
   static constexpr double kNu0 = 0.0;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(682.5, x, -4926.796875), x, 15015.0), x, -24633.984375), x, 22522.5), x, -9853.59375), x, 0.0), x, 1407.65625), x, 0.0), x, -234.609375), x, 0.0), x, 21.328125); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 682.5; dd = b; b = fma(a, b, -4926.796875); dd = fma(dd, x, b); b = fma(a, b, 15015.0); dd = fma(dd, x, b); b = fma(a, b, -24633.984375); dd = fma(dd, x, b); b = fma(a, b, 22522.5); dd = fma(dd, x, b); b = fma(a, b, -9853.59375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 1407.65625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -234.609375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 11;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 682.5; b[1] = fma(a, b[0], -4926.796875); b[2] = fma(a, b[1], 15015.0); b[3] = fma(a, b[2], -24633.984375); b[4] = fma(a, b[3], 22522.5); b[5] = fma(a, b[4], -9853.59375); b[6] = fma(a, b[5], 0.0); b[7] = fma(a, b[6], 1407.65625); b[8] = fma(a, b[7], 0.0); b[9] = fma(a, b[8], -234.609375); b[10] = fma(a, b[9], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); dd = fma(dd, x, b[10]); return dd; }
 };
 template <> struct MeshFn<Mesh_w6, 5> {   // A2_K2
   static constexpr int kNeg = 1;
   static constexpr double kNu0 = -0.010416666666666666;
   __host__ __device__ static __forceinline__ double poly0(double x) { return fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(fma(0.21875, x, -1.955078125), x, 7.5), x, -15.791015625), x, 18.958333333333332), x, -11.197265625), x, 0.0), x, 3.2584635416666665), x, 0.0), x, -1.396484375), x, 0.0), x, 0.533203125), x, 0.0), x, -0.15950520833333334), x, 0.0), x, 0.041015625); }
   __host__ __device__ static __forceinline__ double dd0(double x, double a) { double dd; double b = 0.21875; dd = b; b = fma(a, b, -1.955078125); dd = fma(dd, x, b); b = fma(a, b, 7.5); dd = fma(dd, x, b); b = fma(a, b, -15.791015625); dd = fma(dd, x, b); b = fma(a, b, 18.958333333333332); dd = fma(dd, x, b); b = fma(a, b, -11.197265625); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 3.2584635416666665); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -1.396484375); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, 0.533203125); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); b = fma(a, b, -0.15950520833333334); dd = fma(dd, x, b); b = fma(a, b, 0.0); dd = fma(dd, x, b); return dd; }
+  static constexpr int kDD0 = 15;
+  __host__ __device__ static __forceinline__ void ddb0(double a, double* b) { b[0] = 0.21875; b[1] = fma(a, b[0], -1.955078125); b[2] = fma(a, b[1], 7.5); b[3] = fma(a, b[2], -15.791015625); b[4] = fma(a, b[3], 18.958333333333332); b[5] = fma(a, b[4], -11.197265625); b[6] = fma(a, b[5], 0.0); b[7] = fma(a, b[6], 3.2584635416666665); b[8] = fma(a, b[7], 0.0); b[9] = fma(a, b[8], -1.396484375); b[10] = fma(a, b[9], 0.0); b[11] = fma(a, b[10], 0.533203125); b[12] = fma(a, b[11], 0.0); b[13] = fma(a, b[12], -0.15950520833333334); b[14] = fma(a, b[13], 0.0); }
+  __host__ __device__ static __forceinline__ double ddh0(double x, const double* b) { double dd = b[0]; dd = fma(dd, x, b[1]); dd = fma(dd, x, b[2]); dd = fma(dd, x, b[3]); dd = fma(dd, x, b[4]); dd = fma(dd, x, b[5]); dd = fma(dd, x, b[6]); dd = fma(dd, x, b[7]); dd = fma(dd, x, b[8]); dd = fma(dd, x, b[9]); dd = fma(dd, x, b[10]); dd = fma(dd, x, b[11]); dd = fma(dd, x, b[12]); dd = fma(dd, x, b[13]); dd = fma(dd, x, b[14]); return dd; }
 };
 
 // ---- 2-D conditioned triangles: pi W and rho = -pi W'/r per piece (unit support)

@@ -357,6 +357,28 @@ __device__ __forceinline__ double fdd(int p, double x, double a) {
   }
   return MeshFn<M, Fn>::dd0(x, a);
 }
+// the divided difference fdd in two halves: the synthetic-division coefficients of piece p at a (kMeshDD slots), and
+// Horner's rule over them at x -- the same fma sequence as fdd, so the same value
+constexpr int kMeshDD = 24;
+template <class M, int Fn>
+__device__ __forceinline__ void fddb(int p, double a, double* b) {
+  static_assert(MeshFn<M, Fn>::kDD0 <= kMeshDD, "coefficient slots");
+  if constexpr (M::kPieces > 1) {
+    static_assert(MeshFn<M, Fn>::kDD1 <= kMeshDD, "coefficient slots");
+    if (p) {
+      MeshFn<M, Fn>::ddb1(a, b);
+      return;
+    }
+  }
+  MeshFn<M, Fn>::ddb0(a, b);
+}
+template <class M, int Fn>
+__device__ __forceinline__ double fddh(int p, double x, const double* b) {
+  if constexpr (M::kPieces > 1) {
+    if (p) return MeshFn<M, Fn>::ddh1(x, b);
+  }
+  return MeshFn<M, Fn>::ddh0(x, b);
+}
 template <class M, int Fn>
 __device__ __forceinline__ double fnu(int p) {
   if constexpr (M::kPieces > 1) {
@@ -418,12 +440,12 @@ struct Node {
 // nu r^-m gives -nu S_m(r, a) / (r^m a^m), whose 1 / a^m is absorbed by z^ZP.  Across the knot B the two pieces'
 // differences are weighted by (B - a) and (r - B) over r - a = rho^2 / (r + a).
 template <class M, int Fn, int ZP>
-__device__ __forceinline__ double dd2(const Node& nd, double a, double z, double sg) {
+__device__ __forceinline__ double dd2(const Node& nd, double a, double z, double sg, const double* fb) {
   constexpr int m = MeshFn<M, Fn>::kNeg;
   static_assert(ZP >= m, "z power must absorb the negative power");
   const int pa = piece<M>(a);
   if (!nd.split) {
-    double d0 = fdd<M, Fn>(pa, nd.r, a) * zpow<ZP>(z);
+    double d0 = fddh<M, Fn>(pa, nd.r, fb + Fn * kMeshDD) * zpow<ZP>(z);
     if constexpr (m > 0) d0 -= fnu<M, Fn>(pa) * smix<m>(nd.r, a) * zpow<m>(nd.ir) * zpow<ZP - m>(z) * zpow<m>(sg);
     return d0 * nd.irpa;
   }
@@ -464,7 +486,7 @@ struct EdgeSums {
 // ms with a loop for each)
 template <class M>
 __device__ __forceinline__ void node_eval_dd(double u, double wt, double c2, double a, double z, double sg, double w,
-                                             EdgeSums& S) {
+                                             const double* fb, EdgeSums& S) {
   const double rho2 = fma(u, u, w * w);
   Node nd;
   nd.r = sqrt(fma(u, u, c2));
@@ -473,12 +495,12 @@ __device__ __forceinline__ void node_eval_dd(double u, double wt, double c2, dou
   nd.irpa = 1.0 / (nd.r + a);
   nd.irho2 = nd.split ? 1.0 / rho2 : 0.0;
   const double ww = w * wt;
-  S.J[0] = fma(ww, dd2<M, 0, 1>(nd, a, z, sg), S.J[0]);
-  S.J[1] = fma(ww, dd2<M, 1, 2>(nd, a, z, sg), S.J[1]);
-  S.J[2] = fma(ww, dd2<M, 2, 3>(nd, a, z, sg), S.J[2]);
-  S.J[3] = fma(ww, dd2<M, 3, 0>(nd, a, z, sg), S.J[3]);
-  S.J[4] = fma(ww, dd2<M, 4, 0>(nd, a, z, sg), S.J[4]);
-  S.J[5] = fma(ww, dd2<M, 5, 1>(nd, a, z, sg), S.J[5]);
+  S.J[0] = fma(ww, dd2<M, 0, 1>(nd, a, z, sg, fb), S.J[0]);
+  S.J[1] = fma(ww, dd2<M, 1, 2>(nd, a, z, sg, fb), S.J[1]);
+  S.J[2] = fma(ww, dd2<M, 2, 3>(nd, a, z, sg, fb), S.J[2]);
+  S.J[3] = fma(ww, dd2<M, 3, 0>(nd, a, z, sg, fb), S.J[3]);
+  S.J[4] = fma(ww, dd2<M, 4, 0>(nd, a, z, sg, fb), S.J[4]);
+  S.J[5] = fma(ww, dd2<M, 5, 1>(nd, a, z, sg, fb), S.J[5]);
 }
 
 template <class M>
@@ -637,7 +659,7 @@ __device__ __forceinline__ double face_term_j(const AccSlot& sl, const double N[
 // the candidate search visits only faces within the support.  q in world units, ih = 1 / support.
 template <class M>
 __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], double ih, PanelList* PL3,
-                                  EdgeGeo* G3, int lane, const AccSlot& slot, double& acc) {
+                                  EdgeGeo* G3, double* FB, int lane, const AccSlot& slot, double& acc) {
   const double* F = Mv.fdata + (int64_t)f * kFaceDoubles;
   double P[3][3];
 #pragma unroll
@@ -675,6 +697,16 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
     ge.s0 = s0;
     ge.s1 = s1;
     ge.np = s1 > s0 ? build_panels<M>(PL3[e], s0, s1, c) : 0;
+  } else if (lane == 3) {
+    // the synthetic-division coefficients of the six divided differences at a = |z| (a face constant), once per face
+    // instead of once per node
+    const int pa = piece<M>(a);
+    fddb<M, 0>(pa, a, FB);
+    fddb<M, 1>(pa, a, FB + kMeshDD);
+    fddb<M, 2>(pa, a, FB + 2 * kMeshDD);
+    fddb<M, 3>(pa, a, FB + 3 * kMeshDD);
+    fddb<M, 4>(pa, a, FB + 4 * kMeshDD);
+    fddb<M, 5>(pa, a, FB + 5 * kMeshDD);
   }
   __syncwarp();
   double Jf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};          // the face's J sums over its edges
@@ -699,7 +731,7 @@ __device__ void face_contrib_warp(const MeshView& Mv, int f, const double q[3], 
         const double x0 = PL.lo[p], x1 = PL.hi[p];
         const double hc = 0.5 * (x1 - x0);
         const double u = fma(hc, xg, 0.5 * (x1 + x0)), wt = wg * hc;
-        if (w != 0.0) node_eval_dd<M>(u, wt, c2, a, z, sg, w, S);
+        if (w != 0.0) node_eval_dd<M>(u, wt, c2, a, z, sg, w, FB, S);
         node_eval_pot<M>(u, wt, PL.sg[p], c2, z, S);
       }
       double v[12] = {S.J[0], S.J[1], S.J[2], S.J[3], S.J[4], S.J[5], S.LK1, S.LK2, S.LK2b, S.TK2, S.LW, S.LL};
@@ -886,10 +918,11 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_rows(const double* __rest
 
 // one warp per work row; warps take rows from a counter (rows differ in their number of faces), and the row's
 // result does not depend on which warp computes it
-// 3 resident CTAs per SM (at most 168 registers a thread, some spills): the c3 leg measured 9.0 ms on B200 against
-// 9.9 ms with 2 CTAs (no cap) and 10.2 ms with 4 (128 registers, more spills)
+// 4 resident CTAs per SM (at most 128 registers a thread): with the divided-difference coefficients formed once per
+// face the c3 leg measured 8.14 ms on B200 against 8.26 ms with 3 CTAs (before that change 3 CTAs were best: 9.0 ms
+// against 9.9 ms with 2 and 10.2 ms with 4)
 #ifndef WSB_MESH_MIN_BLOCKS
-#define WSB_MESH_MIN_BLOCKS 3
+#define WSB_MESH_MIN_BLOCKS 4
 #endif
 template <class M>
 __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval(MeshView Mv, const double* __restrict__ pos,
@@ -900,6 +933,7 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
                                                            int32_t* __restrict__ grab, double* __restrict__ out) {
   __shared__ PanelList pl[kMeshThreads / 32][3];
   __shared__ EdgeGeo eg[kMeshThreads / 32][3];
+  __shared__ double fb[kMeshThreads / 32][6 * kMeshDD];
   __shared__ double acc[kMeshThreads / 32][28];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const AccSlot aslot = acc_slot(lane);                  // the accumulator this lane assembles
@@ -913,7 +947,9 @@ __global__ void __launch_bounds__(kMeshThreads, WSB_MESH_MIN_BLOCKS) k_mesh_eval
     const double q[3] = {pos[3 * row], pos[3 * row + 1], pos[3 * row + 2]};
     const double h = sup[row], ih = 1.0 / h;
     double mine = 0.0;                                   // accumulator `lane` of the row (lanes < 28)
-    for_candidates_warp(Mv, q, h, lane, [&](int f) { face_contrib_warp<M>(Mv, f, q, ih, pl[wib], eg[wib], lane, aslot, mine); });
+    for_candidates_warp(Mv, q, h, lane, [&](int f) {
+      face_contrib_warp<M>(Mv, f, q, ih, pl[wib], eg[wib], fb[wib], lane, aslot, mine);
+    });
     if (lane < 28) acc[wib][lane] = mine;
     __syncwarp();
     if (lane == 0) {

@@ -866,6 +866,21 @@ def emit_mesh() -> list:
                 out.append(f"  __host__ __device__ static __forceinline__ double poly{p}(double x) {{ return {_horner(poly, 'x')}; }}")
                 body = " ".join(_emit_dd(poly, "x", "a"))
                 out.append(f"  __host__ __device__ static __forceinline__ double dd{p}(double x, double a) {{ double dd; {body} return dd; }}")
+                # the same divided difference in two halves: the synthetic-division coefficients b (they depend on a
+                # only, so a caller forms them once per a) and Horner's rule over b at x -- the same fma sequence
+                cs = list(poly)
+                while len(cs) > 1 and cs[-1] == 0:
+                    cs.pop()
+                D = len(cs) - 1
+                out.append(f"  static constexpr int kDD{p} = {max(D, 0)};")
+                if D >= 1:
+                    bs = [f"b[0] = {_lit(cs[D])};"] + [f"b[{k}] = fma(a, b[{k - 1}], {_lit(cs[D - k])});"
+                                                       for k in range(1, D)]
+                    hs = ["double dd = b[0];"] + [f"dd = fma(dd, x, b[{k}]);" for k in range(1, D)]
+                else:
+                    bs, hs = [], ["double dd = 0.0;"]
+                out.append(f"  __host__ __device__ static __forceinline__ void ddb{p}(double a, double* b) {{ {' '.join(bs)} }}")
+                out.append(f"  __host__ __device__ static __forceinline__ double ddh{p}(double x, const double* b) {{ {' '.join(hs)} return dd; }}")
             out.append("};")
     out.append("")
     return out
