@@ -818,7 +818,10 @@ __global__ void __launch_bounds__(kMeshThreads) k_mesh_rowinfo(MeshView M, const
       const int cx = cell_coord(q[0], M.lo0, M.cell, M.nx), cy = cell_coord(q[1], M.lo1, M.cell, M.ny),
                 cz = cell_coord(q[2], M.lo2, M.cell, M.nz);
       const bool in_grid = cx >= 0 && cy >= 0 && cz >= 0 && cx < M.nx && cy < M.ny && cz < M.nz;
-      const uint8_t f = in_grid ? M.cflag[((int64_t)cz * M.ny + cy) * M.nx + cx] : (uint8_t)kCellNear;
+      // more than a cell outside the grid along some axis (cell_coord gives -2 or n + 1): the grid reaches a cell
+      // (>= the support) past the surface's box, so no face is within the support and the query is outside the solid
+      const bool far = cx == -2 || cy == -2 || cz == -2 || cx == M.nx + 1 || cy == M.ny + 1 || cz == M.nz + 1;
+      const uint8_t f = in_grid ? M.cflag[((int64_t)cz * M.ny + cy) * M.nx + cx] : (uint8_t)(far ? 0 : kCellNear);
       if (!(f & kCellNear)) {
         ind[row] = (f & kCellInside) ? 1 : 0;     // no face box in the 27 cells: the cell is empty as well
       } else {
