@@ -208,7 +208,7 @@ class Clocks:
 
 
 # ----------------------------------------------------------------------------------------------- serving stream
-def serving_run(n_requests, dev, pair_density, seed=0, start_load=0.9, max_streams=5):
+def serving_run(n_requests, dev, pair_density, seed=0, start_load=0.9, max_streams=6):
     """Poisson stream of boundary queries over 32 resident scenes: 16 of the large 2-D kind (64 star polygons each,
     h = 0.02) and 16 of the 3-D kind, as the 3-D configuration has them: 8 closed icospheres of 20480 faces (radius
     U(0.3, 0.8), 5 % jitter, h = 0.03) and 8 solid-sphere scenes whose requests are (query, sphere) rows (radii
@@ -330,7 +330,7 @@ def serving_run(n_requests, dev, pair_density, seed=0, start_load=0.9, max_strea
     _, _, warm = stream(start_load, n_requests)
     # the arrival rate is chosen so the device is 80-90 % busy: the first measured stream runs at start_load of the
     # burst capacity; while a stream leaves the device outside that window, the next one's rate is scaled by the busy
-    # fraction towards 84 % (at most 4x a step, max_streams streams in all).  The burst's capacity is only a starting point: with several streams and
+    # fraction towards 84 % (at most 6x a step, max_streams streams in all).  The burst's capacity is only a starting point: with several streams and
     # the host issuing one batch at a time it understates what the device absorbs under a stream.
     tried = []
     load = start_load
@@ -344,7 +344,7 @@ def serving_run(n_requests, dev, pair_density, seed=0, start_load=0.9, max_strea
             break
         # busy is close to proportional to the arrival rate below saturation; above 90 % the queue grows (an overloaded
         # stream's latencies say nothing of the server), so the rate comes down again
-        load *= min(4.0, 0.84 / max(busy, 0.05))
+        load *= min(6.0, 0.84 / max(busy, 0.05))
     rows_total = sum(r for _, r, _, _ in specs)
     rows_2d = sum(r for sid, r, _, _ in specs if sid.startswith("scene"))
     return {"requests": n_requests, "scenes": 32, "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"),
