@@ -171,3 +171,26 @@ def test_tetrahedral_mesh_equals_its_surface():
     for k in range(len(Qc)):
         ref = M3.channels(cube.vertices, cube.faces, Qc[k], hc[k], "w2")
         assert np.abs(got[k] - ref).max() / (1 + np.abs(ref).max()) < 1e-8
+
+
+def test_queries_outside_the_face_grid():
+    """queries beyond the surface's box along each axis, from within the support (0.1) to several cells out (0.3 /
+    0.6: at and past the grid's one-cell margin; 2.0: settled by the first row pass as outside with no face in reach):
+    all outside, channels equal to the oracle (zero beyond the support)."""
+    from warpsphboundaries_b200 import workloads as W
+    V, Fc = W.box_mesh((-1, -1, -1), (1, 1, 1))
+    Q = []
+    for axis in range(3):
+        for sign in (-1.0, 1.0):
+            for d in (0.1, 0.3, 0.6, 2.0):
+                q = np.array([0.13, -0.07, 0.21])
+                q[axis] = sign * (1.0 + d)
+                Q.append(q)
+    Q = np.array(Q)
+    got, ind = _run(V, Fc, Q, 0.25, "w4")
+    assert (ind == 0).all()
+    for k, q in enumerate(Q):
+        ref = M3.channels(V, Fc, q, 0.25, "w4")
+        assert np.abs(got[k] - ref).max() < 1e-10 * (1 + np.abs(ref).max()), k
+    far = np.abs(Q).max(axis=1) > 1.25
+    assert np.abs(got[far]).max() == 0.0 and np.abs(got[~far]).max() > 0.0
